@@ -1,0 +1,127 @@
+/*
+ * astr_b200.h — C ABI of the B200 (sm_100a) implementation of ASTR's per-step RHS hot path.
+ *
+ * Every entry point is extern "C", takes plain pointers and sizes, returns an int status
+ * (ASTR_OK = 0, negative on error, never aborts) and records a message readable through
+ * astr_last_error(). Arrays crossing the boundary are Fortran-ordered (first index fastest)
+ * with explicit lower bounds, so a Fortran caller passes c_loc(f(lb0,lb1,lb2)) together with
+ * shape(f) and lbound(f). `where` says whether a pointer is host (ASTR_HOST) or device
+ * (ASTR_DEVICE) memory; host pointers are only borrowed for the duration of the call.
+ *
+ * Reference interfaces replaced (paths inside Perrbit/astr_gpu):
+ *   astr_fd_scheme_create   fd_scheme_initiate(asolver,scheme,ntype,dim,dir)  src/derivative.F90:63
+ *   astr_filter_create      filter_coefficient_cal(alfa,beter_halo,beter_bouond) src/filter.F90:299
+ *                           + compact_filter_initiate(afilter,ntype,dim,note)  src/filter.F90:31
+ *   astr_scheme_ac          compact_scheme%ac (tridiagonal_thomas_proprocess)  src/commtype.F90:13-23,
+ *                                                                              src/commfunc.F90:752
+ *   astr_deriv_lines        df = fds%central(asolver,f,dim) over every line    src/derivative.F90:22-41,171
+ *   astr_filter_lines       ff = compact_filter(afilter,f,dim[,note])          src/filter.F90:112
+ *   astr_state_*            the module arrays q/rho/vel/prs/tmp of commarray  miniapps/tgv_solver_3d/
+ *                                                                              tgvsolver.F90:1-40
+ *   astr_state_init_tgv     flowfield_init                                    tgvsolver.F90:172-234
+ *   astr_cfl_dt             cflcal (spectral radius sum, dt held fixed)        src/commcal.F90:27-87
+ *   astr_rhs                rhscal (gradcal, convection, -qrhs, diffusion)      tgvsolver.F90:962-992
+ *   astr_rk3_step           rk3 x nsteps (SSP-RK3, filter after each stage)     tgvsolver.F90:994-1082,
+ *                                                                              steploop :944-960
+ *   astr_history            stacal rows (nstep, time, tke, enstrophy) + dissipation
+ *                                                                              tgvsolver.F90:893-942,
+ *                                                                              src/statistic.F90:993-1040
+ *   astr_rk3_step_host      one call of rk3 with the state in host memory: upload, nsteps, download
+ */
+#ifndef ASTR_B200_H
+#define ASTR_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  ASTR_OK = 0,
+  ASTR_ERR_ARG = -1,         /* bad argument (null pointer, size, unsupported ntype/scheme) */
+  ASTR_ERR_CUDA = -2,        /* a CUDA runtime call failed */
+  ASTR_ERR_STATE = -3,       /* device-side invalid state (non-finite or non-positive density) */
+  ASTR_ERR_UNSUPPORTED = -4, /* size outside what the compiled kernels cover */
+  ASTR_ERR_NOMEM = -5        /* device allocation failed */
+};
+enum { ASTR_HOST = 0, ASTR_DEVICE = 1 };
+
+typedef struct astr_ctx astr_ctx;
+typedef struct astr_scheme astr_scheme;
+typedef struct astr_state astr_state;
+
+/* Flow and scheme parameters of one periodic box (commvar of the reference). */
+typedef struct {
+  int im, jm, km;          /* nodes 0..im etc.; im = N means N^3 unique points, (N+1)^3 stored */
+  double mach, reynolds, prandtl, gamma;
+  double ref_tem;          /* 273.15 */
+  double sutherland;       /* Sutherland constant in kelvin: 110.4 (miniapp) or 110.3 (full solver) */
+  double alfa_filter;      /* 0.49 */
+  double beta_halo;        /* 1.11 */
+  double beta_bound;       /* 1.09 (miniapp) or 0.98 (full solver) */
+  int filter_on;           /* apply filterq after every RK stage */
+} astr_params;
+
+/* ---- context ------------------------------------------------------------------------ */
+int astr_init(int device, astr_ctx** ctx);
+int astr_destroy(astr_ctx* ctx);
+const char* astr_last_error(astr_ctx* ctx);
+/* Use the caller's CUDA stream (cudaStream_t) for all later work of this context. */
+int astr_set_stream(astr_ctx* ctx, void* cuda_stream);
+int astr_synchronize(astr_ctx* ctx);
+
+/* ---- schemes (line operators) ----------------------------------------------------- */
+/* scheme: "643c" (6th-order compact) or "643e" (explicit 6th-order, diff6ec). ntype 1..4 as in
+ * fd_scheme_initiate: 1 boundary at i=0, 2 boundary at i=dim, 3 inner/periodic, 4 both. */
+int astr_fd_scheme_create(astr_ctx* ctx, const char scheme[4], int ntype, int dim, astr_scheme** out);
+/* compact 10th-order filter with LHS coefficient alpha_f; boundary_no_filter selects the
+ * note='boundary_no_filter' variant of compact_filter_initiate. */
+int astr_filter_create(astr_ctx* ctx, int ntype, int dim, double alpha_f, double beta_halo,
+                       double beta_bound, int boundary_no_filter, astr_scheme** out);
+int astr_scheme_destroy(astr_scheme* s);
+/* Pre-factored Thomas table ac(3, first:last): ac[3*r + c], r = 0..last-first. */
+int astr_scheme_ac(const astr_scheme* s, double* ac, int* first_node, int* last_node);
+
+/* ---- line-level operators --------------------------------------------------------- */
+/* Apply the scheme along dir (0,1,2) to every line of f: for each index pair of the output's
+ * other two axes and t = 0..dim along dir,
+ *     df(t) = scale * fds%central(asolver, f(-hm:dim+hm), dim)(t).
+ * f(f_lb : f_lb+f_shape-1, ..., 1:nfields) must hold the line's halo nodes -5..dim+5 along dir
+ * when the scheme reads them (ntype 1..3); df's range along dir must cover 0..dim and its other
+ * axes must lie inside f's. */
+int astr_deriv_lines(astr_ctx* ctx, const astr_scheme* s, int dir, const double* f,
+                     const int64_t f_shape[3], const int64_t f_lbound[3], double* df,
+                     const int64_t df_shape[3], const int64_t df_lbound[3], int nfields,
+                     double scale, int where);
+int astr_filter_lines(astr_ctx* ctx, const astr_scheme* s, int dir, const double* f,
+                      const int64_t f_shape[3], const int64_t f_lbound[3], double* ff,
+                      const int64_t ff_shape[3], const int64_t ff_lbound[3], int nfields, int where);
+
+/* ---- solver state and the RK3 step ------------------------------------------------ */
+int astr_state_create(astr_ctx* ctx, const astr_params* p, astr_state** out);
+int astr_state_destroy(astr_state* st);
+int astr_state_init_tgv(astr_state* st);
+/* Conserved variables q(lb.., 1:5) on nodes 0..im x 0..jm x 0..km (any halo in the caller's
+ * array is ignored on upload and left untouched on download). */
+int astr_state_upload(astr_state* st, const double* q, const int64_t shape[3], const int64_t lbound[3], int where);
+int astr_state_download(astr_state* st, double* q, const int64_t shape[3], const int64_t lbound[3], int where);
+/* dt such that cflcal's CFL equals `cfl` on the current state. */
+int astr_cfl_dt(astr_state* st, double cfl, double* dt);
+/* One rhscal of the current state into qrhs(lb.., 1:5) on nodes 0..im etc. */
+int astr_rhs(astr_state* st, double* qrhs, const int64_t shape[3], const int64_t lbound[3], int where);
+int astr_rk3_step(astr_state* st, double dt, int nsteps);
+/* The same, with the state in host memory for the duration of the call. */
+int astr_rk3_step_host(astr_state* st, double* q, const int64_t shape[3], const int64_t lbound[3],
+                       double dt, int nsteps, double diag_out[3]);
+/* stacal rows written so far: (nstep, time, tke, enstrophy, dissipation), 5 doubles per row. */
+int astr_history(astr_state* st, double* rows, int maxrows, int* nrows);
+/* tke, enstrophy, dissipation of the current state (one gradient evaluation). */
+int astr_diagnostics(astr_state* st, double out[3]);
+/* Capture each RK3 step as one CUDA graph (default on). */
+int astr_state_use_graph(astr_state* st, int on);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,223 @@
+"""ORACLE — test infrastructure only.
+
+ctypes binding of ``oracle/astr_oracle.cpp``, a CPU restatement of the reference ASTR
+(Perrbit/astr_gpu) hot path: compact derivatives (derivative.F90), compact filter (filter.F90),
+Thomas solver (commfunc.F90:752-813) and the Taylor-Green miniapp driver
+(miniapps/tgv_solver_3d/tgvsolver.F90). Only ``tests/``, ``__graft_entry__.smoke()`` and the
+``cpu_baseline`` leg / ``--impl reference`` arm of ``bench.py`` may import this module, and only
+as the checker or the timed CPU reference — never as part of the product path.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from dataclasses import dataclass
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "_build", "libastr_oracle.so")
+_lib = None
+
+HM = 5  # halo width, commvar.F90:190
+
+
+def build(force: bool = False) -> str:
+    """Compile the oracle shared library in-tree (``make -C oracle``)."""
+    src = os.path.join(_HERE, "astr_oracle.cpp")
+    if force or not os.path.exists(_LIB_PATH) or os.path.getmtime(_LIB_PATH) < os.path.getmtime(src):
+        subprocess.run(["make", "-C", _HERE, "-B" if force else "-s"], check=True,
+                       stdout=subprocess.DEVNULL)
+    return _LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        L = ctypes.CDLL(_LIB_PATH)
+        vp, dp, ip, i64p = ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int), \
+            ctypes.POINTER(ctypes.c_int64)
+        d, i = ctypes.c_double, ctypes.c_int
+        sig = {
+            "orc_fd_scheme_create": (vp, [ctypes.c_char_p, i, i]),
+            "orc_filter_create": (vp, [i, i, d, d, d, i]),
+            "orc_scheme_free": (None, [vp]),
+            "orc_scheme_info": (i, [vp, ip, ip]),
+            "orc_scheme_ac": (None, [vp, dp, dp, dp]),
+            "orc_deriv_line": (None, [vp, dp, dp]),
+            "orc_filter_line": (None, [vp, dp, dp]),
+            "orc_deriv3d": (None, [vp, i, dp, i64p, i64p, i, dp]),
+            "orc_filter3d": (None, [vp, i, dp, i64p, i64p, i, dp]),
+            "orc_tgv_create": (vp, [i, i, i, d, d, d, d, d, d, d, d, d, i]),
+            "orc_tgv_free": (None, [vp]),
+            "orc_tgv_init_tgv": (None, [vp]),
+            "orc_tgv_set_q": (None, [vp, dp]),
+            "orc_tgv_get_q": (None, [vp, dp]),
+            "orc_tgv_set_dt": (None, [vp, d]),
+            "orc_tgv_cfl_dt": (d, [vp, d]),
+            "orc_tgv_steps": (None, [vp, i]),
+            "orc_tgv_history": (i, [vp, dp, i]),
+            "orc_tgv_rhs": (None, [vp, dp]),
+            "orc_tgv_diagnostics": (None, [vp, dp]),
+            "orc_num_threads": (i, []),
+            "orc_set_num_threads": (None, [i]),
+        }
+        for name, (res, args) in sig.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _dp(a: np.ndarray):
+    assert a.dtype == np.float64 and a.flags["F_CONTIGUOUS"] or a.ndim == 1
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+class Scheme:
+    """A ``compact_scheme`` (commtype.F90:13-23): derivative (``fd_scheme_initiate``) or filter
+    (``compact_filter_initiate`` + ``filter_coefficient_cal``)."""
+
+    def __init__(self, handle, dim, ntype, is_filter):
+        self._h = handle
+        self.dim = dim
+        self.ntype = ntype
+        self.is_filter = is_filter
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.orc_scheme_free(self._h)
+            self._h = None
+
+    def ac(self):
+        L = lib()
+        f, l = ctypes.c_int(), ctypes.c_int()
+        n = L.orc_scheme_info(self._h, ctypes.byref(f), ctypes.byref(l))
+        a1, a2, a3 = (np.zeros(n) for _ in range(3))
+        L.orc_scheme_ac(self._h, _dp(a1), _dp(a2), _dp(a3))
+        return f.value, l.value, a1, a2, a3
+
+    def line(self, f: np.ndarray) -> np.ndarray:
+        """f holds f(-5..dim+5); returns the dim+1 outputs (df_compact / compact_filter)."""
+        f = np.ascontiguousarray(f, dtype=np.float64)
+        assert f.shape == (self.dim + 1 + 2 * HM,)
+        out = np.zeros(self.dim + 1)
+        (lib().orc_filter_line if self.is_filter else lib().orc_deriv_line)(self._h, _dp(f), _dp(out))
+        return out
+
+    def apply3d(self, f: np.ndarray, direction: int, lbound=(0, 0, 0)) -> np.ndarray:
+        """Apply along ``direction`` (0,1,2) to every line of a Fortran-ordered array
+        f(l0:, l1:, l2:[, nfields]); the output spans 0..dim along that direction."""
+        f = np.asfortranarray(f, dtype=np.float64)
+        nf = f.shape[3] if f.ndim == 4 else 1
+        shape = np.array(f.shape[:3], dtype=np.int64)
+        lb = np.array(lbound, dtype=np.int64)
+        oshape = list(f.shape)
+        oshape[direction] = self.dim + 1
+        out = np.zeros(oshape, order="F")
+        fn = lib().orc_filter3d if self.is_filter else lib().orc_deriv3d
+        fn(self._h, direction, _dp(f), shape.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)),
+           lb.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), nf, _dp(out))
+        return out
+
+
+def fd_scheme_initiate(scheme: str, ntype: int, dim: int) -> Scheme:
+    """derivative.F90:63-158."""
+    h = lib().orc_fd_scheme_create(scheme.encode(), ntype, dim)
+    if not h:
+        raise ValueError(f"scheme not defined: {scheme}")
+    return Scheme(h, dim, ntype, False)
+
+
+def compact_filter_initiate(ntype: int, dim: int, alfa: float = 0.49, beta_halo: float = 1.11,
+                            beta_bound: float = 0.98, boundary_no_filter: bool = False) -> Scheme:
+    """filter.F90:31-100 with the coefficients of filter_coefficient_cal (filter.F90:299-432)."""
+    h = lib().orc_filter_create(ntype, dim, alfa, beta_halo, beta_bound, int(boundary_no_filter))
+    return Scheme(h, dim, ntype, True)
+
+
+@dataclass
+class FlowParams:
+    mach: float = 0.1
+    reynolds: float = 1600.0
+    prandtl: float = 0.72
+    gamma: float = 1.4
+    ref_tem: float = 273.15
+    sutherland: float = 110.4     # tgvsolver.F90:133 (the full solver uses 110.3)
+    alfa_filter: float = 0.49
+    beta_halo: float = 1.11
+    beta_bound: float = 1.09      # tgvsolver.F90:253
+    filter_on: bool = True
+
+
+class TGVOracle:
+    """The miniapp ``boxsolver`` (tgvsolver.F90:1086-1116) on an im x jm x km periodic box."""
+
+    def __init__(self, im: int, jm: int | None = None, km: int | None = None, params: FlowParams | None = None):
+        self.im, self.jm, self.km = im, jm or im, km or im
+        p = params or FlowParams()
+        self.params = p
+        self._h = lib().orc_tgv_create(self.im, self.jm, self.km, p.mach, p.reynolds, p.prandtl, p.gamma,
+                                       p.ref_tem, p.sutherland, p.alfa_filter, p.beta_halo, p.beta_bound,
+                                       int(p.filter_on))
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.orc_tgv_free(self._h)
+            self._h = None
+
+    @property
+    def shape(self):
+        return (self.im + 1, self.jm + 1, self.km + 1)
+
+    def init_tgv(self):
+        lib().orc_tgv_init_tgv(self._h)
+
+    def set_q(self, q: np.ndarray):
+        q = np.asfortranarray(q, dtype=np.float64)
+        assert q.shape == self.shape + (5,)
+        lib().orc_tgv_set_q(self._h, _dp(q))
+
+    def get_q(self) -> np.ndarray:
+        out = np.zeros(self.shape + (5,), order="F")
+        lib().orc_tgv_get_q(self._h, _dp(out))
+        return out
+
+    def set_dt(self, dt: float):
+        lib().orc_tgv_set_dt(self._h, dt)
+
+    def cfl_dt(self, cfl: float) -> float:
+        return lib().orc_tgv_cfl_dt(self._h, cfl)
+
+    def steps(self, n: int):
+        lib().orc_tgv_steps(self._h, n)
+
+    def history(self) -> np.ndarray:
+        """Rows of (nstep, time, tke, enstrophy, dissipation), one per step (stacal)."""
+        L = lib()
+        n = L.orc_tgv_history(self._h, _dp(np.zeros(5)), 0)
+        out = np.zeros(5 * max(n, 1))
+        L.orc_tgv_history(self._h, _dp(out), n)
+        return out[: 5 * n].reshape(n, 5)
+
+    def rhs(self) -> np.ndarray:
+        out = np.zeros(self.shape + (5,), order="F")
+        lib().orc_tgv_rhs(self._h, _dp(out))
+        return out
+
+    def diagnostics(self) -> np.ndarray:
+        out = np.zeros(3)
+        lib().orc_tgv_diagnostics(self._h, _dp(out))
+        return out
+
+
+def num_threads() -> int:
+    return lib().orc_num_threads()
+
+
+def set_num_threads(n: int):
+    lib().orc_set_num_threads(n)

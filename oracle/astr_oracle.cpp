@@ -1,0 +1,969 @@
+// ORACLE — test infrastructure only. Nothing in the product path links or calls this file.
+//
+// A CPU restatement, in C++17, of the reference ASTR (Perrbit/astr_gpu) CPU algorithm for the
+// per-step RHS hot path. Each routine follows the reference routine it names, in the same
+// operation order, so that with -ffp-contract=off it reproduces the reference's arithmetic:
+//
+//   commfunc.F90:752-813        tridiagonal_thomas_proprocess / tridiagonal_thomas_solver
+//   derivative.F90:63-306       fd_scheme_initiate, df_compact, compact_fd_rhs
+//   derivative.F90:350-413      diff6ec (explicit 6th-order, the '643e' scheme)
+//   filter.F90:31-285, 299-432  compact_filter_initiate, compact_filter, compact_filter_rhs,
+//                               filter_coefficient_cal
+//   miniapps/tgv_solver_3d/tgvsolver.F90:48-1082
+//                               the Taylor-Green miniapp: fvar2q, thermal_scar, q2fvar, miucal,
+//                               flowfield_init, bchomo/bchomovec, gradcal, convection,
+//                               diffusion, filterq, stacal, rhscal, rk3
+//   commcal.F90:27-87           cflcal (only to fix dt once at t=0)
+//   statistic.F90:993-1040      diss_rate_cal (dissipation diagnostic)
+//
+// Parity is pinned by the reference's golden history miniapps/tgv_solver_3d/state.ref_128
+// (kinetic energy and enstrophy, 100 steps at 128^3), checked in tests/test_oracle_golden.py.
+//
+// OpenMP splits only independent line loops; every reduction keeps the reference's
+// sequential i-fastest order.
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+#include <string>
+#include <algorithm>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace {
+
+constexpr int HM = 5;                      // halo width, commvar.F90:190
+constexpr double num1d3 = 1.0 / 3.0;       // constdef.F90:13-27
+constexpr double num2d3 = 2.0 / 3.0;
+constexpr double num7d9 = 7.0 / 9.0;
+constexpr double num1d36 = 1.0 / 36.0;
+constexpr double num1d60 = 1.0 / 60.0;
+constexpr double num1d12 = 1.0 / 12.0;
+
+// ---------------------------------------------------------------- compact_scheme (commtype.F90:13-23)
+struct Scheme {
+  int first_node = 0, last_node = 0, dimension = 0, nbctype = 3;
+  bool compact = true;       // '643c' (compact) or '643e' (explicit)
+  bool is_filter = false;
+  bool no_filter_note = false;
+  std::vector<double> a, c;  // index 0 <-> first_node
+  std::vector<double> ac1, ac2, ac3;
+  // filter coefficients carried by the scheme (filter.F90:17-20 keeps them module-global)
+  double coef6i[4], coef8i[5], coef10i[6], coefb[5][9], coefh[5][11];
+  int n() const { return last_node - first_node + 1; }
+};
+
+// tridiagonal_thomas_proprocess, commfunc.F90:752-774
+void thomas_proprocess(Scheme& s) {
+  const int n = s.n();
+  s.ac1.assign(n, 0.0); s.ac2.assign(n, 0.0); s.ac3.assign(n, 0.0);
+  s.ac1[0] = s.c[0];
+  for (int i = 1; i < n; ++i) {
+    s.ac1[i] = s.c[i] / (1.0 - s.a[i] * s.ac1[i - 1]);
+    s.ac2[i] = 1.0 / (1.0 - s.a[i] * s.ac1[i - 1]);
+    s.ac3[i] = s.a[i] / (1.0 - s.a[i] * s.ac1[i - 1]);
+  }
+}
+
+// tridiagonal_thomas_solver, commfunc.F90:790-813 (d is overwritten, x returned)
+void thomas_solve(const Scheme& s, double* d, double* x) {
+  const int n = s.n();
+  for (int i = 1; i < n; ++i) d[i] = d[i] * s.ac2[i] - d[i - 1] * s.ac3[i];
+  x[n - 1] = d[n - 1];
+  for (int i = n - 2; i >= 0; --i) x[i] = d[i] - s.ac1[i] * x[i + 1];
+}
+
+void node_range(int ntype, int dim, int ext, int& i0, int& im_) {
+  switch (ntype) {
+    case 1: i0 = 0;    im_ = dim + ext; break;
+    case 2: i0 = -ext; im_ = dim;       break;
+    case 3: i0 = -ext; im_ = dim + ext; break;
+    default: i0 = 0;   im_ = dim;       break;  // 4
+  }
+}
+
+// fd_scheme_initiate, derivative.F90:63-158 ('643c' and '643e' are the only schemes it defines)
+bool fd_scheme_initiate(Scheme& s, const char* scheme, int ntype, int dim) {
+  int i0, imx;
+  node_range(ntype, dim, 1, i0, imx);
+  s.first_node = i0; s.last_node = imx; s.dimension = dim; s.nbctype = ntype;
+  const int n = s.n();
+  s.a.assign(n, 0.0); s.c.assign(n, 0.0);
+  int nscheme = (scheme[0] - '0') * 100 + (scheme[1] - '0') * 10 + (scheme[2] - '0');
+  if (scheme[3] == 'e') { s.compact = false; return nscheme == 643 || nscheme / 100 == 6; }
+  if (scheme[3] != 'c' || nscheme != 643) return false;
+  s.compact = true;
+  for (int i = 0; i < n; ++i) { s.a[i] = num1d3; s.c[i] = num1d3; }
+  s.a[0] = 0.0; s.c[0] = 0.0;
+  s.a[n - 1] = 0.0; s.c[n - 1] = 0.0;
+  if (ntype == 1 || ntype == 4) {
+    s.a[0] = 2.0; s.c[0] = 2.0;
+    s.a[1] = 0.25; s.c[1] = 0.25;
+  }
+  if (ntype == 2 || ntype == 4) {
+    s.a[n - 1] = 2.0; s.c[n - 1] = 2.0;
+    s.a[n - 2] = 0.25; s.c[n - 2] = 0.25;
+  }
+  thomas_proprocess(s);
+  return true;
+}
+
+// compact_fd_rhs, derivative.F90:210-306. f points at f(0); valid f(-HM..dim+HM).
+void compact_fd_rhs(const Scheme& s, const double* f, double* d) {
+  const int i0 = s.first_node, im_ = s.last_node, nt = s.nbctype;
+  auto D = [&](int j) -> double& { return d[j - i0]; };
+  int is, ie;
+  if (nt == 1 || nt == 4) {
+    is = i0 + 2;
+    int j = i0 + 1;
+    double var1 = f[j + 1] - f[j - 1];
+    D(j) = 0.75 * var1;
+    j = i0;
+    D(j) = -2.5 * f[j] + 2.0 * f[j + 1] + 0.5 * f[j + 2];
+  } else {
+    is = i0 + 1;
+    int j = i0;
+    double var1 = f[j + 1] - f[j - 1];
+    double var2 = f[j + 2] - f[j - 2];
+    double var3 = f[j + 3] - f[j - 3];
+    D(j) = 0.75 * var1 - 0.15 * var2 + num1d60 * var3;
+  }
+  if (nt == 2 || nt == 4) {
+    ie = im_ - 2;
+    int j = im_ - 1;
+    double var1 = f[j + 1] - f[j - 1];
+    D(j) = 0.75 * var1;
+    j = im_;
+    D(j) = 2.5 * f[j] - 2.0 * f[j - 1] - 0.5 * f[j - 2];
+  } else {
+    ie = im_ - 1;
+    int j = im_;
+    double var1 = f[j + 1] - f[j - 1];
+    double var2 = f[j + 2] - f[j - 2];
+    double var3 = f[j + 3] - f[j - 3];
+    D(j) = 0.75 * var1 - 0.15 * var2 + num1d60 * var3;
+  }
+  for (int j = is; j <= ie; ++j) {
+    double var1 = f[j + 1] - f[j - 1];
+    double var2 = f[j + 2] - f[j - 2];
+    D(j) = num7d9 * var1 + num1d36 * var2;
+  }
+}
+
+// diff6ec, derivative.F90:350-413
+void diff6ec(const double* v, int dim, int ntype, double* out) {
+  auto e6 = [&](int i) {
+    return 0.75 * (v[i + 1] - v[i - 1]) - 0.15 * (v[i + 2] - v[i - 2]) + num1d60 * (v[i + 3] - v[i - 3]);
+  };
+  switch (ntype) {
+    case 1:
+      out[0] = -0.5 * v[2] + 2.0 * v[1] - 1.5 * v[0];
+      out[1] = 0.5 * (v[2] - v[0]);
+      out[2] = num2d3 * (v[3] - v[1]) - num1d12 * (v[4] - v[0]);
+      for (int i = 3; i <= dim; ++i) out[i] = e6(i);
+      break;
+    case 2:
+      for (int i = 0; i <= dim - 3; ++i) out[i] = e6(i);
+      out[dim - 2] = num2d3 * (v[dim - 1] - v[dim - 3]) - num1d12 * (v[dim] - v[dim - 4]);
+      out[dim - 1] = 0.5 * (v[dim] - v[dim - 2]);
+      out[dim] = 0.5 * v[dim - 2] - 2.0 * v[dim - 1] + 1.5 * v[dim];
+      break;
+    case 3:
+      for (int i = 0; i <= dim; ++i) out[i] = e6(i);
+      break;
+    default:
+      out[0] = -0.5 * v[2] + 2.0 * v[1] - 1.5 * v[0];
+      out[1] = 0.5 * (v[2] - v[0]);
+      out[2] = num2d3 * (v[3] - v[1]) - num1d12 * (v[4] - v[0]);
+      for (int i = 3; i <= dim - 3; ++i) out[i] = e6(i);
+      out[dim - 2] = num2d3 * (v[dim - 1] - v[dim - 3]) - num1d12 * (v[dim] - v[dim - 4]);
+      out[dim - 1] = 0.5 * (v[dim] - v[dim - 2]);
+      out[dim] = 0.5 * v[dim - 2] - 2.0 * v[dim - 1] + 1.5 * v[dim];
+      break;
+  }
+}
+
+// df_compact / df_explicit, derivative.F90:171-198 and :319-336. scratch >= 2*(dim+3)
+void df_line(const Scheme& s, const double* f, double* df, double* scratch) {
+  if (!s.compact) { diff6ec(f, s.dimension, s.nbctype, df); return; }
+  const int n = s.n();
+  double* d = scratch;
+  double* xx = scratch + n;
+  compact_fd_rhs(s, f, d);
+  thomas_solve(s, d, xx);
+  for (int i = 0; i <= s.dimension; ++i) df[i] = xx[i - s.first_node];
+}
+
+// filter_coefficient_cal, filter.F90:299-432
+void filter_coefficient_cal(Scheme& s, double alfa, double beter_halo, double beter_bouond) {
+  s.coef6i[0] = (11.0 + 10.0 * alfa) / 32.0;
+  s.coef6i[1] = (15.0 + 34.0 * alfa) / 64.0;
+  s.coef6i[2] = (-3.0 + 6.0 * alfa) / 32.0;
+  s.coef6i[3] = (1.0 - 2.0 * alfa) / 64.0;
+  s.coef8i[0] = (93.0 + 70.0 * alfa) / 256.0;
+  s.coef8i[1] = (7.0 + 18.0 * alfa) / 32.0;
+  s.coef8i[2] = (-7.0 + 14.0 * alfa) / 64.0;
+  s.coef8i[3] = (1.0 - 2.0 * alfa) / 32.0;
+  s.coef8i[4] = (-1.0 + 2.0 * alfa) / 256.0;
+  s.coef10i[0] = (193.0 + 126.0 * alfa) / 512.0;
+  s.coef10i[1] = (105.0 + 302.0 * alfa) / 512.0;
+  s.coef10i[2] = (-15.0 + 30.0 * alfa) / 128.0;
+  s.coef10i[3] = (45.0 - 90.0 * alfa) / 1024.0;
+  s.coef10i[4] = (-5.0 + 10.0 * alfa) / 512.0;
+  s.coef10i[5] = (1.0 - 2.0 * alfa) / 1024.0;
+  for (auto& r : s.coefb) for (double& v : r) v = 0.0;
+  for (auto& r : s.coefh) for (double& v : r) v = 0.0;
+  s.coefb[3][0] = (1.0 - 2.0 * alfa) / 256.0;
+  s.coefb[3][1] = (-1.0 + 2.0 * alfa) / 32.0;
+  s.coefb[3][2] = (7.0 + 50.0 * alfa) / 64.0;
+  s.coefb[3][3] = (25.0 + 14.0 * alfa) / 32.0;
+  s.coefb[3][4] = (35.0 + 58.0 * alfa) / 128.0;
+  s.coefb[3][5] = (-7.0 + 14.0 * alfa) / 32.0;
+  s.coefb[3][6] = (7.0 - 14.0 * alfa) / 64.0;
+  s.coefb[3][7] = (-1.0 + 2.0 * alfa) / 32.0;
+  s.coefb[3][8] = (1.0 - 2.0 * alfa) / 256.0;
+  s.coefb[2][0] = (-1.0 + 2.0 * alfa) / 64.0;
+  s.coefb[2][1] = (3.0 + 26.0 * alfa) / 32.0;
+  s.coefb[2][2] = (49.0 + 30.0 * alfa) / 64.0;
+  s.coefb[2][3] = (5.0 + 6.0 * alfa) / 16.0;
+  s.coefb[2][4] = (-15.0 + 30.0 * alfa) / 64.0;
+  s.coefb[2][5] = (3.0 - 6.0 * alfa) / 32.0;
+  s.coefb[2][6] = (-1.0 + 2.0 * alfa) / 64.0;
+  s.coefb[1][0] = (1.0 + 62.0 * alfa) / 64.0;
+  s.coefb[1][1] = (29.0 + 6.0 * alfa) / 32.0;
+  s.coefb[1][2] = (15.0 + 34.0 * alfa) / 64.0;
+  s.coefb[1][3] = (-5.0 + 10.0 * alfa) / 16.0;
+  s.coefb[1][4] = (15.0 - 30.0 * alfa) / 64.0;
+  s.coefb[1][5] = (-3.0 + 6.0 * alfa) / 32.0;
+  s.coefb[1][6] = (1.0 - 2.0 * alfa) / 64.0;
+  s.coefb[0][0] = (63.0 + 1.0 * beter_bouond) / 64.0;
+  s.coefb[0][1] = (3.0 + 29.0 * beter_bouond) / 32.0;
+  s.coefb[0][2] = (-15.0 + 15.0 * beter_bouond) / 64.0;
+  s.coefb[0][3] = (5.0 - 5.0 * beter_bouond) / 16.0;
+  s.coefb[0][4] = (-15.0 + 15.0 * beter_bouond) / 64.0;
+  s.coefb[0][5] = (3.0 - 3.0 * beter_bouond) / 32.0;
+  s.coefb[0][6] = (-1.0 + 1.0 * beter_bouond) / 64.0;
+  s.coefh[0][0] = (-1.0 + 1.0 * beter_halo) / 1024.0;
+  s.coefh[0][1] = (5.0 - 5.0 * beter_halo) / 512.0;
+  s.coefh[0][2] = (979.0 + 45.0 * beter_halo) / 1024.0;
+  s.coefh[0][3] = (15.0 + 113.0 * beter_halo) / 128.0;
+  s.coefh[0][4] = (-105.0 + 105.0 * beter_halo) / 512.0;
+  s.coefh[0][5] = (63.0 - 63.0 * beter_halo) / 256.0;
+  s.coefh[0][6] = (-105.0 + 105.0 * beter_halo) / 512.0;
+  s.coefh[0][7] = (15.0 - 15.0 * beter_halo) / 128.0;
+  s.coefh[0][8] = (-45.0 + 45.0 * beter_halo) / 1024.0;
+  s.coefh[0][9] = (5.0 - 5.0 * beter_halo) / 512.0;
+  s.coefh[0][10] = (-1.0 + 1.0 * beter_halo) / 1024.0;
+  s.coefh[1][0] = (1.0 - 2.0 * alfa) / 1024.0;
+  s.coefh[1][1] = (-5.0 + 10.0 * alfa) / 512.0;
+  s.coefh[1][2] = (45.0 + 934.0 * alfa) / 1024.0;
+  s.coefh[1][3] = (113.0 + 30.0 * alfa) / 128.0;
+  s.coefh[1][4] = (105.0 + 302.0 * alfa) / 512.0;
+  s.coefh[1][5] = (-63.0 + 126.0 * alfa) / 256.0;
+  s.coefh[1][6] = (105.0 - 210.0 * alfa) / 512.0;
+  s.coefh[1][7] = (-15.0 + 30.0 * alfa) / 128.0;
+  s.coefh[1][8] = (45.0 - 90.0 * alfa) / 1024.0;
+  s.coefh[1][9] = (-5.0 + 10.0 * alfa) / 512.0;
+  s.coefh[1][10] = (1.0 - 2.0 * alfa) / 1024.0;
+  s.coefh[2][0] = (-1.0 + 2.0 * alfa) / 1024.0;
+  s.coefh[2][1] = (5.0 - 10.0 * alfa) / 512.0;
+  s.coefh[2][2] = (-45.0 + 90.0 * alfa) / 1024.0;
+  s.coefh[2][3] = (15.0 + 98.0 * alfa) / 128.0;
+  s.coefh[2][4] = (407.0 + 210.0 * alfa) / 512.0;
+  s.coefh[2][5] = (63.0 + 130.0 * alfa) / 256.0;
+  s.coefh[2][6] = (-105.0 + 210.0 * alfa) / 512.0;
+  s.coefh[2][7] = (15.0 - 30.0 * alfa) / 128.0;
+  s.coefh[2][8] = (-45.0 + 90.0 * alfa) / 1024.0;
+  s.coefh[2][9] = (5.0 - 10.0 * alfa) / 512.0;
+  s.coefh[2][10] = (-1.0 + 2.0 * alfa) / 1024.0;
+}
+
+// compact_filter_initiate, filter.F90:31-100 (alfa plays the role of commvar's alfa_filter)
+void compact_filter_initiate(Scheme& s, int ntype, int dim, double alfa, bool no_filter_note) {
+  int i0, imx;
+  double b0, bm;
+  switch (ntype) {
+    case 1: i0 = 0;  imx = dim + 3; b0 = 0.98; bm = 1.11; break;
+    case 2: i0 = -3; imx = dim;     b0 = 1.11; bm = 0.98; break;
+    case 3: i0 = -3; imx = dim + 3; b0 = 1.11; bm = 1.11; break;
+    default: i0 = 0; imx = dim;     b0 = 0.98; bm = 0.98; break;
+  }
+  s.first_node = i0; s.last_node = imx; s.dimension = dim; s.nbctype = ntype;
+  s.is_filter = true; s.no_filter_note = no_filter_note;
+  const int n = s.n();
+  s.a.assign(n, alfa); s.c.assign(n, alfa);
+  if (no_filter_note) {
+    s.a[0] = 0.0; s.c[0] = 0.0; s.a[n - 1] = 0.0; s.c[n - 1] = 0.0;
+  } else {
+    s.a[0] = b0; s.c[0] = b0; s.a[n - 1] = bm; s.c[n - 1] = bm;
+  }
+  thomas_proprocess(s);
+}
+
+// compact_filter_rhs, filter.F90:156-285. f points at f(0).
+void compact_filter_rhs(const Scheme& s, const double* f, double* d) {
+  const int i0 = s.first_node, im_ = s.last_node, nt = s.nbctype;
+  auto D = [&](int j) -> double& { return d[j - i0]; };
+  int is, ie;
+  if (nt == 1 || nt == 4) {
+    is = i0 + 5;
+    for (int k = i0; k <= i0 + 2; ++k) {
+      double var0 = 0.0;
+      for (int j = 0; j <= 6; ++j) var0 = var0 + s.coefb[k - i0][j] * f[i0 + j];
+      D(k) = var0;
+    }
+    int j = i0 + 3;
+    double var0 = f[j] + f[j], var1 = f[j + 1] + f[j - 1], var2 = f[j + 2] + f[j - 2],
+           var3 = f[j + 3] + f[j - 3];
+    D(j) = s.coef6i[0] * var0 + s.coef6i[1] * var1 + s.coef6i[2] * var2 + s.coef6i[3] * var3;
+    j = i0 + 4;
+    var0 = f[j] + f[j]; var1 = f[j + 1] + f[j - 1]; var2 = f[j + 2] + f[j - 2];
+    var3 = f[j + 3] + f[j - 3];
+    double var4 = f[j + 4] + f[j - 4];
+    D(j) = s.coef8i[0] * var0 + s.coef8i[1] * var1 + s.coef8i[2] * var2 + s.coef8i[3] * var3 +
+           s.coef8i[4] * var4;
+  } else {
+    is = i0 + 3;
+    for (int k = i0; k <= i0 + 2; ++k) {
+      double var0 = 0.0;
+      for (int j = 0; j <= 10; ++j) var0 = var0 + s.coefh[k - i0][j] * f[i0 - 2 + j];
+      D(k) = var0;
+    }
+  }
+  if (nt == 2 || nt == 4) {
+    ie = im_ - 5;
+    for (int k = im_ - 2; k <= im_; ++k) {
+      double var0 = 0.0;
+      for (int j = 0; j <= 6; ++j) var0 = var0 + s.coefb[im_ - k][j] * f[im_ - j];
+      D(k) = var0;
+    }
+    int j = im_ - 3;
+    double var0 = f[j] + f[j], var1 = f[j + 1] + f[j - 1], var2 = f[j + 2] + f[j - 2],
+           var3 = f[j + 3] + f[j - 3];
+    D(j) = s.coef6i[0] * var0 + s.coef6i[1] * var1 + s.coef6i[2] * var2 + s.coef6i[3] * var3;
+    j = im_ - 4;
+    var0 = f[j] + f[j]; var1 = f[j + 1] + f[j - 1]; var2 = f[j + 2] + f[j - 2];
+    var3 = f[j + 3] + f[j - 3];
+    double var4 = f[j + 4] + f[j - 4];
+    D(j) = s.coef8i[0] * var0 + s.coef8i[1] * var1 + s.coef8i[2] * var2 + s.coef8i[3] * var3 +
+           s.coef8i[4] * var4;
+  } else {
+    ie = im_ - 3;
+    for (int k = im_ - 2; k <= im_; ++k) {
+      double var0 = 0.0;
+      for (int j = 0; j <= 10; ++j) var0 = var0 + s.coefh[im_ - k][j] * f[im_ + 2 - j];
+      D(k) = var0;
+    }
+  }
+  if (s.no_filter_note) { D(i0) = f[i0]; D(im_) = f[im_]; }
+  for (int j = is; j <= ie; ++j) {
+    double var0 = f[j] + f[j];
+    double var1 = f[j + 1] + f[j - 1];
+    double var2 = f[j + 2] + f[j - 2];
+    double var3 = f[j + 3] + f[j - 3];
+    double var4 = f[j + 4] + f[j - 4];
+    double var5 = f[j + 5] + f[j - 5];
+    D(j) = s.coef10i[0] * var0 + s.coef10i[1] * var1 + s.coef10i[2] * var2 + s.coef10i[3] * var3 +
+           s.coef10i[4] * var4 + s.coef10i[5] * var5;
+  }
+}
+
+// compact_filter, filter.F90:112-144. scratch >= 2*(dim+7)
+void filter_line(const Scheme& s, const double* f, double* ff, double* scratch) {
+  const int n = s.n();
+  double* d = scratch;
+  double* xx = scratch + n;
+  compact_filter_rhs(s, f, d);
+  thomas_solve(s, d, xx);
+  for (int i = 0; i <= s.dimension; ++i) ff[i] = xx[i - s.first_node];
+  if (s.nbctype == 1 || s.nbctype == 4) ff[0] = f[0];
+  if (s.nbctype == 2 || s.nbctype == 4) ff[s.dimension] = f[s.dimension];
+}
+
+// ---------------------------------------------------------------- 3-D helpers
+// Fortran-ordered array a(l0:l0+n0-1, l1:l1+n1-1, l2:l2+n2-1, 1:nf), first index fastest.
+struct Box {
+  int64_t n[3], l[3];
+  int64_t idx(int64_t i, int64_t j, int64_t k) const {
+    return ((k - l[2]) * n[1] + (j - l[1])) * n[0] + (i - l[0]);
+  }
+  int64_t size() const { return n[0] * n[1] * n[2]; }
+};
+
+// Apply a line operator along `dir` (0,1,2) to every line of every field. Input lines must
+// carry f(-HM..dim+HM) along dir (ntype 3) or f(0..dim) (ntype 4); output spans 0..dim.
+template <class LineFn>
+void apply_lines(const Scheme& s, int dir, const double* f, const Box& bf, int nfields, double* out,
+                 LineFn fn) {
+  Box bo = bf;
+  bo.n[dir] = s.dimension + 1;
+  bo.l[dir] = 0;
+  const int o1 = (dir == 0) ? 1 : 0;
+  const int o2 = (dir == 2) ? 1 : 2;
+  const int64_t n1 = bf.n[o1], n2 = bf.n[o2];
+  const int L = s.dimension + 1 + 2 * HM;
+#pragma omp parallel
+  {
+    std::vector<double> lin(L, 0.0), lout(s.dimension + 1), scr(2 * (s.dimension + 8));
+#pragma omp for collapse(2) schedule(static)
+    for (int64_t b = 0; b < n2; ++b)
+      for (int64_t a = 0; a < n1; ++a) {
+        int64_t ijk[3];
+        ijk[o1] = bf.l[o1] + a;
+        ijk[o2] = bf.l[o2] + b;
+        for (int m = 0; m < nfields; ++m) {
+          const double* fm = f + m * bf.size();
+          double* om = out + m * bo.size();
+          for (int t = -HM; t <= s.dimension + HM; ++t) {
+            int64_t p[3] = {ijk[0], ijk[1], ijk[2]};
+            p[dir] = t;
+            lin[t + HM] = (t >= bf.l[dir] && t < bf.l[dir] + bf.n[dir]) ? fm[bf.idx(p[0], p[1], p[2])] : 0.0;
+          }
+          fn(s, lin.data() + HM, lout.data(), scr.data());
+          for (int t = 0; t <= s.dimension; ++t) {
+            int64_t p[3] = {ijk[0], ijk[1], ijk[2]};
+            p[dir] = t;
+            om[bo.idx(p[0], p[1], p[2])] = lout[t];
+          }
+        }
+      }
+  }
+}
+
+// ---------------------------------------------------------------- TGV miniapp (tgvsolver.F90)
+struct Field3 {
+  int64_t ni, nj, nk, li, lj, lk;
+  std::vector<double> v;
+  void init(int im, int jm, int km, int h, int ncomp) {
+    ni = im + 1 + 2 * h; nj = jm + 1 + 2 * h; nk = km + 1 + 2 * h;
+    li = lj = lk = -h;
+    v.assign((size_t)(ni * nj * nk * ncomp), 0.0);
+  }
+  double& operator()(int64_t i, int64_t j, int64_t k, int m = 0) {
+    return v[(size_t)((((int64_t)m * nk + (k - lk)) * nj + (j - lj)) * ni + (i - li))];
+  }
+};
+
+struct TGV {
+  int im, jm, km;
+  double gamma, mach, reynolds, prandtl, ref_tem, suth;
+  double const1, const2, const3, const4, const5, const6, const7;
+  double dx, dy, dz, deltat, time;
+  int nstep;
+  bool lfilter;
+  Scheme fds[3], flt[3];
+  Field3 q, rho, prs, tmp, vel, qrhs, dvel, dtmp, sigma, qflux, qsave;
+  std::vector<double> hist;   // rows of (nstep, time, tke, enst, diss)
+
+  void setup(int im_, int jm_, int km_, double mach_, double re_, double pr_, double gam_,
+             double ref_tem_, double suth_, double alfa_filter, double beta_halo, double beta_bound,
+             int filter_on) {
+    im = im_; jm = jm_; km = km_;
+    mach = mach_; reynolds = re_; prandtl = pr_; gamma = gam_; ref_tem = ref_tem_; suth = suth_;
+    lfilter = filter_on != 0;
+    const int dims[3] = {im, jm, km};
+    for (int d = 0; d < 3; ++d) {
+      fd_scheme_initiate(fds[d], "643c", 3, dims[d]);
+      compact_filter_initiate(flt[d], 3, dims[d], alfa_filter, false);
+      filter_coefficient_cal(flt[d], alfa_filter, beta_halo, beta_bound);
+    }
+    q.init(im, jm, km, HM, 5); rho.init(im, jm, km, HM, 1); prs.init(im, jm, km, HM, 1);
+    tmp.init(im, jm, km, HM, 1); vel.init(im, jm, km, HM, 3);
+    qrhs.init(im, jm, km, 0, 5); dvel.init(im, jm, km, 0, 9); dtmp.init(im, jm, km, 0, 3);
+    sigma.init(im, jm, km, HM, 6); qflux.init(im, jm, km, HM, 3); qsave.init(im, jm, km, 0, 5);
+    // flowfield_init constants, tgvsolver.F90:189-195
+    const1 = 1.0 / (gamma * (gamma - 1.0) * (mach * mach));
+    const2 = gamma * (mach * mach);
+    const3 = (gamma - 1.0) / 3.0 * prandtl * (mach * mach);
+    const4 = (gamma - 1.0) * (mach * mach) * reynolds * prandtl;
+    const5 = (gamma - 1.0) * (mach * mach);
+    const6 = 1.0 / (gamma - 1.0);
+    const7 = (gamma - 1.0) * (mach * mach) * reynolds * prandtl;
+    const double pi = 4.0 * std::atan(1.0);
+    dx = 2.0 * pi / double(im); dy = 2.0 * pi / double(jm); dz = 2.0 * pi / double(km);
+    nstep = 0; time = 0.0; deltat = 1e-3;
+    hist.clear();
+  }
+
+  // fvar2q with pressure, tgvsolver.F90:48-71
+  void fvar2q(double* qq, double density, const double* u, double pressure) const {
+    qq[0] = density;
+    qq[1] = density * u[0];
+    qq[2] = density * u[1];
+    qq[3] = density * u[2];
+    double var1 = 0.5 * (u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
+    qq[4] = pressure * const6 + density * var1;
+  }
+  // q2fvar with temperature, tgvsolver.F90:92-121
+  void q2fvar(const double* qq, double& density, double* u, double& pressure, double& temperature) const {
+    density = qq[0];
+    u[0] = qq[1] / density; u[1] = qq[2] / density; u[2] = qq[3] / density;
+    pressure = (qq[4] - 0.5 * density * (u[0] * u[0] + u[1] * u[1] + u[2] * u[2])) / const6;
+    temperature = pressure / density * const2;
+  }
+  double miucal(double t) const {  // tgvsolver.F90:123-140
+    double tc = suth / ref_tem;
+    double tc1 = 1.0 + tc;
+    return t * std::sqrt(t) * tc1 / (t + tc);
+  }
+
+  // flowfield_init, tgvsolver.F90:172-234
+  void init_tgv() {
+    const double pi = 4.0 * std::atan(1.0);
+    const double pinf = 1.0 / const2;
+    for (int k = 0; k <= km; ++k)
+      for (int j = 0; j <= jm; ++j)
+        for (int i = 0; i <= im; ++i) {
+          double x1 = 2.0 * pi / double(im) * double(i);
+          double x2 = 2.0 * pi / double(jm) * double(j);
+          double x3 = 2.0 * pi / double(km) * double(k);
+          rho(i, j, k) = 1.0;
+          vel(i, j, k, 0) = std::sin(x1) * std::cos(x2) * std::cos(x3);
+          vel(i, j, k, 1) = -std::cos(x1) * std::sin(x2) * std::cos(x3);
+          vel(i, j, k, 2) = 0.0;
+          prs(i, j, k) = pinf + 1.0 / 16.0 * (std::cos(2.0 * x1) + std::cos(2.0 * x2)) * (std::cos(2.0 * x3) + 2.0);
+          tmp(i, j, k) = prs(i, j, k) / rho(i, j, k) * const2;
+          double u[3] = {vel(i, j, k, 0), vel(i, j, k, 1), vel(i, j, k, 2)};
+          double qq[5];
+          fvar2q(qq, rho(i, j, k), u, prs(i, j, k));
+          for (int m = 0; m < 5; ++m) q(i, j, k, m) = qq[m];
+        }
+    nstep = 0; time = 0.0;
+  }
+
+  // Start from user conserved variables on nodes 0..N (Fortran order, 5 fields); prims by q2fvar.
+  void set_q(const double* qin) {
+    const int64_t n0 = im + 1, n1 = jm + 1, n2 = km + 1, nn = n0 * n1 * n2;
+    for (int k = 0; k <= km; ++k)
+      for (int j = 0; j <= jm; ++j)
+        for (int i = 0; i <= im; ++i) {
+          double qq[5];
+          for (int m = 0; m < 5; ++m) { qq[m] = qin[m * nn + ((int64_t)k * n1 + j) * n0 + i]; q(i, j, k, m) = qq[m]; }
+          double u[3], r, p, t;
+          q2fvar(qq, r, u, p, t);
+          rho(i, j, k) = r; prs(i, j, k) = p; tmp(i, j, k) = t;
+          for (int c = 0; c < 3; ++c) vel(i, j, k, c) = u[c];
+        }
+  }
+  void get_q(double* out) {
+    const int64_t n0 = im + 1, n1 = jm + 1, n2 = km + 1, nn = n0 * n1 * n2;
+    for (int m = 0; m < 5; ++m)
+      for (int k = 0; k <= km; ++k)
+        for (int j = 0; j <= jm; ++j)
+          for (int i = 0; i <= im; ++i) out[m * nn + ((int64_t)k * n1 + j) * n0 + i] = q(i, j, k, m);
+  }
+
+  // bchomo, tgvsolver.F90:271-369
+  void bchomo() {
+    auto setq = [&](int i, int j, int k) {
+      double u[3] = {vel(i, j, k, 0), vel(i, j, k, 1), vel(i, j, k, 2)};
+      double qq[5];
+      fvar2q(qq, rho(i, j, k), u, prs(i, j, k));
+      for (int m = 0; m < 5; ++m) q(i, j, k, m) = qq[m];
+    };
+    auto cp = [&](int i, int j, int k, int si, int sj, int sk) {
+      rho(i, j, k) = rho(si, sj, sk);
+      for (int c = 0; c < 3; ++c) vel(i, j, k, c) = vel(si, sj, sk, c);
+      tmp(i, j, k) = tmp(si, sj, sk);
+      prs(i, j, k) = prs(si, sj, sk);
+      setq(i, j, k);
+    };
+#pragma omp parallel for collapse(2)
+    for (int k = 0; k <= km; ++k)
+      for (int j = 0; j <= jm; ++j) {
+        for (int i = -HM; i <= -1; ++i) cp(i, j, k, im + i, j, k);
+        for (int i = im + 1; i <= im + HM; ++i) cp(i, j, k, i - im, j, k);
+      }
+#pragma omp parallel for collapse(2)
+    for (int k = 0; k <= km; ++k)
+      for (int i = 0; i <= im; ++i) {
+        for (int j = -HM; j <= -1; ++j) cp(i, j, k, i, jm + j, k);
+        for (int j = jm + 1; j <= jm + HM; ++j) cp(i, j, k, i, j - jm, k);
+      }
+#pragma omp parallel for collapse(2)
+    for (int j = 0; j <= jm; ++j)
+      for (int i = 0; i <= im; ++i) {
+        for (int k = -HM; k <= -1; ++k) cp(i, j, k, i, j, km + k);
+        for (int k = km + 1; k <= km + HM; ++k) cp(i, j, k, i, j, k - km);
+      }
+  }
+
+  // bchomovec, tgvsolver.F90:371-440 (ndir: 0 = all, 1..3 one direction)
+  void bchomovec(Field3& var, int ncomp, int ndir) {
+    if (ndir == 1 || ndir == 0) {
+#pragma omp parallel for collapse(2)
+      for (int k = 0; k <= km; ++k)
+        for (int j = 0; j <= jm; ++j)
+          for (int m = 0; m < ncomp; ++m) {
+            for (int i = -HM; i <= -1; ++i) var(i, j, k, m) = var(im + i, j, k, m);
+            for (int i = im + 1; i <= im + HM; ++i) var(i, j, k, m) = var(i - im, j, k, m);
+          }
+    }
+    if (ndir == 2 || ndir == 0) {
+#pragma omp parallel for collapse(2)
+      for (int k = 0; k <= km; ++k)
+        for (int i = 0; i <= im; ++i)
+          for (int m = 0; m < ncomp; ++m) {
+            for (int j = -HM; j <= -1; ++j) var(i, j, k, m) = var(i, jm + j, k, m);
+            for (int j = jm + 1; j <= jm + HM; ++j) var(i, j, k, m) = var(i, j - jm, k, m);
+          }
+    }
+    if (ndir == 3 || ndir == 0) {
+#pragma omp parallel for collapse(2)
+      for (int j = 0; j <= jm; ++j)
+        for (int i = 0; i <= im; ++i)
+          for (int m = 0; m < ncomp; ++m) {
+            for (int k = -HM; k <= -1; ++k) var(i, j, k, m) = var(i, j, km + k, m);
+            for (int k = km + 1; k <= km + HM; ++k) var(i, j, k, m) = var(i, j, k - km, m);
+          }
+    }
+  }
+
+  // Generic line loop: for each line along dir, gather ncolm inputs f(-HM..dim+HM) via `gather`,
+  // take the compact derivative, hand the result to `scatter`.
+  template <class Gather, class Scatter>
+  void line_loop(int dir, int ncolm, Gather gather, Scatter scatter) {
+    const int dims[3] = {im, jm, km};
+    const int dim = dims[dir];
+    const int o1 = (dir == 0) ? 1 : 0, o2 = (dir == 2) ? 1 : 2;
+#pragma omp parallel
+    {
+      std::vector<double> ff((size_t)ncolm * (dim + 1 + 2 * HM)), df((size_t)ncolm * (dim + 1)),
+          scr(2 * (dim + 8));
+#pragma omp for collapse(2) schedule(static)
+      for (int b = 0; b <= dims[o2]; ++b)
+        for (int a = 0; a <= dims[o1]; ++a) {
+          int ijk[3];
+          ijk[o1] = a; ijk[o2] = b; ijk[dir] = 0;
+          for (int n = 0; n < ncolm; ++n) {
+            double* fn = ff.data() + (size_t)n * (dim + 1 + 2 * HM) + HM;
+            for (int t = -HM; t <= dim + HM; ++t) {
+              int p[3] = {ijk[0], ijk[1], ijk[2]};
+              p[dir] = t;
+              fn[t] = gather(n, p[0], p[1], p[2]);
+            }
+          }
+          for (int n = 0; n < ncolm; ++n)
+            df_line(fds[dir], ff.data() + (size_t)n * (dim + 1 + 2 * HM) + HM, df.data() + (size_t)n * (dim + 1), scr.data());
+          for (int t = 0; t <= dim; ++t) {
+            int p[3] = {ijk[0], ijk[1], ijk[2]};
+            p[dir] = t;
+            for (int n = 0; n < ncolm; ++n) scatter(n, p[0], p[1], p[2], df[(size_t)n * (dim + 1) + t]);
+          }
+        }
+    }
+  }
+
+  double dstep(int dir) const { return dir == 0 ? dx : (dir == 1 ? dy : dz); }
+
+  // gradcal, tgvsolver.F90:450-537
+  void gradcal() {
+    for (int dir = 0; dir < 3; ++dir) {
+      const double h = dstep(dir);
+      line_loop(dir, 4,
+                [&](int n, int i, int j, int k) { return n < 3 ? vel(i, j, k, n) : tmp(i, j, k); },
+                [&](int n, int i, int j, int k, double v) {
+                  if (n < 3) dvel(i, j, k, n + 3 * dir) = v / h;  // dvel(:,:,:,n,dir)
+                  else dtmp(i, j, k, dir) = v / h;
+                });
+    }
+  }
+
+  // convection, tgvsolver.F90:539-633
+  void convection() {
+    for (int dir = 0; dir < 3; ++dir) {
+      const double h = dstep(dir);
+      line_loop(dir, 5,
+                [&](int n, int i, int j, int k) {
+                  double uu = vel(i, j, k, dir);
+                  if (n == 4) return (q(i, j, k, 4) + prs(i, j, k)) * uu;
+                  if (n == dir + 1) return q(i, j, k, n) * uu + prs(i, j, k);
+                  return q(i, j, k, n) * uu;
+                },
+                [&](int n, int i, int j, int k, double v) { qrhs(i, j, k, n) = qrhs(i, j, k, n) + v / h; });
+    }
+  }
+
+  // diffusion, tgvsolver.F90:635-789
+  void diffusion() {
+#pragma omp parallel for collapse(2)
+    for (int k = 0; k <= km; ++k)
+      for (int j = 0; j <= jm; ++j)
+        for (int i = 0; i <= im; ++i) {
+          double s11 = dvel(i, j, k, 0);
+          double s12 = 0.5 * (dvel(i, j, k, 3) + dvel(i, j, k, 1));
+          double s13 = 0.5 * (dvel(i, j, k, 6) + dvel(i, j, k, 2));
+          double s22 = dvel(i, j, k, 4);
+          double s23 = 0.5 * (dvel(i, j, k, 7) + dvel(i, j, k, 5));
+          double s33 = dvel(i, j, k, 8);
+          double skk = num1d3 * (s11 + s22 + s33);
+          double miu = miucal(tmp(i, j, k)) / reynolds;
+          double miu2 = 2.0 * miu;
+          double hcc = (miu / prandtl) / const5;
+          sigma(i, j, k, 0) = miu2 * (s11 - skk);
+          sigma(i, j, k, 1) = miu2 * s12;
+          sigma(i, j, k, 2) = miu2 * s13;
+          sigma(i, j, k, 3) = miu2 * (s22 - skk);
+          sigma(i, j, k, 4) = miu2 * s23;
+          sigma(i, j, k, 5) = miu2 * (s33 - skk);
+          qflux(i, j, k, 0) = hcc * dtmp(i, j, k, 0) + sigma(i, j, k, 0) * vel(i, j, k, 0) +
+                              sigma(i, j, k, 1) * vel(i, j, k, 1) + sigma(i, j, k, 2) * vel(i, j, k, 2);
+          qflux(i, j, k, 1) = hcc * dtmp(i, j, k, 1) + sigma(i, j, k, 1) * vel(i, j, k, 0) +
+                              sigma(i, j, k, 3) * vel(i, j, k, 1) + sigma(i, j, k, 4) * vel(i, j, k, 2);
+          qflux(i, j, k, 2) = hcc * dtmp(i, j, k, 2) + sigma(i, j, k, 2) * vel(i, j, k, 0) +
+                              sigma(i, j, k, 4) * vel(i, j, k, 1) + sigma(i, j, k, 5) * vel(i, j, k, 2);
+        }
+    bchomovec(sigma, 6, 0);
+    bchomovec(qflux, 3, 0);
+    // (sigma component, qflux component) per direction: x: s1 s2 s3 q1; y: s2 s4 s5 q2; z: s3 s5 s6 q3
+    static const int sg[3][3] = {{0, 1, 2}, {1, 3, 4}, {2, 4, 5}};
+    for (int dir = 0; dir < 3; ++dir) {
+      const double h = dstep(dir);
+      line_loop(dir, 4,
+                [&](int n, int i, int j, int k) { return n < 3 ? sigma(i, j, k, sg[dir][n]) : qflux(i, j, k, dir); },
+                [&](int n, int i, int j, int k, double v) { qrhs(i, j, k, n + 1) = qrhs(i, j, k, n + 1) + v / h; });
+    }
+  }
+
+  // filterq, tgvsolver.F90:791-883
+  void filterq() {
+    const int dims[3] = {im, jm, km};
+    for (int dir = 0; dir < 3; ++dir) {
+      bchomovec(q, 5, dir + 1);
+      const int dim = dims[dir];
+      const int o1 = (dir == 0) ? 1 : 0, o2 = (dir == 2) ? 1 : 2;
+#pragma omp parallel
+      {
+        std::vector<double> phi(dim + 1 + 2 * HM), fph((size_t)5 * (dim + 1)), scr(2 * (dim + 8));
+#pragma omp for collapse(2) schedule(static)
+        for (int b = 0; b <= dims[o2]; ++b)
+          for (int a = 0; a <= dims[o1]; ++a) {
+            int ijk[3];
+            ijk[o1] = a; ijk[o2] = b; ijk[dir] = 0;
+            for (int n = 0; n < 5; ++n) {
+              for (int t = -HM; t <= dim + HM; ++t) {
+                int p[3] = {ijk[0], ijk[1], ijk[2]};
+                p[dir] = t;
+                phi[t + HM] = q(p[0], p[1], p[2], n);
+              }
+              filter_line(flt[dir], phi.data() + HM, fph.data() + (size_t)n * (dim + 1), scr.data());
+            }
+            for (int t = 0; t <= dim; ++t) {
+              int p[3] = {ijk[0], ijk[1], ijk[2]};
+              p[dir] = t;
+              for (int n = 0; n < 5; ++n) q(p[0], p[1], p[2], n) = fph[(size_t)n * (dim + 1) + t];
+            }
+          }
+      }
+    }
+  }
+
+  // stacal, tgvsolver.F90:893-942, plus diss_rate_cal (statistic.F90:993-1040); sequential sums
+  void stacal() {
+    double tke = 0.0, enst = 0.0, diss = 0.0;
+    for (int k = 1; k <= km; ++k)
+      for (int j = 1; j <= jm; ++j)
+        for (int i = 1; i <= im; ++i) {
+          double var1 = vel(i, j, k, 0) * vel(i, j, k, 0) + vel(i, j, k, 1) * vel(i, j, k, 1) +
+                        vel(i, j, k, 2) * vel(i, j, k, 2);
+          tke = tke + rho(i, j, k) * var1;
+          double om1 = dvel(i, j, k, 2 + 3) - dvel(i, j, k, 1 + 6);
+          double om2 = dvel(i, j, k, 0 + 6) - dvel(i, j, k, 2 + 0);
+          double om3 = dvel(i, j, k, 1 + 0) - dvel(i, j, k, 0 + 3);
+          enst = enst + rho(i, j, k) * (om1 * om1 + om2 * om2 + om3 * om3);
+          double miu = miucal(tmp(i, j, k)) / reynolds;
+          double du11 = dvel(i, j, k, 0), du12 = dvel(i, j, k, 3), du13 = dvel(i, j, k, 6);
+          double du21 = dvel(i, j, k, 1), du22 = dvel(i, j, k, 4), du23 = dvel(i, j, k, 7);
+          double du31 = dvel(i, j, k, 2), du32 = dvel(i, j, k, 5), du33 = dvel(i, j, k, 8);
+          double s11 = du11, s12 = 0.5 * (du12 + du21), s13 = 0.5 * (du13 + du31);
+          double s22 = du22, s23 = 0.5 * (du23 + du32), s33 = du33;
+          double div = s11 + s22 + s33;
+          double v = 2.0 * miu * (s11 * s11 + s22 * s22 + s33 * s33 + 2.0 * (s12 * s12 + s13 * s13 + s23 * s23) -
+                                  num1d3 * (div * div));
+          diss = diss + v;
+        }
+    const double nn = double((int64_t)im * jm * km);
+    tke = 0.5 * tke / nn;
+    enst = 0.5 * enst / nn;
+    diss = diss / nn;
+    hist.push_back(nstep); hist.push_back(time); hist.push_back(tke); hist.push_back(enst); hist.push_back(diss);
+  }
+
+  // rhscal, tgvsolver.F90:962-992
+  void rhscal() {
+    std::fill(qrhs.v.begin(), qrhs.v.end(), 0.0);
+    gradcal();
+    convection();
+    for (double& v : qrhs.v) v = -v;
+    diffusion();
+  }
+
+  void update_prims() {
+#pragma omp parallel for collapse(2)
+    for (int k = 0; k <= km; ++k)
+      for (int j = 0; j <= jm; ++j)
+        for (int i = 0; i <= im; ++i) {
+          double qq[5] = {q(i, j, k, 0), q(i, j, k, 1), q(i, j, k, 2), q(i, j, k, 3), q(i, j, k, 4)};
+          double u[3], r, p, t;
+          q2fvar(qq, r, u, p, t);
+          rho(i, j, k) = r; prs(i, j, k) = p; tmp(i, j, k) = t;
+          for (int c = 0; c < 3; ++c) vel(i, j, k, c) = u[c];
+        }
+  }
+
+  // rk3, tgvsolver.F90:994-1082, and the step counter of steploop (:944-960)
+  void rk3() {
+    static const double rkcoe[3][3] = {{1.0, 0.0, 1.0}, {0.75, 0.25, 0.25}, {num1d3, num2d3, num2d3}};
+    for (int rk = 0; rk < 3; ++rk) {
+      bchomo();
+      rhscal();
+      if (rk == 0) {
+        stacal();
+#pragma omp parallel for collapse(2)
+        for (int k = 0; k <= km; ++k)
+          for (int j = 0; j <= jm; ++j)
+            for (int i = 0; i <= im; ++i)
+              for (int m = 0; m < 5; ++m) qsave(i, j, k, m) = q(i, j, k, m);
+      }
+      const double c1 = rkcoe[rk][0], c2 = rkcoe[rk][1], c3 = rkcoe[rk][2];
+#pragma omp parallel for collapse(2)
+      for (int k = 0; k <= km; ++k)
+        for (int j = 0; j <= jm; ++j)
+          for (int i = 0; i <= im; ++i)
+            for (int m = 0; m < 5; ++m)
+              q(i, j, k, m) = c1 * qsave(i, j, k, m) + c2 * q(i, j, k, m) + c3 * qrhs(i, j, k, m) * deltat;
+      if (lfilter) filterq();
+      update_prims();
+    }
+    nstep += 1;
+    time = time + deltat;
+  }
+
+  // cflcal's spectral-radius sum (commcal.F90:46-77) on a uniform grid, dxi = diag(1/dx,1/dy,1/dz)
+  double cfl_dt(double cfl) {
+    double di = 0.0, dj = 0.0, dk = 0.0;
+    const double dxi[3] = {1.0 / dx, 1.0 / dy, 1.0 / dz};
+    for (int k = 0; k <= km; ++k)
+      for (int j = 0; j <= jm; ++j)
+        for (int i = 0; i <= im; ++i) {
+          double ubar = dxi[0] * vel(i, j, k, 0), vbar = dxi[1] * vel(i, j, k, 1), wbar = dxi[2] * vel(i, j, k, 2);
+          double css = std::sqrt(tmp(i, j, k)) / mach;
+          double csi = css * std::sqrt(dxi[0] * dxi[0]), csj = css * std::sqrt(dxi[1] * dxi[1]),
+                 csk = css * std::sqrt(dxi[2] * dxi[2]);
+          di = std::max({di, ubar, ubar - csi, ubar + csi});
+          dj = std::max({dj, vbar, vbar - csj, vbar + csj});
+          dk = std::max({dk, wbar, wbar - csk, wbar + csk});
+        }
+    return cfl / (di + dj + dk);
+  }
+};
+
+}  // namespace
+
+// ================================================================ C entry points (ctypes)
+extern "C" {
+
+void* orc_fd_scheme_create(const char* scheme, int ntype, int dim) {
+  Scheme* s = new Scheme();
+  if (!fd_scheme_initiate(*s, scheme, ntype, dim)) { delete s; return nullptr; }
+  return s;
+}
+void* orc_filter_create(int ntype, int dim, double alfa, double beta_halo, double beta_bound, int no_filter_note) {
+  Scheme* s = new Scheme();
+  compact_filter_initiate(*s, ntype, dim, alfa, no_filter_note != 0);
+  filter_coefficient_cal(*s, alfa, beta_halo, beta_bound);
+  return s;
+}
+void orc_scheme_free(void* h) { delete static_cast<Scheme*>(h); }
+int orc_scheme_info(void* h, int* first_node, int* last_node) {
+  Scheme* s = static_cast<Scheme*>(h);
+  *first_node = s->first_node; *last_node = s->last_node;
+  return s->n();
+}
+void orc_scheme_ac(void* h, double* ac1, double* ac2, double* ac3) {
+  Scheme* s = static_cast<Scheme*>(h);
+  for (int i = 0; i < s->n(); ++i) { ac1[i] = s->ac1[i]; ac2[i] = s->ac2[i]; ac3[i] = s->ac3[i]; }
+}
+
+// One line: f holds f(-5..dim+5), out holds dim+1 values.
+void orc_deriv_line(void* h, const double* f, double* out) {
+  Scheme* s = static_cast<Scheme*>(h);
+  std::vector<double> scr(2 * (s->dimension + 8));
+  df_line(*s, f + HM, out, scr.data());
+}
+void orc_filter_line(void* h, const double* f, double* out) {
+  Scheme* s = static_cast<Scheme*>(h);
+  std::vector<double> scr(2 * (s->dimension + 8));
+  filter_line(*s, f + HM, out, scr.data());
+}
+
+// Every line of a Fortran-ordered multi-field array; output extent along dir is 0..dim.
+void orc_deriv3d(void* h, int dir, const double* f, const int64_t* shape, const int64_t* lbound, int nfields, double* out) {
+  Scheme* s = static_cast<Scheme*>(h);
+  Box b{{shape[0], shape[1], shape[2]}, {lbound[0], lbound[1], lbound[2]}};
+  apply_lines(*s, dir, f, b, nfields, out, [](const Scheme& sc, const double* fi, double* o, double* scr) { df_line(sc, fi, o, scr); });
+}
+void orc_filter3d(void* h, int dir, const double* f, const int64_t* shape, const int64_t* lbound, int nfields, double* out) {
+  Scheme* s = static_cast<Scheme*>(h);
+  Box b{{shape[0], shape[1], shape[2]}, {lbound[0], lbound[1], lbound[2]}};
+  apply_lines(*s, dir, f, b, nfields, out, [](const Scheme& sc, const double* fi, double* o, double* scr) { filter_line(sc, fi, o, scr); });
+}
+
+void* orc_tgv_create(int im, int jm, int km, double mach, double re, double pr, double gamma, double ref_tem,
+                     double suth, double alfa_filter, double beta_halo, double beta_bound, int filter_on) {
+  TGV* t = new TGV();
+  t->setup(im, jm, km, mach, re, pr, gamma, ref_tem, suth, alfa_filter, beta_halo, beta_bound, filter_on);
+  return t;
+}
+void orc_tgv_free(void* h) { delete static_cast<TGV*>(h); }
+void orc_tgv_init_tgv(void* h) { static_cast<TGV*>(h)->init_tgv(); }
+void orc_tgv_set_q(void* h, const double* q) { static_cast<TGV*>(h)->set_q(q); }
+void orc_tgv_get_q(void* h, double* q) { static_cast<TGV*>(h)->get_q(q); }
+void orc_tgv_set_dt(void* h, double dt) { static_cast<TGV*>(h)->deltat = dt; }
+double orc_tgv_cfl_dt(void* h, double cfl) { return static_cast<TGV*>(h)->cfl_dt(cfl); }
+void orc_tgv_steps(void* h, int n) { TGV* t = static_cast<TGV*>(h); for (int s = 0; s < n; ++s) t->rk3(); }
+int orc_tgv_history(void* h, double* out, int maxrows) {
+  TGV* t = static_cast<TGV*>(h);
+  int rows = (int)(t->hist.size() / 5);
+  int nr = std::min(rows, maxrows);
+  std::memcpy(out, t->hist.data(), sizeof(double) * 5 * nr);
+  return rows;
+}
+// One rhscal on the current state (after the halo fill): qrhs on nodes 0..N, Fortran order.
+void orc_tgv_rhs(void* h, double* out) {
+  TGV* t = static_cast<TGV*>(h);
+  t->bchomo();
+  t->rhscal();
+  const int64_t n0 = t->im + 1, n1 = t->jm + 1, n2 = t->km + 1, nn = n0 * n1 * n2;
+  for (int m = 0; m < 5; ++m)
+    for (int k = 0; k <= t->km; ++k)
+      for (int j = 0; j <= t->jm; ++j)
+        for (int i = 0; i <= t->im; ++i) out[m * nn + ((int64_t)k * n1 + j) * n0 + i] = t->qrhs(i, j, k, m);
+}
+// Diagnostics of the current state computed the way stacal does (needs one gradcal).
+void orc_tgv_diagnostics(void* h, double* out3) {
+  TGV* t = static_cast<TGV*>(h);
+  t->bchomo();
+  t->gradcal();
+  t->stacal();
+  size_t n = t->hist.size();
+  out3[0] = t->hist[n - 3]; out3[1] = t->hist[n - 2]; out3[2] = t->hist[n - 1];
+  t->hist.resize(n - 5);
+}
+int orc_num_threads() {
+#ifdef _OPENMP
+  return omp_get_max_threads();
+#else
+  return 1;
+#endif
+}
+void orc_set_num_threads(int n) {
+#ifdef _OPENMP
+  if (n > 0) omp_set_num_threads(n);
+#else
+  (void)n;
+#endif
+}
+
+}  // extern "C"
