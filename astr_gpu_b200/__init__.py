@@ -1,0 +1,269 @@
+"""B200-native (sm_100a) implementation of ASTR's per-step RHS hot path.
+
+Host-side mirror of the reference's interface (Perrbit/astr_gpu), over the C ABI of
+``include/astr_b200.h``:
+
+* ``fd_scheme_initiate`` / ``compact_filter_initiate``  (src/derivative.F90:63, src/filter.F90:31)
+* ``central`` — ``fds%central`` over every line of an array (src/derivative.F90:22-41)
+* ``compact_filter`` — every line of an array (src/filter.F90:112)
+* ``TGVSolver`` — the Taylor-Green miniapp driver: ``flowfield_init``, ``rhscal``, ``rk3``,
+  ``stacal`` (miniapps/tgv_solver_3d/tgvsolver.F90)
+
+Arrays are Fortran-ordered numpy arrays (host) or CUDA torch tensors laid out the same way
+(device). All compute runs in the CUDA library; there is no CPU path.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass, fields
+
+import numpy as np
+
+from . import _lib
+from ._lib import ASTR_DEVICE, ASTR_HOST, AstrParams
+
+__all__ = ["AstrError", "Context", "Scheme", "fd_scheme_initiate", "compact_filter_initiate", "central",
+           "compact_filter", "FlowParams", "TGVSolver"]
+
+
+class AstrError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"astr error {code}: {msg}")
+        self.code = code
+
+
+def _i64(v):
+    return (ctypes.c_int64 * 3)(*[int(x) for x in v])
+
+
+class Context:
+    """One device and one CUDA stream (``astr_init``). ``stream`` may be a ``torch.cuda.Stream``
+    or a raw ``cudaStream_t`` integer; by default the library owns a non-blocking stream."""
+
+    def __init__(self, device: int = 0, stream=None):
+        self.L = _lib.load()
+        h = ctypes.c_void_p()
+        rc = self.L.astr_init(device, ctypes.byref(h))
+        if rc != 0:
+            raise AstrError(rc, "astr_init failed (no CUDA device?)")
+        self._h = h
+        self.device = device
+        if stream is not None:
+            raw = getattr(stream, "cuda_stream", stream)
+            self.check(self.L.astr_set_stream(self._h, ctypes.c_void_p(int(raw))))
+
+    def check(self, rc):
+        if rc != 0:
+            raise AstrError(rc, self.L.astr_last_error(self._h).decode())
+        return rc
+
+    def synchronize(self):
+        self.check(self.L.astr_synchronize(self._h))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self.L.astr_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Scheme:
+    """A ``compact_scheme`` living on the device (derivative or filter)."""
+
+    def __init__(self, ctx: Context, h, dim: int, ntype: int, is_filter: bool):
+        self.ctx, self._h, self.dim, self.ntype, self.is_filter = ctx, h, dim, ntype, is_filter
+
+    def ac(self):
+        """(first_node, last_node, ac(3,n)) — the pre-factored Thomas table."""
+        n = 0
+        f, l = ctypes.c_int(), ctypes.c_int()
+        buf = np.zeros(3 * (self.dim + 7))
+        self.ctx.check(self.ctx.L.astr_scheme_ac(self._h, buf.ctypes.data_as(_lib._dp), ctypes.byref(f), ctypes.byref(l)))
+        n = l.value - f.value + 1
+        return f.value, l.value, buf[: 3 * n].reshape(n, 3).T.copy()
+
+    def __del__(self):
+        try:
+            if getattr(self, "_h", None):
+                self.ctx.L.astr_scheme_destroy(self._h)
+                self._h = None
+        except Exception:
+            pass
+
+
+def fd_scheme_initiate(ctx: Context, scheme: str, ntype: int, dim: int) -> Scheme:
+    """derivative.F90:63 — '643c' (compact 6th order) or '643e' (explicit 6th order)."""
+    h = ctypes.c_void_p()
+    ctx.check(ctx.L.astr_fd_scheme_create(ctx._h, scheme.encode()[:4], ntype, dim, ctypes.byref(h)))
+    return Scheme(ctx, h, dim, ntype, False)
+
+
+def compact_filter_initiate(ctx: Context, ntype: int, dim: int, alfa: float = 0.49, beta_halo: float = 1.11,
+                            beta_bound: float = 0.98, note: str | None = None) -> Scheme:
+    """filter.F90:31 with filter_coefficient_cal(alfa, beta_halo, beta_bound) (filter.F90:299)."""
+    h = ctypes.c_void_p()
+    ctx.check(ctx.L.astr_filter_create(ctx._h, ntype, dim, alfa, beta_halo, beta_bound,
+                                       int(note == "boundary_no_filter"), ctypes.byref(h)))
+    return Scheme(ctx, h, dim, ntype, True)
+
+
+def _is_torch(x):
+    return type(x).__module__.startswith("torch")
+
+
+def _apply(ctx, scheme, f, direction, lbound, out_lbound, out_shape, scale, is_filter):
+    dim = scheme.dim
+    nf = f.shape[3] if f.ndim == 4 else 1
+    fshape = list(f.shape[:3])
+    lb = list(lbound)
+    oshape = list(out_shape) if out_shape is not None else [fshape[d] if d != direction else dim + 1 for d in range(3)]
+    olb = list(out_lbound) if out_lbound is not None else [lb[d] if d != direction else 0 for d in range(3)]
+    if _is_torch(f):
+        import torch
+        assert f.is_cuda and f.dtype == torch.float64
+        # Fortran order <=> the tensor's strides are column-major
+        fp = f
+        out = torch.empty(tuple(oshape) + ((nf,) if f.ndim == 4 else ()), dtype=torch.float64, device=f.device)
+        out = out.permute(*reversed(range(out.ndim))).contiguous().permute(*reversed(range(out.ndim)))
+        assert fp.stride(0) == 1 and out.stride(0) == 1, "device arrays must be Fortran-ordered"
+        torch.cuda.current_stream(f.device).synchronize()
+        fptr, optr, where = fp.data_ptr(), out.data_ptr(), ASTR_DEVICE
+    else:
+        fp = np.asfortranarray(f, dtype=np.float64)
+        out = np.zeros(tuple(oshape) + ((nf,) if f.ndim == 4 else ()), order="F")
+        fptr, optr, where = fp.ctypes.data, out.ctypes.data, ASTR_HOST
+    L = ctx.L
+    if is_filter:
+        ctx.check(L.astr_filter_lines(ctx._h, scheme._h, direction, ctypes.c_void_p(fptr), _i64(fshape), _i64(lb),
+                                      ctypes.c_void_p(optr), _i64(oshape), _i64(olb), nf, where))
+    else:
+        ctx.check(L.astr_deriv_lines(ctx._h, scheme._h, direction, ctypes.c_void_p(fptr), _i64(fshape), _i64(lb),
+                                     ctypes.c_void_p(optr), _i64(oshape), _i64(olb), nf, float(scale), where))
+    if where == ASTR_DEVICE:
+        ctx.synchronize()
+    return out
+
+
+def central(ctx: Context, scheme: Scheme, f, direction: int, lbound=(0, 0, 0), scale: float = 1.0,
+            out_lbound=None, out_shape=None):
+    """``df = fds%central(asolver, f, dim)`` for every line of ``f`` along ``direction``.
+    ``f(lbound...)`` must carry nodes -5..dim+5 along ``direction`` when the scheme reads halos.
+    The result spans nodes 0..dim along ``direction`` (index-space derivative times ``scale``)."""
+    return _apply(ctx, scheme, f, direction, lbound, out_lbound, out_shape, scale, False)
+
+
+def compact_filter(ctx: Context, scheme: Scheme, f, direction: int, lbound=(0, 0, 0), out_lbound=None,
+                   out_shape=None):
+    """``ff = compact_filter(afilter, f, dim)`` for every line of ``f`` along ``direction``."""
+    return _apply(ctx, scheme, f, direction, lbound, out_lbound, out_shape, 1.0, True)
+
+
+@dataclass
+class FlowParams:
+    """commvar of the miniapp (tgvsolver.F90:152-195, :253)."""
+    mach: float = 0.1
+    reynolds: float = 1600.0
+    prandtl: float = 0.72
+    gamma: float = 1.4
+    ref_tem: float = 273.15
+    sutherland: float = 110.4
+    alfa_filter: float = 0.49
+    beta_halo: float = 1.11
+    beta_bound: float = 1.09
+    filter_on: bool = True
+
+
+class TGVSolver:
+    """The miniapp ``boxsolver`` on the GPU: a periodic im x jm x km box advanced by SSP-RK3 with
+    the compact scheme and the compact filter (tgvsolver.F90:994-1082)."""
+
+    def __init__(self, ctx: Context, im: int, jm: int | None = None, km: int | None = None,
+                 params: FlowParams | None = None):
+        self.ctx = ctx
+        self.im, self.jm, self.km = im, jm or im, km or im
+        p = params or FlowParams()
+        self.params = p
+        cp = AstrParams(self.im, self.jm, self.km, p.mach, p.reynolds, p.prandtl, p.gamma, p.ref_tem, p.sutherland,
+                        p.alfa_filter, p.beta_halo, p.beta_bound, int(p.filter_on))
+        h = ctypes.c_void_p()
+        ctx.check(ctx.L.astr_state_create(ctx._h, ctypes.byref(cp), ctypes.byref(h)))
+        self._h = h
+
+    @property
+    def shape(self):
+        return (self.im + 1, self.jm + 1, self.km + 1)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self.ctx.L.astr_state_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def init_tgv(self):
+        """flowfield_init (tgvsolver.F90:172-234)."""
+        self.ctx.check(self.ctx.L.astr_state_init_tgv(self._h))
+
+    def set_q(self, q, lbound=(0, 0, 0)):
+        L = self.ctx.L
+        if _is_torch(q):
+            assert q.stride(0) == 1
+            self.ctx.check(L.astr_state_upload(self._h, ctypes.c_void_p(q.data_ptr()), _i64(q.shape[:3]), _i64(lbound),
+                                               ASTR_DEVICE))
+        else:
+            qf = np.asfortranarray(q, dtype=np.float64)
+            self.ctx.check(L.astr_state_upload(self._h, ctypes.c_void_p(qf.ctypes.data), _i64(qf.shape[:3]),
+                                               _i64(lbound), ASTR_HOST))
+
+    def get_q(self) -> np.ndarray:
+        out = np.zeros(self.shape + (5,), order="F")
+        self.ctx.check(self.ctx.L.astr_state_download(self._h, ctypes.c_void_p(out.ctypes.data), _i64(self.shape),
+                                                      _i64((0, 0, 0)), ASTR_HOST))
+        return out
+
+    def cfl_dt(self, cfl: float) -> float:
+        dt = ctypes.c_double()
+        self.ctx.check(self.ctx.L.astr_cfl_dt(self._h, cfl, ctypes.byref(dt)))
+        return dt.value
+
+    def rhs(self) -> np.ndarray:
+        out = np.zeros(self.shape + (5,), order="F")
+        self.ctx.check(self.ctx.L.astr_rhs(self._h, ctypes.c_void_p(out.ctypes.data), _i64(self.shape),
+                                           _i64((0, 0, 0)), ASTR_HOST))
+        return out
+
+    def rk3(self, dt: float, nsteps: int = 1):
+        self.ctx.check(self.ctx.L.astr_rk3_step(self._h, dt, nsteps))
+
+    def rk3_host(self, q: np.ndarray, dt: float, nsteps: int = 1) -> np.ndarray:
+        """One call with the state in host memory (uploaded, advanced, downloaded in place)."""
+        assert q.flags["F_CONTIGUOUS"] and q.dtype == np.float64
+        diag = np.zeros(3)
+        self.ctx.check(self.ctx.L.astr_rk3_step_host(self._h, ctypes.c_void_p(q.ctypes.data), _i64(q.shape[:3]),
+                                                     _i64((0, 0, 0)), dt, nsteps, diag.ctypes.data_as(_lib._dp)))
+        return diag
+
+    def history(self) -> np.ndarray:
+        """stacal rows (nstep, time, tke, enstrophy, dissipation)."""
+        n = ctypes.c_int()
+        self.ctx.check(self.ctx.L.astr_history(self._h, None, 0, ctypes.byref(n)))
+        out = np.zeros(max(n.value, 1) * 5)
+        self.ctx.check(self.ctx.L.astr_history(self._h, out.ctypes.data_as(_lib._dp), n.value, ctypes.byref(n)))
+        return out[: 5 * n.value].reshape(n.value, 5)
+
+    def diagnostics(self) -> np.ndarray:
+        out = np.zeros(3)
+        self.ctx.check(self.ctx.L.astr_diagnostics(self._h, out.ctypes.data_as(_lib._dp)))
+        return out
+
+    def use_graph(self, on: bool):
+        self.ctx.check(self.ctx.L.astr_state_use_graph(self._h, int(on)))

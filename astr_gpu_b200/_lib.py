@@ -1,0 +1,74 @@
+"""ctypes loader for libastr_b200.so (the sm_100a C ABI declared in include/astr_b200.h).
+
+The library is built in-tree by ``python -m astr_gpu_b200.build``. There is no CPU fallback:
+importing a compute entry point without the library raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libastr_b200.so")
+
+ASTR_OK, ASTR_ERR_ARG, ASTR_ERR_CUDA, ASTR_ERR_STATE, ASTR_ERR_UNSUPPORTED, ASTR_ERR_NOMEM = 0, -1, -2, -3, -4, -5
+ASTR_HOST, ASTR_DEVICE = 0, 1
+
+_vp = ctypes.c_void_p
+_pvp = ctypes.POINTER(ctypes.c_void_p)
+_dp = ctypes.POINTER(ctypes.c_double)
+_i64p = ctypes.POINTER(ctypes.c_int64)
+_ip = ctypes.POINTER(ctypes.c_int)
+_i = ctypes.c_int
+_d = ctypes.c_double
+
+
+class AstrParams(ctypes.Structure):
+    _fields_ = [("im", _i), ("jm", _i), ("km", _i), ("mach", _d), ("reynolds", _d), ("prandtl", _d),
+                ("gamma", _d), ("ref_tem", _d), ("sutherland", _d), ("alfa_filter", _d), ("beta_halo", _d),
+                ("beta_bound", _d), ("filter_on", _i)]
+
+
+SIGNATURES = {
+    "astr_init": (_i, [_i, _pvp]),
+    "astr_destroy": (_i, [_vp]),
+    "astr_last_error": (ctypes.c_char_p, [_vp]),
+    "astr_set_stream": (_i, [_vp, _vp]),
+    "astr_synchronize": (_i, [_vp]),
+    "astr_fd_scheme_create": (_i, [_vp, ctypes.c_char_p, _i, _i, _pvp]),
+    "astr_filter_create": (_i, [_vp, _i, _i, _d, _d, _d, _i, _pvp]),
+    "astr_scheme_destroy": (_i, [_vp]),
+    "astr_scheme_ac": (_i, [_vp, _dp, _ip, _ip]),
+    "astr_deriv_lines": (_i, [_vp, _vp, _i, _vp, _i64p, _i64p, _vp, _i64p, _i64p, _i, _d, _i]),
+    "astr_filter_lines": (_i, [_vp, _vp, _i, _vp, _i64p, _i64p, _vp, _i64p, _i64p, _i, _i]),
+    "astr_state_create": (_i, [_vp, ctypes.POINTER(AstrParams), _pvp]),
+    "astr_state_destroy": (_i, [_vp]),
+    "astr_state_init_tgv": (_i, [_vp]),
+    "astr_state_upload": (_i, [_vp, _vp, _i64p, _i64p, _i]),
+    "astr_state_download": (_i, [_vp, _vp, _i64p, _i64p, _i]),
+    "astr_cfl_dt": (_i, [_vp, _d, _dp]),
+    "astr_rhs": (_i, [_vp, _vp, _i64p, _i64p, _i]),
+    "astr_rk3_step": (_i, [_vp, _d, _i]),
+    "astr_rk3_step_host": (_i, [_vp, _vp, _i64p, _i64p, _d, _i, _dp]),
+    "astr_history": (_i, [_vp, _dp, _i, _ip]),
+    "astr_diagnostics": (_i, [_vp, _dp]),
+    "astr_state_use_graph": (_i, [_vp, _i]),
+    "astr_pass_timings": (_i, [_vp, _d, _i, _dp]),
+}
+
+_lib = None
+
+
+def load():
+    """Load the shared library (no compute happens here; works on a machine without a GPU)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -m astr_gpu_b200.build`")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib

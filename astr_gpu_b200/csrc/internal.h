@@ -1,0 +1,50 @@
+// Host-side internals shared by the C-ABI implementation and the kernel launchers.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "ops.cuh"
+
+namespace astr {
+
+// A line operator as built on the host: the reference's compact_scheme (a, c, ac) plus the
+// RHS coefficients, and the device copy of its lane tables for one (S, WPL) layout.
+struct HostOp {
+  int kind = OP_DERIV;
+  int ntype = 3, dim = 0, first_node = 0, last_node = 0;
+  bool left_phys = false, right_phys = false, no_note = false;
+  std::vector<double> a, c, ac1, ac2, ac3;
+  double c10[6] = {0}, ch[3][11] = {{0}}, cb[3][7] = {{0}}, c6[4] = {0}, c8[5] = {0};
+  int nsys() const { return last_node - first_node + 1; }
+};
+
+bool build_fd_op(HostOp& op, const char* scheme, int ntype, int dim);
+void build_filter_op(HostOp& op, int ntype, int dim, double alfa, double beta_halo, double beta_bound, bool note);
+// Lane tables for S rows per lane and nseg segments (see ops.cuh). Returns host vector.
+std::vector<double> lane_tables(const HostOp& op, int S, int nseg);
+
+// Solve layout: S rows per lane, WPL warps per line.
+struct Layout { int S, WPL; };
+Layout pick_layout(int nsys_max);
+
+// Device-resident line operator for a given layout.
+struct DevOp {
+  LineOp op{};
+  double* dtab = nullptr;
+  int S = 0, WPL = 0;
+};
+cudaError_t make_devop(const HostOp& h, Layout lay, DevOp& out);
+void free_devop(DevOp& d);
+
+// Tile line pitch (doubles) for TI lines of dim+1 nodes plus halos, chosen so that line-fastest
+// shared-memory accesses of a warp are free of bank conflicts.
+int tile_pitch(int dim, int TI);
+
+// Line-level API launch: op along dir over every line of an arbitrary strided array.
+struct ArrDesc { int64_t s[3]; int64_t lb[3]; int64_t n[3]; int64_t fs; };
+cudaError_t launch_line_api(const DevOp& op, int dir, const double* f, const ArrDesc& fa, double* out,
+                            const ArrDesc& oa, int nfields, double scale, cudaStream_t st);
+
+}  // namespace astr

@@ -1,0 +1,271 @@
+#!/usr/bin/env python
+"""Benchmark: SSP-RK3 steps of the Taylor-Green vortex at 512^3 in FP64 (ASTR miniapp setup:
+Mach 0.1, Re 1600, Pr 0.72, gamma 1.4, Sutherland, 6th-order compact derivatives, 10th-order
+compact filter alpha_f = 0.49 after every stage, dt fixed from CFL 0.5 at t = 0).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--size 512]
+
+One JSON line on rank 0. `value` = grid-point RK3 updates/s over all ranks (each rank advances
+its own 512^3 box: replicas, weak scaling), device-timed with CUDA events on the library's stream,
+max over ranks. `e2e` = the same metric through the host-buffer C-ABI call (astr_rk3_step_host:
+upload q, one step, download q + diagnostics, every step). `--impl reference` times the CPU
+restatement of the reference (the oracle) on all host threads on a bounded sample.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "RK3 grid-point updates/s FP64 TGV 512³ + %HBM peak; adjoint:forward step time"
+UNIT = "grid-point RK3 updates/s"
+B_ALG_STEP = 2720.0      # algorithmic bytes per unique grid point per RK3 step (pass model)
+# fields read + written per stored point by one launch of each pass (A with the filter)
+PASS_NAMES = ["A", "B", "C", "A'", "B'", "F"]
+PASS_FIELDS = {"A": 19, "B": 19, "C": 30, "A'": 12, "B'": 67 / 3, "F": 10}
+PASS_PER_STEP = {"A": 3, "B": 3, "C": 3, "A'": 3, "B'": 3, "F": 3}
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if len(r) > 5 + i and r[5 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def dist_setup(args):
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def cpu_reference(n, steps, warmup):
+    """The oracle (CPU restatement of the reference miniapp) on all host threads."""
+    import oracle
+    threads = os.cpu_count() or 1
+    oracle.set_num_threads(threads)
+    o = oracle.TGVOracle(n)
+    o.init_tgv()
+    o.set_dt(o.cfl_dt(0.5))
+    o.steps(warmup)
+    t0 = time.perf_counter()
+    o.steps(steps)
+    dt = time.perf_counter() - t0
+    return n ** 3 * steps / dt, dt, oracle.num_threads()
+
+
+def run_reference(args, ws, rank):
+    if rank != 0:
+        return
+    n = args.ref_size
+    value, secs, cores = cpu_reference(n, args.steps, max(args.warmup, 0))
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * secs / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (analytic Taylor-Green initial field)",
+        "config": {"workload": f"TGV {args.size}^3 FP64 SSP-RK3 + compact filter (CPU sample {n}^3)",
+                   "grid": args.size, "sample_grid": n},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": f"oracle restatement of the reference miniapp (no Fortran compiler on the box), "
+                                   f"TGV {n}^3, one RK3 step per bench step, {cores} OpenMP threads"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, ws, rank, local):
+    import numpy as np
+    import torch
+    import astr_gpu_b200 as ag
+
+    torch.cuda.set_device(local)
+    pg = None
+    if ws > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+        pg = dist
+    stream = torch.cuda.Stream(device=local)
+    ctx = ag.Context(local, stream=stream)
+    n = args.size
+    s = ag.TGVSolver(ctx, n)
+    s.init_tgv()
+    dt = s.cfl_dt(0.5)
+    s.rk3(dt, args.warmup)
+    ctx.synchronize()
+
+    def barrier():
+        torch.cuda.synchronize(local)
+        if pg:
+            pg.barrier()
+        torch.cuda.synchronize(local)
+
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        s.rk3(dt, args.steps)
+        e1.record(stream)
+        e1.synchronize()
+    barrier()
+    ms = e0.elapsed_time(e1)
+    t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{local}")
+    if pg:
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    ms_max = float(t.item())
+    ms_step = ms_max / args.steps
+    value = ws * n ** 3 * args.steps / (ms_max * 1e-3)
+
+    # live per-pass timing with CUDA events on the library stream (eager launches)
+    per = np.zeros(7)
+    ctx.check(ctx.L.astr_pass_timings(s._h, dt, 2, per.ctypes.data_as(ag._lib._dp)))
+    pk, pk_kind = peaks()
+    pts = (n + 1) ** 3
+    shares = {nm: per[i] * PASS_PER_STEP[nm] for i, nm in enumerate(PASS_NAMES)}
+    dom = max(shares, key=shares.get)
+    di = PASS_NAMES.index(dom)
+    alg_bytes = PASS_FIELDS[dom] * 8.0 * pts
+    achieved = alg_bytes / (per[di] * 1e-3) / 1e9
+    traffic = None
+    tf = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tf):
+        tr = json.load(open(tf)).get(str(n), {}).get(dom)
+        traffic = tr
+    roof = {"kernel": f"pass {dom}", "bound": "hbm", "achieved": achieved, "peak": pk, "unit": "GB/s",
+            "frac": achieved / pk, "traffic": traffic, "peak_kind": pk_kind,
+            "alg_bytes_per_launch": alg_bytes, "ms_per_launch": float(per[di]),
+            "per_pass_ms": {nm: float(per[i]) for i, nm in enumerate(PASS_NAMES)},
+            "diag_reduce_ms": float(per[6])}
+    step_bytes = B_ALG_STEP * n ** 3
+    step_roof = {"bytes_per_step": step_bytes, "achieved": step_bytes / (ms_step * 1e-3) / 1e9, "peak": pk,
+                 "unit": "GB/s", "frac": step_bytes / (ms_step * 1e-3) / 1e9 / pk, "peak_kind": pk_kind}
+
+    # end to end through the host-buffer C-ABI call: upload, one step, download, every step
+    e2e = None
+    if not args.no_e2e:
+        qh = torch.empty((5, n + 1, n + 1, n + 1), dtype=torch.float64, pin_memory=True)
+        q = qh.numpy().transpose(3, 2, 1, 0)          # Fortran-ordered view of pinned memory
+        q[...] = s.get_q()
+        ne = args.e2e_steps
+        s.rk3_host(q, dt, 1)
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(ne):
+            s.rk3_host(q, dt, 1)
+        te = time.perf_counter() - t0
+        tt = torch.tensor([te], dtype=torch.float64, device=f"cuda:{local}")
+        if pg:
+            pg.all_reduce(tt, op=pg.ReduceOp.MAX)
+        te = float(tt.item())
+        qb = 5 * (n + 1) ** 3 * 8
+        e2e = {"value": ws * n ** 3 * ne / te, "unit": UNIT, "h2d_bytes_per_step": qb,
+               "d2h_bytes_per_step": qb + 24, "steps": ne, "call": "astr_rk3_step_host"}
+        del qh
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        cn = args.ref_size
+        v, secs, cores = cpu_reference(cn, args.cpu_steps, 0)
+        cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
+               "sample": f"oracle restatement of the reference miniapp, TGV {cn}^3, {args.cpu_steps} RK3 steps, "
+                         f"{cores} OpenMP threads, {secs:.1f} s"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (analytic Taylor-Green initial field)",
+            "config": {"workload": f"TGV {n}^3 FP64 SSP-RK3 + compact filter, dt from CFL 0.5",
+                       "grid": n, "dt": dt, "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",
+                       "l2": "inputs larger than L2 (5 x 1.1 GB state per box)", "graph": "one CUDA graph per step"},
+            "roofline": roof, "step_roofline": step_roof, "cpu_baseline": cpu, "e2e": e2e,
+            "gpu_launches": 19 * args.steps, "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    s.close()
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--size", type=int, default=512)
+    ap.add_argument("--ref-size", type=int, default=128)
+    ap.add_argument("--cpu-steps", type=int, default=3)
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        print("warning: fewer than 3 warm-up steps", file=sys.stderr)
+    ws, rank, local = dist_setup(args)
+    if args.impl == "reference":
+        run_reference(args, ws, rank)
+    else:
+        run_ours(args, ws, rank, local)
+
+
+if __name__ == "__main__":
+    main()

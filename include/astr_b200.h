@@ -120,6 +120,10 @@ int astr_history(astr_state* st, double* rows, int maxrows, int* nrows);
 int astr_diagnostics(astr_state* st, double out[3]);
 /* Capture each RK3 step as one CUDA graph (default on). */
 int astr_state_use_graph(astr_state* st, int on);
+/* Instrumentation (no counterpart in the reference): run `nsteps` RK3 steps eagerly with CUDA
+ * events around every pass launch on the context stream and return the mean device time of
+ * one launch of each pass, ms[0..6] = A, B, C, A', B', F(C), diagnostics reduce. */
+int astr_pass_timings(astr_state* st, double dt, int nsteps, double ms[7]);
 
 #ifdef __cplusplus
 }
