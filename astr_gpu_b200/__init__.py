@@ -267,3 +267,14 @@ class TGVSolver:
 
     def use_graph(self, on: bool):
         self.ctx.check(self.ctx.L.astr_state_use_graph(self._h, int(on)))
+
+    def autotune(self, on: bool):
+        """Per-pass launch-shape autotuning at the first RK3 step (default on above 100^3)."""
+        self.ctx.check(self.ctx.L.astr_state_autotune(self._h, int(on)))
+
+    def launch_shapes(self) -> dict:
+        """{pass: (rows per lane, warps per line, lines per CTA, tile pitch)}."""
+        buf = (ctypes.c_int * 28)()
+        self.ctx.check(self.ctx.L.astr_state_launch_shapes(self._h, buf))
+        names = ["A", "B", "C", "A'", "B'", "F_C", "F_A"]
+        return {nm: tuple(buf[4 * i:4 * i + 4]) for i, nm in enumerate(names)}

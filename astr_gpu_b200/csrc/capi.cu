@@ -4,6 +4,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <new>
 #include <string>
 #include <vector>
@@ -27,6 +28,13 @@ struct astr_scheme {
   DevOp d;
 };
 
+// Launch shape of one pass: solve layout (S rows per lane, WPL warps per line) and TI lines
+// per CTA with tile pitch LP.
+struct PassCfg { int S = 0, WPL = 0, TI = 0, LP = 0; };
+enum { CFG_A = 0, CFG_B, CFG_C, CFG_VA, CFG_VB, CFG_FC, CFG_FA, NCFG };
+static const int CFG_PASS[NCFG] = {PASS_A, PASS_B, PASS_C, PASS_VA, PASS_VB, PASS_F, PASS_F};
+static const int CFG_DIR[NCFG] = {DIR_A, DIR_B, DIR_C, DIR_A, DIR_B, DIR_C, DIR_A};
+
 struct astr_state {
   astr_ctx* ctx = nullptr;
   astr_params p{};
@@ -40,10 +48,10 @@ struct astr_state {
   int* counter = nullptr;
   int* err = nullptr;
   int hist_cap = 1 << 16;
-  DevOp opd[3], opf[3];
-  Layout lay[3]{};
-  int TI[8][3]{};
-  int LP[8][3]{};
+  HostOp hd[3], hf[3];                     // derivative and filter operators per direction
+  std::map<int, std::pair<DevOp, DevOp>> ops;   // lane tables per (direction, layout)
+  PassCfg cfg[NCFG];                       // launch shape of every pass
+  bool autotune = true, tuned = false;
   bool pending = false;       // filter along DIR_A of the last stage not yet applied
   int nstep = 0;
   double time = 0.0;
@@ -70,18 +78,22 @@ int cuda_fail(astr_ctx* c, cudaError_t e, const char* where) {
 
 // Lines per CTA for a pass along a direction: at most 512 threads and ~110 KB of tiles so that
 // two CTAs fit on an SM.
-int pick_ti(int pass, int dim, int WPL) {
+int pick_ti(int pass, int dim, int WPL, size_t budget = 110 * 1024) {
   int ti_thr = 512 / (WPL * 32);
   if (ti_thr < 1) ti_thr = 1;
   const int ntile = pass_tiles(pass);
   int ti = ti_thr > 16 ? 16 : ti_thr;
+  if (WPL > 1 && ti > 8) ti = 8;   // one named barrier per line: at most 15 lines
   while (ti > 1) {
     const size_t bytes = (size_t)ntile * ti * tile_pitch(dim, ti) * 8;
-    if (bytes <= 110 * 1024) break;
+    if (bytes <= budget) break;
     ti >>= 1;
   }
   return ti;
 }
+
+// Solve layouts compiled into the library (tgv_l*.cu, lines.cu).
+const Layout kLayouts[] = {{3, 1}, {5, 1}, {9, 1}, {5, 2}, {9, 2}, {5, 4}, {9, 4}};
 
 bool covers(const int64_t* shape, const int64_t* lb, int d, int64_t lo, int64_t hi) {
   return lb[d] <= lo && lb[d] + shape[d] - 1 >= hi;
@@ -139,16 +151,36 @@ int line_call(astr_ctx* ctx, const astr_scheme* s, int dir, const double* f, con
   return ASTR_OK;
 }
 
-PassArgs base_args(astr_state* st, int pass, int dir) {
+std::pair<DevOp, DevOp>& get_ops(astr_state* st, int dir, int S, int WPL) {
+  const int key = dir * 10000 + S * 100 + WPL;
+  auto it = st->ops.find(key);
+  if (it != st->ops.end()) return it->second;
+  std::pair<DevOp, DevOp> o;
+  make_devop(st->hd[dir], Layout{S, WPL}, o.first);
+  make_devop(st->hf[dir], Layout{S, WPL}, o.second);
+  return st->ops.emplace(key, o).first->second;
+}
+
+// Number of pass-C CTAs, i.e. of partial sums the diagnostics reduce.
+int diag_parts(astr_state* st) {
+  const int o1 = (DIR_C == 0) ? 1 : 0, o2 = (DIR_C == 2) ? 1 : 2;
+  const int ti = st->cfg[CFG_C].TI;
+  return (int)(((st->g.N[o1] + 1 + ti - 1) / ti) * (int64_t)(st->g.N[o2] + 1));
+}
+
+PassArgs base_args(astr_state* st, int id) {
+  const PassCfg& pc = st->cfg[id];
+  const int dir = CFG_DIR[id];
+  auto& o = get_ops(st, dir, pc.S, pc.WPL);
   PassArgs a{};
   a.g = st->g;
   a.th = st->th;
-  a.opd = st->opd[dir].op;
-  a.opf = st->opf[dir].op;
+  a.opd = o.first.op;
+  a.opf = o.second.op;
   a.dir = dir;
   a.dA = DIR_A; a.dB = DIR_B; a.dC = DIR_C;
-  a.TI = st->TI[pass][dir];
-  a.LP = st->LP[pass][dir];
+  a.TI = pc.TI;
+  a.LP = pc.LP;
   a.R = st->R;
   a.VF = st->VF;
   a.err = st->err;
@@ -162,14 +194,15 @@ struct PassTimer {
 };
 thread_local PassTimer* g_timer = nullptr;
 
-cudaError_t run_pass(astr_state* st, int pass, PassArgs& a) {
+cudaError_t run_pass(astr_state* st, int id, PassArgs& a) {
+  const int pass = CFG_PASS[id];
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   if (g_timer) {
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     cudaEventRecord(e0, st->ctx->stream);
   }
-  cudaError_t e = launch_pass(pass, a, st->lay[a.dir].S, st->lay[a.dir].WPL, st->ctx->stream);
+  cudaError_t e = launch_pass(pass, a, st->cfg[id].S, st->cfg[id].WPL, st->ctx->stream);
   if (g_timer) {
     cudaEventRecord(e1, st->ctx->stream);
     g_timer->ev.push_back(e0);
@@ -182,30 +215,30 @@ cudaError_t run_pass(astr_state* st, int pass, PassArgs& a) {
 // Filter along DIR_A still owed by the last stage.
 cudaError_t finalize_filter(astr_state* st) {
   if (!st->pending) return cudaSuccess;
-  PassArgs a = base_args(st, PASS_F, DIR_A);
+  PassArgs a = base_args(st, CFG_FA);
   a.q = st->Q0;
-  cudaError_t e = run_pass(st, PASS_F, a);
+  cudaError_t e = run_pass(st, CFG_FA, a);
   if (e == cudaSuccess) st->pending = false;
   return e;
 }
 
 // rhscal of the state in q into R (no filter, no update).
 cudaError_t run_rhs(astr_state* st, double* q) {
-  PassArgs a = base_args(st, PASS_A, DIR_A);
+  PassArgs a = base_args(st, CFG_A);
   a.q = q; a.D = st->DA; a.do_filter = 0;
-  cudaError_t e = run_pass(st, PASS_A, a);
+  cudaError_t e = run_pass(st, CFG_A, a);
   if (e != cudaSuccess) return e;
-  a = base_args(st, PASS_B, DIR_B);
+  a = base_args(st, CFG_B);
   a.q = q; a.D = st->DB;
-  if ((e = run_pass(st, PASS_B, a)) != cudaSuccess) return e;
-  a = base_args(st, PASS_C, DIR_C);
+  if ((e = run_pass(st, CFG_B, a)) != cudaSuccess) return e;
+  a = base_args(st, CFG_C);
   a.q = q; a.DA = st->DA; a.DB = st->DB;
-  if ((e = run_pass(st, PASS_C, a)) != cudaSuccess) return e;
-  a = base_args(st, PASS_VA, DIR_A);
-  if ((e = run_pass(st, PASS_VA, a)) != cudaSuccess) return e;
-  a = base_args(st, PASS_VB, DIR_B);
+  if ((e = run_pass(st, CFG_C, a)) != cudaSuccess) return e;
+  a = base_args(st, CFG_VA);
+  if ((e = run_pass(st, CFG_VA, a)) != cudaSuccess) return e;
+  a = base_args(st, CFG_VB);
   a.mode = 0;
-  return run_pass(st, PASS_VB, a);
+  return run_pass(st, CFG_VB, a);
 }
 
 // One SSP-RK3 step (tgvsolver.F90:1037-1074): 6 passes per stage, diagnostics at stage 1.
@@ -216,39 +249,39 @@ cudaError_t run_step(astr_state* st, double dt, bool pending_at_start) {
   for (int s = 0; s < 3; ++s) {
     double* qin = (s == 0) ? st->Q0 : st->Q1;
     double* qout = (s == 2) ? st->Q0 : st->Q1;
-    PassArgs a = base_args(st, PASS_A, DIR_A);
+    PassArgs a = base_args(st, CFG_A);
     a.q = qin; a.D = st->DA;
     a.do_filter = filt && (s > 0 || pending_at_start);
-    if ((e = run_pass(st, PASS_A, a)) != cudaSuccess) return e;
-    a = base_args(st, PASS_B, DIR_B);
+    if ((e = run_pass(st, CFG_A, a)) != cudaSuccess) return e;
+    a = base_args(st, CFG_B);
     a.q = qin; a.D = st->DB;
-    if ((e = run_pass(st, PASS_B, a)) != cudaSuccess) return e;
-    a = base_args(st, PASS_C, DIR_C);
+    if ((e = run_pass(st, CFG_B, a)) != cudaSuccess) return e;
+    a = base_args(st, CFG_C);
     a.q = qin; a.DA = st->DA; a.DB = st->DB;
     a.partials = (s == 0) ? st->partials : nullptr;
-    if ((e = run_pass(st, PASS_C, a)) != cudaSuccess) return e;
+    if ((e = run_pass(st, CFG_C, a)) != cudaSuccess) return e;
     if (s == 0) {
       const double norm = (double)st->p.im * (double)st->p.jm * (double)st->p.km;
       cudaEvent_t e0 = nullptr, e1 = nullptr;
       if (g_timer) { cudaEventCreate(&e0); cudaEventCreate(&e1); cudaEventRecord(e0, st->ctx->stream); }
-      if ((e = launch_diag_reduce(st->partials, st->nparts, st->hist, st->counter, norm, st->ctx->stream)) != cudaSuccess)
+      if ((e = launch_diag_reduce(st->partials, diag_parts(st), st->hist, st->counter, norm, st->ctx->stream)) != cudaSuccess)
         return e;
       if (g_timer) {
         cudaEventRecord(e1, st->ctx->stream);
         g_timer->ev.push_back(e0); g_timer->ev.push_back(e1); g_timer->kind.push_back(6);
       }
     }
-    a = base_args(st, PASS_VA, DIR_A);
-    if ((e = run_pass(st, PASS_VA, a)) != cudaSuccess) return e;
-    a = base_args(st, PASS_VB, DIR_B);
+    a = base_args(st, CFG_VA);
+    if ((e = run_pass(st, CFG_VA, a)) != cudaSuccess) return e;
+    a = base_args(st, CFG_VB);
     a.q = qin; a.qsave = st->Q0; a.qout = qout;
     a.mode = 1; a.do_filter = filt;
     a.c1 = rk[s][0]; a.c2 = rk[s][1]; a.c3 = rk[s][2]; a.dt = dt;
-    if ((e = run_pass(st, PASS_VB, a)) != cudaSuccess) return e;
+    if ((e = run_pass(st, CFG_VB, a)) != cudaSuccess) return e;
     if (filt) {
-      a = base_args(st, PASS_F, DIR_C);
+      a = base_args(st, CFG_FC);
       a.q = qout;
-      if ((e = run_pass(st, PASS_F, a)) != cudaSuccess) return e;
+      if ((e = run_pass(st, CFG_FC, a)) != cudaSuccess) return e;
     }
   }
   return cudaSuccess;
@@ -286,6 +319,63 @@ int copy_fields(astr_state* st, double* dev, double* user, const int64_t* shape,
     CK(cudaMemcpy3DAsync(&prm, ctx->stream));
   }
   return ASTR_OK;
+}
+
+// Per-pass autotuner: every compiled solve layout that covers the longest system of the pass
+// direction with at least half of its rows used, and two or three tile widths each, timed on
+// scratch copies of the live state (the solution is not touched). Picks the fastest.
+cudaError_t autotune(astr_state* st) {
+  cudaStream_t sm = st->ctx->stream;
+  cudaError_t e = cudaMemcpyAsync(st->Q1, st->Q0, 5 * (size_t)st->g.fs * sizeof(double), cudaMemcpyDeviceToDevice, sm);
+  if (e != cudaSuccess) return e;
+  cudaEvent_t t0, t1;
+  cudaEventCreate(&t0);
+  cudaEventCreate(&t1);
+  for (int id = 0; id < NCFG; ++id) {
+    const int dir = CFG_DIR[id], pass = CFG_PASS[id];
+    const int nsys = st->hf[dir].nsys();
+    const int dim = st->g.N[dir];
+    float best = 1e30f;
+    PassCfg bestc = st->cfg[id];
+    for (const Layout& L : kLayouts) {
+      const int rows = 32 * L.WPL * L.S;
+      if (rows < nsys || 2 * nsys < rows) continue;
+      const int tis[3] = {pick_ti(pass, dim, L.WPL), pick_ti(pass, dim, L.WPL) / 2, pick_ti(pass, dim, L.WPL, 220 * 1024)};
+      for (int ti : tis) {
+        if (ti < 1) continue;
+        PassCfg c;
+        c.S = L.S; c.WPL = L.WPL; c.TI = ti; c.LP = tile_pitch(dim, ti);
+        const PassCfg saved = st->cfg[id];
+        st->cfg[id] = c;
+        PassArgs a = base_args(st, id);
+        a.q = st->Q1; a.D = st->DA; a.DA = st->DA; a.DB = st->DB;
+        a.qsave = st->Q1; a.qout = st->Q1; a.mode = 1; a.do_filter = st->p.filter_on;
+        a.c1 = 1.0; a.c2 = 0.0; a.c3 = 0.0; a.dt = 0.0;
+        float ms = 1e30f;
+        if ((e = launch_pass(pass, a, c.S, c.WPL, sm)) == cudaSuccess) {
+          cudaEventRecord(t0, sm);
+          for (int r = 0; r < 2 && e == cudaSuccess; ++r) e = launch_pass(pass, a, c.S, c.WPL, sm);
+          cudaEventRecord(t1, sm);
+          cudaEventSynchronize(t1);
+          cudaEventElapsedTime(&ms, t0, t1);
+        }
+        if (e != cudaSuccess) {   // a shape the device cannot launch (e.g. too much shared memory)
+          cudaGetLastError();
+          e = cudaSuccess;
+          ms = 1e30f;
+        }
+        st->cfg[id] = saved;
+        if (ms < best) { best = ms; bestc = c; }
+      }
+    }
+    st->cfg[id] = bestc;
+  }
+  cudaEventDestroy(t0);
+  cudaEventDestroy(t1);
+  e = cudaMemsetAsync(st->err, 0, sizeof(int), sm);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(sm);
+  st->tuned = true;
+  return e;
 }
 
 void drop_graphs(astr_state* st) {
@@ -345,7 +435,7 @@ int astr_fd_scheme_create(astr_ctx* ctx, const char scheme[4], int ntype, int di
     return fail(ctx, ASTR_ERR_ARG, "scheme not defined (only 643c and 643e) or bad ntype/dim");
   }
   Layout lay = pick_layout(s->h.nsys());
-  if (lay.S == 0) { delete s; return fail(ctx, ASTR_ERR_UNSUPPORTED, "line longer than 1280 rows"); }
+  if (lay.S == 0) { delete s; return fail(ctx, ASTR_ERR_UNSUPPORTED, "line longer than 1152 rows"); }
   cudaError_t e = make_devop(s->h, lay, s->d);
   if (e != cudaSuccess) { free_devop(s->d); delete s; return cuda_fail(ctx, e, "scheme tables"); }
   *out = s;
@@ -360,7 +450,7 @@ int astr_filter_create(astr_ctx* ctx, int ntype, int dim, double alpha_f, double
   s->ctx = ctx;
   build_filter_op(s->h, ntype, dim, alpha_f, beta_halo, beta_bound, boundary_no_filter != 0);
   Layout lay = pick_layout(s->h.nsys());
-  if (lay.S == 0) { delete s; return fail(ctx, ASTR_ERR_UNSUPPORTED, "line longer than 1280 rows"); }
+  if (lay.S == 0) { delete s; return fail(ctx, ASTR_ERR_UNSUPPORTED, "line longer than 1152 rows"); }
   cudaError_t e = make_devop(s->h, lay, s->d);
   if (e != cudaSuccess) { free_devop(s->d); delete s; return cuda_fail(ctx, e, "scheme tables"); }
   *out = s;
@@ -426,21 +516,22 @@ int astr_state_create(astr_ctx* ctx, const astr_params* p, astr_state** out) {
   st->th.tc = p->sutherland / p->ref_tem;
   st->th.tc1 = 1.0 + st->th.tc;
   st->th.mach = m;
-  // operators and launch shapes per direction
+  // operators per direction and default launch shapes
   for (int d = 0; d < 3; ++d) {
-    HostOp hd, hf;
-    build_fd_op(hd, "643c", 3, N[d]);
-    build_filter_op(hf, 3, N[d], p->alfa_filter, p->beta_halo, p->beta_bound, false);
-    st->lay[d] = pick_layout(hf.nsys());
-    if (st->lay[d].S == 0) { delete st; return fail(ctx, ASTR_ERR_UNSUPPORTED, "dimension too large (max 1273)"); }
-    cudaError_t e1 = make_devop(hd, st->lay[d], st->opd[d]);
-    cudaError_t e2 = make_devop(hf, st->lay[d], st->opf[d]);
-    if (e1 != cudaSuccess || e2 != cudaSuccess) { delete st; return fail(ctx, ASTR_ERR_NOMEM, "scheme tables"); }
-    for (int pass = 1; pass <= 6; ++pass) {
-      st->TI[pass][d] = pick_ti(pass, N[d], st->lay[d].WPL);
-      st->LP[pass][d] = tile_pitch(N[d], st->TI[pass][d]);
-    }
+    build_fd_op(st->hd[d], "643c", 3, N[d]);
+    build_filter_op(st->hf[d], 3, N[d], p->alfa_filter, p->beta_halo, p->beta_bound, false);
+    if (pick_layout(st->hf[d].nsys()).S == 0) { delete st; return fail(ctx, ASTR_ERR_UNSUPPORTED, "dimension too large (max 1145)"); }
   }
+  for (int id = 0; id < NCFG; ++id) {
+    const int d = CFG_DIR[id];
+    const Layout L = pick_layout(st->hf[d].nsys());
+    PassCfg& c = st->cfg[id];
+    c.S = L.S; c.WPL = L.WPL;
+    c.TI = pick_ti(CFG_PASS[id], N[d], L.WPL);
+    c.LP = tile_pitch(N[d], c.TI);
+  }
+  // a small box gains nothing from tuning
+  st->autotune = (N[0] + 1) * (int64_t)(N[1] + 1) * (N[2] + 1) >= 100 * 100 * 100;
   // 30 fields: Q0(5) Q1(5) R(5) DA(4) DB(4) VF(7)
   const size_t nf = 30;
   cudaError_t e = cudaMalloc(&st->buf, nf * (size_t)st->g.fs * sizeof(double));
@@ -453,9 +544,8 @@ int astr_state_create(astr_ctx* ctx, const astr_params* p, astr_state** out) {
   st->DB = st->DA + 4 * st->g.fs;
   st->VF = st->DB + 4 * st->g.fs;
   // partial sums of pass C: one per CTA
-  const int ti = st->TI[PASS_C][DIR_C];
   const int o1 = (DIR_C == 0) ? 1 : 0, o2 = (DIR_C == 2) ? 1 : 2;
-  st->nparts = (int)(((N[o1] + 1 + ti - 1) / ti) * (int64_t)(N[o2] + 1));
+  st->nparts = (int)((N[o1] + 1) * (int64_t)(N[o2] + 1));   // one per CTA; at least one line per CTA
   if (cudaMalloc(&st->partials, (size_t)st->nparts * 3 * sizeof(double)) != cudaSuccess ||
       cudaMalloc(&st->hist, (size_t)st->hist_cap * 3 * sizeof(double)) != cudaSuccess ||
       cudaMalloc(&st->counter, 2 * sizeof(int)) != cudaSuccess) {
@@ -471,7 +561,7 @@ int astr_state_create(astr_ctx* ctx, const astr_params* p, astr_state** out) {
 int astr_state_destroy(astr_state* st) {
   if (!st) return ASTR_ERR_ARG;
   drop_graphs(st);
-  for (int d = 0; d < 3; ++d) { free_devop(st->opd[d]); free_devop(st->opf[d]); }
+  for (auto& kv : st->ops) { free_devop(kv.second.first); free_devop(kv.second.second); }
   if (st->buf) cudaFree(st->buf);
   if (st->partials) cudaFree(st->partials);
   if (st->hist) cudaFree(st->hist);
@@ -562,6 +652,23 @@ int astr_rhs(astr_state* st, double* qrhs, const int64_t shape[3], const int64_t
   return check_err(st);
 }
 
+int astr_state_autotune(astr_state* st, int on) {
+  if (!st) return ASTR_ERR_ARG;
+  st->autotune = on != 0;
+  return ASTR_OK;
+}
+
+int astr_state_launch_shapes(astr_state* st, int shapes[28]) {
+  if (!st || !shapes) return ASTR_ERR_ARG;
+  for (int id = 0; id < NCFG; ++id) {
+    shapes[4 * id] = st->cfg[id].S;
+    shapes[4 * id + 1] = st->cfg[id].WPL;
+    shapes[4 * id + 2] = st->cfg[id].TI;
+    shapes[4 * id + 3] = st->cfg[id].LP;
+  }
+  return ASTR_OK;
+}
+
 int astr_state_use_graph(astr_state* st, int on) {
   if (!st) return ASTR_ERR_ARG;
   st->use_graph = on != 0;
@@ -572,6 +679,10 @@ int astr_rk3_step(astr_state* st, double dt, int nsteps) {
   if (!st || nsteps < 0 || !(dt > 0.0)) return ASTR_ERR_ARG;
   astr_ctx* ctx = st->ctx;
   if (st->nstep + nsteps > st->hist_cap) return fail(ctx, ASTR_ERR_UNSUPPORTED, "history buffer full (65536 steps)");
+  if (st->autotune && !st->tuned && nsteps > 0) {
+    drop_graphs(st);
+    CK(autotune(st));
+  }
   for (int s = 0; s < nsteps; ++s) {
     const int variant = st->pending ? 1 : 0;
     st->row_key.push_back((double)st->nstep);
@@ -675,22 +786,22 @@ int astr_diagnostics(astr_state* st, double out[3]) {
   astr_ctx* ctx = st->ctx;
   CK(finalize_filter(st));
   // one gradient evaluation of the current state, reduced like stacal
-  PassArgs a = base_args(st, PASS_A, DIR_A);
+  PassArgs a = base_args(st, CFG_A);
   a.q = st->Q0; a.D = st->DA; a.do_filter = 0;
-  CK(run_pass(st, PASS_A, a));
-  a = base_args(st, PASS_B, DIR_B);
+  CK(run_pass(st, CFG_A, a));
+  a = base_args(st, CFG_B);
   a.q = st->Q0; a.D = st->DB;
-  CK(run_pass(st, PASS_B, a));
-  a = base_args(st, PASS_C, DIR_C);
+  CK(run_pass(st, CFG_B, a));
+  a = base_args(st, CFG_C);
   a.q = st->Q0; a.DA = st->DA; a.DB = st->DB; a.partials = st->partials;
-  CK(run_pass(st, PASS_C, a));
+  CK(run_pass(st, CFG_C, a));
   int* cnt = nullptr;
   double* h = nullptr;
   CK(cudaMalloc(&cnt, sizeof(int)));
   CK(cudaMalloc(&h, 3 * sizeof(double)));
   CK(cudaMemsetAsync(cnt, 0, sizeof(int), ctx->stream));
   const double norm = (double)st->p.im * (double)st->p.jm * (double)st->p.km;
-  CK(launch_diag_reduce(st->partials, st->nparts, h, cnt, norm, ctx->stream));
+  CK(launch_diag_reduce(st->partials, diag_parts(st), h, cnt, norm, ctx->stream));
   CK(cudaMemcpyAsync(out, h, 3 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
   cudaFree(cnt);

@@ -17,7 +17,7 @@ __global__ void __launch_bounds__(1024) k_line_api(LineOp op, int dir, const dou
                                                    double scale) {
   extern __shared__ double sm[];
   double* tile = sm;
-  double* scan = sm + (size_t)TI * LP;
+  double* scan = sm + (size_t)TI * LP;   // 2*WPL per line
   const int o1 = (dir == 0) ? 1 : 0;
   const int o2 = (dir == 2) ? 1 : 2;
   const int64_t l1_0 = oa.lb[o1] + (int64_t)blockIdx.x * TI;
@@ -52,10 +52,10 @@ __global__ void __launch_bounds__(1024) k_line_api(LineOp op, int dir, const dou
   double v[S];
   if (op.kind == OP_DERIV) {
     rhs_deriv<S>(v, op, seg, get);
-    seg_solve<S, WPL>(v, op, seg, lane, part, scan + l * 4 * WPL);
+    seg_solve<S, WPL>(v, op.tab, seg, lane, part, l, scan + l * 2 * WPL);
   } else if (op.kind == OP_FILTER) {
     rhs_filter<S>(v, op, seg, get);
-    seg_solve<S, WPL>(v, op, seg, lane, part, scan + l * 4 * WPL);
+    seg_solve<S, WPL>(v, op.tab, seg, lane, part, l, scan + l * 2 * WPL);
   } else {
 #pragma unroll
     for (int t = 0; t < S; ++t) {
@@ -81,8 +81,7 @@ __global__ void __launch_bounds__(1024) k_line_api(LineOp op, int dir, const dou
     else { n = idx / TI; l2 = idx - n * TI; }
     const int64_t i1 = l1_0 + l2;
     if (i1 >= l1_end) continue;
-    double val = tile[l2 * LP + HT + n];
-    if (op.kind == OP_FILTER && ((n == 0 && op.left_phys) || (n == dim && op.right_phys))) val = tile[l2 * LP + HT + n];
+    const double val = tile[l2 * LP + HT + n];
     ob[obase2 + (i1 - oa.lb[o1]) * oa.s[o1] + (n - oa.lb[dir]) * oa.s[dir]] = val;
   }
 }
@@ -91,11 +90,11 @@ template <int S, int WPL>
 static cudaError_t launch_t(const DevOp& op, int dir, const double* f, const ArrDesc& fa, double* out,
                             const ArrDesc& oa, int nfields, double scale, cudaStream_t st) {
   const int o1 = (dir == 0) ? 1 : 0, o2 = (dir == 2) ? 1 : 2;
-  int TI = 32 / WPL;
+  int TI = 512 / (32 * WPL);   // <= 15 lines when WPL > 1 (one named barrier per line)
   if (TI > 16) TI = 16;
   if (TI < 1) TI = 1;
   const int LP = tile_pitch(op.op.dim, TI);
-  const size_t smem = ((size_t)TI * LP + (size_t)TI * 4 * WPL) * sizeof(double);
+  const size_t smem = ((size_t)TI * LP + (size_t)TI * 2 * WPL) * sizeof(double);
   auto kern = k_line_api<S, WPL>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
@@ -110,7 +109,9 @@ cudaError_t launch_line_api(const DevOp& op, int dir, const double* f, const Arr
   if (op.S == 5 && op.WPL == 1) return launch_t<5, 1>(op, dir, f, fa, out, oa, nfields, scale, st);
   if (op.S == 5 && op.WPL == 2) return launch_t<5, 2>(op, dir, f, fa, out, oa, nfields, scale, st);
   if (op.S == 5 && op.WPL == 4) return launch_t<5, 4>(op, dir, f, fa, out, oa, nfields, scale, st);
-  if (op.S == 5 && op.WPL == 8) return launch_t<5, 8>(op, dir, f, fa, out, oa, nfields, scale, st);
+  if (op.S == 9 && op.WPL == 1) return launch_t<9, 1>(op, dir, f, fa, out, oa, nfields, scale, st);
+  if (op.S == 9 && op.WPL == 2) return launch_t<9, 2>(op, dir, f, fa, out, oa, nfields, scale, st);
+  if (op.S == 9 && op.WPL == 4) return launch_t<9, 4>(op, dir, f, fa, out, oa, nfields, scale, st);
   return cudaErrorInvalidValue;
 }
 

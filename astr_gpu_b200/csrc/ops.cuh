@@ -22,9 +22,14 @@ constexpr unsigned FULL = 0xffffffffu;
 enum OpKind { OP_DERIV = 0, OP_FILTER = 1, OP_EXPLICIT = 2 };
 
 // One line operator (a compact_scheme of the reference plus the lane tables of its solve).
+// Table layout (doubles), nseg = 32*WPL segments of S rows:
+//   [(f*S + t)*nseg + seg]  f = 0 ac1, 1 ac2, 2 ac3, 3 pf (forward prefix product within the
+//                           segment), 4 qb (backward suffix product within the segment)
+//   then per segment (nseg each): FS[0..4] forward scan composites for shuffle offsets 1..16,
+//   FE forward exclusive product within the warp, BS[0..4], BE (backward), and per warp
+//   MW[WPL], MWB[WPL] (whole-warp products).
 struct LineOp {
-  const double* tab;   // lane-major: tab[(f*S + t)*nseg + seg], f = ac1, ac2, ac3, pf, qb;
-                       // then mf[nseg], mb[nseg]
+  const double* tab;
   int nsys;            // rows of the system (last_node - first_node + 1)
   int ext_lo;          // -first_node: node = r - ext_lo
   int dim;
@@ -36,68 +41,74 @@ struct LineOp {
   double c10[6], ch[3][11], cb[3][7], c6[4], c8[5];  // filter coefficients (filter.F90:299-432)
 };
 
-__device__ __forceinline__ double tabv(const LineOp& op, int f, int t, int seg) {
-  return __ldg(op.tab + (size_t)(f * op.S + t) * op.nseg + seg);
+enum TabOff { T_FS = 0, T_FE = 5, T_BS = 6, T_BE = 11, T_NSEGTAB = 12 };
+
+// Barrier among the WPL warps of one line (named barrier 1 + line).
+template <int WPL>
+__device__ __forceinline__ void line_sync(int line) {
+  if (WPL > 1) asm volatile("bar.sync %0, %1;" ::"r"(1 + line), "r"(32 * WPL) : "memory");
 }
 
 // Segmented Thomas solve. v holds the RHS rows of this lane on entry and the solution on exit.
-// scan_sm: 4*WPL doubles private to this line (used only when WPL > 1). All threads of the
-// block must call this together when WPL > 1 (it contains __syncthreads).
+// tab is the operator's lane table laid out for this (S, WPL); all offsets are compile-time.
+// scan_sm: 2*WPL doubles private to this line (used only when WPL > 1). All warps of the line
+// must call it together.
 template <int S, int WPL>
-__device__ __forceinline__ void seg_solve(double (&v)[S], const LineOp& op, int seg, int lane, int part,
-                                          double* scan_sm) {
+__device__ __forceinline__ void seg_solve(double (&v)[S], const double* __restrict__ tab, int seg, int lane, int part,
+                                          int line, double* scan_sm) {
+  constexpr int NS = 32 * WPL;
+  const double* tb = tab + seg;
+  const double* ws = tab + (5 * S + T_NSEGTAB) * NS;   // per-warp products
   // forward sweep from a zero carry
   double g = 0.0;
 #pragma unroll
   for (int t = 0; t < S; ++t) {
-    g = v[t] * tabv(op, 1, t, seg) - g * tabv(op, 2, t, seg);
+    g = v[t] * __ldg(tb + (S + t) * NS) - g * __ldg(tb + (2 * S + t) * NS);
     v[t] = g;
   }
-  const double* mfp = op.tab + (size_t)5 * S * op.nseg;
-  double M = __ldg(mfp + seg), G = g;
+  // inclusive scan of the segment maps c -> G + M c across the warp (composite M precomputed)
+  double G = g;
 #pragma unroll
-  for (int off = 1; off < 32; off <<= 1) {
-    double Mo = __shfl_up_sync(FULL, M, off), Go = __shfl_up_sync(FULL, G, off);
-    if (lane >= off) { G = fma(M, Go, G); M = M * Mo; }
+  for (int k = 0; k < 5; ++k) {
+    const double Go = __shfl_up_sync(FULL, G, 1 << k);
+    G = fma(__ldg(tb + (5 * S + T_FS + k) * NS), Go, G);
   }
-  double Me = __shfl_up_sync(FULL, M, 1), Ge = __shfl_up_sync(FULL, G, 1);
-  if (lane == 0) { Me = 1.0; Ge = 0.0; }
+  double Ge = __shfl_up_sync(FULL, G, 1);
+  if (lane == 0) Ge = 0.0;
   double cw = 0.0;
   if (WPL > 1) {
-    if (lane == 31) { scan_sm[2 * part] = M; scan_sm[2 * part + 1] = G; }
-    __syncthreads();
-    for (int p = 0; p < part; ++p) cw = fma(scan_sm[2 * p], cw, scan_sm[2 * p + 1]);
+    if (lane == 31) scan_sm[part] = G;
+    line_sync<WPL>(line);
+    for (int p = 0; p < part; ++p) cw = fma(__ldg(ws + p), cw, scan_sm[p]);
   }
-  double cin = fma(Me, cw, Ge);
+  const double cin = fma(__ldg(tb + (5 * S + T_FE) * NS), cw, Ge);
 #pragma unroll
-  for (int t = 0; t < S; ++t) v[t] = fma(tabv(op, 3, t, seg), cin, v[t]);
+  for (int t = 0; t < S; ++t) v[t] = fma(__ldg(tb + (3 * S + t) * NS), cin, v[t]);
 
   // backward sweep from a zero carry
   double h = 0.0;
 #pragma unroll
   for (int t = S - 1; t >= 0; --t) {
-    h = v[t] - tabv(op, 0, t, seg) * h;
+    h = v[t] - __ldg(tb + t * NS) * h;
     v[t] = h;
   }
-  M = __ldg(mfp + op.nseg + seg);
   G = h;
 #pragma unroll
-  for (int off = 1; off < 32; off <<= 1) {
-    double Mo = __shfl_down_sync(FULL, M, off), Go = __shfl_down_sync(FULL, G, off);
-    if (lane + off < 32) { G = fma(M, Go, G); M = M * Mo; }
+  for (int k = 0; k < 5; ++k) {
+    const double Go = __shfl_down_sync(FULL, G, 1 << k);
+    G = fma(__ldg(tb + (5 * S + T_BS + k) * NS), Go, G);
   }
-  Me = __shfl_down_sync(FULL, M, 1);
   Ge = __shfl_down_sync(FULL, G, 1);
-  if (lane == 31) { Me = 1.0; Ge = 0.0; }
+  if (lane == 31) Ge = 0.0;
   cw = 0.0;
   if (WPL > 1) {
-    if (lane == 0) { scan_sm[2 * WPL + 2 * part] = M; scan_sm[2 * WPL + 2 * part + 1] = G; }
-    __syncthreads();
-    for (int p = WPL - 1; p > part; --p) cw = fma(scan_sm[2 * WPL + 2 * p], cw, scan_sm[2 * WPL + 2 * p + 1]);
+    if (lane == 0) scan_sm[WPL + part] = G;
+    line_sync<WPL>(line);
+    for (int p = WPL - 1; p > part; --p) cw = fma(__ldg(ws + WPL + p), cw, scan_sm[WPL + p]);
   }
-  cin = fma(Me, cw, Ge);
+  const double cb = fma(__ldg(tb + (5 * S + T_BE) * NS), cw, Ge);
 #pragma unroll
-  for (int t = 0; t < S; ++t) v[t] = fma(tabv(op, 4, t, seg), cin, v[t]);
+  for (int t = 0; t < S; ++t) v[t] = fma(__ldg(tb + (4 * S + t) * NS), cb, v[t]);
 }
 
 // ---------------------------------------------------------------- right-hand sides
@@ -122,30 +133,51 @@ __device__ __forceinline__ bool deriv_special(const LineOp& op, int r, Get f, do
   return false;
 }
 
-// Interior compact RHS 7/9(f+1 - f-1) + 1/36(f+2 - f-2) (derivative.F90:296-304) over a
-// sliding window, then the closure rows. f(node) must accept nodes in [-HT, dim+HT].
+// Interior compact RHS 7/9(f+1 - f-1) + 1/36(f+2 - f-2) (derivative.F90:296-304) on a window
+// w[t] = f(n0 - 2 + t), n0 = node of the lane's first row.
+template <int S>
+__device__ __forceinline__ void stencil_deriv(double (&v)[S], const double (&w)[S + 4]) {
+#pragma unroll
+  for (int t = 0; t < S; ++t) v[t] = (7.0 / 9.0) * (w[t + 3] - w[t + 1]) + (1.0 / 36.0) * (w[t + 4] - w[t]);
+}
+// Closure rows of the compact derivative and zero padding rows; only lanes that hold them call
+// this (deriv_edge_lane).
+template <int S, class Get>
+__device__ __forceinline__ void fix_deriv_rows(double (&v)[S], const LineOp& op, int r0, Get f) {
+#pragma unroll
+  for (int t = 0; t < S; ++t) {
+    const int r = r0 + t;
+    double s;
+    if (r >= op.nsys) v[t] = 0.0;
+    else if (deriv_special(op, r, f, s)) v[t] = s;
+  }
+}
+template <int S>
+__device__ __forceinline__ bool deriv_edge_lane(const LineOp& op, int r0) { return r0 < 2 || r0 + S > op.nsys - 2; }
+
+// Fill w[t] = f(n0 + t), t < W, clamping to the staged range only for lanes near the ends.
+template <int W, class Get>
+__device__ __forceinline__ void fill_window(double (&w)[W], int n0, int dim, Get f) {
+  if (n0 >= -HT && n0 + W - 1 <= dim + HT) {
+#pragma unroll
+    for (int t = 0; t < W; ++t) w[t] = f(n0 + t);
+  } else {
+#pragma unroll
+    for (int t = 0; t < W; ++t) {
+      int n = n0 + t;
+      n = n < -HT ? -HT : (n > dim + HT ? dim + HT : n);
+      w[t] = f(n);
+    }
+  }
+}
+
 template <int S, class Get>
 __device__ __forceinline__ void rhs_deriv(double (&v)[S], const LineOp& op, int seg, Get f) {
   const int r0 = seg * S;
-  const int n0 = r0 - op.ext_lo;
   double w[S + 4];
-#pragma unroll
-  for (int t = 0; t < S + 4; ++t) {
-    int n = n0 - 2 + t;
-    n = n < -HT ? -HT : (n > op.dim + HT ? op.dim + HT : n);
-    w[t] = f(n);
-  }
-#pragma unroll
-  for (int t = 0; t < S; ++t) v[t] = (7.0 / 9.0) * (w[t + 3] - w[t + 1]) + (1.0 / 36.0) * (w[t + 4] - w[t]);
-  if (r0 < 2 || r0 + S > op.nsys - 2) {
-#pragma unroll
-    for (int t = 0; t < S; ++t) {
-      const int r = r0 + t;
-      double s;
-      if (r >= op.nsys) v[t] = 0.0;
-      else if (deriv_special(op, r, f, s)) v[t] = s;
-    }
-  }
+  fill_window<S + 4>(w, r0 - op.ext_lo - 2, op.dim, f);
+  stencil_deriv<S>(v, w);
+  if (deriv_edge_lane<S>(op, r0)) fix_deriv_rows<S>(v, op, r0, f);
 }
 
 // Explicit 6th-order derivative with its closures (diff6ec, derivative.F90:350-413); rows are
@@ -223,14 +255,8 @@ __device__ __forceinline__ bool filter_special(const LineOp& op, int r, Get f, d
 template <int S, class Get>
 __device__ __forceinline__ void rhs_filter(double (&v)[S], const LineOp& op, int seg, Get f) {
   const int r0 = seg * S;
-  const int n0 = r0 - op.ext_lo;
   double w[S + 10];
-#pragma unroll
-  for (int t = 0; t < S + 10; ++t) {
-    int n = n0 - 5 + t;
-    n = n < -HT ? -HT : (n > op.dim + HT ? op.dim + HT : n);
-    w[t] = f(n);
-  }
+  fill_window<S + 10>(w, r0 - op.ext_lo - 5, op.dim, f);
 #pragma unroll
   for (int t = 0; t < S; ++t) {
     double var0 = w[t + 5] + w[t + 5];

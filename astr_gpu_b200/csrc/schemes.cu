@@ -129,8 +129,12 @@ void build_filter_op(HostOp& op, int ntype, int dim, double alfa, double bh, dou
 
 std::vector<double> lane_tables(const HostOp& op, int S, int nseg) {
   const int nsys = op.nsys();
-  std::vector<double> t((size_t)5 * S * nseg + 2 * (size_t)nseg, 0.0);
+  const int WPL = nseg / 32;
+  const size_t base = (size_t)5 * S * nseg;
+  std::vector<double> t(base + (size_t)T_NSEGTAB * nseg + 2 * (size_t)WPL, 0.0);
   auto at = [&](int f, int tt, int seg) -> double& { return t[(size_t)(f * S + tt) * nseg + seg]; };
+  auto sg = [&](int k, int seg) -> double& { return t[base + (size_t)k * nseg + seg]; };
+  std::vector<double> mf(nseg), mb(nseg);
   for (int seg = 0; seg < nseg; ++seg) {
     double e1[64], e2[64], e3[64];
     for (int tt = 0; tt < S; ++tt) {
@@ -148,10 +152,33 @@ std::vector<double> lane_tables(const HostOp& op, int S, int nseg) {
     }
     double p = 1.0;
     for (int tt = 0; tt < S; ++tt) { p *= -e3[tt]; at(3, tt, seg) = p; }
-    t[(size_t)5 * S * nseg + seg] = p;
+    mf[seg] = p;
     double q = 1.0;
     for (int tt = S - 1; tt >= 0; --tt) { q *= -e1[tt]; at(4, tt, seg) = q; }
-    t[(size_t)5 * S * nseg + nseg + seg] = q;
+    mb[seg] = q;
+  }
+  // scan composites within each warp (see seg_solve)
+  for (int w = 0; w < WPL; ++w) {
+    const int s0 = 32 * w;
+    for (int l = 0; l < 32; ++l) {
+      for (int k = 0; k < 5; ++k) {
+        const int off = 1 << k;
+        double pf = 0.0, pb = 0.0;
+        if (l >= off) { pf = 1.0; for (int j = l - off + 1; j <= l; ++j) pf *= mf[s0 + j]; }
+        if (l + off <= 31) { pb = 1.0; for (int j = l; j <= l + off - 1; ++j) pb *= mb[s0 + j]; }
+        sg(T_FS + k, s0 + l) = pf;
+        sg(T_BS + k, s0 + l) = pb;
+      }
+      double fe = 1.0, be = 1.0;
+      for (int j = 0; j < l; ++j) fe *= mf[s0 + j];
+      for (int j = l + 1; j < 32; ++j) be *= mb[s0 + j];
+      sg(T_FE, s0 + l) = fe;
+      sg(T_BE, s0 + l) = be;
+    }
+    double mw = 1.0, mwb = 1.0;
+    for (int j = 0; j < 32; ++j) { mw *= mf[s0 + j]; mwb *= mb[s0 + j]; }
+    t[base + (size_t)T_NSEGTAB * nseg + w] = mw;
+    t[base + (size_t)T_NSEGTAB * nseg + WPL + w] = mwb;
   }
   return t;
 }
@@ -159,9 +186,9 @@ std::vector<double> lane_tables(const HostOp& op, int S, int nseg) {
 Layout pick_layout(int nsys_max) {
   if (nsys_max <= 96) return {3, 1};
   if (nsys_max <= 160) return {5, 1};
-  if (nsys_max <= 320) return {5, 2};
-  if (nsys_max <= 640) return {5, 4};
-  if (nsys_max <= 1280) return {5, 8};
+  if (nsys_max <= 288) return {9, 1};
+  if (nsys_max <= 576) return {9, 2};
+  if (nsys_max <= 1152) return {9, 4};
   return {0, 0};
 }
 

@@ -23,485 +23,6 @@ namespace astr {
 
 namespace {
 
-struct TileCtx {
-  int dir, o1, o2, dim, TI, LP;
-  int64_t i1_0, i2, n1;
-  int64_t sd, so1, so2;
-};
-
-__device__ __forceinline__ TileCtx tile_ctx(const PassArgs& a) {
-  TileCtx c;
-  c.dir = a.dir;
-  c.o1 = (a.dir == 0) ? 1 : 0;
-  c.o2 = (a.dir == 2) ? 1 : 2;
-  c.dim = a.g.N[a.dir];
-  c.TI = a.TI;
-  c.LP = a.LP;
-  c.i1_0 = (int64_t)blockIdx.x * a.TI;
-  c.i2 = blockIdx.y;
-  c.n1 = a.g.N[c.o1] + 1;
-  c.sd = a.g.st[a.dir];
-  c.so1 = a.g.st[c.o1];
-  c.so2 = a.g.st[c.o2];
-  return c;
-}
-
-// Tile slot of a flat index: node-fastest for x lines (contiguous), line-fastest otherwise
-// (TI adjacent lines are contiguous in x).
-__device__ __forceinline__ void slot(const TileCtx& c, int idx, int npl, int& l, int& n) {
-  if (c.dir == 0) { l = idx / npl; n = idx - l * npl; }
-  else { n = idx / c.TI; l = idx - n * c.TI; }
-}
-
-__device__ __forceinline__ void load_tile(const TileCtx& c, double* tile, const double* __restrict__ fld) {
-  const int LPn = c.dim + 1 + 2 * HT;
-  const double* b2 = fld + c.i2 * c.so2;
-  for (int idx = threadIdx.x; idx < c.TI * LPn; idx += blockDim.x) {
-    int l, nn;
-    slot(c, idx, LPn, l, nn);
-    const int64_t i1 = c.i1_0 + l;
-    double v = 0.0;
-    if (i1 < c.n1) v = __ldg(b2 + i1 * c.so1 + (int64_t)wrap_node(nn - HT, c.dim) * c.sd);
-    tile[l * c.LP + nn] = v;
-  }
-}
-
-template <class Epi>
-__device__ __forceinline__ void store_tile(const TileCtx& c, Epi epi) {
-  const int npl = c.dim + 1;
-  const int64_t b2 = c.i2 * c.so2;
-  for (int idx = threadIdx.x; idx < c.TI * npl; idx += blockDim.x) {
-    int l, n;
-    slot(c, idx, npl, l, n);
-    const int64_t i1 = c.i1_0 + l;
-    if (i1 >= c.n1) continue;
-    epi(b2 + i1 * c.so1 + (int64_t)n * c.sd, l, n);
-  }
-}
-
-// Write a lane's solution rows (nodes 0..dim) into a tile line, optionally with the periodic
-// halo images of those nodes.
-template <int S>
-__device__ __forceinline__ void put_lane(double* line, const double (&v)[S], int seg, int ext, int dim, bool images) {
-#pragma unroll
-  for (int t = 0; t < S; ++t) {
-    const int n = seg * S + t - ext;
-    if (n < 0 || n > dim) continue;
-    line[n] = v[t];
-    if (images) {
-      if (n >= 1 && n <= HT) line[dim + n] = v[t];
-      if (n >= dim - HT && n <= dim - 1) line[n - dim] = v[t];
-    }
-  }
-}
-
-__device__ __forceinline__ void put_images(double* line, int n, int dim, double v) {
-  if (n >= 1 && n <= HT) line[dim + n] = v;
-  if (n >= dim - HT && n <= dim - 1) line[n - dim] = v;
-}
-
-// Pointwise function k of the conserved variables at node n of a line:
-// 0..2 velocity u,v,w; 3 temperature (q2fvar, tgvsolver.F90:92-121); 4..8 Euler flux
-// components along `dir` (convection, tgvsolver.F90:559-564).
-__device__ __forceinline__ double gfun(int k, int dir, const double* L, int tsz, int n, int dim, const Thermo& th) {
-  const double q0 = L[n];
-  if (k < 3) return L[(k + 1) * tsz + n] / q0;
-  double q1 = L[tsz + n], q2 = L[2 * tsz + n], q3 = L[3 * tsz + n], q4 = L[4 * tsz + n];
-  const double u = q1 / q0, v = q2 / q0, w = q3 / q0;
-  const double p = (q4 - 0.5 * q0 * (u * u + v * v + w * w)) / th.const6;
-  if (k == 3) return p / q0 * th.const2;
-  if (n < 0 || n > dim) {
-    q1 = q0 * u;
-    q2 = q0 * v;
-    q3 = q0 * w;
-    q4 = p * th.const6 + q0 * (0.5 * (u * u + v * v + w * w));
-  }
-  const double uu = dir == 0 ? u : (dir == 1 ? v : w);
-  switch (k - 4) {
-    case 0: return q0 * uu;
-    case 1: return dir == 0 ? q1 * uu + p : q1 * uu;
-    case 2: return dir == 1 ? q2 * uu + p : q2 * uu;
-    case 3: return dir == 2 ? q3 * uu + p : q3 * uu;
-    default: return (q4 + p) * uu;
-  }
-}
-
-__device__ __forceinline__ int sidx(int a, int b) {
-  // symmetric 3x3 stored as (11,12,13,22,23,33)
-  const int lo = a < b ? a : b, hi = a < b ? b : a;
-  return lo == 0 ? hi : (lo == 1 ? 2 + hi : 5);
-}
-
-__device__ __forceinline__ double miucal(const Thermo& th, double t) {
-  return t * sqrt(t) * th.tc1 / (t + th.tc);
-}
-
-struct LaneIds {
-  int warp, lane, l, part, seg;
-};
-template <int WPL>
-__device__ __forceinline__ LaneIds lane_ids() {
-  LaneIds z;
-  z.warp = threadIdx.x >> 5;
-  z.lane = threadIdx.x & 31;
-  z.l = z.warp / WPL;
-  z.part = z.warp - z.l * WPL;
-  z.seg = z.part * 32 + z.lane;
-  return z;
-}
-
-// ------------------------------------------------------------------ pass A and pass B
-template <int S, int WPL>
-__global__ void __launch_bounds__(512) k_pass_ab(PassArgs a, int is_a) {
-  extern __shared__ double sm[];
-  const TileCtx c = tile_ctx(a);
-  const int tsz = c.TI * c.LP;
-  double* T = sm;
-  double* O = sm + 5 * tsz;
-  double* scan = O + tsz;
-  for (int m = 0; m < 5; ++m) load_tile(c, T + m * tsz, a.q + m * a.g.fs);
-  __syncthreads();
-  const LaneIds z = lane_ids<WPL>();
-  double* scl = scan + z.l * 4 * WPL;
-  const int dim = c.dim;
-  const int64_t fs = a.g.fs;
-
-  if (is_a && a.do_filter) {
-    for (int m = 0; m < 5; ++m) {
-      double* line = T + m * tsz + z.l * c.LP + HT;
-      double v[S];
-      rhs_filter<S>(v, a.opf, z.seg, [line](int n) { return line[n]; });
-      seg_solve<S, WPL>(v, a.opf, z.seg, z.lane, z.part, scl);
-      put_lane<S>(line, v, z.seg, a.opf.ext_lo, dim, true);
-    }
-    __syncthreads();
-    double* q = a.q;
-    store_tile(c, [&](int64_t off, int l, int n) {
-#pragma unroll
-      for (int m = 0; m < 5; ++m) q[m * fs + off] = T[m * tsz + l * c.LP + HT + n];
-    });
-  }
-
-  const double rd = a.g.rd[a.dir];
-  const double* L0 = T + z.l * c.LP + HT;
-  double* oline = O + z.l * c.LP + HT;
-  for (int k = 0; k < 9; ++k) {
-    double v[S];
-    rhs_deriv<S>(v, a.opd, z.seg, [&](int n) { return gfun(k, c.dir, L0, tsz, n, dim, a.th); });
-    seg_solve<S, WPL>(v, a.opd, z.seg, z.lane, z.part, scl);
-#pragma unroll
-    for (int t = 0; t < S; ++t) v[t] *= rd;
-    put_lane<S>(oline, v, z.seg, a.opd.ext_lo, dim, false);
-    __syncthreads();
-    if (k < 4) {
-      double* dst = a.D + k * fs;
-      store_tile(c, [&](int64_t off, int l, int n) { dst[off] = O[l * c.LP + HT + n]; });
-    } else {
-      double* dst = a.R + (k - 4) * fs;
-      if (is_a) store_tile(c, [&](int64_t off, int l, int n) { dst[off] = -O[l * c.LP + HT + n]; });
-      else store_tile(c, [&](int64_t off, int l, int n) { dst[off] = dst[off] - O[l * c.LP + HT + n]; });
-    }
-    __syncthreads();
-  }
-}
-
-// ------------------------------------------------------------------ pass C
-template <int S, int WPL>
-__global__ void __launch_bounds__(512) k_pass_c(PassArgs a) {
-  extern __shared__ double sm[];
-  const TileCtx c = tile_ctx(a);
-  const int tsz = c.TI * c.LP;
-  double* T = sm;
-  double* Dt = sm + 5 * tsz;
-  double* O = Dt + 4 * tsz;
-  double* scan = O + tsz;
-  double* red = scan + c.TI * 4 * WPL;
-  for (int m = 0; m < 5; ++m) load_tile(c, T + m * tsz, a.q + m * a.g.fs);
-  __syncthreads();
-  const LaneIds z = lane_ids<WPL>();
-  double* scl = scan + z.l * 4 * WPL;
-  const int dim = c.dim;
-  const int64_t fs = a.g.fs;
-  const double rd = a.g.rd[a.dir];
-  const double* L0 = T + z.l * c.LP + HT;
-
-  // gradients along C
-  for (int k = 0; k < 4; ++k) {
-    double v[S];
-    rhs_deriv<S>(v, a.opd, z.seg, [&](int n) { return gfun(k, c.dir, L0, tsz, n, dim, a.th); });
-    seg_solve<S, WPL>(v, a.opd, z.seg, z.lane, z.part, scl);
-#pragma unroll
-    for (int t = 0; t < S; ++t) v[t] *= rd;
-    put_lane<S>(Dt + k * tsz + z.l * c.LP + HT, v, z.seg, a.opd.ext_lo, dim, false);
-  }
-  __syncthreads();
-
-  // sigma and heat flux at every node (diffusion, tgvsolver.F90:659-694)
-  const Thermo th = a.th;
-  constexpr int dA = DIR_A, dB = DIR_B, dC = DIR_C;
-  constexpr int co1 = (DIR_C == 0) ? 1 : 0, co2 = (DIR_C == 2) ? 1 : 2;
-  double ke = 0.0, en = 0.0, di = 0.0;
-  const bool diag = a.partials != nullptr;
-  int bad = 0;
-  {
-    const int npl = dim + 1;
-    const int64_t b2 = c.i2 * c.so2;
-    for (int idx = threadIdx.x; idx < c.TI * npl; idx += blockDim.x) {
-      int l, n;
-      slot(c, idx, npl, l, n);
-      const int64_t i1 = c.i1_0 + l;
-      if (i1 >= c.n1) continue;
-      const int64_t off = b2 + i1 * c.so1 + (int64_t)n * c.sd;
-      const int tix = l * c.LP + HT + n;
-      double gr[4][3];
-#pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        gr[k][dA] = __ldg(a.DA + k * fs + off);
-        gr[k][dB] = __ldg(a.DB + k * fs + off);
-        gr[k][dC] = Dt[k * tsz + tix];
-      }
-      const double q0 = T[tix], q1 = T[tsz + tix], q2 = T[2 * tsz + tix], q3 = T[3 * tsz + tix],
-                   q4 = T[4 * tsz + tix];
-      const double u = q1 / q0, v = q2 / q0, w = q3 / q0;
-      const double p = (q4 - 0.5 * q0 * (u * u + v * v + w * w)) / th.const6;
-      const double tmp = p / q0 * th.const2;
-      if (!(q0 > 0.0) || !isfinite(q4)) bad = 1;
-      const double s11 = gr[0][0];
-      const double s12 = 0.5 * (gr[0][1] + gr[1][0]);
-      const double s13 = 0.5 * (gr[0][2] + gr[2][0]);
-      const double s22 = gr[1][1];
-      const double s23 = 0.5 * (gr[1][2] + gr[2][1]);
-      const double s33 = gr[2][2];
-      const double skk = (1.0 / 3.0) * (s11 + s22 + s33);
-      const double miu = miucal(th, tmp) / th.reynolds;
-      const double miu2 = 2.0 * miu;
-      const double hcc = (miu / th.prandtl) / th.const5;
-      double sg[6];
-      sg[0] = miu2 * (s11 - skk);
-      sg[1] = miu2 * s12;
-      sg[2] = miu2 * s13;
-      sg[3] = miu2 * (s22 - skk);
-      sg[4] = miu2 * s23;
-      sg[5] = miu2 * (s33 - skk);
-      double qf[3];
-      qf[0] = hcc * gr[3][0] + sg[0] * u + sg[1] * v + sg[2] * w;
-      qf[1] = hcc * gr[3][1] + sg[1] * u + sg[3] * v + sg[4] * w;
-      qf[2] = hcc * gr[3][2] + sg[2] * u + sg[4] * v + sg[5] * w;
-      double* VF = a.VF;
-      VF[0 * fs + off] = sg[sidx(dA, 0)];
-      VF[1 * fs + off] = sg[sidx(dA, 1)];
-      VF[2 * fs + off] = sg[sidx(dA, 2)];
-      VF[3 * fs + off] = qf[dA];
-      VF[4 * fs + off] = sg[sidx(dB, dB)];
-      VF[5 * fs + off] = sg[sidx(dB, dC)];
-      VF[6 * fs + off] = qf[dB];
-      const double vc[4] = {sg[sidx(dC, 0)], sg[sidx(dC, 1)], sg[sidx(dC, 2)], qf[dC]};
-#pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        double* line = Dt + k * tsz + l * c.LP + HT;
-        line[n] = vc[k];
-        put_images(line, n, dim, vc[k]);
-      }
-      if (diag) {
-        // node n along C, i1 along the first other axis, i2 along the second
-        (void)co1; (void)co2;
-        if (n >= 1 && i1 >= 1 && c.i2 >= 1) {
-          // stacal (tgvsolver.F90:913-931) and diss_rate_cal (statistic.F90:1009-1034)
-          ke += q0 * (u * u + v * v + w * w);
-          const double om1 = gr[2][1] - gr[1][2];
-          const double om2 = gr[0][2] - gr[2][0];
-          const double om3 = gr[1][0] - gr[0][1];
-          en += q0 * (om1 * om1 + om2 * om2 + om3 * om3);
-          const double div = s11 + s22 + s33;
-          di += 2.0 * miu * (s11 * s11 + s22 * s22 + s33 * s33 + 2.0 * (s12 * s12 + s13 * s13 + s23 * s23) -
-                             (1.0 / 3.0) * (div * div));
-        }
-      }
-    }
-  }
-  if (bad) atomicOr(a.err, 1);
-  if (diag) {
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) {
-      ke += __shfl_down_sync(FULL, ke, off);
-      en += __shfl_down_sync(FULL, en, off);
-      di += __shfl_down_sync(FULL, di, off);
-    }
-    if (z.lane == 0) { red[3 * z.warp] = ke; red[3 * z.warp + 1] = en; red[3 * z.warp + 2] = di; }
-  }
-  __syncthreads();
-  if (diag && threadIdx.x == 0) {
-    double s0 = 0.0, s1 = 0.0, s2 = 0.0;
-    const int nw = blockDim.x >> 5;
-    for (int w = 0; w < nw; ++w) { s0 += red[3 * w]; s1 += red[3 * w + 1]; s2 += red[3 * w + 2]; }
-    double* pp = a.partials + 3 * ((int64_t)blockIdx.y * gridDim.x + blockIdx.x);
-    pp[0] = s0; pp[1] = s1; pp[2] = s2;
-  }
-
-  // viscous divergence along C (diffusion, tgvsolver.F90:763-787), kept in Dt
-  for (int k = 0; k < 4; ++k) {
-    double* line = Dt + k * tsz + z.l * c.LP + HT;
-    double v[S];
-    rhs_deriv<S>(v, a.opd, z.seg, [line](int n) { return line[n]; });
-    seg_solve<S, WPL>(v, a.opd, z.seg, z.lane, z.part, scl);
-#pragma unroll
-    for (int t = 0; t < S; ++t) v[t] *= rd;
-    put_lane<S>(line, v, z.seg, a.opd.ext_lo, dim, false);
-  }
-  // convection along C; R += visc_C - conv_C
-  double* oline = O + z.l * c.LP + HT;
-  for (int k = 4; k < 9; ++k) {
-    double v[S];
-    rhs_deriv<S>(v, a.opd, z.seg, [&](int n) { return gfun(k, c.dir, L0, tsz, n, dim, a.th); });
-    seg_solve<S, WPL>(v, a.opd, z.seg, z.lane, z.part, scl);
-#pragma unroll
-    for (int t = 0; t < S; ++t) v[t] *= rd;
-    put_lane<S>(oline, v, z.seg, a.opd.ext_lo, dim, false);
-    __syncthreads();
-    const int m = k - 4;
-    double* dst = a.R + m * fs;
-    if (m == 0) {
-      store_tile(c, [&](int64_t off, int l, int n) { dst[off] = dst[off] - O[l * c.LP + HT + n]; });
-    } else {
-      const double* vis = Dt + (m - 1) * tsz;
-      store_tile(c, [&](int64_t off, int l, int n) {
-        const int tix = l * c.LP + HT + n;
-        dst[off] = dst[off] - O[tix] + vis[tix];
-      });
-    }
-    __syncthreads();
-  }
-}
-
-// ------------------------------------------------------------------ pass A' (visc along A)
-template <int S, int WPL>
-__global__ void __launch_bounds__(512) k_pass_va(PassArgs a) {
-  extern __shared__ double sm[];
-  const TileCtx c = tile_ctx(a);
-  const int tsz = c.TI * c.LP;
-  double* V = sm;
-  double* scan = sm + 4 * tsz;
-  const int64_t fs = a.g.fs;
-  for (int k = 0; k < 4; ++k) load_tile(c, V + k * tsz, a.VF + k * fs);
-  __syncthreads();
-  const LaneIds z = lane_ids<WPL>();
-  double* scl = scan + z.l * 4 * WPL;
-  const double rd = a.g.rd[a.dir];
-  for (int k = 0; k < 4; ++k) {
-    double* line = V + k * tsz + z.l * c.LP + HT;
-    double v[S];
-    rhs_deriv<S>(v, a.opd, z.seg, [line](int n) { return line[n]; });
-    seg_solve<S, WPL>(v, a.opd, z.seg, z.lane, z.part, scl);
-#pragma unroll
-    for (int t = 0; t < S; ++t) v[t] *= rd;
-    put_lane<S>(line, v, z.seg, a.opd.ext_lo, c.dim, false);
-  }
-  __syncthreads();
-  double* R = a.R;
-  store_tile(c, [&](int64_t off, int l, int n) {
-    const int tix = l * c.LP + HT + n;
-#pragma unroll
-    for (int k = 0; k < 4; ++k) R[(1 + k) * fs + off] = R[(1 + k) * fs + off] + V[k * tsz + tix];
-  });
-}
-
-// ------------------------------------------------------------------ pass B' (visc along B, update, filter)
-template <int S, int WPL>
-__global__ void __launch_bounds__(512) k_pass_vb(PassArgs a) {
-  extern __shared__ double sm[];
-  const TileCtx c = tile_ctx(a);
-  const int tsz = c.TI * c.LP;
-  double* V = sm;
-  double* O = sm + 4 * tsz;
-  double* scan = O + tsz;
-  const int64_t fs = a.g.fs;
-  constexpr int dA = DIR_A, dB = DIR_B;
-  // viscous flux along B for momentum component k (physical) and energy: see pass C's VF layout
-  for (int k = 0; k < 4; ++k) {
-    const int vf = (k == 3) ? 6 : (k == dA ? dB : (k == dB ? 4 : 5));
-    load_tile(c, V + k * tsz, a.VF + vf * fs);
-  }
-  __syncthreads();
-  const LaneIds z = lane_ids<WPL>();
-  double* scl = scan + z.l * 4 * WPL;
-  const double rd = a.g.rd[a.dir];
-  const int dim = c.dim;
-  double* oline = O + z.l * c.LP + HT;
-  for (int m = 0; m < 5; ++m) {
-    if (m >= 1) {
-      const double* line = V + (m - 1) * tsz + z.l * c.LP + HT;
-      double v[S];
-      rhs_deriv<S>(v, a.opd, z.seg, [line](int n) { return line[n]; });
-      seg_solve<S, WPL>(v, a.opd, z.seg, z.lane, z.part, scl);
-#pragma unroll
-      for (int t = 0; t < S; ++t) v[t] *= rd;
-      put_lane<S>(oline, v, z.seg, a.opd.ext_lo, dim, false);
-    }
-    __syncthreads();
-    double* R = a.R + m * fs;
-    if (a.mode == 0) {
-      store_tile(c, [&](int64_t off, int l, int n) {
-        const double vis = (m >= 1) ? O[l * c.LP + HT + n] : 0.0;
-        R[off] = R[off] + vis;
-      });
-      __syncthreads();
-      continue;
-    }
-    // SSP-RK3 stage update, tgvsolver.F90:1055-1057
-    const double* qs = a.qsave + m * fs;
-    const double* qq = a.q + m * fs;
-    const double c1 = a.c1, c2 = a.c2, c3 = a.c3, dt = a.dt;
-    store_tile(c, [&](int64_t off, int l, int n) {
-      double* line = O + l * c.LP + HT;
-      const double vis = (m >= 1) ? line[n] : 0.0;
-      const double r = R[off] + vis;
-      const double qc = (c2 != 0.0) ? c2 * qq[off] : 0.0;
-      const double qn = c1 * qs[off] + qc + c3 * r * dt;
-      line[n] = qn;
-      put_images(line, n, dim, qn);
-    });
-    __syncthreads();
-    if (a.do_filter) {
-      double v[S];
-      rhs_filter<S>(v, a.opf, z.seg, [oline](int n) { return oline[n]; });
-      seg_solve<S, WPL>(v, a.opf, z.seg, z.lane, z.part, scl);
-      put_lane<S>(oline, v, z.seg, a.opf.ext_lo, dim, false);
-      __syncthreads();
-    }
-    double* qo = a.qout + m * fs;
-    store_tile(c, [&](int64_t off, int l, int n) { qo[off] = O[l * c.LP + HT + n]; });
-    __syncthreads();
-  }
-}
-
-// ------------------------------------------------------------------ pass F (filter only, 5 fields)
-template <int S, int WPL>
-__global__ void __launch_bounds__(512) k_pass_f(PassArgs a) {
-  extern __shared__ double sm[];
-  const TileCtx c = tile_ctx(a);
-  const int tsz = c.TI * c.LP;
-  double* T = sm;
-  double* scan = sm + 5 * tsz;
-  const int64_t fs = a.g.fs;
-  for (int m = 0; m < 5; ++m) load_tile(c, T + m * tsz, a.q + m * fs);
-  __syncthreads();
-  const LaneIds z = lane_ids<WPL>();
-  double* scl = scan + z.l * 4 * WPL;
-  for (int m = 0; m < 5; ++m) {
-    double* line = T + m * tsz + z.l * c.LP + HT;
-    double v[S];
-    rhs_filter<S>(v, a.opf, z.seg, [line](int n) { return line[n]; });
-    seg_solve<S, WPL>(v, a.opf, z.seg, z.lane, z.part, scl);
-    put_lane<S>(line, v, z.seg, a.opf.ext_lo, c.dim, false);
-  }
-  __syncthreads();
-  double* q = a.q;
-  store_tile(c, [&](int64_t off, int l, int n) {
-#pragma unroll
-    for (int m = 0; m < 5; ++m) q[m * fs + off] = T[m * tsz + l * c.LP + HT + n];
-  });
-}
-
 // ------------------------------------------------------------------ small kernels
 __global__ void k_diag_reduce(const double* __restrict__ partials, int nparts, double* hist, int* counter,
                               double norm) {
@@ -608,45 +129,6 @@ __global__ void k_pack(BoxGeo g, double* state, double* user, int64_t us0, int64
   }
 }
 
-template <int S, int WPL>
-cudaError_t launch_pass_t(int pass, const PassArgs& a, cudaStream_t st) {
-  const int o1 = (a.dir == 0) ? 1 : 0, o2 = (a.dir == 2) ? 1 : 2;
-  const int tsz = a.TI * a.LP;
-  const int ntile = pass_tiles(pass);
-  size_t smem = ((size_t)ntile * tsz + (size_t)a.TI * 4 * WPL) * sizeof(double);
-  if (pass == PASS_C) smem += 32 * 3 * sizeof(double);
-  dim3 grid((unsigned)((a.g.N[o1] + 1 + a.TI - 1) / a.TI), (unsigned)(a.g.N[o2] + 1));
-  const int threads = a.TI * WPL * 32;
-  cudaError_t e = cudaSuccess;
-  switch (pass) {
-    case PASS_A:
-    case PASS_B:
-      e = cudaFuncSetAttribute(k_pass_ab<S, WPL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      if (e == cudaSuccess) k_pass_ab<S, WPL><<<grid, threads, smem, st>>>(a, pass == PASS_A ? 1 : 0);
-      break;
-    case PASS_C:
-      e = cudaFuncSetAttribute(k_pass_c<S, WPL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      if (e == cudaSuccess) k_pass_c<S, WPL><<<grid, threads, smem, st>>>(a);
-      break;
-    case PASS_VA:
-      e = cudaFuncSetAttribute(k_pass_va<S, WPL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      if (e == cudaSuccess) k_pass_va<S, WPL><<<grid, threads, smem, st>>>(a);
-      break;
-    case PASS_VB:
-      e = cudaFuncSetAttribute(k_pass_vb<S, WPL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      if (e == cudaSuccess) k_pass_vb<S, WPL><<<grid, threads, smem, st>>>(a);
-      break;
-    case PASS_F:
-      e = cudaFuncSetAttribute(k_pass_f<S, WPL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      if (e == cudaSuccess) k_pass_f<S, WPL><<<grid, threads, smem, st>>>(a);
-      break;
-    default:
-      return cudaErrorInvalidValue;
-  }
-  if (e != cudaSuccess) return e;
-  return cudaGetLastError();
-}
-
 }  // namespace
 
 int pass_tiles(int pass) {
@@ -660,12 +142,17 @@ int pass_tiles(int pass) {
   return 0;
 }
 
+template <int S, int WPL>
+cudaError_t launch_pass_t(int pass, const PassArgs& a, cudaStream_t st);
+
 cudaError_t launch_pass(int pass, const PassArgs& a, int S, int WPL, cudaStream_t st) {
   if (S == 3 && WPL == 1) return launch_pass_t<3, 1>(pass, a, st);
   if (S == 5 && WPL == 1) return launch_pass_t<5, 1>(pass, a, st);
   if (S == 5 && WPL == 2) return launch_pass_t<5, 2>(pass, a, st);
   if (S == 5 && WPL == 4) return launch_pass_t<5, 4>(pass, a, st);
-  if (S == 5 && WPL == 8) return launch_pass_t<5, 8>(pass, a, st);
+  if (S == 9 && WPL == 1) return launch_pass_t<9, 1>(pass, a, st);
+  if (S == 9 && WPL == 2) return launch_pass_t<9, 2>(pass, a, st);
+  if (S == 9 && WPL == 4) return launch_pass_t<9, 4>(pass, a, st);
   return cudaErrorInvalidValue;
 }
 

@@ -1,0 +1,594 @@
+// Pass kernels of the RK3 step (see tgv.cu for the pass structure). Included once per solve
+// layout (S rows per lane, WPL warps per line) by tgv_l*.cu so the layouts compile in parallel.
+//
+// Thread roles in a CTA of TI lines x WPL warps:
+//  * solve role: warp w works on line w / WPL, lanes own S consecutive rows (seg_solve);
+//  * slot role (staging, pointwise work, stores): for x lines each line's 32*WPL threads walk
+//    its contiguous nodes; for y/z lines consecutive threads take consecutive lines (TI adjacent
+//    lines are contiguous in x) and walk the nodes with stride 32*WPL. Each thread keeps one
+//    line in this role, so no index arithmetic beyond one multiply-add per node.
+#pragma once
+#include "tgv.cuh"
+
+namespace astr {
+
+namespace pass_detail {
+
+template <int DIR, int WPL>
+struct TileCtx {
+  static constexpr int o1 = (DIR == 0) ? 1 : 0;
+  static constexpr int o2 = (DIR == 2) ? 1 : 2;
+  static constexpr int TPL = 32 * WPL;   // threads per line
+  int dim, TI, LP;
+  int sl, sn0;          // slot role: this thread's line and first node offset
+  bool svalid;          // that line exists
+  int64_t sbase;        // element offset of node 0 of that line
+  int64_t sd;
+  __device__ __forceinline__ TileCtx(const PassArgs& a) {
+    dim = a.g.N[DIR];
+    TI = a.TI;
+    LP = a.LP;
+    sd = a.g.st[DIR];
+    if (DIR == 0) {
+      sl = threadIdx.x / TPL;
+      sn0 = threadIdx.x - sl * TPL;
+    } else {
+      sl = threadIdx.x & (a.TI - 1);
+      sn0 = threadIdx.x / a.TI;
+    }
+    const int64_t i1 = (int64_t)blockIdx.x * a.TI + sl;
+    svalid = i1 < a.g.N[o1] + 1;
+    sbase = i1 * a.g.st[o1] + (int64_t)blockIdx.y * a.g.st[o2];
+  }
+  // f(tile offset of node n on the slot line, global offset) for n = n_lo.. n_hi
+  template <class F>
+  __device__ __forceinline__ void for_nodes(int n_lo, int n_hi, F f) const {
+    const int tix0 = sl * LP + HT;
+    for (int n = n_lo + sn0; n <= n_hi; n += TPL) f(tix0 + n, n);
+  }
+  // Two-phase form for read-modify-write of global fields: ld(n) for NB nodes first (their loads
+  // overlap), then st(tile offset, n, loaded value).
+  template <int NB, class Ld, class St>
+  __device__ __forceinline__ void for_nodes_rmw(int n_lo, int n_hi, Ld ld, St st) const {
+    const int tix0 = sl * LP + HT;
+    for (int nb = n_lo + sn0; nb <= n_hi; nb += NB * TPL) {
+      double r[NB];
+#pragma unroll
+      for (int b = 0; b < NB; ++b) {
+        const int n = nb + b * TPL;
+        r[b] = (n <= n_hi) ? ld(n) : 0.0;
+      }
+#pragma unroll
+      for (int b = 0; b < NB; ++b) {
+        const int n = nb + b * TPL;
+        if (n <= n_hi) st(tix0 + n, n, r[b]);
+      }
+    }
+  }
+};
+
+__device__ __forceinline__ void cp_async8(double* sdst, const double* gsrc) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+}
+
+// Stage the slot line of one field, nodes -HT..dim+HT with the periodic wrap, asynchronously.
+template <int DIR, int WPL>
+__device__ __forceinline__ void load_tile(const TileCtx<DIR, WPL>& c, double* tile, const double* __restrict__ fld) {
+  const double* src = fld + c.sbase;
+  const int dim = c.dim;
+  if (c.svalid) {
+    c.for_nodes(-HT, dim + HT, [&](int tix, int n) { cp_async8(tile + tix, src + (int64_t)wrap_node(n, dim) * c.sd); });
+  } else {
+    c.for_nodes(-HT, dim + HT, [&](int tix, int n) { tile[tix] = 1.0; });   // finite filler, never stored
+  }
+}
+
+// Write a lane's solution rows (nodes 0..dim) into a tile line, optionally with the periodic
+// halo images of those nodes.
+template <int S>
+__device__ __forceinline__ void put_lane(double* line, const double (&v)[S], int seg, int ext, int dim, bool images) {
+#pragma unroll
+  for (int t = 0; t < S; ++t) {
+    const int n = seg * S + t - ext;
+    if (n < 0 || n > dim) continue;
+    line[n] = v[t];
+    if (images) {
+      if (n >= 1 && n <= HT) line[dim + n] = v[t];
+      if (n >= dim - HT && n <= dim - 1) line[n - dim] = v[t];
+    }
+  }
+}
+
+__device__ __forceinline__ void put_images(double* line, int n, int dim, double v) {
+  if (n >= 1 && n <= HT) line[dim + n] = v;
+  if (n >= dim - HT && n <= dim - 1) line[n - dim] = v;
+}
+
+// q -> (rho, u, v, w, p) in place over every staged node of the 5 tiles (q2fvar,
+// tgvsolver.F90:92-121), once per node.
+template <int DIR, int WPL>
+__device__ __forceinline__ void to_prims(const TileCtx<DIR, WPL>& c, double* T, int tsz, const Thermo& th) {
+  c.for_nodes(-HT, c.dim + HT, [&](int o, int) {
+    const double q0 = T[o], q1 = T[tsz + o], q2 = T[2 * tsz + o], q3 = T[3 * tsz + o], q4 = T[4 * tsz + o];
+    const double u = q1 / q0, v = q2 / q0, w = q3 / q0;
+    const double p = (q4 - 0.5 * q0 * (u * u + v * v + w * w)) / th.const6;
+    T[tsz + o] = u;
+    T[2 * tsz + o] = v;
+    T[3 * tsz + o] = w;
+    T[4 * tsz + o] = p;
+  });
+}
+
+// Pointwise function K of the primitive tiles at node n of a line (L = tile 0 of the line):
+// 0..2 velocity, 3 temperature, 4..8 the Euler flux along DIR (convection,
+// tgvsolver.F90:559-564; q_m = rho*u_m and E = p/(gamma-1) + rho|u|^2/2 as fvar2q rebuilds them).
+template <int K, int DIR>
+__device__ __forceinline__ double gprim(const double* L, int tsz, int n, const Thermo& th) {
+  if (K < 3) return L[(K + 1) * tsz + n];
+  if (K == 3) return L[4 * tsz + n] / L[n] * th.const2;
+  const double rho = L[n];
+  const double ud = L[(1 + DIR) * tsz + n];
+  constexpr int m = K - 4;
+  if (m == 0) return rho * ud;
+  if (m <= 3) {
+    const double f = rho * L[m * tsz + n] * ud;
+    return (m - 1 == DIR) ? f + L[4 * tsz + n] : f;
+  }
+  const double u = L[tsz + n], v = L[2 * tsz + n], w = L[3 * tsz + n], p = L[4 * tsz + n];
+  const double E = p * th.const6 + rho * (0.5 * (u * u + v * v + w * w));
+  return (E + p) * ud;
+}
+
+template <int DIR>
+__device__ __forceinline__ double gprim_rt(int K, const double* L, int tsz, int n, const Thermo& th) {
+  switch (K) {
+    case 0: return gprim<0, DIR>(L, tsz, n, th);
+    case 1: return gprim<1, DIR>(L, tsz, n, th);
+    case 2: return gprim<2, DIR>(L, tsz, n, th);
+    case 3: return gprim<3, DIR>(L, tsz, n, th);
+    case 4: return gprim<4, DIR>(L, tsz, n, th);
+    case 5: return gprim<5, DIR>(L, tsz, n, th);
+    case 6: return gprim<6, DIR>(L, tsz, n, th);
+    case 7: return gprim<7, DIR>(L, tsz, n, th);
+    default: return gprim<8, DIR>(L, tsz, n, th);
+  }
+}
+
+// Window of pointwise function K (branch once per solve, not per node).
+template <int W, int DIR>
+__device__ __forceinline__ void prim_window(double (&w)[W], int K, const double* L, int tsz, int n0, int dim,
+                                            const Thermo& th) {
+  switch (K) {
+    case 0: fill_window<W>(w, n0, dim, [&](int n) { return gprim<0, DIR>(L, tsz, n, th); }); break;
+    case 1: fill_window<W>(w, n0, dim, [&](int n) { return gprim<1, DIR>(L, tsz, n, th); }); break;
+    case 2: fill_window<W>(w, n0, dim, [&](int n) { return gprim<2, DIR>(L, tsz, n, th); }); break;
+    case 3: fill_window<W>(w, n0, dim, [&](int n) { return gprim<3, DIR>(L, tsz, n, th); }); break;
+    case 4: fill_window<W>(w, n0, dim, [&](int n) { return gprim<4, DIR>(L, tsz, n, th); }); break;
+    case 5: fill_window<W>(w, n0, dim, [&](int n) { return gprim<5, DIR>(L, tsz, n, th); }); break;
+    case 6: fill_window<W>(w, n0, dim, [&](int n) { return gprim<6, DIR>(L, tsz, n, th); }); break;
+    case 7: fill_window<W>(w, n0, dim, [&](int n) { return gprim<7, DIR>(L, tsz, n, th); }); break;
+    default: fill_window<W>(w, n0, dim, [&](int n) { return gprim<8, DIR>(L, tsz, n, th); }); break;
+  }
+}
+
+__device__ __forceinline__ int sidx(int a, int b) {
+  // symmetric 3x3 stored as (11,12,13,22,23,33)
+  const int lo = a < b ? a : b, hi = a < b ? b : a;
+  return lo == 0 ? hi : (lo == 1 ? 2 + hi : 5);
+}
+
+__device__ __forceinline__ double miucal(const Thermo& th, double t) {
+  return t * sqrt(t) * th.tc1 / (t + th.tc);
+}
+
+struct LaneIds {
+  int warp, lane, l, part, seg;
+};
+template <int WPL>
+__device__ __forceinline__ LaneIds lane_ids() {
+  LaneIds z;
+  z.warp = threadIdx.x >> 5;
+  z.lane = threadIdx.x & 31;
+  z.l = z.warp / WPL;
+  z.part = z.warp - z.l * WPL;
+  z.seg = z.part * 32 + z.lane;
+  return z;
+}
+
+// Derivative of pointwise function K along DIR for this lane's rows (scaled by 1/dx).
+template <int S, int WPL, int DIR>
+__device__ __forceinline__ void dsolve(double (&v)[S], int K, const PassArgs& a, const LaneIds& z, const double* L0,
+                                       int tsz, double* scl, double rd) {
+  const LineOp& op = a.opd;
+  const int r0 = z.seg * S;
+  double w[S + 4];
+  prim_window<S + 4, DIR>(w, K, L0, tsz, r0 - op.ext_lo - 2, op.dim, a.th);
+  stencil_deriv<S>(v, w);
+  if (deriv_edge_lane<S>(op, r0)) fix_deriv_rows<S>(v, op, r0, [&](int n) { return gprim_rt<DIR>(K, L0, tsz, n, a.th); });
+  seg_solve<S, WPL>(v, op.tab, z.seg, z.lane, z.part, z.l, scl);
+#pragma unroll
+  for (int t = 0; t < S; ++t) v[t] *= rd;
+}
+
+// Solve of a staged tile line (derivative or filter) in place; the filter keeps its physical
+// end values (it never runs with physical closures here: every pass line is periodic).
+template <int S, int WPL>
+__device__ __forceinline__ void solve_line(double* line, const LineOp& op, const LaneIds& z, double* scl, double scale,
+                                           bool images) {
+  double v[S];
+  if (op.kind == OP_FILTER) rhs_filter<S>(v, op, z.seg, [line](int n) { return line[n]; });
+  else rhs_deriv<S>(v, op, z.seg, [line](int n) { return line[n]; });
+  seg_solve<S, WPL>(v, op.tab, z.seg, z.lane, z.part, z.l, scl);
+  if (scale != 1.0) {
+#pragma unroll
+    for (int t = 0; t < S; ++t) v[t] *= scale;
+  }
+  put_lane<S>(line, v, z.seg, op.ext_lo, op.dim, images);
+}
+
+// ------------------------------------------------------------------ pass A and pass B
+template <int S, int WPL, int DIR, bool IS_A>
+__global__ void __launch_bounds__(512) k_pass_ab(PassArgs a) {
+  extern __shared__ double sm[];
+  const TileCtx<DIR, WPL> c(a);
+  const int tsz = c.TI * c.LP;
+  double* T = sm;
+  double* O = sm + 5 * tsz;
+  double* scan = O + tsz;
+  const int64_t fs = a.g.fs;
+  for (int m = 0; m < 5; ++m) load_tile(c, T + m * tsz, a.q + m * fs);
+  cp_async_wait_all();
+  __syncthreads();
+  const LaneIds z = lane_ids<WPL>();
+  double* scl = scan + z.l * 2 * WPL;
+  const int dim = c.dim;
+
+  if (IS_A && a.do_filter) {
+    for (int m = 0; m < 5; ++m) solve_line<S, WPL>(T + m * tsz + z.l * c.LP + HT, a.opf, z, scl, 1.0, true);
+    __syncthreads();
+    if (c.svalid) {
+      double* q = a.q + c.sbase;
+      c.for_nodes(0, dim, [&](int o, int n) {
+        const int64_t off = (int64_t)n * c.sd;
+#pragma unroll
+        for (int m = 0; m < 5; ++m) q[m * fs + off] = T[m * tsz + o];
+      });
+    }
+    __syncthreads();   // every filtered value is stored before the tiles turn into primitives
+  }
+  to_prims(c, T, tsz, a.th);
+  __syncthreads();
+
+  const double rd = a.g.rd[DIR];
+  const double* L0 = T + z.l * c.LP + HT;
+  double* oline = O + z.l * c.LP + HT;
+  for (int K = 0; K < 9; ++K) {
+    double v[S];
+    dsolve<S, WPL, DIR>(v, K, a, z, L0, tsz, scl, rd);
+    put_lane<S>(oline, v, z.seg, a.opd.ext_lo, dim, false);
+    __syncthreads();
+    if (c.svalid) {
+      double* dst = (K < 4) ? a.D + K * fs + c.sbase : a.R + (K - 4) * fs + c.sbase;
+      if (K < 4) c.for_nodes(0, dim, [&](int o, int n) { dst[(int64_t)n * c.sd] = O[o]; });
+      else if (IS_A) c.for_nodes(0, dim, [&](int o, int n) { dst[(int64_t)n * c.sd] = -O[o]; });
+      else c.for_nodes_rmw<4>(0, dim, [&](int n) { return dst[(int64_t)n * c.sd]; },
+                              [&](int o, int n, double r) { dst[(int64_t)n * c.sd] = r - O[o]; });
+    }
+    __syncthreads();
+  }
+}
+
+// ------------------------------------------------------------------ pass C
+template <int S, int WPL, int DIR>
+__global__ void __launch_bounds__(512) k_pass_c(PassArgs a) {
+  extern __shared__ double sm[];
+  const TileCtx<DIR, WPL> c(a);
+  const int tsz = c.TI * c.LP;
+  double* T = sm;
+  double* Dt = sm + 5 * tsz;
+  double* O = Dt + 4 * tsz;
+  double* scan = O + tsz;
+  double* red = scan + c.TI * 2 * WPL;
+  const int64_t fs = a.g.fs;
+  for (int m = 0; m < 5; ++m) load_tile(c, T + m * tsz, a.q + m * fs);
+  cp_async_wait_all();
+  __syncthreads();
+  const int dim = c.dim;
+  to_prims(c, T, tsz, a.th);
+  __syncthreads();
+  const LaneIds z = lane_ids<WPL>();
+  double* scl = scan + z.l * 2 * WPL;
+  const double rd = a.g.rd[DIR];
+  const double* L0 = T + z.l * c.LP + HT;
+
+  // gradients along C
+  for (int K = 0; K < 4; ++K) {
+    double v[S];
+    dsolve<S, WPL, DIR>(v, K, a, z, L0, tsz, scl, rd);
+    put_lane<S>(Dt + K * tsz + z.l * c.LP + HT, v, z.seg, a.opd.ext_lo, dim, false);
+  }
+  __syncthreads();
+
+  // sigma and heat flux at every node (diffusion, tgvsolver.F90:659-694)
+  const Thermo th = a.th;
+  constexpr int dA = DIR_A, dB = DIR_B, dC = DIR_C;
+  static_assert(DIR == DIR_C, "pass C runs along DIR_C");
+  double ke = 0.0, en = 0.0, di = 0.0;
+  const bool diag = a.partials != nullptr;
+  int bad = 0;
+  if (c.svalid) {
+    const double* DA = a.DA + c.sbase;
+    const double* DB = a.DB + c.sbase;
+    double* VF = a.VF + c.sbase;
+    const bool row_ok = (blockIdx.x * (int64_t)c.TI + c.sl) >= 1 && blockIdx.y >= 1;
+    c.for_nodes(0, dim, [&](int tix, int n) {
+      const int64_t off = (int64_t)n * c.sd;
+      double gr[4][3];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        gr[k][dA] = __ldg(DA + k * fs + off);
+        gr[k][dB] = __ldg(DB + k * fs + off);
+        gr[k][dC] = Dt[k * tsz + tix];
+      }
+      const double q0 = T[tix], u = T[tsz + tix], v = T[2 * tsz + tix], w = T[3 * tsz + tix], p = T[4 * tsz + tix];
+      const double tmp = p / q0 * th.const2;
+      if (!(q0 > 0.0) || !isfinite(p)) bad = 1;
+      const double s11 = gr[0][0];
+      const double s12 = 0.5 * (gr[0][1] + gr[1][0]);
+      const double s13 = 0.5 * (gr[0][2] + gr[2][0]);
+      const double s22 = gr[1][1];
+      const double s23 = 0.5 * (gr[1][2] + gr[2][1]);
+      const double s33 = gr[2][2];
+      const double skk = (1.0 / 3.0) * (s11 + s22 + s33);
+      const double miu = miucal(th, tmp) / th.reynolds;
+      const double miu2 = 2.0 * miu;
+      const double hcc = (miu / th.prandtl) / th.const5;
+      double sg[6];
+      sg[0] = miu2 * (s11 - skk);
+      sg[1] = miu2 * s12;
+      sg[2] = miu2 * s13;
+      sg[3] = miu2 * (s22 - skk);
+      sg[4] = miu2 * s23;
+      sg[5] = miu2 * (s33 - skk);
+      double qf[3];
+      qf[0] = hcc * gr[3][0] + sg[0] * u + sg[1] * v + sg[2] * w;
+      qf[1] = hcc * gr[3][1] + sg[1] * u + sg[3] * v + sg[4] * w;
+      qf[2] = hcc * gr[3][2] + sg[2] * u + sg[4] * v + sg[5] * w;
+      VF[0 * fs + off] = sg[sidx(dA, 0)];
+      VF[1 * fs + off] = sg[sidx(dA, 1)];
+      VF[2 * fs + off] = sg[sidx(dA, 2)];
+      VF[3 * fs + off] = qf[dA];
+      VF[4 * fs + off] = sg[sidx(dB, dB)];
+      VF[5 * fs + off] = sg[sidx(dB, dC)];
+      VF[6 * fs + off] = qf[dB];
+      const double vc[4] = {sg[sidx(dC, 0)], sg[sidx(dC, 1)], sg[sidx(dC, 2)], qf[dC]};
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        double* line = Dt + k * tsz + c.sl * c.LP + HT;
+        line[n] = vc[k];
+        put_images(line, n, dim, vc[k]);
+      }
+      if (diag && n >= 1 && row_ok) {
+        // stacal (tgvsolver.F90:913-931) and diss_rate_cal (statistic.F90:1009-1034)
+        ke += q0 * (u * u + v * v + w * w);
+        const double om1 = gr[2][1] - gr[1][2];
+        const double om2 = gr[0][2] - gr[2][0];
+        const double om3 = gr[1][0] - gr[0][1];
+        en += q0 * (om1 * om1 + om2 * om2 + om3 * om3);
+        const double div = s11 + s22 + s33;
+        di += 2.0 * miu * (s11 * s11 + s22 * s22 + s33 * s33 + 2.0 * (s12 * s12 + s13 * s13 + s23 * s23) -
+                           (1.0 / 3.0) * (div * div));
+      }
+    });
+  }
+  if (bad) atomicOr(a.err, 1);
+  if (diag) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      ke += __shfl_down_sync(FULL, ke, off);
+      en += __shfl_down_sync(FULL, en, off);
+      di += __shfl_down_sync(FULL, di, off);
+    }
+    if (z.lane == 0) { red[3 * z.warp] = ke; red[3 * z.warp + 1] = en; red[3 * z.warp + 2] = di; }
+  }
+  __syncthreads();
+  if (diag && threadIdx.x == 0) {
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+    const int nw = blockDim.x >> 5;
+    for (int w = 0; w < nw; ++w) { s0 += red[3 * w]; s1 += red[3 * w + 1]; s2 += red[3 * w + 2]; }
+    double* pp = a.partials + 3 * ((int64_t)blockIdx.y * gridDim.x + blockIdx.x);
+    pp[0] = s0; pp[1] = s1; pp[2] = s2;
+  }
+
+  // viscous divergence along C (diffusion, tgvsolver.F90:763-787), kept in Dt
+  for (int k = 0; k < 4; ++k) solve_line<S, WPL>(Dt + k * tsz + z.l * c.LP + HT, a.opd, z, scl, rd, false);
+  // convection along C; R += visc_C - conv_C
+  double* oline = O + z.l * c.LP + HT;
+  for (int K = 4; K < 9; ++K) {
+    double v[S];
+    dsolve<S, WPL, DIR>(v, K, a, z, L0, tsz, scl, rd);
+    put_lane<S>(oline, v, z.seg, a.opd.ext_lo, dim, false);
+    __syncthreads();
+    const int m = K - 4;
+    if (c.svalid) {
+      double* dst = a.R + m * fs + c.sbase;
+      if (m == 0) {
+        c.for_nodes_rmw<4>(0, dim, [&](int n) { return dst[(int64_t)n * c.sd]; },
+                           [&](int o, int n, double r) { dst[(int64_t)n * c.sd] = r - O[o]; });
+      } else {
+        const double* vis = Dt + (m - 1) * tsz;
+        c.for_nodes_rmw<4>(0, dim, [&](int n) { return dst[(int64_t)n * c.sd]; },
+                           [&](int o, int n, double r) { dst[(int64_t)n * c.sd] = r - O[o] + vis[o]; });
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// ------------------------------------------------------------------ pass A' (visc along A)
+template <int S, int WPL, int DIR>
+__global__ void __launch_bounds__(512) k_pass_va(PassArgs a) {
+  extern __shared__ double sm[];
+  const TileCtx<DIR, WPL> c(a);
+  const int tsz = c.TI * c.LP;
+  double* V = sm;
+  double* scan = sm + 4 * tsz;
+  const int64_t fs = a.g.fs;
+  for (int k = 0; k < 4; ++k) load_tile(c, V + k * tsz, a.VF + k * fs);
+  cp_async_wait_all();
+  __syncthreads();
+  const LaneIds z = lane_ids<WPL>();
+  double* scl = scan + z.l * 2 * WPL;
+  const double rd = a.g.rd[DIR];
+  for (int k = 0; k < 4; ++k) solve_line<S, WPL>(V + k * tsz + z.l * c.LP + HT, a.opd, z, scl, rd, false);
+  __syncthreads();
+  if (c.svalid) {
+    double* R = a.R + c.sbase;
+#pragma unroll 1
+    for (int k = 0; k < 4; ++k) {
+      double* Rk = R + (1 + k) * fs;
+      const double* Vk = V + k * tsz;
+      c.for_nodes_rmw<4>(0, c.dim, [&](int n) { return Rk[(int64_t)n * c.sd]; },
+                         [&](int o, int n, double r) { Rk[(int64_t)n * c.sd] = r + Vk[o]; });
+    }
+  }
+}
+
+// ------------------------------------------------------------------ pass B' (visc along B, update, filter)
+template <int S, int WPL, int DIR>
+__global__ void __launch_bounds__(512) k_pass_vb(PassArgs a) {
+  extern __shared__ double sm[];
+  const TileCtx<DIR, WPL> c(a);
+  const int tsz = c.TI * c.LP;
+  double* V = sm;
+  double* O = sm + 4 * tsz;
+  double* scan = O + tsz;
+  const int64_t fs = a.g.fs;
+  constexpr int dA = DIR_A, dB = DIR_B;
+  // viscous flux along B for momentum component k (physical) and energy: see pass C's VF layout
+  for (int k = 0; k < 4; ++k) {
+    const int vf = (k == 3) ? 6 : (k == dA ? dB : (k == dB ? 4 : 5));
+    load_tile(c, V + k * tsz, a.VF + vf * fs);
+  }
+  cp_async_wait_all();
+  __syncthreads();
+  const LaneIds z = lane_ids<WPL>();
+  double* scl = scan + z.l * 2 * WPL;
+  const double rd = a.g.rd[DIR];
+  const int dim = c.dim;
+  double* oline = O + z.l * c.LP + HT;
+  for (int m = 0; m < 5; ++m) {
+    if (m >= 1) {
+      const double* line = V + (m - 1) * tsz + z.l * c.LP + HT;
+      double v[S];
+      rhs_deriv<S>(v, a.opd, z.seg, [line](int n) { return line[n]; });
+      seg_solve<S, WPL>(v, a.opd.tab, z.seg, z.lane, z.part, z.l, scl);
+#pragma unroll
+      for (int t = 0; t < S; ++t) v[t] *= rd;
+      put_lane<S>(oline, v, z.seg, a.opd.ext_lo, dim, false);
+    }
+    __syncthreads();
+    double* R = a.R + m * fs + c.sbase;
+    if (a.mode == 0) {
+      if (c.svalid)
+        c.for_nodes_rmw<4>(0, dim, [&](int n) { return R[(int64_t)n * c.sd]; },
+                           [&](int o, int n, double r) { R[(int64_t)n * c.sd] = r + ((m >= 1) ? O[o] : 0.0); });
+      __syncthreads();
+      continue;
+    }
+    // SSP-RK3 stage update, tgvsolver.F90:1055-1057
+    if (c.svalid) {
+      const double* qs = a.qsave + m * fs + c.sbase;
+      const double* qq = a.q + m * fs + c.sbase;
+      const double c1 = a.c1, c2 = a.c2, c3 = a.c3, dt = a.dt;
+      double* sline = O + c.sl * c.LP + HT;
+      c.for_nodes(0, dim, [&](int o, int n) {
+        const int64_t off = (int64_t)n * c.sd;
+        const double vis = (m >= 1) ? O[o] : 0.0;
+        const double r = R[off] + vis;
+        const double qc = (c2 != 0.0) ? c2 * qq[off] : 0.0;
+        const double qn = c1 * qs[off] + qc + c3 * r * dt;
+        O[o] = qn;
+        put_images(sline, n, dim, qn);
+      });
+    }
+    __syncthreads();
+    if (a.do_filter) {
+      solve_line<S, WPL>(oline, a.opf, z, scl, 1.0, false);
+      __syncthreads();
+    }
+    if (c.svalid) {
+      double* qo = a.qout + m * fs + c.sbase;
+      c.for_nodes(0, dim, [&](int o, int n) { qo[(int64_t)n * c.sd] = O[o]; });
+    }
+    __syncthreads();
+  }
+}
+
+// ------------------------------------------------------------------ pass F (filter only, 5 fields)
+template <int S, int WPL, int DIR>
+__global__ void __launch_bounds__(512) k_pass_f(PassArgs a) {
+  extern __shared__ double sm[];
+  const TileCtx<DIR, WPL> c(a);
+  const int tsz = c.TI * c.LP;
+  double* T = sm;
+  double* scan = sm + 5 * tsz;
+  const int64_t fs = a.g.fs;
+  for (int m = 0; m < 5; ++m) load_tile(c, T + m * tsz, a.q + m * fs);
+  cp_async_wait_all();
+  __syncthreads();
+  const LaneIds z = lane_ids<WPL>();
+  double* scl = scan + z.l * 2 * WPL;
+  for (int m = 0; m < 5; ++m) solve_line<S, WPL>(T + m * tsz + z.l * c.LP + HT, a.opf, z, scl, 1.0, false);
+  __syncthreads();
+  if (c.svalid) {
+    double* q = a.q + c.sbase;
+    c.for_nodes(0, c.dim, [&](int o, int n) {
+      const int64_t off = (int64_t)n * c.sd;
+#pragma unroll
+      for (int m = 0; m < 5; ++m) q[m * fs + off] = T[m * tsz + o];
+    });
+  }
+}
+
+}  // namespace pass_detail
+
+using namespace pass_detail;
+
+template <class KernT>
+cudaError_t launch_k(KernT kern, dim3 grid, int threads, size_t smem, cudaStream_t st, const PassArgs& a) {
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  kern<<<grid, threads, smem, st>>>(a);
+  return cudaGetLastError();
+}
+
+template <int S, int WPL>
+cudaError_t launch_pass_t(int pass, const PassArgs& a, cudaStream_t st) {
+  const int o1 = (a.dir == 0) ? 1 : 0, o2 = (a.dir == 2) ? 1 : 2;
+  const int tsz = a.TI * a.LP;
+  const int ntile = pass_tiles(pass);
+  size_t smem = ((size_t)ntile * tsz + (size_t)a.TI * 2 * WPL) * sizeof(double);
+  if (pass == PASS_C) smem += 32 * 3 * sizeof(double);
+  dim3 grid((unsigned)((a.g.N[o1] + 1 + a.TI - 1) / a.TI), (unsigned)(a.g.N[o2] + 1));
+  const int threads = a.TI * WPL * 32;
+  switch (pass) {
+    case PASS_A: return launch_k(k_pass_ab<S, WPL, DIR_A, true>, grid, threads, smem, st, a);
+    case PASS_B: return launch_k(k_pass_ab<S, WPL, DIR_B, false>, grid, threads, smem, st, a);
+    case PASS_C: return launch_k(k_pass_c<S, WPL, DIR_C>, grid, threads, smem, st, a);
+    case PASS_VA: return launch_k(k_pass_va<S, WPL, DIR_A>, grid, threads, smem, st, a);
+    case PASS_VB: return launch_k(k_pass_vb<S, WPL, DIR_B>, grid, threads, smem, st, a);
+    case PASS_F:
+      if (a.dir == DIR_C) return launch_k(k_pass_f<S, WPL, DIR_C>, grid, threads, smem, st, a);
+      if (a.dir == DIR_A) return launch_k(k_pass_f<S, WPL, DIR_A>, grid, threads, smem, st, a);
+      return launch_k(k_pass_f<S, WPL, DIR_B>, grid, threads, smem, st, a);
+    default:
+      return cudaErrorInvalidValue;
+  }
+}
+
+}  // namespace astr

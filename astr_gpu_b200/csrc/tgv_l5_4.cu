@@ -1,0 +1,6 @@
+// Pass kernels for the solve layout S = 5 rows per lane, WPL = 4 warp(s) per line.
+#include "tgv_kernels.cuh"
+
+namespace astr {
+template cudaError_t launch_pass_t<5, 4>(int pass, const PassArgs& a, cudaStream_t st);
+}  // namespace astr

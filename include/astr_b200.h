@@ -120,6 +120,11 @@ int astr_history(astr_state* st, double* rows, int maxrows, int* nrows);
 int astr_diagnostics(astr_state* st, double out[3]);
 /* Capture each RK3 step as one CUDA graph (default on). */
 int astr_state_use_graph(astr_state* st, int on);
+/* Per-pass autotuning of the launch shape (rows per lane, warps per line, lines per CTA) at the
+ * first RK3 step of a state, on scratch copies of the live fields (default on above 100^3 nodes). */
+int astr_state_autotune(astr_state* st, int on);
+/* Launch shape of each pass A, B, C, A', B', filter-C, filter-A as (S, WPL, TI, LP): 28 ints. */
+int astr_state_launch_shapes(astr_state* st, int shapes[28]);
 /* Instrumentation (no counterpart in the reference): run `nsteps` RK3 steps eagerly with CUDA
  * events around every pass launch on the context stream and return the mean device time of
  * one launch of each pass, ms[0..6] = A, B, C, A', B', F(C), diagnostics reduce. */
