@@ -18,6 +18,7 @@ __global__ void __launch_bounds__(1024) k_line_api(LineOp op, int dir, const dou
   extern __shared__ double sm[];
   double* tile = sm;
   double* scan = sm + (size_t)TI * LP;   // 2*WPL per line
+  double* sp = scan + (size_t)TI * 2 * WPL;   // closure rows, 2*NSP per line
   const int o1 = (dir == 0) ? 1 : 0;
   const int o2 = (dir == 2) ? 1 : 2;
   const int64_t l1_0 = oa.lb[o1] + (int64_t)blockIdx.x * TI;
@@ -43,6 +44,18 @@ __global__ void __launch_bounds__(1024) k_line_api(LineOp op, int dir, const dou
     tile[l * LP + nn] = val;
   }
   __syncthreads();
+  if (op.kind != OP_EXPLICIT) {
+    // closure-row RHS values, computed once per line before the solves
+    for (int it = tid; it < TI * 2 * NSP; it += nthr) {
+      const int j = it % (2 * NSP), ll = it / (2 * NSP);
+      const bool lo = j < NSP;
+      if (lo ? (j >= op.spec_lo) : (j - NSP >= op.spec_hi)) continue;
+      const int r = lo ? j : op.nsys - op.spec_hi + (j - NSP);
+      const double* li = tile + ll * LP + HT;
+      sp[it] = special_value(op, r, [li](int n) { return li[n]; });
+    }
+    __syncthreads();
+  }
 
   const int warp = tid >> 5, lane = tid & 31;
   const int l = warp / WPL, part = warp - l * WPL;
@@ -51,10 +64,10 @@ __global__ void __launch_bounds__(1024) k_line_api(LineOp op, int dir, const dou
   auto get = [line](int n) { return line[n]; };
   double v[S];
   if (op.kind == OP_DERIV) {
-    rhs_deriv<S>(v, op, seg, get);
+    rhs_deriv<S>(v, op, seg, get, sp + l * 2 * NSP);
     seg_solve<S, WPL>(v, op.tab, seg, lane, part, l, scan + l * 2 * WPL);
   } else if (op.kind == OP_FILTER) {
-    rhs_filter<S>(v, op, seg, get);
+    rhs_filter<S>(v, op, seg, get, sp + l * 2 * NSP);
     seg_solve<S, WPL>(v, op.tab, seg, lane, part, l, scan + l * 2 * WPL);
   } else {
 #pragma unroll
@@ -94,7 +107,7 @@ static cudaError_t launch_t(const DevOp& op, int dir, const double* f, const Arr
   if (TI > 16) TI = 16;
   if (TI < 1) TI = 1;
   const int LP = tile_pitch(op.op.dim, TI);
-  const size_t smem = ((size_t)TI * LP + (size_t)TI * 2 * WPL) * sizeof(double);
+  const size_t smem = ((size_t)TI * LP + (size_t)TI * (2 * WPL + 2 * NSP)) * sizeof(double);
   auto kern = k_line_api<S, WPL>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;

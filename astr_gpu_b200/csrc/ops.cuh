@@ -16,18 +16,22 @@
 
 namespace astr {
 
-constexpr int HT = 8;             // tile halo nodes kept on each side of a line
+// Tile halo nodes kept on each side of a line. A lane owning the last real row of a system
+// reads a window up to dim + S + 7 (filter, S <= 9); with 16 halo nodes only lanes whose rows are
+// all padding reach past the staged range (window_base).
+constexpr int HT = 16;
 constexpr unsigned FULL = 0xffffffffu;
 
 enum OpKind { OP_DERIV = 0, OP_FILTER = 1, OP_EXPLICIT = 2 };
 
 // One line operator (a compact_scheme of the reference plus the lane tables of its solve).
-// Table layout (doubles), nseg = 32*WPL segments of S rows:
-//   [(f*S + t)*nseg + seg]  f = 0 ac1, 1 ac2, 2 ac3, 3 pf (forward prefix product within the
-//                           segment), 4 qb (backward suffix product within the segment)
-//   then per segment (nseg each): FS[0..4] forward scan composites for shuffle offsets 1..16,
-//   FE forward exclusive product within the warp, BS[0..4], BE (backward), and per warp
-//   MW[WPL], MWB[WPL] (whole-warp products).
+// Table layout (doubles), NS = 32*WPL segments of S rows, row t of segment seg:
+//   [2*(t*NS + seg)]            (ac2, ac3) pair for the forward sweep
+//   [2*S*NS + t*NS + seg]       pf, forward prefix product of -ac3 within the segment
+//   [3*S*NS + 2*(t*NS + seg)]   (ac1, qb) pair for the backward sweep (qb: suffix product of -ac1)
+//   [5*S*NS + k*NS + seg]       per segment: FS[0..4] forward scan composites for shuffle offsets
+//                               1..16, FE forward exclusive product within the warp, BS[0..4], BE
+//   [(5*S + 12)*NS + ...]       per warp: MW[WPL], MWB[WPL] (whole-warp products)
 struct LineOp {
   const double* tab;
   int nsys;            // rows of the system (last_node - first_node + 1)
@@ -38,8 +42,11 @@ struct LineOp {
   int no_filter_note;          // note='boundary_no_filter'
   int nseg;
   int S;
+  int spec_lo, spec_hi;        // closure rows at the start / end of the system (RHS not interior)
   double c10[6], ch[3][11], cb[3][7], c6[4], c8[5];  // filter coefficients (filter.F90:299-432)
 };
+
+constexpr int NSP = 5;   // closure rows kept per end: sp[0..4] start, sp[5..9] end
 
 enum TabOff { T_FS = 0, T_FE = 5, T_BS = 6, T_BE = 11, T_NSEGTAB = 12 };
 
@@ -49,66 +56,107 @@ __device__ __forceinline__ void line_sync(int line) {
   if (WPL > 1) asm volatile("bar.sync %0, %1;" ::"r"(1 + line), "r"(32 * WPL) : "memory");
 }
 
-// Segmented Thomas solve. v holds the RHS rows of this lane on entry and the solution on exit.
-// tab is the operator's lane table laid out for this (S, WPL); all offsets are compile-time.
-// scan_sm: 2*WPL doubles private to this line (used only when WPL > 1). All warps of the line
-// must call it together.
+// Segmented Thomas solve of NV right-hand sides at once (the coefficients are shared, the
+// chains interleave). v[i] holds the RHS rows of this lane on entry and the solution on exit.
+// scan_sm: 2*WPL*NV doubles private to this line (used only when WPL > 1). All warps of the
+// line must call it together.
+template <int S, int WPL, int NV>
+__device__ __forceinline__ void seg_solve_n(double (&v)[NV][S], const double* __restrict__ tab, int seg, int lane,
+                                            int part, int line, double* scan_sm) {
+  constexpr int NS = 32 * WPL;
+  const double2* fwd = reinterpret_cast<const double2*>(tab) + seg;
+  const double* pfp = tab + 2 * S * NS + seg;
+  const double2* bwd = reinterpret_cast<const double2*>(tab + 3 * S * NS) + seg;
+  const double* sg = tab + 5 * S * NS + seg;
+  const double* ws = tab + (5 * S + T_NSEGTAB) * NS;   // per-warp products
+  // forward sweeps from a zero carry
+  double g[NV];
+#pragma unroll
+  for (int i = 0; i < NV; ++i) g[i] = 0.0;
+#pragma unroll
+  for (int t = 0; t < S; ++t) {
+    const double2 c = __ldg(fwd + t * NS);
+#pragma unroll
+    for (int i = 0; i < NV; ++i) {
+      g[i] = v[i][t] * c.x - g[i] * c.y;
+      v[i][t] = g[i];
+    }
+  }
+  // inclusive scans of the segment maps c -> G + M c across the warp (composite M precomputed)
+#pragma unroll
+  for (int k = 0; k < 5; ++k) {
+    const double m = __ldg(sg + (T_FS + k) * NS);
+#pragma unroll
+    for (int i = 0; i < NV; ++i) g[i] = fma(m, __shfl_up_sync(FULL, g[i], 1 << k), g[i]);
+  }
+  double cin[NV];
+  const double fe = __ldg(sg + T_FE * NS);
+  if (WPL > 1) {
+#pragma unroll
+    for (int i = 0; i < NV; ++i)
+      if (lane == 31) scan_sm[i * 2 * WPL + part] = g[i];
+    line_sync<WPL>(line);
+  }
+#pragma unroll
+  for (int i = 0; i < NV; ++i) {
+    double ge = __shfl_up_sync(FULL, g[i], 1);
+    if (lane == 0) ge = 0.0;
+    double cw = 0.0;
+    if (WPL > 1)
+      for (int p = 0; p < part; ++p) cw = fma(__ldg(ws + p), cw, scan_sm[i * 2 * WPL + p]);
+    cin[i] = fma(fe, cw, ge);
+  }
+#pragma unroll
+  for (int t = 0; t < S; ++t) {
+    const double pf = __ldg(pfp + t * NS);
+#pragma unroll
+    for (int i = 0; i < NV; ++i) v[i][t] = fma(pf, cin[i], v[i][t]);
+  }
+
+  // backward sweeps from a zero carry
+  double qb[S];
+#pragma unroll
+  for (int i = 0; i < NV; ++i) g[i] = 0.0;
+#pragma unroll
+  for (int t = S - 1; t >= 0; --t) {
+    const double2 c = __ldg(bwd + t * NS);
+    qb[t] = c.y;
+#pragma unroll
+    for (int i = 0; i < NV; ++i) {
+      g[i] = v[i][t] - c.x * g[i];
+      v[i][t] = g[i];
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < 5; ++k) {
+    const double m = __ldg(sg + (T_BS + k) * NS);
+#pragma unroll
+    for (int i = 0; i < NV; ++i) g[i] = fma(m, __shfl_down_sync(FULL, g[i], 1 << k), g[i]);
+  }
+  const double be = __ldg(sg + T_BE * NS);
+  if (WPL > 1) {
+#pragma unroll
+    for (int i = 0; i < NV; ++i)
+      if (lane == 0) scan_sm[i * 2 * WPL + WPL + part] = g[i];
+    line_sync<WPL>(line);
+  }
+#pragma unroll
+  for (int i = 0; i < NV; ++i) {
+    double ge = __shfl_down_sync(FULL, g[i], 1);
+    if (lane == 31) ge = 0.0;
+    double cw = 0.0;
+    if (WPL > 1)
+      for (int p = WPL - 1; p > part; --p) cw = fma(__ldg(ws + WPL + p), cw, scan_sm[i * 2 * WPL + WPL + p]);
+    const double cb = fma(be, cw, ge);
+#pragma unroll
+    for (int t = 0; t < S; ++t) v[i][t] = fma(qb[t], cb, v[i][t]);
+  }
+}
+
 template <int S, int WPL>
 __device__ __forceinline__ void seg_solve(double (&v)[S], const double* __restrict__ tab, int seg, int lane, int part,
                                           int line, double* scan_sm) {
-  constexpr int NS = 32 * WPL;
-  const double* tb = tab + seg;
-  const double* ws = tab + (5 * S + T_NSEGTAB) * NS;   // per-warp products
-  // forward sweep from a zero carry
-  double g = 0.0;
-#pragma unroll
-  for (int t = 0; t < S; ++t) {
-    g = v[t] * __ldg(tb + (S + t) * NS) - g * __ldg(tb + (2 * S + t) * NS);
-    v[t] = g;
-  }
-  // inclusive scan of the segment maps c -> G + M c across the warp (composite M precomputed)
-  double G = g;
-#pragma unroll
-  for (int k = 0; k < 5; ++k) {
-    const double Go = __shfl_up_sync(FULL, G, 1 << k);
-    G = fma(__ldg(tb + (5 * S + T_FS + k) * NS), Go, G);
-  }
-  double Ge = __shfl_up_sync(FULL, G, 1);
-  if (lane == 0) Ge = 0.0;
-  double cw = 0.0;
-  if (WPL > 1) {
-    if (lane == 31) scan_sm[part] = G;
-    line_sync<WPL>(line);
-    for (int p = 0; p < part; ++p) cw = fma(__ldg(ws + p), cw, scan_sm[p]);
-  }
-  const double cin = fma(__ldg(tb + (5 * S + T_FE) * NS), cw, Ge);
-#pragma unroll
-  for (int t = 0; t < S; ++t) v[t] = fma(__ldg(tb + (3 * S + t) * NS), cin, v[t]);
-
-  // backward sweep from a zero carry
-  double h = 0.0;
-#pragma unroll
-  for (int t = S - 1; t >= 0; --t) {
-    h = v[t] - __ldg(tb + t * NS) * h;
-    v[t] = h;
-  }
-  G = h;
-#pragma unroll
-  for (int k = 0; k < 5; ++k) {
-    const double Go = __shfl_down_sync(FULL, G, 1 << k);
-    G = fma(__ldg(tb + (5 * S + T_BS + k) * NS), Go, G);
-  }
-  Ge = __shfl_down_sync(FULL, G, 1);
-  if (lane == 31) Ge = 0.0;
-  cw = 0.0;
-  if (WPL > 1) {
-    if (lane == 0) scan_sm[WPL + part] = G;
-    line_sync<WPL>(line);
-    for (int p = WPL - 1; p > part; --p) cw = fma(__ldg(ws + WPL + p), cw, scan_sm[WPL + p]);
-  }
-  const double cb = fma(__ldg(tb + (5 * S + T_BE) * NS), cw, Ge);
-#pragma unroll
-  for (int t = 0; t < S; ++t) v[t] = fma(__ldg(tb + (4 * S + t) * NS), cb, v[t]);
+  seg_solve_n<S, WPL, 1>(reinterpret_cast<double(&)[1][S]>(v), tab, seg, lane, part, line, scan_sm);
 }
 
 // ---------------------------------------------------------------- right-hand sides
@@ -140,44 +188,59 @@ __device__ __forceinline__ void stencil_deriv(double (&v)[S], const double (&w)[
 #pragma unroll
   for (int t = 0; t < S; ++t) v[t] = (7.0 / 9.0) * (w[t + 3] - w[t + 1]) + (1.0 / 36.0) * (w[t + 4] - w[t]);
 }
-// Closure rows of the compact derivative and zero padding rows; only lanes that hold them call
-// this (deriv_edge_lane).
-template <int S, class Get>
-__device__ __forceinline__ void fix_deriv_rows(double (&v)[S], const LineOp& op, int r0, Get f) {
-#pragma unroll
-  for (int t = 0; t < S; ++t) {
-    const int r = r0 + t;
-    double s;
-    if (r >= op.nsys) v[t] = 0.0;
-    else if (deriv_special(op, r, f, s)) v[t] = s;
-  }
-}
-template <int S>
-__device__ __forceinline__ bool deriv_edge_lane(const LineOp& op, int r0) { return r0 < 2 || r0 + S > op.nsys - 2; }
 
-// Fill w[t] = f(n0 + t), t < W, clamping to the staged range only for lanes near the ends.
+// First node of a lane's window of W nodes starting at n0. Only lanes holding nothing but
+// padding rows run past the staged range (HT covers the others); they read the last W staged
+// nodes instead (their rows are zeroed), so every lane loads its window without per-node clamps.
+template <int W>
+__device__ __forceinline__ int window_base(int n0, int dim) {
+  return n0 + W - 1 > dim + HT ? dim + HT - W + 1 : n0;
+}
 template <int W, class Get>
 __device__ __forceinline__ void fill_window(double (&w)[W], int n0, int dim, Get f) {
-  if (n0 >= -HT && n0 + W - 1 <= dim + HT) {
+  const int b = window_base<W>(n0, dim);
 #pragma unroll
-    for (int t = 0; t < W; ++t) w[t] = f(n0 + t);
-  } else {
+  for (int t = 0; t < W; ++t) w[t] = f(b + t);
+}
+
+template <class Get>
+__device__ __forceinline__ bool filter_special(const LineOp& op, int r, Get f, double& out);
+
+// RHS value of closure row r (derivative or filter), for the precomputed closure table.
+template <class Get>
+__device__ __forceinline__ double special_value(const LineOp& op, int r, Get f) {
+  double s = 0.0;
+  if (op.kind == OP_FILTER) filter_special(op, r, f, s);
+  else deriv_special(op, r, f, s);
+  return s;
+}
+// Index of row r in the closure table sp, or -1 for an interior row.
+__device__ __forceinline__ int special_slot(const LineOp& op, int r) {
+  if (r < op.spec_lo) return r;
+  if (r >= op.nsys - op.spec_hi) return NSP + r - (op.nsys - op.spec_hi);
+  return -1;
+}
+// Replace the closure rows of this lane by their precomputed values and zero its padding rows.
+template <int S>
+__device__ __forceinline__ void apply_specials(double (&v)[S], const LineOp& op, int r0, const double* sp) {
+  if (r0 < op.spec_lo || r0 + S > op.nsys - op.spec_hi) {
 #pragma unroll
-    for (int t = 0; t < W; ++t) {
-      int n = n0 + t;
-      n = n < -HT ? -HT : (n > dim + HT ? dim + HT : n);
-      w[t] = f(n);
+    for (int t = 0; t < S; ++t) {
+      const int r = r0 + t;
+      const int k = special_slot(op, r);
+      if (r >= op.nsys) v[t] = 0.0;
+      else if (k >= 0) v[t] = sp[k];
     }
   }
 }
 
 template <int S, class Get>
-__device__ __forceinline__ void rhs_deriv(double (&v)[S], const LineOp& op, int seg, Get f) {
+__device__ __forceinline__ void rhs_deriv(double (&v)[S], const LineOp& op, int seg, Get f, const double* sp) {
   const int r0 = seg * S;
   double w[S + 4];
   fill_window<S + 4>(w, r0 - op.ext_lo - 2, op.dim, f);
   stencil_deriv<S>(v, w);
-  if (deriv_edge_lane<S>(op, r0)) fix_deriv_rows<S>(v, op, r0, f);
+  apply_specials<S>(v, op, r0, sp);
 }
 
 // Explicit 6th-order derivative with its closures (diff6ec, derivative.F90:350-413); rows are
@@ -251,9 +314,9 @@ __device__ __forceinline__ bool filter_special(const LineOp& op, int r, Get f, d
   return false;
 }
 
-// Interior 11-point filter RHS (filter.F90:271-283) over a sliding window, then closure rows.
+// Interior 11-point filter RHS (filter.F90:271-283) over a window, then closure rows.
 template <int S, class Get>
-__device__ __forceinline__ void rhs_filter(double (&v)[S], const LineOp& op, int seg, Get f) {
+__device__ __forceinline__ void rhs_filter(double (&v)[S], const LineOp& op, int seg, Get f, const double* sp) {
   const int r0 = seg * S;
   double w[S + 10];
   fill_window<S + 10>(w, r0 - op.ext_lo - 5, op.dim, f);
@@ -268,16 +331,7 @@ __device__ __forceinline__ void rhs_filter(double (&v)[S], const LineOp& op, int
     v[t] = op.c10[0] * var0 + op.c10[1] * var1 + op.c10[2] * var2 + op.c10[3] * var3 + op.c10[4] * var4 +
            op.c10[5] * var5;
   }
-  const int nspec = op.left_phys || op.right_phys ? 5 : 3;
-  if (r0 < nspec || r0 + S > op.nsys - nspec) {
-#pragma unroll
-    for (int t = 0; t < S; ++t) {
-      const int r = r0 + t;
-      double s;
-      if (r >= op.nsys) v[t] = 0.0;
-      else if (filter_special(op, r, f, s)) v[t] = s;
-    }
-  }
+  apply_specials<S>(v, op, r0, sp);
 }
 
 // Periodic node wrap of the reference's halo copy: f(-k) = f(dim-k), f(dim+k) = f(k).

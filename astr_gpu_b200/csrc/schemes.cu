@@ -132,7 +132,17 @@ std::vector<double> lane_tables(const HostOp& op, int S, int nseg) {
   const int WPL = nseg / 32;
   const size_t base = (size_t)5 * S * nseg;
   std::vector<double> t(base + (size_t)T_NSEGTAB * nseg + 2 * (size_t)WPL, 0.0);
-  auto at = [&](int f, int tt, int seg) -> double& { return t[(size_t)(f * S + tt) * nseg + seg]; };
+  // f: 0 ac1, 1 ac2, 2 ac3, 3 pf, 4 qb (see the layout in ops.cuh)
+  auto at = [&](int f, int tt, int seg) -> double& {
+    const size_t rs = (size_t)tt * nseg + seg;
+    switch (f) {
+      case 1: return t[2 * rs];
+      case 2: return t[2 * rs + 1];
+      case 3: return t[(size_t)2 * S * nseg + rs];
+      case 0: return t[(size_t)3 * S * nseg + 2 * rs];
+      default: return t[(size_t)3 * S * nseg + 2 * rs + 1];
+    }
+  };
   auto sg = [&](int k, int seg) -> double& { return t[base + (size_t)k * nseg + seg]; };
   std::vector<double> mf(nseg), mb(nseg);
   for (int seg = 0; seg < nseg; ++seg) {
@@ -212,6 +222,14 @@ cudaError_t make_devop(const HostOp& h, Layout lay, DevOp& out) {
   o.no_filter_note = h.no_note;
   o.nseg = nseg;
   o.S = lay.S;
+  // closure rows with their own RHS formulas (derivative.F90:230-294, filter.F90:176-269)
+  if (h.kind == OP_FILTER) {
+    o.spec_lo = h.left_phys ? 5 : 3;
+    o.spec_hi = h.right_phys ? 5 : 3;
+  } else {
+    o.spec_lo = h.left_phys ? 2 : 1;
+    o.spec_hi = h.right_phys ? 2 : 1;
+  }
   std::memcpy(o.c10, h.c10, sizeof(o.c10));
   std::memcpy(o.ch, h.ch, sizeof(o.ch));
   std::memcpy(o.cb, h.cb, sizeof(o.cb));

@@ -199,35 +199,85 @@ __device__ __forceinline__ LaneIds lane_ids() {
   return z;
 }
 
-// Derivative of pointwise function K along DIR for this lane's rows (scaled by 1/dx).
-template <int S, int WPL, int DIR>
-__device__ __forceinline__ void dsolve(double (&v)[S], int K, const PassArgs& a, const LaneIds& z, const double* L0,
-                                       int tsz, double* scl, double rd) {
-  const LineOp& op = a.opd;
-  const int r0 = z.seg * S;
-  double w[S + 4];
-  prim_window<S + 4, DIR>(w, K, L0, tsz, r0 - op.ext_lo - 2, op.dim, a.th);
-  stencil_deriv<S>(v, w);
-  if (deriv_edge_lane<S>(op, r0)) fix_deriv_rows<S>(v, op, r0, [&](int n) { return gprim_rt<DIR>(K, L0, tsz, n, a.th); });
-  seg_solve<S, WPL>(v, op.tab, z.seg, z.lane, z.part, z.l, scl);
-#pragma unroll
-  for (int t = 0; t < S; ++t) v[t] *= rd;
+constexpr int SCAN_PER_LINE = 4;   // scan scratch per line in units of WPL doubles (NV <= 2)
+constexpr int SP_SOLVES = 13;      // closure tables kept per line (one per pending solve)
+constexpr int SP_PER_LINE = SP_SOLVES * 2 * NSP;
+
+// Closure-row RHS values of `ns` pending solves on every line of the tile, computed up front by
+// a few threads so that no warp diverges on closure rows during its solve:
+// sp[(l*ns + k)*2*NSP + j] for line l, solve k. getk(l, k, n) = input of solve k at node n.
+template <class GetK>
+__device__ __forceinline__ void compute_specials(const LineOp& op, int TI, double* sp, int ns, GetK getk) {
+  const int per = 2 * NSP;
+  for (int it = threadIdx.x; it < TI * ns * per; it += blockDim.x) {
+    const int j = it % per, lk = it / per;
+    const int k = lk % ns, l = lk / ns;
+    const bool lo = j < NSP;
+    if (lo ? (j >= op.spec_lo) : (j - NSP >= op.spec_hi)) continue;
+    const int r = lo ? j : op.nsys - op.spec_hi + (j - NSP);
+    sp[(l * ns + k) * per + j] = special_value(op, r, [&](int n) { return getk(l, k, n); });
+  }
 }
 
-// Solve of a staged tile line (derivative or filter) in place; the filter keeps its physical
-// end values (it never runs with physical closures here: every pass line is periodic).
-template <int S, int WPL>
-__device__ __forceinline__ void solve_line(double* line, const LineOp& op, const LaneIds& z, double* scl, double scale,
-                                           bool images) {
-  double v[S];
-  if (op.kind == OP_FILTER) rhs_filter<S>(v, op, z.seg, [line](int n) { return line[n]; });
-  else rhs_deriv<S>(v, op, z.seg, [line](int n) { return line[n]; });
-  seg_solve<S, WPL>(v, op.tab, z.seg, z.lane, z.part, z.l, scl);
-  if (scale != 1.0) {
+// Derivatives of pointwise functions K0..K0+NV-1 along DIR for this lane's rows, solved together
+// (scaled by 1/dx).
+template <int S, int WPL, int DIR, int NV>
+__device__ __forceinline__ void dsolve_n(double (&v)[NV][S], int K0, const PassArgs& a, const LaneIds& z,
+                                         const double* L0, int tsz, double* scl, double rd, const double* sp) {
+  const LineOp& op = a.opd;
+  const int r0 = z.seg * S;
 #pragma unroll
-    for (int t = 0; t < S; ++t) v[t] *= scale;
+  for (int i = 0; i < NV; ++i) {
+    double w[S + 4];
+    prim_window<S + 4, DIR>(w, K0 + i, L0, tsz, r0 - op.ext_lo - 2, op.dim, a.th);
+    stencil_deriv<S>(v[i], w);
+    apply_specials<S>(v[i], op, r0, sp + i * 2 * NSP);
   }
-  put_lane<S>(line, v, z.seg, op.ext_lo, op.dim, images);
+  seg_solve_n<S, WPL, NV>(v, op.tab, z.seg, z.lane, z.part, z.l, scl);
+#pragma unroll
+  for (int i = 0; i < NV; ++i)
+#pragma unroll
+    for (int t = 0; t < S; ++t) v[i][t] *= rd;
+}
+
+// Solves of NV staged tile lines (derivative or filter) in place, together; `stride` separates
+// the lines of consecutive solves.
+template <int S, int WPL, int NV>
+__device__ __forceinline__ void solve_lines_n(double* line, int stride, const LineOp& op, const LaneIds& z, double* scl,
+                                              double scale, bool images, const double* sp) {
+  double v[NV][S];
+#pragma unroll
+  for (int i = 0; i < NV; ++i) {
+    const double* li = line + i * stride;
+    if (op.kind == OP_FILTER) rhs_filter<S>(v[i], op, z.seg, [li](int n) { return li[n]; }, sp + i * 2 * NSP);
+    else rhs_deriv<S>(v[i], op, z.seg, [li](int n) { return li[n]; }, sp + i * 2 * NSP);
+  }
+  seg_solve_n<S, WPL, NV>(v, op.tab, z.seg, z.lane, z.part, z.l, scl);
+#pragma unroll
+  for (int i = 0; i < NV; ++i) {
+    if (scale != 1.0) {
+#pragma unroll
+      for (int t = 0; t < S; ++t) v[i][t] *= scale;
+    }
+    put_lane<S>(line + i * stride, v[i], z.seg, op.ext_lo, op.dim, images);
+  }
+}
+
+// Solve `count` staged lines spaced by `stride`, one at a time (pairing the solves raised
+// register pressure past the 128-register cap and ran slower).
+// sp: this line's closure tables of the `count` solves (see compute_specials).
+template <int S, int WPL>
+__device__ __forceinline__ void solve_lines(double* line, int stride, int count, const LineOp& op, const LaneIds& z,
+                                            double* scl, double scale, bool images, const double* sp) {
+  for (int i = 0; i < count; ++i)
+    solve_lines_n<S, WPL, 1>(line + i * stride, stride, op, z, scl, scale, images, sp + i * 2 * NSP);
+}
+
+// Closure tables of `count` tile lines spaced by `stride` (line l of solve k at
+// base + k*stride + l*LP + HT).
+__device__ __forceinline__ void tile_specials(const LineOp& op, int TI, int LP, const double* base, int stride, int count,
+                                              double* sp) {
+  compute_specials(op, TI, sp, count, [&](int l, int k, int n) { return base[k * stride + l * LP + HT + n]; });
 }
 
 // ------------------------------------------------------------------ pass A and pass B
@@ -239,16 +289,19 @@ __global__ void __launch_bounds__(512) k_pass_ab(PassArgs a) {
   double* T = sm;
   double* O = sm + 5 * tsz;
   double* scan = O + tsz;
+  double* spb = scan + c.TI * SCAN_PER_LINE * WPL;   // closure tables
   const int64_t fs = a.g.fs;
   for (int m = 0; m < 5; ++m) load_tile(c, T + m * tsz, a.q + m * fs);
   cp_async_wait_all();
   __syncthreads();
   const LaneIds z = lane_ids<WPL>();
-  double* scl = scan + z.l * 2 * WPL;
+  double* scl = scan + z.l * SCAN_PER_LINE * WPL;
   const int dim = c.dim;
 
   if (IS_A && a.do_filter) {
-    for (int m = 0; m < 5; ++m) solve_line<S, WPL>(T + m * tsz + z.l * c.LP + HT, a.opf, z, scl, 1.0, true);
+    tile_specials(a.opf, c.TI, c.LP, T, tsz, 5, spb);
+    __syncthreads();
+    solve_lines<S, WPL>(T + z.l * c.LP + HT, tsz, 5, a.opf, z, scl, 1.0, true, spb + z.l * 5 * 2 * NSP);
     __syncthreads();
     if (c.svalid) {
       double* q = a.q + c.sbase;
@@ -262,13 +315,14 @@ __global__ void __launch_bounds__(512) k_pass_ab(PassArgs a) {
   }
   to_prims(c, T, tsz, a.th);
   __syncthreads();
+  compute_specials(a.opd, c.TI, spb, 9, [&](int l, int k, int n) { return gprim_rt<DIR>(k, T + l * c.LP + HT, tsz, n, a.th); });
+  __syncthreads();
 
   const double rd = a.g.rd[DIR];
   const double* L0 = T + z.l * c.LP + HT;
   double* oline = O + z.l * c.LP + HT;
-  for (int K = 0; K < 9; ++K) {
-    double v[S];
-    dsolve<S, WPL, DIR>(v, K, a, z, L0, tsz, scl, rd);
+  // stage one output in O and store it with the pass's epilogue
+  auto emit = [&](const double (&v)[S], int K) {
     put_lane<S>(oline, v, z.seg, a.opd.ext_lo, dim, false);
     __syncthreads();
     if (c.svalid) {
@@ -279,6 +333,11 @@ __global__ void __launch_bounds__(512) k_pass_ab(PassArgs a) {
                               [&](int o, int n, double r) { dst[(int64_t)n * c.sd] = r - O[o]; });
     }
     __syncthreads();
+  };
+  for (int K = 0; K < 9; ++K) {
+    double v[1][S];
+    dsolve_n<S, WPL, DIR, 1>(v, K, a, z, L0, tsz, scl, rd, spb + (z.l * 9 + K) * 2 * NSP);
+    emit(v[0], K);
   }
 }
 
@@ -292,7 +351,9 @@ __global__ void __launch_bounds__(512) k_pass_c(PassArgs a) {
   double* Dt = sm + 5 * tsz;
   double* O = Dt + 4 * tsz;
   double* scan = O + tsz;
-  double* red = scan + c.TI * 2 * WPL;
+  double* spb = scan + c.TI * SCAN_PER_LINE * WPL;   // closure tables: 9 convective/gradient + 4 viscous
+  double* spv = spb + c.TI * 9 * 2 * NSP;
+  double* red = spb + c.TI * SP_PER_LINE;
   const int64_t fs = a.g.fs;
   for (int m = 0; m < 5; ++m) load_tile(c, T + m * tsz, a.q + m * fs);
   cp_async_wait_all();
@@ -300,16 +361,18 @@ __global__ void __launch_bounds__(512) k_pass_c(PassArgs a) {
   const int dim = c.dim;
   to_prims(c, T, tsz, a.th);
   __syncthreads();
+  compute_specials(a.opd, c.TI, spb, 9, [&](int l, int k, int n) { return gprim_rt<DIR>(k, T + l * c.LP + HT, tsz, n, a.th); });
+  __syncthreads();
   const LaneIds z = lane_ids<WPL>();
-  double* scl = scan + z.l * 2 * WPL;
+  double* scl = scan + z.l * SCAN_PER_LINE * WPL;
   const double rd = a.g.rd[DIR];
   const double* L0 = T + z.l * c.LP + HT;
 
   // gradients along C
   for (int K = 0; K < 4; ++K) {
-    double v[S];
-    dsolve<S, WPL, DIR>(v, K, a, z, L0, tsz, scl, rd);
-    put_lane<S>(Dt + K * tsz + z.l * c.LP + HT, v, z.seg, a.opd.ext_lo, dim, false);
+    double v[1][S];
+    dsolve_n<S, WPL, DIR, 1>(v, K, a, z, L0, tsz, scl, rd, spb + (z.l * 9 + K) * 2 * NSP);
+    put_lane<S>(Dt + K * tsz + z.l * c.LP + HT, v[0], z.seg, a.opd.ext_lo, dim, false);
   }
   __syncthreads();
 
@@ -405,15 +468,14 @@ __global__ void __launch_bounds__(512) k_pass_c(PassArgs a) {
   }
 
   // viscous divergence along C (diffusion, tgvsolver.F90:763-787), kept in Dt
-  for (int k = 0; k < 4; ++k) solve_line<S, WPL>(Dt + k * tsz + z.l * c.LP + HT, a.opd, z, scl, rd, false);
+  tile_specials(a.opd, c.TI, c.LP, Dt, tsz, 4, spv);
+  __syncthreads();
+  solve_lines<S, WPL>(Dt + z.l * c.LP + HT, tsz, 4, a.opd, z, scl, rd, false, spv + z.l * 4 * 2 * NSP);
   // convection along C; R += visc_C - conv_C
   double* oline = O + z.l * c.LP + HT;
-  for (int K = 4; K < 9; ++K) {
-    double v[S];
-    dsolve<S, WPL, DIR>(v, K, a, z, L0, tsz, scl, rd);
+  auto emit = [&](const double (&v)[S], int m) {
     put_lane<S>(oline, v, z.seg, a.opd.ext_lo, dim, false);
     __syncthreads();
-    const int m = K - 4;
     if (c.svalid) {
       double* dst = a.R + m * fs + c.sbase;
       if (m == 0) {
@@ -426,6 +488,11 @@ __global__ void __launch_bounds__(512) k_pass_c(PassArgs a) {
       }
     }
     __syncthreads();
+  };
+  for (int K = 4; K < 9; ++K) {
+    double v[1][S];
+    dsolve_n<S, WPL, DIR, 1>(v, K, a, z, L0, tsz, scl, rd, spb + (z.l * 9 + K) * 2 * NSP);
+    emit(v[0], K - 4);
   }
 }
 
@@ -437,14 +504,17 @@ __global__ void __launch_bounds__(512) k_pass_va(PassArgs a) {
   const int tsz = c.TI * c.LP;
   double* V = sm;
   double* scan = sm + 4 * tsz;
+  double* spb = scan + c.TI * SCAN_PER_LINE * WPL;
   const int64_t fs = a.g.fs;
   for (int k = 0; k < 4; ++k) load_tile(c, V + k * tsz, a.VF + k * fs);
   cp_async_wait_all();
   __syncthreads();
+  tile_specials(a.opd, c.TI, c.LP, V, tsz, 4, spb);
+  __syncthreads();
   const LaneIds z = lane_ids<WPL>();
-  double* scl = scan + z.l * 2 * WPL;
+  double* scl = scan + z.l * SCAN_PER_LINE * WPL;
   const double rd = a.g.rd[DIR];
-  for (int k = 0; k < 4; ++k) solve_line<S, WPL>(V + k * tsz + z.l * c.LP + HT, a.opd, z, scl, rd, false);
+  solve_lines<S, WPL>(V + z.l * c.LP + HT, tsz, 4, a.opd, z, scl, rd, false, spb + z.l * 4 * 2 * NSP);
   __syncthreads();
   if (c.svalid) {
     double* R = a.R + c.sbase;
@@ -467,6 +537,8 @@ __global__ void __launch_bounds__(512) k_pass_vb(PassArgs a) {
   double* V = sm;
   double* O = sm + 4 * tsz;
   double* scan = O + tsz;
+  double* spb = scan + c.TI * SCAN_PER_LINE * WPL;   // closure tables: 4 viscous + 1 filter
+  double* spf = spb + c.TI * 4 * 2 * NSP;
   const int64_t fs = a.g.fs;
   constexpr int dA = DIR_A, dB = DIR_B;
   // viscous flux along B for momentum component k (physical) and energy: see pass C's VF layout
@@ -476,8 +548,10 @@ __global__ void __launch_bounds__(512) k_pass_vb(PassArgs a) {
   }
   cp_async_wait_all();
   __syncthreads();
+  tile_specials(a.opd, c.TI, c.LP, V, tsz, 4, spb);
+  __syncthreads();
   const LaneIds z = lane_ids<WPL>();
-  double* scl = scan + z.l * 2 * WPL;
+  double* scl = scan + z.l * SCAN_PER_LINE * WPL;
   const double rd = a.g.rd[DIR];
   const int dim = c.dim;
   double* oline = O + z.l * c.LP + HT;
@@ -485,7 +559,7 @@ __global__ void __launch_bounds__(512) k_pass_vb(PassArgs a) {
     if (m >= 1) {
       const double* line = V + (m - 1) * tsz + z.l * c.LP + HT;
       double v[S];
-      rhs_deriv<S>(v, a.opd, z.seg, [line](int n) { return line[n]; });
+      rhs_deriv<S>(v, a.opd, z.seg, [line](int n) { return line[n]; }, spb + (z.l * 4 + m - 1) * 2 * NSP);
       seg_solve<S, WPL>(v, a.opd.tab, z.seg, z.lane, z.part, z.l, scl);
 #pragma unroll
       for (int t = 0; t < S; ++t) v[t] *= rd;
@@ -518,7 +592,9 @@ __global__ void __launch_bounds__(512) k_pass_vb(PassArgs a) {
     }
     __syncthreads();
     if (a.do_filter) {
-      solve_line<S, WPL>(oline, a.opf, z, scl, 1.0, false);
+      tile_specials(a.opf, c.TI, c.LP, O, 0, 1, spf);
+      __syncthreads();
+      solve_lines<S, WPL>(oline, 0, 1, a.opf, z, scl, 1.0, false, spf + z.l * 2 * NSP);
       __syncthreads();
     }
     if (c.svalid) {
@@ -537,13 +613,16 @@ __global__ void __launch_bounds__(512) k_pass_f(PassArgs a) {
   const int tsz = c.TI * c.LP;
   double* T = sm;
   double* scan = sm + 5 * tsz;
+  double* spb = scan + c.TI * SCAN_PER_LINE * WPL;
   const int64_t fs = a.g.fs;
   for (int m = 0; m < 5; ++m) load_tile(c, T + m * tsz, a.q + m * fs);
   cp_async_wait_all();
   __syncthreads();
+  tile_specials(a.opf, c.TI, c.LP, T, tsz, 5, spb);
+  __syncthreads();
   const LaneIds z = lane_ids<WPL>();
-  double* scl = scan + z.l * 2 * WPL;
-  for (int m = 0; m < 5; ++m) solve_line<S, WPL>(T + m * tsz + z.l * c.LP + HT, a.opf, z, scl, 1.0, false);
+  double* scl = scan + z.l * SCAN_PER_LINE * WPL;
+  solve_lines<S, WPL>(T + z.l * c.LP + HT, tsz, 5, a.opf, z, scl, 1.0, false, spb + z.l * 5 * 2 * NSP);
   __syncthreads();
   if (c.svalid) {
     double* q = a.q + c.sbase;
@@ -572,7 +651,7 @@ cudaError_t launch_pass_t(int pass, const PassArgs& a, cudaStream_t st) {
   const int o1 = (a.dir == 0) ? 1 : 0, o2 = (a.dir == 2) ? 1 : 2;
   const int tsz = a.TI * a.LP;
   const int ntile = pass_tiles(pass);
-  size_t smem = ((size_t)ntile * tsz + (size_t)a.TI * 2 * WPL) * sizeof(double);
+  size_t smem = ((size_t)ntile * tsz + (size_t)a.TI * (SCAN_PER_LINE * WPL + SP_PER_LINE)) * sizeof(double);
   if (pass == PASS_C) smem += 32 * 3 * sizeof(double);
   dim3 grid((unsigned)((a.g.N[o1] + 1 + a.TI - 1) / a.TI), (unsigned)(a.g.N[o2] + 1));
   const int threads = a.TI * WPL * 32;
