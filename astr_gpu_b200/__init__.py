@@ -272,6 +272,11 @@ class TGVSolver:
         """Per-pass launch-shape autotuning at the first RK3 step (default on above 100^3)."""
         self.ctx.check(self.ctx.L.astr_state_autotune(self._h, int(on)))
 
+    def set_launch_shape(self, pass_name: str, S: int, WPL: int, TI: int):
+        """Pin one pass's launch shape (disables autotuning)."""
+        names = ["A", "B", "C", "A'", "B'", "F_C", "F_A"]
+        self.ctx.check(self.ctx.L.astr_state_set_launch_shape(self._h, names.index(pass_name), S, WPL, TI))
+
     def launch_shapes(self) -> dict:
         """{pass: (rows per lane, warps per line, lines per CTA, tile pitch)}."""
         buf = (ctypes.c_int * 28)()

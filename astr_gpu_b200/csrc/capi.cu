@@ -669,6 +669,23 @@ int astr_state_launch_shapes(astr_state* st, int shapes[28]) {
   return ASTR_OK;
 }
 
+int astr_state_set_launch_shape(astr_state* st, int pass, int S, int WPL, int TI) {
+  if (!st || pass < 0 || pass >= NCFG) return ASTR_ERR_ARG;
+  astr_ctx* ctx = st->ctx;
+  bool known = false;
+  for (const Layout& L : kLayouts) known |= (L.S == S && L.WPL == WPL);
+  const int dir = CFG_DIR[pass];
+  if (!known || 32 * WPL * S < st->hf[dir].nsys()) return fail(ctx, ASTR_ERR_ARG, "layout not compiled or too short");
+  if (TI < 1 || (TI & (TI - 1)) || TI * WPL * 32 > 1024 || (WPL > 1 && TI > 15))
+    return fail(ctx, ASTR_ERR_ARG, "TI must be a power of 2 with TI*WPL*32 <= 1024");
+  PassCfg c;
+  c.S = S; c.WPL = WPL; c.TI = TI; c.LP = tile_pitch(st->g.N[dir], TI);
+  st->cfg[pass] = c;
+  st->autotune = false;
+  drop_graphs(st);
+  return ASTR_OK;
+}
+
 int astr_state_use_graph(astr_state* st, int on) {
   if (!st) return ASTR_ERR_ARG;
   st->use_graph = on != 0;

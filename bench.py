@@ -184,10 +184,9 @@ def run_ours(args, ws, rank, local):
     alg_bytes = PASS_FIELDS[dom] * 8.0 * pts
     achieved = alg_bytes / (per[di] * 1e-3) / 1e9
     traffic = None
-    tf = os.path.join(ROOT, "profiles", "traffic.json")
+    tf = os.path.join(ROOT, "profiles", "dram_traffic.json")
     if os.path.exists(tf):
-        tr = json.load(open(tf)).get(str(n), {}).get(dom)
-        traffic = tr
+        traffic = json.load(open(tf)).get(str(n), {}).get(dom)
     roof = {"kernel": f"pass {dom}", "bound": "hbm", "achieved": achieved, "peak": pk, "unit": "GB/s",
             "frac": achieved / pk, "traffic": traffic, "peak_kind": pk_kind,
             "alg_bytes_per_launch": alg_bytes, "ms_per_launch": float(per[di]),

@@ -125,6 +125,9 @@ int astr_state_use_graph(astr_state* st, int on);
 int astr_state_autotune(astr_state* st, int on);
 /* Launch shape of each pass A, B, C, A', B', filter-C, filter-A as (S, WPL, TI, LP): 28 ints. */
 int astr_state_launch_shapes(astr_state* st, int shapes[28]);
+/* Pin pass `pass` (0..6 in the order above) to S rows per lane, WPL warps per line and TI lines
+ * per CTA (a compiled layout whose 32*WPL*S rows cover the pass's line systems; TI a power of 2). */
+int astr_state_set_launch_shape(astr_state* st, int pass, int S, int WPL, int TI);
 /* Instrumentation (no counterpart in the reference): run `nsteps` RK3 steps eagerly with CUDA
  * events around every pass launch on the context stream and return the mean device time of
  * one launch of each pass, ms[0..6] = A, B, C, A', B', F(C), diagnostics reduce. */
