@@ -385,6 +385,10 @@ void drop_graphs(astr_state* st) {
 
 }  // namespace
 
+// Used by noalloc.cu.
+cudaStream_t astr_ctx_stream(astr_ctx* ctx) { return ctx->stream; }
+void astr_ctx_set_error(astr_ctx* ctx, const char* msg) { ctx->err = msg; }
+
 extern "C" {
 
 int astr_init(int device, astr_ctx** out) {

@@ -133,6 +133,20 @@ int astr_state_set_launch_shape(astr_state* st, int pass, int S, int WPL, int TI
  * one launch of each pass, ms[0..6] = A, B, C, A', B', F(C), diagnostics reduce. */
 int astr_pass_timings(astr_state* st, double dt, int nsteps, double ms[7]);
 
+/* ---- no-allocation variant -------------------------------------------------------- */
+/* dt such that cflcal's CFL equals `cfl` for the conserved variables q (a DEVICE array,
+ * Fortran order q(lb.., 1:5) covering nodes 0..im x 0..jm x 0..km of a periodic box of side
+ * 2*pi), like astr_cfl_dt but for callers that cannot let the library allocate device memory
+ * (codes that run inside a fixed device pool or a capped allocator, where cudaMalloc fails or
+ * synchronises the device mid-step). It has no counterpart in the reference.
+ * It allocates nothing: its scratch is a 1.5 MB static device array that every GPU loading the
+ * library holds until exit, which caps (jm+1)*(km+1) at 524288 (ASTR_ERR_UNSUPPORTED beyond).
+ * The first call on a device looks the array up on that device (make it before any stream
+ * capture). All calls share the array: calls that overlap on the GPU race. ctx may be NULL
+ * (default stream, no message); otherwise its stream is used and errors set its message. */
+int astr_cfl_dt_noalloc(astr_ctx* ctx, const double* q, const int64_t shape[3], const int64_t lbound[3],
+                        int im, int jm, int km, double mach, double gamma, double cfl, double* dt);
+
 #ifdef __cplusplus
 }
 #endif
