@@ -283,3 +283,33 @@ class TGVSolver:
         self.ctx.check(self.ctx.L.astr_state_launch_shapes(self._h, buf))
         names = ["A", "B", "C", "A'", "B'", "F_C", "F_A"]
         return {nm: tuple(buf[4 * i:4 * i + 4]) for i, nm in enumerate(names)}
+
+
+class Ensemble:
+    """Independent periodic boxes (``TGVSolver`` objects of one context, sizes may differ)
+    advanced together: each pass of an RK3 stage is one launch over every box sharing a solve
+    layout, and each step is one CUDA graph. Per-box results equal ``TGVSolver.rk3``."""
+
+    def __init__(self, ctx: Context, boxes: list[TGVSolver]):
+        self.ctx = ctx
+        self.boxes = list(boxes)
+        arr = (ctypes.c_void_p * len(self.boxes))(*[b._h.value for b in self.boxes])
+        h = ctypes.c_void_p()
+        ctx.check(ctx.L.astr_ensemble_create(ctx._h, arr, len(self.boxes), ctypes.byref(h)))
+        self._h = h
+
+    def step(self, dt, nsteps: int = 1):
+        """``nsteps`` RK3 steps of every box; ``dt`` is one time step per box (or one for all)."""
+        d = np.broadcast_to(np.asarray(dt, dtype=np.float64), (len(self.boxes),)).copy()
+        self.ctx.check(self.ctx.L.astr_ensemble_step(self._h, d.ctypes.data_as(_lib._dp), nsteps))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self.ctx.L.astr_ensemble_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

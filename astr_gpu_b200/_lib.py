@@ -57,6 +57,9 @@ SIGNATURES = {
     "astr_state_autotune": (_i, [_vp, _i]),
     "astr_state_launch_shapes": (_i, [_vp, _ip]),
     "astr_state_set_launch_shape": (_i, [_vp, _i, _i, _i, _i]),
+    "astr_ensemble_create": (_i, [_vp, _pvp, _i, _pvp]),
+    "astr_ensemble_destroy": (_i, [_vp]),
+    "astr_ensemble_step": (_i, [_vp, _dp, _i]),
     "astr_cfl_dt_noalloc": (_i, [_vp, _vp, _i64p, _i64p, _i, _i, _i, _d, _d, _d, _dp]),
 }
 

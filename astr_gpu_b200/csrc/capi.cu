@@ -7,6 +7,7 @@
 #include <map>
 #include <new>
 #include <string>
+#include <array>
 #include <vector>
 
 #include "../../include/astr_b200.h"
@@ -59,6 +60,32 @@ struct astr_state {
   bool use_graph = true;
   cudaGraphExec_t gexec[2] = {nullptr, nullptr};
   double gdt[2] = {0.0, 0.0};
+};
+
+// One launch of the batched step: a pass over the boxes of one solve layout, or the batched
+// diagnostics reduce (pass == 0).
+struct EnsLaunch {
+  int pass = 0, dir = 0, S = 0, WPL = 0, nbox = 0, nctas = 0, threads = 0;
+  size_t smem = 0, args_off = 0, cum_off = 0;
+};
+
+struct astr_ensemble {
+  astr_ctx* ctx = nullptr;
+  std::vector<astr_state*> boxes;
+  struct Group {
+    int S = 0, WPL = 0;
+    std::vector<int> members;
+    int TI[NCFG] = {0};
+  };
+  std::vector<Group> groups;
+  PassArgs* dargs = nullptr;
+  int* dcum = nullptr;
+  DiagArgs* ddiag = nullptr;
+  std::vector<EnsLaunch> plan[2];   // per variant: filter along A owed at the start of the step or not
+  std::vector<double> dt;
+  cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+  bool pending = false;
+  bool tuned = false;
 };
 
 namespace {
@@ -828,6 +855,233 @@ int astr_diagnostics(astr_state* st, double out[3]) {
   cudaFree(cnt);
   cudaFree(h);
   return check_err(st);
+}
+
+}  // extern "C"
+
+// ====================================================================== batched ensemble
+// Many independent periodic boxes of uneven sizes advanced together: boxes are grouped by the
+// solve layout their size selects, and every pass of a stage is one launch per group whose
+// CTAs walk the concatenated tile grids of the group's boxes (launch_pass_batch); the stage's
+// diagnostics reduce is one launch for all boxes. Each ensemble step is one CUDA graph.
+namespace {
+
+void ens_drop_graphs(astr_ensemble* e) {
+  for (auto& g : e->gexec)
+    if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+}
+
+void ens_free_plan(astr_ensemble* e) {
+  if (e->dargs) cudaFree(e->dargs);
+  if (e->dcum) cudaFree(e->dcum);
+  if (e->ddiag) cudaFree(e->ddiag);
+  e->dargs = nullptr; e->dcum = nullptr; e->ddiag = nullptr;
+}
+
+// Build the launch plans of both variants for the current dt and upload their arguments.
+int ens_build(astr_ensemble* e) {
+  astr_ctx* ctx = e->ctx;
+  static const double rk[3][3] = {{1.0, 0.0, 1.0}, {0.75, 0.25, 0.25}, {1.0 / 3.0, 2.0 / 3.0, 2.0 / 3.0}};
+  std::vector<PassArgs> hargs;
+  std::vector<int> hcum;
+  std::vector<DiagArgs> hdiag;
+  for (astr_state* st : e->boxes) {
+    DiagArgs d;
+    d.partials = st->partials; d.nparts = 0; d.hist = st->hist; d.counter = st->counter;
+    d.norm = (double)st->p.im * (double)st->p.jm * (double)st->p.km;
+    hdiag.push_back(d);
+  }
+  const int slots[6] = {CFG_A, CFG_B, CFG_C, CFG_VA, CFG_VB, CFG_FC};
+  // base_args reads a box's launch configuration: lend it the group's for the build only.
+  std::vector<std::array<PassCfg, NCFG>> saved(e->boxes.size());
+  for (size_t b = 0; b < e->boxes.size(); ++b)
+    for (int id = 0; id < NCFG; ++id) saved[b][id] = e->boxes[b]->cfg[id];
+  for (int variant = 0; variant < 2; ++variant) {
+    e->plan[variant].clear();
+    for (int s = 0; s < 3; ++s) {
+      for (int si = 0; si < 6; ++si) {
+        const int id = slots[si];
+        for (auto& g : e->groups) {
+          EnsLaunch L;
+          L.pass = CFG_PASS[id]; L.dir = CFG_DIR[id]; L.S = g.S; L.WPL = g.WPL;
+          L.nbox = (int)g.members.size();
+          L.threads = g.TI[id] * g.WPL * 32;
+          L.args_off = hargs.size();
+          L.cum_off = hcum.size();
+          int ctas = 0;
+          for (int b : g.members) {
+            astr_state* st = e->boxes[b];
+            const int dir = CFG_DIR[id];
+            PassCfg c;
+            c.S = g.S; c.WPL = g.WPL; c.TI = g.TI[id]; c.LP = tile_pitch(st->g.N[dir], c.TI);
+            st->cfg[id] = c;
+            PassArgs a = base_args(st, id);
+            double* qin = (s == 0) ? st->Q0 : st->Q1;
+            double* qout = (s == 2) ? st->Q0 : st->Q1;
+            const int filt = st->p.filter_on;
+            switch (id) {
+              case CFG_A: a.q = qin; a.D = st->DA; a.do_filter = filt && (s > 0 || variant == 1); break;
+              case CFG_B: a.q = qin; a.D = st->DB; break;
+              case CFG_C: a.q = qin; a.DA = st->DA; a.DB = st->DB; a.partials = (s == 0) ? st->partials : nullptr; break;
+              case CFG_VB:
+                a.q = qin; a.qsave = st->Q0; a.qout = qout; a.mode = 1; a.do_filter = filt;
+                a.c1 = rk[s][0]; a.c2 = rk[s][1]; a.c3 = rk[s][2]; a.dt = e->dt[b];
+                break;
+              case CFG_FC: a.q = qout; break;
+              default: break;
+            }
+            hargs.push_back(a);
+            hcum.push_back(ctas);
+            const int o1 = (dir == 0) ? 1 : 0, o2 = (dir == 2) ? 1 : 2;
+            ctas += ((st->g.N[o1] + 1 + c.TI - 1) / c.TI) * (st->g.N[o2] + 1);
+            L.smem = std::max(L.smem, pass_shared_bytes(L.pass, c.TI, c.LP, g.WPL));
+            if (id == CFG_C) hdiag[b].nparts = diag_parts(st);
+          }
+          L.nctas = ctas;
+          if (id == CFG_FC && !e->boxes[0]->p.filter_on) continue;
+          e->plan[variant].push_back(L);
+        }
+        if (s == 0 && id == CFG_C) {   // the stage-1 diagnostics of every box
+          EnsLaunch L;
+          L.pass = 0; L.nbox = (int)e->boxes.size();
+          e->plan[variant].push_back(L);
+        }
+      }
+    }
+  }
+  for (size_t b = 0; b < e->boxes.size(); ++b)
+    for (int id = 0; id < NCFG; ++id) e->boxes[b]->cfg[id] = saved[b][id];
+  ens_free_plan(e);
+  CK(cudaMalloc(&e->dargs, hargs.size() * sizeof(PassArgs)));
+  CK(cudaMalloc(&e->dcum, hcum.size() * sizeof(int)));
+  CK(cudaMalloc(&e->ddiag, hdiag.size() * sizeof(DiagArgs)));
+  CK(cudaMemcpy(e->dargs, hargs.data(), hargs.size() * sizeof(PassArgs), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(e->dcum, hcum.data(), hcum.size() * sizeof(int), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(e->ddiag, hdiag.data(), hdiag.size() * sizeof(DiagArgs), cudaMemcpyHostToDevice));
+  return ASTR_OK;
+}
+
+cudaError_t ens_run(astr_ensemble* e, int variant) {
+  cudaStream_t sm = e->ctx->stream;
+  for (const EnsLaunch& L : e->plan[variant]) {
+    cudaError_t err;
+    if (L.pass == 0) err = launch_diag_reduce_batch(e->ddiag, L.nbox, sm);
+    else err = launch_pass_batch(L.pass, L.dir, L.S, L.WPL, e->dargs + L.args_off, e->dcum + L.cum_off, L.nbox, L.nctas,
+                                 L.threads, L.smem, sm);
+    if (err != cudaSuccess) return err;
+  }
+  return cudaSuccess;
+}
+
+// Lines per CTA of each pass of each group: the largest power of two (<= 512 threads) whose
+// tiles fit in ~110 KB for every box of the group, then timed against half and double.
+int ens_tune(astr_ensemble* e) {
+  astr_ctx* ctx = e->ctx;
+  for (auto& g : e->groups) {
+    for (int id = 0; id < NCFG; ++id) {
+      int ti = 16;
+      for (int b : g.members) ti = std::min(ti, pick_ti(CFG_PASS[id], e->boxes[b]->g.N[CFG_DIR[id]], g.WPL));
+      g.TI[id] = std::max(ti, 1);
+    }
+  }
+  return ASTR_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int astr_ensemble_create(astr_ctx* ctx, astr_state* const* boxes, int nbox, astr_ensemble** out) {
+  if (!ctx || !boxes || nbox < 1 || !out) return fail(ctx, ASTR_ERR_ARG, "null argument or empty ensemble");
+  astr_ensemble* e = new astr_ensemble();
+  e->ctx = ctx;
+  for (int b = 0; b < nbox; ++b) {
+    if (!boxes[b] || boxes[b]->ctx != ctx) { delete e; return fail(ctx, ASTR_ERR_ARG, "every box must belong to ctx"); }
+    if (boxes[b]->p.filter_on != boxes[0]->p.filter_on) { delete e; return fail(ctx, ASTR_ERR_ARG, "mixed filter_on"); }
+    e->boxes.push_back(boxes[b]);
+  }
+  for (int b = 0; b < nbox; ++b) {
+    astr_state* st = boxes[b];
+    int mx = 0;
+    for (int d = 0; d < 3; ++d) mx = std::max(mx, st->hf[d].nsys());
+    const Layout L = pick_layout(mx);
+    bool found = false;
+    for (auto& g : e->groups)
+      if (g.S == L.S && g.WPL == L.WPL) { g.members.push_back(b); found = true; }
+    if (!found) {
+      astr_ensemble::Group g;
+      g.S = L.S; g.WPL = L.WPL;
+      g.members.push_back(b);
+      e->groups.push_back(g);
+    }
+  }
+  ens_tune(e);
+  *out = e;
+  return ASTR_OK;
+}
+
+int astr_ensemble_destroy(astr_ensemble* e) {
+  if (!e) return ASTR_ERR_ARG;
+  ens_drop_graphs(e);
+  ens_free_plan(e);
+  delete e;
+  return ASTR_OK;
+}
+
+int astr_ensemble_step(astr_ensemble* e, const double* dt, int nsteps) {
+  if (!e || !dt || nsteps < 0) return ASTR_ERR_ARG;
+  astr_ctx* ctx = e->ctx;
+  const int nbox = (int)e->boxes.size();
+  for (int b = 0; b < nbox; ++b) {
+    if (!(dt[b] > 0.0)) return fail(ctx, ASTR_ERR_ARG, "dt must be positive");
+    if (e->boxes[b]->nstep + nsteps > e->boxes[b]->hist_cap) return fail(ctx, ASTR_ERR_UNSUPPORTED, "history buffer full");
+  }
+  bool changed = e->dt.size() != (size_t)nbox;
+  for (int b = 0; b < nbox && !changed; ++b) changed = e->dt[b] != dt[b];
+  // The filter along A still owed by each box's last stage is applied by the first pass of
+  // the step when every box owes it; otherwise the boxes that owe it apply it now.
+  bool all_pending = true;
+  for (int b = 0; b < nbox; ++b) all_pending = all_pending && e->boxes[b]->pending;
+  if (!all_pending)
+    for (int b = 0; b < nbox; ++b) CK(finalize_filter(e->boxes[b]));
+  e->pending = all_pending;
+  if (changed) {
+    e->dt.assign(dt, dt + nbox);
+    ens_drop_graphs(e);
+    int rc = ens_build(e);
+    if (rc) return rc;
+  }
+  for (int s = 0; s < nsteps; ++s) {
+    const int variant = e->pending ? 1 : 0;
+    for (int b = 0; b < nbox; ++b) {
+      astr_state* st = e->boxes[b];
+      st->row_key.push_back((double)st->nstep);
+      st->row_key.push_back(st->time);
+    }
+    if (!e->gexec[variant]) {
+      cudaGraph_t graph;
+      CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeRelaxed));
+      cudaError_t err = ens_run(e, variant);
+      cudaError_t err2 = cudaStreamEndCapture(ctx->stream, &graph);
+      if (err != cudaSuccess) return cuda_fail(ctx, err, "ensemble step capture");
+      if (err2 != cudaSuccess) return cuda_fail(ctx, err2, "cudaStreamEndCapture");
+      CK(cudaGraphInstantiate(&e->gexec[variant], graph, 0));
+      cudaGraphDestroy(graph);
+    }
+    CK(cudaGraphLaunch(e->gexec[variant], ctx->stream));
+    e->pending = e->boxes[0]->p.filter_on != 0;
+    for (int b = 0; b < nbox; ++b) {
+      astr_state* st = e->boxes[b];
+      st->pending = e->pending;
+      st->nstep += 1;
+      st->time = st->time + dt[b];
+    }
+  }
+  for (int b = 0; b < nbox; ++b) {
+    int rc = check_err(e->boxes[b]);
+    if (rc) return rc;
+  }
+  return ASTR_OK;
 }
 
 }  // extern "C"

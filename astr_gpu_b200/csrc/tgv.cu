@@ -54,6 +54,36 @@ __global__ void k_diag_reduce(const double* __restrict__ partials, int nparts, d
   }
 }
 
+__global__ void k_diag_reduce_batch(const DiagArgs* __restrict__ args) {
+  const DiagArgs a = args[blockIdx.x];
+  __shared__ double s[3][256];
+  double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+  for (int i = threadIdx.x; i < a.nparts; i += blockDim.x) {
+    a0 += a.partials[3 * i];
+    a1 += a.partials[3 * i + 1];
+    a2 += a.partials[3 * i + 2];
+  }
+  s[0][threadIdx.x] = a0;
+  s[1][threadIdx.x] = a1;
+  s[2][threadIdx.x] = a2;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w) {
+      s[0][threadIdx.x] += s[0][threadIdx.x + w];
+      s[1][threadIdx.x] += s[1][threadIdx.x + w];
+      s[2][threadIdx.x] += s[2][threadIdx.x + w];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    const int row = *a.counter;
+    a.hist[3 * row] = 0.5 * s[0][0] / a.norm;
+    a.hist[3 * row + 1] = 0.5 * s[1][0] / a.norm;
+    a.hist[3 * row + 2] = s[2][0] / a.norm;
+    *a.counter = row + 1;
+  }
+}
+
 // flowfield_init (tgvsolver.F90:203-224). Arithmetic is spelled with explicit _rn intrinsics so
 // that no multiply-add is contracted: the state matches the reference's bit for bit.
 __global__ void k_init_tgv(BoxGeo g, double const6, double pinf, double* q, const double* __restrict__ tabs) {
@@ -144,6 +174,24 @@ int pass_tiles(int pass) {
 
 template <int S, int WPL>
 cudaError_t launch_pass_t(int pass, const PassArgs& a, cudaStream_t st);
+template <int S, int WPL>
+cudaError_t launch_pass_batch_t(int pass, int dir, const PassArgs* dargs, const int* dcum, int nbox, int nctas,
+                                int threads, size_t smem, cudaStream_t st);
+
+cudaError_t launch_pass_batch(int pass, int dir, int S, int WPL, const PassArgs* dargs, const int* dcum, int nbox,
+                              int nctas, int threads, size_t smem, cudaStream_t st) {
+#define ASTR_B(s_, w_) \
+  if (S == s_ && WPL == w_) return launch_pass_batch_t<s_, w_>(pass, dir, dargs, dcum, nbox, nctas, threads, smem, st);
+  ASTR_B(3, 1) ASTR_B(5, 1) ASTR_B(5, 2) ASTR_B(5, 4) ASTR_B(9, 1) ASTR_B(9, 2) ASTR_B(9, 4)
+#undef ASTR_B
+  return cudaErrorInvalidValue;
+}
+
+size_t pass_shared_bytes(int pass, int TI, int LP, int WPL) {
+  size_t smem = ((size_t)pass_tiles(pass) * TI * LP + (size_t)TI * (SCAN_PER_LINE * WPL + SP_PER_LINE)) * sizeof(double);
+  if (pass == PASS_C) smem += 32 * 3 * sizeof(double);
+  return smem;
+}
 
 cudaError_t launch_pass(int pass, const PassArgs& a, int S, int WPL, cudaStream_t st) {
   if (S == 3 && WPL == 1) return launch_pass_t<3, 1>(pass, a, st);
@@ -159,6 +207,11 @@ cudaError_t launch_pass(int pass, const PassArgs& a, int S, int WPL, cudaStream_
 cudaError_t launch_diag_reduce(const double* partials, int nparts, double* hist, int* counter, double norm,
                                cudaStream_t st) {
   k_diag_reduce<<<1, 1024, 0, st>>>(partials, nparts, hist, counter, norm);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_diag_reduce_batch(const DiagArgs* dargs, int nbox, cudaStream_t st) {
+  k_diag_reduce_batch<<<nbox, 256, 0, st>>>(dargs);
   return cudaGetLastError();
 }
 

@@ -46,6 +46,21 @@ struct PassArgs {
 
 cudaError_t launch_pass(int pass, const PassArgs& a, int S, int WPL, cudaStream_t st);
 int pass_tiles(int pass);
+// One launch of a pass over nbox boxes of one solve layout: dargs[k] are box k's arguments
+// (device memory), dcum[k] its first CTA, nctas the total.
+cudaError_t launch_pass_batch(int pass, int dir, int S, int WPL, const PassArgs* dargs, const int* dcum, int nbox,
+                              int nctas, int threads, size_t smem, cudaStream_t st);
+size_t pass_shared_bytes(int pass, int TI, int LP, int WPL);
+
+// Batched diagnostics reduce: one CTA per box.
+struct DiagArgs {
+  const double* partials;
+  int nparts;
+  double* hist;
+  int* counter;
+  double norm;
+};
+cudaError_t launch_diag_reduce_batch(const DiagArgs* dargs, int nbox, cudaStream_t st);
 
 // Final ordered reduction of the pass-C partial sums into the history buffer.
 cudaError_t launch_diag_reduce(const double* partials, int nparts, double* hist, int* counter, double norm,
@@ -60,6 +75,10 @@ cudaError_t launch_pack(const BoxGeo& g, double* state, double* user, const int6
                         int nfields, int to_state, cudaStream_t st);
 
 enum Pass { PASS_A = 1, PASS_B = 2, PASS_C = 3, PASS_VA = 4, PASS_VB = 5, PASS_F = 6 };
+
+constexpr int SCAN_PER_LINE = 4;   // scan scratch per line in units of WPL doubles (NV <= 2)
+constexpr int SP_SOLVES = 13;      // closure tables kept per line (one per pending solve)
+constexpr int SP_PER_LINE = SP_SOLVES * 2 * NSP;
 
 // Physical directions of passes A, B, C. C is x: the heaviest pass (13 line solves and the
 // stress tensor) runs on contiguous lines, where any number of lines per CTA stays coalesced.

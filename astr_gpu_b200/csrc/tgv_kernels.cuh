@@ -24,7 +24,7 @@ struct TileCtx {
   bool svalid;          // that line exists
   int64_t sbase;        // element offset of node 0 of that line
   int64_t sd;
-  __device__ __forceinline__ TileCtx(const PassArgs& a) {
+  __device__ __forceinline__ TileCtx(const PassArgs& a, int bx, int by) {
     dim = a.g.N[DIR];
     TI = a.TI;
     LP = a.LP;
@@ -36,9 +36,9 @@ struct TileCtx {
       sl = threadIdx.x & (a.TI - 1);
       sn0 = threadIdx.x / a.TI;
     }
-    const int64_t i1 = (int64_t)blockIdx.x * a.TI + sl;
+    const int64_t i1 = (int64_t)bx * a.TI + sl;
     svalid = i1 < a.g.N[o1] + 1;
-    sbase = i1 * a.g.st[o1] + (int64_t)blockIdx.y * a.g.st[o2];
+    sbase = i1 * a.g.st[o1] + (int64_t)by * a.g.st[o2];
   }
   // f(tile offset of node n on the slot line, global offset) for n = n_lo.. n_hi
   template <class F>
@@ -199,9 +199,6 @@ __device__ __forceinline__ LaneIds lane_ids() {
   return z;
 }
 
-constexpr int SCAN_PER_LINE = 4;   // scan scratch per line in units of WPL doubles (NV <= 2)
-constexpr int SP_SOLVES = 13;      // closure tables kept per line (one per pending solve)
-constexpr int SP_PER_LINE = SP_SOLVES * 2 * NSP;
 
 // Closure-row RHS values of `ns` pending solves on every line of the tile, computed up front by
 // a few threads so that no warp diverges on closure rows during its solve:
@@ -282,9 +279,9 @@ __device__ __forceinline__ void tile_specials(const LineOp& op, int TI, int LP, 
 
 // ------------------------------------------------------------------ pass A and pass B
 template <int S, int WPL, int DIR, bool IS_A>
-__global__ void __launch_bounds__(512) k_pass_ab(PassArgs a) {
+__device__ __forceinline__ void k_pass_ab_body(const PassArgs& a, int bx, int by) {
   extern __shared__ double sm[];
-  const TileCtx<DIR, WPL> c(a);
+  const TileCtx<DIR, WPL> c(a, bx, by);
   const int tsz = c.TI * c.LP;
   double* T = sm;
   double* O = sm + 5 * tsz;
@@ -343,9 +340,9 @@ __global__ void __launch_bounds__(512) k_pass_ab(PassArgs a) {
 
 // ------------------------------------------------------------------ pass C
 template <int S, int WPL, int DIR>
-__global__ void __launch_bounds__(512) k_pass_c(PassArgs a) {
+__device__ __forceinline__ void k_pass_c_body(const PassArgs& a, int bx, int by) {
   extern __shared__ double sm[];
-  const TileCtx<DIR, WPL> c(a);
+  const TileCtx<DIR, WPL> c(a, bx, by);
   const int tsz = c.TI * c.LP;
   double* T = sm;
   double* Dt = sm + 5 * tsz;
@@ -387,7 +384,7 @@ __global__ void __launch_bounds__(512) k_pass_c(PassArgs a) {
     const double* DA = a.DA + c.sbase;
     const double* DB = a.DB + c.sbase;
     double* VF = a.VF + c.sbase;
-    const bool row_ok = (blockIdx.x * (int64_t)c.TI + c.sl) >= 1 && blockIdx.y >= 1;
+    const bool row_ok = (bx * (int64_t)c.TI + c.sl) >= 1 && by >= 1;
     c.for_nodes(0, dim, [&](int tix, int n) {
       const int64_t off = (int64_t)n * c.sd;
       double gr[4][3];
@@ -463,7 +460,8 @@ __global__ void __launch_bounds__(512) k_pass_c(PassArgs a) {
     double s0 = 0.0, s1 = 0.0, s2 = 0.0;
     const int nw = blockDim.x >> 5;
     for (int w = 0; w < nw; ++w) { s0 += red[3 * w]; s1 += red[3 * w + 1]; s2 += red[3 * w + 2]; }
-    double* pp = a.partials + 3 * ((int64_t)blockIdx.y * gridDim.x + blockIdx.x);
+    const int ntx = (a.g.N[TileCtx<DIR, WPL>::o1] + 1 + c.TI - 1) / c.TI;
+    double* pp = a.partials + 3 * ((int64_t)by * ntx + bx);
     pp[0] = s0; pp[1] = s1; pp[2] = s2;
   }
 
@@ -498,9 +496,9 @@ __global__ void __launch_bounds__(512) k_pass_c(PassArgs a) {
 
 // ------------------------------------------------------------------ pass A' (visc along A)
 template <int S, int WPL, int DIR>
-__global__ void __launch_bounds__(512) k_pass_va(PassArgs a) {
+__device__ __forceinline__ void k_pass_va_body(const PassArgs& a, int bx, int by) {
   extern __shared__ double sm[];
-  const TileCtx<DIR, WPL> c(a);
+  const TileCtx<DIR, WPL> c(a, bx, by);
   const int tsz = c.TI * c.LP;
   double* V = sm;
   double* scan = sm + 4 * tsz;
@@ -530,9 +528,9 @@ __global__ void __launch_bounds__(512) k_pass_va(PassArgs a) {
 
 // ------------------------------------------------------------------ pass B' (visc along B, update, filter)
 template <int S, int WPL, int DIR>
-__global__ void __launch_bounds__(512) k_pass_vb(PassArgs a) {
+__device__ __forceinline__ void k_pass_vb_body(const PassArgs& a, int bx, int by) {
   extern __shared__ double sm[];
-  const TileCtx<DIR, WPL> c(a);
+  const TileCtx<DIR, WPL> c(a, bx, by);
   const int tsz = c.TI * c.LP;
   double* V = sm;
   double* O = sm + 4 * tsz;
@@ -584,8 +582,10 @@ __global__ void __launch_bounds__(512) k_pass_vb(PassArgs a) {
         const int64_t off = (int64_t)n * c.sd;
         const double vis = (m >= 1) ? O[o] : 0.0;
         const double r = R[off] + vis;
-        const double qc = (c2 != 0.0) ? c2 * qq[off] : 0.0;
-        const double qn = c1 * qs[off] + qc + c3 * r * dt;
+        // (c1 qsave + c2 q) + (c3 qrhs) dt in the reference's order, rounded at every step so
+        // that the result does not depend on how the compiler contracts this kernel
+        const double qc = (c2 != 0.0) ? __dmul_rn(c2, qq[off]) : 0.0;
+        const double qn = __dadd_rn(__dadd_rn(__dmul_rn(c1, qs[off]), qc), __dmul_rn(__dmul_rn(c3, r), dt));
         O[o] = qn;
         put_images(sline, n, dim, qn);
       });
@@ -607,9 +607,9 @@ __global__ void __launch_bounds__(512) k_pass_vb(PassArgs a) {
 
 // ------------------------------------------------------------------ pass F (filter only, 5 fields)
 template <int S, int WPL, int DIR>
-__global__ void __launch_bounds__(512) k_pass_f(PassArgs a) {
+__device__ __forceinline__ void k_pass_f_body(const PassArgs& a, int bx, int by) {
   extern __shared__ double sm[];
-  const TileCtx<DIR, WPL> c(a);
+  const TileCtx<DIR, WPL> c(a, bx, by);
   const int tsz = c.TI * c.LP;
   double* T = sm;
   double* scan = sm + 5 * tsz;
@@ -634,9 +634,64 @@ __global__ void __launch_bounds__(512) k_pass_f(PassArgs a) {
   }
 }
 
+// ------------------------------------------------------------------ kernels
+// One box: the grid is the box's tile grid. Batch: blockIdx.x walks the concatenated tile grids
+// of nbox boxes (cum[k] = first CTA of box k); each CTA copies its box's arguments to shared
+// memory and runs the same body.
+struct BatchArgs {
+  const PassArgs* args;
+  const int* cum;
+  int nbox;
+};
+
+__device__ __forceinline__ const PassArgs& batch_decode(const BatchArgs& b, PassArgs& sa, int& bx, int& by) {
+  int lo = 0, hi = b.nbox - 1;
+  const int blk = blockIdx.x;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (__ldg(b.cum + mid) <= blk) lo = mid;
+    else hi = mid - 1;
+  }
+  const PassArgs* src = b.args + lo;
+  const int nwords = (int)(sizeof(PassArgs) / sizeof(unsigned long long));
+  for (int w = threadIdx.x; w < nwords; w += blockDim.x)
+    reinterpret_cast<unsigned long long*>(&sa)[w] = __ldg(reinterpret_cast<const unsigned long long*>(src) + w);
+  __syncthreads();
+  const int o1 = (sa.dir == 0) ? 1 : 0;
+  const int ntx = (sa.g.N[o1] + 1 + sa.TI - 1) / sa.TI;
+  const int local = blk - __ldg(b.cum + lo);
+  by = local / ntx;
+  bx = local - by * ntx;
+  return sa;
+}
+
+#define ASTR_PASS_KERNELS(NAME, TPARAMS, TARGS)                                      \
+  template <TPARAMS>                                                                   \
+  __global__ void __launch_bounds__(512) NAME(PassArgs a) {                            \
+    NAME##_body<TARGS>(a, blockIdx.x, blockIdx.y);                                     \
+  }                                                                                    \
+  template <TPARAMS>                                                                   \
+  __global__ void __launch_bounds__(512) NAME##_batch(BatchArgs b) {                   \
+    __shared__ PassArgs sa;                                                            \
+    int bx, by;                                                                        \
+    const PassArgs& a = batch_decode(b, sa, bx, by);                                   \
+    NAME##_body<TARGS>(a, bx, by);                                                     \
+  }
+
+#define ASTR_COMMA ,
+ASTR_PASS_KERNELS(k_pass_ab, int S ASTR_COMMA int WPL ASTR_COMMA int DIR ASTR_COMMA bool IS_A, S ASTR_COMMA WPL ASTR_COMMA DIR ASTR_COMMA IS_A)
+ASTR_PASS_KERNELS(k_pass_c, int S ASTR_COMMA int WPL ASTR_COMMA int DIR, S ASTR_COMMA WPL ASTR_COMMA DIR)
+ASTR_PASS_KERNELS(k_pass_va, int S ASTR_COMMA int WPL ASTR_COMMA int DIR, S ASTR_COMMA WPL ASTR_COMMA DIR)
+ASTR_PASS_KERNELS(k_pass_vb, int S ASTR_COMMA int WPL ASTR_COMMA int DIR, S ASTR_COMMA WPL ASTR_COMMA DIR)
+ASTR_PASS_KERNELS(k_pass_f, int S ASTR_COMMA int WPL ASTR_COMMA int DIR, S ASTR_COMMA WPL ASTR_COMMA DIR)
+#undef ASTR_PASS_KERNELS
+#undef ASTR_COMMA
+
 }  // namespace pass_detail
 
 using namespace pass_detail;
+
+inline size_t pass_smem(int pass, int TI, int LP, int WPL);
 
 template <class KernT>
 cudaError_t launch_k(KernT kern, dim3 grid, int threads, size_t smem, cudaStream_t st, const PassArgs& a) {
@@ -649,10 +704,7 @@ cudaError_t launch_k(KernT kern, dim3 grid, int threads, size_t smem, cudaStream
 template <int S, int WPL>
 cudaError_t launch_pass_t(int pass, const PassArgs& a, cudaStream_t st) {
   const int o1 = (a.dir == 0) ? 1 : 0, o2 = (a.dir == 2) ? 1 : 2;
-  const int tsz = a.TI * a.LP;
-  const int ntile = pass_tiles(pass);
-  size_t smem = ((size_t)ntile * tsz + (size_t)a.TI * (SCAN_PER_LINE * WPL + SP_PER_LINE)) * sizeof(double);
-  if (pass == PASS_C) smem += 32 * 3 * sizeof(double);
+  const size_t smem = pass_smem(pass, a.TI, a.LP, WPL);
   dim3 grid((unsigned)((a.g.N[o1] + 1 + a.TI - 1) / a.TI), (unsigned)(a.g.N[o2] + 1));
   const int threads = a.TI * WPL * 32;
   switch (pass) {
@@ -665,6 +717,37 @@ cudaError_t launch_pass_t(int pass, const PassArgs& a, cudaStream_t st) {
       if (a.dir == DIR_C) return launch_k(k_pass_f<S, WPL, DIR_C>, grid, threads, smem, st, a);
       if (a.dir == DIR_A) return launch_k(k_pass_f<S, WPL, DIR_A>, grid, threads, smem, st, a);
       return launch_k(k_pass_f<S, WPL, DIR_B>, grid, threads, smem, st, a);
+    default:
+      return cudaErrorInvalidValue;
+  }
+}
+
+// Dynamic shared memory of one pass launch for a tile of TI lines with pitch LP.
+inline size_t pass_smem(int pass, int TI, int LP, int WPL) { return pass_shared_bytes(pass, TI, LP, WPL); }
+
+template <class KernT>
+cudaError_t launch_kb(KernT kern, int nctas, int threads, size_t smem, cudaStream_t st, const BatchArgs& b) {
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  kern<<<nctas, threads, smem, st>>>(b);
+  return cudaGetLastError();
+}
+
+// One launch of a pass over several boxes of the same solve layout (see BatchArgs).
+template <int S, int WPL>
+cudaError_t launch_pass_batch_t(int pass, int dir, const PassArgs* dargs, const int* dcum, int nbox, int nctas,
+                                int threads, size_t smem, cudaStream_t st) {
+  const BatchArgs b{dargs, dcum, nbox};
+  switch (pass) {
+    case PASS_A: return launch_kb(k_pass_ab_batch<S, WPL, DIR_A, true>, nctas, threads, smem, st, b);
+    case PASS_B: return launch_kb(k_pass_ab_batch<S, WPL, DIR_B, false>, nctas, threads, smem, st, b);
+    case PASS_C: return launch_kb(k_pass_c_batch<S, WPL, DIR_C>, nctas, threads, smem, st, b);
+    case PASS_VA: return launch_kb(k_pass_va_batch<S, WPL, DIR_A>, nctas, threads, smem, st, b);
+    case PASS_VB: return launch_kb(k_pass_vb_batch<S, WPL, DIR_B>, nctas, threads, smem, st, b);
+    case PASS_F:
+      if (dir == DIR_C) return launch_kb(k_pass_f_batch<S, WPL, DIR_C>, nctas, threads, smem, st, b);
+      if (dir == DIR_A) return launch_kb(k_pass_f_batch<S, WPL, DIR_A>, nctas, threads, smem, st, b);
+      return launch_kb(k_pass_f_batch<S, WPL, DIR_B>, nctas, threads, smem, st, b);
     default:
       return cudaErrorInvalidValue;
   }

@@ -3,4 +3,6 @@
 
 namespace astr {
 template cudaError_t launch_pass_t<5, 1>(int pass, const PassArgs& a, cudaStream_t st);
+template cudaError_t launch_pass_batch_t<5, 1>(int pass, int dir, const PassArgs* dargs, const int* dcum,
+                                                     int nbox, int nctas, int threads, size_t smem, cudaStream_t st);
 }  // namespace astr

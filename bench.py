@@ -4,6 +4,7 @@ Mach 0.1, Re 1600, Pr 0.72, gamma 1.4, Sutherland, 6th-order compact derivatives
 compact filter alpha_f = 0.49 after every stage, dt fixed from CFL 0.5 at t = 0).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--size 512]
+    python bench.py --workload ensemble [--gpus N] [--steps K]   # 48 uneven boxes, batched
 
 One JSON line on rank 0. `value` = grid-point RK3 updates/s over all ranks (each rank advances
 its own 512^3 box: replicas, weak scaling), device-timed with CUDA events on the library's stream,
@@ -244,6 +245,135 @@ def run_ours(args, ws, rank, local):
         pg.destroy_process_group()
 
 
+ENS_METRIC = "ensemble grid-point RK3 updates/s FP64 (48 uneven periodic boxes)"
+
+
+def ensemble_boxes(ctx, specs):
+    import astr_gpu_b200 as ag
+    from astr_gpu_b200.fields import solenoidal_q
+    boxes = []
+    for sp in specs:
+        b = ag.TGVSolver(ctx, sp.n, params=ag.FlowParams(mach=sp.mach, reynolds=sp.reynolds))
+        if sp.kind == "tgv":
+            b.init_tgv()
+        else:
+            b.set_q(solenoidal_q(sp.n, sp.mach, sp.seed))
+        boxes.append(b)
+    return boxes
+
+
+def run_ensemble(args, ws, rank, local):
+    """Batched ensemble: every rank advances its LPT share of the 48 boxes (no collective on the
+    data path); value = all boxes' grid points x steps / the slowest rank's device time. On one
+    GPU the same boxes are also timed one at a time (each box its own per-step graph)."""
+    import torch
+    import astr_gpu_b200 as ag
+    from astr_gpu_b200.fields import ensemble_specs
+    from astr_gpu_b200.shard import box_cost, lpt_partition
+
+    torch.cuda.set_device(local)
+    pg = None
+    if ws > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+        pg = dist
+    specs = ensemble_specs(48, 48)
+    mine = lpt_partition([box_cost(sp.n) for sp in specs], ws)[rank]
+    stream = torch.cuda.Stream(device=local)
+    ctx = ag.Context(local, stream=stream)
+    boxes = ensemble_boxes(ctx, [specs[i] for i in mine])
+    dts = [b.cfl_dt(0.5) for b in boxes]
+    ens = ag.Ensemble(ctx, boxes)
+    ens.step(dts, args.warmup)
+    ctx.synchronize()
+
+    def barrier():
+        torch.cuda.synchronize(local)
+        if pg:
+            pg.barrier()
+        torch.cuda.synchronize(local)
+
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        ens.step(dts, args.steps)
+        e1.record(stream)
+        e1.synchronize()
+    barrier()
+    t = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device=f"cuda:{local}")
+    if pg:
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    ms_max = float(t.item())
+    pts_all = sum(sp.n ** 3 for sp in specs)
+    value = pts_all * args.steps / (ms_max * 1e-3)
+    single = None
+    if ws == 1 and not args.no_single:
+        solo = ensemble_boxes(ctx, specs)
+        sdts = [b.cfl_dt(0.5) for b in solo]
+        for b, dt in zip(solo, sdts):
+            b.rk3(dt, args.warmup)
+        ctx.synchronize()
+        e0.record(stream)
+        for b, dt in zip(solo, sdts):
+            b.rk3(dt, args.steps)
+        e1.record(stream)
+        e1.synchronize()
+        ms_solo = e0.elapsed_time(e1)
+        single = {"value": pts_all * args.steps / (ms_solo * 1e-3), "ms_per_step": ms_solo / args.steps,
+                  "how": "each box alone, its own autotuned launch shapes and per-step CUDA graph, boxes in turn"}
+        for b in solo:
+            b.close()
+    e2e = None
+    if not args.no_e2e:
+        # end to end: upload every box's state from pinned host memory, step, download, per step
+        import numpy as np
+        host = []
+        for b in boxes:
+            qh = torch.empty((5,) + b.shape[::-1], dtype=torch.float64, pin_memory=True)
+            q = qh.numpy().transpose(3, 2, 1, 0)
+            q[...] = b.get_q()
+            host.append((qh, q))
+        ne = args.e2e_steps
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(ne):
+            for b, (_, q) in zip(boxes, host):
+                b.set_q(q)
+            ens.step(dts, 1)
+            for b, (_, q) in zip(boxes, host):
+                q[...] = b.get_q()
+        te = time.perf_counter() - t0
+        tt = torch.tensor([te], dtype=torch.float64, device=f"cuda:{local}")
+        if pg:
+            pg.all_reduce(tt, op=pg.ReduceOp.MAX)
+        qb = sum(5 * 8 * int(np.prod(b.shape)) for b in boxes)
+        e2e = {"value": pts_all * ne / float(tt.item()), "unit": UNIT, "h2d_bytes_per_step": qb,
+               "d2h_bytes_per_step": qb, "steps": ne, "call": "astr_state_upload + astr_ensemble_step + astr_state_download"}
+    if rank == 0:
+        from collections import Counter
+        line = {
+            "metric": ENS_METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (24 Taylor-Green, 24 seeded solenoidal k^4 exp(-2(k/4)^2) boxes)",
+            "config": {"workload": "48 periodic boxes, sizes seeded from {32,48,64,96,128}^3, Mach U[0.1,0.5], "
+                                   "Re U[400,3200], dt per box from CFL 0.5",
+                       "sizes": dict(Counter(sp.n for sp in specs)), "points": pts_all,
+                       "parallelism": f"LPT box shards x{ws}" if ws > 1 else "single GPU",
+                       "graph": "one CUDA graph per ensemble step", "l2": "total state 6 GB > L2"},
+            "one_at_a_time": single, "e2e": e2e, "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    ens.close()
+    for b in boxes:
+        b.close()
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -256,12 +386,16 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--workload", default="tgv", choices=["tgv", "ensemble"])
+    ap.add_argument("--no-single", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         print("warning: fewer than 3 warm-up steps", file=sys.stderr)
     ws, rank, local = dist_setup(args)
     if args.impl == "reference":
         run_reference(args, ws, rank)
+    elif args.workload == "ensemble":
+        run_ensemble(args, ws, rank, local)
     else:
         run_ours(args, ws, rank, local)
 

@@ -133,6 +133,17 @@ int astr_state_set_launch_shape(astr_state* st, int pass, int S, int WPL, int TI
  * one launch of each pass, ms[0..6] = A, B, C, A', B', F(C), diagnostics reduce. */
 int astr_pass_timings(astr_state* st, double dt, int nsteps, double ms[7]);
 
+/* ---- batched ensemble ---------------------------------------------------------------- */
+/* Several independent boxes (each an astr_state of the same context, sizes may differ)
+ * advanced together: every pass of an RK3 stage is one launch per group of boxes sharing a
+ * solve layout, and each ensemble step is one CUDA graph. No counterpart in the reference
+ * (ASTR runs one block per MPI rank); the per-box results equal astr_rk3_step's. */
+typedef struct astr_ensemble astr_ensemble;
+int astr_ensemble_create(astr_ctx* ctx, astr_state* const* boxes, int nbox, astr_ensemble** out);
+int astr_ensemble_destroy(astr_ensemble* e);
+/* nsteps RK3 steps of every box; dt[b] is box b's time step. History rows go to each box. */
+int astr_ensemble_step(astr_ensemble* e, const double* dt, int nsteps);
+
 /* ---- no-allocation variant -------------------------------------------------------- */
 /* dt such that cflcal's CFL equals `cfl` for the conserved variables q (a DEVICE array,
  * Fortran order q(lb.., 1:5) covering nodes 0..im x 0..jm x 0..km of a periodic box of side
