@@ -60,6 +60,12 @@ SIGNATURES = {
     "astr_ensemble_create": (_i, [_vp, _pvp, _i, _pvp]),
     "astr_ensemble_destroy": (_i, [_vp]),
     "astr_ensemble_step": (_i, [_vp, _dp, _i]),
+    "astr_adjoint_create": (_i, [_vp, _i, _pvp]),
+    "astr_adjoint_destroy": (_i, [_vp]),
+    "astr_adjoint_forward": (_i, [_vp, _d, _i, _dp]),
+    "astr_adjoint_backward": (_i, [_vp, _vp, _i64p, _i64p, _i]),
+    "astr_step_vjp": (_i, [_vp, _d, _vp, _vp, _i64p, _i64p, _i]),
+    "astr_scheme_apply_transpose": (_i, [_vp, _vp, _i, _vp, _i64p, _vp, _i, _d]),
     "astr_cfl_dt_noalloc": (_i, [_vp, _vp, _i64p, _i64p, _i, _i, _i, _d, _d, _d, _dp]),
 }
 

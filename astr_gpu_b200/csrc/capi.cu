@@ -13,6 +13,7 @@
 #include "../../include/astr_b200.h"
 #include "internal.h"
 #include "tgv.cuh"
+#include "adjoint.cuh"
 
 using namespace astr;
 
@@ -1081,6 +1082,336 @@ int astr_ensemble_step(astr_ensemble* e, const double* dt, int nsteps) {
     int rc = check_err(e->boxes[b]);
     if (rc) return rc;
   }
+  return ASTR_OK;
+}
+
+}  // extern "C"
+
+// ====================================================================== discrete adjoint
+// Gradient of J = <|rho u|^2 / (2 rho)> over nodes 1..N of the state after nsteps RK3 steps with
+// respect to the initial conserved variables: checkpoints every `every` steps, each segment
+// recomputed stage by stage (stage inputs kept), then reversed stage by stage.
+struct astr_adjoint {
+  astr_state* st = nullptr;
+  int every = 20;
+  AdjDevOp td[3], tf[3];        // transposed derivative / filter per direction
+  PassCfg lcfg[3], gcfg[3];     // adjoint line kernels / gradient kernels per direction
+  double* buf = nullptr;
+  double *lam = nullptr, *lq = nullptr, *t1 = nullptr, *t2 = nullptr, *lnew = nullptr, *G = nullptr, *Y = nullptr,
+         *lsave = nullptr, *U = nullptr, *lp = nullptr, *LG = nullptr, *part = nullptr, *jval = nullptr;
+  std::vector<double*> ckpt;    // state at steps 0, every, 2*every, ...
+  double* seg = nullptr;        // stage inputs of one segment: every x 3 states
+  int nsteps = 0;
+  double dt = 0.0;
+  double J = 0.0;
+  bool have_forward = false;
+};
+
+namespace {
+
+void adj_free(astr_adjoint* a) {
+  for (int d = 0; d < 3; ++d) { free_adj_devop(a->td[d]); free_adj_devop(a->tf[d]); }
+  if (a->buf) cudaFree(a->buf);
+  a->buf = nullptr;
+  for (double* c : a->ckpt) cudaFree(c);
+  a->ckpt.clear();
+  if (a->seg) cudaFree(a->seg);
+  a->seg = nullptr;
+}
+
+// One RK3 stage with every filter applied: qout = F(c1 qsave + c2 qin + c3 dt rhs(qin)).
+cudaError_t run_stage_full(astr_state* st, int s, const double* qin, const double* qsave, double* qout, double dt) {
+  static const double rk[3][3] = {{1.0, 0.0, 1.0}, {0.75, 0.25, 0.25}, {1.0 / 3.0, 2.0 / 3.0, 2.0 / 3.0}};
+  double* qi = const_cast<double*>(qin);
+  cudaError_t e;
+  PassArgs a = base_args(st, CFG_A);
+  a.q = qi; a.D = st->DA; a.do_filter = 0;
+  if ((e = run_pass(st, CFG_A, a)) != cudaSuccess) return e;
+  a = base_args(st, CFG_B);
+  a.q = qi; a.D = st->DB;
+  if ((e = run_pass(st, CFG_B, a)) != cudaSuccess) return e;
+  a = base_args(st, CFG_C);
+  a.q = qi; a.DA = st->DA; a.DB = st->DB; a.partials = nullptr;
+  if ((e = run_pass(st, CFG_C, a)) != cudaSuccess) return e;
+  a = base_args(st, CFG_VA);
+  if ((e = run_pass(st, CFG_VA, a)) != cudaSuccess) return e;
+  a = base_args(st, CFG_VB);
+  a.q = qi; a.qsave = qsave; a.qout = qout;
+  a.mode = 1; a.do_filter = st->p.filter_on;
+  a.c1 = rk[s][0]; a.c2 = rk[s][1]; a.c3 = rk[s][2]; a.dt = dt;
+  if ((e = run_pass(st, CFG_VB, a)) != cudaSuccess) return e;
+  if (st->p.filter_on) {
+    a = base_args(st, CFG_FC);
+    a.q = qout;
+    if ((e = run_pass(st, CFG_FC, a)) != cudaSuccess) return e;
+    a = base_args(st, CFG_FA);
+    a.q = qout;
+    if ((e = run_pass(st, CFG_FA, a)) != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+AdjLineArgs adj_line_args(astr_adjoint* A, int dir, bool filter, const double* in, double* out, int nf, double alpha,
+                          bool acc) {
+  astr_state* st = A->st;
+  const AdjDevOp& op = filter ? A->tf[dir] : A->td[dir];
+  AdjLineArgs a{};
+  a.p.g = st->g;
+  a.p.th = st->th;
+  a.p.opd = op.tri.op;
+  a.p.dir = dir;
+  a.p.TI = A->lcfg[dir].TI;
+  a.p.LP = A->lcfg[dir].LP;
+  a.w = op.w;
+  a.in = in;
+  a.out = out;
+  a.nf = nf;
+  a.alpha = alpha;
+  a.accumulate = acc ? 1 : 0;
+  return a;
+}
+
+cudaError_t adj_lines(astr_adjoint* A, int dir, bool filter, const double* in, double* out, int nf, double alpha,
+                      bool acc) {
+  const AdjLineArgs a = adj_line_args(A, dir, filter, in, out, nf, alpha, acc);
+  return launch_adj_lines(a, A->lcfg[dir].S, A->lcfg[dir].WPL, A->st->ctx->stream);
+}
+
+cudaError_t adj_grad(astr_adjoint* A, int dir, const double* q, double* D) {
+  astr_state* st = A->st;
+  const PassCfg& c = A->gcfg[dir];
+  auto& o = get_ops(st, dir, c.S, c.WPL);
+  PassArgs a{};
+  a.g = st->g;
+  a.th = st->th;
+  a.opd = o.first.op;
+  a.opf = o.second.op;
+  a.dir = dir;
+  a.dA = DIR_A; a.dB = DIR_B; a.dC = DIR_C;
+  a.TI = c.TI;
+  a.LP = c.LP;
+  a.q = const_cast<double*>(q);
+  a.D = D;
+  a.err = st->err;
+  return launch_adj_grad(a, c.S, c.WPL, st->ctx->stream);
+}
+
+// lam <- (d q_out / d q_in)^T lam for one RK3 step whose stage inputs are S0, S1, S2.
+cudaError_t adj_step(astr_adjoint* A, const double* S0, const double* S1, const double* S2) {
+  static const double rk[3][3] = {{1.0, 0.0, 1.0}, {0.75, 0.25, 0.25}, {1.0 / 3.0, 2.0 / 3.0, 2.0 / 3.0}};
+  astr_state* st = A->st;
+  cudaStream_t sm = st->ctx->stream;
+  const int64_t fs = st->g.fs;
+  const double* Ss[3] = {S0, S1, S2};
+  cudaError_t e;
+  if ((e = cudaMemsetAsync(A->lsave, 0, 5 * fs * sizeof(double), sm)) != cudaSuccess) return e;
+  for (int s = 2; s >= 0; --s) {
+    const double* qs = Ss[s];
+    const double c1 = rk[s][0], c2 = rk[s][1], c3 = rk[s][2];
+    // filters: lam_new = F_A^T F_C^T F_B^T lam
+    if (st->p.filter_on) {
+      if ((e = adj_lines(A, DIR_B, true, A->lam, A->t1, 5, 1.0, false)) != cudaSuccess) return e;
+      if ((e = adj_lines(A, DIR_C, true, A->t1, A->t2, 5, 1.0, false)) != cudaSuccess) return e;
+      if ((e = adj_lines(A, DIR_A, true, A->t2, A->lnew, 5, 1.0, false)) != cudaSuccess) return e;
+    } else {
+      if ((e = cudaMemcpyAsync(A->lnew, A->lam, 5 * fs * sizeof(double), cudaMemcpyDeviceToDevice, sm)) != cudaSuccess)
+        return e;
+    }
+    for (int d = 0; d < 3; ++d) {
+      if ((e = adj_grad(A, d, qs, A->G + 4 * d * fs)) != cudaSuccess) return e;
+      if ((e = adj_lines(A, d, false, A->lnew, A->Y + 5 * d * fs, 5, c3 * A->dt * st->g.rd[d], false)) != cudaSuccess)
+        return e;
+    }
+    if ((e = launch_adj_point1(st->g, st->th, qs, A->G, A->Y, A->lnew, c1, c2, A->lsave, A->lq, A->U, A->lp, A->LG,
+                               sm)) != cudaSuccess)
+      return e;
+    for (int d = 0; d < 3; ++d)
+      if ((e = adj_lines(A, d, false, A->LG + 4 * d * fs, A->U, 4, st->g.rd[d], true)) != cudaSuccess) return e;
+    if ((e = launch_adj_point2(st->g, st->th, qs, A->U, A->lp, A->lq, s == 0 ? A->lsave : nullptr, sm)) != cudaSuccess)
+      return e;
+    std::swap(A->lam, A->lq);
+  }
+  return cudaSuccess;
+}
+
+int adj_setup(astr_adjoint* A) {
+  astr_state* st = A->st;
+  astr_ctx* ctx = st->ctx;
+  for (int d = 0; d < 3; ++d) {
+    std::string err;
+    AdjHostOp hd, hf;
+    if (!build_adjoint_op(st->hd[d], hd, err) || !build_adjoint_op(st->hf[d], hf, err))
+      return fail(ctx, ASTR_ERR_UNSUPPORTED, err);
+    const Layout L = pick_layout(st->hf[d].nsys());
+    if (L.S == 0) return fail(ctx, ASTR_ERR_UNSUPPORTED, "line too long for the adjoint layouts");
+    CK(make_adj_devop(hd, L, A->td[d]));
+    CK(make_adj_devop(hf, L, A->tf[d]));
+    PassCfg lc;
+    lc.S = L.S; lc.WPL = L.WPL;
+    lc.TI = std::min(16, 512 / (32 * L.WPL));
+    while (lc.TI > 1 && adj_lines_smem(lc.TI, tile_pitch(st->g.N[d], lc.TI), L.WPL) > 100 * 1024) lc.TI >>= 1;
+    lc.LP = tile_pitch(st->g.N[d], lc.TI);
+    A->lcfg[d] = lc;
+    PassCfg gc;
+    gc.S = L.S; gc.WPL = L.WPL;
+    gc.TI = pick_ti(PASS_A, st->g.N[d], L.WPL);
+    gc.LP = tile_pitch(st->g.N[d], gc.TI);
+    A->gcfg[d] = gc;
+  }
+  const int64_t fs = st->g.fs;
+  const int nf = 5 * 5 + 12 + 15 + 5 + 4 + 1 + 12;
+  CK(cudaMalloc(&A->buf, ((size_t)nf * fs + (st->g.N[2] + 1) + 8) * sizeof(double)));
+  double* p = A->buf;
+  auto take = [&](int n) { double* r = p; p += (size_t)n * fs; return r; };
+  A->lam = take(5); A->lq = take(5); A->t1 = take(5); A->t2 = take(5); A->lnew = take(5);
+  A->G = take(12); A->Y = take(15); A->lsave = take(5); A->U = take(4); A->lp = take(1); A->LG = take(12);
+  A->part = p;
+  A->jval = p + (st->g.N[2] + 1);
+  CK(cudaMalloc(&A->seg, (size_t)A->every * 3 * 5 * fs * sizeof(double)));
+  return ASTR_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int astr_adjoint_create(astr_state* st, int checkpoint_every, astr_adjoint** out) {
+  if (!st || !out || checkpoint_every < 1) return ASTR_ERR_ARG;
+  astr_adjoint* A = new astr_adjoint();
+  A->st = st;
+  A->every = checkpoint_every;
+  int rc = adj_setup(A);
+  if (rc) { adj_free(A); delete A; return rc; }
+  *out = A;
+  return ASTR_OK;
+}
+
+int astr_adjoint_destroy(astr_adjoint* A) {
+  if (!A) return ASTR_ERR_ARG;
+  adj_free(A);
+  delete A;
+  return ASTR_OK;
+}
+
+int astr_adjoint_forward(astr_adjoint* A, double dt, int nsteps, double* J) {
+  if (!A || !(dt > 0.0) || nsteps < 1) return ASTR_ERR_ARG;
+  astr_state* st = A->st;
+  astr_ctx* ctx = st->ctx;
+  const size_t qb = 5 * (size_t)st->g.fs * sizeof(double);
+  for (double* c : A->ckpt) cudaFree(c);
+  A->ckpt.clear();
+  CK(finalize_filter(st));
+  for (int s0 = 0; s0 < nsteps; s0 += A->every) {
+    double* c = nullptr;
+    CK(cudaMalloc(&c, qb));
+    A->ckpt.push_back(c);
+    CK(cudaMemcpyAsync(c, st->Q0, qb, cudaMemcpyDeviceToDevice, ctx->stream));
+    const int n = std::min(A->every, nsteps - s0);
+    int rc = astr_rk3_step(st, dt, n);
+    if (rc) return rc;
+    CK(finalize_filter(st));
+  }
+  CK(launch_kinetic_energy(st->g, st->Q0, A->part, A->jval, ctx->stream));
+  CK(cudaMemcpyAsync(&A->J, A->jval, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  A->nsteps = nsteps;
+  A->dt = dt;
+  A->have_forward = true;
+  if (J) *J = A->J;
+  return check_err(st);
+}
+
+int astr_adjoint_backward(astr_adjoint* A, double* grad, const int64_t shape[3], const int64_t lbound[3], int where) {
+  if (!A || !grad || !shape || !lbound) return ASTR_ERR_ARG;
+  astr_state* st = A->st;
+  astr_ctx* ctx = st->ctx;
+  if (!A->have_forward) return fail(ctx, ASTR_ERR_STATE, "astr_adjoint_backward needs astr_adjoint_forward first");
+  cudaStream_t sm = ctx->stream;
+  const int64_t fs = st->g.fs;
+  const size_t qb = 5 * (size_t)fs * sizeof(double);
+  // dJ/dq at the final state (the state's Q0 after the forward run)
+  CK(finalize_filter(st));
+  CK(launch_adj_objective(st->g, st->Q0, A->lam, sm));
+  const int nseg = (int)A->ckpt.size();
+  for (int j = nseg - 1; j >= 0; --j) {
+    const int s0 = j * A->every;
+    const int len = std::min(A->every, A->nsteps - s0);
+    auto stage = [&](int n, int s) { return A->seg + ((size_t)n * 3 + s) * 5 * fs; };
+    CK(cudaMemcpyAsync(stage(0, 0), A->ckpt[j], qb, cudaMemcpyDeviceToDevice, sm));
+    for (int n = 0; n < len; ++n) {
+      CK(run_stage_full(st, 0, stage(n, 0), stage(n, 0), stage(n, 1), A->dt));
+      CK(run_stage_full(st, 1, stage(n, 1), stage(n, 0), stage(n, 2), A->dt));
+      if (n + 1 < len) CK(run_stage_full(st, 2, stage(n, 2), stage(n, 0), stage(n + 1, 0), A->dt));
+    }
+    for (int n = len - 1; n >= 0; --n) CK(adj_step(A, stage(n, 0), stage(n, 1), stage(n, 2)));
+  }
+  int rc = copy_fields(st, A->lam, grad, shape, lbound, 0, where);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(sm));
+  return check_err(st);
+}
+
+// lam_out = (d step / d q)^T lam_in for one RK3 step of size dt at the state's current q (the
+// state is not advanced). Arrays hold 5 fields of nodes 0..N.
+int astr_step_vjp(astr_adjoint* A, double dt, const double* lam_in, double* lam_out, const int64_t shape[3],
+                  const int64_t lbound[3], int where) {
+  if (!A || !lam_in || !lam_out || !shape || !lbound || !(dt > 0.0)) return ASTR_ERR_ARG;
+  astr_state* st = A->st;
+  astr_ctx* ctx = st->ctx;
+  cudaStream_t sm = ctx->stream;
+  const size_t qb = 5 * (size_t)st->g.fs * sizeof(double);
+  CK(finalize_filter(st));
+  double* S0 = A->seg;
+  double* S1 = S0 + 5 * st->g.fs;
+  double* S2 = S1 + 5 * st->g.fs;
+  if (A->every < 1) return ASTR_ERR_ARG;
+  CK(cudaMemcpyAsync(S0, st->Q0, qb, cudaMemcpyDeviceToDevice, sm));
+  CK(run_stage_full(st, 0, S0, S0, S1, dt));
+  CK(run_stage_full(st, 1, S1, S0, S2, dt));
+  int rc = copy_fields(st, A->lam, const_cast<double*>(lam_in), shape, lbound, 1, where);
+  if (rc) return rc;
+  const double keep = A->dt;
+  A->dt = dt;
+  cudaError_t e = adj_step(A, S0, S1, S2);
+  A->dt = keep;
+  CK(e);
+  rc = copy_fields(st, A->lam, lam_out, shape, lbound, 0, where);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(sm));
+  return ASTR_OK;
+}
+
+// out = scale * L^T g for every line along dir of nfields fields of nodes 0..N (periodic
+// operators; device arrays of shape (n0, n1, n2) in Fortran order, fields contiguous).
+int astr_scheme_apply_transpose(astr_ctx* ctx, astr_scheme* s, int dir, const double* g, const int64_t dims[3],
+                                double* out, int nfields, double scale) {
+  if (!ctx || !s || !g || !out || !dims || dir < 0 || dir > 2 || nfields < 1) return fail(ctx, ASTR_ERR_ARG, "bad argument");
+  if (dims[dir] != s->h.dim + 1) return fail(ctx, ASTR_ERR_ARG, "dims[dir] must be dim+1");
+  std::string err;
+  AdjHostOp h;
+  if (!build_adjoint_op(s->h, h, err)) return fail(ctx, ASTR_ERR_UNSUPPORTED, err);
+  const Layout L = pick_layout(s->h.nsys());
+  AdjDevOp op;
+  CK(make_adj_devop(h, L, op));
+  AdjLineArgs a{};
+  a.p.g.N[0] = (int)dims[0] - 1; a.p.g.N[1] = (int)dims[1] - 1; a.p.g.N[2] = (int)dims[2] - 1;
+  a.p.g.st[0] = 1; a.p.g.st[1] = dims[0]; a.p.g.st[2] = dims[0] * dims[1];
+  a.p.g.fs = dims[0] * dims[1] * dims[2];
+  a.p.opd = op.tri.op;
+  a.p.dir = dir;
+  a.p.TI = std::min(16, 512 / (32 * L.WPL));
+  while (a.p.TI > 1 && adj_lines_smem(a.p.TI, tile_pitch(s->h.dim, a.p.TI), L.WPL) > 100 * 1024) a.p.TI >>= 1;
+  a.p.LP = tile_pitch(s->h.dim, a.p.TI);
+  a.w = op.w;
+  a.in = g;
+  a.out = out;
+  a.nf = nfields;
+  a.alpha = scale;
+  a.accumulate = 0;
+  cudaError_t e = launch_adj_lines(a, L.S, L.WPL, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  free_adj_devop(op);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "transposed line kernel");
   return ASTR_OK;
 }
 

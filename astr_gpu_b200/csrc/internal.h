@@ -36,6 +36,8 @@ struct DevOp {
   int S = 0, WPL = 0;
 };
 cudaError_t make_devop(const HostOp& h, Layout lay, DevOp& out);
+// The LineOp fields of a host operator (no lane tables).
+void fill_lineop(const HostOp& h, LineOp& o);
 void free_devop(DevOp& d);
 
 // Tile line pitch (doubles) for TI lines of dim+1 nodes plus halos, chosen so that line-fastest

@@ -162,7 +162,7 @@ __device__ __forceinline__ void seg_solve(double (&v)[S], const double* __restri
 // ---------------------------------------------------------------- right-hand sides
 // Compact derivative closure rows, derivative.F90:230-294. Returns false for interior rows.
 template <class Get>
-__device__ __forceinline__ bool deriv_special(const LineOp& op, int r, Get f, double& out) {
+__host__ __device__ __forceinline__ bool deriv_special(const LineOp& op, int r, Get f, double& out) {
   const int j = r - op.ext_lo;
   if (r == 0) {
     if (op.left_phys) { out = -2.5 * f(j) + 2.0 * f(j + 1) + 0.5 * f(j + 2); return true; }
@@ -204,7 +204,7 @@ __device__ __forceinline__ void fill_window(double (&w)[W], int n0, int dim, Get
 }
 
 template <class Get>
-__device__ __forceinline__ bool filter_special(const LineOp& op, int r, Get f, double& out);
+__host__ __device__ __forceinline__ bool filter_special(const LineOp& op, int r, Get f, double& out);
 
 // RHS value of closure row r (derivative or filter), for the precomputed closure table.
 template <class Get>
@@ -263,7 +263,7 @@ __device__ __forceinline__ double explicit_row(const LineOp& op, int i, Get v) {
 
 // Compact filter closure rows, filter.F90:176-269. Returns false for interior rows.
 template <class Get>
-__device__ __forceinline__ bool filter_special(const LineOp& op, int r, Get f, double& out) {
+__host__ __device__ __forceinline__ bool filter_special(const LineOp& op, int r, Get f, double& out) {
   const int i0 = -op.ext_lo;
   const int im = op.nsys - 1 - op.ext_lo;
   const int j = r - op.ext_lo;

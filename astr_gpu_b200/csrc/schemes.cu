@@ -202,17 +202,8 @@ Layout pick_layout(int nsys_max) {
   return {0, 0};
 }
 
-cudaError_t make_devop(const HostOp& h, Layout lay, DevOp& out) {
-  out.S = lay.S;
-  out.WPL = lay.WPL;
-  const int nseg = 32 * lay.WPL;
-  std::vector<double> tab = lane_tables(h, lay.S, nseg);
-  cudaError_t e = cudaMalloc(&out.dtab, tab.size() * sizeof(double));
-  if (e != cudaSuccess) return e;
-  e = cudaMemcpy(out.dtab, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice);
-  if (e != cudaSuccess) return e;
-  LineOp& o = out.op;
-  o.tab = out.dtab;
+void fill_lineop(const HostOp& h, LineOp& o) {
+  o.tab = nullptr;
   o.nsys = h.nsys();
   o.ext_lo = -h.first_node;
   o.dim = h.dim;
@@ -220,8 +211,8 @@ cudaError_t make_devop(const HostOp& h, Layout lay, DevOp& out) {
   o.left_phys = h.left_phys;
   o.right_phys = h.right_phys;
   o.no_filter_note = h.no_note;
-  o.nseg = nseg;
-  o.S = lay.S;
+  o.nseg = 0;
+  o.S = 0;
   // closure rows with their own RHS formulas (derivative.F90:230-294, filter.F90:176-269)
   if (h.kind == OP_FILTER) {
     o.spec_lo = h.left_phys ? 5 : 3;
@@ -235,6 +226,22 @@ cudaError_t make_devop(const HostOp& h, Layout lay, DevOp& out) {
   std::memcpy(o.cb, h.cb, sizeof(o.cb));
   std::memcpy(o.c6, h.c6, sizeof(o.c6));
   std::memcpy(o.c8, h.c8, sizeof(o.c8));
+}
+
+cudaError_t make_devop(const HostOp& h, Layout lay, DevOp& out) {
+  out.S = lay.S;
+  out.WPL = lay.WPL;
+  const int nseg = 32 * lay.WPL;
+  std::vector<double> tab = lane_tables(h, lay.S, nseg);
+  cudaError_t e = cudaMalloc(&out.dtab, tab.size() * sizeof(double));
+  if (e != cudaSuccess) return e;
+  e = cudaMemcpy(out.dtab, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) return e;
+  LineOp& o = out.op;
+  fill_lineop(h, o);
+  o.tab = out.dtab;
+  o.nseg = nseg;
+  o.S = lay.S;
   return cudaSuccess;
 }
 

@@ -144,6 +144,27 @@ int astr_ensemble_destroy(astr_ensemble* e);
 /* nsteps RK3 steps of every box; dt[b] is box b's time step. History rows go to each box. */
 int astr_ensemble_step(astr_ensemble* e, const double* dt, int nsteps);
 
+/* ---- discrete adjoint ---------------------------------------------------------------- */
+/* Gradient of the final volume-averaged kinetic energy J = sum_{nodes 1..N} |rho u|^2/(2 rho) /
+ * (im jm km) of nsteps RK3 steps (compact scheme, filter) with respect to the initial conserved
+ * variables, by the discrete adjoint of the step: transposed compact solves and stencils,
+ * pointwise vector-Jacobian products of the fluxes, reverse SSP-RK3 with a checkpoint every
+ * `checkpoint_every` steps. No counterpart in the reference (ASTR has no adjoint); the forward
+ * steps are the reference's rk3/rhscal (tgvsolver.F90:962-1082). Periodic boxes only. */
+typedef struct astr_adjoint astr_adjoint;
+int astr_adjoint_create(astr_state* st, int checkpoint_every, astr_adjoint** out);
+int astr_adjoint_destroy(astr_adjoint* adj);
+/* Advance the state nsteps steps from its current q, keeping checkpoints; *J = the objective. */
+int astr_adjoint_forward(astr_adjoint* adj, double dt, int nsteps, double* J);
+/* dJ/dq(step 0) into grad (5 fields of nodes 0..N, Fortran order, host or device). */
+int astr_adjoint_backward(astr_adjoint* adj, double* grad, const int64_t shape[3], const int64_t lbound[3], int where);
+/* lam_out = (d step/d q)^T lam_in for one step of size dt at the state's q (state unchanged). */
+int astr_step_vjp(astr_adjoint* adj, double dt, const double* lam_in, double* lam_out, const int64_t shape[3],
+                  const int64_t lbound[3], int where);
+/* out = scale * L^T g along dir for a periodic scheme L (device arrays of dims, nodes 0..N along dir). */
+int astr_scheme_apply_transpose(astr_ctx* ctx, astr_scheme* s, int dir, const double* g, const int64_t dims[3],
+                                double* out, int nfields, double scale);
+
 /* ---- no-allocation variant -------------------------------------------------------- */
 /* dt such that cflcal's CFL equals `cfl` for the conserved variables q (a DEVICE array,
  * Fortran order q(lb.., 1:5) covering nodes 0..im x 0..jm x 0..km of a periodic box of side
