@@ -5,6 +5,7 @@ compact filter alpha_f = 0.49 after every stage, dt fixed from CFL 0.5 at t = 0)
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--size 512]
     python bench.py --workload ensemble [--gpus N] [--steps K]   # 48 uneven boxes, batched
+    python bench.py --workload adjoint                          # 128^3 gradient, adjoint:forward
 
 One JSON line on rank 0. `value` = grid-point RK3 updates/s over all ranks (each rank advances
 its own 512^3 box: replicas, weak scaling), device-timed with CUDA events on the library's stream,
@@ -374,6 +375,84 @@ def run_ensemble(args, ws, rank, local):
         pg.destroy_process_group()
 
 
+ADJ_METRIC = "adjoint:forward time ratio, 128^3 decaying turbulence, 200 RK3 steps, checkpoint every 20"
+
+
+def run_adjoint(args, ws, rank, local):
+    """Discrete adjoint: 128^3 periodic random solenoidal field (M_t 0.3, Re for Re_lambda = 50),
+    200 steps with filter, J = final kinetic energy, dJ/dq0 with a checkpoint every 20 steps.
+    Times (device, CUDA events): the plain forward (200 graph-captured steps), the checkpointed
+    forward, and the reverse sweep (segment recomputation + adjoint stages). Every rank runs its
+    own replica (no collective on the data path)."""
+    import torch
+    import astr_gpu_b200 as ag
+    from astr_gpu_b200.adjoint import Adjoint, fortran_empty
+    from astr_gpu_b200.fields import solenoidal_q, solenoidal_velocity
+    import numpy as np
+
+    torch.cuda.set_device(local)
+    pg = None
+    if ws > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+        pg = dist
+    n, nsteps, every, mach, seed = args.adj_size, args.adj_steps, 20, 0.3, 2024
+    u = solenoidal_velocity(n, seed)
+    k = np.fft.fftfreq(n, 1.0 / n)
+    d2 = [np.mean(np.fft.ifftn(1j * [k[:, None, None], k[None, :, None], k[None, None, :]][a]
+                                * np.fft.fftn(u[a])).real ** 2) for a in range(3)]
+    up = np.sqrt(np.mean(u[0] ** 2 + u[1] ** 2 + u[2] ** 2) / 3.0)
+    re = 50.0 / (up * up / np.sqrt(np.mean(d2)))
+    stream = torch.cuda.Stream(device=local)
+    ctx = ag.Context(local, stream=stream)
+    s = ag.TGVSolver(ctx, n, params=ag.FlowParams(mach=mach, reynolds=re))
+    q0 = solenoidal_q(n, mach, seed)
+    s.set_q(q0)
+    dt = s.cfl_dt(0.5)
+    s.rk3(dt, args.warmup)
+    ctx.synchronize()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(6)]
+    g = fortran_empty(s.shape + (5,), f"cuda:{local}")
+    with ClockSampler(local) as clk:
+        s.set_q(q0)
+        ev[0].record(stream)
+        s.rk3(dt, nsteps)
+        ev[1].record(stream)
+        s.set_q(q0)
+        adj = Adjoint(s, every)
+        ev[2].record(stream)
+        J = adj.forward(dt, nsteps)
+        ev[3].record(stream)
+        ev[4].record(stream)
+        adj.backward(g)
+        ev[5].record(stream)
+        ev[5].synchronize()
+    t_plain, t_fwd, t_bwd = ev[0].elapsed_time(ev[1]), ev[2].elapsed_time(ev[3]), ev[4].elapsed_time(ev[5])
+    t = torch.tensor([t_plain, t_fwd, t_bwd], dtype=torch.float64, device=f"cuda:{local}")
+    if pg:
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    t_plain, t_fwd, t_bwd = (float(x) for x in t.tolist())
+    if rank == 0:
+        line = {
+            "metric": ADJ_METRIC, "value": t_bwd / t_plain, "unit": "reverse sweep time / plain forward time",
+            "n_gpus": ws, "steps": nsteps, "warmup": args.warmup, "ms_per_step": t_bwd / nsteps,
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded solenoidal k^4 exp(-2(k/4)^2) field, uniform rho and p)",
+            "config": {"workload": f"adjoint {n}^3, {nsteps} steps, checkpoint every {every}", "grid": n,
+                       "mach_t": mach, "reynolds": re, "dt": dt, "J": J},
+            "forward_ms_per_step": t_plain / nsteps, "checkpointed_forward_ms_per_step": t_fwd / nsteps,
+            "reverse_ms_per_step": t_bwd / nsteps,
+            "gradient_ratio_incl_forward": (t_fwd + t_bwd) / t_plain, "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    adj.close()
+    s.close()
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -386,7 +465,9 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", default="tgv", choices=["tgv", "ensemble"])
+    ap.add_argument("--workload", default="tgv", choices=["tgv", "ensemble", "adjoint"])
+    ap.add_argument("--adj-size", type=int, default=128)
+    ap.add_argument("--adj-steps", type=int, default=200)
     ap.add_argument("--no-single", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
@@ -396,6 +477,8 @@ def main():
         run_reference(args, ws, rank)
     elif args.workload == "ensemble":
         run_ensemble(args, ws, rank, local)
+    elif args.workload == "adjoint":
+        run_adjoint(args, ws, rank, local)
     else:
         run_ours(args, ws, rank, local)
 
