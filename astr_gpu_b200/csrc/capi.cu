@@ -263,8 +263,10 @@ cudaError_t run_rhs(astr_state* st, double* q) {
   a.q = q; a.DA = st->DA; a.DB = st->DB;
   if ((e = run_pass(st, CFG_C, a)) != cudaSuccess) return e;
   a = base_args(st, CFG_VA);
+  a.q = q;
   if ((e = run_pass(st, CFG_VA, a)) != cudaSuccess) return e;
   a = base_args(st, CFG_VB);
+  a.q = q;
   a.mode = 0;
   return run_pass(st, CFG_VB, a);
 }
@@ -300,6 +302,7 @@ cudaError_t run_step(astr_state* st, double dt, bool pending_at_start) {
       }
     }
     a = base_args(st, CFG_VA);
+    a.q = qin;
     if ((e = run_pass(st, CFG_VA, a)) != cudaSuccess) return e;
     a = base_args(st, CFG_VB);
     a.q = qin; a.qsave = st->Q0; a.qout = qout;
@@ -924,6 +927,7 @@ int ens_build(astr_ensemble* e) {
               case CFG_A: a.q = qin; a.D = st->DA; a.do_filter = filt && (s > 0 || variant == 1); break;
               case CFG_B: a.q = qin; a.D = st->DB; break;
               case CFG_C: a.q = qin; a.DA = st->DA; a.DB = st->DB; a.partials = (s == 0) ? st->partials : nullptr; break;
+              case CFG_VA: a.q = qin; break;
               case CFG_VB:
                 a.q = qin; a.qsave = st->Q0; a.qout = qout; a.mode = 1; a.do_filter = filt;
                 a.c1 = rk[s][0]; a.c2 = rk[s][1]; a.c3 = rk[s][2]; a.dt = e->dt[b];
@@ -1134,6 +1138,7 @@ cudaError_t run_stage_full(astr_state* st, int s, const double* qin, const doubl
   a.q = qi; a.DA = st->DA; a.DB = st->DB; a.partials = nullptr;
   if ((e = run_pass(st, CFG_C, a)) != cudaSuccess) return e;
   a = base_args(st, CFG_VA);
+  a.q = qi;
   if ((e = run_pass(st, CFG_VA, a)) != cudaSuccess) return e;
   a = base_args(st, CFG_VB);
   a.q = qi; a.qsave = qsave; a.qout = qout;

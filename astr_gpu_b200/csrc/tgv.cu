@@ -163,9 +163,9 @@ __global__ void k_pack(BoxGeo g, double* state, double* user, int64_t us0, int64
 
 int pass_tiles(int pass) {
   switch (pass) {
-    case PASS_A: case PASS_B: return 6;
+    case PASS_A: case PASS_B: return 5;
     case PASS_C: return 10;
-    case PASS_VA: return 4;
+    case PASS_VA: return 5;
     case PASS_VB: return 5;
     case PASS_F: return 5;
   }

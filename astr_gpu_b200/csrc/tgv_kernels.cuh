@@ -277,15 +277,78 @@ __device__ __forceinline__ void tile_specials(const LineOp& op, int TI, int LP, 
   compute_specials(op, TI, sp, count, [&](int l, int k, int n) { return base[k * stride + l * LP + HT + n]; });
 }
 
+// Euler flux along DIR at one node from the primitives (convection, tgvsolver.F90:559-564, with
+// q rebuilt by fvar2q): F0 = rho u_d, F_{1+j} = rho u_j u_d (+ p when j = d), F4 = (E + p) u_d.
+template <int DIR>
+__device__ __forceinline__ void euler_flux(double rho, double u, double v, double w, double p, const Thermo& th,
+                                           double (&F)[5]) {
+  const double ud = (DIR == 0) ? u : (DIR == 1 ? v : w);
+  F[0] = rho * ud;
+  F[1] = rho * u * ud;
+  F[2] = rho * v * ud;
+  F[3] = rho * w * ud;
+  F[1 + DIR] = F[1 + DIR] + p;
+  const double E = p * th.const6 + rho * (0.5 * (u * u + v * v + w * w));
+  F[4] = (E + p) * ud;
+}
+
+// Field of pass C's viscous-flux array VF holding (sigma_{DIR,0..2}, qflux_DIR)[k] for the
+// directions A and B (pass C stores sigma_A*, qflux_A, sigma_BB, sigma_BC, qflux_B).
+template <int DIR>
+__device__ __forceinline__ int vf_index(int k) {
+  if (DIR == DIR_A) return k;
+  return k == 3 ? 6 : (k == DIR_A ? DIR_B : (k == DIR_B ? 4 : 5));
+}
+
+// Tiles of primitives -> the 5 combined fluxes G_m = VF_{DIR,m} - F_{DIR,m} (VF_0 = 0) at every
+// staged node, halos included (VF read from the wrapped node, as bchomovec copies it).
+template <int DIR, int WPL>
+__device__ __forceinline__ void combine_flux_tiles(const TileCtx<DIR, WPL>& c, double* T, int tsz, const PassArgs& a) {
+  const double* VF = a.VF + c.sbase;
+  const int dim = c.dim;
+  const int64_t fs = a.g.fs;
+  c.for_nodes(-HT, dim + HT, [&](int o, int n) {
+    double vf[4] = {0.0, 0.0, 0.0, 0.0};
+    if (c.svalid) {
+      const int64_t off = (int64_t)wrap_node(n, dim) * c.sd;
+#pragma unroll
+      for (int k = 0; k < 4; ++k) vf[k] = __ldg(VF + vf_index<DIR>(k) * fs + off);
+    }
+    double F[5];
+    euler_flux<DIR>(T[o], T[tsz + o], T[2 * tsz + o], T[3 * tsz + o], T[4 * tsz + o], a.th, F);
+    T[o] = -F[0];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) T[(k + 1) * tsz + o] = vf[k] - F[k + 1];
+  });
+}
+
+// Store tiles [k0, k0 + nf) (nodes 0..dim of the slot line) to fields dst + m*fs (or add them).
+template <int DIR, int WPL, bool ADD>
+__device__ __forceinline__ void store_tiles(const TileCtx<DIR, WPL>& c, const double* T, int tsz, double* dst,
+                                            int64_t fs, int nf) {
+  if (!c.svalid) return;
+  double* d = dst + c.sbase;
+#pragma unroll 1
+  for (int m = 0; m < nf; ++m) {
+    double* dm = d + m * fs;
+    const double* Tm = T + m * tsz;
+    if (ADD) c.for_nodes_rmw<4>(0, c.dim, [&](int n) { return dm[(int64_t)n * c.sd]; },
+                                [&](int o, int n, double r) { dm[(int64_t)n * c.sd] = r + Tm[o]; });
+    else c.for_nodes(0, c.dim, [&](int o, int n) { dm[(int64_t)n * c.sd] = Tm[o]; });
+  }
+}
+
 // ------------------------------------------------------------------ pass A and pass B
+// Gradients of (u, v, w, T) along DIR into D (gradcal, tgvsolver.F90:450-537); pass A first
+// applies the filter along A still owed by the previous stage. Each solve writes its result over
+// the primitive tile it no longer needs (u, v, w -> themselves, T -> the pressure tile).
 template <int S, int WPL, int DIR, bool IS_A>
 __device__ __forceinline__ void k_pass_ab_body(const PassArgs& a, int bx, int by) {
   extern __shared__ double sm[];
   const TileCtx<DIR, WPL> c(a, bx, by);
   const int tsz = c.TI * c.LP;
   double* T = sm;
-  double* O = sm + 5 * tsz;
-  double* scan = O + tsz;
+  double* scan = sm + 5 * tsz;
   double* spb = scan + c.TI * SCAN_PER_LINE * WPL;   // closure tables
   const int64_t fs = a.g.fs;
   for (int m = 0; m < 5; ++m) load_tile(c, T + m * tsz, a.q + m * fs);
@@ -300,56 +363,38 @@ __device__ __forceinline__ void k_pass_ab_body(const PassArgs& a, int bx, int by
     __syncthreads();
     solve_lines<S, WPL>(T + z.l * c.LP + HT, tsz, 5, a.opf, z, scl, 1.0, true, spb + z.l * 5 * 2 * NSP);
     __syncthreads();
-    if (c.svalid) {
-      double* q = a.q + c.sbase;
-      c.for_nodes(0, dim, [&](int o, int n) {
-        const int64_t off = (int64_t)n * c.sd;
-#pragma unroll
-        for (int m = 0; m < 5; ++m) q[m * fs + off] = T[m * tsz + o];
-      });
-    }
+    store_tiles<DIR, WPL, false>(c, T, tsz, a.q, fs, 5);
     __syncthreads();   // every filtered value is stored before the tiles turn into primitives
   }
   to_prims(c, T, tsz, a.th);
   __syncthreads();
-  compute_specials(a.opd, c.TI, spb, 9, [&](int l, int k, int n) { return gprim_rt<DIR>(k, T + l * c.LP + HT, tsz, n, a.th); });
+  compute_specials(a.opd, c.TI, spb, 4, [&](int l, int k, int n) { return gprim_rt<DIR>(k, T + l * c.LP + HT, tsz, n, a.th); });
   __syncthreads();
-
   const double rd = a.g.rd[DIR];
   const double* L0 = T + z.l * c.LP + HT;
-  double* oline = O + z.l * c.LP + HT;
-  // stage one output in O and store it with the pass's epilogue
-  auto emit = [&](const double (&v)[S], int K) {
-    put_lane<S>(oline, v, z.seg, a.opd.ext_lo, dim, false);
-    __syncthreads();
-    if (c.svalid) {
-      double* dst = (K < 4) ? a.D + K * fs + c.sbase : a.R + (K - 4) * fs + c.sbase;
-      if (K < 4) c.for_nodes(0, dim, [&](int o, int n) { dst[(int64_t)n * c.sd] = O[o]; });
-      else if (IS_A) c.for_nodes(0, dim, [&](int o, int n) { dst[(int64_t)n * c.sd] = -O[o]; });
-      else c.for_nodes_rmw<4>(0, dim, [&](int n) { return dst[(int64_t)n * c.sd]; },
-                              [&](int o, int n, double r) { dst[(int64_t)n * c.sd] = r - O[o]; });
-    }
-    __syncthreads();
-  };
-  for (int K = 0; K < 9; ++K) {
+  for (int K = 0; K < 4; ++K) {
     double v[1][S];
-    dsolve_n<S, WPL, DIR, 1>(v, K, a, z, L0, tsz, scl, rd, spb + (z.l * 9 + K) * 2 * NSP);
-    emit(v[0], K);
+    dsolve_n<S, WPL, DIR, 1>(v, K, a, z, L0, tsz, scl, rd, spb + (z.l * 4 + K) * 2 * NSP);
+    put_lane<S>(T + (K + 1) * tsz + z.l * c.LP + HT, v[0], z.seg, a.opd.ext_lo, dim, false);
   }
+  __syncthreads();
+  store_tiles<DIR, WPL, false>(c, T + tsz, tsz, a.D, fs, 4);
 }
 
 // ------------------------------------------------------------------ pass C
+// Gradients along C, viscous stress and heat flux at every node (diffusion,
+// tgvsolver.F90:635-694) with the A and B gradients, the viscous fluxes of A and B stored for
+// passes A' and B', diagnostics, then R = D_C(VF_C - F_C) (the first contribution to R).
 template <int S, int WPL, int DIR>
 __device__ __forceinline__ void k_pass_c_body(const PassArgs& a, int bx, int by) {
   extern __shared__ double sm[];
   const TileCtx<DIR, WPL> c(a, bx, by);
   const int tsz = c.TI * c.LP;
   double* T = sm;
-  double* Dt = sm + 5 * tsz;
-  double* O = Dt + 4 * tsz;
-  double* scan = O + tsz;
-  double* spb = scan + c.TI * SCAN_PER_LINE * WPL;   // closure tables: 9 convective/gradient + 4 viscous
-  double* spv = spb + c.TI * 9 * 2 * NSP;
+  double* G = sm + 5 * tsz;   // 4 gradient tiles, then the 5 combined-flux tiles G1..G4, G0
+  double* scan = G + 5 * tsz;
+  double* spb = scan + c.TI * SCAN_PER_LINE * WPL;   // closure tables: 4 gradients, then 5 fluxes
+  double* spv = spb + c.TI * 4 * 2 * NSP;
   double* red = spb + c.TI * SP_PER_LINE;
   const int64_t fs = a.g.fs;
   for (int m = 0; m < 5; ++m) load_tile(c, T + m * tsz, a.q + m * fs);
@@ -358,7 +403,7 @@ __device__ __forceinline__ void k_pass_c_body(const PassArgs& a, int bx, int by)
   const int dim = c.dim;
   to_prims(c, T, tsz, a.th);
   __syncthreads();
-  compute_specials(a.opd, c.TI, spb, 9, [&](int l, int k, int n) { return gprim_rt<DIR>(k, T + l * c.LP + HT, tsz, n, a.th); });
+  compute_specials(a.opd, c.TI, spb, 4, [&](int l, int k, int n) { return gprim_rt<DIR>(k, T + l * c.LP + HT, tsz, n, a.th); });
   __syncthreads();
   const LaneIds z = lane_ids<WPL>();
   double* scl = scan + z.l * SCAN_PER_LINE * WPL;
@@ -368,12 +413,11 @@ __device__ __forceinline__ void k_pass_c_body(const PassArgs& a, int bx, int by)
   // gradients along C
   for (int K = 0; K < 4; ++K) {
     double v[1][S];
-    dsolve_n<S, WPL, DIR, 1>(v, K, a, z, L0, tsz, scl, rd, spb + (z.l * 9 + K) * 2 * NSP);
-    put_lane<S>(Dt + K * tsz + z.l * c.LP + HT, v[0], z.seg, a.opd.ext_lo, dim, false);
+    dsolve_n<S, WPL, DIR, 1>(v, K, a, z, L0, tsz, scl, rd, spb + (z.l * 4 + K) * 2 * NSP);
+    put_lane<S>(G + K * tsz + z.l * c.LP + HT, v[0], z.seg, a.opd.ext_lo, dim, false);
   }
   __syncthreads();
 
-  // sigma and heat flux at every node (diffusion, tgvsolver.F90:659-694)
   const Thermo th = a.th;
   constexpr int dA = DIR_A, dB = DIR_B, dC = DIR_C;
   static_assert(DIR == DIR_C, "pass C runs along DIR_C");
@@ -392,7 +436,7 @@ __device__ __forceinline__ void k_pass_c_body(const PassArgs& a, int bx, int by)
       for (int k = 0; k < 4; ++k) {
         gr[k][dA] = __ldg(DA + k * fs + off);
         gr[k][dB] = __ldg(DB + k * fs + off);
-        gr[k][dC] = Dt[k * tsz + tix];
+        gr[k][dC] = G[k * tsz + tix];
       }
       const double q0 = T[tix], u = T[tsz + tix], v = T[2 * tsz + tix], w = T[3 * tsz + tix], p = T[4 * tsz + tix];
       const double tmp = p / q0 * th.const2;
@@ -425,12 +469,15 @@ __device__ __forceinline__ void k_pass_c_body(const PassArgs& a, int bx, int by)
       VF[4 * fs + off] = sg[sidx(dB, dB)];
       VF[5 * fs + off] = sg[sidx(dB, dC)];
       VF[6 * fs + off] = qf[dB];
-      const double vc[4] = {sg[sidx(dC, 0)], sg[sidx(dC, 1)], sg[sidx(dC, 2)], qf[dC]};
+      // combined fluxes along C, with their periodic images
+      double F[5];
+      euler_flux<DIR>(q0, u, v, w, p, th, F);
+      const double gv[5] = {sg[sidx(dC, 0)] - F[1], sg[sidx(dC, 1)] - F[2], sg[sidx(dC, 2)] - F[3], qf[dC] - F[4], -F[0]};
 #pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        double* line = Dt + k * tsz + c.sl * c.LP + HT;
-        line[n] = vc[k];
-        put_images(line, n, dim, vc[k]);
+      for (int k = 0; k < 5; ++k) {
+        double* line = G + k * tsz + c.sl * c.LP + HT;
+        line[n] = gv[k];
+        put_images(line, n, dim, gv[k]);
       }
       if (diag && n >= 1 && row_ok) {
         // stacal (tgvsolver.F90:913-931) and diss_rate_cal (statistic.F90:1009-1034)
@@ -443,6 +490,12 @@ __device__ __forceinline__ void k_pass_c_body(const PassArgs& a, int bx, int by)
         di += 2.0 * miu * (s11 * s11 + s22 * s22 + s33 * s33 + 2.0 * (s12 * s12 + s13 * s13 + s23 * s23) -
                            (1.0 / 3.0) * (div * div));
       }
+    });
+  } else {
+    // lines past the box: finite filler for the solves (never stored)
+    c.for_nodes(-HT, dim + HT, [&](int tix, int) {
+#pragma unroll
+      for (int k = 0; k < 5; ++k) G[k * tsz + tix] = 0.0;
     });
   }
   if (bad) atomicOr(a.err, 1);
@@ -464,145 +517,102 @@ __device__ __forceinline__ void k_pass_c_body(const PassArgs& a, int bx, int by)
     double* pp = a.partials + 3 * ((int64_t)by * ntx + bx);
     pp[0] = s0; pp[1] = s1; pp[2] = s2;
   }
-
-  // viscous divergence along C (diffusion, tgvsolver.F90:763-787), kept in Dt
-  tile_specials(a.opd, c.TI, c.LP, Dt, tsz, 4, spv);
+  // R = D_C(VF_C - F_C): one solve per component (convection + diffusion, tgvsolver.F90:539-787)
+  tile_specials(a.opd, c.TI, c.LP, G, tsz, 5, spv);
   __syncthreads();
-  solve_lines<S, WPL>(Dt + z.l * c.LP + HT, tsz, 4, a.opd, z, scl, rd, false, spv + z.l * 4 * 2 * NSP);
-  // convection along C; R += visc_C - conv_C
-  double* oline = O + z.l * c.LP + HT;
-  auto emit = [&](const double (&v)[S], int m) {
-    put_lane<S>(oline, v, z.seg, a.opd.ext_lo, dim, false);
-    __syncthreads();
-    if (c.svalid) {
-      double* dst = a.R + m * fs + c.sbase;
-      if (m == 0) {
-        c.for_nodes_rmw<4>(0, dim, [&](int n) { return dst[(int64_t)n * c.sd]; },
-                           [&](int o, int n, double r) { dst[(int64_t)n * c.sd] = r - O[o]; });
-      } else {
-        const double* vis = Dt + (m - 1) * tsz;
-        c.for_nodes_rmw<4>(0, dim, [&](int n) { return dst[(int64_t)n * c.sd]; },
-                           [&](int o, int n, double r) { dst[(int64_t)n * c.sd] = r - O[o] + vis[o]; });
-      }
-    }
-    __syncthreads();
-  };
-  for (int K = 4; K < 9; ++K) {
-    double v[1][S];
-    dsolve_n<S, WPL, DIR, 1>(v, K, a, z, L0, tsz, scl, rd, spb + (z.l * 9 + K) * 2 * NSP);
-    emit(v[0], K - 4);
-  }
+  solve_lines<S, WPL>(G + z.l * c.LP + HT, tsz, 5, a.opd, z, scl, rd, false, spv + z.l * 5 * 2 * NSP);
+  __syncthreads();
+  store_tiles<DIR, WPL, false>(c, G, tsz, a.R + fs, fs, 4);
+  store_tiles<DIR, WPL, false>(c, G + 4 * tsz, tsz, a.R, fs, 1);
 }
 
-// ------------------------------------------------------------------ pass A' (visc along A)
+// ------------------------------------------------------------------ pass A' (fluxes along A)
+// R += D_A(VF_A - F_A).
 template <int S, int WPL, int DIR>
 __device__ __forceinline__ void k_pass_va_body(const PassArgs& a, int bx, int by) {
   extern __shared__ double sm[];
   const TileCtx<DIR, WPL> c(a, bx, by);
   const int tsz = c.TI * c.LP;
-  double* V = sm;
-  double* scan = sm + 4 * tsz;
+  double* T = sm;
+  double* scan = sm + 5 * tsz;
   double* spb = scan + c.TI * SCAN_PER_LINE * WPL;
   const int64_t fs = a.g.fs;
-  for (int k = 0; k < 4; ++k) load_tile(c, V + k * tsz, a.VF + k * fs);
+  for (int m = 0; m < 5; ++m) load_tile(c, T + m * tsz, a.q + m * fs);
   cp_async_wait_all();
   __syncthreads();
-  tile_specials(a.opd, c.TI, c.LP, V, tsz, 4, spb);
+  to_prims(c, T, tsz, a.th);
+  __syncthreads();
+  combine_flux_tiles(c, T, tsz, a);
+  __syncthreads();
+  tile_specials(a.opd, c.TI, c.LP, T, tsz, 5, spb);
   __syncthreads();
   const LaneIds z = lane_ids<WPL>();
   double* scl = scan + z.l * SCAN_PER_LINE * WPL;
-  const double rd = a.g.rd[DIR];
-  solve_lines<S, WPL>(V + z.l * c.LP + HT, tsz, 4, a.opd, z, scl, rd, false, spb + z.l * 4 * 2 * NSP);
+  solve_lines<S, WPL>(T + z.l * c.LP + HT, tsz, 5, a.opd, z, scl, a.g.rd[DIR], false, spb + z.l * 5 * 2 * NSP);
   __syncthreads();
-  if (c.svalid) {
-    double* R = a.R + c.sbase;
-#pragma unroll 1
-    for (int k = 0; k < 4; ++k) {
-      double* Rk = R + (1 + k) * fs;
-      const double* Vk = V + k * tsz;
-      c.for_nodes_rmw<4>(0, c.dim, [&](int n) { return Rk[(int64_t)n * c.sd]; },
-                         [&](int o, int n, double r) { Rk[(int64_t)n * c.sd] = r + Vk[o]; });
-    }
-  }
+  store_tiles<DIR, WPL, true>(c, T, tsz, a.R, fs, 5);
 }
 
-// ------------------------------------------------------------------ pass B' (visc along B, update, filter)
+// ------------------------------------------------------------------ pass B' (fluxes along B, update, filter)
+// R += D_B(VF_B - F_B); mode 1: q_out = F_B(c1 qsave + c2 q + c3 dt R) (rk3, tgvsolver.F90:1055-1057,
+// filterq along B); mode 0: R only.
 template <int S, int WPL, int DIR>
 __device__ __forceinline__ void k_pass_vb_body(const PassArgs& a, int bx, int by) {
   extern __shared__ double sm[];
   const TileCtx<DIR, WPL> c(a, bx, by);
   const int tsz = c.TI * c.LP;
-  double* V = sm;
-  double* O = sm + 4 * tsz;
-  double* scan = O + tsz;
-  double* spb = scan + c.TI * SCAN_PER_LINE * WPL;   // closure tables: 4 viscous + 1 filter
-  double* spf = spb + c.TI * 4 * 2 * NSP;
+  double* T = sm;
+  double* scan = sm + 5 * tsz;
+  double* spb = scan + c.TI * SCAN_PER_LINE * WPL;
   const int64_t fs = a.g.fs;
-  constexpr int dA = DIR_A, dB = DIR_B;
-  // viscous flux along B for momentum component k (physical) and energy: see pass C's VF layout
-  for (int k = 0; k < 4; ++k) {
-    const int vf = (k == 3) ? 6 : (k == dA ? dB : (k == dB ? 4 : 5));
-    load_tile(c, V + k * tsz, a.VF + vf * fs);
-  }
+  for (int m = 0; m < 5; ++m) load_tile(c, T + m * tsz, a.q + m * fs);
   cp_async_wait_all();
   __syncthreads();
-  tile_specials(a.opd, c.TI, c.LP, V, tsz, 4, spb);
+  to_prims(c, T, tsz, a.th);
+  __syncthreads();
+  combine_flux_tiles(c, T, tsz, a);
+  __syncthreads();
+  tile_specials(a.opd, c.TI, c.LP, T, tsz, 5, spb);
   __syncthreads();
   const LaneIds z = lane_ids<WPL>();
   double* scl = scan + z.l * SCAN_PER_LINE * WPL;
-  const double rd = a.g.rd[DIR];
+  solve_lines<S, WPL>(T + z.l * c.LP + HT, tsz, 5, a.opd, z, scl, a.g.rd[DIR], false, spb + z.l * 5 * 2 * NSP);
+  __syncthreads();
+  if (a.mode == 0) {
+    store_tiles<DIR, WPL, true>(c, T, tsz, a.R, fs, 5);
+    return;
+  }
+  // SSP-RK3 stage update of every field, with the periodic images for the filter
   const int dim = c.dim;
-  double* oline = O + z.l * c.LP + HT;
-  for (int m = 0; m < 5; ++m) {
-    if (m >= 1) {
-      const double* line = V + (m - 1) * tsz + z.l * c.LP + HT;
-      double v[S];
-      rhs_deriv<S>(v, a.opd, z.seg, [line](int n) { return line[n]; }, spb + (z.l * 4 + m - 1) * 2 * NSP);
-      seg_solve<S, WPL>(v, a.opd.tab, z.seg, z.lane, z.part, z.l, scl);
-#pragma unroll
-      for (int t = 0; t < S; ++t) v[t] *= rd;
-      put_lane<S>(oline, v, z.seg, a.opd.ext_lo, dim, false);
-    }
-    __syncthreads();
-    double* R = a.R + m * fs + c.sbase;
-    if (a.mode == 0) {
-      if (c.svalid)
-        c.for_nodes_rmw<4>(0, dim, [&](int n) { return R[(int64_t)n * c.sd]; },
-                           [&](int o, int n, double r) { R[(int64_t)n * c.sd] = r + ((m >= 1) ? O[o] : 0.0); });
-      __syncthreads();
-      continue;
-    }
-    // SSP-RK3 stage update, tgvsolver.F90:1055-1057
-    if (c.svalid) {
-      const double* qs = a.qsave + m * fs + c.sbase;
-      const double* qq = a.q + m * fs + c.sbase;
-      const double c1 = a.c1, c2 = a.c2, c3 = a.c3, dt = a.dt;
-      double* sline = O + c.sl * c.LP + HT;
+  if (c.svalid) {
+    const double c1 = a.c1, c2 = a.c2, c3 = a.c3, dt = a.dt;
+    const double* qs = a.qsave + c.sbase;
+    const double* qq = a.q + c.sbase;
+    const double* R = a.R + c.sbase;
+#pragma unroll 1
+    for (int m = 0; m < 5; ++m) {
+      double* Tm = T + m * tsz;
+      double* sline = Tm + c.sl * c.LP + HT;
       c.for_nodes(0, dim, [&](int o, int n) {
-        const int64_t off = (int64_t)n * c.sd;
-        const double vis = (m >= 1) ? O[o] : 0.0;
-        const double r = R[off] + vis;
+        const int64_t off = m * fs + (int64_t)n * c.sd;
+        const double r = R[off] + Tm[o];
         // (c1 qsave + c2 q) + (c3 qrhs) dt in the reference's order, rounded at every step so
         // that the result does not depend on how the compiler contracts this kernel
         const double qc = (c2 != 0.0) ? __dmul_rn(c2, qq[off]) : 0.0;
         const double qn = __dadd_rn(__dadd_rn(__dmul_rn(c1, qs[off]), qc), __dmul_rn(__dmul_rn(c3, r), dt));
-        O[o] = qn;
+        Tm[o] = qn;
         put_images(sline, n, dim, qn);
       });
     }
+  }
+  __syncthreads();
+  if (a.do_filter) {
+    tile_specials(a.opf, c.TI, c.LP, T, tsz, 5, spb);
     __syncthreads();
-    if (a.do_filter) {
-      tile_specials(a.opf, c.TI, c.LP, O, 0, 1, spf);
-      __syncthreads();
-      solve_lines<S, WPL>(oline, 0, 1, a.opf, z, scl, 1.0, false, spf + z.l * 2 * NSP);
-      __syncthreads();
-    }
-    if (c.svalid) {
-      double* qo = a.qout + m * fs + c.sbase;
-      c.for_nodes(0, dim, [&](int o, int n) { qo[(int64_t)n * c.sd] = O[o]; });
-    }
+    solve_lines<S, WPL>(T + z.l * c.LP + HT, tsz, 5, a.opf, z, scl, 1.0, false, spb + z.l * 5 * 2 * NSP);
     __syncthreads();
   }
+  store_tiles<DIR, WPL, false>(c, T, tsz, a.qout, fs, 5);
 }
 
 // ------------------------------------------------------------------ pass F (filter only, 5 fields)
@@ -624,14 +634,7 @@ __device__ __forceinline__ void k_pass_f_body(const PassArgs& a, int bx, int by)
   double* scl = scan + z.l * SCAN_PER_LINE * WPL;
   solve_lines<S, WPL>(T + z.l * c.LP + HT, tsz, 5, a.opf, z, scl, 1.0, false, spb + z.l * 5 * 2 * NSP);
   __syncthreads();
-  if (c.svalid) {
-    double* q = a.q + c.sbase;
-    c.for_nodes(0, c.dim, [&](int o, int n) {
-      const int64_t off = (int64_t)n * c.sd;
-#pragma unroll
-      for (int m = 0; m < 5; ++m) q[m * fs + off] = T[m * tsz + o];
-    });
-  }
+  store_tiles<DIR, WPL, false>(c, T, tsz, a.q, fs, 5);
 }
 
 // ------------------------------------------------------------------ kernels
