@@ -46,6 +46,25 @@ struct TileCtx {
     const int tix0 = sl * LP + HT;
     for (int n = n_lo + sn0; n <= n_hi; n += TPL) f(tix0 + n, n);
   }
+  // Two-phase form for work that reads global memory: ld(n) -> P for NB nodes first (their
+  // loads overlap), then use(tile offset, n, P) for the same nodes.
+  template <int NB, class P, class Ld, class Use>
+  __device__ __forceinline__ void for_nodes_batched(int n_lo, int n_hi, Ld ld, Use use) const {
+    const int tix0 = sl * LP + HT;
+    for (int nb = n_lo + sn0; nb <= n_hi; nb += NB * TPL) {
+      P r[NB];
+#pragma unroll
+      for (int b = 0; b < NB; ++b) {
+        const int n = nb + b * TPL;
+        if (n <= n_hi) r[b] = ld(n);
+      }
+#pragma unroll
+      for (int b = 0; b < NB; ++b) {
+        const int n = nb + b * TPL;
+        if (n <= n_hi) use(tix0 + n, n, r[b]);
+      }
+    }
+  }
   // Two-phase form for read-modify-write of global fields: ld(n) for NB nodes first (their loads
   // overlap), then st(tile offset, n, loaded value).
   template <int NB, class Ld, class St>
@@ -307,19 +326,26 @@ __device__ __forceinline__ void combine_flux_tiles(const TileCtx<DIR, WPL>& c, d
   const double* VF = a.VF + c.sbase;
   const int dim = c.dim;
   const int64_t fs = a.g.fs;
-  c.for_nodes(-HT, dim + HT, [&](int o, int n) {
-    double vf[4] = {0.0, 0.0, 0.0, 0.0};
-    if (c.svalid) {
-      const int64_t off = (int64_t)wrap_node(n, dim) * c.sd;
+  struct V4 { double v[4]; };
+  const bool ok = c.svalid;
+  c.template for_nodes_batched<2, V4>(
+      -HT, dim + HT,
+      [&](int n) {
+        V4 r{{0.0, 0.0, 0.0, 0.0}};
+        if (ok) {
+          const int64_t off = (int64_t)wrap_node(n, dim) * c.sd;
 #pragma unroll
-      for (int k = 0; k < 4; ++k) vf[k] = __ldg(VF + vf_index<DIR>(k) * fs + off);
-    }
-    double F[5];
-    euler_flux<DIR>(T[o], T[tsz + o], T[2 * tsz + o], T[3 * tsz + o], T[4 * tsz + o], a.th, F);
-    T[o] = -F[0];
+          for (int k = 0; k < 4; ++k) r.v[k] = __ldg(VF + vf_index<DIR>(k) * fs + off);
+        }
+        return r;
+      },
+      [&](int o, int, const V4& vf) {
+        double F[5];
+        euler_flux<DIR>(T[o], T[tsz + o], T[2 * tsz + o], T[3 * tsz + o], T[4 * tsz + o], a.th, F);
+        T[o] = -F[0];
 #pragma unroll
-    for (int k = 0; k < 4; ++k) T[(k + 1) * tsz + o] = vf[k] - F[k + 1];
-  });
+        for (int k = 0; k < 4; ++k) T[(k + 1) * tsz + o] = vf.v[k] - F[k + 1];
+      });
 }
 
 // Store tiles [k0, k0 + nf) (nodes 0..dim of the slot line) to fields dst + m*fs (or add them).
@@ -429,13 +455,20 @@ __device__ __forceinline__ void k_pass_c_body(const PassArgs& a, int bx, int by)
     const double* DB = a.DB + c.sbase;
     double* VF = a.VF + c.sbase;
     const bool row_ok = (bx * (int64_t)c.TI + c.sl) >= 1 && by >= 1;
-    c.for_nodes(0, dim, [&](int tix, int n) {
+    struct G8 { double ga[4], gb[4]; };
+    c.template for_nodes_batched<2, G8>(0, dim, [&](int n) {
+      const int64_t off = (int64_t)n * c.sd;
+      G8 r;
+#pragma unroll
+      for (int k = 0; k < 4; ++k) { r.ga[k] = __ldg(DA + k * fs + off); r.gb[k] = __ldg(DB + k * fs + off); }
+      return r;
+    }, [&](int tix, int n, const G8& gl) {
       const int64_t off = (int64_t)n * c.sd;
       double gr[4][3];
 #pragma unroll
       for (int k = 0; k < 4; ++k) {
-        gr[k][dA] = __ldg(DA + k * fs + off);
-        gr[k][dB] = __ldg(DB + k * fs + off);
+        gr[k][dA] = gl.ga[k];
+        gr[k][dB] = gl.gb[k];
         gr[k][dC] = G[k * tsz + tix];
       }
       const double q0 = T[tix], u = T[tsz + tix], v = T[2 * tsz + tix], w = T[3 * tsz + tix], p = T[4 * tsz + tix];
@@ -593,13 +626,16 @@ __device__ __forceinline__ void k_pass_vb_body(const PassArgs& a, int bx, int by
     for (int m = 0; m < 5; ++m) {
       double* Tm = T + m * tsz;
       double* sline = Tm + c.sl * c.LP + HT;
-      c.for_nodes(0, dim, [&](int o, int n) {
+      struct L3 { double r, s, q; };
+      c.template for_nodes_batched<4, L3>(0, dim, [&](int n) {
         const int64_t off = m * fs + (int64_t)n * c.sd;
-        const double r = R[off] + Tm[o];
+        return L3{R[off], qs[off], (c2 != 0.0) ? qq[off] : 0.0};
+      }, [&](int o, int n, const L3& l) {
+        const double r = l.r + Tm[o];
         // (c1 qsave + c2 q) + (c3 qrhs) dt in the reference's order, rounded at every step so
         // that the result does not depend on how the compiler contracts this kernel
-        const double qc = (c2 != 0.0) ? __dmul_rn(c2, qq[off]) : 0.0;
-        const double qn = __dadd_rn(__dadd_rn(__dmul_rn(c1, qs[off]), qc), __dmul_rn(__dmul_rn(c3, r), dt));
+        const double qc = (c2 != 0.0) ? __dmul_rn(c2, l.q) : 0.0;
+        const double qn = __dadd_rn(__dadd_rn(__dmul_rn(c1, l.s), qc), __dmul_rn(__dmul_rn(c3, r), dt));
         Tm[o] = qn;
         put_images(sline, n, dim, qn);
       });

@@ -236,7 +236,8 @@ def run_ours(args, ws, rank, local):
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (analytic Taylor-Green initial field)",
             "config": {"workload": f"TGV {n}^3 FP64 SSP-RK3 + compact filter, dt from CFL 0.5",
                        "grid": n, "dt": dt, "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",
-                       "l2": "inputs larger than L2 (5 x 1.1 GB state per box)", "graph": "one CUDA graph per step"},
+                       "l2": "inputs larger than L2 (5 x 1.1 GB state per box)", "graph": "one CUDA graph per step",
+                       "launch_shapes": {k: list(v) for k, v in s.launch_shapes().items()}},
             "roofline": roof, "step_roofline": step_roof, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": 19 * args.steps, "clocks": clk.summary(),
         }
