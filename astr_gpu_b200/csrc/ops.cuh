@@ -214,22 +214,22 @@ __device__ __forceinline__ double special_value(const LineOp& op, int r, Get f) 
   else deriv_special(op, r, f, s);
   return s;
 }
-// Index of row r in the closure table sp, or -1 for an interior row.
-__device__ __forceinline__ int special_slot(const LineOp& op, int r) {
-  if (r < op.spec_lo) return r;
-  if (r >= op.nsys - op.spec_hi) return NSP + r - (op.nsys - op.spec_hi);
-  return -1;
-}
 // Replace the closure rows of this lane by their precomputed values and zero its padding rows.
+// Only the first lanes of a line (start rows) and the lanes at or past the end rows branch in.
 template <int S>
 __device__ __forceinline__ void apply_specials(double (&v)[S], const LineOp& op, int r0, const double* sp) {
-  if (r0 < op.spec_lo || r0 + S > op.nsys - op.spec_hi) {
+  if (r0 < op.spec_lo) {
+#pragma unroll
+    for (int t = 0; t < S; ++t)
+      if (r0 + t < op.spec_lo) v[t] = sp[r0 + t];
+  }
+  const int e0 = op.nsys - op.spec_hi;   // first closure row at the end
+  if (r0 + S > e0) {
 #pragma unroll
     for (int t = 0; t < S; ++t) {
-      const int r = r0 + t;
-      const int k = special_slot(op, r);
-      if (r >= op.nsys) v[t] = 0.0;
-      else if (k >= 0) v[t] = sp[k];
+      const int k = r0 + t - e0;
+      if (k >= op.spec_hi) v[t] = 0.0;
+      else if (k >= 0) v[t] = sp[NSP + k];
     }
   }
 }

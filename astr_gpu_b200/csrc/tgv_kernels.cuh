@@ -110,10 +110,11 @@ __device__ __forceinline__ void load_tile(const TileCtx<DIR, WPL>& c, double* ti
 // halo images of those nodes.
 template <int S>
 __device__ __forceinline__ void put_lane(double* line, const double (&v)[S], int seg, int ext, int dim, bool images) {
+  const int n0 = seg * S - ext;
 #pragma unroll
   for (int t = 0; t < S; ++t) {
-    const int n = seg * S + t - ext;
-    if (n < 0 || n > dim) continue;
+    const int n = n0 + t;
+    if ((unsigned)n > (unsigned)dim) continue;   // outside nodes 0..dim
     line[n] = v[t];
     if (images) {
       if (n >= 1 && n <= HT) line[dim + n] = v[t];
