@@ -22,7 +22,7 @@ namespace adj_detail {
 using namespace pass_detail;
 
 // out(f) = alpha * L^T in(f) (+ out(f) when accumulating) for nf fields along DIR.
-template <int S, int WPL, int DIR>
+template <int S, int WPL, int DIR, int NB>
 __global__ void __launch_bounds__(512) k_adj_lines(AdjLineArgs a) {
   extern __shared__ double sm[];
   const TileCtx<DIR, WPL> c(a.p, blockIdx.x, blockIdx.y);
@@ -63,7 +63,7 @@ __global__ void __launch_bounds__(512) k_adj_lines(AdjLineArgs a) {
         if (n >= w.mlo && n <= w.mhi) {
           const double* y = T + o + w.jlo;
 #pragma unroll
-          for (int j = 0; j < ADJ_BAND; ++j) s = fma(w.wint[j], y[j], s);
+          for (int j = 0; j < NB; ++j) s = fma(w.wint[j], y[j], s);
         } else {
           const int k = n < w.mlo ? n : w.mlo + (n - w.mhi - 1);
           const double* y = T + o - n;
@@ -131,9 +131,14 @@ cudaError_t launch_adj_lines_t(const AdjLineArgs& a, cudaStream_t st) {
   dim3 grid((unsigned)((a.p.g.N[o1] + 1 + a.p.TI - 1) / a.p.TI), (unsigned)(a.p.g.N[o2] + 1));
   const int threads = a.p.TI * WPL * 32;
   const size_t smem = adj_lines_smem(a.p.TI, a.p.LP, WPL);
-  if (dir == 0) return launch_adj_k(adj_detail::k_adj_lines<S, WPL, 0>, grid, threads, smem, st, a);
-  if (dir == 1) return launch_adj_k(adj_detail::k_adj_lines<S, WPL, 1>, grid, threads, smem, st, a);
-  return launch_adj_k(adj_detail::k_adj_lines<S, WPL, 2>, grid, threads, smem, st, a);
+  const int nb = a.w.nint <= 5 ? 5 : (a.w.nint <= 11 ? 11 : ADJ_BAND);
+#define ASTR_ADJ_LINES(D, NB) \
+  if (dir == D && nb == NB) return launch_adj_k(adj_detail::k_adj_lines<S, WPL, D, NB>, grid, threads, smem, st, a);
+  ASTR_ADJ_LINES(0, 5) ASTR_ADJ_LINES(0, 11) ASTR_ADJ_LINES(0, ADJ_BAND)
+  ASTR_ADJ_LINES(1, 5) ASTR_ADJ_LINES(1, 11) ASTR_ADJ_LINES(1, ADJ_BAND)
+  ASTR_ADJ_LINES(2, 5) ASTR_ADJ_LINES(2, 11) ASTR_ADJ_LINES(2, ADJ_BAND)
+#undef ASTR_ADJ_LINES
+  return cudaErrorInvalidValue;
 }
 
 template <int S, int WPL>

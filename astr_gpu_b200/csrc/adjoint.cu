@@ -98,6 +98,15 @@ bool build_adjoint_op(const HostOp& fwd, AdjHostOp& out, std::string& err) {
   while (w.mlo > 0 && band_ok(w.mlo - 1, w.wint)) --w.mlo;
   w.mhi = mid;
   while (w.mhi < dim && band_ok(w.mhi + 1, w.wint)) ++w.mhi;
+  // trim the interior stencil to its nonzero span (5 points for the derivative, 11 for the filter)
+  int j0 = 0, j1 = ADJ_BAND - 1;
+  while (j0 < j1 && w.wint[j0] == 0.0) ++j0;
+  while (j1 > j0 && w.wint[j1] == 0.0) --j1;
+  double trimmed[ADJ_BAND] = {0.0};
+  for (int j = j0; j <= j1; ++j) trimmed[j - j0] = w.wint[j];
+  std::memcpy(w.wint, trimmed, sizeof(trimmed));
+  w.jlo += j0;
+  w.nint = j1 - j0 + 1;
   out.sptr.assign(1, 0);
   out.snode.clear();
   out.scoef.clear();

@@ -8,8 +8,8 @@ constexpr int ADJ_BAND = 17;   // interior stencil of W = E^T B^T: rows node-8 .
 
 // out(m) = sum_r W(m, r) y(r) of a transposed line operator, y indexed by node (= row - ext_lo).
 struct AdjW {
-  double wint[ADJ_BAND];   // interior nodes mlo..mhi: y(m + jlo + j), j = 0..ADJ_BAND-1
-  int jlo;
+  double wint[ADJ_BAND];   // interior nodes mlo..mhi: y(m + jlo + j), j = 0..nint-1
+  int jlo, nint;
   int mlo, mhi;
   const int* sptr;          // other nodes, k = m (m < mlo) or mlo + m - mhi - 1: entries sptr[k]..sptr[k+1]-1
   const int* snode;         // node index of y

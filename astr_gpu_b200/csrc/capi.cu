@@ -978,9 +978,11 @@ cudaError_t ens_run(astr_ensemble* e, int variant) {
   return cudaSuccess;
 }
 
-// Lines per CTA of each pass of each group: the largest power of two (<= 512 threads) whose
-// tiles fit in ~110 KB for every box of the group, then timed against half and double.
-int ens_tune(astr_ensemble* e) {
+// Lines per CTA of each pass of each group: start from the largest power of two (<= 512
+// threads) whose tiles fit in ~110 KB for every box of the group; with `timed`, also time the
+// batched launch of each pass at that width, half and a quarter of it on scratch copies of the
+// boxes' states (Q1) and keep the fastest.
+int ens_tune(astr_ensemble* e, bool timed) {
   astr_ctx* ctx = e->ctx;
   for (auto& g : e->groups) {
     for (int id = 0; id < NCFG; ++id) {
@@ -989,6 +991,75 @@ int ens_tune(astr_ensemble* e) {
       g.TI[id] = std::max(ti, 1);
     }
   }
+  if (!timed) return ASTR_OK;
+  cudaStream_t sm = ctx->stream;
+  for (astr_state* st : e->boxes)
+    CK(cudaMemcpyAsync(st->Q1, st->Q0, 5 * (size_t)st->g.fs * sizeof(double), cudaMemcpyDeviceToDevice, sm));
+  PassArgs* dargs = nullptr;
+  int* dcum = nullptr;
+  CK(cudaMalloc(&dargs, e->boxes.size() * sizeof(PassArgs)));
+  CK(cudaMalloc(&dcum, e->boxes.size() * sizeof(int)));
+  cudaEvent_t t0, t1;
+  cudaEventCreate(&t0);
+  cudaEventCreate(&t1);
+  const int ids[6] = {CFG_A, CFG_B, CFG_C, CFG_VA, CFG_VB, CFG_FC};
+  for (auto& g : e->groups) {
+    for (int id : ids) {
+      const int ti0 = g.TI[id];
+      float best = 1e30f;
+      int best_ti = ti0;
+      for (int ti : {ti0, ti0 / 2, ti0 / 4}) {
+        if (ti < 1) continue;
+        std::vector<PassArgs> ha;
+        std::vector<int> hc;
+        int ctas = 0;
+        size_t smem = 0;
+        for (int b : g.members) {
+          astr_state* st = e->boxes[b];
+          const int dir = CFG_DIR[id];
+          const PassCfg saved = st->cfg[id];
+          PassCfg c;
+          c.S = g.S; c.WPL = g.WPL; c.TI = ti; c.LP = tile_pitch(st->g.N[dir], ti);
+          st->cfg[id] = c;
+          PassArgs a = base_args(st, id);
+          st->cfg[id] = saved;
+          a.q = st->Q1; a.D = st->DA; a.DA = st->DA; a.DB = st->DB; a.partials = nullptr;
+          a.qsave = st->Q1; a.qout = st->Q1; a.mode = 1; a.do_filter = st->p.filter_on;
+          a.c1 = 1.0; a.c2 = 0.0; a.c3 = 0.0; a.dt = 0.0;
+          ha.push_back(a);
+          hc.push_back(ctas);
+          const int o1 = (dir == 0) ? 1 : 0, o2 = (dir == 2) ? 1 : 2;
+          ctas += ((st->g.N[o1] + 1 + ti - 1) / ti) * (st->g.N[o2] + 1);
+          smem = std::max(smem, pass_shared_bytes(CFG_PASS[id], ti, c.LP, g.WPL));
+        }
+        CK(cudaMemcpyAsync(dargs, ha.data(), ha.size() * sizeof(PassArgs), cudaMemcpyHostToDevice, sm));
+        CK(cudaMemcpyAsync(dcum, hc.data(), hc.size() * sizeof(int), cudaMemcpyHostToDevice, sm));
+        const int threads = ti * g.WPL * 32;
+        float ms = 1e30f;
+        cudaError_t err = launch_pass_batch(CFG_PASS[id], CFG_DIR[id], g.S, g.WPL, dargs, dcum, (int)ha.size(), ctas,
+                                            threads, smem, sm);
+        if (err == cudaSuccess) {
+          cudaEventRecord(t0, sm);
+          for (int r = 0; r < 2 && err == cudaSuccess; ++r)
+            err = launch_pass_batch(CFG_PASS[id], CFG_DIR[id], g.S, g.WPL, dargs, dcum, (int)ha.size(), ctas, threads,
+                                    smem, sm);
+          cudaEventRecord(t1, sm);
+          cudaEventSynchronize(t1);
+          cudaEventElapsedTime(&ms, t0, t1);
+        }
+        if (err != cudaSuccess) { cudaGetLastError(); ms = 1e30f; }   // a width the device cannot launch
+        if (ms < best) { best = ms; best_ti = ti; }
+      }
+      g.TI[id] = best_ti;
+    }
+  }
+  cudaEventDestroy(t0);
+  cudaEventDestroy(t1);
+  cudaFree(dargs);
+  cudaFree(dcum);
+  for (astr_state* st : e->boxes) CK(cudaMemsetAsync(st->err, 0, sizeof(int), sm));
+  CK(cudaStreamSynchronize(sm));
+  e->tuned = true;
   return ASTR_OK;
 }
 
@@ -1020,7 +1091,7 @@ int astr_ensemble_create(astr_ctx* ctx, astr_state* const* boxes, int nbox, astr
       e->groups.push_back(g);
     }
   }
-  ens_tune(e);
+  ens_tune(e, false);
   *out = e;
   return ASTR_OK;
 }
@@ -1050,6 +1121,11 @@ int astr_ensemble_step(astr_ensemble* e, const double* dt, int nsteps) {
   if (!all_pending)
     for (int b = 0; b < nbox; ++b) CK(finalize_filter(e->boxes[b]));
   e->pending = all_pending;
+  if (!e->tuned && nsteps > 0) {
+    int rc = ens_tune(e, true);
+    if (rc) return rc;
+    changed = true;
+  }
   if (changed) {
     e->dt.assign(dt, dt + nbox);
     ens_drop_graphs(e);
@@ -1105,6 +1181,7 @@ struct astr_adjoint {
          *lsave = nullptr, *U = nullptr, *lp = nullptr, *LG = nullptr, *part = nullptr, *jval = nullptr;
   std::vector<double*> ckpt;    // state at steps 0, every, 2*every, ...
   double* seg = nullptr;        // stage inputs of one segment: every x 3 states
+  double* gstore = nullptr;     // their gradients (every x 3 x 12 fields) when memory allows
   int nsteps = 0;
   double dt = 0.0;
   double J = 0.0;
@@ -1121,21 +1198,30 @@ void adj_free(astr_adjoint* a) {
   a->ckpt.clear();
   if (a->seg) cudaFree(a->seg);
   a->seg = nullptr;
+  if (a->gstore) cudaFree(a->gstore);
+  a->gstore = nullptr;
 }
 
-// One RK3 stage with every filter applied: qout = F(c1 qsave + c2 qin + c3 dt rhs(qin)).
-cudaError_t run_stage_full(astr_state* st, int s, const double* qin, const double* qsave, double* qout, double dt) {
+// One RK3 stage with every filter applied: qout = F(c1 qsave + c2 qin + c3 dt rhs(qin)). With G,
+// the velocity/temperature gradients of qin go to G[4d + k] (physical direction d, as the
+// adjoint's gradient kernel lays them out).
+cudaError_t run_stage_full(astr_state* st, int s, const double* qin, const double* qsave, double* qout, double dt,
+                           double* G = nullptr) {
   static const double rk[3][3] = {{1.0, 0.0, 1.0}, {0.75, 0.25, 0.25}, {1.0 / 3.0, 2.0 / 3.0, 2.0 / 3.0}};
   double* qi = const_cast<double*>(qin);
+  const int64_t fs = st->g.fs;
+  double* DA = G ? G + 4 * DIR_A * fs : st->DA;
+  double* DB = G ? G + 4 * DIR_B * fs : st->DB;
   cudaError_t e;
   PassArgs a = base_args(st, CFG_A);
-  a.q = qi; a.D = st->DA; a.do_filter = 0;
+  a.q = qi; a.D = DA; a.do_filter = 0;
   if ((e = run_pass(st, CFG_A, a)) != cudaSuccess) return e;
   a = base_args(st, CFG_B);
-  a.q = qi; a.D = st->DB;
+  a.q = qi; a.D = DB;
   if ((e = run_pass(st, CFG_B, a)) != cudaSuccess) return e;
   a = base_args(st, CFG_C);
-  a.q = qi; a.DA = st->DA; a.DB = st->DB; a.partials = nullptr;
+  a.q = qi; a.DA = DA; a.DB = DB; a.partials = nullptr;
+  a.DC = G ? G + 4 * DIR_C * fs : nullptr;
   if ((e = run_pass(st, CFG_C, a)) != cudaSuccess) return e;
   a = base_args(st, CFG_VA);
   a.q = qi;
@@ -1202,7 +1288,8 @@ cudaError_t adj_grad(astr_adjoint* A, int dir, const double* q, double* D) {
 }
 
 // lam <- (d q_out / d q_in)^T lam for one RK3 step whose stage inputs are S0, S1, S2.
-cudaError_t adj_step(astr_adjoint* A, const double* S0, const double* S1, const double* S2) {
+cudaError_t adj_step(astr_adjoint* A, const double* S0, const double* S1, const double* S2,
+                     const double* const* Gs = nullptr) {
   static const double rk[3][3] = {{1.0, 0.0, 1.0}, {0.75, 0.25, 0.25}, {1.0 / 3.0, 2.0 / 3.0, 2.0 / 3.0}};
   astr_state* st = A->st;
   cudaStream_t sm = st->ctx->stream;
@@ -1222,12 +1309,13 @@ cudaError_t adj_step(astr_adjoint* A, const double* S0, const double* S1, const 
       if ((e = cudaMemcpyAsync(A->lnew, A->lam, 5 * fs * sizeof(double), cudaMemcpyDeviceToDevice, sm)) != cudaSuccess)
         return e;
     }
+    const double* Gq = Gs ? Gs[s] : A->G;
     for (int d = 0; d < 3; ++d) {
-      if ((e = adj_grad(A, d, qs, A->G + 4 * d * fs)) != cudaSuccess) return e;
+      if (!Gs && (e = adj_grad(A, d, qs, A->G + 4 * d * fs)) != cudaSuccess) return e;
       if ((e = adj_lines(A, d, false, A->lnew, A->Y + 5 * d * fs, 5, c3 * A->dt * st->g.rd[d], false)) != cudaSuccess)
         return e;
     }
-    if ((e = launch_adj_point1(st->g, st->th, qs, A->G, A->Y, A->lnew, c1, c2, A->lsave, A->lq, A->U, A->lp, A->LG,
+    if ((e = launch_adj_point1(st->g, st->th, qs, Gq, A->Y, A->lnew, c1, c2, A->lsave, A->lq, A->U, A->lp, A->LG,
                                sm)) != cudaSuccess)
       return e;
     for (int d = 0; d < 3; ++d)
@@ -1273,6 +1361,13 @@ int adj_setup(astr_adjoint* A) {
   A->part = p;
   A->jval = p + (st->g.N[2] + 1);
   CK(cudaMalloc(&A->seg, (size_t)A->every * 3 * 5 * fs * sizeof(double)));
+  // keep the stage gradients of a segment from its recomputation when they fit in a quarter of
+  // the free memory; otherwise the reverse sweep recomputes them stage by stage
+  size_t free_b = 0, total_b = 0;
+  const size_t need = (size_t)A->every * 3 * 12 * fs * sizeof(double);
+  if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess && need < free_b / 4) {
+    if (cudaMalloc(&A->gstore, need) != cudaSuccess) { cudaGetLastError(); A->gstore = nullptr; }
+  }
   return ASTR_OK;
 }
 
@@ -1342,13 +1437,22 @@ int astr_adjoint_backward(astr_adjoint* A, double* grad, const int64_t shape[3],
     const int s0 = j * A->every;
     const int len = std::min(A->every, A->nsteps - s0);
     auto stage = [&](int n, int s) { return A->seg + ((size_t)n * 3 + s) * 5 * fs; };
+    auto grads = [&](int n, int s) -> double* {
+      return A->gstore ? A->gstore + ((size_t)n * 3 + s) * 12 * fs : nullptr;
+    };
     CK(cudaMemcpyAsync(stage(0, 0), A->ckpt[j], qb, cudaMemcpyDeviceToDevice, sm));
     for (int n = 0; n < len; ++n) {
-      CK(run_stage_full(st, 0, stage(n, 0), stage(n, 0), stage(n, 1), A->dt));
-      CK(run_stage_full(st, 1, stage(n, 1), stage(n, 0), stage(n, 2), A->dt));
-      if (n + 1 < len) CK(run_stage_full(st, 2, stage(n, 2), stage(n, 0), stage(n + 1, 0), A->dt));
+      CK(run_stage_full(st, 0, stage(n, 0), stage(n, 0), stage(n, 1), A->dt, grads(n, 0)));
+      CK(run_stage_full(st, 1, stage(n, 1), stage(n, 0), stage(n, 2), A->dt, grads(n, 1)));
+      // the last stage's output is the next step's input; with stored gradients the last step
+      // still runs it for them
+      if (n + 1 < len) CK(run_stage_full(st, 2, stage(n, 2), stage(n, 0), stage(n + 1, 0), A->dt, grads(n, 2)));
+      else if (A->gstore) CK(run_stage_full(st, 2, stage(n, 2), stage(n, 0), A->t1, A->dt, grads(n, 2)));
     }
-    for (int n = len - 1; n >= 0; --n) CK(adj_step(A, stage(n, 0), stage(n, 1), stage(n, 2)));
+    for (int n = len - 1; n >= 0; --n) {
+      const double* Gs[3] = {grads(n, 0), grads(n, 1), grads(n, 2)};
+      CK(adj_step(A, stage(n, 0), stage(n, 1), stage(n, 2), A->gstore ? Gs : nullptr));
+    }
   }
   int rc = copy_fields(st, A->lam, grad, shape, lbound, 0, where);
   if (rc) return rc;

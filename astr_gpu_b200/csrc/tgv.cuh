@@ -41,6 +41,7 @@ struct PassArgs {
   int mode;                 // pass B': 0 = only R += visc_B, 1 = RK update (+ filter)
   double c1, c2, c3, dt;    // SSP-RK3 stage coefficients (mainloop.F90:350-360)
   double* partials;         // pass C at the first stage: per-CTA (tke, enstrophy, dissipation)
+  double* DC;               // pass C, optional: its 4 gradients along C are also stored here
   int* err;                 // device error word: bit 0 = non-finite or non-positive density
 };
 

@@ -444,6 +444,10 @@ __device__ __forceinline__ void k_pass_c_body(const PassArgs& a, int bx, int by)
     put_lane<S>(G + K * tsz + z.l * c.LP + HT, v[0], z.seg, a.opd.ext_lo, dim, false);
   }
   __syncthreads();
+  if (a.DC) {   // kept for the discrete adjoint
+    store_tiles<DIR, WPL, false>(c, G, tsz, a.DC, fs, 4);
+    __syncthreads();
+  }
 
   const Thermo th = a.th;
   constexpr int dA = DIR_A, dB = DIR_B, dC = DIR_C;
