@@ -455,6 +455,23 @@ def run_adjoint(args, ws, rank, local):
         pg.destroy_process_group()
 
 
+def run_profile(args, local):
+    """The workload for an ncu capture: `--steps` eager RK3 steps of a TGV box (no graph, no
+    timing, no JSON line), with the pass launch shapes pinned by `--shapes`."""
+    import astr_gpu_b200 as ag
+    ctx = ag.Context(local)
+    s = ag.TGVSolver(ctx, args.size)
+    if args.shapes:
+        for nm, v in json.loads(args.shapes).items():
+            s.set_launch_shape(nm, *v[:3])
+    s.init_tgv()
+    dt = s.cfl_dt(0.5)
+    s.use_graph(False)
+    s.rk3(dt, args.steps)
+    ctx.synchronize()
+    print(json.dumps({"profiled_steps": args.steps, "grid": args.size, "launch_shapes": s.launch_shapes()}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -471,11 +488,15 @@ def main():
     ap.add_argument("--adj-size", type=int, default=128)
     ap.add_argument("--adj-steps", type=int, default=200)
     ap.add_argument("--no-single", action="store_true")
+    ap.add_argument("--profile", action="store_true", help="eager steps only, for ncu captures")
+    ap.add_argument("--shapes", default="", help='pinned launch shapes, e.g. {"A": [9, 2, 8], ...}')
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         print("warning: fewer than 3 warm-up steps", file=sys.stderr)
     ws, rank, local = dist_setup(args)
-    if args.impl == "reference":
+    if args.profile:
+        run_profile(args, local)
+    elif args.impl == "reference":
         run_reference(args, ws, rank)
     elif args.workload == "ensemble":
         run_ensemble(args, ws, rank, local)
