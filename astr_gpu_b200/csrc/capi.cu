@@ -121,7 +121,7 @@ int pick_ti(int pass, int dim, int WPL, size_t budget = 110 * 1024) {
 }
 
 // Solve layouts compiled into the library (tgv_l*.cu, lines.cu).
-const Layout kLayouts[] = {{3, 1}, {5, 1}, {9, 1}, {5, 2}, {9, 2}, {5, 4}, {9, 4}};
+const Layout kLayouts[] = {{3, 1}, {5, 1}, {9, 1}, {5, 2}, {9, 2}, {5, 4}, {9, 4}, {17, 1}};
 
 bool covers(const int64_t* shape, const int64_t* lb, int d, int64_t lo, int64_t hi) {
   return lb[d] <= lo && lb[d] + shape[d] - 1 >= hi;

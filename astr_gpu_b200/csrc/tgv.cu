@@ -182,7 +182,7 @@ cudaError_t launch_pass_batch(int pass, int dir, int S, int WPL, const PassArgs*
                               int nctas, int threads, size_t smem, cudaStream_t st) {
 #define ASTR_B(s_, w_) \
   if (S == s_ && WPL == w_) return launch_pass_batch_t<s_, w_>(pass, dir, dargs, dcum, nbox, nctas, threads, smem, st);
-  ASTR_B(3, 1) ASTR_B(5, 1) ASTR_B(5, 2) ASTR_B(5, 4) ASTR_B(9, 1) ASTR_B(9, 2) ASTR_B(9, 4)
+  ASTR_B(3, 1) ASTR_B(5, 1) ASTR_B(5, 2) ASTR_B(5, 4) ASTR_B(9, 1) ASTR_B(9, 2) ASTR_B(9, 4) ASTR_B(17, 1)
 #undef ASTR_B
   return cudaErrorInvalidValue;
 }
@@ -200,7 +200,9 @@ cudaError_t launch_pass(int pass, const PassArgs& a, int S, int WPL, cudaStream_
   if (S == 5 && WPL == 4) return launch_pass_t<5, 4>(pass, a, st);
   if (S == 9 && WPL == 1) return launch_pass_t<9, 1>(pass, a, st);
   if (S == 9 && WPL == 2) return launch_pass_t<9, 2>(pass, a, st);
+
   if (S == 9 && WPL == 4) return launch_pass_t<9, 4>(pass, a, st);
+  if (S == 17 && WPL == 1) return launch_pass_t<17, 1>(pass, a, st);
   return cudaErrorInvalidValue;
 }
 

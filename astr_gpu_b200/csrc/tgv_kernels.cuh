@@ -94,16 +94,43 @@ __device__ __forceinline__ void cp_async_wait_all() {
   asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
 }
 
+__device__ __forceinline__ void cp_async16(uint32_t sdst, const double* gsrc) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sdst), "l"(gsrc) : "memory");
+}
+
 // Stage the slot line of one field, nodes -HT..dim+HT with the periodic wrap, asynchronously.
+// The node progression of each thread runs through the low halo, the line and the high halo
+// with the wrap applied per range; x lines (contiguous) copy node pairs with 16-byte copies
+// when the line and the tile row start on 16-byte boundaries.
 template <int DIR, int WPL>
 __device__ __forceinline__ void load_tile(const TileCtx<DIR, WPL>& c, double* tile, const double* __restrict__ fld) {
-  const double* src = fld + c.sbase;
   const int dim = c.dim;
-  if (c.svalid) {
-    c.for_nodes(-HT, dim + HT, [&](int tix, int n) { cp_async8(tile + tix, src + (int64_t)wrap_node(n, dim) * c.sd); });
-  } else {
+  double* trow = tile + c.sl * c.LP + HT;   // node 0 of the slot line
+  if (!c.svalid) {
     c.for_nodes(-HT, dim + HT, [&](int tix, int n) { tile[tix] = 1.0; });   // finite filler, never stored
+    return;
   }
+  const double* src = fld + c.sbase;
+  const uint32_t s0 = (uint32_t)__cvta_generic_to_shared(trow);
+  constexpr int TPL = TileCtx<DIR, WPL>::TPL;
+  if (DIR == 0 && ((dim & 1) == 0) && ((c.LP & 1) == 0) && ((s0 & 15u) == 0)) {
+    // pairs (n, n+1), n even, from -HT to dim+HT-1; then node dim+HT alone
+    int n = -HT + 2 * c.sn0;
+    for (; n < 0; n += 2 * TPL) cp_async16(s0 + 8 * n, src + (n + dim));
+    for (; n + 1 <= dim; n += 2 * TPL) cp_async16(s0 + 8 * n, src + n);
+    for (; n < dim + HT; n += 2 * TPL) {
+      // the pair (dim, dim+1) straddles the wrap: node dim, then node 1
+      if (n == dim) { cp_async8(trow + n, src + n); cp_async8(trow + n + 1, src + 1); }
+      else cp_async16(s0 + 8 * n, src + (n - dim));
+    }
+    if (c.sn0 == 0) cp_async8(trow + dim + HT, src + HT);
+    return;
+  }
+  const int64_t sd = c.sd;
+  int n = -HT + c.sn0;
+  for (; n < 0; n += TPL) cp_async8(trow + n, src + (int64_t)(n + dim) * sd);
+  for (; n <= dim; n += TPL) cp_async8(trow + n, src + (int64_t)n * sd);
+  for (; n <= dim + HT; n += TPL) cp_async8(trow + n, src + (int64_t)(n - dim) * sd);
 }
 
 // Write a lane's solution rows (nodes 0..dim) into a tile line, optionally with the periodic
@@ -350,18 +377,41 @@ __device__ __forceinline__ void combine_flux_tiles(const TileCtx<DIR, WPL>& c, d
 }
 
 // Store tiles [k0, k0 + nf) (nodes 0..dim of the slot line) to fields dst + m*fs (or add them).
+// x lines store node pairs with 16-byte accesses when aligned.
 template <int DIR, int WPL, bool ADD>
 __device__ __forceinline__ void store_tiles(const TileCtx<DIR, WPL>& c, const double* T, int tsz, double* dst,
                                             int64_t fs, int nf) {
   if (!c.svalid) return;
   double* d = dst + c.sbase;
+  const int dim = c.dim;
+  constexpr int TPL = TileCtx<DIR, WPL>::TPL;
+  const int row = c.sl * c.LP + HT;
+  if (DIR == 0 && ((c.LP & 1) == 0) && ((reinterpret_cast<uintptr_t>(T + row) & 15u) == 0)) {
+#pragma unroll 1
+    for (int m = 0; m < nf; ++m) {
+      double* dm = d + m * fs;
+      const double* Tm = T + m * tsz + row;
+      int n = 2 * c.sn0;
+      for (; n + 1 <= dim; n += 2 * TPL) {
+        double2 v = *reinterpret_cast<const double2*>(Tm + n);
+        if (ADD) {
+          const double2 r = *reinterpret_cast<const double2*>(dm + n);
+          v.x += r.x;
+          v.y += r.y;
+        }
+        *reinterpret_cast<double2*>(dm + n) = v;
+      }
+      if (n == dim) dm[n] = ADD ? dm[n] + Tm[n] : Tm[n];   // odd node count: the last node alone
+    }
+    return;
+  }
 #pragma unroll 1
   for (int m = 0; m < nf; ++m) {
     double* dm = d + m * fs;
     const double* Tm = T + m * tsz;
-    if (ADD) c.for_nodes_rmw<4>(0, c.dim, [&](int n) { return dm[(int64_t)n * c.sd]; },
+    if (ADD) c.for_nodes_rmw<4>(0, dim, [&](int n) { return dm[(int64_t)n * c.sd]; },
                                 [&](int o, int n, double r) { dm[(int64_t)n * c.sd] = r + Tm[o]; });
-    else c.for_nodes(0, c.dim, [&](int o, int n) { dm[(int64_t)n * c.sd] = Tm[o]; });
+    else c.for_nodes(0, dim, [&](int o, int n) { dm[(int64_t)n * c.sd] = Tm[o]; });
   }
 }
 
