@@ -567,8 +567,8 @@ int astr_state_create(astr_ctx* ctx, const astr_params* p, astr_state** out) {
   }
   // a small box gains nothing from tuning
   st->autotune = (N[0] + 1) * (int64_t)(N[1] + 1) * (N[2] + 1) >= 100 * 100 * 100;
-  // 30 fields: Q0(5) Q1(5) R(5) DA(4) DB(4) VF(7)
-  const size_t nf = 30;
+  // 33 fields: Q0(5) Q1(5) R(5) DA(4) DB(4) VF(10: the combined fluxes along A and along B)
+  const size_t nf = 33;
   cudaError_t e = cudaMalloc(&st->buf, nf * (size_t)st->g.fs * sizeof(double));
   if (e != cudaSuccess) { delete st; return fail(ctx, ASTR_ERR_NOMEM, "state allocation"); }
   cudaMemsetAsync(st->buf, 0, nf * (size_t)st->g.fs * sizeof(double), ctx->stream);

@@ -36,7 +36,7 @@ struct PassArgs {
   double* D;                // 4 fields: du, dv, dw, dT along this direction (A and B passes)
   const double* DA;         // 4 fields read by pass C
   const double* DB;
-  double* VF;               // 7 viscous-flux fields written by pass C, read by passes A' and B'
+  double* VF;               // 10 fields written by pass C: G_A = VF_A - F_A (5), then G_B (5)
   int do_filter;
   int mode;                 // pass B': 0 = only R += visc_B, 1 = RK update (+ filter)
   double c1, c2, c3, dt;    // SSP-RK3 stage coefficients (mainloop.F90:350-360)

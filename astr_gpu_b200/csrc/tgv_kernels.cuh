@@ -339,43 +339,6 @@ __device__ __forceinline__ void euler_flux(double rho, double u, double v, doubl
   F[4] = (E + p) * ud;
 }
 
-// Field of pass C's viscous-flux array VF holding (sigma_{DIR,0..2}, qflux_DIR)[k] for the
-// directions A and B (pass C stores sigma_A*, qflux_A, sigma_BB, sigma_BC, qflux_B).
-template <int DIR>
-__device__ __forceinline__ int vf_index(int k) {
-  if (DIR == DIR_A) return k;
-  return k == 3 ? 6 : (k == DIR_A ? DIR_B : (k == DIR_B ? 4 : 5));
-}
-
-// Tiles of primitives -> the 5 combined fluxes G_m = VF_{DIR,m} - F_{DIR,m} (VF_0 = 0) at every
-// staged node, halos included (VF read from the wrapped node, as bchomovec copies it).
-template <int DIR, int WPL>
-__device__ __forceinline__ void combine_flux_tiles(const TileCtx<DIR, WPL>& c, double* T, int tsz, const PassArgs& a) {
-  const double* VF = a.VF + c.sbase;
-  const int dim = c.dim;
-  const int64_t fs = a.g.fs;
-  struct V4 { double v[4]; };
-  const bool ok = c.svalid;
-  c.template for_nodes_batched<2, V4>(
-      -HT, dim + HT,
-      [&](int n) {
-        V4 r{{0.0, 0.0, 0.0, 0.0}};
-        if (ok) {
-          const int64_t off = (int64_t)wrap_node(n, dim) * c.sd;
-#pragma unroll
-          for (int k = 0; k < 4; ++k) r.v[k] = __ldg(VF + vf_index<DIR>(k) * fs + off);
-        }
-        return r;
-      },
-      [&](int o, int, const V4& vf) {
-        double F[5];
-        euler_flux<DIR>(T[o], T[tsz + o], T[2 * tsz + o], T[3 * tsz + o], T[4 * tsz + o], a.th, F);
-        T[o] = -F[0];
-#pragma unroll
-        for (int k = 0; k < 4; ++k) T[(k + 1) * tsz + o] = vf.v[k] - F[k + 1];
-      });
-}
-
 // Store tiles [k0, k0 + nf) (nodes 0..dim of the slot line) to fields dst + m*fs (or add them).
 // x lines store node pairs with 16-byte accesses when aligned.
 template <int DIR, int WPL, bool ADD>
@@ -550,13 +513,22 @@ __device__ __forceinline__ void k_pass_c_body(const PassArgs& a, int bx, int by)
       qf[0] = hcc * gr[3][0] + sg[0] * u + sg[1] * v + sg[2] * w;
       qf[1] = hcc * gr[3][1] + sg[1] * u + sg[3] * v + sg[4] * w;
       qf[2] = hcc * gr[3][2] + sg[2] * u + sg[4] * v + sg[5] * w;
-      VF[0 * fs + off] = sg[sidx(dA, 0)];
-      VF[1 * fs + off] = sg[sidx(dA, 1)];
-      VF[2 * fs + off] = sg[sidx(dA, 2)];
-      VF[3 * fs + off] = qf[dA];
-      VF[4 * fs + off] = sg[sidx(dB, dB)];
-      VF[5 * fs + off] = sg[sidx(dB, dC)];
-      VF[6 * fs + off] = qf[dB];
+      // combined fluxes G_d = VF_d - F_d along A and B for passes A' and B'
+      {
+        double FA[5], FB[5];
+        euler_flux<dA>(q0, u, v, w, p, th, FA);
+        euler_flux<dB>(q0, u, v, w, p, th, FB);
+        VF[0 * fs + off] = -FA[0];
+        VF[1 * fs + off] = sg[sidx(dA, 0)] - FA[1];
+        VF[2 * fs + off] = sg[sidx(dA, 1)] - FA[2];
+        VF[3 * fs + off] = sg[sidx(dA, 2)] - FA[3];
+        VF[4 * fs + off] = qf[dA] - FA[4];
+        VF[5 * fs + off] = -FB[0];
+        VF[6 * fs + off] = sg[sidx(dB, 0)] - FB[1];
+        VF[7 * fs + off] = sg[sidx(dB, 1)] - FB[2];
+        VF[8 * fs + off] = sg[sidx(dB, 2)] - FB[3];
+        VF[9 * fs + off] = qf[dB] - FB[4];
+      }
       // combined fluxes along C, with their periodic images
       double F[5];
       euler_flux<DIR>(q0, u, v, w, p, th, F);
@@ -615,7 +587,7 @@ __device__ __forceinline__ void k_pass_c_body(const PassArgs& a, int bx, int by)
 }
 
 // ------------------------------------------------------------------ pass A' (fluxes along A)
-// R += D_A(VF_A - F_A).
+// R += D_A(G_A), G_A = VF_A - F_A as pass C stored it.
 template <int S, int WPL, int DIR>
 __device__ __forceinline__ void k_pass_va_body(const PassArgs& a, int bx, int by) {
   extern __shared__ double sm[];
@@ -625,12 +597,8 @@ __device__ __forceinline__ void k_pass_va_body(const PassArgs& a, int bx, int by
   double* scan = sm + 5 * tsz;
   double* spb = scan + c.TI * SCAN_PER_LINE * WPL;
   const int64_t fs = a.g.fs;
-  for (int m = 0; m < 5; ++m) load_tile(c, T + m * tsz, a.q + m * fs);
+  for (int m = 0; m < 5; ++m) load_tile(c, T + m * tsz, a.VF + m * fs);
   cp_async_wait_all();
-  __syncthreads();
-  to_prims(c, T, tsz, a.th);
-  __syncthreads();
-  combine_flux_tiles(c, T, tsz, a);
   __syncthreads();
   tile_specials(a.opd, c.TI, c.LP, T, tsz, 5, spb);
   __syncthreads();
@@ -642,7 +610,7 @@ __device__ __forceinline__ void k_pass_va_body(const PassArgs& a, int bx, int by
 }
 
 // ------------------------------------------------------------------ pass B' (fluxes along B, update, filter)
-// R += D_B(VF_B - F_B); mode 1: q_out = F_B(c1 qsave + c2 q + c3 dt R) (rk3, tgvsolver.F90:1055-1057,
+// R += D_B(G_B); mode 1: q_out = F_B(c1 qsave + c2 q + c3 dt R) (rk3, tgvsolver.F90:1055-1057,
 // filterq along B); mode 0: R only.
 template <int S, int WPL, int DIR>
 __device__ __forceinline__ void k_pass_vb_body(const PassArgs& a, int bx, int by) {
@@ -653,12 +621,8 @@ __device__ __forceinline__ void k_pass_vb_body(const PassArgs& a, int bx, int by
   double* scan = sm + 5 * tsz;
   double* spb = scan + c.TI * SCAN_PER_LINE * WPL;
   const int64_t fs = a.g.fs;
-  for (int m = 0; m < 5; ++m) load_tile(c, T + m * tsz, a.q + m * fs);
+  for (int m = 0; m < 5; ++m) load_tile(c, T + m * tsz, a.VF + (5 + m) * fs);
   cp_async_wait_all();
-  __syncthreads();
-  to_prims(c, T, tsz, a.th);
-  __syncthreads();
-  combine_flux_tiles(c, T, tsz, a);
   __syncthreads();
   tile_specials(a.opd, c.TI, c.LP, T, tsz, 5, spb);
   __syncthreads();

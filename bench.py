@@ -29,11 +29,11 @@ sys.path.insert(0, ROOT)
 
 METRIC = "RK3 grid-point updates/s FP64 TGV 512³ + %HBM peak; adjoint:forward step time"
 UNIT = "grid-point RK3 updates/s"
-B_ALG_STEP = 2504.0      # algorithmic bytes per unique grid point per RK3 step (pass model)
+B_ALG_STEP = 2384.0      # algorithmic bytes per unique grid point per RK3 step (pass model)
 # fields read + written per stored point by one launch of each pass (A with the filter; B' reads q
 # for the c2 term at two of the three stages)
 PASS_NAMES = ["A", "B", "C", "A'", "B'", "F"]
-PASS_FIELDS = {"A": 14, "B": 9, "C": 25, "A'": 19, "B'": 24 + 10 / 3, "F": 10}
+PASS_FIELDS = {"A": 14, "B": 9, "C": 28, "A'": 15, "B'": 20 + 10 / 3, "F": 10}
 PASS_PER_STEP = {"A": 3, "B": 3, "C": 3, "A'": 3, "B'": 3, "F": 3}
 
 
