@@ -546,6 +546,7 @@ int astr_state_create(astr_ctx* ctx, const astr_params* p, astr_state** out) {
   st->th.const2 = g * (m * m);
   st->th.const5 = (g - 1.0) * (m * m);
   st->th.const6 = 1.0 / (g - 1.0);
+  st->th.gm1 = g - 1.0;
   st->th.reynolds = p->reynolds;
   st->th.prandtl = p->prandtl;
   st->th.tc = p->sutherland / p->ref_tem;

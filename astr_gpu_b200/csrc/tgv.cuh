@@ -17,6 +17,7 @@ struct BoxGeo {
 // Thermodynamic constants of tgvsolver.F90:183-195 and miucal (:123-140).
 struct Thermo {
   double const2, const5, const6;
+  double gm1;       // gamma - 1 (= 1/const6)
   double reynolds, prandtl;
   double tc, tc1;   // Sutherland: tempconst = S/ref_tem, 1 + tempconst
   double mach;

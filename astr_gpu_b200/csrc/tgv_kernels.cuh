@@ -157,16 +157,20 @@ __device__ __forceinline__ void put_images(double* line, int n, int dim, double 
 
 // q -> (rho, u, v, w, p) in place over every staged node of the 5 tiles (q2fvar,
 // tgvsolver.F90:92-121), once per node.
-template <int DIR, int WPL>
+// With TEMP, tile 4 receives the temperature p/rho * gamma M^2 instead of the pressure (the
+// gradient passes need only u, v, w, T). One reciprocal of rho per node; the results equal
+// q2fvar's divisions to within an ulp.
+template <int DIR, int WPL, bool TEMP = false>
 __device__ __forceinline__ void to_prims(const TileCtx<DIR, WPL>& c, double* T, int tsz, const Thermo& th) {
   c.for_nodes(-HT, c.dim + HT, [&](int o, int) {
     const double q0 = T[o], q1 = T[tsz + o], q2 = T[2 * tsz + o], q3 = T[3 * tsz + o], q4 = T[4 * tsz + o];
-    const double u = q1 / q0, v = q2 / q0, w = q3 / q0;
-    const double p = (q4 - 0.5 * q0 * (u * u + v * v + w * w)) / th.const6;
+    const double ri = 1.0 / q0;
+    const double u = q1 * ri, v = q2 * ri, w = q3 * ri;
+    const double p = (q4 - 0.5 * q0 * (u * u + v * v + w * w)) * th.gm1;
     T[tsz + o] = u;
     T[2 * tsz + o] = v;
     T[3 * tsz + o] = w;
-    T[4 * tsz + o] = p;
+    T[4 * tsz + o] = TEMP ? p * ri * th.const2 : p;
   });
 }
 
@@ -406,17 +410,11 @@ __device__ __forceinline__ void k_pass_ab_body(const PassArgs& a, int bx, int by
     store_tiles<DIR, WPL, false>(c, T, tsz, a.q, fs, 5);
     __syncthreads();   // every filtered value is stored before the tiles turn into primitives
   }
-  to_prims(c, T, tsz, a.th);
+  to_prims<DIR, WPL, true>(c, T, tsz, a.th);
   __syncthreads();
-  compute_specials(a.opd, c.TI, spb, 4, [&](int l, int k, int n) { return gprim_rt<DIR>(k, T + l * c.LP + HT, tsz, n, a.th); });
+  tile_specials(a.opd, c.TI, c.LP, T + tsz, tsz, 4, spb);
   __syncthreads();
-  const double rd = a.g.rd[DIR];
-  const double* L0 = T + z.l * c.LP + HT;
-  for (int K = 0; K < 4; ++K) {
-    double v[1][S];
-    dsolve_n<S, WPL, DIR, 1>(v, K, a, z, L0, tsz, scl, rd, spb + (z.l * 4 + K) * 2 * NSP);
-    put_lane<S>(T + (K + 1) * tsz + z.l * c.LP + HT, v[0], z.seg, a.opd.ext_lo, dim, false);
-  }
+  solve_lines<S, WPL>(T + tsz + z.l * c.LP + HT, tsz, 4, a.opd, z, scl, a.g.rd[DIR], false, spb + z.l * 4 * 2 * NSP);
   __syncthreads();
   store_tiles<DIR, WPL, false>(c, T + tsz, tsz, a.D, fs, 4);
 }
@@ -443,19 +441,20 @@ __device__ __forceinline__ void k_pass_c_body(const PassArgs& a, int bx, int by)
   const int dim = c.dim;
   to_prims(c, T, tsz, a.th);
   __syncthreads();
-  compute_specials(a.opd, c.TI, spb, 4, [&](int l, int k, int n) { return gprim_rt<DIR>(k, T + l * c.LP + HT, tsz, n, a.th); });
+  // gradients along C of (u, v, w, T), solved in place in the G tiles
+  c.for_nodes(-HT, dim + HT, [&](int o, int) {
+    G[o] = T[tsz + o];
+    G[tsz + o] = T[2 * tsz + o];
+    G[2 * tsz + o] = T[3 * tsz + o];
+    G[3 * tsz + o] = T[4 * tsz + o] / T[o] * a.th.const2;
+  });
+  __syncthreads();
+  tile_specials(a.opd, c.TI, c.LP, G, tsz, 4, spb);
   __syncthreads();
   const LaneIds z = lane_ids<WPL>();
   double* scl = scan + z.l * SCAN_PER_LINE * WPL;
   const double rd = a.g.rd[DIR];
-  const double* L0 = T + z.l * c.LP + HT;
-
-  // gradients along C
-  for (int K = 0; K < 4; ++K) {
-    double v[1][S];
-    dsolve_n<S, WPL, DIR, 1>(v, K, a, z, L0, tsz, scl, rd, spb + (z.l * 4 + K) * 2 * NSP);
-    put_lane<S>(G + K * tsz + z.l * c.LP + HT, v[0], z.seg, a.opd.ext_lo, dim, false);
-  }
+  solve_lines<S, WPL>(G + z.l * c.LP + HT, tsz, 4, a.opd, z, scl, rd, false, spb + z.l * 4 * 2 * NSP);
   __syncthreads();
   if (a.DC) {   // kept for the discrete adjoint
     store_tiles<DIR, WPL, false>(c, G, tsz, a.DC, fs, 4);
