@@ -547,6 +547,8 @@ int astr_state_create(astr_ctx* ctx, const astr_params* p, astr_state** out) {
   st->th.const5 = (g - 1.0) * (m * m);
   st->th.const6 = 1.0 / (g - 1.0);
   st->th.gm1 = g - 1.0;
+  st->th.inv_re = 1.0 / st->p.reynolds;
+  st->th.inv_prc5 = 1.0 / (st->p.prandtl * st->th.const5);
   st->th.reynolds = p->reynolds;
   st->th.prandtl = p->prandtl;
   st->th.tc = p->sutherland / p->ref_tem;

@@ -18,6 +18,8 @@ struct BoxGeo {
 struct Thermo {
   double const2, const5, const6;
   double gm1;       // gamma - 1 (= 1/const6)
+  double inv_re;    // 1/Re
+  double inv_prc5;  // 1/(Pr const5): heat conductivity per unit viscosity
   double reynolds, prandtl;
   double tc, tc1;   // Sutherland: tempconst = S/ref_tem, 1 + tempconst
   double mach;

@@ -489,7 +489,8 @@ __device__ __forceinline__ void k_pass_c_body(const PassArgs& a, int bx, int by)
         gr[k][dC] = G[k * tsz + tix];
       }
       const double q0 = T[tix], u = T[tsz + tix], v = T[2 * tsz + tix], w = T[3 * tsz + tix], p = T[4 * tsz + tix];
-      const double tmp = p / q0 * th.const2;
+      // divisions by constants as products with their reciprocals (equal to within an ulp)
+      const double tmp = p * (1.0 / q0) * th.const2;
       if (!(q0 > 0.0) || !isfinite(p)) bad = 1;
       const double s11 = gr[0][0];
       const double s12 = 0.5 * (gr[0][1] + gr[1][0]);
@@ -498,9 +499,9 @@ __device__ __forceinline__ void k_pass_c_body(const PassArgs& a, int bx, int by)
       const double s23 = 0.5 * (gr[1][2] + gr[2][1]);
       const double s33 = gr[2][2];
       const double skk = (1.0 / 3.0) * (s11 + s22 + s33);
-      const double miu = miucal(th, tmp) / th.reynolds;
+      const double miu = miucal(th, tmp) * th.inv_re;
       const double miu2 = 2.0 * miu;
-      const double hcc = (miu / th.prandtl) / th.const5;
+      const double hcc = miu * th.inv_prc5;
       double sg[6];
       sg[0] = miu2 * (s11 - skk);
       sg[1] = miu2 * s12;
