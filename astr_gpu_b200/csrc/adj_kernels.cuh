@@ -21,57 +21,72 @@ namespace adj_detail {
 
 using namespace pass_detail;
 
-// out(f) = alpha * L^T in(f) (+ out(f) when accumulating) for nf fields along DIR.
+// out(f) = alpha * L^T in(f) (+ out(f) when accumulating) for nf fields along DIR. Up to
+// ADJ_MAXF fields are staged together (asynchronous copies, zeros outside nodes 0..dim), solved
+// one after the other in place, then gathered through W and stored.
 template <int S, int WPL, int DIR, int NB>
 __global__ void __launch_bounds__(512) k_adj_lines(AdjLineArgs a) {
   extern __shared__ double sm[];
   const TileCtx<DIR, WPL> c(a.p, blockIdx.x, blockIdx.y);
   const int dim = c.dim;
   const int tsz = c.TI * c.LP;
+  const int nstage = a.nf < ADJ_MAXF ? a.nf : ADJ_MAXF;
   double* T = sm;
-  double* scan = sm + tsz;
+  double* scan = sm + (size_t)nstage * tsz;
   const LaneIds z = lane_ids<WPL>();
   double* scl = scan + z.l * SCAN_PER_LINE * WPL;
   const LineOp& op = a.p.opd;
   const int e = op.ext_lo, nsys = op.nsys;
-  double* line = T + z.l * c.LP + HT;
   const int64_t fs = a.p.g.fs;
-  for (int f = 0; f < a.nf; ++f) {
-    const double* g = a.in + f * fs + c.sbase;
-    c.for_nodes(-HT, dim + HT, [&](int o, int n) {
-      T[o] = (c.svalid && n >= 0 && n <= dim) ? a.alpha * g[(int64_t)n * c.sd] : 0.0;
-    });
-    __syncthreads();
-    double v[1][S];
-#pragma unroll
-    for (int t = 0; t < S; ++t) {
-      const int r = z.seg * S + t;
-      v[0][t] = (r < nsys) ? line[r - e] : 0.0;
+  const AdjW& w = a.w;
+  for (int f0 = 0; f0 < a.nf; f0 += ADJ_MAXF) {
+    const int nfc = (a.nf - f0) < ADJ_MAXF ? (a.nf - f0) : ADJ_MAXF;
+    for (int f = 0; f < nfc; ++f) {
+      double* Tf = T + f * tsz;
+      const double* g = a.in + (f0 + f) * fs + c.sbase;
+      c.for_nodes(-HT, dim + HT, [&](int o, int n) {
+        if (c.svalid && n >= 0 && n <= dim) cp_async8(Tf + o, g + (int64_t)n * c.sd);
+        else Tf[o] = 0.0;
+      });
     }
-    seg_solve_n<S, WPL, 1>(v, op.tab, z.seg, z.lane, z.part, z.l, scl);
+    cp_async_wait_all();
+    __syncthreads();
+    for (int f = 0; f < nfc; ++f) {
+      double* line = T + f * tsz + z.l * c.LP + HT;
+      double v[1][S];
 #pragma unroll
-    for (int t = 0; t < S; ++t) {
-      const int r = z.seg * S + t;
-      if (r < nsys) line[r - e] = v[0][t];
+      for (int t = 0; t < S; ++t) {
+        const int r = z.seg * S + t;
+        v[0][t] = (r < nsys) ? line[r - e] : 0.0;
+      }
+      seg_solve_n<S, WPL, 1>(v, op.tab, z.seg, z.lane, z.part, z.l, scl);
+#pragma unroll
+      for (int t = 0; t < S; ++t) {
+        const int r = z.seg * S + t;
+        if (r < nsys) line[r - e] = v[0][t];
+      }
     }
     __syncthreads();
     if (c.svalid) {
-      double* dst = a.out + f * fs + c.sbase;
-      const AdjW& w = a.w;
-      c.for_nodes(0, dim, [&](int o, int n) {
-        double s = 0.0;
-        if (n >= w.mlo && n <= w.mhi) {
-          const double* y = T + o + w.jlo;
+      for (int f = 0; f < nfc; ++f) {
+        const double* Tf = T + f * tsz;
+        double* dst = a.out + (f0 + f) * fs + c.sbase;
+        c.for_nodes(0, dim, [&](int o, int n) {
+          double s = 0.0;
+          if (n >= w.mlo && n <= w.mhi) {
+            const double* y = Tf + o + w.jlo;
 #pragma unroll
-          for (int j = 0; j < NB; ++j) s = fma(w.wint[j], y[j], s);
-        } else {
-          const int k = n < w.mlo ? n : w.mlo + (n - w.mhi - 1);
-          const double* y = T + o - n;
-          for (int q = w.sptr[k]; q < w.sptr[k + 1]; ++q) s = fma(w.scoef[q], y[w.snode[q]], s);
-        }
-        const int64_t off = (int64_t)n * c.sd;
-        dst[off] = a.accumulate ? dst[off] + s : s;
-      });
+            for (int j = 0; j < NB; ++j) s = fma(w.wint[j], y[j], s);
+          } else {
+            const int k = n < w.mlo ? n : w.mlo + (n - w.mhi - 1);
+            const double* y = Tf + o - n;
+            for (int q = w.sptr[k]; q < w.sptr[k + 1]; ++q) s = fma(w.scoef[q], y[w.snode[q]], s);
+          }
+          s *= a.alpha;
+          const int64_t off = (int64_t)n * c.sd;
+          dst[off] = a.accumulate ? dst[off] + s : s;
+        });
+      }
     }
     __syncthreads();
   }
@@ -130,7 +145,7 @@ cudaError_t launch_adj_lines_t(const AdjLineArgs& a, cudaStream_t st) {
   const int o1 = (dir == 0) ? 1 : 0, o2 = (dir == 2) ? 1 : 2;
   dim3 grid((unsigned)((a.p.g.N[o1] + 1 + a.p.TI - 1) / a.p.TI), (unsigned)(a.p.g.N[o2] + 1));
   const int threads = a.p.TI * WPL * 32;
-  const size_t smem = adj_lines_smem(a.p.TI, a.p.LP, WPL);
+  const size_t smem = adj_lines_smem(a.p.TI, a.p.LP, WPL, a.nf < ADJ_MAXF ? a.nf : ADJ_MAXF);
   const int nb = a.w.nint <= 5 ? 5 : (a.w.nint <= 11 ? 11 : ADJ_BAND);
 #define ASTR_ADJ_LINES(D, NB) \
   if (dir == D && nb == NB) return launch_adj_k(adj_detail::k_adj_lines<S, WPL, D, NB>, grid, threads, smem, st, a);

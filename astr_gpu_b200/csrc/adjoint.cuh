@@ -26,8 +26,11 @@ struct AdjLineArgs {
   int accumulate;
 };
 
-inline size_t adj_lines_smem(int TI, int LP, int WPL) {
-  return ((size_t)TI * LP + (size_t)TI * SCAN_PER_LINE * WPL) * sizeof(double);
+constexpr int ADJ_MAXF = 5;   // fields staged together by one CTA of the transposed line kernel
+
+// Shared memory of the transposed line kernel staging nf fields at a time (nf <= ADJ_MAXF).
+inline size_t adj_lines_smem(int TI, int LP, int WPL, int nf = ADJ_MAXF) {
+  return ((size_t)nf * TI * LP + (size_t)TI * SCAN_PER_LINE * WPL) * sizeof(double);
 }
 inline size_t adj_grad_smem(int TI, int LP, int WPL) {
   return ((size_t)6 * TI * LP + (size_t)TI * SCAN_PER_LINE * WPL + (size_t)TI * 4 * 2 * NSP) * sizeof(double);

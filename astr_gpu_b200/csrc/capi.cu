@@ -1205,11 +1205,13 @@ void adj_free(astr_adjoint* a) {
   a->gstore = nullptr;
 }
 
-// One RK3 stage with every filter applied: qout = F(c1 qsave + c2 qin + c3 dt rhs(qin)). With G,
-// the velocity/temperature gradients of qin go to G[4d + k] (physical direction d, as the
-// adjoint's gradient kernel lays them out).
+// One RK3 stage: qout = F(c1 qsave + c2 qin + c3 dt rhs(qin)) with the filter along A left
+// owed, as in the time step: the next stage's first pass applies it to qout in place. With
+// pending_in, qin still owes that filter and receives it here first (in place). With G, the
+// velocity/temperature gradients of qin go to G[4d + k] (physical direction d, as the adjoint's
+// gradient kernel lays them out).
 cudaError_t run_stage_full(astr_state* st, int s, const double* qin, const double* qsave, double* qout, double dt,
-                           double* G = nullptr) {
+                           double* G, bool pending_in) {
   static const double rk[3][3] = {{1.0, 0.0, 1.0}, {0.75, 0.25, 0.25}, {1.0 / 3.0, 2.0 / 3.0, 2.0 / 3.0}};
   double* qi = const_cast<double*>(qin);
   const int64_t fs = st->g.fs;
@@ -1217,7 +1219,7 @@ cudaError_t run_stage_full(astr_state* st, int s, const double* qin, const doubl
   double* DB = G ? G + 4 * DIR_B * fs : st->DB;
   cudaError_t e;
   PassArgs a = base_args(st, CFG_A);
-  a.q = qi; a.D = DA; a.do_filter = 0;
+  a.q = qi; a.D = DA; a.do_filter = (pending_in && st->p.filter_on) ? 1 : 0;
   if ((e = run_pass(st, CFG_A, a)) != cudaSuccess) return e;
   a = base_args(st, CFG_B);
   a.q = qi; a.D = DB;
@@ -1238,9 +1240,6 @@ cudaError_t run_stage_full(astr_state* st, int s, const double* qin, const doubl
     a = base_args(st, CFG_FC);
     a.q = qout;
     if ((e = run_pass(st, CFG_FC, a)) != cudaSuccess) return e;
-    a = base_args(st, CFG_FA);
-    a.q = qout;
-    if ((e = run_pass(st, CFG_FA, a)) != cudaSuccess) return e;
   }
   return cudaSuccess;
 }
@@ -1401,13 +1400,16 @@ int astr_adjoint_forward(astr_adjoint* A, double dt, int nsteps, double* J) {
   astr_state* st = A->st;
   astr_ctx* ctx = st->ctx;
   const size_t qb = 5 * (size_t)st->g.fs * sizeof(double);
-  for (double* c : A->ckpt) cudaFree(c);
-  A->ckpt.clear();
-  CK(finalize_filter(st));
-  for (int s0 = 0; s0 < nsteps; s0 += A->every) {
+  // checkpoint buffers are kept across calls; the missing ones are allocated before any step
+  const size_t nck = (size_t)((nsteps + A->every - 1) / A->every);
+  while (A->ckpt.size() < nck) {
     double* c = nullptr;
     CK(cudaMalloc(&c, qb));
     A->ckpt.push_back(c);
+  }
+  CK(finalize_filter(st));
+  for (int s0 = 0; s0 < nsteps; s0 += A->every) {
+    double* c = A->ckpt[(size_t)(s0 / A->every)];
     CK(cudaMemcpyAsync(c, st->Q0, qb, cudaMemcpyDeviceToDevice, ctx->stream));
     const int n = std::min(A->every, nsteps - s0);
     int rc = astr_rk3_step(st, dt, n);
@@ -1435,7 +1437,7 @@ int astr_adjoint_backward(astr_adjoint* A, double* grad, const int64_t shape[3],
   // dJ/dq at the final state (the state's Q0 after the forward run)
   CK(finalize_filter(st));
   CK(launch_adj_objective(st->g, st->Q0, A->lam, sm));
-  const int nseg = (int)A->ckpt.size();
+  const int nseg = (A->nsteps + A->every - 1) / A->every;
   for (int j = nseg - 1; j >= 0; --j) {
     const int s0 = j * A->every;
     const int len = std::min(A->every, A->nsteps - s0);
@@ -1445,12 +1447,13 @@ int astr_adjoint_backward(astr_adjoint* A, double* grad, const int64_t shape[3],
     };
     CK(cudaMemcpyAsync(stage(0, 0), A->ckpt[j], qb, cudaMemcpyDeviceToDevice, sm));
     for (int n = 0; n < len; ++n) {
-      CK(run_stage_full(st, 0, stage(n, 0), stage(n, 0), stage(n, 1), A->dt, grads(n, 0)));
-      CK(run_stage_full(st, 1, stage(n, 1), stage(n, 0), stage(n, 2), A->dt, grads(n, 1)));
-      // the last stage's output is the next step's input; with stored gradients the last step
-      // still runs it for them
-      if (n + 1 < len) CK(run_stage_full(st, 2, stage(n, 2), stage(n, 0), stage(n + 1, 0), A->dt, grads(n, 2)));
-      else if (A->gstore) CK(run_stage_full(st, 2, stage(n, 2), stage(n, 0), A->t1, A->dt, grads(n, 2)));
+      // every stage input receives the filter along A owed by the stage before it from its own
+      // first pass (the checkpoint at n = 0 is fully filtered); the last step's third stage
+      // still runs (into scratch) so that its input is filtered and its gradients are kept
+      CK(run_stage_full(st, 0, stage(n, 0), stage(n, 0), stage(n, 1), A->dt, grads(n, 0), n > 0));
+      CK(run_stage_full(st, 1, stage(n, 1), stage(n, 0), stage(n, 2), A->dt, grads(n, 1), true));
+      CK(run_stage_full(st, 2, stage(n, 2), stage(n, 0), n + 1 < len ? stage(n + 1, 0) : A->t1, A->dt, grads(n, 2),
+                        true));
     }
     for (int n = len - 1; n >= 0; --n) {
       const double* Gs[3] = {grads(n, 0), grads(n, 1), grads(n, 2)};
@@ -1478,8 +1481,9 @@ int astr_step_vjp(astr_adjoint* A, double dt, const double* lam_in, double* lam_
   double* S2 = S1 + 5 * st->g.fs;
   if (A->every < 1) return ASTR_ERR_ARG;
   CK(cudaMemcpyAsync(S0, st->Q0, qb, cudaMemcpyDeviceToDevice, sm));
-  CK(run_stage_full(st, 0, S0, S0, S1, dt));
-  CK(run_stage_full(st, 1, S1, S0, S2, dt));
+  CK(run_stage_full(st, 0, S0, S0, S1, dt, nullptr, false));
+  CK(run_stage_full(st, 1, S1, S0, S2, dt, nullptr, true));
+  CK(run_stage_full(st, 2, S2, S0, A->t1, dt, nullptr, true));   // filters S2 in place
   int rc = copy_fields(st, A->lam, const_cast<double*>(lam_in), shape, lbound, 1, where);
   if (rc) return rc;
   const double keep = A->dt;
