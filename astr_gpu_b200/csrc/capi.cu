@@ -338,6 +338,22 @@ int copy_fields(astr_state* st, double* dev, double* user, const int64_t* shape,
     return ASTR_OK;
   }
   const size_t ufs = (size_t)(shape[0] * shape[1] * shape[2]);
+  // A host array of exactly nodes 0..N moves as one contiguous copy through the stage buffer Q1
+  // (free between steps), repacked to the padded state layout on the device: one large DMA instead
+  // of 5 (N+1)^2 short rows.
+  const bool exact = lb[0] == 0 && lb[1] == 0 && lb[2] == 0 && shape[0] == N[0] + 1 && shape[1] == N[1] + 1 &&
+                     shape[2] == N[2] + 1;
+  if (exact && dev != st->Q1) {
+    const size_t bytes = 5 * ufs * sizeof(double);
+    if (to_state) {
+      CK(cudaMemcpyAsync(st->Q1, user, bytes, cudaMemcpyHostToDevice, ctx->stream));
+      CK(launch_pack(st->g, dev, st->Q1, shape, lb, 5, 1, ctx->stream));
+    } else {
+      CK(launch_pack(st->g, dev, st->Q1, shape, lb, 5, 0, ctx->stream));
+      CK(cudaMemcpyAsync(user, st->Q1, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+    }
+    return ASTR_OK;
+  }
   for (int m = 0; m < 5; ++m) {
     cudaMemcpy3DParms prm{};
     cudaPitchedPtr hp = make_cudaPitchedPtr(user + m * ufs, (size_t)shape[0] * 8, (size_t)shape[0], (size_t)shape[1]);
