@@ -32,6 +32,8 @@ enum OpKind { OP_DERIV = 0, OP_FILTER = 1, OP_EXPLICIT = 2 };
 //   [5*S*NS + k*NS + seg]       per segment: FS[0..4] forward scan composites for shuffle offsets
 //                               1..16, FE forward exclusive product within the warp, BS[0..4], BE
 //   [(5*S + 12)*NS + ...]       per warp: MW[WPL], MWB[WPL] (whole-warp products)
+//   [(5*S + 12)*NS + 2*WPL]     int per segment: the slot whose row columns (the first three
+//                               arrays) it reads; segments with identical columns share a slot
 struct LineOp {
   const double* tab;
   int nsys;            // rows of the system (last_node - first_node + 1)
@@ -64,9 +66,11 @@ template <int S, int WPL, int NV>
 __device__ __forceinline__ void seg_solve_n(double (&v)[NV][S], const double* __restrict__ tab, int seg, int lane,
                                             int part, int line, double* scan_sm) {
   constexpr int NS = 32 * WPL;
-  const double2* fwd = reinterpret_cast<const double2*>(tab) + seg;
-  const double* pfp = tab + 2 * S * NS + seg;
-  const double2* bwd = reinterpret_cast<const double2*>(tab + 3 * S * NS) + seg;
+  // row coefficients from this segment's slot (shared by segments with identical columns)
+  const int rs = __ldg(reinterpret_cast<const int*>(tab + (5 * S + T_NSEGTAB) * NS + 2 * WPL) + seg);
+  const double2* fwd = reinterpret_cast<const double2*>(tab) + rs;
+  const double* pfp = tab + 2 * S * NS + rs;
+  const double2* bwd = reinterpret_cast<const double2*>(tab + 3 * S * NS) + rs;
   const double* sg = tab + 5 * S * NS + seg;
   const double* ws = tab + (5 * S + T_NSEGTAB) * NS;   // per-warp products
   // forward sweeps from a zero carry

@@ -131,7 +131,8 @@ std::vector<double> lane_tables(const HostOp& op, int S, int nseg) {
   const int nsys = op.nsys();
   const int WPL = nseg / 32;
   const size_t base = (size_t)5 * S * nseg;
-  std::vector<double> t(base + (size_t)T_NSEGTAB * nseg + 2 * (size_t)WPL, 0.0);
+  const size_t slot_off = base + (size_t)T_NSEGTAB * nseg + 2 * (size_t)WPL;
+  std::vector<double> t(slot_off + (size_t)(nseg + 1) / 2, 0.0);
   // f: 0 ac1, 1 ac2, 2 ac3, 3 pf, 4 qb (see the layout in ops.cuh)
   auto at = [&](int f, int tt, int seg) -> double& {
     const size_t rs = (size_t)tt * nseg + seg;
@@ -189,6 +190,19 @@ std::vector<double> lane_tables(const HostOp& op, int S, int nseg) {
     for (int j = 0; j < 32; ++j) { mw *= mf[s0 + j]; mwb *= mb[s0 + j]; }
     t[base + (size_t)T_NSEGTAB * nseg + w] = mw;
     t[base + (size_t)T_NSEGTAB * nseg + WPL + w] = mwb;
+  }
+  // Row-coefficient slot of every segment: the first segment whose (ac2, ac3, pf, ac1, qb)
+  // column is bitwise the same. Interior segments (converged factors) share one slot, so the
+  // lanes of a warp read the same addresses and the loads are broadcasts.
+  int* slot = reinterpret_cast<int*>(t.data() + slot_off);
+  for (int seg = 0; seg < nseg; ++seg) {
+    slot[seg] = seg;
+    for (int o = 0; o < seg; ++o) {
+      bool same = true;
+      for (int f = 0; f < 5 && same; ++f)
+        for (int tt = 0; tt < S && same; ++tt) same = at(f, tt, o) == at(f, tt, seg);
+      if (same) { slot[seg] = o; break; }
+    }
   }
   return t;
 }
