@@ -327,11 +327,6 @@ __global__ void k_ke_final(const double* __restrict__ part, int n, double scale,
   }
 }
 
-__global__ void k_axpby(int64_t n, double a, const double* __restrict__ x, double b, double* __restrict__ y) {
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) y[i] = a * x[i] + (b == 0.0 ? 0.0 : b * y[i]);
-}
-
 PtGeo pt_geo(const BoxGeo& g) {
   PtGeo p;
   p.n0 = g.N[0] + 1; p.n1 = g.N[1] + 1; p.n2 = g.N[2] + 1;
@@ -371,11 +366,6 @@ cudaError_t launch_kinetic_energy(const BoxGeo& g, const double* q, double* part
   const double scale = 1.0 / ((double)g.N[0] * (double)g.N[1] * (double)g.N[2]);
   k_ke_planes<<<p.n2, 256, 0, st>>>(p, q, part);
   k_ke_final<<<1, 32, 0, st>>>(part, p.n2, scale, out);
-  return cudaGetLastError();
-}
-
-cudaError_t launch_axpby(int64_t n, double a, const double* x, double b, double* y, cudaStream_t st) {
-  k_axpby<<<pt_blocks(n), 256, 0, st>>>(n, a, x, b, y);
   return cudaGetLastError();
 }
 

@@ -58,7 +58,6 @@ cudaError_t launch_adj_point2(const BoxGeo& g, const Thermo& th, const double* q
                               double* lq, const double* lsum, cudaStream_t st);
 cudaError_t launch_adj_objective(const BoxGeo& g, const double* q, double* lam, cudaStream_t st);
 cudaError_t launch_kinetic_energy(const BoxGeo& g, const double* q, double* part, double* out, cudaStream_t st);
-cudaError_t launch_axpby(int64_t n, double a, const double* x, double b, double* y, cudaStream_t st);
 
 cudaError_t launch_adj_lines(const AdjLineArgs& a, int S, int WPL, cudaStream_t st);
 cudaError_t launch_adj_grad(const PassArgs& a, int S, int WPL, cudaStream_t st);
