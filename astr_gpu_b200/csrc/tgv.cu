@@ -165,9 +165,7 @@ int pass_tiles(int pass) {
   switch (pass) {
     case PASS_A: case PASS_B: return 5;
     case PASS_C: return 10;
-    case PASS_VA: return 5;
-    case PASS_VB: return 5;
-    case PASS_F: return 5;
+    case PASS_VA: case PASS_VB: case PASS_F: return 2;   // two field buffers (stream_fields)
   }
   return 0;
 }

@@ -94,6 +94,13 @@ __device__ __forceinline__ void cp_async_wait_all() {
   asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
 }
 
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+// Wait until at most N committed groups of this thread are still in flight.
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
 __device__ __forceinline__ void cp_async16(uint32_t sdst, const double* gsrc) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sdst), "l"(gsrc) : "memory");
 }
@@ -586,68 +593,86 @@ __device__ __forceinline__ void k_pass_c_body(const PassArgs& a, int bx, int by)
   store_tiles<DIR, WPL, false>(c, G + 4 * tsz, tsz, a.R, fs, 1);
 }
 
+// ------------------------------------------------------------------ field streaming
+// Passes whose fields are independent (A', B', F) take one field at a time through two tile
+// buffers: the copies of field m+1 are in flight while field m is solved, and the smaller
+// footprint lets two CTAs share an SM, so one CTA's loads overlap the other's solves.
+// body(m, tile) runs between CTA barriers and leaves the tile free for reuse.
+template <int DIR, int WPL, class Src, class Body>
+__device__ __forceinline__ void stream_fields(const TileCtx<DIR, WPL>& c, double* buf, int tsz, int nf, Src src,
+                                              Body body) {
+  load_tile(c, buf, src(0));
+  cp_async_commit();
+#pragma unroll 1
+  for (int m = 0; m < nf; ++m) {
+    if (m + 1 < nf) {
+      load_tile(c, buf + ((m + 1) & 1) * tsz, src(m + 1));
+      cp_async_commit();
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    __syncthreads();
+    body(m, buf + (m & 1) * tsz);
+    __syncthreads();
+  }
+}
+
 // ------------------------------------------------------------------ pass A' (fluxes along A)
-// R += D_A(G_A), G_A = VF_A - F_A as pass C stored it.
+// R += D_A(G_A), G_A = VF_A - F_A stored by pass C (convection + diffusion along A).
 template <int S, int WPL, int DIR>
 __device__ __forceinline__ void k_pass_va_body(const PassArgs& a, int bx, int by) {
   extern __shared__ double sm[];
   const TileCtx<DIR, WPL> c(a, bx, by);
   const int tsz = c.TI * c.LP;
-  double* T = sm;
-  double* scan = sm + 5 * tsz;
+  double* scan = sm + 2 * tsz;
   double* spb = scan + c.TI * SCAN_PER_LINE * WPL;
   const int64_t fs = a.g.fs;
-  for (int m = 0; m < 5; ++m) load_tile(c, T + m * tsz, a.VF + m * fs);
-  cp_async_wait_all();
-  __syncthreads();
-  tile_specials(a.opd, c.TI, c.LP, T, tsz, 5, spb);
-  __syncthreads();
   const LaneIds z = lane_ids<WPL>();
   double* scl = scan + z.l * SCAN_PER_LINE * WPL;
-  solve_lines<S, WPL>(T + z.l * c.LP + HT, tsz, 5, a.opd, z, scl, a.g.rd[DIR], false, spb + z.l * 5 * 2 * NSP);
-  __syncthreads();
-  store_tiles<DIR, WPL, true>(c, T, tsz, a.R, fs, 5);
+  stream_fields(c, sm, tsz, 5, [&](int m) { return a.VF + m * fs; }, [&](int m, double* Tm) {
+    tile_specials(a.opd, c.TI, c.LP, Tm, tsz, 1, spb);
+    __syncthreads();
+    solve_lines<S, WPL>(Tm + z.l * c.LP + HT, tsz, 1, a.opd, z, scl, a.g.rd[DIR], false, spb + z.l * 2 * NSP);
+    __syncthreads();
+    store_tiles<DIR, WPL, true>(c, Tm, tsz, a.R + m * fs, fs, 1);
+  });
 }
 
 // ------------------------------------------------------------------ pass B' (fluxes along B, update, filter)
 // R += D_B(G_B); mode 1: q_out = F_B(c1 qsave + c2 q + c3 dt R) (rk3, tgvsolver.F90:1055-1057,
-// filterq along B); mode 0: R only.
+// filterq along B); mode 0: R only. Every field is independent of the others.
 template <int S, int WPL, int DIR>
 __device__ __forceinline__ void k_pass_vb_body(const PassArgs& a, int bx, int by) {
   extern __shared__ double sm[];
   const TileCtx<DIR, WPL> c(a, bx, by);
   const int tsz = c.TI * c.LP;
-  double* T = sm;
-  double* scan = sm + 5 * tsz;
+  double* scan = sm + 2 * tsz;
   double* spb = scan + c.TI * SCAN_PER_LINE * WPL;
   const int64_t fs = a.g.fs;
-  for (int m = 0; m < 5; ++m) load_tile(c, T + m * tsz, a.VF + (5 + m) * fs);
-  cp_async_wait_all();
-  __syncthreads();
-  tile_specials(a.opd, c.TI, c.LP, T, tsz, 5, spb);
-  __syncthreads();
   const LaneIds z = lane_ids<WPL>();
   double* scl = scan + z.l * SCAN_PER_LINE * WPL;
-  solve_lines<S, WPL>(T + z.l * c.LP + HT, tsz, 5, a.opd, z, scl, a.g.rd[DIR], false, spb + z.l * 5 * 2 * NSP);
-  __syncthreads();
-  if (a.mode == 0) {
-    store_tiles<DIR, WPL, true>(c, T, tsz, a.R, fs, 5);
-    return;
-  }
-  // SSP-RK3 stage update of every field, with the periodic images for the filter
   const int dim = c.dim;
-  if (c.svalid) {
-    const double c1 = a.c1, c2 = a.c2, c3 = a.c3, dt = a.dt;
-    const double* qs = a.qsave + c.sbase;
-    const double* qq = a.q + c.sbase;
-    const double* R = a.R + c.sbase;
-#pragma unroll 1
-    for (int m = 0; m < 5; ++m) {
-      double* Tm = T + m * tsz;
+  stream_fields(c, sm, tsz, 5, [&](int m) { return a.VF + (5 + m) * fs; }, [&](int m, double* Tm) {
+    tile_specials(a.opd, c.TI, c.LP, Tm, tsz, 1, spb);
+    __syncthreads();
+    solve_lines<S, WPL>(Tm + z.l * c.LP + HT, tsz, 1, a.opd, z, scl, a.g.rd[DIR], false, spb + z.l * 2 * NSP);
+    __syncthreads();
+    if (a.mode == 0) {
+      store_tiles<DIR, WPL, true>(c, Tm, tsz, a.R + m * fs, fs, 1);
+      return;
+    }
+    // SSP-RK3 stage update of the field, with the periodic images for the filter
+    if (c.svalid) {
+      const double c1 = a.c1, c2 = a.c2, c3 = a.c3, dt = a.dt;
+      const int64_t fo = m * fs + c.sbase;
+      const double* qs = a.qsave + fo;
+      const double* qq = a.q + fo;
+      const double* R = a.R + fo;
       double* sline = Tm + c.sl * c.LP + HT;
       struct L3 { double r, s, q; };
       c.template for_nodes_batched<4, L3>(0, dim, [&](int n) {
-        const int64_t off = m * fs + (int64_t)n * c.sd;
+        const int64_t off = (int64_t)n * c.sd;
         return L3{R[off], qs[off], (c2 != 0.0) ? qq[off] : 0.0};
       }, [&](int o, int n, const L3& l) {
         const double r = l.r + Tm[o];
@@ -659,15 +684,15 @@ __device__ __forceinline__ void k_pass_vb_body(const PassArgs& a, int bx, int by
         put_images(sline, n, dim, qn);
       });
     }
-  }
-  __syncthreads();
-  if (a.do_filter) {
-    tile_specials(a.opf, c.TI, c.LP, T, tsz, 5, spb);
     __syncthreads();
-    solve_lines<S, WPL>(T + z.l * c.LP + HT, tsz, 5, a.opf, z, scl, 1.0, false, spb + z.l * 5 * 2 * NSP);
-    __syncthreads();
-  }
-  store_tiles<DIR, WPL, false>(c, T, tsz, a.qout, fs, 5);
+    if (a.do_filter) {
+      tile_specials(a.opf, c.TI, c.LP, Tm, tsz, 1, spb);
+      __syncthreads();
+      solve_lines<S, WPL>(Tm + z.l * c.LP + HT, tsz, 1, a.opf, z, scl, 1.0, false, spb + z.l * 2 * NSP);
+      __syncthreads();
+    }
+    store_tiles<DIR, WPL, false>(c, Tm, tsz, a.qout + m * fs, fs, 1);
+  });
 }
 
 // ------------------------------------------------------------------ pass F (filter only, 5 fields)
@@ -676,20 +701,18 @@ __device__ __forceinline__ void k_pass_f_body(const PassArgs& a, int bx, int by)
   extern __shared__ double sm[];
   const TileCtx<DIR, WPL> c(a, bx, by);
   const int tsz = c.TI * c.LP;
-  double* T = sm;
-  double* scan = sm + 5 * tsz;
+  double* scan = sm + 2 * tsz;
   double* spb = scan + c.TI * SCAN_PER_LINE * WPL;
   const int64_t fs = a.g.fs;
-  for (int m = 0; m < 5; ++m) load_tile(c, T + m * tsz, a.q + m * fs);
-  cp_async_wait_all();
-  __syncthreads();
-  tile_specials(a.opf, c.TI, c.LP, T, tsz, 5, spb);
-  __syncthreads();
   const LaneIds z = lane_ids<WPL>();
   double* scl = scan + z.l * SCAN_PER_LINE * WPL;
-  solve_lines<S, WPL>(T + z.l * c.LP + HT, tsz, 5, a.opf, z, scl, 1.0, false, spb + z.l * 5 * 2 * NSP);
-  __syncthreads();
-  store_tiles<DIR, WPL, false>(c, T, tsz, a.q, fs, 5);
+  stream_fields(c, sm, tsz, 5, [&](int m) { return a.q + m * fs; }, [&](int m, double* Tm) {
+    tile_specials(a.opf, c.TI, c.LP, Tm, tsz, 1, spb);
+    __syncthreads();
+    solve_lines<S, WPL>(Tm + z.l * c.LP + HT, tsz, 1, a.opf, z, scl, 1.0, false, spb + z.l * 2 * NSP);
+    __syncthreads();
+    store_tiles<DIR, WPL, false>(c, Tm, tsz, a.q + m * fs, fs, 1);
+  });
 }
 
 // ------------------------------------------------------------------ kernels
