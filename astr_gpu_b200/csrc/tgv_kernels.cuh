@@ -383,7 +383,7 @@ __device__ __forceinline__ void store_tiles(const TileCtx<DIR, WPL>& c, const do
   for (int m = 0; m < nf; ++m) {
     double* dm = d + m * fs;
     const double* Tm = T + m * tsz;
-    if (ADD) c.for_nodes_rmw<4>(0, dim, [&](int n) { return dm[(int64_t)n * c.sd]; },
+    if (ADD) c.for_nodes_rmw<8>(0, dim, [&](int n) { return dm[(int64_t)n * c.sd]; },
                                 [&](int o, int n, double r) { dm[(int64_t)n * c.sd] = r + Tm[o]; });
     else c.for_nodes(0, dim, [&](int o, int n) { dm[(int64_t)n * c.sd] = Tm[o]; });
   }
