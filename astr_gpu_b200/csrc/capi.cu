@@ -32,7 +32,7 @@ struct astr_scheme {
 
 // Launch shape of one pass: solve layout (S rows per lane, WPL warps per line) and TI lines
 // per CTA with tile pitch LP.
-struct PassCfg { int S = 0, WPL = 0, TI = 0, LP = 0; };
+struct PassCfg { int S = 0, WPL = 0, TI = 0, LP = 0, LPW = 1; };
 enum { CFG_A = 0, CFG_B, CFG_C, CFG_VA, CFG_VB, CFG_FC, CFG_FA, NCFG };
 static const int CFG_PASS[NCFG] = {PASS_A, PASS_B, PASS_C, PASS_VA, PASS_VB, PASS_F, PASS_F};
 static const int CFG_DIR[NCFG] = {DIR_A, DIR_B, DIR_C, DIR_A, DIR_B, DIR_C, DIR_A};
@@ -209,6 +209,7 @@ PassArgs base_args(astr_state* st, int id) {
   a.dA = DIR_A; a.dB = DIR_B; a.dC = DIR_C;
   a.TI = pc.TI;
   a.LP = pc.LP;
+  a.LPW = pc.LPW;
   a.R = st->R;
   a.VF = st->VF;
   a.err = st->err;
@@ -235,7 +236,7 @@ cudaError_t run_pass(astr_state* st, int id, PassArgs& a) {
     cudaEventRecord(e1, st->ctx->stream);
     g_timer->ev.push_back(e0);
     g_timer->ev.push_back(e1);
-    g_timer->kind.push_back(pass == PASS_F ? 5 : pass - 1);
+    g_timer->kind.push_back(id == CFG_FA ? 7 : (pass == PASS_F ? 5 : pass - 1));
   }
   return e;
 }
@@ -279,9 +280,13 @@ cudaError_t run_step(astr_state* st, double dt, bool pending_at_start) {
   for (int s = 0; s < 3; ++s) {
     double* qin = (s == 0) ? st->Q0 : st->Q1;
     double* qout = (s == 2) ? st->Q0 : st->Q1;
+    if (filt && (s > 0 || pending_at_start)) {   // the filter along A owed by the last stage
+      PassArgs f = base_args(st, CFG_FA);
+      f.q = qin;
+      if ((e = run_pass(st, CFG_FA, f)) != cudaSuccess) return e;
+    }
     PassArgs a = base_args(st, CFG_A);
     a.q = qin; a.D = st->DA;
-    a.do_filter = filt && (s > 0 || pending_at_start);
     if ((e = run_pass(st, CFG_A, a)) != cudaSuccess) return e;
     a = base_args(st, CFG_B);
     a.q = qin; a.D = st->DB;
@@ -387,17 +392,26 @@ cudaError_t autotune(astr_state* st) {
     for (const Layout& L : kLayouts) {
       const int rows = 32 * L.WPL * L.S;
       if (rows < nsys || 2 * nsys < rows) continue;
-      const int tis[3] = {pick_ti(pass, dim, L.WPL), pick_ti(pass, dim, L.WPL) / 2, pick_ti(pass, dim, L.WPL, 220 * 1024)};
-      for (int ti : tis) {
-        if (ti < 1) continue;
+      // (lines per CTA, lines per warp group): y and z streaming passes also try warps that
+      // loop over 2 lines of a wider tile (rows of 8*TI contiguous bytes in each load)
+      const bool loop_lines = dir != 0 && (pass == PASS_VA || pass == PASS_VB || pass == PASS_F);
+      std::vector<std::pair<int, int>> shapes;
+      for (int ti : {pick_ti(pass, dim, L.WPL), pick_ti(pass, dim, L.WPL) / 2, pick_ti(pass, dim, L.WPL, 220 * 1024)})
+        if (ti >= 1) shapes.push_back({ti, 1});
+      if (loop_lines)
+        for (int ti : {8, 16})
+          if (ti * L.WPL * 32 / 2 <= 512 && (L.WPL == 1 || ti / 2 <= 8)) shapes.push_back({ti, 2});
+      for (const auto& sh : shapes) {
+        const int ti = sh.first;
         PassCfg c;
-        c.S = L.S; c.WPL = L.WPL; c.TI = ti; c.LP = tile_pitch(dim, ti);
+        c.S = L.S; c.WPL = L.WPL; c.TI = ti; c.LP = tile_pitch(dim, ti); c.LPW = sh.second;
         const PassCfg saved = st->cfg[id];
         st->cfg[id] = c;
         PassArgs a = base_args(st, id);
         a.q = st->Q1; a.D = st->DA; a.DA = st->DA; a.DB = st->DB;
-        a.qsave = st->Q1; a.qout = st->Q1; a.mode = 1; a.do_filter = st->p.filter_on;
-        a.c1 = 1.0; a.c2 = 0.0; a.c3 = 0.0; a.dt = 0.0;
+        // stage 2-3 form of the update (q is read), values kept bounded: q <- (q + q) / 2
+        a.qsave = st->Q1; a.qout = st->Q1; a.mode = 1; a.do_filter = (id == CFG_A) ? 0 : st->p.filter_on;
+        a.c1 = 0.5; a.c2 = 0.5; a.c3 = 0.0; a.dt = 0.0;
         float ms = 1e30f;
         if ((e = launch_pass(pass, a, c.S, c.WPL, sm)) == cudaSuccess) {
           cudaEventRecord(t0, sm);
@@ -712,18 +726,19 @@ int astr_state_autotune(astr_state* st, int on) {
   return ASTR_OK;
 }
 
-int astr_state_launch_shapes(astr_state* st, int shapes[28]) {
+int astr_state_launch_shapes(astr_state* st, int shapes[35]) {
   if (!st || !shapes) return ASTR_ERR_ARG;
   for (int id = 0; id < NCFG; ++id) {
-    shapes[4 * id] = st->cfg[id].S;
-    shapes[4 * id + 1] = st->cfg[id].WPL;
-    shapes[4 * id + 2] = st->cfg[id].TI;
-    shapes[4 * id + 3] = st->cfg[id].LP;
+    shapes[5 * id] = st->cfg[id].S;
+    shapes[5 * id + 1] = st->cfg[id].WPL;
+    shapes[5 * id + 2] = st->cfg[id].TI;
+    shapes[5 * id + 3] = st->cfg[id].LP;
+    shapes[5 * id + 4] = st->cfg[id].LPW;
   }
   return ASTR_OK;
 }
 
-int astr_state_set_launch_shape(astr_state* st, int pass, int S, int WPL, int TI) {
+int astr_state_set_launch_shape(astr_state* st, int pass, int S, int WPL, int TI, int LPW) {
   if (!st || pass < 0 || pass >= NCFG) return ASTR_ERR_ARG;
   astr_ctx* ctx = st->ctx;
   bool known = false;
@@ -732,8 +747,12 @@ int astr_state_set_launch_shape(astr_state* st, int pass, int S, int WPL, int TI
   if (!known || 32 * WPL * S < st->hf[dir].nsys()) return fail(ctx, ASTR_ERR_ARG, "layout not compiled or too short");
   if (TI < 1 || (TI & (TI - 1)) || TI * WPL * 32 > 1024 || (WPL > 1 && TI > 15))
     return fail(ctx, ASTR_ERR_ARG, "TI must be a power of 2 with TI*WPL*32 <= 1024");
+  const int pk = CFG_PASS[pass];
+  const bool loop_ok = dir != 0 && (pk == PASS_VA || pk == PASS_VB || pk == PASS_F);
+  if (LPW < 1 || (LPW > 1 && (!loop_ok || TI % LPW != 0)))
+    return fail(ctx, ASTR_ERR_ARG, "lines per warp: 1, or a divisor of TI for the y/z passes A', B' and filter-A");
   PassCfg c;
-  c.S = S; c.WPL = WPL; c.TI = TI; c.LP = tile_pitch(st->g.N[dir], TI);
+  c.S = S; c.WPL = WPL; c.TI = TI; c.LP = tile_pitch(st->g.N[dir], TI); c.LPW = LPW;
   st->cfg[pass] = c;
   st->autotune = false;
   drop_graphs(st);
@@ -802,7 +821,7 @@ int astr_rk3_step_host(astr_state* st, double* q, const int64_t shape[3], const 
   return ASTR_OK;
 }
 
-int astr_pass_timings(astr_state* st, double dt, int nsteps, double ms[7]) {
+int astr_pass_timings(astr_state* st, double dt, int nsteps, double ms[8]) {
   if (!st || !ms || nsteps < 1) return ASTR_ERR_ARG;
   astr_ctx* ctx = st->ctx;
   if (st->nstep + nsteps > st->hist_cap) return fail(ctx, ASTR_ERR_UNSUPPORTED, "history buffer full");
@@ -820,7 +839,7 @@ int astr_pass_timings(astr_state* st, double dt, int nsteps, double ms[7]) {
   g_timer = nullptr;
   if (e != cudaSuccess) return cuda_fail(ctx, e, "timed step");
   CK(cudaStreamSynchronize(ctx->stream));
-  double sum[7] = {0}, cnt[7] = {0};
+  double sum[8] = {0}, cnt[8] = {0};
   for (size_t i = 0; i < timer.kind.size(); ++i) {
     float t = 0.f;
     cudaEventElapsedTime(&t, timer.ev[2 * i], timer.ev[2 * i + 1]);
@@ -828,7 +847,7 @@ int astr_pass_timings(astr_state* st, double dt, int nsteps, double ms[7]) {
     cnt[timer.kind[i]] += 1;
   }
   for (cudaEvent_t ev : timer.ev) cudaEventDestroy(ev);
-  for (int k = 0; k < 7; ++k) ms[k] = cnt[k] > 0 ? sum[k] / cnt[k] : 0.0;
+  for (int k = 0; k < 8; ++k) ms[k] = cnt[k] > 0 ? sum[k] / cnt[k] : 0.0;
   return check_err(st);
 }
 
@@ -1234,8 +1253,13 @@ cudaError_t run_stage_full(astr_state* st, int s, const double* qin, const doubl
   double* DA = G ? G + 4 * DIR_A * fs : st->DA;
   double* DB = G ? G + 4 * DIR_B * fs : st->DB;
   cudaError_t e;
+  if (pending_in && st->p.filter_on) {
+    PassArgs f = base_args(st, CFG_FA);
+    f.q = qi;
+    if ((e = run_pass(st, CFG_FA, f)) != cudaSuccess) return e;
+  }
   PassArgs a = base_args(st, CFG_A);
-  a.q = qi; a.D = DA; a.do_filter = (pending_in && st->p.filter_on) ? 1 : 0;
+  a.q = qi; a.D = DA;
   if ((e = run_pass(st, CFG_A, a)) != cudaSuccess) return e;
   a = base_args(st, CFG_B);
   a.q = qi; a.D = DB;

@@ -185,8 +185,11 @@ cudaError_t launch_pass_batch(int pass, int dir, int S, int WPL, const PassArgs*
   return cudaErrorInvalidValue;
 }
 
-size_t pass_shared_bytes(int pass, int TI, int LP, int WPL) {
-  size_t smem = ((size_t)pass_tiles(pass) * TI * LP + (size_t)TI * (SCAN_PER_LINE * WPL + SP_PER_LINE)) * sizeof(double);
+size_t pass_shared_bytes(int pass, int TI, int LP, int WPL, int LPW) {
+  // streaming passes: one field buffer when warps loop over lines, else two (stream_fields)
+  const bool streaming = pass == PASS_VA || pass == PASS_VB || pass == PASS_F;
+  const size_t tiles = streaming ? (LPW > 1 ? 1 : 2) : pass_tiles(pass);
+  size_t smem = (tiles * TI * LP + (size_t)TI * (SCAN_PER_LINE * WPL + SP_PER_LINE)) * sizeof(double);
   if (pass == PASS_C) smem += 32 * 3 * sizeof(double);
   return smem;
 }

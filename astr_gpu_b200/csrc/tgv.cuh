@@ -32,6 +32,7 @@ struct PassArgs {
   int dir;                  // physical direction of the lines (0 x, 1 y, 2 z)
   int dA, dB, dC;           // physical directions assigned to passes A, B, C
   int TI, LP;               // lines per CTA, tile line pitch
+  int LPW;                  // lines per warp group (y and z streaming passes; 1 elsewhere)
   double* q;                // 5 fields
   const double* qsave;      // 5 fields (RK update)
   double* qout;             // 5 fields (RK update output)
@@ -54,7 +55,7 @@ int pass_tiles(int pass);
 // (device memory), dcum[k] its first CTA, nctas the total.
 cudaError_t launch_pass_batch(int pass, int dir, int S, int WPL, const PassArgs* dargs, const int* dcum, int nbox,
                               int nctas, int threads, size_t smem, cudaStream_t st);
-size_t pass_shared_bytes(int pass, int TI, int LP, int WPL);
+size_t pass_shared_bytes(int pass, int TI, int LP, int WPL, int LPW = 1);
 
 // Batched diagnostics reduce: one CTA per box.
 struct DiagArgs {

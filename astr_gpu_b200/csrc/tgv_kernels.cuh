@@ -18,9 +18,10 @@ template <int DIR, int WPL>
 struct TileCtx {
   static constexpr int o1 = (DIR == 0) ? 1 : 0;
   static constexpr int o2 = (DIR == 2) ? 1 : 2;
-  static constexpr int TPL = 32 * WPL;   // threads per line
+  static constexpr int TPL = 32 * WPL;   // threads per line (x lines)
   int dim, TI, LP;
   int sl, sn0;          // slot role: this thread's line and first node offset
+  int nst;              // node stride of a slot: TPL on x lines, blockDim / TI on y and z lines
   bool svalid;          // that line exists
   int64_t sbase;        // element offset of node 0 of that line
   int64_t sd;
@@ -32,9 +33,11 @@ struct TileCtx {
     if (DIR == 0) {
       sl = threadIdx.x / TPL;
       sn0 = threadIdx.x - sl * TPL;
+      nst = TPL;
     } else {
       sl = threadIdx.x & (a.TI - 1);
       sn0 = threadIdx.x / a.TI;
+      nst = blockDim.x / a.TI;
     }
     const int64_t i1 = (int64_t)bx * a.TI + sl;
     svalid = i1 < a.g.N[o1] + 1;
@@ -44,23 +47,23 @@ struct TileCtx {
   template <class F>
   __device__ __forceinline__ void for_nodes(int n_lo, int n_hi, F f) const {
     const int tix0 = sl * LP + HT;
-    for (int n = n_lo + sn0; n <= n_hi; n += TPL) f(tix0 + n, n);
+    for (int n = n_lo + sn0; n <= n_hi; n += nst) f(tix0 + n, n);
   }
   // Two-phase form for work that reads global memory: ld(n) -> P for NB nodes first (their
   // loads overlap), then use(tile offset, n, P) for the same nodes.
   template <int NB, class P, class Ld, class Use>
   __device__ __forceinline__ void for_nodes_batched(int n_lo, int n_hi, Ld ld, Use use) const {
     const int tix0 = sl * LP + HT;
-    for (int nb = n_lo + sn0; nb <= n_hi; nb += NB * TPL) {
+    for (int nb = n_lo + sn0; nb <= n_hi; nb += NB * nst) {
       P r[NB];
 #pragma unroll
       for (int b = 0; b < NB; ++b) {
-        const int n = nb + b * TPL;
+        const int n = nb + b * nst;
         if (n <= n_hi) r[b] = ld(n);
       }
 #pragma unroll
       for (int b = 0; b < NB; ++b) {
-        const int n = nb + b * TPL;
+        const int n = nb + b * nst;
         if (n <= n_hi) use(tix0 + n, n, r[b]);
       }
     }
@@ -70,16 +73,16 @@ struct TileCtx {
   template <int NB, class Ld, class St>
   __device__ __forceinline__ void for_nodes_rmw(int n_lo, int n_hi, Ld ld, St st) const {
     const int tix0 = sl * LP + HT;
-    for (int nb = n_lo + sn0; nb <= n_hi; nb += NB * TPL) {
+    for (int nb = n_lo + sn0; nb <= n_hi; nb += NB * nst) {
       double r[NB];
 #pragma unroll
       for (int b = 0; b < NB; ++b) {
-        const int n = nb + b * TPL;
+        const int n = nb + b * nst;
         r[b] = (n <= n_hi) ? ld(n) : 0.0;
       }
 #pragma unroll
       for (int b = 0; b < NB; ++b) {
-        const int n = nb + b * TPL;
+        const int n = nb + b * nst;
         if (n <= n_hi) st(tix0 + n, n, r[b]);
       }
     }
@@ -134,10 +137,11 @@ __device__ __forceinline__ void load_tile(const TileCtx<DIR, WPL>& c, double* ti
     return;
   }
   const int64_t sd = c.sd;
+  const int nst = c.nst;
   int n = -HT + c.sn0;
-  for (; n < 0; n += TPL) cp_async8(trow + n, src + (int64_t)(n + dim) * sd);
-  for (; n <= dim; n += TPL) cp_async8(trow + n, src + (int64_t)n * sd);
-  for (; n <= dim + HT; n += TPL) cp_async8(trow + n, src + (int64_t)(n - dim) * sd);
+  for (; n < 0; n += nst) cp_async8(trow + n, src + (int64_t)(n + dim) * sd);
+  for (; n <= dim; n += nst) cp_async8(trow + n, src + (int64_t)n * sd);
+  for (; n <= dim + HT; n += nst) cp_async8(trow + n, src + (int64_t)(n - dim) * sd);
 }
 
 // Write a lane's solution rows (nodes 0..dim) into a tile line, optionally with the periodic
@@ -598,9 +602,22 @@ __device__ __forceinline__ void k_pass_c_body(const PassArgs& a, int bx, int by)
 // buffers: the copies of field m+1 are in flight while field m is solved, and the smaller
 // footprint lets two CTAs share an SM, so one CTA's loads overlap the other's solves.
 // body(m, tile) runs between CTA barriers and leaves the tile free for reuse.
+// With one buffer (nbuf = 1) each field is copied, waited for and processed in turn; the overlap
+// then comes from the other CTAs on the SM.
 template <int DIR, int WPL, class Src, class Body>
-__device__ __forceinline__ void stream_fields(const TileCtx<DIR, WPL>& c, double* buf, int tsz, int nf, Src src,
-                                              Body body) {
+__device__ __forceinline__ void stream_fields(const TileCtx<DIR, WPL>& c, double* buf, int tsz, int nf, int nbuf,
+                                              Src src, Body body) {
+  if (nbuf == 1) {
+#pragma unroll 1
+    for (int m = 0; m < nf; ++m) {
+      load_tile(c, buf, src(m));
+      cp_async_wait_all();
+      __syncthreads();
+      body(m, buf);
+      __syncthreads();
+    }
+    return;
+  }
   load_tile(c, buf, src(0));
   cp_async_commit();
 #pragma unroll 1
@@ -618,6 +635,19 @@ __device__ __forceinline__ void stream_fields(const TileCtx<DIR, WPL>& c, double
   }
 }
 
+// One solve on every line of a tile: the CTA's warps form TI / LPW line groups of WPL warps,
+// and group g solves lines g, g + TI/LPW, ... (LPW lines per group; LPW = 1 on x lines).
+template <int S, int WPL>
+__device__ __forceinline__ void solve_tile(double* tile, int TI, int LP, int LPW, const LineOp& op, const LaneIds& z,
+                                           double* scl, double scale, bool images, const double* spb) {
+  const int ng = TI / LPW;
+#pragma unroll 1
+  for (int k = 0; k < LPW; ++k) {
+    const int l = z.l + k * ng;
+    solve_lines<S, WPL>(tile + l * LP + HT, 0, 1, op, z, scl, scale, images, spb + l * 2 * NSP);
+  }
+}
+
 // ------------------------------------------------------------------ pass A' (fluxes along A)
 // R += D_A(G_A), G_A = VF_A - F_A stored by pass C (convection + diffusion along A).
 template <int S, int WPL, int DIR>
@@ -625,15 +655,15 @@ __device__ __forceinline__ void k_pass_va_body(const PassArgs& a, int bx, int by
   extern __shared__ double sm[];
   const TileCtx<DIR, WPL> c(a, bx, by);
   const int tsz = c.TI * c.LP;
-  double* scan = sm + 2 * tsz;
+  double* scan = sm + (a.LPW > 1 ? 1 : 2) * tsz;
   double* spb = scan + c.TI * SCAN_PER_LINE * WPL;
   const int64_t fs = a.g.fs;
   const LaneIds z = lane_ids<WPL>();
   double* scl = scan + z.l * SCAN_PER_LINE * WPL;
-  stream_fields(c, sm, tsz, 5, [&](int m) { return a.VF + m * fs; }, [&](int m, double* Tm) {
+  stream_fields(c, sm, tsz, 5, a.LPW > 1 ? 1 : 2, [&](int m) { return a.VF + m * fs; }, [&](int m, double* Tm) {
     tile_specials(a.opd, c.TI, c.LP, Tm, tsz, 1, spb);
     __syncthreads();
-    solve_lines<S, WPL>(Tm + z.l * c.LP + HT, tsz, 1, a.opd, z, scl, a.g.rd[DIR], false, spb + z.l * 2 * NSP);
+    solve_tile<S, WPL>(Tm, c.TI, c.LP, a.LPW, a.opd, z, scl, a.g.rd[DIR], false, spb);
     __syncthreads();
     store_tiles<DIR, WPL, true>(c, Tm, tsz, a.R + m * fs, fs, 1);
   });
@@ -647,16 +677,16 @@ __device__ __forceinline__ void k_pass_vb_body(const PassArgs& a, int bx, int by
   extern __shared__ double sm[];
   const TileCtx<DIR, WPL> c(a, bx, by);
   const int tsz = c.TI * c.LP;
-  double* scan = sm + 2 * tsz;
+  double* scan = sm + (a.LPW > 1 ? 1 : 2) * tsz;
   double* spb = scan + c.TI * SCAN_PER_LINE * WPL;
   const int64_t fs = a.g.fs;
   const LaneIds z = lane_ids<WPL>();
   double* scl = scan + z.l * SCAN_PER_LINE * WPL;
   const int dim = c.dim;
-  stream_fields(c, sm, tsz, 5, [&](int m) { return a.VF + (5 + m) * fs; }, [&](int m, double* Tm) {
+  stream_fields(c, sm, tsz, 5, a.LPW > 1 ? 1 : 2, [&](int m) { return a.VF + (5 + m) * fs; }, [&](int m, double* Tm) {
     tile_specials(a.opd, c.TI, c.LP, Tm, tsz, 1, spb);
     __syncthreads();
-    solve_lines<S, WPL>(Tm + z.l * c.LP + HT, tsz, 1, a.opd, z, scl, a.g.rd[DIR], false, spb + z.l * 2 * NSP);
+    solve_tile<S, WPL>(Tm, c.TI, c.LP, a.LPW, a.opd, z, scl, a.g.rd[DIR], false, spb);
     __syncthreads();
     if (a.mode == 0) {
       store_tiles<DIR, WPL, true>(c, Tm, tsz, a.R + m * fs, fs, 1);
@@ -688,7 +718,7 @@ __device__ __forceinline__ void k_pass_vb_body(const PassArgs& a, int bx, int by
     if (a.do_filter) {
       tile_specials(a.opf, c.TI, c.LP, Tm, tsz, 1, spb);
       __syncthreads();
-      solve_lines<S, WPL>(Tm + z.l * c.LP + HT, tsz, 1, a.opf, z, scl, 1.0, false, spb + z.l * 2 * NSP);
+      solve_tile<S, WPL>(Tm, c.TI, c.LP, a.LPW, a.opf, z, scl, 1.0, false, spb);
       __syncthreads();
     }
     store_tiles<DIR, WPL, false>(c, Tm, tsz, a.qout + m * fs, fs, 1);
@@ -701,15 +731,15 @@ __device__ __forceinline__ void k_pass_f_body(const PassArgs& a, int bx, int by)
   extern __shared__ double sm[];
   const TileCtx<DIR, WPL> c(a, bx, by);
   const int tsz = c.TI * c.LP;
-  double* scan = sm + 2 * tsz;
+  double* scan = sm + (a.LPW > 1 ? 1 : 2) * tsz;
   double* spb = scan + c.TI * SCAN_PER_LINE * WPL;
   const int64_t fs = a.g.fs;
   const LaneIds z = lane_ids<WPL>();
   double* scl = scan + z.l * SCAN_PER_LINE * WPL;
-  stream_fields(c, sm, tsz, 5, [&](int m) { return a.q + m * fs; }, [&](int m, double* Tm) {
+  stream_fields(c, sm, tsz, 5, a.LPW > 1 ? 1 : 2, [&](int m) { return a.q + m * fs; }, [&](int m, double* Tm) {
     tile_specials(a.opf, c.TI, c.LP, Tm, tsz, 1, spb);
     __syncthreads();
-    solve_lines<S, WPL>(Tm + z.l * c.LP + HT, tsz, 1, a.opf, z, scl, 1.0, false, spb + z.l * 2 * NSP);
+    solve_tile<S, WPL>(Tm, c.TI, c.LP, a.LPW, a.opf, z, scl, 1.0, false, spb);
     __syncthreads();
     store_tiles<DIR, WPL, false>(c, Tm, tsz, a.q + m * fs, fs, 1);
   });
@@ -772,7 +802,7 @@ ASTR_PASS_KERNELS(k_pass_f, int S ASTR_COMMA int WPL ASTR_COMMA int DIR, S ASTR_
 
 using namespace pass_detail;
 
-inline size_t pass_smem(int pass, int TI, int LP, int WPL);
+inline size_t pass_smem(int pass, int TI, int LP, int WPL, int LPW);
 
 template <class KernT>
 cudaError_t launch_k(KernT kern, dim3 grid, int threads, size_t smem, cudaStream_t st, const PassArgs& a) {
@@ -785,9 +815,10 @@ cudaError_t launch_k(KernT kern, dim3 grid, int threads, size_t smem, cudaStream
 template <int S, int WPL>
 cudaError_t launch_pass_t(int pass, const PassArgs& a, cudaStream_t st) {
   const int o1 = (a.dir == 0) ? 1 : 0, o2 = (a.dir == 2) ? 1 : 2;
-  const size_t smem = pass_smem(pass, a.TI, a.LP, WPL);
+  const int lpw = a.LPW > 1 ? a.LPW : 1;
+  const size_t smem = pass_smem(pass, a.TI, a.LP, WPL, lpw);
   dim3 grid((unsigned)((a.g.N[o1] + 1 + a.TI - 1) / a.TI), (unsigned)(a.g.N[o2] + 1));
-  const int threads = a.TI * WPL * 32;
+  const int threads = (a.TI / lpw) * WPL * 32;
   switch (pass) {
     case PASS_A: return launch_k(k_pass_ab<S, WPL, DIR_A, true>, grid, threads, smem, st, a);
     case PASS_B: return launch_k(k_pass_ab<S, WPL, DIR_B, false>, grid, threads, smem, st, a);
@@ -804,7 +835,7 @@ cudaError_t launch_pass_t(int pass, const PassArgs& a, cudaStream_t st) {
 }
 
 // Dynamic shared memory of one pass launch for a tile of TI lines with pitch LP.
-inline size_t pass_smem(int pass, int TI, int LP, int WPL) { return pass_shared_bytes(pass, TI, LP, WPL); }
+inline size_t pass_smem(int pass, int TI, int LP, int WPL, int LPW) { return pass_shared_bytes(pass, TI, LP, WPL, LPW); }
 
 template <class KernT>
 cudaError_t launch_kb(KernT kern, int nctas, int threads, size_t smem, cudaStream_t st, const BatchArgs& b) {
