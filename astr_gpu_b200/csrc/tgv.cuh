@@ -81,7 +81,7 @@ cudaError_t launch_pack(const BoxGeo& g, double* state, double* user, const int6
 
 enum Pass { PASS_A = 1, PASS_B = 2, PASS_C = 3, PASS_VA = 4, PASS_VB = 5, PASS_F = 6 };
 
-constexpr int SCAN_PER_LINE = 4;   // scan scratch per line in units of WPL doubles (NV <= 2)
+constexpr int SCAN_PER_LINE = 8;   // scan scratch per line in units of WPL doubles (NV <= 4)
 constexpr int SP_SOLVES = 13;      // closure tables kept per line (one per pending solve)
 constexpr int SP_PER_LINE = SP_SOLVES * 2 * NSP;
 

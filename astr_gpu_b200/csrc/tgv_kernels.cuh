@@ -322,14 +322,18 @@ __device__ __forceinline__ void solve_lines_n(double* line, int stride, const Li
   }
 }
 
-// Solve `count` staged lines spaced by `stride`: in pairs for layouts of up to 9 rows per lane
-// (two independent recurrences and scans interleave; 512^3: pass C 11.8 -> 10.7 ms, A and B
-// -7 %), one at a time for 17 rows per lane, where a pair's registers exceed the 128 cap.
+// Solve `count` staged lines spaced by `stride`: four at a time for 5 rows per lane, in pairs
+// for up to 9 rows per lane (independent recurrences and scans interleave; 512^3: pass C
+// 11.8 -> 10.4 ms, A and B -7 %), one at a time for 17 rows per lane, where a pair's registers
+// exceed the 128 cap.
 // sp: this line's closure tables of the `count` solves (see compute_specials).
 template <int S, int WPL>
 __device__ __forceinline__ void solve_lines(double* line, int stride, int count, const LineOp& op, const LaneIds& z,
                                             double* scl, double scale, bool images, const double* sp) {
   int i = 0;
+  if (S <= 5)
+    for (; i + 3 < count; i += 4)
+      solve_lines_n<S, WPL, 4>(line + i * stride, stride, op, z, scl, scale, images, sp + i * 2 * NSP);
   if (S <= 9)
     for (; i + 1 < count; i += 2)
       solve_lines_n<S, WPL, 2>(line + i * stride, stride, op, z, scl, scale, images, sp + i * 2 * NSP);
