@@ -106,14 +106,14 @@ int cuda_fail(astr_ctx* c, cudaError_t e, const char* where) {
 
 // Lines per CTA for a pass along a direction: at most 512 threads and ~110 KB of tiles so that
 // two CTAs fit on an SM.
-int pick_ti(int pass, int dim, int WPL, size_t budget = 110 * 1024) {
+int pick_ti(int pass, int dim, int WPL, int S, size_t budget = 110 * 1024) {
   int ti_thr = 512 / (WPL * 32);
   if (ti_thr < 1) ti_thr = 1;
   const int ntile = pass_tiles(pass);
   int ti = ti_thr > 16 ? 16 : ti_thr;
   if (WPL > 1 && ti > 8) ti = 8;   // one named barrier per line: at most 15 lines
   while (ti > 1) {
-    const size_t bytes = (size_t)ntile * ti * tile_pitch(dim, ti) * 8;
+    const size_t bytes = (size_t)ntile * ti * tile_pitch(dim, ti, S) * 8;
     if (bytes <= budget) break;
     ti >>= 1;
   }
@@ -396,7 +396,7 @@ cudaError_t autotune(astr_state* st) {
       // loop over 2 lines of a wider tile (rows of 8*TI contiguous bytes in each load)
       const bool loop_lines = dir != 0 && (pass == PASS_VA || pass == PASS_VB || pass == PASS_F);
       std::vector<std::pair<int, int>> shapes;
-      for (int ti : {pick_ti(pass, dim, L.WPL), pick_ti(pass, dim, L.WPL) / 2, pick_ti(pass, dim, L.WPL, 220 * 1024)})
+      for (int ti : {pick_ti(pass, dim, L.WPL, L.S), pick_ti(pass, dim, L.WPL, L.S) / 2, pick_ti(pass, dim, L.WPL, L.S, 220 * 1024)})
         if (ti >= 1) shapes.push_back({ti, 1});
       if (loop_lines)
         for (int ti : {8, 16})
@@ -404,7 +404,7 @@ cudaError_t autotune(astr_state* st) {
       for (const auto& sh : shapes) {
         const int ti = sh.first;
         PassCfg c;
-        c.S = L.S; c.WPL = L.WPL; c.TI = ti; c.LP = tile_pitch(dim, ti); c.LPW = sh.second;
+        c.S = L.S; c.WPL = L.WPL; c.TI = ti; c.LP = tile_pitch(dim, ti, L.S); c.LPW = sh.second;
         const PassCfg saved = st->cfg[id];
         st->cfg[id] = c;
         PassArgs a = base_args(st, id);
@@ -595,8 +595,8 @@ int astr_state_create(astr_ctx* ctx, const astr_params* p, astr_state** out) {
     const Layout L = pick_layout(st->hf[d].nsys());
     PassCfg& c = st->cfg[id];
     c.S = L.S; c.WPL = L.WPL;
-    c.TI = pick_ti(CFG_PASS[id], N[d], L.WPL);
-    c.LP = tile_pitch(N[d], c.TI);
+    c.TI = pick_ti(CFG_PASS[id], N[d], L.WPL, L.S);
+    c.LP = tile_pitch(N[d], c.TI, c.S);
   }
   // a small box gains nothing from tuning
   st->autotune = (N[0] + 1) * (int64_t)(N[1] + 1) * (N[2] + 1) >= 100 * 100 * 100;
@@ -752,7 +752,7 @@ int astr_state_set_launch_shape(astr_state* st, int pass, int S, int WPL, int TI
   if (LPW < 1 || (LPW > 1 && (!loop_ok || TI % LPW != 0)))
     return fail(ctx, ASTR_ERR_ARG, "lines per warp: 1, or a divisor of TI for the y/z passes A', B' and filter-A");
   PassCfg c;
-  c.S = S; c.WPL = WPL; c.TI = TI; c.LP = tile_pitch(st->g.N[dir], TI); c.LPW = LPW;
+  c.S = S; c.WPL = WPL; c.TI = TI; c.LP = tile_pitch(st->g.N[dir], TI, S); c.LPW = LPW;
   st->cfg[pass] = c;
   st->autotune = false;
   drop_graphs(st);
@@ -955,7 +955,7 @@ int ens_build(astr_ensemble* e) {
             astr_state* st = e->boxes[b];
             const int dir = CFG_DIR[id];
             PassCfg c;
-            c.S = g.S; c.WPL = g.WPL; c.TI = g.TI[id]; c.LP = tile_pitch(st->g.N[dir], c.TI);
+            c.S = g.S; c.WPL = g.WPL; c.TI = g.TI[id]; c.LP = tile_pitch(st->g.N[dir], c.TI, g.S);
             st->cfg[id] = c;
             PassArgs a = base_args(st, id);
             double* qin = (s == 0) ? st->Q0 : st->Q1;
@@ -1025,7 +1025,7 @@ int ens_tune(astr_ensemble* e, bool timed) {
   for (auto& g : e->groups) {
     for (int id = 0; id < NCFG; ++id) {
       int ti = 16;
-      for (int b : g.members) ti = std::min(ti, pick_ti(CFG_PASS[id], e->boxes[b]->g.N[CFG_DIR[id]], g.WPL));
+      for (int b : g.members) ti = std::min(ti, pick_ti(CFG_PASS[id], e->boxes[b]->g.N[CFG_DIR[id]], g.WPL, g.S));
       g.TI[id] = std::max(ti, 1);
     }
   }
@@ -1057,7 +1057,7 @@ int ens_tune(astr_ensemble* e, bool timed) {
           const int dir = CFG_DIR[id];
           const PassCfg saved = st->cfg[id];
           PassCfg c;
-          c.S = g.S; c.WPL = g.WPL; c.TI = ti; c.LP = tile_pitch(st->g.N[dir], ti);
+          c.S = g.S; c.WPL = g.WPL; c.TI = ti; c.LP = tile_pitch(st->g.N[dir], ti, g.S);
           st->cfg[id] = c;
           PassArgs a = base_args(st, id);
           st->cfg[id] = saved;
@@ -1384,13 +1384,13 @@ int adj_setup(astr_adjoint* A) {
     PassCfg lc;
     lc.S = L.S; lc.WPL = L.WPL;
     lc.TI = std::min(16, 512 / (32 * L.WPL));
-    while (lc.TI > 1 && adj_lines_smem(lc.TI, tile_pitch(st->g.N[d], lc.TI), L.WPL) > 100 * 1024) lc.TI >>= 1;
-    lc.LP = tile_pitch(st->g.N[d], lc.TI);
+    while (lc.TI > 1 && adj_lines_smem(lc.TI, tile_pitch(st->g.N[d], lc.TI, L.S), L.WPL) > 100 * 1024) lc.TI >>= 1;
+    lc.LP = tile_pitch(st->g.N[d], lc.TI, L.S);
     A->lcfg[d] = lc;
     PassCfg gc;
     gc.S = L.S; gc.WPL = L.WPL;
-    gc.TI = pick_ti(PASS_A, st->g.N[d], L.WPL);
-    gc.LP = tile_pitch(st->g.N[d], gc.TI);
+    gc.TI = pick_ti(PASS_A, st->g.N[d], L.WPL, L.S);
+    gc.LP = tile_pitch(st->g.N[d], gc.TI, L.S);
     A->gcfg[d] = gc;
   }
   const int64_t fs = st->g.fs;
@@ -1556,8 +1556,8 @@ int astr_scheme_apply_transpose(astr_ctx* ctx, astr_scheme* s, int dir, const do
   a.p.opd = op.tri.op;
   a.p.dir = dir;
   a.p.TI = std::min(16, 512 / (32 * L.WPL));
-  while (a.p.TI > 1 && adj_lines_smem(a.p.TI, tile_pitch(s->h.dim, a.p.TI), L.WPL) > 100 * 1024) a.p.TI >>= 1;
-  a.p.LP = tile_pitch(s->h.dim, a.p.TI);
+  while (a.p.TI > 1 && adj_lines_smem(a.p.TI, tile_pitch(s->h.dim, a.p.TI, L.S), L.WPL) > 100 * 1024) a.p.TI >>= 1;
+  a.p.LP = tile_pitch(s->h.dim, a.p.TI, L.S);
   a.w = op.w;
   a.in = g;
   a.out = out;

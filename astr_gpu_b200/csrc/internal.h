@@ -42,7 +42,8 @@ void free_devop(DevOp& d);
 
 // Tile line pitch (doubles) for TI lines of dim+1 nodes plus halos, chosen so that line-fastest
 // shared-memory accesses of a warp are free of bank conflicts.
-int tile_pitch(int dim, int TI);
+// Tile line pitch for lines of dim + 1 nodes, TI lines per tile, S rows per lane (schemes.cu).
+int tile_pitch(int dim, int TI, int S);
 
 // Line-level API launch: op along dir over every line of an arbitrary strided array.
 struct ArrDesc { int64_t s[3]; int64_t lb[3]; int64_t n[3]; int64_t fs; };

@@ -106,7 +106,7 @@ static cudaError_t launch_t(const DevOp& op, int dir, const double* f, const Arr
   int TI = 512 / (32 * WPL);   // <= 15 lines when WPL > 1 (one named barrier per line)
   if (TI > 16) TI = 16;
   if (TI < 1) TI = 1;
-  const int LP = tile_pitch(op.op.dim, TI);
+  const int LP = tile_pitch(op.op.dim, TI, S);
   const size_t smem = ((size_t)TI * LP + (size_t)TI * (2 * WPL + 2 * NSP)) * sizeof(double);
   auto kern = k_line_api<S, WPL>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

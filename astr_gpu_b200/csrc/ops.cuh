@@ -16,10 +16,15 @@
 
 namespace astr {
 
-// Tile halo nodes kept on each side of a line. A lane owning the last real row of a system
-// reads a window up to dim + S + 7 (filter, S <= 9); with 16 halo nodes only lanes whose rows are
-// all padding reach past the staged range (window_base).
+// Tile halo nodes kept on each side of a line. The real rows of a system read nodes up to
+// dim + 8 (filter: 3 extension rows and a half-width of 5); the window of the lane holding the
+// last real row reaches S - 1 nodes further for its trailing padding rows: up to dim + 24 for
+// 17 rows per lane. Tile lines of layouts with more than 9 rows per lane therefore end with
+// WIN_SLACK unstaged slots after the high halo (read only for padding rows, which are zeroed
+// before the solve), and only lanes whose rows are all padding reach past that (window_base).
 constexpr int HT = 16;
+constexpr int WIN_SLACK = 8;
+__host__ __device__ constexpr int win_slack(int S) { return S > 9 ? WIN_SLACK : 0; }
 constexpr unsigned FULL = 0xffffffffu;
 
 enum OpKind { OP_DERIV = 0, OP_FILTER = 1, OP_EXPLICIT = 2 };
@@ -193,16 +198,18 @@ __device__ __forceinline__ void stencil_deriv(double (&v)[S], const double (&w)[
   for (int t = 0; t < S; ++t) v[t] = (7.0 / 9.0) * (w[t + 3] - w[t + 1]) + (1.0 / 36.0) * (w[t + 4] - w[t]);
 }
 
-// First node of a lane's window of W nodes starting at n0. Only lanes holding nothing but
-// padding rows run past the staged range (HT covers the others); they read the last W staged
-// nodes instead (their rows are zeroed), so every lane loads its window without per-node clamps.
-template <int W>
+// First node of a lane's window of W nodes starting at n0 (layout of S rows per lane). Only
+// lanes holding nothing but padding rows run past the tile line (nodes up to dim + HT +
+// win_slack(S)); they read its last W slots instead (their rows are zeroed), so every lane loads
+// its window without per-node clamps.
+template <int W, int S>
 __device__ __forceinline__ int window_base(int n0, int dim) {
-  return n0 + W - 1 > dim + HT ? dim + HT - W + 1 : n0;
+  constexpr int top = HT + win_slack(S);
+  return n0 + W - 1 > dim + top ? dim + top - W + 1 : n0;
 }
-template <int W, class Get>
+template <int W, int S, class Get>
 __device__ __forceinline__ void fill_window(double (&w)[W], int n0, int dim, Get f) {
-  const int b = window_base<W>(n0, dim);
+  const int b = window_base<W, S>(n0, dim);
 #pragma unroll
   for (int t = 0; t < W; ++t) w[t] = f(b + t);
 }
@@ -242,7 +249,7 @@ template <int S, class Get>
 __device__ __forceinline__ void rhs_deriv(double (&v)[S], const LineOp& op, int seg, Get f, const double* sp) {
   const int r0 = seg * S;
   double w[S + 4];
-  fill_window<S + 4>(w, r0 - op.ext_lo - 2, op.dim, f);
+  fill_window<S + 4, S>(w, r0 - op.ext_lo - 2, op.dim, f);
   stencil_deriv<S>(v, w);
   apply_specials<S>(v, op, r0, sp);
 }
@@ -323,7 +330,7 @@ template <int S, class Get>
 __device__ __forceinline__ void rhs_filter(double (&v)[S], const LineOp& op, int seg, Get f, const double* sp) {
   const int r0 = seg * S;
   double w[S + 10];
-  fill_window<S + 10>(w, r0 - op.ext_lo - 5, op.dim, f);
+  fill_window<S + 10, S>(w, r0 - op.ext_lo - 5, op.dim, f);
 #pragma unroll
   for (int t = 0; t < S; ++t) {
     double var0 = w[t + 5] + w[t + 5];

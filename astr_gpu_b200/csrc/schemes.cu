@@ -264,8 +264,8 @@ void free_devop(DevOp& d) {
   d.dtab = nullptr;
 }
 
-int tile_pitch(int dim, int TI) {
-  const int need = dim + 1 + 2 * HT;
+int tile_pitch(int dim, int TI, int S) {
+  const int need = dim + 1 + 2 * HT + win_slack(S);   // halos and the window slack (ops.cuh)
   const int want = TI >= 16 ? 1 : 16 / TI;   // residue mod 16 for conflict-free line-fastest access
   int lp = need;
   while ((lp % 16) != (want % 16)) ++lp;

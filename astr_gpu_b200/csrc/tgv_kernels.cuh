@@ -221,19 +221,19 @@ __device__ __forceinline__ double gprim_rt(int K, const double* L, int tsz, int 
 }
 
 // Window of pointwise function K (branch once per solve, not per node).
-template <int W, int DIR>
+template <int W, int S, int DIR>
 __device__ __forceinline__ void prim_window(double (&w)[W], int K, const double* L, int tsz, int n0, int dim,
                                             const Thermo& th) {
   switch (K) {
-    case 0: fill_window<W>(w, n0, dim, [&](int n) { return gprim<0, DIR>(L, tsz, n, th); }); break;
-    case 1: fill_window<W>(w, n0, dim, [&](int n) { return gprim<1, DIR>(L, tsz, n, th); }); break;
-    case 2: fill_window<W>(w, n0, dim, [&](int n) { return gprim<2, DIR>(L, tsz, n, th); }); break;
-    case 3: fill_window<W>(w, n0, dim, [&](int n) { return gprim<3, DIR>(L, tsz, n, th); }); break;
-    case 4: fill_window<W>(w, n0, dim, [&](int n) { return gprim<4, DIR>(L, tsz, n, th); }); break;
-    case 5: fill_window<W>(w, n0, dim, [&](int n) { return gprim<5, DIR>(L, tsz, n, th); }); break;
-    case 6: fill_window<W>(w, n0, dim, [&](int n) { return gprim<6, DIR>(L, tsz, n, th); }); break;
-    case 7: fill_window<W>(w, n0, dim, [&](int n) { return gprim<7, DIR>(L, tsz, n, th); }); break;
-    default: fill_window<W>(w, n0, dim, [&](int n) { return gprim<8, DIR>(L, tsz, n, th); }); break;
+    case 0: fill_window<W, S>(w, n0, dim, [&](int n) { return gprim<0, DIR>(L, tsz, n, th); }); break;
+    case 1: fill_window<W, S>(w, n0, dim, [&](int n) { return gprim<1, DIR>(L, tsz, n, th); }); break;
+    case 2: fill_window<W, S>(w, n0, dim, [&](int n) { return gprim<2, DIR>(L, tsz, n, th); }); break;
+    case 3: fill_window<W, S>(w, n0, dim, [&](int n) { return gprim<3, DIR>(L, tsz, n, th); }); break;
+    case 4: fill_window<W, S>(w, n0, dim, [&](int n) { return gprim<4, DIR>(L, tsz, n, th); }); break;
+    case 5: fill_window<W, S>(w, n0, dim, [&](int n) { return gprim<5, DIR>(L, tsz, n, th); }); break;
+    case 6: fill_window<W, S>(w, n0, dim, [&](int n) { return gprim<6, DIR>(L, tsz, n, th); }); break;
+    case 7: fill_window<W, S>(w, n0, dim, [&](int n) { return gprim<7, DIR>(L, tsz, n, th); }); break;
+    default: fill_window<W, S>(w, n0, dim, [&](int n) { return gprim<8, DIR>(L, tsz, n, th); }); break;
   }
 }
 
@@ -288,7 +288,7 @@ __device__ __forceinline__ void dsolve_n(double (&v)[NV][S], int K0, const PassA
 #pragma unroll
   for (int i = 0; i < NV; ++i) {
     double w[S + 4];
-    prim_window<S + 4, DIR>(w, K0 + i, L0, tsz, r0 - op.ext_lo - 2, op.dim, a.th);
+    prim_window<S + 4, S, DIR>(w, K0 + i, L0, tsz, r0 - op.ext_lo - 2, op.dim, a.th);
     stencil_deriv<S>(v[i], w);
     apply_specials<S>(v[i], op, r0, sp + i * 2 * NSP);
   }
