@@ -272,17 +272,18 @@ class TGVSolver:
         """Per-pass launch-shape autotuning at the first RK3 step (default on above 100^3)."""
         self.ctx.check(self.ctx.L.astr_state_autotune(self._h, int(on)))
 
-    def set_launch_shape(self, pass_name: str, S: int, WPL: int, TI: int, LPW: int = 1):
+    def set_launch_shape(self, pass_name: str, S: int, WPL: int, TI: int, LPW: int = 1, FPS: int = 5):
         """Pin one pass's launch shape (disables autotuning)."""
         names = ["A", "B", "C", "A'", "B'", "F_C", "F_A"]
-        self.ctx.check(self.ctx.L.astr_state_set_launch_shape(self._h, names.index(pass_name), S, WPL, TI, LPW))
+        self.ctx.check(self.ctx.L.astr_state_set_launch_shape(self._h, names.index(pass_name), S, WPL, TI, LPW, FPS))
 
     def launch_shapes(self) -> dict:
-        """{pass: (rows per lane, warps per line, lines per CTA, tile pitch, lines per warp group)}."""
-        buf = (ctypes.c_int * 35)()
+        """{pass: (rows per lane, warps per line, lines per CTA, tile pitch, lines per warp group,
+        fields per step)}."""
+        buf = (ctypes.c_int * 42)()
         self.ctx.check(self.ctx.L.astr_state_launch_shapes(self._h, buf))
         names = ["A", "B", "C", "A'", "B'", "F_C", "F_A"]
-        return {nm: tuple(buf[5 * i:5 * i + 5]) for i, nm in enumerate(names)}
+        return {nm: tuple(buf[6 * i:6 * i + 6]) for i, nm in enumerate(names)}
 
 
 class Ensemble:

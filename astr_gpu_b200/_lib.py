@@ -56,7 +56,7 @@ SIGNATURES = {
     "astr_pass_timings": (_i, [_vp, _d, _i, _dp]),
     "astr_state_autotune": (_i, [_vp, _i]),
     "astr_state_launch_shapes": (_i, [_vp, _ip]),
-    "astr_state_set_launch_shape": (_i, [_vp, _i, _i, _i, _i, _i]),
+    "astr_state_set_launch_shape": (_i, [_vp, _i, _i, _i, _i, _i, _i]),
     "astr_ensemble_create": (_i, [_vp, _pvp, _i, _pvp]),
     "astr_ensemble_destroy": (_i, [_vp]),
     "astr_ensemble_step": (_i, [_vp, _dp, _i]),

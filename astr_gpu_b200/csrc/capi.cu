@@ -32,7 +32,8 @@ struct astr_scheme {
 
 // Launch shape of one pass: solve layout (S rows per lane, WPL warps per line) and TI lines
 // per CTA with tile pitch LP.
-struct PassCfg { int S = 0, WPL = 0, TI = 0, LP = 0, LPW = 1; };
+// FPS: fields per step of A', B' and the filters: 5 (all at once) or 1 (streamed one at a time)
+struct PassCfg { int S = 0, WPL = 0, TI = 0, LP = 0, LPW = 1, FPS = 5; };
 enum { CFG_A = 0, CFG_B, CFG_C, CFG_VA, CFG_VB, CFG_FC, CFG_FA, NCFG };
 static const int CFG_PASS[NCFG] = {PASS_A, PASS_B, PASS_C, PASS_VA, PASS_VB, PASS_F, PASS_F};
 static const int CFG_DIR[NCFG] = {DIR_A, DIR_B, DIR_C, DIR_A, DIR_B, DIR_C, DIR_A};
@@ -55,6 +56,7 @@ struct astr_state {
   PassCfg cfg[NCFG];                       // launch shape of every pass
   bool autotune = true, tuned = false;
   bool pending = false;       // filter along DIR_A of the last stage not yet applied
+  bool split_fa = false;      // that filter as its own streaming pass (else fused into pass A)
   int nstep = 0;
   double time = 0.0;
   std::vector<double> row_key;  // (nstep, time) per history row
@@ -106,10 +108,9 @@ int cuda_fail(astr_ctx* c, cudaError_t e, const char* where) {
 
 // Lines per CTA for a pass along a direction: at most 512 threads and ~110 KB of tiles so that
 // two CTAs fit on an SM.
-int pick_ti(int pass, int dim, int WPL, int S, size_t budget = 110 * 1024) {
+int pick_ti(int ntile, int dim, int WPL, int S, size_t budget = 110 * 1024) {
   int ti_thr = 512 / (WPL * 32);
   if (ti_thr < 1) ti_thr = 1;
-  const int ntile = pass_tiles(pass);
   int ti = ti_thr > 16 ? 16 : ti_thr;
   if (WPL > 1 && ti > 8) ti = 8;   // one named barrier per line: at most 15 lines
   while (ti > 1) {
@@ -210,6 +211,7 @@ PassArgs base_args(astr_state* st, int id) {
   a.TI = pc.TI;
   a.LP = pc.LP;
   a.LPW = pc.LPW;
+  a.FPS = pc.FPS;
   a.R = st->R;
   a.VF = st->VF;
   a.err = st->err;
@@ -280,13 +282,15 @@ cudaError_t run_step(astr_state* st, double dt, bool pending_at_start) {
   for (int s = 0; s < 3; ++s) {
     double* qin = (s == 0) ? st->Q0 : st->Q1;
     double* qout = (s == 2) ? st->Q0 : st->Q1;
-    if (filt && (s > 0 || pending_at_start)) {   // the filter along A owed by the last stage
+    const bool owed = filt && (s > 0 || pending_at_start);   // the filter along A of the last stage
+    if (owed && st->split_fa) {
       PassArgs f = base_args(st, CFG_FA);
       f.q = qin;
       if ((e = run_pass(st, CFG_FA, f)) != cudaSuccess) return e;
     }
     PassArgs a = base_args(st, CFG_A);
     a.q = qin; a.D = st->DA;
+    a.do_filter = owed && !st->split_fa;
     if ((e = run_pass(st, CFG_A, a)) != cudaSuccess) return e;
     a = base_args(st, CFG_B);
     a.q = qin; a.D = st->DB;
@@ -383,6 +387,11 @@ cudaError_t autotune(astr_state* st) {
   cudaEvent_t t0, t1;
   cudaEventCreate(&t0);
   cudaEventCreate(&t1);
+  // pass A is timed without and with the owed filter along A fused in; the filter goes into its
+  // own pass F_A only where A + F_A beat the fused pass
+  const bool filt = st->p.filter_on != 0;
+  float tbest[NCFG], tfused = 1e30f;
+  PassCfg fusedc = st->cfg[CFG_A];
   for (int id = 0; id < NCFG; ++id) {
     const int dir = CFG_DIR[id], pass = CFG_PASS[id];
     const int nsys = st->hf[dir].nsys();
@@ -392,45 +401,60 @@ cudaError_t autotune(astr_state* st) {
     for (const Layout& L : kLayouts) {
       const int rows = 32 * L.WPL * L.S;
       if (rows < nsys || 2 * nsys < rows) continue;
-      // (lines per CTA, lines per warp group): y and z streaming passes also try warps that
-      // loop over 2 lines of a wider tile (rows of 8*TI contiguous bytes in each load)
-      const bool loop_lines = dir != 0 && (pass == PASS_VA || pass == PASS_VB || pass == PASS_F);
-      std::vector<std::pair<int, int>> shapes;
-      for (int ti : {pick_ti(pass, dim, L.WPL, L.S), pick_ti(pass, dim, L.WPL, L.S) / 2, pick_ti(pass, dim, L.WPL, L.S, 220 * 1024)})
-        if (ti >= 1) shapes.push_back({ti, 1});
-      if (loop_lines)
+      // (lines per CTA, lines per warp group, fields per step): A', B' and the filters also try
+      // streaming one field at a time, and along y and z warps that loop over 2 lines of a wider
+      // tile (rows of 8*TI contiguous bytes in each load)
+      const bool streaming = pass == PASS_VA || pass == PASS_VB || pass == PASS_F;
+      struct Shape { int ti, lpw, fps; };
+      std::vector<Shape> shapes;
+      for (int fps : {5, 1}) {
+        if (fps == 1 && !streaming) continue;
+        const int nt = shape_tiles(pass, 1, fps);
+        for (int ti : {pick_ti(nt, dim, L.WPL, L.S), pick_ti(nt, dim, L.WPL, L.S) / 2, pick_ti(nt, dim, L.WPL, L.S, 220 * 1024)})
+          if (ti >= 1) shapes.push_back({ti, 1, fps});
+      }
+      if (streaming && dir != 0)
         for (int ti : {8, 16})
-          if (ti * L.WPL * 32 / 2 <= 512 && (L.WPL == 1 || ti / 2 <= 8)) shapes.push_back({ti, 2});
-      for (const auto& sh : shapes) {
-        const int ti = sh.first;
+          if (ti * L.WPL * 32 / 2 <= 512 && (L.WPL == 1 || ti / 2 <= 8)) shapes.push_back({ti, 2, 1});
+      for (const Shape& sh : shapes) {
+        const int ti = sh.ti;
         PassCfg c;
-        c.S = L.S; c.WPL = L.WPL; c.TI = ti; c.LP = tile_pitch(dim, ti, L.S); c.LPW = sh.second;
+        c.S = L.S; c.WPL = L.WPL; c.TI = ti; c.LP = tile_pitch(dim, ti, L.S); c.LPW = sh.lpw; c.FPS = sh.fps;
         const PassCfg saved = st->cfg[id];
         st->cfg[id] = c;
-        PassArgs a = base_args(st, id);
-        a.q = st->Q1; a.D = st->DA; a.DA = st->DA; a.DB = st->DB;
-        // stage 2-3 form of the update (q is read), values kept bounded: q <- (q + q) / 2
-        a.qsave = st->Q1; a.qout = st->Q1; a.mode = 1; a.do_filter = (id == CFG_A) ? 0 : st->p.filter_on;
-        a.c1 = 0.5; a.c2 = 0.5; a.c3 = 0.0; a.dt = 0.0;
-        float ms = 1e30f;
-        if ((e = launch_pass(pass, a, c.S, c.WPL, sm)) == cudaSuccess) {
-          cudaEventRecord(t0, sm);
-          for (int r = 0; r < 2 && e == cudaSuccess; ++r) e = launch_pass(pass, a, c.S, c.WPL, sm);
-          cudaEventRecord(t1, sm);
-          cudaEventSynchronize(t1);
-          cudaEventElapsedTime(&ms, t0, t1);
-        }
-        if (e != cudaSuccess) {   // a shape the device cannot launch (e.g. too much shared memory)
-          cudaGetLastError();
-          e = cudaSuccess;
-          ms = 1e30f;
+        for (int fused = 0; fused < ((id == CFG_A && filt) ? 2 : 1); ++fused) {
+          PassArgs a = base_args(st, id);
+          a.q = st->Q1; a.D = st->DA; a.DA = st->DA; a.DB = st->DB;
+          // stage 2-3 form of the update (q is read), values kept bounded: q <- (q + q) / 2
+          a.qsave = st->Q1; a.qout = st->Q1; a.mode = 1; a.do_filter = (id == CFG_A) ? fused : st->p.filter_on;
+          a.c1 = 0.5; a.c2 = 0.5; a.c3 = 0.0; a.dt = 0.0;
+          float ms = 1e30f;
+          if ((e = launch_pass(pass, a, c.S, c.WPL, sm)) == cudaSuccess) {
+            cudaEventRecord(t0, sm);
+            for (int r = 0; r < 2 && e == cudaSuccess; ++r) e = launch_pass(pass, a, c.S, c.WPL, sm);
+            cudaEventRecord(t1, sm);
+            cudaEventSynchronize(t1);
+            cudaEventElapsedTime(&ms, t0, t1);
+          }
+          if (e != cudaSuccess) {   // a shape the device cannot launch (e.g. too much shared memory)
+            cudaGetLastError();
+            e = cudaSuccess;
+            ms = 1e30f;
+          }
+          if (fused) {
+            if (ms < tfused) { tfused = ms; fusedc = c; }
+          } else if (ms < best) {
+            best = ms; bestc = c;
+          }
         }
         st->cfg[id] = saved;
-        if (ms < best) { best = ms; bestc = c; }
       }
     }
     st->cfg[id] = bestc;
+    tbest[id] = best;
   }
+  st->split_fa = filt && tbest[CFG_A] + tbest[CFG_FA] < tfused;
+  if (filt && !st->split_fa) st->cfg[CFG_A] = fusedc;
   cudaEventDestroy(t0);
   cudaEventDestroy(t1);
   e = cudaMemsetAsync(st->err, 0, sizeof(int), sm);
@@ -595,7 +619,7 @@ int astr_state_create(astr_ctx* ctx, const astr_params* p, astr_state** out) {
     const Layout L = pick_layout(st->hf[d].nsys());
     PassCfg& c = st->cfg[id];
     c.S = L.S; c.WPL = L.WPL;
-    c.TI = pick_ti(CFG_PASS[id], N[d], L.WPL, L.S);
+    c.TI = pick_ti(pass_tiles(CFG_PASS[id]), N[d], L.WPL, L.S);
     c.LP = tile_pitch(N[d], c.TI, c.S);
   }
   // a small box gains nothing from tuning
@@ -726,19 +750,20 @@ int astr_state_autotune(astr_state* st, int on) {
   return ASTR_OK;
 }
 
-int astr_state_launch_shapes(astr_state* st, int shapes[35]) {
+int astr_state_launch_shapes(astr_state* st, int shapes[42]) {
   if (!st || !shapes) return ASTR_ERR_ARG;
   for (int id = 0; id < NCFG; ++id) {
-    shapes[5 * id] = st->cfg[id].S;
-    shapes[5 * id + 1] = st->cfg[id].WPL;
-    shapes[5 * id + 2] = st->cfg[id].TI;
-    shapes[5 * id + 3] = st->cfg[id].LP;
-    shapes[5 * id + 4] = st->cfg[id].LPW;
+    shapes[6 * id] = st->cfg[id].S;
+    shapes[6 * id + 1] = st->cfg[id].WPL;
+    shapes[6 * id + 2] = st->cfg[id].TI;
+    shapes[6 * id + 3] = st->cfg[id].LP;
+    shapes[6 * id + 4] = st->cfg[id].LPW;
+    shapes[6 * id + 5] = st->cfg[id].FPS;
   }
   return ASTR_OK;
 }
 
-int astr_state_set_launch_shape(astr_state* st, int pass, int S, int WPL, int TI, int LPW) {
+int astr_state_set_launch_shape(astr_state* st, int pass, int S, int WPL, int TI, int LPW, int FPS) {
   if (!st || pass < 0 || pass >= NCFG) return ASTR_ERR_ARG;
   astr_ctx* ctx = st->ctx;
   bool known = false;
@@ -751,8 +776,12 @@ int astr_state_set_launch_shape(astr_state* st, int pass, int S, int WPL, int TI
   const bool loop_ok = dir != 0 && (pk == PASS_VA || pk == PASS_VB || pk == PASS_F);
   if (LPW < 1 || (LPW > 1 && (!loop_ok || TI % LPW != 0)))
     return fail(ctx, ASTR_ERR_ARG, "lines per warp: 1, or a divisor of TI for the y/z passes A', B' and filter-A");
+  const bool streaming = pk == PASS_VA || pk == PASS_VB || pk == PASS_F;
+  if (FPS != 5 && !(FPS == 1 && streaming))
+    return fail(ctx, ASTR_ERR_ARG, "fields per step: 5, or 1 for the passes A', B' and the filters");
+  if (LPW > 1 && FPS != 1) return fail(ctx, ASTR_ERR_ARG, "lines per warp 2 streams one field per step");
   PassCfg c;
-  c.S = S; c.WPL = WPL; c.TI = TI; c.LP = tile_pitch(st->g.N[dir], TI, S); c.LPW = LPW;
+  c.S = S; c.WPL = WPL; c.TI = TI; c.LP = tile_pitch(st->g.N[dir], TI, S); c.LPW = LPW; c.FPS = FPS;
   st->cfg[pass] = c;
   st->autotune = false;
   drop_graphs(st);
@@ -1025,7 +1054,7 @@ int ens_tune(astr_ensemble* e, bool timed) {
   for (auto& g : e->groups) {
     for (int id = 0; id < NCFG; ++id) {
       int ti = 16;
-      for (int b : g.members) ti = std::min(ti, pick_ti(CFG_PASS[id], e->boxes[b]->g.N[CFG_DIR[id]], g.WPL, g.S));
+      for (int b : g.members) ti = std::min(ti, pick_ti(pass_tiles(CFG_PASS[id]), e->boxes[b]->g.N[CFG_DIR[id]], g.WPL, g.S));
       g.TI[id] = std::max(ti, 1);
     }
   }
@@ -1253,13 +1282,15 @@ cudaError_t run_stage_full(astr_state* st, int s, const double* qin, const doubl
   double* DA = G ? G + 4 * DIR_A * fs : st->DA;
   double* DB = G ? G + 4 * DIR_B * fs : st->DB;
   cudaError_t e;
-  if (pending_in && st->p.filter_on) {
+  const bool owed = pending_in && st->p.filter_on;
+  if (owed && st->split_fa) {
     PassArgs f = base_args(st, CFG_FA);
     f.q = qi;
     if ((e = run_pass(st, CFG_FA, f)) != cudaSuccess) return e;
   }
   PassArgs a = base_args(st, CFG_A);
   a.q = qi; a.D = DA;
+  a.do_filter = owed && !st->split_fa;
   if ((e = run_pass(st, CFG_A, a)) != cudaSuccess) return e;
   a = base_args(st, CFG_B);
   a.q = qi; a.D = DB;
@@ -1389,7 +1420,7 @@ int adj_setup(astr_adjoint* A) {
     A->lcfg[d] = lc;
     PassCfg gc;
     gc.S = L.S; gc.WPL = L.WPL;
-    gc.TI = pick_ti(PASS_A, st->g.N[d], L.WPL, L.S);
+    gc.TI = pick_ti(pass_tiles(PASS_A), st->g.N[d], L.WPL, L.S);
     gc.LP = tile_pitch(st->g.N[d], gc.TI, L.S);
     A->gcfg[d] = gc;
   }

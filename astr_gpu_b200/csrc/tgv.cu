@@ -165,7 +165,7 @@ int pass_tiles(int pass) {
   switch (pass) {
     case PASS_A: case PASS_B: return 5;
     case PASS_C: return 10;
-    case PASS_VA: case PASS_VB: case PASS_F: return 2;   // two field buffers (stream_fields)
+    case PASS_VA: case PASS_VB: case PASS_F: return 5;   // all fields at once (see shape_tiles)
   }
   return 0;
 }
@@ -185,10 +185,15 @@ cudaError_t launch_pass_batch(int pass, int dir, int S, int WPL, const PassArgs*
   return cudaErrorInvalidValue;
 }
 
-size_t pass_shared_bytes(int pass, int TI, int LP, int WPL, int LPW) {
-  // streaming passes: one field buffer when warps loop over lines, else two (stream_fields)
-  const bool streaming = pass == PASS_VA || pass == PASS_VB || pass == PASS_F;
-  const size_t tiles = streaming ? (LPW > 1 ? 1 : 2) : pass_tiles(pass);
+int shape_tiles(int pass, int LPW, int FPS) {
+  // A', B' and the filters (stream_fields): all five fields in one buffer, or one field at a time
+  // through one buffer (warps looping over lines) or two
+  if (pass == PASS_VA || pass == PASS_VB || pass == PASS_F) return FPS > 1 ? 5 : (LPW > 1 ? 1 : 2);
+  return pass_tiles(pass);
+}
+
+size_t pass_shared_bytes(int pass, int TI, int LP, int WPL, int LPW, int FPS) {
+  const size_t tiles = shape_tiles(pass, LPW, FPS);
   size_t smem = (tiles * TI * LP + (size_t)TI * (SCAN_PER_LINE * WPL + SP_PER_LINE)) * sizeof(double);
   if (pass == PASS_C) smem += 32 * 3 * sizeof(double);
   return smem;

@@ -33,6 +33,7 @@ struct PassArgs {
   int dA, dB, dC;           // physical directions assigned to passes A, B, C
   int TI, LP;               // lines per CTA, tile line pitch
   int LPW;                  // lines per warp group (y and z streaming passes; 1 elsewhere)
+  int FPS;                  // fields per step of A', B' and the filters: 1 (streaming) or 5
   double* q;                // 5 fields
   const double* qsave;      // 5 fields (RK update)
   double* qout;             // 5 fields (RK update output)
@@ -55,7 +56,10 @@ int pass_tiles(int pass);
 // (device memory), dcum[k] its first CTA, nctas the total.
 cudaError_t launch_pass_batch(int pass, int dir, int S, int WPL, const PassArgs* dargs, const int* dcum, int nbox,
                               int nctas, int threads, size_t smem, cudaStream_t st);
-size_t pass_shared_bytes(int pass, int TI, int LP, int WPL, int LPW = 1);
+size_t pass_shared_bytes(int pass, int TI, int LP, int WPL, int LPW = 1, int FPS = 5);
+// Field tiles of a pass's shared memory for a launch shape (LPW lines per warp group, FPS fields
+// per step of the streaming passes).
+int shape_tiles(int pass, int LPW, int FPS);
 
 // Batched diagnostics reduce: one CTA per box.
 struct DiagArgs {

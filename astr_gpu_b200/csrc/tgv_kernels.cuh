@@ -323,18 +323,18 @@ __device__ __forceinline__ void solve_lines_n(double* line, int stride, const Li
 }
 
 // Solve `count` staged lines spaced by `stride`: four at a time for 5 rows per lane, in pairs
-// for up to 9 rows per lane (independent recurrences and scans interleave; 512^3: pass C
-// 11.8 -> 10.4 ms, A and B -7 %), one at a time for 17 rows per lane, where a pair's registers
-// exceed the 128 cap.
+// for 9 (independent recurrences and scans interleave; 512^3: pass C 11.8 -> 10.4 ms, A and B
+// -7 %), one at a time for 17 rows per lane, where a pair's registers exceed the 128 cap, and
+// for 3, the small boxes' layout.
 // sp: this line's closure tables of the `count` solves (see compute_specials).
 template <int S, int WPL>
 __device__ __forceinline__ void solve_lines(double* line, int stride, int count, const LineOp& op, const LaneIds& z,
                                             double* scl, double scale, bool images, const double* sp) {
   int i = 0;
-  if (S <= 5)
+  if (S == 5)
     for (; i + 3 < count; i += 4)
       solve_lines_n<S, WPL, 4>(line + i * stride, stride, op, z, scl, scale, images, sp + i * 2 * NSP);
-  if (S <= 9)
+  if (S == 5 || S == 9)
     for (; i + 1 < count; i += 2)
       solve_lines_n<S, WPL, 2>(line + i * stride, stride, op, z, scl, scale, images, sp + i * 2 * NSP);
   for (; i < count; ++i)
@@ -611,107 +611,225 @@ __device__ __forceinline__ void k_pass_c_body(const PassArgs& a, int bx, int by)
 // buffers: the copies of field m+1 are in flight while field m is solved, and the smaller
 // footprint lets two CTAs share an SM, so one CTA's loads overlap the other's solves.
 // body(m, tile) runs between CTA barriers and leaves the tile free for reuse.
-// With one buffer (nbuf = 1) each field is copied, waited for and processed in turn; the overlap
-// then comes from the other CTAs on the SM.
+// Fields go in groups of fps (1, or all 5 at once); with one buffer (nbuf = 1) each group is
+// copied, waited for and processed in turn, the overlap then coming from the other CTAs on the
+// SM; with two, group g+1 is copied while group g is solved. body(first field, count, tiles).
 template <int DIR, int WPL, class Src, class Body>
 __device__ __forceinline__ void stream_fields(const TileCtx<DIR, WPL>& c, double* buf, int tsz, int nf, int nbuf,
-                                              Src src, Body body) {
+                                              int fps, Src src, Body body) {
+  const int ngrp = (nf + fps - 1) / fps;
+  const int gsz = fps * tsz;
+  auto load_group = [&](int g, double* dst) {
+    for (int j = 0; j < fps && g * fps + j < nf; ++j) load_tile(c, dst + j * tsz, src(g * fps + j));
+  };
   if (nbuf == 1) {
 #pragma unroll 1
-    for (int m = 0; m < nf; ++m) {
-      load_tile(c, buf, src(m));
+    for (int g = 0; g < ngrp; ++g) {
+      load_group(g, buf);
       cp_async_wait_all();
       __syncthreads();
-      body(m, buf);
+      body(g * fps, min(fps, nf - g * fps), buf);
       __syncthreads();
     }
     return;
   }
-  load_tile(c, buf, src(0));
+  load_group(0, buf);
   cp_async_commit();
 #pragma unroll 1
-  for (int m = 0; m < nf; ++m) {
-    if (m + 1 < nf) {
-      load_tile(c, buf + ((m + 1) & 1) * tsz, src(m + 1));
+  for (int g = 0; g < ngrp; ++g) {
+    if (g + 1 < ngrp) {
+      load_group(g + 1, buf + ((g + 1) & 1) * gsz);
       cp_async_commit();
       cp_async_wait<1>();
     } else {
       cp_async_wait<0>();
     }
     __syncthreads();
-    body(m, buf + (m & 1) * tsz);
+    body(g * fps, min(fps, nf - g * fps), buf + (g & 1) * gsz);
     __syncthreads();
   }
 }
 
-// One solve on every line of a tile: the CTA's warps form TI / LPW line groups of WPL warps,
-// and group g solves lines g, g + TI/LPW, ... (LPW lines per group; LPW = 1 on x lines).
+// `count` solves (tiles spaced by tsz) on every line of a tile: the CTA's warps form TI / LPW
+// line groups of WPL warps, and group g solves lines g, g + TI/LPW, ... (LPW lines per group;
+// LPW = 1 on x lines). spb: closure tables laid out by tile_specials with `count` solves.
 template <int S, int WPL>
-__device__ __forceinline__ void solve_tile(double* tile, int TI, int LP, int LPW, const LineOp& op, const LaneIds& z,
-                                           double* scl, double scale, bool images, const double* spb) {
+__device__ __forceinline__ void solve_tile(double* tile, int tsz, int count, int TI, int LP, int LPW, const LineOp& op,
+                                           const LaneIds& z, double* scl, double scale, const double* spb) {
   const int ng = TI / LPW;
 #pragma unroll 1
   for (int k = 0; k < LPW; ++k) {
     const int l = z.l + k * ng;
-    solve_lines<S, WPL>(tile + l * LP + HT, 0, 1, op, z, scl, scale, images, spb + l * 2 * NSP);
+    solve_lines<S, WPL>(tile + l * LP + HT, tsz, count, op, z, scl, scale, false, spb + l * count * 2 * NSP);
   }
 }
 
-// ------------------------------------------------------------------ pass A' (fluxes along A)
-// R += D_A(G_A), G_A = VF_A - F_A stored by pass C (convection + diffusion along A).
+// Buffers of the streamed passes: one field tile, or two (shape_tiles on the host).
+__device__ __forceinline__ int stream_nbuf(const PassArgs& a) { return a.LPW > 1 ? 1 : 2; }
+
+// ------------------------------------------------------------------ streamed A', B', F
+// The same passes with their fields streamed one at a time (FPS = 1), for large boxes; separate
+// kernels, so that the all-fields forms below keep their own (smaller) register allocation.
 template <int S, int WPL, int DIR>
-__device__ __forceinline__ void k_pass_va_body(const PassArgs& a, int bx, int by) {
+__device__ __forceinline__ void k_pass_vas_body(const PassArgs& a, int bx, int by) {
   extern __shared__ double sm[];
   const TileCtx<DIR, WPL> c(a, bx, by);
   const int tsz = c.TI * c.LP;
-  double* scan = sm + (a.LPW > 1 ? 1 : 2) * tsz;
+  const int nbuf = stream_nbuf(a), fps = 1;
+  double* scan = sm + nbuf * fps * tsz;
   double* spb = scan + c.TI * SCAN_PER_LINE * WPL;
   const int64_t fs = a.g.fs;
   const LaneIds z = lane_ids<WPL>();
   double* scl = scan + z.l * SCAN_PER_LINE * WPL;
-  stream_fields(c, sm, tsz, 5, a.LPW > 1 ? 1 : 2, [&](int m) { return a.VF + m * fs; }, [&](int m, double* Tm) {
-    tile_specials(a.opd, c.TI, c.LP, Tm, tsz, 1, spb);
+  stream_fields(c, sm, tsz, 5, nbuf, fps, [&](int m) { return a.VF + m * fs; }, [&](int m0, int cnt, double* T) {
+    tile_specials(a.opd, c.TI, c.LP, T, tsz, cnt, spb);
     __syncthreads();
-    solve_tile<S, WPL>(Tm, c.TI, c.LP, a.LPW, a.opd, z, scl, a.g.rd[DIR], false, spb);
+    solve_tile<S, WPL>(T, tsz, cnt, c.TI, c.LP, a.LPW, a.opd, z, scl, a.g.rd[DIR], spb);
     __syncthreads();
-    store_tiles<DIR, WPL, true>(c, Tm, tsz, a.R + m * fs, fs, 1);
+    store_tiles<DIR, WPL, true>(c, T, tsz, a.R + m0 * fs, fs, cnt);
   });
 }
 
-// ------------------------------------------------------------------ pass B' (fluxes along B, update, filter)
-// R += D_B(G_B); mode 1: q_out = F_B(c1 qsave + c2 q + c3 dt R) (rk3, tgvsolver.F90:1055-1057,
-// filterq along B); mode 0: R only. Every field is independent of the others.
 template <int S, int WPL, int DIR>
-__device__ __forceinline__ void k_pass_vb_body(const PassArgs& a, int bx, int by) {
+__device__ __forceinline__ void k_pass_vbs_body(const PassArgs& a, int bx, int by) {
   extern __shared__ double sm[];
   const TileCtx<DIR, WPL> c(a, bx, by);
   const int tsz = c.TI * c.LP;
-  double* scan = sm + (a.LPW > 1 ? 1 : 2) * tsz;
+  const int nbuf = stream_nbuf(a), fps = 1;
+  double* scan = sm + nbuf * fps * tsz;
   double* spb = scan + c.TI * SCAN_PER_LINE * WPL;
   const int64_t fs = a.g.fs;
   const LaneIds z = lane_ids<WPL>();
   double* scl = scan + z.l * SCAN_PER_LINE * WPL;
   const int dim = c.dim;
-  stream_fields(c, sm, tsz, 5, a.LPW > 1 ? 1 : 2, [&](int m) { return a.VF + (5 + m) * fs; }, [&](int m, double* Tm) {
-    tile_specials(a.opd, c.TI, c.LP, Tm, tsz, 1, spb);
+  stream_fields(c, sm, tsz, 5, nbuf, fps, [&](int m) { return a.VF + (5 + m) * fs; }, [&](int m0, int cnt, double* T) {
+    tile_specials(a.opd, c.TI, c.LP, T, tsz, cnt, spb);
     __syncthreads();
-    solve_tile<S, WPL>(Tm, c.TI, c.LP, a.LPW, a.opd, z, scl, a.g.rd[DIR], false, spb);
+    solve_tile<S, WPL>(T, tsz, cnt, c.TI, c.LP, a.LPW, a.opd, z, scl, a.g.rd[DIR], spb);
     __syncthreads();
     if (a.mode == 0) {
-      store_tiles<DIR, WPL, true>(c, Tm, tsz, a.R + m * fs, fs, 1);
+      store_tiles<DIR, WPL, true>(c, T, tsz, a.R + m0 * fs, fs, cnt);
       return;
     }
-    // SSP-RK3 stage update of the field, with the periodic images for the filter
+    // SSP-RK3 stage update of the group's fields, with the periodic images for the filter
     if (c.svalid) {
       const double c1 = a.c1, c2 = a.c2, c3 = a.c3, dt = a.dt;
-      const int64_t fo = m * fs + c.sbase;
-      const double* qs = a.qsave + fo;
-      const double* qq = a.q + fo;
-      const double* R = a.R + fo;
+#pragma unroll 1
+      for (int j = 0; j < cnt; ++j) {
+        double* Tm = T + j * tsz;
+        const int64_t fo = (m0 + j) * fs + c.sbase;
+        const double* qs = a.qsave + fo;
+        const double* qq = a.q + fo;
+        const double* R = a.R + fo;
+        double* sline = Tm + c.sl * c.LP + HT;
+        struct L3 { double r, s, q; };
+        c.template for_nodes_batched<4, L3>(0, dim, [&](int n) {
+          const int64_t off = (int64_t)n * c.sd;
+          return L3{R[off], qs[off], (c2 != 0.0) ? qq[off] : 0.0};
+        }, [&](int o, int n, const L3& l) {
+          const double r = l.r + Tm[o];
+          // (c1 qsave + c2 q) + (c3 qrhs) dt in the reference's order, rounded at every step so
+          // that the result does not depend on how the compiler contracts this kernel
+          const double qc = (c2 != 0.0) ? __dmul_rn(c2, l.q) : 0.0;
+          const double qn = __dadd_rn(__dadd_rn(__dmul_rn(c1, l.s), qc), __dmul_rn(__dmul_rn(c3, r), dt));
+          Tm[o] = qn;
+          put_images(sline, n, dim, qn);
+        });
+      }
+    }
+    __syncthreads();
+    if (a.do_filter) {
+      tile_specials(a.opf, c.TI, c.LP, T, tsz, cnt, spb);
+      __syncthreads();
+      solve_tile<S, WPL>(T, tsz, cnt, c.TI, c.LP, a.LPW, a.opf, z, scl, 1.0, spb);
+      __syncthreads();
+    }
+    store_tiles<DIR, WPL, false>(c, T, tsz, a.qout + m0 * fs, fs, cnt);
+  });
+}
+
+template <int S, int WPL, int DIR>
+__device__ __forceinline__ void k_pass_fs_body(const PassArgs& a, int bx, int by) {
+  extern __shared__ double sm[];
+  const TileCtx<DIR, WPL> c(a, bx, by);
+  const int tsz = c.TI * c.LP;
+  const int nbuf = stream_nbuf(a), fps = 1;
+  double* scan = sm + nbuf * fps * tsz;
+  double* spb = scan + c.TI * SCAN_PER_LINE * WPL;
+  const int64_t fs = a.g.fs;
+  const LaneIds z = lane_ids<WPL>();
+  double* scl = scan + z.l * SCAN_PER_LINE * WPL;
+  stream_fields(c, sm, tsz, 5, nbuf, fps, [&](int m) { return a.q + m * fs; }, [&](int m0, int cnt, double* T) {
+    tile_specials(a.opf, c.TI, c.LP, T, tsz, cnt, spb);
+    __syncthreads();
+    solve_tile<S, WPL>(T, tsz, cnt, c.TI, c.LP, a.LPW, a.opf, z, scl, 1.0, spb);
+    __syncthreads();
+    store_tiles<DIR, WPL, false>(c, T, tsz, a.q + m0 * fs, fs, cnt);
+  });
+}
+
+// ------------------------------------------------------------------ pass A' (fluxes along A)
+// R += D_A(G_A), G_A = VF_A - F_A as pass C stored it.
+template <int S, int WPL, int DIR>
+__device__ __forceinline__ void k_pass_va_body(const PassArgs& a, int bx, int by) {
+  extern __shared__ double sm[];
+  const TileCtx<DIR, WPL> c(a, bx, by);
+  const int tsz = c.TI * c.LP;
+  double* T = sm;
+  double* scan = sm + 5 * tsz;
+  double* spb = scan + c.TI * SCAN_PER_LINE * WPL;
+  const int64_t fs = a.g.fs;
+  for (int m = 0; m < 5; ++m) load_tile(c, T + m * tsz, a.VF + m * fs);
+  cp_async_wait_all();
+  __syncthreads();
+  tile_specials(a.opd, c.TI, c.LP, T, tsz, 5, spb);
+  __syncthreads();
+  const LaneIds z = lane_ids<WPL>();
+  double* scl = scan + z.l * SCAN_PER_LINE * WPL;
+  solve_lines<S, WPL>(T + z.l * c.LP + HT, tsz, 5, a.opd, z, scl, a.g.rd[DIR], false, spb + z.l * 5 * 2 * NSP);
+  __syncthreads();
+  store_tiles<DIR, WPL, true>(c, T, tsz, a.R, fs, 5);
+}
+
+// ------------------------------------------------------------------ pass B' (fluxes along B, update, filter)
+// R += D_B(G_B); mode 1: q_out = F_B(c1 qsave + c2 q + c3 dt R) (rk3, tgvsolver.F90:1055-1057,
+// filterq along B); mode 0: R only.
+template <int S, int WPL, int DIR>
+__device__ __forceinline__ void k_pass_vb_body(const PassArgs& a, int bx, int by) {
+  extern __shared__ double sm[];
+  const TileCtx<DIR, WPL> c(a, bx, by);
+  const int tsz = c.TI * c.LP;
+  double* T = sm;
+  double* scan = sm + 5 * tsz;
+  double* spb = scan + c.TI * SCAN_PER_LINE * WPL;
+  const int64_t fs = a.g.fs;
+  for (int m = 0; m < 5; ++m) load_tile(c, T + m * tsz, a.VF + (5 + m) * fs);
+  cp_async_wait_all();
+  __syncthreads();
+  tile_specials(a.opd, c.TI, c.LP, T, tsz, 5, spb);
+  __syncthreads();
+  const LaneIds z = lane_ids<WPL>();
+  double* scl = scan + z.l * SCAN_PER_LINE * WPL;
+  solve_lines<S, WPL>(T + z.l * c.LP + HT, tsz, 5, a.opd, z, scl, a.g.rd[DIR], false, spb + z.l * 5 * 2 * NSP);
+  __syncthreads();
+  if (a.mode == 0) {
+    store_tiles<DIR, WPL, true>(c, T, tsz, a.R, fs, 5);
+    return;
+  }
+  // SSP-RK3 stage update of every field, with the periodic images for the filter
+  const int dim = c.dim;
+  if (c.svalid) {
+    const double c1 = a.c1, c2 = a.c2, c3 = a.c3, dt = a.dt;
+    const double* qs = a.qsave + c.sbase;
+    const double* qq = a.q + c.sbase;
+    const double* R = a.R + c.sbase;
+#pragma unroll 1
+    for (int m = 0; m < 5; ++m) {
+      double* Tm = T + m * tsz;
       double* sline = Tm + c.sl * c.LP + HT;
       struct L3 { double r, s, q; };
       c.template for_nodes_batched<4, L3>(0, dim, [&](int n) {
-        const int64_t off = (int64_t)n * c.sd;
+        const int64_t off = m * fs + (int64_t)n * c.sd;
         return L3{R[off], qs[off], (c2 != 0.0) ? qq[off] : 0.0};
       }, [&](int o, int n, const L3& l) {
         const double r = l.r + Tm[o];
@@ -723,15 +841,15 @@ __device__ __forceinline__ void k_pass_vb_body(const PassArgs& a, int bx, int by
         put_images(sline, n, dim, qn);
       });
     }
+  }
+  __syncthreads();
+  if (a.do_filter) {
+    tile_specials(a.opf, c.TI, c.LP, T, tsz, 5, spb);
     __syncthreads();
-    if (a.do_filter) {
-      tile_specials(a.opf, c.TI, c.LP, Tm, tsz, 1, spb);
-      __syncthreads();
-      solve_tile<S, WPL>(Tm, c.TI, c.LP, a.LPW, a.opf, z, scl, 1.0, false, spb);
-      __syncthreads();
-    }
-    store_tiles<DIR, WPL, false>(c, Tm, tsz, a.qout + m * fs, fs, 1);
-  });
+    solve_lines<S, WPL>(T + z.l * c.LP + HT, tsz, 5, a.opf, z, scl, 1.0, false, spb + z.l * 5 * 2 * NSP);
+    __syncthreads();
+  }
+  store_tiles<DIR, WPL, false>(c, T, tsz, a.qout, fs, 5);
 }
 
 // ------------------------------------------------------------------ pass F (filter only, 5 fields)
@@ -740,18 +858,20 @@ __device__ __forceinline__ void k_pass_f_body(const PassArgs& a, int bx, int by)
   extern __shared__ double sm[];
   const TileCtx<DIR, WPL> c(a, bx, by);
   const int tsz = c.TI * c.LP;
-  double* scan = sm + (a.LPW > 1 ? 1 : 2) * tsz;
+  double* T = sm;
+  double* scan = sm + 5 * tsz;
   double* spb = scan + c.TI * SCAN_PER_LINE * WPL;
   const int64_t fs = a.g.fs;
+  for (int m = 0; m < 5; ++m) load_tile(c, T + m * tsz, a.q + m * fs);
+  cp_async_wait_all();
+  __syncthreads();
+  tile_specials(a.opf, c.TI, c.LP, T, tsz, 5, spb);
+  __syncthreads();
   const LaneIds z = lane_ids<WPL>();
   double* scl = scan + z.l * SCAN_PER_LINE * WPL;
-  stream_fields(c, sm, tsz, 5, a.LPW > 1 ? 1 : 2, [&](int m) { return a.q + m * fs; }, [&](int m, double* Tm) {
-    tile_specials(a.opf, c.TI, c.LP, Tm, tsz, 1, spb);
-    __syncthreads();
-    solve_tile<S, WPL>(Tm, c.TI, c.LP, a.LPW, a.opf, z, scl, 1.0, false, spb);
-    __syncthreads();
-    store_tiles<DIR, WPL, false>(c, Tm, tsz, a.q + m * fs, fs, 1);
-  });
+  solve_lines<S, WPL>(T + z.l * c.LP + HT, tsz, 5, a.opf, z, scl, 1.0, false, spb + z.l * 5 * 2 * NSP);
+  __syncthreads();
+  store_tiles<DIR, WPL, false>(c, T, tsz, a.q, fs, 5);
 }
 
 // ------------------------------------------------------------------ kernels
@@ -807,11 +927,22 @@ ASTR_PASS_KERNELS(k_pass_f, int S ASTR_COMMA int WPL ASTR_COMMA int DIR, S ASTR_
 #undef ASTR_PASS_KERNELS
 #undef ASTR_COMMA
 
+// streamed forms: single-box launches only (the batched ensemble passes take all fields at once)
+#define ASTR_STREAM_KERNEL(NAME)                                         \
+  template <int S, int WPL, int DIR>                                     \
+  __global__ void __launch_bounds__(512) NAME(PassArgs a) {              \
+    NAME##_body<S, WPL, DIR>(a, blockIdx.x, blockIdx.y);                 \
+  }
+ASTR_STREAM_KERNEL(k_pass_vas)
+ASTR_STREAM_KERNEL(k_pass_vbs)
+ASTR_STREAM_KERNEL(k_pass_fs)
+#undef ASTR_STREAM_KERNEL
+
 }  // namespace pass_detail
 
 using namespace pass_detail;
 
-inline size_t pass_smem(int pass, int TI, int LP, int WPL, int LPW);
+inline size_t pass_smem(int pass, int TI, int LP, int WPL, int LPW, int FPS);
 
 template <class KernT>
 cudaError_t launch_k(KernT kern, dim3 grid, int threads, size_t smem, cudaStream_t st, const PassArgs& a) {
@@ -825,16 +956,25 @@ template <int S, int WPL>
 cudaError_t launch_pass_t(int pass, const PassArgs& a, cudaStream_t st) {
   const int o1 = (a.dir == 0) ? 1 : 0, o2 = (a.dir == 2) ? 1 : 2;
   const int lpw = a.LPW > 1 ? a.LPW : 1;
-  const size_t smem = pass_smem(pass, a.TI, a.LP, WPL, lpw);
+  const size_t smem = pass_smem(pass, a.TI, a.LP, WPL, lpw, a.FPS > 1 ? 5 : 1);
   dim3 grid((unsigned)((a.g.N[o1] + 1 + a.TI - 1) / a.TI), (unsigned)(a.g.N[o2] + 1));
   const int threads = (a.TI / lpw) * WPL * 32;
   switch (pass) {
     case PASS_A: return launch_k(k_pass_ab<S, WPL, DIR_A, true>, grid, threads, smem, st, a);
     case PASS_B: return launch_k(k_pass_ab<S, WPL, DIR_B, false>, grid, threads, smem, st, a);
     case PASS_C: return launch_k(k_pass_c<S, WPL, DIR_C>, grid, threads, smem, st, a);
-    case PASS_VA: return launch_k(k_pass_va<S, WPL, DIR_A>, grid, threads, smem, st, a);
-    case PASS_VB: return launch_k(k_pass_vb<S, WPL, DIR_B>, grid, threads, smem, st, a);
+    case PASS_VA:
+      if (a.FPS == 1) return launch_k(k_pass_vas<S, WPL, DIR_A>, grid, threads, smem, st, a);
+      return launch_k(k_pass_va<S, WPL, DIR_A>, grid, threads, smem, st, a);
+    case PASS_VB:
+      if (a.FPS == 1) return launch_k(k_pass_vbs<S, WPL, DIR_B>, grid, threads, smem, st, a);
+      return launch_k(k_pass_vb<S, WPL, DIR_B>, grid, threads, smem, st, a);
     case PASS_F:
+      if (a.FPS == 1) {
+        if (a.dir == DIR_C) return launch_k(k_pass_fs<S, WPL, DIR_C>, grid, threads, smem, st, a);
+        if (a.dir == DIR_A) return launch_k(k_pass_fs<S, WPL, DIR_A>, grid, threads, smem, st, a);
+        return launch_k(k_pass_fs<S, WPL, DIR_B>, grid, threads, smem, st, a);
+      }
       if (a.dir == DIR_C) return launch_k(k_pass_f<S, WPL, DIR_C>, grid, threads, smem, st, a);
       if (a.dir == DIR_A) return launch_k(k_pass_f<S, WPL, DIR_A>, grid, threads, smem, st, a);
       return launch_k(k_pass_f<S, WPL, DIR_B>, grid, threads, smem, st, a);
@@ -844,7 +984,9 @@ cudaError_t launch_pass_t(int pass, const PassArgs& a, cudaStream_t st) {
 }
 
 // Dynamic shared memory of one pass launch for a tile of TI lines with pitch LP.
-inline size_t pass_smem(int pass, int TI, int LP, int WPL, int LPW) { return pass_shared_bytes(pass, TI, LP, WPL, LPW); }
+inline size_t pass_smem(int pass, int TI, int LP, int WPL, int LPW, int FPS) {
+  return pass_shared_bytes(pass, TI, LP, WPL, LPW, FPS);
+}
 
 template <class KernT>
 cudaError_t launch_kb(KernT kern, int nctas, int threads, size_t smem, cudaStream_t st, const BatchArgs& b) {

@@ -30,13 +30,15 @@ sys.path.insert(0, ROOT)
 METRIC = "RK3 grid-point updates/s FP64 TGV 512³ + %HBM peak; adjoint:forward step time"
 UNIT = "grid-point RK3 updates/s"
 B_ALG_STEP = 2504.0      # algorithmic bytes per unique grid point per RK3 step (pass model)
+B_ALG_STEP_FUSED = 2384.0   # the same with the owed filter along A fused into pass A
 # fields read + written per stored point by one launch of each pass (B' reads q for the c2 term at
-# two of the three stages; the filter along A owed by each stage is its own pass, F_A)
+# two of the three stages; the filter along A owed by each stage is its own pass F_A where the
+# autotuner found that faster, else pass A filters first and moves 14 fields)
 PASS_NAMES = ["A", "B", "C", "A'", "B'", "F", "diag", "F_A"]   # astr_pass_timings order
 PASS_FIELDS = {"A": 9, "B": 9, "C": 28, "A'": 15, "B'": 20 + 10 / 3, "F": 10, "F_A": 10}
 PASS_PER_STEP = {"A": 3, "B": 3, "C": 3, "A'": 3, "B'": 3, "F": 3, "F_A": 3}
-# kernels of one filtered RK3 step in the timed region: 7 passes per stage and the diagnostics reduce
-LAUNCHES_PER_STEP = 3 * 7 + 1
+# kernels of one filtered RK3 step in the timed region: 7 passes per stage (6 with filter-A fused
+# into pass A) and the diagnostics reduce
 
 
 def peaks():
@@ -184,9 +186,11 @@ def run_ours(args, ws, rank, local):
     pk, pk_kind = peaks()
     pts = (n + 1) ** 3
     shares = {nm: per[i] * PASS_PER_STEP[nm] for i, nm in enumerate(PASS_NAMES) if nm in PASS_PER_STEP}
+    split_fa = per[PASS_NAMES.index("F_A")] > 0.0   # no F_A launches: filter-A fused into pass A
+    fields = dict(PASS_FIELDS, A=PASS_FIELDS["A"] if split_fa else 14)
     dom = max(shares, key=shares.get)
     di = PASS_NAMES.index(dom)
-    alg_bytes = PASS_FIELDS[dom] * 8.0 * pts
+    alg_bytes = fields[dom] * 8.0 * pts
     achieved = alg_bytes / (per[di] * 1e-3) / 1e9
     traffic = None
     tf = os.path.join(ROOT, "profiles", "dram_traffic.json")
@@ -197,7 +201,7 @@ def run_ours(args, ws, rank, local):
             "alg_bytes_per_launch": alg_bytes, "ms_per_launch": float(per[di]),
             "per_pass_ms": {nm: float(per[i]) for i, nm in enumerate(PASS_NAMES) if nm != "diag"},
             "diag_reduce_ms": float(per[6])}
-    step_bytes = B_ALG_STEP * n ** 3
+    step_bytes = (B_ALG_STEP if split_fa else B_ALG_STEP_FUSED) * n ** 3
     step_roof = {"bytes_per_step": step_bytes, "achieved": step_bytes / (ms_step * 1e-3) / 1e9, "peak": pk,
                  "unit": "GB/s", "frac": step_bytes / (ms_step * 1e-3) / 1e9 / pk, "peak_kind": pk_kind}
 
@@ -241,7 +245,7 @@ def run_ours(args, ws, rank, local):
                        "l2": "inputs larger than L2 (5 x 1.1 GB state per box)", "graph": "one CUDA graph per step",
                        "launch_shapes": {k: list(v) for k, v in s.launch_shapes().items()}},
             "roofline": roof, "step_roofline": step_roof, "cpu_baseline": cpu, "e2e": e2e,
-            "gpu_launches": LAUNCHES_PER_STEP * args.steps, "clocks": clk.summary(),
+            "gpu_launches": (3 * (7 if split_fa else 6) + 1) * args.steps, "clocks": clk.summary(),
         }
         print(json.dumps(line), flush=True)
     s.close()
@@ -465,7 +469,7 @@ def run_profile(args, local):
     s = ag.TGVSolver(ctx, args.size)
     if args.shapes:
         for nm, v in json.loads(args.shapes).items():
-            s.set_launch_shape(nm, v[0], v[1], v[2], v[4] if len(v) > 4 else 1)
+            s.set_launch_shape(nm, v[0], v[1], v[2], v[4] if len(v) > 4 else 1, v[5] if len(v) > 5 else (1 if len(v) > 4 and v[4] > 1 else 5))
     s.init_tgv()
     dt = s.cfl_dt(0.5)
     s.use_graph(False)

@@ -123,13 +123,16 @@ int astr_state_use_graph(astr_state* st, int on);
 /* Per-pass autotuning of the launch shape (rows per lane, warps per line, lines per CTA) at the
  * first RK3 step of a state, on scratch copies of the live fields (default on above 100^3 nodes). */
 int astr_state_autotune(astr_state* st, int on);
-/* Launch shape of each pass A, B, C, A', B', filter-C, filter-A as (S, WPL, TI, LP, LPW): 35 ints. */
-int astr_state_launch_shapes(astr_state* st, int shapes[35]);
+/* Launch shape of each pass A, B, C, A', B', filter-C, filter-A as (S, WPL, TI, LP, LPW, FPS):
+ * 42 ints. */
+int astr_state_launch_shapes(astr_state* st, int shapes[42]);
 /* Pin pass `pass` (0..6 in the order above) to S rows per lane, WPL warps per line, TI lines per
  * CTA (a compiled layout whose 32*WPL*S rows cover the pass's line systems; TI a power of 2) and
  * LPW lines per warp group (1; or a divisor of TI for the y/z passes A', B' and filter-A, whose
- * warps then loop over LPW lines of the tile). */
-int astr_state_set_launch_shape(astr_state* st, int pass, int S, int WPL, int TI, int LPW);
+ * warps then loop over LPW lines of the tile) and FPS fields per step (5: all fields of the pass
+ * at once; or 1 for A', B' and the filter passes, which then stream their independent fields one
+ * at a time; LPW 2 needs FPS 1). */
+int astr_state_set_launch_shape(astr_state* st, int pass, int S, int WPL, int TI, int LPW, int FPS);
 /* Instrumentation (no counterpart in the reference): run `nsteps` RK3 steps eagerly with CUDA
  * events around every pass launch on the context stream and return the mean device time of
  * one launch of each pass, ms[0..7] = A, B, C, A', B', filter-C, diagnostics reduce, filter-A. */

@@ -210,7 +210,8 @@ def test_noncubic_box_steps_match_oracle(ctx, dims):
 
 def test_every_layout_agrees_at_256(ctx):
     """Every compiled solve layout that covers the 257-node lines, pinned on each pass in turn
-    (lines per warp group 2 as well where a pass allows it), gives the state of the default
+    (streamed fields and lines per warp group 2 as well where a pass allows them), gives the
+    state of the default
     shapes after 2 RK3 steps to rounding. At this size the lane holding the last real rows of a
     filter system with 17 rows per lane reaches past the staged halo with its padding rows.
     Layouts with other rows per lane segment the solves differently, so the states agree to
@@ -239,8 +240,10 @@ def test_every_layout_agrees_at_256(ctx):
         for S, W in layouts:
             ti = 2 if W == 4 else 4
             pins = [(nm, S, W, ti)]
-            if nm in ("A'", "B'", "F_A") and W <= 2:
-                pins.append((nm, S, W, 8, 2))
+            if nm in ("A'", "B'", "F_C", "F_A"):   # fields streamed one at a time
+                pins.append((nm, S, W, ti, 1, 1))
+                if nm != "F_C" and W <= 2:      # warps looping over 2 lines of 8
+                    pins.append((nm, S, W, 8, 2, 1))
             for pin in pins:
                 d = _rel_scaled(run(pin), ref)
                 if not d <= 1e-12:
