@@ -14,14 +14,14 @@ namespace astr {
 
 namespace pass_detail {
 
-template <int DIR, int WPL>
+template <int DIR, int WPL, bool LW = false>   // LW: warps may loop over lines (blockDim < TI*TPL)
 struct TileCtx {
   static constexpr int o1 = (DIR == 0) ? 1 : 0;
   static constexpr int o2 = (DIR == 2) ? 1 : 2;
   static constexpr int TPL = 32 * WPL;   // threads per line (x lines)
   int dim, TI, LP;
   int sl, sn0;          // slot role: this thread's line and first node offset
-  int nst;              // node stride of a slot: TPL on x lines, blockDim / TI on y and z lines
+  int nst;              // node stride of a slot: TPL, or blockDim / TI on y/z lines when LW
   bool svalid;          // that line exists
   int64_t sbase;        // element offset of node 0 of that line
   int64_t sd;
@@ -37,7 +37,7 @@ struct TileCtx {
     } else {
       sl = threadIdx.x & (a.TI - 1);
       sn0 = threadIdx.x / a.TI;
-      nst = blockDim.x / a.TI;
+      nst = LW ? (int)blockDim.x / a.TI : TPL;
     }
     const int64_t i1 = (int64_t)bx * a.TI + sl;
     svalid = i1 < a.g.N[o1] + 1;
@@ -112,8 +112,8 @@ __device__ __forceinline__ void cp_async16(uint32_t sdst, const double* gsrc) {
 // The node progression of each thread runs through the low halo, the line and the high halo
 // with the wrap applied per range; x lines (contiguous) copy node pairs with 16-byte copies
 // when the line and the tile row start on 16-byte boundaries.
-template <int DIR, int WPL>
-__device__ __forceinline__ void load_tile(const TileCtx<DIR, WPL>& c, double* tile, const double* __restrict__ fld) {
+template <int DIR, int WPL, bool LW>
+__device__ __forceinline__ void load_tile(const TileCtx<DIR, WPL, LW>& c, double* tile, const double* __restrict__ fld) {
   const int dim = c.dim;
   double* trow = tile + c.sl * c.LP + HT;   // node 0 of the slot line
   if (!c.svalid) {
@@ -171,8 +171,8 @@ __device__ __forceinline__ void put_images(double* line, int n, int dim, double 
 // With TEMP, tile 4 receives the temperature p/rho * gamma M^2 instead of the pressure (the
 // gradient passes need only u, v, w, T). One reciprocal of rho per node; the results equal
 // q2fvar's divisions to within an ulp.
-template <int DIR, int WPL, bool TEMP = false>
-__device__ __forceinline__ void to_prims(const TileCtx<DIR, WPL>& c, double* T, int tsz, const Thermo& th) {
+template <int DIR, int WPL, bool TEMP = false, bool LW = false>
+__device__ __forceinline__ void to_prims(const TileCtx<DIR, WPL, LW>& c, double* T, int tsz, const Thermo& th) {
   c.for_nodes(-HT, c.dim + HT, [&](int o, int) {
     const double q0 = T[o], q1 = T[tsz + o], q2 = T[2 * tsz + o], q3 = T[3 * tsz + o], q4 = T[4 * tsz + o];
     const double ri = 1.0 / q0;
@@ -365,8 +365,8 @@ __device__ __forceinline__ void euler_flux(double rho, double u, double v, doubl
 
 // Store tiles [k0, k0 + nf) (nodes 0..dim of the slot line) to fields dst + m*fs (or add them).
 // x lines store node pairs with 16-byte accesses when aligned.
-template <int DIR, int WPL, bool ADD>
-__device__ __forceinline__ void store_tiles(const TileCtx<DIR, WPL>& c, const double* T, int tsz, double* dst,
+template <int DIR, int WPL, bool ADD, bool LW>
+__device__ __forceinline__ void store_tiles(const TileCtx<DIR, WPL, LW>& c, const double* T, int tsz, double* dst,
                                             int64_t fs, int nf) {
   if (!c.svalid) return;
   double* d = dst + c.sbase;
@@ -614,8 +614,8 @@ __device__ __forceinline__ void k_pass_c_body(const PassArgs& a, int bx, int by)
 // Fields go in groups of fps (1, or all 5 at once); with one buffer (nbuf = 1) each group is
 // copied, waited for and processed in turn, the overlap then coming from the other CTAs on the
 // SM; with two, group g+1 is copied while group g is solved. body(first field, count, tiles).
-template <int DIR, int WPL, class Src, class Body>
-__device__ __forceinline__ void stream_fields(const TileCtx<DIR, WPL>& c, double* buf, int tsz, int nf, int nbuf,
+template <int DIR, int WPL, bool LW, class Src, class Body>
+__device__ __forceinline__ void stream_fields(const TileCtx<DIR, WPL, LW>& c, double* buf, int tsz, int nf, int nbuf,
                                               int fps, Src src, Body body) {
   const int ngrp = (nf + fps - 1) / fps;
   const int gsz = fps * tsz;
@@ -673,7 +673,7 @@ __device__ __forceinline__ int stream_nbuf(const PassArgs& a) { return a.LPW > 1
 template <int S, int WPL, int DIR>
 __device__ __forceinline__ void k_pass_vas_body(const PassArgs& a, int bx, int by) {
   extern __shared__ double sm[];
-  const TileCtx<DIR, WPL> c(a, bx, by);
+  const TileCtx<DIR, WPL, true> c(a, bx, by);
   const int tsz = c.TI * c.LP;
   const int nbuf = stream_nbuf(a), fps = 1;
   double* scan = sm + nbuf * fps * tsz;
@@ -693,7 +693,7 @@ __device__ __forceinline__ void k_pass_vas_body(const PassArgs& a, int bx, int b
 template <int S, int WPL, int DIR>
 __device__ __forceinline__ void k_pass_vbs_body(const PassArgs& a, int bx, int by) {
   extern __shared__ double sm[];
-  const TileCtx<DIR, WPL> c(a, bx, by);
+  const TileCtx<DIR, WPL, true> c(a, bx, by);
   const int tsz = c.TI * c.LP;
   const int nbuf = stream_nbuf(a), fps = 1;
   double* scan = sm + nbuf * fps * tsz;
@@ -751,7 +751,7 @@ __device__ __forceinline__ void k_pass_vbs_body(const PassArgs& a, int bx, int b
 template <int S, int WPL, int DIR>
 __device__ __forceinline__ void k_pass_fs_body(const PassArgs& a, int bx, int by) {
   extern __shared__ double sm[];
-  const TileCtx<DIR, WPL> c(a, bx, by);
+  const TileCtx<DIR, WPL, true> c(a, bx, by);
   const int tsz = c.TI * c.LP;
   const int nbuf = stream_nbuf(a), fps = 1;
   double* scan = sm + nbuf * fps * tsz;
