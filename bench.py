@@ -195,7 +195,8 @@ def run_ours(args, ws, rank, local):
     traffic = None
     tf = os.path.join(ROOT, "profiles", "dram_traffic.json")
     if os.path.exists(tf):
-        traffic = json.load(open(tf)).get(str(n), {}).get(dom)
+        tkey = "A_fused" if dom == "A" and not split_fa else dom
+        traffic = json.load(open(tf)).get(str(n), {}).get(tkey)
     roof = {"kernel": f"pass {dom}", "bound": "hbm", "achieved": achieved, "peak": pk, "unit": "GB/s",
             "frac": achieved / pk, "traffic": traffic, "peak_kind": pk_kind,
             "alg_bytes_per_launch": alg_bytes, "ms_per_launch": float(per[di]),
