@@ -607,13 +607,12 @@ __device__ __forceinline__ void k_pass_c_body(const PassArgs& a, int bx, int by)
 }
 
 // ------------------------------------------------------------------ field streaming
-// Passes whose fields are independent (A', B', F) take one field at a time through two tile
-// buffers: the copies of field m+1 are in flight while field m is solved, and the smaller
-// footprint lets two CTAs share an SM, so one CTA's loads overlap the other's solves.
-// body(m, tile) runs between CTA barriers and leaves the tile free for reuse.
-// Fields go in groups of fps (1, or all 5 at once); with one buffer (nbuf = 1) each group is
-// copied, waited for and processed in turn, the overlap then coming from the other CTAs on the
-// SM; with two, group g+1 is copied while group g is solved. body(first field, count, tiles).
+// Passes whose fields are independent (A', B', F) can take their fields in groups of fps (the
+// streamed kernels below use fps = 1) through one buffer or two. With two, the copies of group g+1
+// are in flight while group g is solved; with one (warps looping over lines), each group is copied,
+// waited for and processed in turn, and the overlap comes from the other CTAs on the SM, which the
+// small footprint lets in. body(first field, count, tiles) runs between CTA barriers and leaves
+// the tiles free for reuse.
 template <int DIR, int WPL, bool LW, class Src, class Body>
 __device__ __forceinline__ void stream_fields(const TileCtx<DIR, WPL, LW>& c, double* buf, int tsz, int nf, int nbuf,
                                               int fps, Src src, Body body) {
