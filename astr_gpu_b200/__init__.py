@@ -268,6 +268,11 @@ class TGVSolver:
     def use_graph(self, on: bool):
         self.ctx.check(self.ctx.L.astr_state_use_graph(self._h, int(on)))
 
+    def split_filter(self, on: bool):
+        """Run the filter along y owed by each stage as its own pass (True) or fused into the
+        first gradient pass (False); turns autotuning off."""
+        self.ctx.check(self.ctx.L.astr_state_split_filter(self._h, int(on)))
+
     def autotune(self, on: bool):
         """Per-pass launch-shape autotuning at the first RK3 step (default on above 100^3)."""
         self.ctx.check(self.ctx.L.astr_state_autotune(self._h, int(on)))

@@ -53,6 +53,7 @@ SIGNATURES = {
     "astr_history": (_i, [_vp, _dp, _i, _ip]),
     "astr_diagnostics": (_i, [_vp, _dp]),
     "astr_state_use_graph": (_i, [_vp, _i]),
+    "astr_state_split_filter": (_i, [_vp, _i]),
     "astr_pass_timings": (_i, [_vp, _d, _i, _dp]),
     "astr_state_autotune": (_i, [_vp, _i]),
     "astr_state_launch_shapes": (_i, [_vp, _ip]),

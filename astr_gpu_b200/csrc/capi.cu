@@ -788,6 +788,14 @@ int astr_state_set_launch_shape(astr_state* st, int pass, int S, int WPL, int TI
   return ASTR_OK;
 }
 
+int astr_state_split_filter(astr_state* st, int on) {
+  if (!st) return ASTR_ERR_ARG;
+  st->split_fa = on != 0;
+  st->autotune = false;
+  drop_graphs(st);
+  return ASTR_OK;
+}
+
 int astr_state_use_graph(astr_state* st, int on) {
   if (!st) return ASTR_ERR_ARG;
   st->use_graph = on != 0;

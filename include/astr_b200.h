@@ -120,6 +120,11 @@ int astr_history(astr_state* st, double* rows, int maxrows, int* nrows);
 int astr_diagnostics(astr_state* st, double out[3]);
 /* Capture each RK3 step as one CUDA graph (default on). */
 int astr_state_use_graph(astr_state* st, int on);
+/* Apply the filter along y owed by each RK3 stage as its own pass (on) or fused into the first
+ * gradient pass (off, the default); the autotuner times both at the first step and keeps the
+ * faster unless this call (which turns autotuning off) or a pinned launch shape came first.
+ * The two differ by rounding only (filterq, tgvsolver.F90:791-883). */
+int astr_state_split_filter(astr_state* st, int on);
 /* Per-pass autotuning of the launch shape (rows per lane, warps per line, lines per CTA) at the
  * first RK3 step of a state, on scratch copies of the live fields (default on above 100^3 nodes). */
 int astr_state_autotune(astr_state* st, int on);
