@@ -431,7 +431,7 @@ cudaError_t autotune(astr_state* st) {
           float ms = 1e30f;
           if ((e = launch_pass(pass, a, c.S, c.WPL, sm)) == cudaSuccess) {
             cudaEventRecord(t0, sm);
-            for (int r = 0; r < 2 && e == cudaSuccess; ++r) e = launch_pass(pass, a, c.S, c.WPL, sm);
+            for (int r = 0; r < 4 && e == cudaSuccess; ++r) e = launch_pass(pass, a, c.S, c.WPL, sm);
             cudaEventRecord(t1, sm);
             cudaEventSynchronize(t1);
             cudaEventElapsedTime(&ms, t0, t1);
