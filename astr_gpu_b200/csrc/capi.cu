@@ -425,8 +425,9 @@ cudaError_t autotune(astr_state* st) {
         for (int fused = 0; fused < ((id == CFG_A && filt) ? 2 : 1); ++fused) {
           PassArgs a = base_args(st, id);
           a.q = st->Q1; a.D = st->DA; a.DA = st->DA; a.DB = st->DB;
-          // stage 2-3 form of the update (q is read), values kept bounded: q <- (q + q) / 2
-          a.qsave = st->Q1; a.qout = st->Q1; a.mode = 1; a.do_filter = (id == CFG_A) ? fused : st->p.filter_on;
+          // stage 2-3 form of the update, reading q (the scratch copy) and qsave (the live state,
+          // only read) from distinct arrays as the step does; values stay bounded: q <- (q + q) / 2
+          a.qsave = st->Q0; a.qout = st->Q1; a.mode = 1; a.do_filter = (id == CFG_A) ? fused : st->p.filter_on;
           a.c1 = 0.5; a.c2 = 0.5; a.c3 = 0.0; a.dt = 0.0;
           float ms = 1e30f;
           if ((e = launch_pass(pass, a, c.S, c.WPL, sm)) == cudaSuccess) {
@@ -1099,8 +1100,9 @@ int ens_tune(astr_ensemble* e, bool timed) {
           PassArgs a = base_args(st, id);
           st->cfg[id] = saved;
           a.q = st->Q1; a.D = st->DA; a.DA = st->DA; a.DB = st->DB; a.partials = nullptr;
-          a.qsave = st->Q1; a.qout = st->Q1; a.mode = 1; a.do_filter = st->p.filter_on;
-          a.c1 = 1.0; a.c2 = 0.0; a.c3 = 0.0; a.dt = 0.0;
+          // stage 2-3 form of the update: q (scratch) and qsave (live state, only read) distinct
+          a.qsave = st->Q0; a.qout = st->Q1; a.mode = 1; a.do_filter = st->p.filter_on;
+          a.c1 = 0.5; a.c2 = 0.5; a.c3 = 0.0; a.dt = 0.0;
           ha.push_back(a);
           hc.push_back(ctas);
           const int o1 = (dir == 0) ? 1 : 0, o2 = (dir == 2) ? 1 : 2;
