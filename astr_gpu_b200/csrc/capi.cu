@@ -106,8 +106,9 @@ int cuda_fail(astr_ctx* c, cudaError_t e, const char* where) {
     if (e_ != cudaSuccess) return cuda_fail(ctx, e_, #call); \
   } while (0)
 
-// Lines per CTA for a pass along a direction: at most 512 threads and ~110 KB of tiles so that
-// two CTAs fit on an SM.
+// Lines per CTA of a launch shape with `ntile` field tiles (shape_tiles) along a direction of dim
+// + 1 nodes, solve layout (S, WPL): at most 512 threads and ~110 KB of tiles, so that two CTAs fit
+// on an SM.
 int pick_ti(int ntile, int dim, int WPL, int S, size_t budget = 110 * 1024) {
   int ti_thr = 512 / (WPL * 32);
   if (ti_thr < 1) ti_thr = 1;
