@@ -455,6 +455,13 @@ __device__ __forceinline__ void k_pass_c_body(const PassArgs& a, int bx, int by)
   double* spv = spb + c.TI * 4 * 2 * NSP;
   double* red = spb + c.TI * SP_PER_LINE;
   const int64_t fs = a.g.fs;
+  // the A and B gradients of the line (read by the flux loop after the C solves) start moving
+  // into L2 now: one bulk prefetch per contiguous x line of each of the 8 fields
+  if (DIR == 0 && c.svalid && c.sn0 < 8 && a.DA && a.DB) {
+    const double* src = (c.sn0 < 4 ? a.DA + c.sn0 * fs : a.DB + (c.sn0 - 4) * fs) + c.sbase;
+    const unsigned bytes = (unsigned)(((c.dim + 1) * 8 + 15) & ~15);   // within the padded row
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
+  }
   for (int m = 0; m < 5; ++m) load_tile(c, T + m * tsz, a.q + m * fs);
   cp_async_wait_all();
   __syncthreads();
