@@ -38,10 +38,12 @@ def _i64(v):
 
 class Context:
     """One device and one CUDA stream (``astr_init``). ``stream`` may be a ``torch.cuda.Stream``
-    or a raw ``cudaStream_t`` integer; by default the library owns a non-blocking stream."""
+    or a raw ``cudaStream_t`` integer; by default the library owns a non-blocking stream.
+    ``strict`` runs everything made from this context through the strict-parity build of the
+    library (no multiply-add contraction)."""
 
-    def __init__(self, device: int = 0, stream=None):
-        self.L = _lib.load()
+    def __init__(self, device: int = 0, stream=None, strict: bool = False):
+        self.L = _lib.load(strict)
         h = ctypes.c_void_p()
         rc = self.L.astr_init(device, ctypes.byref(h))
         if rc != 0:

@@ -10,6 +10,8 @@ import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libastr_b200.so")
+# the same C ABI built without multiply-add contraction (-fmad=false), for strict-parity checks
+STRICT_LIB_PATH = os.path.join(HERE, "libastr_b200_strict.so")
 
 ASTR_OK, ASTR_ERR_ARG, ASTR_ERR_CUDA, ASTR_ERR_STATE, ASTR_ERR_UNSUPPORTED, ASTR_ERR_NOMEM = 0, -1, -2, -3, -4, -5
 ASTR_HOST, ASTR_DEVICE = 0, 1
@@ -70,19 +72,21 @@ SIGNATURES = {
     "astr_cfl_dt_noalloc": (_i, [_vp, _vp, _i64p, _i64p, _i, _i, _i, _d, _d, _d, _dp]),
 }
 
-_lib = None
+_libs = {}
 
 
-def load():
-    """Load the shared library (no compute happens here; works on a machine without a GPU)."""
-    global _lib
-    if _lib is None:
-        if not os.path.exists(LIB_PATH):
-            raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -m astr_gpu_b200.build`")
-        L = ctypes.CDLL(LIB_PATH)
+def load(strict: bool = False):
+    """Load the shared library (no compute happens here; works on a machine without a GPU).
+    `strict` loads the variant built with -fmad=false."""
+    path = STRICT_LIB_PATH if strict else LIB_PATH
+    if path not in _libs:
+        if not os.path.exists(path):
+            raise RuntimeError(f"{path} is missing: build it with `python -m astr_gpu_b200.build"
+                               f"{' --strict' if strict else ''}`")
+        L = ctypes.CDLL(path)
         for name, (res, args) in SIGNATURES.items():
             fn = getattr(L, name)
             fn.restype = res
             fn.argtypes = args
-        _lib = L
-    return _lib
+        _libs[path] = L
+    return _libs[path]

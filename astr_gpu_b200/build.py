@@ -1,6 +1,9 @@
-"""Build the sm_100a shared library in-tree: astr_gpu_b200/libastr_b200.so.
+"""Build the sm_100a shared library in-tree: astr_gpu_b200/libastr_b200.so, and its strict-parity
+variant astr_gpu_b200/libastr_b200_strict.so (the same sources with -fmad=false: no multiply-add
+contraction, as the reference's gfortran build without -march emits none), used to attribute any
+difference from the oracle above rounding to the algorithm rather than to contraction.
 
-    python -m astr_gpu_b200.build [--force] [--verbose]
+    python -m astr_gpu_b200.build [--force] [--verbose] [--strict]
 """
 from __future__ import annotations
 
@@ -12,6 +15,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libastr_b200.so")
+LIB_STRICT = os.path.join(HERE, "libastr_b200_strict.so")
 SOURCES = ["capi.cu", "tgv.cu", "lines.cu", "schemes.cu", "tgv_l3_1.cu", "tgv_l5_1.cu", "tgv_l9_1.cu", "tgv_l9_2.cu",
            "tgv_l9_4.cu", "tgv_l5_2.cu", "tgv_l5_4.cu", "tgv_l17_1.cu", "noalloc.cu", "adjoint.cu", "adj_l3_1.cu", "adj_l5_1.cu",
            "adj_l9_1.cu", "adj_l9_2.cu", "adj_l9_4.cu", "adj_l5_2.cu", "adj_l5_4.cu"]
@@ -26,24 +30,28 @@ def nvcc() -> str:
     raise RuntimeError("nvcc not found")
 
 
-def _stale() -> bool:
-    if not os.path.exists(LIB):
+def _stale(lib: str) -> bool:
+    if not os.path.exists(lib):
         return True
-    t = os.path.getmtime(LIB)
+    t = os.path.getmtime(lib)
     deps = [os.path.join(CSRC, f) for f in SOURCES + HEADERS]
     deps.append(os.path.join(os.path.dirname(HERE), "include", "astr_b200.h"))
     return any(os.path.getmtime(d) > t for d in deps)
 
 
-def build(force: bool = False, verbose: bool = False, extra: list[str] | None = None) -> str:
-    """Compile each translation unit in parallel, then link the shared library."""
-    if not force and not _stale():
-        return LIB
-    objdir = os.path.join(HERE, "_build")
+def build(force: bool = False, verbose: bool = False, extra: list[str] | None = None, strict: bool = False) -> str:
+    """Compile each translation unit in parallel, then link the shared library (the strict-parity
+    variant with `strict`)."""
+    lib = LIB_STRICT if strict else LIB
+    if not force and not _stale(lib):
+        return lib
+    objdir = os.path.join(HERE, "_build_strict" if strict else "_build")
     os.makedirs(objdir, exist_ok=True)
     flags = [*ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC"]
     if verbose:
         flags.append("-Xptxas=-v")
+    if strict:
+        flags.append("-fmad=false")
     if extra:
         flags.extend(extra)
     procs, objs = [], []
@@ -59,14 +67,13 @@ def build(force: bool = False, verbose: bool = False, extra: list[str] | None = 
         failed |= p.returncode != 0
     if failed:
         raise RuntimeError("nvcc failed:\n" + "".join(logs))
-    res = subprocess.run([nvcc(), *ARCH, "-shared", "-o", LIB, *objs], capture_output=True, text=True)
+    res = subprocess.run([nvcc(), *ARCH, "-shared", "-o", lib, *objs], capture_output=True, text=True)
     if res.returncode != 0:
         raise RuntimeError("link failed:\n" + res.stdout + res.stderr)
     if verbose:
         sys.stdout.write("".join(logs))
-    return LIB
+    return lib
 
 
 if __name__ == "__main__":
-    build(force="--force" in sys.argv, verbose="--verbose" in sys.argv)
-    print(LIB)
+    print(build(force="--force" in sys.argv, verbose="--verbose" in sys.argv, strict="--strict" in sys.argv))

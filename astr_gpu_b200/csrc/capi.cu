@@ -22,6 +22,8 @@ struct astr_ctx {
   cudaStream_t stream = nullptr;
   bool own_stream = false;
   std::string err;
+  double* stage = nullptr;     // device staging of the line calls on host arrays (grows, kept)
+  size_t stage_bytes = 0;
 };
 
 struct astr_scheme {
@@ -100,6 +102,22 @@ int fail(astr_ctx* c, int code, const std::string& msg) {
 int cuda_fail(astr_ctx* c, cudaError_t e, const char* where) {
   return fail(c, ASTR_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
 }
+// Makes a context's device current for the duration of one C-ABI call and restores the caller's
+// device afterwards, so that allocations, launches and graph captures of a context whose device is
+// not the caller's current one land on the right GPU. dev < 0 (a null handle) does nothing.
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    int cur = -1;
+    if (dev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != dev && cudaSetDevice(dev) == cudaSuccess) prev = cur;
+  }
+  ~DeviceGuard() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+  DeviceGuard(const DeviceGuard&) = delete;
+  DeviceGuard& operator=(const DeviceGuard&) = delete;
+};
+
 #define CK(call)                                          \
   do {                                                    \
     cudaError_t e_ = (call);                              \
@@ -160,23 +178,28 @@ int line_call(astr_ctx* ctx, const astr_scheme* s, int dir, const double* f, con
   double *tf = nullptr, *to = nullptr;
   const size_t fb = (size_t)fa.fs * nfields * sizeof(double), ob = (size_t)oa.fs * nfields * sizeof(double);
   if (where == ASTR_HOST) {
-    CK(cudaMalloc(&tf, fb));
-    CK(cudaMalloc(&to, ob));
+    // the context's staging buffer holds the input and the output; it grows when a call needs
+    // more and is kept for the next call (freed by astr_destroy)
+    const size_t fpad = (fb + 255) / 256 * 256;
+    if (ctx->stage_bytes < fpad + ob) {
+      CK(cudaStreamSynchronize(ctx->stream));
+      if (ctx->stage) cudaFree(ctx->stage);
+      ctx->stage = nullptr;
+      ctx->stage_bytes = 0;
+      if (cudaMalloc(&ctx->stage, fpad + ob) != cudaSuccess) return fail(ctx, ASTR_ERR_NOMEM, "line call staging");
+      ctx->stage_bytes = fpad + ob;
+    }
+    tf = ctx->stage;
+    to = ctx->stage + fpad / sizeof(double);
     CK(cudaMemcpyAsync(tf, f, fb, cudaMemcpyHostToDevice, ctx->stream));
     df_ = tf;
     dout = to;
   }
   cudaError_t e = launch_line_api(s->d, dir, df_, fa, dout, oa, nfields, scale, ctx->stream);
-  if (e != cudaSuccess) {
-    if (tf) cudaFree(tf);
-    if (to) cudaFree(to);
-    return cuda_fail(ctx, e, "line kernel");
-  }
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "line kernel");
   if (where == ASTR_HOST) {
     CK(cudaMemcpyAsync(out, to, ob, cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
-    cudaFree(tf);
-    cudaFree(to);
   }
   return ASTR_OK;
 }
@@ -474,6 +497,7 @@ void drop_graphs(astr_state* st) {
 
 // Used by noalloc.cu.
 cudaStream_t astr_ctx_stream(astr_ctx* ctx) { return ctx->stream; }
+int astr_ctx_device(astr_ctx* ctx) { return ctx->device; }
 void astr_ctx_set_error(astr_ctx* ctx, const char* msg) { ctx->err = msg; }
 
 extern "C" {
@@ -484,7 +508,7 @@ int astr_init(int device, astr_ctx** out) {
   int n = 0;
   if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) return ASTR_ERR_CUDA;
   if (device < 0 || device >= n) return ASTR_ERR_ARG;
-  if (cudaSetDevice(device) != cudaSuccess) return ASTR_ERR_CUDA;
+  const DeviceGuard dg_(device);   // the stream belongs to `device`; the caller's device is restored
   astr_ctx* c = new (std::nothrow) astr_ctx();
   if (!c) return ASTR_ERR_NOMEM;
   c->device = device;
@@ -495,7 +519,12 @@ int astr_init(int device, astr_ctx** out) {
 }
 
 int astr_destroy(astr_ctx* c) {
+  const DeviceGuard dg_(c ? c->device : -1);
   if (!c) return ASTR_ERR_ARG;
+  if (c->stage) {
+    cudaStreamSynchronize(c->stream);
+    cudaFree(c->stage);
+  }
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return ASTR_OK;
@@ -504,6 +533,7 @@ int astr_destroy(astr_ctx* c) {
 const char* astr_last_error(astr_ctx* c) { return c ? c->err.c_str() : "null context"; }
 
 int astr_set_stream(astr_ctx* ctx, void* s) {
+  const DeviceGuard dg_(ctx ? ctx->device : -1);
   if (!ctx) return ASTR_ERR_ARG;
   if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
   ctx->stream = (cudaStream_t)s;
@@ -512,12 +542,14 @@ int astr_set_stream(astr_ctx* ctx, void* s) {
 }
 
 int astr_synchronize(astr_ctx* ctx) {
+  const DeviceGuard dg_(ctx ? ctx->device : -1);
   if (!ctx) return ASTR_ERR_ARG;
   CK(cudaStreamSynchronize(ctx->stream));
   return ASTR_OK;
 }
 
 int astr_fd_scheme_create(astr_ctx* ctx, const char scheme[4], int ntype, int dim, astr_scheme** out) {
+  const DeviceGuard dg_(ctx ? ctx->device : -1);
   if (!ctx || !scheme || !out) return fail(ctx, ASTR_ERR_ARG, "null argument");
   astr_scheme* s = new astr_scheme();
   s->ctx = ctx;
@@ -535,6 +567,7 @@ int astr_fd_scheme_create(astr_ctx* ctx, const char scheme[4], int ntype, int di
 
 int astr_filter_create(astr_ctx* ctx, int ntype, int dim, double alpha_f, double beta_halo, double beta_bound,
                        int boundary_no_filter, astr_scheme** out) {
+  const DeviceGuard dg_(ctx ? ctx->device : -1);
   if (!ctx || !out) return fail(ctx, ASTR_ERR_ARG, "null argument");
   if (ntype < 1 || ntype > 4 || dim < 16) return fail(ctx, ASTR_ERR_ARG, "bad ntype or dim < 16");
   astr_scheme* s = new astr_scheme();
@@ -549,6 +582,7 @@ int astr_filter_create(astr_ctx* ctx, int ntype, int dim, double alpha_f, double
 }
 
 int astr_scheme_destroy(astr_scheme* s) {
+  const DeviceGuard dg_(s && s->ctx ? s->ctx->device : -1);
   if (!s) return ASTR_ERR_ARG;
   free_devop(s->d);
   delete s;
@@ -571,6 +605,7 @@ int astr_scheme_ac(const astr_scheme* s, double* ac, int* first_node, int* last_
 int astr_deriv_lines(astr_ctx* ctx, const astr_scheme* s, int dir, const double* f, const int64_t f_shape[3],
                      const int64_t f_lbound[3], double* df, const int64_t df_shape[3], const int64_t df_lbound[3],
                      int nfields, double scale, int where) {
+  const DeviceGuard dg_(ctx ? ctx->device : -1);
   if (s && s->h.kind == OP_FILTER) return fail(ctx, ASTR_ERR_ARG, "scheme is a filter");
   return line_call(ctx, s, dir, f, f_shape, f_lbound, df, df_shape, df_lbound, nfields, scale, where);
 }
@@ -578,11 +613,13 @@ int astr_deriv_lines(astr_ctx* ctx, const astr_scheme* s, int dir, const double*
 int astr_filter_lines(astr_ctx* ctx, const astr_scheme* s, int dir, const double* f, const int64_t f_shape[3],
                       const int64_t f_lbound[3], double* ff, const int64_t ff_shape[3], const int64_t ff_lbound[3],
                       int nfields, int where) {
+  const DeviceGuard dg_(ctx ? ctx->device : -1);
   if (s && s->h.kind != OP_FILTER) return fail(ctx, ASTR_ERR_ARG, "scheme is not a filter");
   return line_call(ctx, s, dir, f, f_shape, f_lbound, ff, ff_shape, ff_lbound, nfields, 1.0, where);
 }
 
 int astr_state_create(astr_ctx* ctx, const astr_params* p, astr_state** out) {
+  const DeviceGuard dg_(ctx ? ctx->device : -1);
   if (!ctx || !p || !out) return fail(ctx, ASTR_ERR_ARG, "null argument");
   const int N[3] = {p->im, p->jm, p->km};
   for (int d = 0; d < 3; ++d)
@@ -653,6 +690,7 @@ int astr_state_create(astr_ctx* ctx, const astr_params* p, astr_state** out) {
 }
 
 int astr_state_destroy(astr_state* st) {
+  const DeviceGuard dg_(st ? st->ctx->device : -1);
   if (!st) return ASTR_ERR_ARG;
   drop_graphs(st);
   for (auto& kv : st->ops) { free_devop(kv.second.first); free_devop(kv.second.second); }
@@ -665,6 +703,7 @@ int astr_state_destroy(astr_state* st) {
 }
 
 int astr_state_init_tgv(astr_state* st) {
+  const DeviceGuard dg_(st ? st->ctx->device : -1);
   if (!st) return ASTR_ERR_ARG;
   astr_ctx* ctx = st->ctx;
   const int N[3] = {st->p.im, st->p.jm, st->p.km};
@@ -697,6 +736,7 @@ int astr_state_init_tgv(astr_state* st) {
 }
 
 int astr_state_upload(astr_state* st, const double* q, const int64_t shape[3], const int64_t lbound[3], int where) {
+  const DeviceGuard dg_(st ? st->ctx->device : -1);
   if (!st || !q || !shape || !lbound) return ASTR_ERR_ARG;
   int rc = copy_fields(st, st->Q0, const_cast<double*>(q), shape, lbound, 1, where);
   if (rc) return rc;
@@ -707,6 +747,7 @@ int astr_state_upload(astr_state* st, const double* q, const int64_t shape[3], c
 }
 
 int astr_state_download(astr_state* st, double* q, const int64_t shape[3], const int64_t lbound[3], int where) {
+  const DeviceGuard dg_(st ? st->ctx->device : -1);
   if (!st || !q || !shape || !lbound) return ASTR_ERR_ARG;
   astr_ctx* ctx = st->ctx;
   CK(finalize_filter(st));
@@ -717,6 +758,7 @@ int astr_state_download(astr_state* st, double* q, const int64_t shape[3], const
 }
 
 int astr_cfl_dt(astr_state* st, double cfl, double* dt) {
+  const DeviceGuard dg_(st ? st->ctx->device : -1);
   if (!st || !dt) return ASTR_ERR_ARG;
   astr_ctx* ctx = st->ctx;
   CK(finalize_filter(st));
@@ -736,6 +778,7 @@ int astr_cfl_dt(astr_state* st, double cfl, double* dt) {
 }
 
 int astr_rhs(astr_state* st, double* qrhs, const int64_t shape[3], const int64_t lbound[3], int where) {
+  const DeviceGuard dg_(st ? st->ctx->device : -1);
   if (!st || !qrhs) return ASTR_ERR_ARG;
   astr_ctx* ctx = st->ctx;
   CK(finalize_filter(st));
@@ -766,18 +809,22 @@ int astr_state_launch_shapes(astr_state* st, int shapes[42]) {
 }
 
 int astr_state_set_launch_shape(astr_state* st, int pass, int S, int WPL, int TI, int LPW, int FPS) {
+  const DeviceGuard dg_(st ? st->ctx->device : -1);
   if (!st || pass < 0 || pass >= NCFG) return ASTR_ERR_ARG;
   astr_ctx* ctx = st->ctx;
   bool known = false;
   for (const Layout& L : kLayouts) known |= (L.S == S && L.WPL == WPL);
   const int dir = CFG_DIR[pass];
   if (!known || 32 * WPL * S < st->hf[dir].nsys()) return fail(ctx, ASTR_ERR_ARG, "layout not compiled or too short");
-  if (TI < 1 || (TI & (TI - 1)) || TI * WPL * 32 > 1024 || (WPL > 1 && TI > 15))
-    return fail(ctx, ASTR_ERR_ARG, "TI must be a power of 2 with TI*WPL*32 <= 1024");
+  if (TI < 1 || (TI & (TI - 1))) return fail(ctx, ASTR_ERR_ARG, "TI must be a power of 2");
   const int pk = CFG_PASS[pass];
   const bool loop_ok = dir != 0 && (pk == PASS_VA || pk == PASS_VB || pk == PASS_F);
   if (LPW < 1 || (LPW > 1 && (!loop_ok || TI % LPW != 0)))
     return fail(ctx, ASTR_ERR_ARG, "lines per warp: 1, or a divisor of TI for the y/z passes A', B' and filter-A");
+  // a CTA runs (TI / LPW) line groups of WPL warps: at most 512 threads (the kernels' launch
+  // bound), and with WPL > 1 one named barrier per group (ids 1..15)
+  if ((TI / LPW) * WPL * 32 > 512 || (WPL > 1 && TI / LPW > 15))
+    return fail(ctx, ASTR_ERR_ARG, "(TI / LPW) * WPL * 32 must be <= 512, and TI / LPW <= 15 when WPL > 1");
   const bool streaming = pk == PASS_VA || pk == PASS_VB || pk == PASS_F;
   if (FPS != 5 && !(FPS == 1 && streaming))
     return fail(ctx, ASTR_ERR_ARG, "fields per step: 5, or 1 for the passes A', B' and the filters");
@@ -791,6 +838,7 @@ int astr_state_set_launch_shape(astr_state* st, int pass, int S, int WPL, int TI
 }
 
 int astr_state_split_filter(astr_state* st, int on) {
+  const DeviceGuard dg_(st ? st->ctx->device : -1);
   if (!st) return ASTR_ERR_ARG;
   st->split_fa = on != 0;
   st->autotune = false;
@@ -805,6 +853,7 @@ int astr_state_use_graph(astr_state* st, int on) {
 }
 
 int astr_rk3_step(astr_state* st, double dt, int nsteps) {
+  const DeviceGuard dg_(st ? st->ctx->device : -1);
   if (!st || nsteps < 0 || !(dt > 0.0)) return ASTR_ERR_ARG;
   astr_ctx* ctx = st->ctx;
   if (st->nstep + nsteps > st->hist_cap) return fail(ctx, ASTR_ERR_UNSUPPORTED, "history buffer full (65536 steps)");
@@ -842,6 +891,7 @@ int astr_rk3_step(astr_state* st, double dt, int nsteps) {
 
 int astr_rk3_step_host(astr_state* st, double* q, const int64_t shape[3], const int64_t lbound[3], double dt,
                        int nsteps, double diag_out[3]) {
+  const DeviceGuard dg_(st ? st->ctx->device : -1);
   if (!st || !q) return ASTR_ERR_ARG;
   astr_ctx* ctx = st->ctx;
   int rc = copy_fields(st, st->Q0, q, shape, lbound, 1, ASTR_HOST);
@@ -861,6 +911,7 @@ int astr_rk3_step_host(astr_state* st, double* q, const int64_t shape[3], const 
 }
 
 int astr_pass_timings(astr_state* st, double dt, int nsteps, double ms[8]) {
+  const DeviceGuard dg_(st ? st->ctx->device : -1);
   if (!st || !ms || nsteps < 1) return ASTR_ERR_ARG;
   astr_ctx* ctx = st->ctx;
   if (st->nstep + nsteps > st->hist_cap) return fail(ctx, ASTR_ERR_UNSUPPORTED, "history buffer full");
@@ -891,6 +942,7 @@ int astr_pass_timings(astr_state* st, double dt, int nsteps, double ms[8]) {
 }
 
 int astr_history(astr_state* st, double* rows, int maxrows, int* nrows) {
+  const DeviceGuard dg_(st ? st->ctx->device : -1);
   if (!st || !nrows) return ASTR_ERR_ARG;
   astr_ctx* ctx = st->ctx;
   const int n = st->nstep;
@@ -911,6 +963,7 @@ int astr_history(astr_state* st, double* rows, int maxrows, int* nrows) {
 }
 
 int astr_diagnostics(astr_state* st, double out[3]) {
+  const DeviceGuard dg_(st ? st->ctx->device : -1);
   if (!st || !out) return ASTR_ERR_ARG;
   astr_ctx* ctx = st->ctx;
   CK(finalize_filter(st));
@@ -1146,6 +1199,7 @@ int ens_tune(astr_ensemble* e, bool timed) {
 extern "C" {
 
 int astr_ensemble_create(astr_ctx* ctx, astr_state* const* boxes, int nbox, astr_ensemble** out) {
+  const DeviceGuard dg_(ctx ? ctx->device : -1);
   if (!ctx || !boxes || nbox < 1 || !out) return fail(ctx, ASTR_ERR_ARG, "null argument or empty ensemble");
   astr_ensemble* e = new astr_ensemble();
   e->ctx = ctx;
@@ -1175,6 +1229,7 @@ int astr_ensemble_create(astr_ctx* ctx, astr_state* const* boxes, int nbox, astr
 }
 
 int astr_ensemble_destroy(astr_ensemble* e) {
+  const DeviceGuard dg_(e ? e->ctx->device : -1);
   if (!e) return ASTR_ERR_ARG;
   ens_drop_graphs(e);
   ens_free_plan(e);
@@ -1183,6 +1238,7 @@ int astr_ensemble_destroy(astr_ensemble* e) {
 }
 
 int astr_ensemble_step(astr_ensemble* e, const double* dt, int nsteps) {
+  const DeviceGuard dg_(e ? e->ctx->device : -1);
   if (!e || !dt || nsteps < 0) return ASTR_ERR_ARG;
   astr_ctx* ctx = e->ctx;
   const int nbox = (int)e->boxes.size();
@@ -1460,6 +1516,7 @@ int adj_setup(astr_adjoint* A) {
 extern "C" {
 
 int astr_adjoint_create(astr_state* st, int checkpoint_every, astr_adjoint** out) {
+  const DeviceGuard dg_(st ? st->ctx->device : -1);
   if (!st || !out || checkpoint_every < 1) return ASTR_ERR_ARG;
   astr_adjoint* A = new astr_adjoint();
   A->st = st;
@@ -1471,6 +1528,7 @@ int astr_adjoint_create(astr_state* st, int checkpoint_every, astr_adjoint** out
 }
 
 int astr_adjoint_destroy(astr_adjoint* A) {
+  const DeviceGuard dg_(A ? A->st->ctx->device : -1);
   if (!A) return ASTR_ERR_ARG;
   adj_free(A);
   delete A;
@@ -1478,6 +1536,7 @@ int astr_adjoint_destroy(astr_adjoint* A) {
 }
 
 int astr_adjoint_forward(astr_adjoint* A, double dt, int nsteps, double* J) {
+  const DeviceGuard dg_(A ? A->st->ctx->device : -1);
   if (!A || !(dt > 0.0) || nsteps < 1) return ASTR_ERR_ARG;
   astr_state* st = A->st;
   astr_ctx* ctx = st->ctx;
@@ -1509,6 +1568,7 @@ int astr_adjoint_forward(astr_adjoint* A, double dt, int nsteps, double* J) {
 }
 
 int astr_adjoint_backward(astr_adjoint* A, double* grad, const int64_t shape[3], const int64_t lbound[3], int where) {
+  const DeviceGuard dg_(A ? A->st->ctx->device : -1);
   if (!A || !grad || !shape || !lbound) return ASTR_ERR_ARG;
   astr_state* st = A->st;
   astr_ctx* ctx = st->ctx;
@@ -1552,6 +1612,7 @@ int astr_adjoint_backward(astr_adjoint* A, double* grad, const int64_t shape[3],
 // state is not advanced). Arrays hold 5 fields of nodes 0..N.
 int astr_step_vjp(astr_adjoint* A, double dt, const double* lam_in, double* lam_out, const int64_t shape[3],
                   const int64_t lbound[3], int where) {
+  const DeviceGuard dg_(A ? A->st->ctx->device : -1);
   if (!A || !lam_in || !lam_out || !shape || !lbound || !(dt > 0.0)) return ASTR_ERR_ARG;
   astr_state* st = A->st;
   astr_ctx* ctx = st->ctx;
@@ -1583,6 +1644,7 @@ int astr_step_vjp(astr_adjoint* A, double dt, const double* lam_in, double* lam_
 // operators; device arrays of shape (n0, n1, n2) in Fortran order, fields contiguous).
 int astr_scheme_apply_transpose(astr_ctx* ctx, astr_scheme* s, int dir, const double* g, const int64_t dims[3],
                                 double* out, int nfields, double scale) {
+  const DeviceGuard dg_(ctx ? ctx->device : -1);
   if (!ctx || !s || !g || !out || !dims || dir < 0 || dir > 2 || nfields < 1) return fail(ctx, ASTR_ERR_ARG, "bad argument");
   if (dims[dir] != s->h.dim + 1) return fail(ctx, ASTR_ERR_ARG, "dims[dir] must be dim+1");
   std::string err;

@@ -20,26 +20,36 @@ constexpr int kScratchDoubles = 3 * kMaxCtas + 3;    // + the final triple
 
 static __device__ __align__(256) double g_cfl_scratch[kScratchDoubles];
 
-// Device address of g_cfl_scratch per device, looked up once with that device current.
+// Device address of g_cfl_scratch per device, looked up once per device with that device
+// current (the call's device, made current by the caller of scratch_address).
 constexpr int kMaxDevices = 64;
 double* g_scratch_addr[kMaxDevices] = {nullptr};
 std::mutex g_scratch_mu;
 
-cudaError_t scratch_address(double** out) {
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess) return e;
+cudaError_t scratch_address(int dev, double** out) {
   if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
   std::lock_guard<std::mutex> lock(g_scratch_mu);
   if (!g_scratch_addr[dev]) {
     void* p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_cfl_scratch);
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_cfl_scratch);
     if (e != cudaSuccess) return e;
     g_scratch_addr[dev] = static_cast<double*>(p);
   }
   *out = g_scratch_addr[dev];
   return cudaSuccess;
 }
+
+// The device of the call current for its duration; the caller's device restored afterwards.
+struct OnDevice {
+  int prev = -1;
+  explicit OnDevice(int dev) {
+    int cur = -1;
+    if (dev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != dev && cudaSetDevice(dev) == cudaSuccess) prev = cur;
+  }
+  ~OnDevice() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+};
 
 struct FieldDesc {
   const double* q;
@@ -106,8 +116,9 @@ __global__ void k_cfl_final(const double* partials, int nctas, double* out) {
 
 }  // namespace
 
-// Defined in capi.cu: stream of a context and its error slot.
+// Defined in capi.cu: stream and device of a context, and its error slot.
 cudaStream_t astr_ctx_stream(astr_ctx* ctx);
+int astr_ctx_device(astr_ctx* ctx);
 void astr_ctx_set_error(astr_ctx* ctx, const char* msg);
 
 extern "C" int astr_cfl_dt_noalloc(astr_ctx* ctx, const double* q, const int64_t shape[3], const int64_t lbound[3],
@@ -130,13 +141,25 @@ extern "C" int astr_cfl_dt_noalloc(astr_ctx* ctx, const double* q, const int64_t
       astr_ctx_set_error(ctx, "astr_cfl_dt_noalloc: (jm+1)*(km+1) exceeds the 524288 x lines its static scratch holds");
     return ASTR_ERR_UNSUPPORTED;
   }
+  // the context's device (else the caller's current one) for the whole call
+  int dev = 0;
+  if (ctx) dev = astr_ctx_device(ctx);
+  else if (cudaGetDevice(&dev) != cudaSuccess) return ASTR_ERR_CUDA;
+  const OnDevice on(dev);
+  cudaStream_t st = ctx ? astr_ctx_stream(ctx) : nullptr;
+  // dt comes back to the host, so the call synchronises its stream: not allowed under capture
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  cudaError_t e = cudaStreamIsCapturing(st, &cap);
+  if (e == cudaSuccess && cap != cudaStreamCaptureStatusNone) {
+    if (ctx) astr_ctx_set_error(ctx, "astr_cfl_dt_noalloc: called during stream capture (it returns dt to the host)");
+    return ASTR_ERR_ARG;
+  }
   double* scratch = nullptr;
-  cudaError_t e = scratch_address(&scratch);
+  if (e == cudaSuccess) e = scratch_address(dev, &scratch);
   if (e != cudaSuccess) {
     if (ctx) astr_ctx_set_error(ctx, cudaGetErrorString(e));
     return ASTR_ERR_CUDA;
   }
-  cudaStream_t st = ctx ? astr_ctx_stream(ctx) : nullptr;
   FieldDesc f;
   f.q = q;
   f.s1 = shape[0];
@@ -148,12 +171,18 @@ extern "C" int astr_cfl_dt_noalloc(astr_ctx* ctx, const double* q, const int64_t
   f.n2 = km + 1;
   const double pi = 4.0 * atan(1.0);
   const double const2 = gamma * (mach * mach), const6 = 1.0 / (gamma - 1.0);
-  k_cfl_lines<<<(unsigned)nctas, 256, 0, st>>>(f, 1.0 / (2.0 * pi / im), 1.0 / (2.0 * pi / jm), 1.0 / (2.0 * pi / km),
-                                               const2, const6, mach, scratch);
-  k_cfl_final<<<1, 256, 0, st>>>(scratch, (int)nctas, scratch + 3 * kMaxCtas);
+  double rd0 = 1.0 / (2.0 * pi / im), rd1 = 1.0 / (2.0 * pi / jm), rd2 = 1.0 / (2.0 * pi / km);
+  double* partials = scratch;
+  double* final3 = scratch + 3 * kMaxCtas;
+  int nc = (int)nctas;
+  // launch errors are taken from each launch itself, so an error left by unrelated earlier work
+  // is neither reported as this call's nor cleared
+  void* a1[] = {&f, &rd0, &rd1, &rd2, (void*)&const2, (void*)&const6, &mach, &partials};
+  e = cudaLaunchKernel((const void*)k_cfl_lines, dim3((unsigned)nctas), dim3(256), a1, 0, st);
+  void* a2[] = {&partials, &nc, &final3};
+  if (e == cudaSuccess) e = cudaLaunchKernel((const void*)k_cfl_final, dim3(1), dim3(256), a2, 0, st);
   double m[3] = {0.0, 0.0, 0.0};
-  e = cudaGetLastError();
-  if (e == cudaSuccess) e = cudaMemcpyAsync(m, scratch + 3 * kMaxCtas, sizeof(m), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(m, final3, sizeof(m), cudaMemcpyDeviceToHost, st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) {
     if (ctx) astr_ctx_set_error(ctx, cudaGetErrorString(e));

@@ -9,6 +9,10 @@
   statistics, not its samples.
 * ``ensemble_specs`` -- the seeded set of uneven boxes (sizes, Mach, Reynolds, initial kind) of a
   batched ensemble run.
+* ``spectral_field`` / ``gradient_input`` -- the scalar test field of the gradient-kernel workload
+  (the reference's ``gradtest`` grid, src/test.F90:440-650: x and z periodic on [0, 2 pi), y
+  non-periodic on [0, 2]): a seeded sum of Fourier modes 0 < |k| <= 16 with amplitudes |k|^(-5/3),
+  and the halo-extended array the line operators read.
 
 Arrays are (im+1, jm+1, km+1, 5) Fortran-ordered conserved variables (rho, rho u, rho v, rho w,
 rho E) on nodes 0..N with node N equal to node 0, the layout ``TGVSolver.set_q`` takes.
@@ -19,7 +23,8 @@ from dataclasses import dataclass
 
 import numpy as np
 
-__all__ = ["tgv_q", "solenoidal_velocity", "solenoidal_q", "BoxSpec", "ensemble_specs"]
+__all__ = ["tgv_q", "solenoidal_velocity", "solenoidal_q", "BoxSpec", "ensemble_specs", "spectral_field",
+           "gradient_input", "write_field", "read_field"]
 
 
 def _conserved(rho, u, v, w, p, gamma):
@@ -121,3 +126,66 @@ def ensemble_specs(nbox: int = 48, seed: int = 48, sizes=(32, 48, 64, 96, 128), 
     rs = rng.uniform(reynolds[0], reynolds[1], size=nbox)
     return [BoxSpec(int(ns[b]), float(ms[b]), float(rs[b]), "tgv" if b < nbox // 2 else "solenoidal",
                     int(seed * 1000 + b)) for b in range(nbox)]
+
+
+SPECTRAL_SEED = 20251203
+HM = 5   # halo width of the reference's arrays (commvar.F90:190)
+
+
+def spectral_field(im: int, jm: int | None = None, km: int | None = None, kmax: int = 16,
+                   seed: int = SPECTRAL_SEED) -> np.ndarray:
+    """f(x, y, z) = sum over integer wavevectors 0 < |k| <= kmax of |k|^(-5/3) cos(k_x x + (pi/2) k_y y
+    + k_z z + phi_k) on nodes x_i = 2 pi i/im, y_j = 2 j/jm, z_k = 2 pi k/km (i = 0..im etc.), the
+    phases phi_k uniform on [0, 2 pi) from numpy's PCG64 seeded with `seed`, drawn in lexicographic
+    order of (k_x, k_y, k_z) from -kmax to kmax. Returns an (im+1, jm+1, km+1) Fortran-ordered
+    array. The mode sum is evaluated axis by axis (a separable complex contraction)."""
+    jm = jm or im
+    km = km or im
+    r = np.arange(-kmax, kmax + 1)
+    KX, KY, KZ = np.meshgrid(r, r, r, indexing="ij")
+    k2 = KX * KX + KY * KY + KZ * KZ
+    keep = (k2 > 0) & (k2 <= kmax * kmax)
+    rng = np.random.default_rng(seed)
+    phi = rng.uniform(0.0, 2.0 * np.pi, size=int(keep.sum()))
+    coef = np.zeros(KX.shape, dtype=np.complex128)
+    coef[keep] = np.power(np.sqrt(k2[keep].astype(np.float64)), -5.0 / 3.0) * np.exp(1j * phi)
+    x = 2.0 * np.pi * np.arange(im + 1) / im
+    y = 2.0 * np.arange(jm + 1) / jm
+    z = 2.0 * np.pi * np.arange(km + 1) / km
+    ex = np.exp(1j * np.outer(r, x))                  # (nk, im+1)
+    ey = np.exp(1j * np.outer(r, 0.5 * np.pi * y))    # (nk, jm+1)
+    ez = np.exp(1j * np.outer(r, z))                  # (nk, km+1)
+    a1 = np.tensordot(coef, ez, axes=([2], [0]))      # (kx, ky, z)
+    a2 = np.einsum("abk,bj->ajk", a1, ey)             # (kx, y, z)
+    f = np.tensordot(ex.T, a2, axes=([1], [0]))       # (x, y, z)
+    return np.asfortranarray(f.real)
+
+
+def gradient_input(f: np.ndarray, periodic=(True, False, True)) -> tuple[np.ndarray, tuple]:
+    """The array the line operators read: f on nodes 0..N of each axis, extended by the
+    reference's periodic halo copy f(-k) = f(N-k), f(N+k) = f(k), k = 1..5, along the periodic
+    axes (dataswap of gradtest). Returns the Fortran-ordered array and its lower bounds."""
+    pads = [(HM, HM) if p else (0, 0) for p in periodic]
+    g = f
+    for ax, p in enumerate(periodic):
+        if not p:
+            continue
+        n = f.shape[ax] - 1
+        lo = np.take(g, np.arange(n - HM, n), axis=ax)
+        hi = np.take(g, np.arange(1, HM + 1), axis=ax)
+        g = np.concatenate([lo, g, hi], axis=ax)
+    return np.asfortranarray(g), tuple(-a for a, _ in pads)
+
+
+def write_field(path: str, f: np.ndarray) -> None:
+    """Raw little-endian float64 in Fortran order, preceded by the three extents as int64."""
+    with open(path, "wb") as fh:
+        np.asarray(f.shape[:3], dtype="<i8").tofile(fh)
+        np.asfortranarray(f, dtype="<f8").ravel(order="F").tofile(fh)
+
+
+def read_field(path: str) -> np.ndarray:
+    with open(path, "rb") as fh:
+        shape = tuple(int(v) for v in np.fromfile(fh, dtype="<i8", count=3))
+        data = np.fromfile(fh, dtype="<f8")
+    return data.reshape(shape, order="F")

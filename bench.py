@@ -6,6 +6,7 @@ compact filter alpha_f = 0.49 after every stage, dt fixed from CFL 0.5 at t = 0)
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--size 512]
     python bench.py --workload ensemble [--gpus N] [--steps K]   # 48 uneven boxes, batched
     python bench.py --workload adjoint                          # 128^3 gradient, adjoint:forward
+    python bench.py --workload gradient                         # 256^3 line operators, GB/s
 
 One JSON line on rank 0. `value` = grid-point RK3 updates/s over all ranks (each rank advances
 its own 512^3 box: replicas, weak scaling), device-timed with CUDA events on the library's stream,
@@ -236,6 +237,29 @@ def run_ours(args, ws, rank, local):
                "sample": f"oracle restatement of the reference miniapp, TGV {cn}^3, {args.cpu_steps} RK3 steps, "
                          f"{cores} OpenMP threads, {secs:.1f} s"}
 
+    # the metric's second part (adjoint:forward step time, config 4) and the batched ensemble
+    # against its boxes one at a time (config 3), on one GPU, after the timed region
+    shapes = {k: list(v) for k, v in s.launch_shapes().items()}
+    adjoint = ensemble = None
+    if ws == 1 and not args.no_extras:
+        s.close()
+        tl, acfg = measure_adjoint(ctx, stream, local, args.adj_size, args.adj_steps, 20, 3)
+        adjoint = dict(adjoint_summary(tl, args.adj_steps), config=acfg, metric=ADJ_METRIC,
+                       how="device time, CUDA events on the library stream; reverse = segment recomputation "
+                           "+ adjoint stages")
+        from astr_gpu_b200.fields import ensemble_specs
+        specs = ensemble_specs(48, 48)
+        es = args.ens_steps
+        ms_b, ms_1, boxes, ens, _ = measure_ensemble(ctx, stream, specs, es, 3, True)
+        pts_all = sum(sp.n ** 3 for sp in specs)
+        ensemble = {"metric": ENS_METRIC, "steps": es, "batched": pts_all * es / (ms_b * 1e-3),
+                    "one_at_a_time": pts_all * es / (ms_1 * 1e-3), "ratio": ms_1 / ms_b,
+                    "batched_ms_per_step": ms_b / es, "one_at_a_time_ms_per_step": ms_1 / es, "unit": UNIT,
+                    "boxes": len(specs), "points": pts_all}
+        ens.close()
+        for b in boxes:
+            b.close()
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
@@ -244,9 +268,10 @@ def run_ours(args, ws, rank, local):
             "config": {"workload": f"TGV {n}^3 FP64 SSP-RK3 + compact filter, dt from CFL 0.5",
                        "grid": n, "dt": dt, "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",
                        "l2": "inputs larger than L2 (5 x 1.1 GB state per box)", "graph": "one CUDA graph per step",
-                       "launch_shapes": {k: list(v) for k, v in s.launch_shapes().items()}},
+                       "launch_shapes": shapes},
             "roofline": roof, "step_roofline": step_roof, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": (3 * (7 if split_fa else 6) + 1) * args.steps, "clocks": clk.summary(),
+            "adjoint": adjoint, "ensemble": ensemble,
         }
         print(json.dumps(line), flush=True)
     s.close()
@@ -272,6 +297,44 @@ def ensemble_boxes(ctx, specs):
     return boxes
 
 
+def measure_ensemble(ctx, stream, specs, steps, warmup, single, barrier=None):
+    """Device time (CUDA events on the library's stream) of `steps` batched ensemble steps of the
+    boxes `specs`, and, with `single`, of the same boxes stepped one at a time (each its own
+    autotuned shapes and per-step graph). Returns (ms batched, ms one at a time or None, boxes,
+    ensemble, time steps); the caller closes the boxes and the ensemble."""
+    import torch
+    import astr_gpu_b200 as ag
+    boxes = ensemble_boxes(ctx, specs)
+    dts = [b.cfl_dt(0.5) for b in boxes]
+    ens = ag.Ensemble(ctx, boxes)
+    ens.step(dts, warmup)
+    ctx.synchronize()
+    if barrier:
+        barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    ens.step(dts, steps)
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    ms_solo = None
+    if single:
+        solo = ensemble_boxes(ctx, specs)
+        sdts = [b.cfl_dt(0.5) for b in solo]
+        for b, dt in zip(solo, sdts):
+            b.rk3(dt, warmup)
+        ctx.synchronize()
+        e0.record(stream)
+        for b, dt in zip(solo, sdts):
+            b.rk3(dt, steps)
+        e1.record(stream)
+        e1.synchronize()
+        ms_solo = e0.elapsed_time(e1)
+        for b in solo:
+            b.close()
+    return ms, ms_solo, boxes, ens, dts
+
+
 def run_ensemble(args, ws, rank, local):
     """Batched ensemble: every rank advances its LPT share of the 48 boxes (no collective on the
     data path); value = all boxes' grid points x steps / the slowest rank's device time. On one
@@ -292,11 +355,6 @@ def run_ensemble(args, ws, rank, local):
     mine = lpt_partition([box_cost(sp.n) for sp in specs], ws)[rank]
     stream = torch.cuda.Stream(device=local)
     ctx = ag.Context(local, stream=stream)
-    boxes = ensemble_boxes(ctx, [specs[i] for i in mine])
-    dts = [b.cfl_dt(0.5) for b in boxes]
-    ens = ag.Ensemble(ctx, boxes)
-    ens.step(dts, args.warmup)
-    ctx.synchronize()
 
     def barrier():
         torch.cuda.synchronize(local)
@@ -304,37 +362,20 @@ def run_ensemble(args, ws, rank, local):
             pg.barrier()
         torch.cuda.synchronize(local)
 
-    barrier()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clk:
-        e0.record(stream)
-        ens.step(dts, args.steps)
-        e1.record(stream)
-        e1.synchronize()
+        ms, ms_solo, boxes, ens, dts = measure_ensemble(ctx, stream, [specs[i] for i in mine], args.steps,
+                                                        args.warmup, ws == 1 and not args.no_single, barrier)
     barrier()
-    t = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device=f"cuda:{local}")
+    t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{local}")
     if pg:
         pg.all_reduce(t, op=pg.ReduceOp.MAX)
     ms_max = float(t.item())
     pts_all = sum(sp.n ** 3 for sp in specs)
     value = pts_all * args.steps / (ms_max * 1e-3)
     single = None
-    if ws == 1 and not args.no_single:
-        solo = ensemble_boxes(ctx, specs)
-        sdts = [b.cfl_dt(0.5) for b in solo]
-        for b, dt in zip(solo, sdts):
-            b.rk3(dt, args.warmup)
-        ctx.synchronize()
-        e0.record(stream)
-        for b, dt in zip(solo, sdts):
-            b.rk3(dt, args.steps)
-        e1.record(stream)
-        e1.synchronize()
-        ms_solo = e0.elapsed_time(e1)
+    if ms_solo is not None:
         single = {"value": pts_all * args.steps / (ms_solo * 1e-3), "ms_per_step": ms_solo / args.steps,
                   "how": "each box alone, its own autotuned launch shapes and per-step CUDA graph, boxes in turn"}
-        for b in solo:
-            b.close()
     e2e = None
     if not args.no_e2e:
         # end to end: upload every box's state from pinned host memory, step, download, per step
@@ -387,6 +428,63 @@ def run_ensemble(args, ws, rank, local):
 ADJ_METRIC = "adjoint:forward time ratio, 128^3 decaying turbulence, 200 RK3 steps, checkpoint every 20"
 
 
+def adjoint_setup(n, seed=2024, mach=0.3):
+    """Config-4 initial state: a seeded solenoidal field with E(k) ~ k^4 exp(-2 (k/4)^2) at
+    turbulent Mach `mach`, and the Reynolds number that makes Re_lambda = 50 for its spectrum."""
+    import numpy as np
+    from astr_gpu_b200.fields import solenoidal_q, solenoidal_velocity
+    u = solenoidal_velocity(n, seed)
+    k = np.fft.fftfreq(n, 1.0 / n)
+    d2 = [np.mean(np.fft.ifftn(1j * [k[:, None, None], k[None, :, None], k[None, None, :]][a]
+                                * np.fft.fftn(u[a])).real ** 2) for a in range(3)]
+    up = np.sqrt(np.mean(u[0] ** 2 + u[1] ** 2 + u[2] ** 2) / 3.0)
+    re = 50.0 / (up * up / np.sqrt(np.mean(d2)))
+    return solenoidal_q(n, mach, seed), re
+
+
+def measure_adjoint(ctx, stream, local, n, nsteps, every, warmup, mach=0.3):
+    """Device times (CUDA events on the library's stream) of the plain forward (nsteps
+    graph-captured steps), the checkpointed forward and the reverse sweep (segment recomputation
+    + adjoint stages) of J = final kinetic energy, dJ/dq0 with a checkpoint every `every` steps."""
+    import torch
+    import astr_gpu_b200 as ag
+    from astr_gpu_b200.adjoint import Adjoint, fortran_empty
+    q0, re = adjoint_setup(n, mach=mach)
+    s = ag.TGVSolver(ctx, n, params=ag.FlowParams(mach=mach, reynolds=re))
+    s.set_q(q0)
+    dt = s.cfl_dt(0.5)
+    s.rk3(dt, warmup)
+    ctx.synchronize()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(6)]
+    g = fortran_empty(s.shape + (5,), f"cuda:{local}")
+    s.set_q(q0)
+    ev[0].record(stream)
+    s.rk3(dt, nsteps)
+    ev[1].record(stream)
+    s.set_q(q0)
+    adj = Adjoint(s, every)
+    ev[2].record(stream)
+    J = adj.forward(dt, nsteps)
+    ev[3].record(stream)
+    ev[4].record(stream)
+    adj.backward(g)
+    ev[5].record(stream)
+    ev[5].synchronize()
+    t = [ev[0].elapsed_time(ev[1]), ev[2].elapsed_time(ev[3]), ev[4].elapsed_time(ev[5])]
+    adj.close()
+    s.close()
+    del g
+    return t, {"grid": n, "steps": nsteps, "checkpoint_every": every, "mach_t": mach, "reynolds": re, "dt": dt,
+               "J": J}
+
+
+def adjoint_summary(t, nsteps):
+    t_plain, t_fwd, t_bwd = t
+    return {"forward_ms_per_step": t_plain / nsteps, "checkpointed_forward_ms_per_step": t_fwd / nsteps,
+            "reverse_ms_per_step": t_bwd / nsteps, "ratio": t_bwd / t_plain,
+            "ratio_incl_forward": (t_fwd + t_bwd) / t_plain}
+
+
 def run_adjoint(args, ws, rank, local):
     """Discrete adjoint: 128^3 periodic random solenoidal field (M_t 0.3, Re for Re_lambda = 50),
     200 steps with filter, J = final kinetic energy, dJ/dq0 with a checkpoint every 20 steps.
@@ -395,9 +493,6 @@ def run_adjoint(args, ws, rank, local):
     own replica (no collective on the data path)."""
     import torch
     import astr_gpu_b200 as ag
-    from astr_gpu_b200.adjoint import Adjoint, fortran_empty
-    from astr_gpu_b200.fields import solenoidal_q, solenoidal_velocity
-    import numpy as np
 
     torch.cuda.set_device(local)
     pg = None
@@ -406,57 +501,201 @@ def run_adjoint(args, ws, rank, local):
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=600))
         pg = dist
-    n, nsteps, every, mach, seed = args.adj_size, args.adj_steps, 20, 0.3, 2024
-    u = solenoidal_velocity(n, seed)
-    k = np.fft.fftfreq(n, 1.0 / n)
-    d2 = [np.mean(np.fft.ifftn(1j * [k[:, None, None], k[None, :, None], k[None, None, :]][a]
-                                * np.fft.fftn(u[a])).real ** 2) for a in range(3)]
-    up = np.sqrt(np.mean(u[0] ** 2 + u[1] ** 2 + u[2] ** 2) / 3.0)
-    re = 50.0 / (up * up / np.sqrt(np.mean(d2)))
+    n, nsteps, every = args.adj_size, args.adj_steps, 20
     stream = torch.cuda.Stream(device=local)
     ctx = ag.Context(local, stream=stream)
-    s = ag.TGVSolver(ctx, n, params=ag.FlowParams(mach=mach, reynolds=re))
-    q0 = solenoidal_q(n, mach, seed)
-    s.set_q(q0)
-    dt = s.cfl_dt(0.5)
-    s.rk3(dt, args.warmup)
-    ctx.synchronize()
-    ev = [torch.cuda.Event(enable_timing=True) for _ in range(6)]
-    g = fortran_empty(s.shape + (5,), f"cuda:{local}")
     with ClockSampler(local) as clk:
-        s.set_q(q0)
-        ev[0].record(stream)
-        s.rk3(dt, nsteps)
-        ev[1].record(stream)
-        s.set_q(q0)
-        adj = Adjoint(s, every)
-        ev[2].record(stream)
-        J = adj.forward(dt, nsteps)
-        ev[3].record(stream)
-        ev[4].record(stream)
-        adj.backward(g)
-        ev[5].record(stream)
-        ev[5].synchronize()
-    t_plain, t_fwd, t_bwd = ev[0].elapsed_time(ev[1]), ev[2].elapsed_time(ev[3]), ev[4].elapsed_time(ev[5])
-    t = torch.tensor([t_plain, t_fwd, t_bwd], dtype=torch.float64, device=f"cuda:{local}")
+        tl, cfg = measure_adjoint(ctx, stream, local, n, nsteps, every, args.warmup)
+    t = torch.tensor(tl, dtype=torch.float64, device=f"cuda:{local}")
     if pg:
         pg.all_reduce(t, op=pg.ReduceOp.MAX)
     t_plain, t_fwd, t_bwd = (float(x) for x in t.tolist())
     if rank == 0:
+        summ = adjoint_summary((t_plain, t_fwd, t_bwd), nsteps)
         line = {
             "metric": ADJ_METRIC, "value": t_bwd / t_plain, "unit": "reverse sweep time / plain forward time",
             "n_gpus": ws, "steps": nsteps, "warmup": args.warmup, "ms_per_step": t_bwd / nsteps,
             "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded solenoidal k^4 exp(-2(k/4)^2) field, uniform rho and p)",
-            "config": {"workload": f"adjoint {n}^3, {nsteps} steps, checkpoint every {every}", "grid": n,
-                       "mach_t": mach, "reynolds": re, "dt": dt, "J": J},
-            "forward_ms_per_step": t_plain / nsteps, "checkpointed_forward_ms_per_step": t_fwd / nsteps,
-            "reverse_ms_per_step": t_bwd / nsteps,
-            "gradient_ratio_incl_forward": (t_fwd + t_bwd) / t_plain, "clocks": clk.summary(),
+            "config": dict(cfg, workload=f"adjoint {n}^3, {nsteps} steps, checkpoint every {every}"),
+            "forward_ms_per_step": summ["forward_ms_per_step"],
+            "checkpointed_forward_ms_per_step": summ["checkpointed_forward_ms_per_step"],
+            "reverse_ms_per_step": summ["reverse_ms_per_step"],
+            "gradient_ratio_incl_forward": summ["ratio_incl_forward"], "clocks": clk.summary(),
         }
         print(json.dumps(line), flush=True)
-    adj.close()
-    s.close()
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
+GRAD_METRIC = "gradient kernel GB/s FP64 256^3 (d/dx, d/dy, d/dz + 3-direction compact filter)"
+
+
+def run_gradient(args, ws, rank, local):
+    """The gradient-kernel workload of the reference's gradient_solver_3d / gradtest setting: a
+    256^3 seeded spectral field (x, z periodic, y non-periodic on [0, 2]); one step = the compact
+    first derivatives along x, y and z (scaled by 1/dx) and the compact filter along x, then y,
+    then z, each a call of the line-level C ABI (astr_deriv_lines / astr_filter_lines) on device
+    arrays. Algorithmic bytes: 16 per stored point per call (read f, write the result), 96 per
+    step. Every rank runs its own replica (no collective)."""
+    import ctypes
+    import numpy as np
+    import torch
+    import astr_gpu_b200 as ag
+    from astr_gpu_b200.fields import gradient_input, spectral_field
+
+    torch.cuda.set_device(local)
+    pg = None
+    if ws > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+        pg = dist
+    n = args.grad_size
+    stream = torch.cuda.Stream(device=local)
+    ctx = ag.Context(local, stream=stream)
+    L = ctx.L
+    f = spectral_field(n)
+    g, lb = gradient_input(f, periodic=(True, False, True))
+
+    def dev(a):
+        return torch.from_numpy(np.ascontiguousarray(a.transpose(2, 1, 0))).to(f"cuda:{local}").permute(2, 1, 0)
+
+    G = dev(g)
+    ntypes = (3, 4, 3)
+    spacing = (2 * np.pi / n, 2.0 / n, 2 * np.pi / n)
+    ders = [ag.fd_scheme_initiate(ctx, "643c", ntypes[d], n) for d in range(3)]
+    flts = [ag.compact_filter_initiate(ctx, ntypes[d], n, 0.49, 1.11, 0.98) for d in range(3)]
+    gshape, glb = list(g.shape), list(lb)
+    dshape = [[n + 1 if a == d else gshape[a] for a in range(3)] for d in range(3)]
+    dlb = [[0 if a == d else glb[a] for a in range(3)] for d in range(3)]
+    dout = [torch.empty(tuple(dshape[d][::-1]), dtype=torch.float64, device=f"cuda:{local}").permute(2, 1, 0)
+            for d in range(3)]
+    # filter chain x -> y -> z: the x result keeps the z halo lines (filtered like their images),
+    # so it feeds y and then z directly
+    f1 = torch.empty((gshape[2], n + 1, n + 1), dtype=torch.float64, device=f"cuda:{local}").permute(2, 1, 0)
+    f2 = torch.empty((gshape[2], n + 1, n + 1), dtype=torch.float64, device=f"cuda:{local}").permute(2, 1, 0)
+    f3 = torch.empty((n + 1, n + 1, n + 1), dtype=torch.float64, device=f"cuda:{local}").permute(2, 1, 0)
+    i64 = lambda v: (ctypes.c_int64 * 3)(*[int(x) for x in v])
+    vp = lambda t: ctypes.c_void_p(t.data_ptr())
+    f1s, f1l = [n + 1, n + 1, gshape[2]], [0, 0, glb[2]]
+    f3s, f3l = [n + 1, n + 1, n + 1], [0, 0, 0]
+
+    def step(where=ag._lib.ASTR_DEVICE, bufs=None):
+        src, d_out, o1, o2, o3 = bufs or (G, dout, f1, f2, f3)
+        ptr = (lambda t: ctypes.c_void_p(t.ctypes.data)) if where == ag._lib.ASTR_HOST else vp
+        for d in range(3):
+            ctx.check(L.astr_deriv_lines(ctx._h, ders[d]._h, d, ptr(src), i64(gshape), i64(glb), ptr(d_out[d]),
+                                         i64(dshape[d]), i64(dlb[d]), 1, 1.0 / spacing[d], where))
+        ctx.check(L.astr_filter_lines(ctx._h, flts[0]._h, 0, ptr(src), i64(gshape), i64(glb), ptr(o1), i64(f1s),
+                                      i64(f1l), 1, where))
+        ctx.check(L.astr_filter_lines(ctx._h, flts[1]._h, 1, ptr(o1), i64(f1s), i64(f1l), ptr(o2), i64(f1s),
+                                      i64(f1l), 1, where))
+        ctx.check(L.astr_filter_lines(ctx._h, flts[2]._h, 2, ptr(o2), i64(f1s), i64(f1l), ptr(o3), i64(f3s),
+                                      i64(f3l), 1, where))
+
+    for _ in range(args.warmup):
+        step()
+    ctx.synchronize()
+
+    def barrier():
+        torch.cuda.synchronize(local)
+        if pg:
+            pg.barrier()
+        torch.cuda.synchronize(local)
+
+    # inputs and outputs are 147 MB + 6 x 136-147 MB: larger than L2 between calls
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(7)]
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            step()
+        e1.record(stream)
+        e1.synchronize()
+    # one more step with events between the calls: per-call times on the library's stream
+    ev[0].record(stream)
+    for d in range(3):
+        ctx.check(L.astr_deriv_lines(ctx._h, ders[d]._h, d, vp(G), i64(gshape), i64(glb), vp(dout[d]),
+                                     i64(dshape[d]), i64(dlb[d]), 1, 1.0 / spacing[d], ag._lib.ASTR_DEVICE))
+        ev[d + 1].record(stream)
+    step_f = [(flts[0], 0, G, gshape, glb, f1, f1s, f1l), (flts[1], 1, f1, f1s, f1l, f2, f1s, f1l),
+              (flts[2], 2, f2, f1s, f1l, f3, f3s, f3l)]
+    for k, (sch, d, a, ash, alb, o, osh, olb) in enumerate(step_f):
+        ctx.check(L.astr_filter_lines(ctx._h, sch._h, d, vp(a), i64(ash), i64(alb), vp(o), i64(osh), i64(olb), 1,
+                                      ag._lib.ASTR_DEVICE))
+        ev[k + 4].record(stream)
+    ev[6].synchronize()
+    per_call = [ev[i].elapsed_time(ev[i + 1]) for i in range(6)]
+    barrier()
+    ms = e0.elapsed_time(e1)
+    t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{local}")
+    if pg:
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    ms_max = float(t.item())
+    pts = (n + 1) ** 3
+    step_bytes = 6 * 16.0 * pts
+    value = ws * step_bytes * args.steps / (ms_max * 1e-3) / 1e9
+    pk, pk_kind = peaks()
+    names = ["d/dx", "d/dy", "d/dz", "filter x", "filter y", "filter z"]
+    dom = int(np.argmax(per_call))
+    achieved = 16.0 * pts / (per_call[dom] * 1e-3) / 1e9
+    roof = {"kernel": f"k_line_api ({names[dom]})", "bound": "hbm", "achieved": achieved, "peak": pk,
+            "unit": "GB/s", "frac": achieved / pk, "traffic": None, "peak_kind": pk_kind,
+            "alg_bytes_per_launch": 16.0 * pts, "ms_per_launch": per_call[dom],
+            "per_call_ms": dict(zip(names, per_call))}
+    e2e = None
+    if not args.no_e2e:
+        # the same calls with host arrays: every call copies its input in and its output back
+        hbufs = (g, [np.zeros(dshape[d], order="F") for d in range(3)], np.zeros(f1s, order="F"),
+                 np.zeros(f1s, order="F"), np.zeros(f3s, order="F"))
+        step(ag._lib.ASTR_HOST, hbufs)
+        barrier()
+        ne = args.e2e_steps
+        t0 = time.perf_counter()
+        for _ in range(ne):
+            step(ag._lib.ASTR_HOST, hbufs)
+        te = time.perf_counter() - t0
+        tt = torch.tensor([te], dtype=torch.float64, device=f"cuda:{local}")
+        if pg:
+            pg.all_reduce(tt, op=pg.ReduceOp.MAX)
+        te = float(tt.item())
+        h2d = 8 * (3 * g.size + g.size + 2 * int(np.prod(f1s)))
+        d2h = 8 * (sum(int(np.prod(s_)) for s_ in dshape) + 2 * int(np.prod(f1s)) + int(np.prod(f3s)))
+        e2e = {"value": ws * step_bytes * ne / te / 1e9, "unit": "GB/s", "h2d_bytes_per_step": h2d,
+               "d2h_bytes_per_step": d2h, "steps": ne, "call": "astr_deriv_lines / astr_filter_lines, host arrays"}
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        import oracle
+        oracle.set_num_threads(os.cpu_count() or 1)
+        ops = [oracle.fd_scheme_initiate("643c", ntypes[d], n) for d in range(3)]
+        t0 = time.perf_counter()
+        for d in range(3):
+            ops[d].apply3d(g, d, lbound=lb)
+        cur = g
+        for d in range(3):
+            cur = oracle.compact_filter_initiate(ntypes[d], n, 0.49, 1.11, 0.98).apply3d(
+                cur, d, lbound=lb if d == 0 else (0, 0, lb[2]))
+        secs = time.perf_counter() - t0
+        cpu = {"value": step_bytes / secs / 1e9, "unit": "GB/s", "cores": oracle.num_threads(), "kind": "port",
+               "sample": f"oracle restatement, the same six calls at {n}^3 once, {oracle.num_threads()} OpenMP threads, "
+                         f"{secs:.1f} s"}
+    if rank == 0:
+        line = {
+            "metric": GRAD_METRIC, "value": value, "unit": "GB/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded spectral field, |k| <= 16, |k|^(-5/3), seed 20251203)",
+            "config": {"workload": f"gradient kernel {n}^3: x, z periodic (ntype 3), y non-periodic (ntype 4) on "
+                                   f"[0, 2]; d/dx, d/dy, d/dz and the filter along x, y, z",
+                       "grid": n, "bytes_per_point_per_step": 96, "points": pts,
+                       "l2": "input and outputs 136-147 MB each, larger than L2"},
+            "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": 6 * args.steps,
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
     if pg:
         pg.barrier()
         pg.destroy_process_group()
@@ -491,10 +730,13 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", default="tgv", choices=["tgv", "ensemble", "adjoint"])
+    ap.add_argument("--workload", default="tgv", choices=["tgv", "ensemble", "adjoint", "gradient"])
+    ap.add_argument("--grad-size", type=int, default=256)
     ap.add_argument("--adj-size", type=int, default=128)
     ap.add_argument("--adj-steps", type=int, default=200)
     ap.add_argument("--no-single", action="store_true")
+    ap.add_argument("--no-extras", action="store_true", help="skip the adjoint and ensemble keys of the default line")
+    ap.add_argument("--ens-steps", type=int, default=10)
     ap.add_argument("--profile", action="store_true", help="eager steps only, for ncu captures")
     ap.add_argument("--shapes", default="", help='pinned launch shapes, e.g. {"A": [9, 2, 8], ...}')
     args = ap.parse_args()
@@ -509,6 +751,8 @@ def main():
         run_ensemble(args, ws, rank, local)
     elif args.workload == "adjoint":
         run_adjoint(args, ws, rank, local)
+    elif args.workload == "gradient":
+        run_gradient(args, ws, rank, local)
     else:
         run_ours(args, ws, rank, local)
 

@@ -97,6 +97,147 @@ module astr_b200
       integer(c_int), value :: maxrows
       integer(c_int) :: nrows
     end function
+    integer(c_int) function astr_set_stream(ctx, stream) bind(C, name="astr_set_stream")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: ctx, stream
+    end function
+    integer(c_int) function astr_synchronize(ctx) bind(C, name="astr_synchronize")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: ctx
+    end function
+    integer(c_int) function astr_scheme_destroy(s) bind(C, name="astr_scheme_destroy")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: s
+    end function
+    integer(c_int) function astr_scheme_ac(s, ac, first_node, last_node) bind(C, name="astr_scheme_ac")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: s, ac
+      integer(c_int) :: first_node, last_node
+    end function
+    integer(c_int) function astr_state_destroy(st) bind(C, name="astr_state_destroy")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: st
+    end function
+    integer(c_int) function astr_state_init_tgv(st) bind(C, name="astr_state_init_tgv")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: st
+    end function
+    integer(c_int) function astr_cfl_dt(st, cfl, dt) bind(C, name="astr_cfl_dt")
+      import :: c_int, c_ptr, c_double
+      type(c_ptr), value :: st
+      real(c_double), value :: cfl
+      real(c_double) :: dt
+    end function
+    integer(c_int) function astr_rk3_step_host(st, q, shape, lb, dt, nsteps, diag_out) bind(C, name="astr_rk3_step_host")
+      import :: c_int, c_ptr, c_double, c_int64_t
+      type(c_ptr), value :: st, q
+      integer(c_int64_t) :: shape(3), lb(3)
+      real(c_double), value :: dt
+      integer(c_int), value :: nsteps
+      real(c_double) :: diag_out(3)
+    end function
+    integer(c_int) function astr_diagnostics(st, out) bind(C, name="astr_diagnostics")
+      import :: c_int, c_ptr, c_double
+      type(c_ptr), value :: st
+      real(c_double) :: out(3)
+    end function
+    integer(c_int) function astr_state_use_graph(st, on) bind(C, name="astr_state_use_graph")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: st
+      integer(c_int), value :: on
+    end function
+    integer(c_int) function astr_state_split_filter(st, on) bind(C, name="astr_state_split_filter")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: st
+      integer(c_int), value :: on
+    end function
+    integer(c_int) function astr_state_autotune(st, on) bind(C, name="astr_state_autotune")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: st
+      integer(c_int), value :: on
+    end function
+    integer(c_int) function astr_state_launch_shapes(st, shapes) bind(C, name="astr_state_launch_shapes")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: st
+      integer(c_int) :: shapes(42)
+    end function
+    integer(c_int) function astr_state_set_launch_shape(st, pass, s, wpl, ti, lpw, fps) &
+        bind(C, name="astr_state_set_launch_shape")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: st
+      integer(c_int), value :: pass, s, wpl, ti, lpw, fps
+    end function
+    integer(c_int) function astr_pass_timings(st, dt, nsteps, ms) bind(C, name="astr_pass_timings")
+      import :: c_int, c_ptr, c_double
+      type(c_ptr), value :: st
+      real(c_double), value :: dt
+      integer(c_int), value :: nsteps
+      real(c_double) :: ms(8)
+    end function
+    integer(c_int) function astr_ensemble_create(ctx, boxes, nbox, e) bind(C, name="astr_ensemble_create")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: ctx
+      type(c_ptr) :: boxes(*)
+      integer(c_int), value :: nbox
+      type(c_ptr) :: e
+    end function
+    integer(c_int) function astr_ensemble_destroy(e) bind(C, name="astr_ensemble_destroy")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: e
+    end function
+    integer(c_int) function astr_ensemble_step(e, dt, nsteps) bind(C, name="astr_ensemble_step")
+      import :: c_int, c_ptr, c_double
+      type(c_ptr), value :: e
+      real(c_double) :: dt(*)
+      integer(c_int), value :: nsteps
+    end function
+    integer(c_int) function astr_adjoint_create(st, checkpoint_every, adj) bind(C, name="astr_adjoint_create")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: st
+      integer(c_int), value :: checkpoint_every
+      type(c_ptr) :: adj
+    end function
+    integer(c_int) function astr_adjoint_destroy(adj) bind(C, name="astr_adjoint_destroy")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: adj
+    end function
+    integer(c_int) function astr_adjoint_forward(adj, dt, nsteps, j) bind(C, name="astr_adjoint_forward")
+      import :: c_int, c_ptr, c_double
+      type(c_ptr), value :: adj
+      real(c_double), value :: dt
+      integer(c_int), value :: nsteps
+      real(c_double) :: j
+    end function
+    integer(c_int) function astr_adjoint_backward(adj, grad, shape, lb, where) bind(C, name="astr_adjoint_backward")
+      import :: c_int, c_ptr, c_int64_t
+      type(c_ptr), value :: adj, grad
+      integer(c_int64_t) :: shape(3), lb(3)
+      integer(c_int), value :: where
+    end function
+    integer(c_int) function astr_step_vjp(adj, dt, lam_in, lam_out, shape, lb, where) bind(C, name="astr_step_vjp")
+      import :: c_int, c_ptr, c_double, c_int64_t
+      type(c_ptr), value :: adj, lam_in, lam_out
+      real(c_double), value :: dt
+      integer(c_int64_t) :: shape(3), lb(3)
+      integer(c_int), value :: where
+    end function
+    integer(c_int) function astr_scheme_apply_transpose(ctx, s, dir, g, dims, out, nfields, scale) &
+        bind(C, name="astr_scheme_apply_transpose")
+      import :: c_int, c_ptr, c_double, c_int64_t
+      type(c_ptr), value :: ctx, s, g, out
+      integer(c_int), value :: dir, nfields
+      integer(c_int64_t) :: dims(3)
+      real(c_double), value :: scale
+    end function
+    integer(c_int) function astr_cfl_dt_noalloc(ctx, q, shape, lb, im, jm, km, mach, gamma, cfl, dt) &
+        bind(C, name="astr_cfl_dt_noalloc")
+      import :: c_int, c_ptr, c_double, c_int64_t
+      type(c_ptr), value :: ctx, q
+      integer(c_int64_t) :: shape(3), lb(3)
+      integer(c_int), value :: im, jm, km
+      real(c_double), value :: mach, gamma, cfl
+      real(c_double) :: dt
+    end function
   end interface
 
 contains

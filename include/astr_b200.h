@@ -3,9 +3,10 @@
  *
  * Every entry point is extern "C", takes plain pointers and sizes, returns an int status
  * (ASTR_OK = 0, negative on error, never aborts) and records a message readable through
- * astr_last_error(). Arrays crossing the boundary are Fortran-ordered (first index fastest)
- * with explicit lower bounds, so a Fortran caller passes c_loc(f(lb0,lb1,lb2)) together with
- * shape(f) and lbound(f). `where` says whether a pointer is host (ASTR_HOST) or device
+ * astr_last_error(). A call on a context (or on a scheme, state, ensemble or adjoint made from
+ * one) runs on the context's device and restores the caller's current device before returning.
+ * Arrays crossing the boundary are Fortran-ordered (first index fastest) with explicit lower
+ * bounds, so a Fortran caller passes c_loc(f(lb0,lb1,lb2)) together with shape(f) and lbound(f). `where` says whether a pointer is host (ASTR_HOST) or device
  * (ASTR_DEVICE) memory; host pointers are only borrowed for the duration of the call.
  *
  * Reference interfaces replaced (paths inside Perrbit/astr_gpu):
@@ -132,7 +133,8 @@ int astr_state_autotune(astr_state* st, int on);
  * 42 ints. */
 int astr_state_launch_shapes(astr_state* st, int shapes[42]);
 /* Pin pass `pass` (0..6 in the order above) to S rows per lane, WPL warps per line, TI lines per
- * CTA (a compiled layout whose 32*WPL*S rows cover the pass's line systems; TI a power of 2) and
+ * CTA (a compiled layout whose 32*WPL*S rows cover the pass's line systems; TI a power of 2 with
+ * (TI/LPW)*WPL*32 <= 512 threads, and TI/LPW <= 15 when WPL > 1) and
  * LPW lines per warp group (1; or a divisor of TI for the y/z passes A', B' and filter-A, whose
  * warps then loop over LPW lines of the tile) and FPS fields per step (5: all fields of the pass
  * at once; or 1 for A', B' and the filter passes, which then stream their independent fields one
@@ -183,9 +185,12 @@ int astr_scheme_apply_transpose(astr_ctx* ctx, astr_scheme* s, int dir, const do
  * synchronises the device mid-step). It has no counterpart in the reference.
  * It allocates nothing: its scratch is a 1.5 MB static device array that every GPU loading the
  * library holds until exit, which caps (jm+1)*(km+1) at 524288 (ASTR_ERR_UNSUPPORTED beyond).
- * The first call on a device looks the array up on that device (make it before any stream
- * capture). All calls share the array: calls that overlap on the GPU race. ctx may be NULL
- * (default stream, no message); otherwise its stream is used and errors set its message. */
+ * The first call on a device looks the array's address up on that device. The call returns dt
+ * to the host and so synchronises its stream: it cannot be made during stream capture (it
+ * returns ASTR_ERR_ARG then). All calls share the array: calls that overlap on the GPU race.
+ * ctx may be NULL (the caller's current device and its default stream, no message); otherwise
+ * the call runs on ctx's device and stream, restores the caller's current device, and errors
+ * set ctx's message. */
 int astr_cfl_dt_noalloc(astr_ctx* ctx, const double* q, const int64_t shape[3], const int64_t lbound[3],
                         int im, int jm, int km, double mach, double gamma, double cfl, double* dt);
 

@@ -60,6 +60,7 @@ def lib():
             "orc_tgv_cfl_dt": (d, [vp, d]),
             "orc_tgv_steps": (None, [vp, i]),
             "orc_tgv_history": (i, [vp, dp, i]),
+            "orc_tgv_history_compensated": (i, [vp, dp, i]),
             "orc_tgv_rhs": (None, [vp, dp]),
             "orc_tgv_diagnostics": (None, [vp, dp]),
             "orc_num_threads": (i, []),
@@ -196,12 +197,16 @@ class TGVOracle:
     def steps(self, n: int):
         lib().orc_tgv_steps(self._h, n)
 
-    def history(self) -> np.ndarray:
-        """Rows of (nstep, time, tke, enstrophy, dissipation), one per step (stacal)."""
+    def history(self, compensated: bool = False) -> np.ndarray:
+        """Rows of (nstep, time, tke, enstrophy, dissipation), one per step (stacal). The sums run
+        over the nodes in the reference's sequential order; with ``compensated`` the same per-node
+        terms are summed with Neumaier's compensation instead (rounding independent of the node
+        count, the reference value for sums taken in another order)."""
         L = lib()
-        n = L.orc_tgv_history(self._h, _dp(np.zeros(5)), 0)
+        fn = L.orc_tgv_history_compensated if compensated else L.orc_tgv_history
+        n = fn(self._h, _dp(np.zeros(5)), 0)
         out = np.zeros(5 * max(n, 1))
-        L.orc_tgv_history(self._h, _dp(out), n)
+        fn(self._h, _dp(out), n)
         return out[: 5 * n].reshape(n, 5)
 
     def rhs(self) -> np.ndarray:

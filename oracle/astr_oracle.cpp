@@ -455,6 +455,7 @@ struct TGV {
   Scheme fds[3], flt[3];
   Field3 q, rho, prs, tmp, vel, qrhs, dvel, dtmp, sigma, qflux, qsave;
   std::vector<double> hist;   // rows of (nstep, time, tke, enst, diss)
+  std::vector<double> hist_c; // the same rows with compensated sums
 
   void setup(int im_, int jm_, int km_, double mach_, double re_, double pr_, double gam_,
              double ref_tem_, double suth_, double alfa_filter, double beta_halo, double beta_bound,
@@ -484,6 +485,7 @@ struct TGV {
     dx = 2.0 * pi / double(im); dy = 2.0 * pi / double(jm); dz = 2.0 * pi / double(km);
     nstep = 0; time = 0.0; deltat = 1e-3;
     hist.clear();
+    hist_c.clear();
   }
 
   // fvar2q with pressure, tgvsolver.F90:48-71
@@ -759,19 +761,38 @@ struct TGV {
     }
   }
 
+  // Neumaier's compensated summation: s + c carries the sum of the added terms to about one
+  // rounding of the final value, independent of their number and order.
+  struct CSum {
+    double s = 0.0, c = 0.0;
+    void add(double x) {
+      const double t = s + x;
+      c += (std::fabs(s) >= std::fabs(x)) ? (s - t) + x : (x - t) + s;
+      s = t;
+    }
+    double value() const { return s + c; }
+  };
+
   // stacal, tgvsolver.F90:893-942, plus diss_rate_cal (statistic.F90:993-1040); sequential sums
+  // in the reference's order. The same per-node terms are also summed with compensation (hist_c),
+  // a reference value for the sums whose rounding does not grow with the number of nodes: a
+  // sequential sum of N terms carries an error of order sqrt(N) ulps (about 1e-12 relative at
+  // 512^3), which an implementation that sums in another order cannot reproduce.
   void stacal() {
     double tke = 0.0, enst = 0.0, diss = 0.0;
+    CSum ctke, censt, cdiss;
     for (int k = 1; k <= km; ++k)
       for (int j = 1; j <= jm; ++j)
         for (int i = 1; i <= im; ++i) {
           double var1 = vel(i, j, k, 0) * vel(i, j, k, 0) + vel(i, j, k, 1) * vel(i, j, k, 1) +
                         vel(i, j, k, 2) * vel(i, j, k, 2);
           tke = tke + rho(i, j, k) * var1;
+          ctke.add(rho(i, j, k) * var1);
           double om1 = dvel(i, j, k, 2 + 3) - dvel(i, j, k, 1 + 6);
           double om2 = dvel(i, j, k, 0 + 6) - dvel(i, j, k, 2 + 0);
           double om3 = dvel(i, j, k, 1 + 0) - dvel(i, j, k, 0 + 3);
           enst = enst + rho(i, j, k) * (om1 * om1 + om2 * om2 + om3 * om3);
+          censt.add(rho(i, j, k) * (om1 * om1 + om2 * om2 + om3 * om3));
           double miu = miucal(tmp(i, j, k)) / reynolds;
           double du11 = dvel(i, j, k, 0), du12 = dvel(i, j, k, 3), du13 = dvel(i, j, k, 6);
           double du21 = dvel(i, j, k, 1), du22 = dvel(i, j, k, 4), du23 = dvel(i, j, k, 7);
@@ -782,12 +803,15 @@ struct TGV {
           double v = 2.0 * miu * (s11 * s11 + s22 * s22 + s33 * s33 + 2.0 * (s12 * s12 + s13 * s13 + s23 * s23) -
                                   num1d3 * (div * div));
           diss = diss + v;
+          cdiss.add(v);
         }
     const double nn = double((int64_t)im * jm * km);
     tke = 0.5 * tke / nn;
     enst = 0.5 * enst / nn;
     diss = diss / nn;
     hist.push_back(nstep); hist.push_back(time); hist.push_back(tke); hist.push_back(enst); hist.push_back(diss);
+    hist_c.push_back(nstep); hist_c.push_back(time); hist_c.push_back(0.5 * ctke.value() / nn);
+    hist_c.push_back(0.5 * censt.value() / nn); hist_c.push_back(cdiss.value() / nn);
   }
 
   // rhscal, tgvsolver.F90:962-992
@@ -930,6 +954,13 @@ int orc_tgv_history(void* h, double* out, int maxrows) {
   std::memcpy(out, t->hist.data(), sizeof(double) * 5 * nr);
   return rows;
 }
+int orc_tgv_history_compensated(void* h, double* out, int maxrows) {
+  TGV* t = static_cast<TGV*>(h);
+  int rows = (int)(t->hist_c.size() / 5);
+  int nr = std::min(rows, maxrows);
+  std::memcpy(out, t->hist_c.data(), sizeof(double) * 5 * nr);
+  return rows;
+}
 // One rhscal on the current state (after the halo fill): qrhs on nodes 0..N, Fortran order.
 void orc_tgv_rhs(void* h, double* out) {
   TGV* t = static_cast<TGV*>(h);
@@ -950,6 +981,7 @@ void orc_tgv_diagnostics(void* h, double* out3) {
   size_t n = t->hist.size();
   out3[0] = t->hist[n - 3]; out3[1] = t->hist[n - 2]; out3[2] = t->hist[n - 1];
   t->hist.resize(n - 5);
+  t->hist_c.resize(t->hist_c.size() - 5);
 }
 int orc_num_threads() {
 #ifdef _OPENMP

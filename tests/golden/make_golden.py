@@ -1,4 +1,6 @@
-"""Regenerate the golden fixtures from the reference tree (run in a container that has it).
+"""Regenerate the golden fixtures from a checkout of the reference tree.
+
+    python tests/golden/make_golden.py <path to the Perrbit/astr_gpu checkout>
 
 state_ref_128.txt: the reference's own committed Taylor-Green history
 miniapps/tgv_solver_3d/state.ref_128 (written by tgvsolver.F90:938: nstep, time, tke,
@@ -8,12 +10,13 @@ import os
 import shutil
 import sys
 
-REF = os.environ.get("ASTR_REFERENCE", "/root/reference")
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 
 def main():
-    src = os.path.join(REF, "miniapps", "tgv_solver_3d", "state.ref_128")
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_golden.py <reference checkout>")
+    src = os.path.join(sys.argv[1], "miniapps", "tgv_solver_3d", "state.ref_128")
     if not os.path.exists(src):
         sys.exit(f"reference tree not found at {src}")
     shutil.copyfile(src, os.path.join(HERE, "state_ref_128.txt"))

@@ -1,0 +1,59 @@
+"""The strict-parity build (-fmad=false: no multiply-add contraction, like the reference's
+gfortran build without -march) against the oracle (itself built with -ffp-contract=off).
+
+What remains between them is the solve algorithm: a segmented affine scan of the Thomas
+recurrences instead of the sequential sweep (commfunc.F90:790-813), whose rounding differs at
+the level of a few ulps per solve. One rhscal (tgvsolver.F90:962-992) of a 64^3 perturbed
+state is compared field by field; each field's error is scaled by max(|R_m|_inf, p0/dx), the
+rounding floor of differentiating the O(p0) pressure (p0 = 1/(gamma M^2) = 71.4) at spacing
+dx. The same comparison of the default (contracting) build is printed beside it."""
+import numpy as np
+import pytest
+
+import oracle
+
+pytestmark = pytest.mark.gpu
+STRICT_TOL = 1e-14
+
+
+def _state(n, seed):
+    rng = np.random.default_rng(seed)
+    k = np.arange(n + 1) * 2 * np.pi / n
+    x, y, z = np.meshgrid(k, k, k, indexing="ij")
+    q = np.zeros((n + 1, n + 1, n + 1, 5), order="F")
+    rho = 1.0 + 0.1 * np.sin(x + 2 * y) * np.cos(z)
+    u = 0.3 * np.sin(x) * np.cos(y) * np.cos(z) + 0.05 * rng.standard_normal() * np.cos(2 * z)
+    v = -0.3 * np.cos(x) * np.sin(y) * np.cos(z) + 0.05 * np.sin(3 * x)
+    w = 0.1 * np.sin(y + z)
+    p = 1.0 / (1.4 * 0.1 ** 2) + 0.2 * np.cos(2 * x)
+    q[..., 0] = rho
+    q[..., 1] = rho * u
+    q[..., 2] = rho * v
+    q[..., 3] = rho * w
+    q[..., 4] = p / 0.4 + 0.5 * rho * (u * u + v * v + w * w)
+    return q
+
+
+def _scaled_err(got, ref, n):
+    p0, dx = 1.0 / (1.4 * 0.1 ** 2), 2 * np.pi / n
+    return max(float(np.abs(got[..., m] - ref[..., m]).max()) / max(np.abs(ref[..., m]).max(), p0 / dx)
+               for m in range(5))
+
+
+def test_strict_build_rhs_matches_oracle():
+    import astr_gpu_b200 as ag
+    n = 64
+    q = _state(n, 3)
+    o = oracle.TGVOracle(n)
+    o.set_q(q)
+    ref = o.rhs()
+    errs = {}
+    for strict in (True, False):
+        ctx = ag.Context(0, strict=strict)
+        s = ag.TGVSolver(ctx, n)
+        s.set_q(q)
+        errs[strict] = _scaled_err(s.rhs(), ref, n)
+        s.close()
+        ctx.close()
+    print(f"rhs vs oracle, scaled: strict {errs[True]:.3e}, default {errs[False]:.3e}")
+    assert errs[True] <= STRICT_TOL, errs

@@ -208,49 +208,6 @@ def test_noncubic_box_steps_match_oracle(ctx, dims):
         assert np.abs(h[:, c] - ho[:, c]).max() / np.abs(ho[:, c]).max() <= 1e-12
 
 
-def test_every_layout_agrees_at_256(ctx):
-    """Every compiled solve layout that covers the 257-node lines, pinned on each pass in turn
-    (streamed fields and lines per warp group 2 as well where a pass allows them), gives the
-    state of the default
-    shapes after 2 RK3 steps to rounding. At this size the lane holding the last real rows of a
-    filter system with 17 rows per lane reaches past the staged halo with its padding rows.
-    Layouts with other rows per lane segment the solves differently, so the states agree to
-    rounding: 1e-12 of each field's largest value, the three momenta sharing their largest (the
-    Taylor-Green w momentum starts at zero and stays small)."""
-    import astr_gpu_b200 as ag
-    n = 256
-
-    def run(pin):
-        s = ag.TGVSolver(ctx, n)
-        s.autotune(False)
-        if pin:
-            s.set_launch_shape(*pin)
-        s.init_tgv()
-        dt = s.cfl_dt(0.5)
-        s.rk3(dt, 2)
-        q = s.get_q()
-        s.close()
-        return q
-
-    ref = run(None)
-    layouts = [(9, 1), (5, 2), (9, 2), (5, 4), (9, 4), (17, 1)]
-    passes = ["A", "B", "C", "A'", "B'", "F_C", "F_A"]
-    bad = []
-    for nm in passes:
-        for S, W in layouts:
-            ti = 2 if W == 4 else 4
-            pins = [(nm, S, W, ti)]
-            if nm in ("A'", "B'", "F_C", "F_A"):   # fields streamed one at a time
-                pins.append((nm, S, W, ti, 1, 1))
-                if nm != "F_C" and W <= 2:      # warps looping over 2 lines of 8
-                    pins.append((nm, S, W, 8, 2, 1))
-            for pin in pins:
-                d = _rel_scaled(run(pin), ref)
-                if not d <= 1e-12:
-                    bad.append((pin, d))
-    assert not bad, bad
-
-
 @pytest.mark.parametrize("n", [96, 130])
 def test_split_and_fused_filter_agree(ctx, n):
     """The filter along y owed by each stage, fused into the first gradient pass or run as its
