@@ -3,116 +3,183 @@
 //   ff = compact_filter(afilter, f, dim)   src/filter.F90:112-144
 // applied to every line of a 3-D array along one direction.
 //
-// One CTA takes TI lines. The lines (nodes -HT..dim+HT, halos read from the caller's array) are
-// staged in shared memory with coalesced loads: node-fastest for x lines, line-fastest for
-// y/z lines (TI adjacent lines are contiguous in x). WPL warps solve each line with the
-// segmented Thomas of ops.cuh; results go back through the tile for coalesced stores.
+// One CTA takes TI lines of one field. The lines (nodes -HT..dim+HT, the halos read from the
+// caller's array, zeros outside it) are staged in shared memory with asynchronous copies, all in
+// flight at once: node-fastest for x lines (16-byte copies of node pairs where aligned),
+// line-fastest for y/z lines (TI adjacent lines are contiguous in x, so each node of the tile is
+// one 8*TI-byte row). Each group of WPL warps solves two lines together with the segmented Thomas
+// of ops.cuh (their recurrences and scans interleave); results go back through the tile for
+// coalesced stores.
 #include "internal.h"
 
 namespace astr {
 
+namespace {
+
+__device__ __forceinline__ void cp8(double* sdst, const double* gsrc) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp16(double* sdst, const double* gsrc) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_wait_all() {
+  asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+}
+
+// The thread's staging line and its walk over the nodes of that line: x lines give each line
+// blockDim/TI consecutive threads; y/z lines give consecutive threads consecutive lines.
+struct Slot {
+  int l, n0, nst;
+};
+__device__ __forceinline__ Slot slot_of(int dir, int TI) {
+  Slot s;
+  if (dir == 0) {
+    const int per = blockDim.x / TI;
+    s.l = threadIdx.x / per;
+    s.n0 = threadIdx.x - s.l * per;
+    s.nst = per;
+  } else {
+    s.l = threadIdx.x % TI;
+    s.n0 = threadIdx.x / TI;
+    s.nst = blockDim.x / TI;
+  }
+  return s;
+}
+
+}  // namespace
+
 template <int S, int WPL>
-__global__ void __launch_bounds__(1024) k_line_api(LineOp op, int dir, const double* __restrict__ f, ArrDesc fa,
-                                                   double* __restrict__ out, ArrDesc oa, int TI, int LP,
-                                                   double scale) {
+__global__ void __launch_bounds__(512) k_line_api(LineOp op, int dir, const double* __restrict__ f, ArrDesc fa,
+                                                  double* __restrict__ out, ArrDesc oa, int TI, int LP, double scale) {
   extern __shared__ double sm[];
   double* tile = sm;
-  double* scan = sm + (size_t)TI * LP;   // 2*WPL per line
-  double* sp = scan + (size_t)TI * 2 * WPL;   // closure rows, 2*NSP per line
+  double* scan = sm + (size_t)TI * LP;                 // SCAN_LINE doubles per line group
+  constexpr int SCAN_LINE = 4 * WPL;                   // two solves at once
+  const int ngroups = blockDim.x / (32 * WPL);
+  double* sp = scan + (size_t)ngroups * SCAN_LINE;     // closure rows, 2*NSP per line
   const int o1 = (dir == 0) ? 1 : 0;
   const int o2 = (dir == 2) ? 1 : 2;
-  const int64_t l1_0 = oa.lb[o1] + (int64_t)blockIdx.x * TI;
-  const int64_t l1_end = oa.lb[o1] + oa.n[o1];
+  const int64_t i1_0 = oa.lb[o1] + (int64_t)blockIdx.x * TI;
+  const int64_t i1_end = oa.lb[o1] + oa.n[o1];
   const int64_t i2 = oa.lb[o2] + blockIdx.y;
-  const double* fb = f + (int64_t)blockIdx.z * fa.fs;
-  double* ob = out + (int64_t)blockIdx.z * oa.fs;
-  const int tid = threadIdx.x, nthr = blockDim.x;
   const int dim = op.dim;
-  const int LPn = dim + 1 + 2 * HT;
-  const int64_t fbase2 = (i2 - fa.lb[o2]) * fa.s[o2];
-  const int64_t obase2 = (i2 - oa.lb[o2]) * oa.s[o2];
 
-  for (int idx = tid; idx < TI * LPn; idx += nthr) {
-    int l, nn;
-    if (dir == 0) { l = idx / LPn; nn = idx - l * LPn; }
-    else { nn = idx / TI; l = idx - nn * TI; }
-    const int n = nn - HT;
-    const int64_t i1 = l1_0 + l;
-    double val = 0.0;
-    if (i1 < l1_end && n >= fa.lb[dir] && n < fa.lb[dir] + fa.n[dir])
-      val = fb[fbase2 + (i1 - fa.lb[o1]) * fa.s[o1] + (n - fa.lb[dir]) * fa.s[dir]];
-    tile[l * LP + nn] = val;
+  // ---- staging: nodes -HT..dim+HT of each line; those outside f along dir are zero
+  const Slot sl = slot_of(dir, TI);
+  const int64_t i1 = i1_0 + sl.l;
+  const bool valid = i1 < i1_end;
+  const int nlo = (int)max((int64_t)-HT, fa.lb[dir]);
+  const int nhi = (int)min((int64_t)(dim + HT), fa.lb[dir] + fa.n[dir] - 1);
+  double* trow = tile + sl.l * LP + HT;   // node 0 of the slot line
+  {
+    const double* src = f + (int64_t)blockIdx.z * fa.fs + (i2 - fa.lb[o2]) * fa.s[o2] + (i1 - fa.lb[o1]) * fa.s[o1] -
+                        fa.lb[dir] * fa.s[dir];   // + n * s[dir] is node n
+    const int64_t sd = fa.s[dir];
+    int n = -HT + sl.n0;
+    if (!valid) {
+      for (; n <= dim + HT; n += sl.nst) trow[n] = 0.0;
+    } else if (dir == 0 && sd == 1 && (((uintptr_t)(src + nlo) ^ (uintptr_t)(trow + nlo)) & 15u) == 0) {
+      // x lines whose array and tile rows share the 16-byte phase: node pairs
+      for (; n < nlo; n += sl.nst) trow[n] = 0.0;
+      int first = nlo;
+      if (((uintptr_t)(trow + nlo) & 15u) != 0) {   // one leading node to reach the phase
+        if (sl.n0 == 0) cp8(trow + nlo, src + nlo);
+        ++first;
+      }
+      const int npair = (nhi - first + 1) / 2;
+      for (int p = sl.n0; p < npair; p += sl.nst) cp16(trow + first + 2 * p, src + first + 2 * p);
+      if (((nhi - first + 1) & 1) && sl.n0 == 0) cp8(trow + nhi, src + nhi);
+      for (int m = nhi + 1 + sl.n0; m <= dim + HT; m += sl.nst) trow[m] = 0.0;
+    } else {
+      for (; n < nlo; n += sl.nst) trow[n] = 0.0;
+      for (; n <= nhi; n += sl.nst) cp8(trow + n, src + (int64_t)n * sd);
+      for (; n <= dim + HT; n += sl.nst) trow[n] = 0.0;
+    }
   }
+  cp_wait_all();
   __syncthreads();
   if (op.kind != OP_EXPLICIT) {
     // closure-row RHS values, computed once per line before the solves
-    for (int it = tid; it < TI * 2 * NSP; it += nthr) {
+    for (int it = threadIdx.x; it < TI * 2 * NSP; it += blockDim.x) {
       const int j = it % (2 * NSP), ll = it / (2 * NSP);
       const bool lo = j < NSP;
       if (lo ? (j >= op.spec_lo) : (j - NSP >= op.spec_hi)) continue;
       const int r = lo ? j : op.nsys - op.spec_hi + (j - NSP);
       const double* li = tile + ll * LP + HT;
-      sp[it] = special_value(op, r, [li](int n) { return li[n]; });
+      sp[it] = special_value(op, r, [li](int nn) { return li[nn]; });
     }
     __syncthreads();
   }
 
-  const int warp = tid >> 5, lane = tid & 31;
-  const int l = warp / WPL, part = warp - l * WPL;
+  // ---- solves: line group g takes lines g and g + ngroups (TI = 2 * ngroups)
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int g = warp / WPL, part = warp - g * WPL;
   const int seg = part * 32 + lane;
-  double* line = tile + l * LP + HT;
-  auto get = [line](int n) { return line[n]; };
-  double v[S];
-  if (op.kind == OP_DERIV) {
-    rhs_deriv<S>(v, op, seg, get, sp + l * 2 * NSP);
-    seg_solve<S, WPL>(v, op.tab, seg, lane, part, l, scan + l * 2 * WPL);
-  } else if (op.kind == OP_FILTER) {
-    rhs_filter<S>(v, op, seg, get, sp + l * 2 * NSP);
-    seg_solve<S, WPL>(v, op.tab, seg, lane, part, l, scan + l * 2 * WPL);
+  const int ext = (op.kind == OP_EXPLICIT) ? 0 : op.ext_lo;
+  double v[2][S];
+  if (op.kind == OP_EXPLICIT) {
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+      const double* line = tile + (g + i * ngroups) * LP + HT;
+#pragma unroll
+      for (int t = 0; t < S; ++t) {
+        const int r = seg * S + t;
+        v[i][t] = (r <= dim) ? explicit_row(op, r, [line](int nn) { return line[nn]; }) : 0.0;
+      }
+    }
   } else {
 #pragma unroll
+    for (int i = 0; i < 2; ++i) {
+      const int l = g + i * ngroups;
+      const double* line = tile + l * LP + HT;
+      auto get = [line](int nn) { return line[nn]; };
+      if (op.kind == OP_DERIV) rhs_deriv<S>(v[i], op, seg, get, sp + l * 2 * NSP);
+      else rhs_filter<S>(v[i], op, seg, get, sp + l * 2 * NSP);
+    }
+    seg_solve_n<S, WPL, 2>(v, op.tab, seg, lane, part, g, scan + g * SCAN_LINE);
+  }
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < 2; ++i) {
+    double* line = tile + (g + i * ngroups) * LP + HT;
+#pragma unroll
     for (int t = 0; t < S; ++t) {
-      const int r = seg * S + t;
-      v[t] = (r <= dim) ? explicit_row(op, r, get) : 0.0;
+      const int n = seg * S + t - ext;
+      if (n < 0 || n > dim) continue;
+      // physical-boundary reset ff(0)=f(0), ff(dim)=f(dim) of compact_filter (filter.F90:141-142)
+      if (op.kind == OP_FILTER && ((n == 0 && op.left_phys) || (n == dim && op.right_phys))) continue;
+      line[n] = (op.kind == OP_FILTER) ? v[i][t] : scale * v[i][t];
     }
   }
   __syncthreads();
-  const int ext = (op.kind == OP_EXPLICIT) ? 0 : op.ext_lo;
-#pragma unroll
-  for (int t = 0; t < S; ++t) {
-    const int n = seg * S + t - ext;
-    if (n < 0 || n > dim) continue;
-    // physical-boundary reset ff(0)=f(0), ff(dim)=f(dim) of compact_filter (filter.F90:141-142)
-    if (op.kind == OP_FILTER && ((n == 0 && op.left_phys) || (n == dim && op.right_phys))) continue;
-    line[n] = (op.kind == OP_FILTER) ? v[t] : scale * v[t];
-  }
-  __syncthreads();
-  const int nout = dim + 1;
-  for (int idx = tid; idx < TI * nout; idx += nthr) {
-    int l2, n;
-    if (dir == 0) { l2 = idx / nout; n = idx - l2 * nout; }
-    else { n = idx / TI; l2 = idx - n * TI; }
-    const int64_t i1 = l1_0 + l2;
-    if (i1 >= l1_end) continue;
-    const double val = tile[l2 * LP + HT + n];
-    ob[obase2 + (i1 - oa.lb[o1]) * oa.s[o1] + (n - oa.lb[dir]) * oa.s[dir]] = val;
-  }
+
+  // ---- stores of nodes 0..dim from the tile
+  if (!valid) return;
+  double* dst = out + (int64_t)blockIdx.z * oa.fs + (i2 - oa.lb[o2]) * oa.s[o2] + (i1 - oa.lb[o1]) * oa.s[o1] -
+                oa.lb[dir] * oa.s[dir];
+  const int64_t od = oa.s[dir];
+  for (int n = sl.n0; n <= dim; n += sl.nst) dst[(int64_t)n * od] = trow[n];
 }
 
+// scan scratch of seg_solve_n: 2 * WPL doubles per solve, two solves per line group
 template <int S, int WPL>
 static cudaError_t launch_t(const DevOp& op, int dir, const double* f, const ArrDesc& fa, double* out,
                             const ArrDesc& oa, int nfields, double scale, cudaStream_t st) {
   const int o1 = (dir == 0) ? 1 : 0, o2 = (dir == 2) ? 1 : 2;
-  int TI = 512 / (32 * WPL);   // <= 15 lines when WPL > 1 (one named barrier per line)
-  if (TI > 16) TI = 16;
-  if (TI < 1) TI = 1;
+  // two lines per group of WPL warps, at most 512 threads and 16 lines, one named barrier per
+  // group (WPL > 1: at most 15 groups)
+  int ngroups = 512 / (32 * WPL);
+  if (ngroups > 8) ngroups = 8;
+  const int TI = 2 * ngroups;
   const int LP = tile_pitch(op.op.dim, TI, S);
-  const size_t smem = ((size_t)TI * LP + (size_t)TI * (2 * WPL + 2 * NSP)) * sizeof(double);
+  const size_t smem = ((size_t)TI * LP + (size_t)ngroups * 4 * WPL + (size_t)TI * 2 * NSP) * sizeof(double);
   auto kern = k_line_api<S, WPL>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   dim3 grid((unsigned)((oa.n[o1] + TI - 1) / TI), (unsigned)oa.n[o2], (unsigned)nfields);
-  kern<<<grid, TI * WPL * 32, smem, st>>>(op.op, dir, f, fa, out, oa, TI, LP, scale);
+  kern<<<grid, ngroups * WPL * 32, smem, st>>>(op.op, dir, f, fa, out, oa, TI, LP, scale);
   return cudaGetLastError();
 }
 
