@@ -8,6 +8,8 @@ Host-side mirror of the reference's interface (Perrbit/astr_gpu), over the C ABI
 * ``compact_filter`` — every line of an array (src/filter.F90:112)
 * ``TGVSolver`` — the Taylor-Green miniapp driver: ``flowfield_init``, ``rhscal``, ``rk3``,
   ``stacal`` (miniapps/tgv_solver_3d/tgvsolver.F90)
+* ``FullSolver`` — the full solver's ``time_integration_rk`` / ``rhscal`` on a periodic box
+  (src/mainloop.F90:298-476, src/solver.F90:184-283)
 
 Arrays are Fortran-ordered numpy arrays (host) or CUDA torch tensors laid out the same way
 (device). All compute runs in the CUDA library; there is no CPU path.
@@ -23,7 +25,7 @@ from . import _lib
 from ._lib import ASTR_DEVICE, ASTR_HOST, AstrParams
 
 __all__ = ["AstrError", "Context", "Scheme", "fd_scheme_initiate", "compact_filter_initiate", "central",
-           "compact_filter", "FlowParams", "TGVSolver"]
+           "compact_filter", "FlowParams", "TGVSolver", "FullSolver", "Ensemble"]
 
 
 class AstrError(RuntimeError):
@@ -291,6 +293,69 @@ class TGVSolver:
         self.ctx.check(self.ctx.L.astr_state_launch_shapes(self._h, buf))
         names = ["A", "B", "C", "A'", "B'", "F_C", "F_A"]
         return {nm: tuple(buf[6 * i:6 * i + 6]) for i, nm in enumerate(names)}
+
+
+class FullSolver:
+    """The full solver's time integration on a periodic box (``time_integration_rk`` with rk3,
+    src/mainloop.F90:298-476), on the reference's array layout with stored halos: the filter before
+    every stage's rhscal, qswap's averaging of nodes 0 and N with primitives recomputed on the
+    boundary planes only, rhscal in its metric form, the update of q*jacob. The default Sutherland
+    constant is the full solver's 110.3 (src/solver.F90:121-122)."""
+
+    def __init__(self, ctx: Context, im: int, jm: int | None = None, km: int | None = None,
+                 params: FlowParams | None = None):
+        self.ctx = ctx
+        self.im, self.jm, self.km = im, jm or im, km or im
+        p = params or FlowParams(sutherland=110.3)
+        self.params = p
+        cp = AstrParams(self.im, self.jm, self.km, p.mach, p.reynolds, p.prandtl, p.gamma, p.ref_tem, p.sutherland,
+                        p.alfa_filter, p.beta_halo, p.beta_bound, int(p.filter_on))
+        h = ctypes.c_void_p()
+        ctx.check(ctx.L.astr_full_create(ctx._h, ctypes.byref(cp), ctypes.byref(h)))
+        self._h = h
+
+    @property
+    def shape(self):
+        return (self.im + 1, self.jm + 1, self.km + 1)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self.ctx.L.astr_full_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_q(self, q, lbound=(0, 0, 0)):
+        qf = np.asfortranarray(q, dtype=np.float64)
+        self.ctx.check(self.ctx.L.astr_full_upload(self._h, ctypes.c_void_p(qf.ctypes.data), _i64(qf.shape[:3]),
+                                                   _i64(lbound), ASTR_HOST))
+
+    def get_q(self) -> np.ndarray:
+        out = np.zeros(self.shape + (5,), order="F")
+        self.ctx.check(self.ctx.L.astr_full_download(self._h, ctypes.c_void_p(out.ctypes.data), _i64(self.shape),
+                                                     _i64((0, 0, 0)), ASTR_HOST))
+        return out
+
+    def step(self, dt: float, nsteps: int = 1):
+        self.ctx.check(self.ctx.L.astr_full_step(self._h, dt, nsteps))
+
+    def rhs(self) -> np.ndarray:
+        """One stage's filterq + qswap + rhscal (the state keeps the filtered, averaged q)."""
+        out = np.zeros(self.shape + (5,), order="F")
+        self.ctx.check(self.ctx.L.astr_full_rhs(self._h, ctypes.c_void_p(out.ctypes.data), _i64(self.shape),
+                                                _i64((0, 0, 0)), ASTR_HOST))
+        return out
+
+    def history(self) -> np.ndarray:
+        n = ctypes.c_int()
+        self.ctx.check(self.ctx.L.astr_full_history(self._h, None, 0, ctypes.byref(n)))
+        out = np.zeros(max(n.value, 1) * 5)
+        self.ctx.check(self.ctx.L.astr_full_history(self._h, out.ctypes.data_as(_lib._dp), n.value, ctypes.byref(n)))
+        return out[: 5 * n.value].reshape(n.value, 5)
 
 
 class Ensemble:

@@ -70,6 +70,13 @@ SIGNATURES = {
     "astr_step_vjp": (_i, [_vp, _d, _vp, _vp, _i64p, _i64p, _i]),
     "astr_scheme_apply_transpose": (_i, [_vp, _vp, _i, _vp, _i64p, _vp, _i, _d]),
     "astr_cfl_dt_noalloc": (_i, [_vp, _vp, _i64p, _i64p, _i, _i, _i, _d, _d, _d, _dp]),
+    "astr_full_create": (_i, [_vp, ctypes.POINTER(AstrParams), _pvp]),
+    "astr_full_destroy": (_i, [_vp]),
+    "astr_full_upload": (_i, [_vp, _vp, _i64p, _i64p, _i]),
+    "astr_full_download": (_i, [_vp, _vp, _i64p, _i64p, _i]),
+    "astr_full_step": (_i, [_vp, _d, _i]),
+    "astr_full_rhs": (_i, [_vp, _vp, _i64p, _i64p, _i]),
+    "astr_full_history": (_i, [_vp, _dp, _i, _ip]),
 }
 
 _libs = {}

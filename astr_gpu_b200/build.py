@@ -17,7 +17,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libastr_b200.so")
 LIB_STRICT = os.path.join(HERE, "libastr_b200_strict.so")
 SOURCES = ["capi.cu", "tgv.cu", "lines.cu", "schemes.cu", "tgv_l3_1.cu", "tgv_l5_1.cu", "tgv_l9_1.cu", "tgv_l9_2.cu",
-           "tgv_l9_4.cu", "tgv_l5_2.cu", "tgv_l5_4.cu", "tgv_l17_1.cu", "noalloc.cu", "adjoint.cu", "adj_l3_1.cu", "adj_l5_1.cu",
+           "tgv_l9_4.cu", "tgv_l5_2.cu", "tgv_l5_4.cu", "tgv_l17_1.cu", "noalloc.cu", "fullsolver.cu", "adjoint.cu", "adj_l3_1.cu", "adj_l5_1.cu",
            "adj_l9_1.cu", "adj_l9_2.cu", "adj_l9_4.cu", "adj_l5_2.cu", "adj_l5_4.cu"]
 HEADERS = ["ops.cuh", "internal.h", "tgv.cuh", "tgv_kernels.cuh", "adjoint.cuh", "adj_kernels.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -1,0 +1,635 @@
+// The full solver's time integration on a periodic box, on the reference's own array layout.
+//
+// ASTR's production stage (time_integration_rk with rk3, src/mainloop.F90:392-476) differs from
+// the miniapp's (tgvsolver.F90:994-1082) in four ways that change results: the filter runs
+// before rhscal at every stage (filterq, src/comsolver.F90:514-632); qswap
+// (src/parallel.F90:4877-5060) copies the periodic halos of q, averages nodes 0 and N per
+// direction and recomputes the primitive variables only on the planes -hm..0 and N..N+hm, so the
+// interior primitives used by rhscal stay those of the unfiltered state of the last updatefvar
+// (src/fludyna.F90:191-242); rhscal takes the metric form (gradcal multiplies by dxi,
+// src/comsolver.F90:244-497; convrsdcal6 and diffrsdcal6 carry the Jacobian,
+// src/solver.F90:2174-2874); the update advances q*jacob (src/mainloop.F90:438-446).
+//
+// Because halo values differ from the periodic images of the interior (stale copies taken before
+// the averaging, primitives of the filtered state), this mode keeps every field on the reference's
+// layout: Fortran order, nodes -hm..N+hm on every axis (hm = 5), halos stored. Each stage is a
+// sequence of small pointwise kernels and line-operator launches (lines.cu) over those arrays,
+// one operation of the reference at a time. The metrics of the uniform grid are taken in closed
+// form: dxi = diag(1/dx, 1/dy, 1/dz), jacob = dx*dy*dz; the off-diagonal terms add zeros.
+#include <cmath>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/astr_b200.h"
+#include "internal.h"
+#include "tgv.cuh"
+
+using namespace astr;
+
+// Defined in capi.cu.
+cudaStream_t astr_ctx_stream(astr_ctx* ctx);
+int astr_ctx_device(astr_ctx* ctx);
+void astr_ctx_set_error(astr_ctx* ctx, const char* msg);
+
+namespace {
+
+constexpr int HMW = 5;   // halo width of the reference's arrays (commvar.F90:190)
+
+struct FsGeo {
+  int N[3];
+  int64_t s[3];    // element strides of i, j, k (s[0] = 1)
+  int64_t fs;      // elements per field
+  double rd[3];    // dxi: 1/dx, 1/dy, 1/dz
+  double jac;      // dx*dy*dz
+  // element offset of node (i, j, k) from node (-hm, -hm, -hm)
+  __host__ __device__ int64_t at(int i, int j, int k) const {
+    return (int64_t)(i + HMW) + (int64_t)(j + HMW) * s[1] + (int64_t)(k + HMW) * s[2];
+  }
+};
+
+struct FsThermo {
+  double const2, const5, const6, reynolds, prandtl, tc, tc1;
+};
+
+// Node (i, j, k) of the flat index p over the box [lo[a], hi[a]] on each axis.
+struct Box3 {
+  int lo[3], n[3];
+  __host__ __device__ int64_t size() const { return (int64_t)n[0] * n[1] * n[2]; }
+  __device__ void node(int64_t p, int& i, int& j, int& k) const {
+    i = lo[0] + (int)(p % n[0]);
+    const int64_t r = p / n[0];
+    j = lo[1] + (int)(r % n[1]);
+    k = lo[2] + (int)(r / n[1]);
+  }
+};
+
+// The box of nodes 0..N on every axis except `dir`, where it spans [a, b].
+__host__ __device__ Box3 box_line(const FsGeo& g, int dir, int a, int b) {
+  Box3 x;
+  for (int d = 0; d < 3; ++d) { x.lo[d] = 0; x.n[d] = g.N[d] + 1; }
+  if (dir >= 0) { x.lo[dir] = a; x.n[dir] = b - a + 1; }
+  return x;
+}
+
+#define GRID_STRIDE(p, total) \
+  for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < (total); p += (int64_t)gridDim.x * blockDim.x)
+
+// q2fvar (fludyna.F90:545-634, tgvsolver.F90:92-121) of one node
+__device__ __forceinline__ void fs_q2fvar(const FsThermo& th, double q0, double q1, double q2, double q3, double q4,
+                                          double& rho, double& u, double& v, double& w, double& p, double& t) {
+  rho = q0;
+  u = q1 / rho;
+  v = q2 / rho;
+  w = q3 / rho;
+  p = (q4 - 0.5 * rho * (u * u + v * v + w * w)) / th.const6;
+  t = p / rho * th.const2;
+}
+
+// Periodic halo copy along dir of nf fields (dataswap / bchomovec): F(-k) = F(N-k), F(N+k) = F(k),
+// k = 1..hm, on the lines whose other indices lie in 0..N.
+__global__ void k_fs_halo(double* F, int nf, int dir, FsGeo g) {
+  const Box3 b = [&] {
+    Box3 x;
+    for (int d = 0; d < 3; ++d) { x.lo[d] = 0; x.n[d] = g.N[d] + 1; }
+    x.lo[dir] = 1; x.n[dir] = HMW;
+    return x;
+  }();
+  const int64_t total = b.size() * nf;
+  const int N = g.N[dir];
+  GRID_STRIDE(p, total) {
+    const int m = (int)(p / b.size());
+    int i, j, k;
+    b.node(p - (int64_t)m * b.size(), i, j, k);
+    int lo[3] = {i, j, k}, hi[3] = {i, j, k}, slo[3] = {i, j, k}, shi[3] = {i, j, k};
+    const int kk = lo[dir];   // 1..hm
+    lo[dir] = -kk; slo[dir] = N - kk;
+    hi[dir] = N + kk; shi[dir] = kk;
+    double* f = F + m * g.fs;
+    f[g.at(lo[0], lo[1], lo[2])] = f[g.at(slo[0], slo[1], slo[2])];
+    f[g.at(hi[0], hi[1], hi[2])] = f[g.at(shi[0], shi[1], shi[2])];
+  }
+}
+
+// qswap along dir (one thread per line): the halo copy of q, the average of nodes 0 and N, and
+// q2fvar on the nodes -hm..0 and N..N+hm of the line (parallel.F90:4877-5060).
+__global__ void k_fs_qswap(double* q, double* rho, double* vel, double* prs, double* tmp, int dir, FsGeo g,
+                           FsThermo th) {
+  const Box3 b = box_line(g, dir, 0, 0);
+  const int N = g.N[dir];
+  const int64_t sd = g.s[dir];
+  GRID_STRIDE(p, b.size()) {
+    int i, j, k;
+    b.node(p, i, j, k);
+    const int64_t o0 = g.at(i, j, k);   // node 0 of the line (index along dir is 0)
+    for (int m = 0; m < 5; ++m) {
+      double* f = q + m * g.fs + o0;
+      for (int kk = 1; kk <= HMW; ++kk) {
+        f[-kk * sd] = f[(int64_t)(N - kk) * sd];
+        f[(int64_t)(N + kk) * sd] = f[(int64_t)kk * sd];
+      }
+      f[0] = 0.5 * (f[0] + f[(int64_t)N * sd]);
+      f[(int64_t)N * sd] = f[0];
+    }
+    for (int t = -HMW; t <= N + HMW; ++t) {
+      if (t > 0 && t < N) { t = N - 1; continue; }
+      const int64_t o = o0 + (int64_t)t * sd;
+      double r, u, v, w, pr, tt;
+      fs_q2fvar(th, q[o], q[g.fs + o], q[2 * g.fs + o], q[3 * g.fs + o], q[4 * g.fs + o], r, u, v, w, pr, tt);
+      rho[o] = r; vel[o] = u; vel[g.fs + o] = v; vel[2 * g.fs + o] = w; prs[o] = pr; tmp[o] = tt;
+    }
+  }
+}
+
+// convrsdcal6's fluxes along dir at nodes -hm..N+hm (solver.F90:2201-2207): uu = dxi u_dir,
+// fcs1 = jacob q1 uu, fcs(1+m) = jacob (q(1+m) uu + dxi p delta(m,dir)), fcs5 = jacob (q5 + p) uu.
+__global__ void k_fs_conv_flux(double* F, const double* q, const double* vel, const double* prs, int dir, FsGeo g) {
+  const Box3 b = box_line(g, dir, -HMW, g.N[dir] + HMW);
+  const double dxi = g.rd[dir], jb = g.jac;
+  GRID_STRIDE(p, b.size()) {
+    int i, j, k;
+    b.node(p, i, j, k);
+    const int64_t o = g.at(i, j, k);
+    const double uu = dxi * vel[dir * g.fs + o];
+    const double pr = prs[o];
+    F[o] = jb * q[o] * uu;
+#pragma unroll
+    for (int m = 1; m <= 3; ++m) {
+      const double qm = q[m * g.fs + o];
+      F[m * g.fs + o] = (m - 1 == dir) ? jb * (qm * uu + dxi * pr) : jb * (qm * uu);
+    }
+    F[4 * g.fs + o] = jb * (q[4 * g.fs + o] + pr) * uu;
+  }
+}
+
+// diffrsdcal6's pointwise part at nodes 0..N (solver.F90:2458-2546): Sutherland viscosity, the
+// viscous stress and the heat flux.
+__global__ void k_fs_stress(double* sigma, double* qflux, const double* dvel, const double* dtmp, const double* vel,
+                            const double* tmp, FsGeo g, FsThermo th) {
+  const Box3 b = box_line(g, -1, 0, 0);
+  const int64_t fs = g.fs;
+  GRID_STRIDE(p, b.size()) {
+    int i, j, k;
+    b.node(p, i, j, k);
+    const int64_t o = g.at(i, j, k);
+    // dvel(:,:,:,n,d) is field 3d + n
+    const double s11 = dvel[0 * fs + o];
+    const double s12 = 0.5 * (dvel[3 * fs + o] + dvel[1 * fs + o]);
+    const double s13 = 0.5 * (dvel[6 * fs + o] + dvel[2 * fs + o]);
+    const double s22 = dvel[4 * fs + o];
+    const double s23 = 0.5 * (dvel[7 * fs + o] + dvel[5 * fs + o]);
+    const double s33 = dvel[8 * fs + o];
+    const double skk = (1.0 / 3.0) * (s11 + s22 + s33);
+    const double t = tmp[o];
+    const double miu = t * sqrt(t) * th.tc1 / (t + th.tc) / th.reynolds;
+    const double miu2 = 2.0 * miu;
+    const double hcc = (miu / th.prandtl) / th.const5;
+    const double sg0 = miu2 * (s11 - skk), sg1 = miu2 * s12, sg2 = miu2 * s13;
+    const double sg3 = miu2 * (s22 - skk), sg4 = miu2 * s23, sg5 = miu2 * (s33 - skk);
+    sigma[o] = sg0; sigma[fs + o] = sg1; sigma[2 * fs + o] = sg2;
+    sigma[3 * fs + o] = sg3; sigma[4 * fs + o] = sg4; sigma[5 * fs + o] = sg5;
+    const double u = vel[o], v = vel[fs + o], w = vel[2 * fs + o];
+    qflux[o] = hcc * dtmp[o] + sg0 * u + sg1 * v + sg2 * w;
+    qflux[fs + o] = hcc * dtmp[fs + o] + sg1 * u + sg3 * v + sg4 * w;
+    qflux[2 * fs + o] = hcc * dtmp[2 * fs + o] + sg2 * u + sg4 * v + sg5 * w;
+  }
+}
+
+// diffrsdcal6's fluxes along dir at nodes -hm..N+hm (solver.F90:2622-2640):
+// ff = (sigma(row dir) . dxi) * jacob for the momenta, (qflux . dxi) * jacob for the energy.
+__global__ void k_fs_visc_flux(double* F, const double* sigma, const double* qflux, int dir, FsGeo g) {
+  const Box3 b = box_line(g, dir, -HMW, g.N[dir] + HMW);
+  const double dxi = g.rd[dir], jb = g.jac;
+  const int sgi[3][3] = {{0, 1, 2}, {1, 3, 4}, {2, 4, 5}};
+  GRID_STRIDE(p, b.size()) {
+    int i, j, k;
+    b.node(p, i, j, k);
+    const int64_t o = g.at(i, j, k);
+#pragma unroll
+    for (int n = 0; n < 3; ++n) F[n * g.fs + o] = sigma[sgi[dir][n] * g.fs + o] * dxi * jb;
+    F[3 * g.fs + o] = qflux[dir * g.fs + o] * dxi * jb;
+  }
+}
+
+__global__ void k_fs_negate(double* f, FsGeo g) {
+  const Box3 b = box_line(g, -1, 0, 0);
+  GRID_STRIDE(p, b.size() * 5) {
+    const int m = (int)(p / b.size());
+    int i, j, k;
+    b.node(p - (int64_t)m * b.size(), i, j, k);
+    const int64_t o = m * g.fs + g.at(i, j, k);
+    f[o] = -f[o];
+  }
+}
+
+// The rk3 update of q*jacob (mainloop.F90:426-446); at the first stage qsave = q*jacob first.
+__global__ void k_fs_update(double* q, double* qsave, const double* qrhs, double c1, double c2, double c3, double dt,
+                            int first, FsGeo g) {
+  const Box3 b = box_line(g, -1, 0, 0);
+  const double jb = g.jac;
+  GRID_STRIDE(p, b.size() * 5) {
+    const int m = (int)(p / b.size());
+    int i, j, k;
+    b.node(p - (int64_t)m * b.size(), i, j, k);
+    const int64_t o = m * g.fs + g.at(i, j, k);
+    if (first) qsave[o] = q[o] * jb;
+    const double v = c1 * qsave[o] + c2 * q[o] * jb + c3 * qrhs[o] * dt;
+    q[o] = v / jb;
+  }
+}
+
+// updatefvar on nodes 0..N (fludyna.F90:191-242)
+__global__ void k_fs_prims(const double* q, double* rho, double* vel, double* prs, double* tmp, FsGeo g, FsThermo th) {
+  const Box3 b = box_line(g, -1, 0, 0);
+  const int64_t fs = g.fs;
+  GRID_STRIDE(p, b.size()) {
+    int i, j, k;
+    b.node(p, i, j, k);
+    const int64_t o = g.at(i, j, k);
+    double r, u, v, w, pr, t;
+    fs_q2fvar(th, q[o], q[fs + o], q[2 * fs + o], q[3 * fs + o], q[4 * fs + o], r, u, v, w, pr, t);
+    rho[o] = r; vel[o] = u; vel[fs + o] = v; vel[2 * fs + o] = w; prs[o] = pr; tmp[o] = t;
+  }
+}
+
+// stacal / diss_rate_cal terms summed over nodes 1..N, per CTA (tgvsolver.F90:913-931,
+// statistic.F90:1009-1034); the ordered final reduction is k_diag_reduce.
+__global__ void k_fs_diag(double* partials, const double* rho, const double* vel, const double* dvel,
+                          const double* tmp, FsGeo g, FsThermo th) {
+  Box3 b;
+  for (int d = 0; d < 3; ++d) { b.lo[d] = 1; b.n[d] = g.N[d]; }
+  const int64_t fs = g.fs;
+  double ke = 0.0, en = 0.0, di = 0.0;
+  GRID_STRIDE(p, b.size()) {
+    int i, j, k;
+    b.node(p, i, j, k);
+    const int64_t o = g.at(i, j, k);
+    const double u = vel[o], v = vel[fs + o], w = vel[2 * fs + o], r = rho[o];
+    ke += r * (u * u + v * v + w * w);
+    const double om1 = dvel[5 * fs + o] - dvel[7 * fs + o];
+    const double om2 = dvel[6 * fs + o] - dvel[2 * fs + o];
+    const double om3 = dvel[1 * fs + o] - dvel[3 * fs + o];
+    en += r * (om1 * om1 + om2 * om2 + om3 * om3);
+    const double t = tmp[o];
+    const double miu = t * sqrt(t) * th.tc1 / (t + th.tc) / th.reynolds;
+    const double s11 = dvel[o], s12 = 0.5 * (dvel[3 * fs + o] + dvel[1 * fs + o]);
+    const double s13 = 0.5 * (dvel[6 * fs + o] + dvel[2 * fs + o]);
+    const double s22 = dvel[4 * fs + o], s23 = 0.5 * (dvel[7 * fs + o] + dvel[5 * fs + o]), s33 = dvel[8 * fs + o];
+    const double div = s11 + s22 + s33;
+    di += 2.0 * miu * (s11 * s11 + s22 * s22 + s33 * s33 + 2.0 * (s12 * s12 + s13 * s13 + s23 * s23) -
+                       (1.0 / 3.0) * (div * div));
+  }
+  __shared__ double s[3][256];
+  s[0][threadIdx.x] = ke; s[1][threadIdx.x] = en; s[2][threadIdx.x] = di;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w)
+      for (int c = 0; c < 3; ++c) s[c][threadIdx.x] += s[c][threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0)
+    for (int c = 0; c < 3; ++c) partials[3 * blockIdx.x + c] = s[c][0];
+}
+
+// Copy between the caller's Fortran array (nodes 0..N inside it) and nodes 0..N of the layout.
+__global__ void k_fs_pack(double* state, double* user, FsGeo g, int64_t u0, int64_t u1, int64_t u2, int64_t ufs,
+                          int64_t uoff, int to_state) {
+  const Box3 b = box_line(g, -1, 0, 0);
+  GRID_STRIDE(p, b.size() * 5) {
+    const int m = (int)(p / b.size());
+    int i, j, k;
+    b.node(p - (int64_t)m * b.size(), i, j, k);
+    const int64_t os = m * g.fs + g.at(i, j, k);
+    const int64_t ou = uoff + m * ufs + i * u0 + j * u1 + k * u2;
+    if (to_state) state[os] = user[ou];
+    else user[ou] = state[os];
+  }
+}
+
+unsigned blocks_for(int64_t n) {
+  int64_t b = (n + 255) / 256;
+  const int64_t cap = 148 * 16;
+  return (unsigned)(b < 1 ? 1 : (b > cap ? cap : b));
+}
+
+}  // namespace
+
+struct astr_full {
+  astr_ctx* ctx = nullptr;
+  astr_params p{};
+  FsGeo g{};
+  FsThermo th{};
+  double* buf = nullptr;
+  double *q = nullptr, *qt = nullptr, *rho = nullptr, *vel = nullptr, *prs = nullptr, *tmp = nullptr;
+  double *qsave = nullptr, *qrhs = nullptr, *dvel = nullptr, *dtmp = nullptr, *sigma = nullptr, *qflux = nullptr;
+  double* work = nullptr;   // flux lines of one direction (5 fields)
+  double* partials = nullptr;
+  int nparts = 0;
+  double* hist = nullptr;
+  int* counter = nullptr;
+  int hist_cap = 1 << 16;
+  HostOp hd[3], hf[3];
+  DevOp dd[3], df[3];
+  int nstep = 0;
+  double time = 0.0;
+  std::vector<double> row_key;
+};
+
+namespace {
+
+int ffail(astr_full* f, int code, const std::string& msg) {
+  if (f && f->ctx) astr_ctx_set_error(f->ctx, msg.c_str());
+  return code;
+}
+#define FCK(call)                                                                          \
+  do {                                                                                     \
+    cudaError_t e_ = (call);                                                               \
+    if (e_ != cudaSuccess) return ffail(fs, ASTR_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+struct OnDev {
+  int prev = -1;
+  explicit OnDev(int dev) {
+    int cur = -1;
+    if (dev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != dev && cudaSetDevice(dev) == cudaSuccess) prev = cur;
+  }
+  ~OnDev() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+};
+
+// Line-operator view of a field of the layout: the full range -hm..N+hm along `full` (or none
+// when full < 0), nodes 0..N on the other axes. Returns the pointer the descriptor is relative to.
+double* view(const astr_full* fs, double* base, int full, ArrDesc& a) {
+  int64_t off = 0;
+  for (int d = 0; d < 3; ++d) {
+    a.s[d] = fs->g.s[d];
+    if (d == full) { a.lb[d] = -HMW; a.n[d] = fs->g.N[d] + 1 + 2 * HMW; }
+    else { a.lb[d] = 0; a.n[d] = fs->g.N[d] + 1; off += HMW * fs->g.s[d]; }
+  }
+  a.fs = fs->g.fs;
+  return base + off;
+}
+
+// out (nodes 0..N) [+]= scale * op(in) along dir for nf fields
+cudaError_t line_op(astr_full* fs, const DevOp& op, int dir, double* in, double* out, int nf, double scale, int add) {
+  ArrDesc fa, oa;
+  double* fp = view(fs, in, dir, fa);
+  double* op_ = view(fs, out, -1, oa);
+  return launch_line_api(op, dir, fp, fa, op_, oa, nf, scale, astr_ctx_stream(fs->ctx), add);
+}
+
+cudaError_t fs_halo(astr_full* fs, double* F, int nf, int dir) {
+  const int64_t n = (int64_t)nf * HMW * (fs->g.N[0] + 1) * (fs->g.N[1] + 1) * (fs->g.N[2] + 1) / (fs->g.N[dir] + 1);
+  k_fs_halo<<<blocks_for(n), 256, 0, astr_ctx_stream(fs->ctx)>>>(F, nf, dir, fs->g);
+  return cudaGetLastError();
+}
+
+int64_t nodes(const astr_full* fs) { return (int64_t)(fs->g.N[0] + 1) * (fs->g.N[1] + 1) * (fs->g.N[2] + 1); }
+
+// filterq, then qswap, then rhscal into qrhs; diagnostics of the stage when `diag`
+cudaError_t fs_stage_rhs(astr_full* fs, bool diag) {
+  cudaStream_t st = astr_ctx_stream(fs->ctx);
+  cudaError_t e;
+  const FsGeo& g = fs->g;
+  const int64_t nn = nodes(fs);
+  if (fs->p.filter_on) {
+    for (int d = 0; d < 3; ++d) {
+      if ((e = fs_halo(fs, fs->q, 5, d)) != cudaSuccess) return e;
+      if ((e = line_op(fs, fs->df[d], d, fs->q, fs->qt, 5, 1.0, 0)) != cudaSuccess) return e;
+      std::swap(fs->q, fs->qt);
+    }
+  }
+  if ((e = cudaMemsetAsync(fs->qrhs, 0, 5 * (size_t)g.fs * sizeof(double), st)) != cudaSuccess) return e;
+  for (int d = 0; d < 3; ++d) {
+    const int64_t nl = nn / (g.N[d] + 1);
+    k_fs_qswap<<<blocks_for(nl), 256, 0, st>>>(fs->q, fs->rho, fs->vel, fs->prs, fs->tmp, d, g, fs->th);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  }
+  // gradcal
+  for (int d = 0; d < 3; ++d) {
+    if ((e = line_op(fs, fs->dd[d], d, fs->vel, fs->dvel + 3 * d * g.fs, 3, g.rd[d], 0)) != cudaSuccess) return e;
+    if ((e = line_op(fs, fs->dd[d], d, fs->tmp, fs->dtmp + d * g.fs, 1, g.rd[d], 0)) != cudaSuccess) return e;
+  }
+  // convrsdcal6
+  for (int d = 0; d < 3; ++d) {
+    const int64_t nl = nn / (g.N[d] + 1) * (g.N[d] + 1 + 2 * HMW);
+    k_fs_conv_flux<<<blocks_for(nl), 256, 0, st>>>(fs->work, fs->q, fs->vel, fs->prs, d, g);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if ((e = line_op(fs, fs->dd[d], d, fs->work, fs->qrhs, 5, 1.0, 1)) != cudaSuccess) return e;
+  }
+  k_fs_negate<<<blocks_for(5 * nn), 256, 0, st>>>(fs->qrhs, g);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  // diffrsdcal6
+  k_fs_stress<<<blocks_for(nn), 256, 0, st>>>(fs->sigma, fs->qflux, fs->dvel, fs->dtmp, fs->vel, fs->tmp, g, fs->th);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  for (int d = 0; d < 3; ++d) {
+    if ((e = fs_halo(fs, fs->sigma, 6, d)) != cudaSuccess) return e;
+    if ((e = fs_halo(fs, fs->qflux, 3, d)) != cudaSuccess) return e;
+  }
+  for (int d = 0; d < 3; ++d) {
+    const int64_t nl = nn / (g.N[d] + 1) * (g.N[d] + 1 + 2 * HMW);
+    k_fs_visc_flux<<<blocks_for(nl), 256, 0, st>>>(fs->work, fs->sigma, fs->qflux, d, g);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if ((e = line_op(fs, fs->dd[d], d, fs->work, fs->qrhs + g.fs, 4, 1.0, 1)) != cudaSuccess) return e;
+  }
+  if (diag) {
+    k_fs_diag<<<fs->nparts, 256, 0, st>>>(fs->partials, fs->rho, fs->vel, fs->dvel, fs->tmp, g, fs->th);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    const double norm = (double)fs->p.im * (double)fs->p.jm * (double)fs->p.km;
+    if ((e = launch_diag_reduce(fs->partials, fs->nparts, fs->hist, fs->counter, norm, st)) != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+cudaError_t fs_step(astr_full* fs, double dt) {
+  static const double rk[3][3] = {{1.0, 0.0, 1.0}, {0.75, 0.25, 0.25}, {1.0 / 3.0, 2.0 / 3.0, 2.0 / 3.0}};
+  cudaStream_t st = astr_ctx_stream(fs->ctx);
+  const int64_t nn = nodes(fs);
+  cudaError_t e;
+  for (int s = 0; s < 3; ++s) {
+    if ((e = fs_stage_rhs(fs, s == 0)) != cudaSuccess) return e;
+    k_fs_update<<<blocks_for(5 * nn), 256, 0, st>>>(fs->q, fs->qsave, fs->qrhs, rk[s][0], rk[s][1], rk[s][2], dt,
+                                                   s == 0, fs->g);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    k_fs_prims<<<blocks_for(nn), 256, 0, st>>>(fs->q, fs->rho, fs->vel, fs->prs, fs->tmp, fs->g, fs->th);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+int fs_copy(astr_full* fs, double* user, const int64_t* shape, const int64_t* lb, int to_state, int where) {
+  const int N[3] = {fs->p.im, fs->p.jm, fs->p.km};
+  for (int d = 0; d < 3; ++d)
+    if (lb[d] > 0 || lb[d] + shape[d] - 1 < N[d]) return ffail(fs, ASTR_ERR_ARG, "array must cover nodes 0..N on every axis");
+  cudaStream_t st = astr_ctx_stream(fs->ctx);
+  const int64_t u1 = shape[0], u2 = shape[0] * shape[1], ufs = shape[0] * shape[1] * shape[2];
+  const int64_t uoff = -lb[0] - lb[1] * u1 - lb[2] * u2;
+  double* dev = user;
+  if (where == ASTR_HOST) {
+    // through the filter's second buffer (free between calls)
+    if ((size_t)(5 * ufs) > 5 * (size_t)fs->g.fs) return ffail(fs, ASTR_ERR_ARG, "host array larger than the staging buffer");
+    dev = fs->qt;
+    if (to_state) FCK(cudaMemcpyAsync(dev, user, 5 * ufs * sizeof(double), cudaMemcpyHostToDevice, st));
+  }
+  k_fs_pack<<<blocks_for(5 * nodes(fs)), 256, 0, st>>>(fs->q, dev, fs->g, 1, u1, u2, ufs, uoff, to_state);
+  FCK(cudaGetLastError());
+  if (where == ASTR_HOST && !to_state) FCK(cudaMemcpyAsync(user, dev, 5 * ufs * sizeof(double), cudaMemcpyDeviceToHost, st));
+  FCK(cudaStreamSynchronize(st));
+  return ASTR_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int astr_full_create(astr_ctx* ctx, const astr_params* p, astr_full** out) {
+  if (!ctx || !p || !out) return ASTR_ERR_ARG;
+  const OnDev on(astr_ctx_device(ctx));
+  const int N[3] = {p->im, p->jm, p->km};
+  for (int d = 0; d < 3; ++d)
+    if (N[d] < 16) {
+      astr_ctx_set_error(ctx, "each dimension must be >= 16");
+      return ASTR_ERR_ARG;
+    }
+  astr_full* fs = new (std::nothrow) astr_full();
+  if (!fs) return ASTR_ERR_NOMEM;
+  fs->ctx = ctx;
+  fs->p = *p;
+  FsGeo& g = fs->g;
+  const double pi = 4.0 * std::atan(1.0);
+  for (int d = 0; d < 3; ++d) g.N[d] = N[d];
+  g.s[0] = 1;
+  g.s[1] = N[0] + 1 + 2 * HMW;
+  g.s[2] = g.s[1] * (N[1] + 1 + 2 * HMW);
+  g.fs = g.s[2] * (N[2] + 1 + 2 * HMW);
+  const double h[3] = {2.0 * pi / double(N[0]), 2.0 * pi / double(N[1]), 2.0 * pi / double(N[2])};
+  for (int d = 0; d < 3; ++d) g.rd[d] = 1.0 / h[d];
+  g.jac = h[0] * h[1] * h[2];
+  const double gm = p->gamma, m = p->mach;
+  fs->th.const2 = gm * (m * m);
+  fs->th.const5 = (gm - 1.0) * (m * m);
+  fs->th.const6 = 1.0 / (gm - 1.0);
+  fs->th.reynolds = p->reynolds;
+  fs->th.prandtl = p->prandtl;
+  fs->th.tc = p->sutherland / p->ref_tem;
+  fs->th.tc1 = 1.0 + fs->th.tc;
+  for (int d = 0; d < 3; ++d) {
+    build_fd_op(fs->hd[d], "643c", 3, N[d]);
+    build_filter_op(fs->hf[d], 3, N[d], p->alfa_filter, p->beta_halo, p->beta_bound, false);
+    const Layout L = pick_layout(fs->hf[d].nsys());
+    if (L.S == 0) { delete fs; astr_ctx_set_error(ctx, "dimension too large (max 1145)"); return ASTR_ERR_UNSUPPORTED; }
+    if (make_devop(fs->hd[d], pick_layout(fs->hd[d].nsys()), fs->dd[d]) != cudaSuccess ||
+        make_devop(fs->hf[d], L, fs->df[d]) != cudaSuccess) {
+      astr_full_destroy(fs);
+      astr_ctx_set_error(ctx, "scheme tables");
+      return ASTR_ERR_CUDA;
+    }
+  }
+  // q(5) qt(5) rho vel(3) prs tmp qsave(5) qrhs(5) dvel(9) dtmp(3) sigma(6) qflux(3) work(5)
+  const size_t nf = 52;
+  if (cudaMalloc(&fs->buf, nf * (size_t)g.fs * sizeof(double)) != cudaSuccess) {
+    astr_full_destroy(fs);
+    astr_ctx_set_error(ctx, "full-solver state allocation");
+    return ASTR_ERR_NOMEM;
+  }
+  cudaStream_t st = astr_ctx_stream(ctx);
+  cudaMemsetAsync(fs->buf, 0, nf * (size_t)g.fs * sizeof(double), st);
+  double* b = fs->buf;
+  auto take = [&](int n) { double* r = b; b += (size_t)n * g.fs; return r; };
+  fs->q = take(5); fs->qt = take(5); fs->rho = take(1); fs->vel = take(3); fs->prs = take(1); fs->tmp = take(1);
+  fs->qsave = take(5); fs->qrhs = take(5); fs->dvel = take(9); fs->dtmp = take(3); fs->sigma = take(6);
+  fs->qflux = take(3); fs->work = take(5);
+  fs->nparts = 148 * 4;
+  if (cudaMalloc(&fs->partials, (size_t)fs->nparts * 3 * sizeof(double)) != cudaSuccess ||
+      cudaMalloc(&fs->hist, (size_t)fs->hist_cap * 3 * sizeof(double)) != cudaSuccess ||
+      cudaMalloc(&fs->counter, sizeof(int)) != cudaSuccess) {
+    astr_full_destroy(fs);
+    astr_ctx_set_error(ctx, "full-solver state allocation");
+    return ASTR_ERR_NOMEM;
+  }
+  cudaMemsetAsync(fs->counter, 0, sizeof(int), st);
+  if (cudaStreamSynchronize(st) != cudaSuccess) { astr_full_destroy(fs); return ASTR_ERR_CUDA; }
+  *out = fs;
+  return ASTR_OK;
+}
+
+int astr_full_destroy(astr_full* fs) {
+  if (!fs) return ASTR_ERR_ARG;
+  const OnDev on(astr_ctx_device(fs->ctx));
+  cudaStreamSynchronize(astr_ctx_stream(fs->ctx));
+  for (int d = 0; d < 3; ++d) { free_devop(fs->dd[d]); free_devop(fs->df[d]); }
+  if (fs->buf) cudaFree(fs->buf);
+  if (fs->partials) cudaFree(fs->partials);
+  if (fs->hist) cudaFree(fs->hist);
+  if (fs->counter) cudaFree(fs->counter);
+  delete fs;
+  return ASTR_OK;
+}
+
+int astr_full_upload(astr_full* fs, const double* q, const int64_t shape[3], const int64_t lbound[3], int where) {
+  if (!fs || !q || !shape || !lbound) return ASTR_ERR_ARG;
+  const OnDev on(astr_ctx_device(fs->ctx));
+  int rc = fs_copy(fs, const_cast<double*>(q), shape, lbound, 1, where);
+  if (rc) return rc;
+  cudaStream_t st = astr_ctx_stream(fs->ctx);
+  k_fs_prims<<<blocks_for(nodes(fs)), 256, 0, st>>>(fs->q, fs->rho, fs->vel, fs->prs, fs->tmp, fs->g, fs->th);
+  FCK(cudaGetLastError());
+  FCK(cudaStreamSynchronize(st));
+  return ASTR_OK;
+}
+
+int astr_full_download(astr_full* fs, double* q, const int64_t shape[3], const int64_t lbound[3], int where) {
+  if (!fs || !q || !shape || !lbound) return ASTR_ERR_ARG;
+  const OnDev on(astr_ctx_device(fs->ctx));
+  return fs_copy(fs, q, shape, lbound, 0, where);
+}
+
+int astr_full_rhs(astr_full* fs, double* qrhs, const int64_t shape[3], const int64_t lbound[3], int where) {
+  if (!fs || !qrhs || !shape || !lbound) return ASTR_ERR_ARG;
+  const OnDev on(astr_ctx_device(fs->ctx));
+  FCK(fs_stage_rhs(fs, false));
+  // qrhs goes out through the pack kernel: swap it in for q for the copy
+  std::swap(fs->q, fs->qrhs);
+  int rc = fs_copy(fs, qrhs, shape, lbound, 0, where);
+  std::swap(fs->q, fs->qrhs);
+  return rc;
+}
+
+int astr_full_step(astr_full* fs, double dt, int nsteps) {
+  if (!fs || !(dt > 0.0) || nsteps < 0) return ASTR_ERR_ARG;
+  const OnDev on(astr_ctx_device(fs->ctx));
+  if (fs->nstep + nsteps > fs->hist_cap) return ffail(fs, ASTR_ERR_UNSUPPORTED, "history buffer full (65536 steps)");
+  for (int s = 0; s < nsteps; ++s) {
+    fs->row_key.push_back((double)fs->nstep);
+    fs->row_key.push_back(fs->time);
+    FCK(fs_step(fs, dt));
+    fs->nstep += 1;
+    fs->time = fs->time + dt;
+  }
+  FCK(cudaStreamSynchronize(astr_ctx_stream(fs->ctx)));
+  return ASTR_OK;
+}
+
+int astr_full_history(astr_full* fs, double* rows, int maxrows, int* nrows) {
+  if (!fs || !nrows) return ASTR_ERR_ARG;
+  const OnDev on(astr_ctx_device(fs->ctx));
+  const int n = fs->nstep;
+  *nrows = n;
+  if (!rows || maxrows <= 0 || n == 0) return ASTR_OK;
+  const int k = n < maxrows ? n : maxrows;
+  std::vector<double> h((size_t)3 * k);
+  cudaStream_t st = astr_ctx_stream(fs->ctx);
+  FCK(cudaMemcpyAsync(h.data(), fs->hist, h.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+  FCK(cudaStreamSynchronize(st));
+  for (int r = 0; r < k; ++r) {
+    rows[5 * r] = fs->row_key[2 * r];
+    rows[5 * r + 1] = fs->row_key[2 * r + 1];
+    rows[5 * r + 2] = h[3 * r];
+    rows[5 * r + 3] = h[3 * r + 1];
+    rows[5 * r + 4] = h[3 * r + 2];
+  }
+  return ASTR_OK;
+}
+
+}  // extern "C"

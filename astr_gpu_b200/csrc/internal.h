@@ -47,7 +47,8 @@ int tile_pitch(int dim, int TI, int S);
 
 // Line-level API launch: op along dir over every line of an arbitrary strided array.
 struct ArrDesc { int64_t s[3]; int64_t lb[3]; int64_t n[3]; int64_t fs; };
+// add != 0 accumulates into out (out += result) instead of storing.
 cudaError_t launch_line_api(const DevOp& op, int dir, const double* f, const ArrDesc& fa, double* out,
-                            const ArrDesc& oa, int nfields, double scale, cudaStream_t st);
+                            const ArrDesc& oa, int nfields, double scale, cudaStream_t st, int add = 0);
 
 }  // namespace astr

@@ -52,7 +52,8 @@ __device__ __forceinline__ Slot slot_of(int dir, int TI) {
 
 template <int S, int WPL>
 __global__ void __launch_bounds__(512) k_line_api(LineOp op, int dir, const double* __restrict__ f, ArrDesc fa,
-                                                  double* __restrict__ out, ArrDesc oa, int TI, int LP, double scale) {
+                                                  double* __restrict__ out, ArrDesc oa, int TI, int LP, double scale,
+                                                  int add) {
   extern __shared__ double sm[];
   double* tile = sm;
   double* scan = sm + (size_t)TI * LP;                 // SCAN_LINE doubles per line group
@@ -160,13 +161,17 @@ __global__ void __launch_bounds__(512) k_line_api(LineOp op, int dir, const doub
   double* dst = out + (int64_t)blockIdx.z * oa.fs + (i2 - oa.lb[o2]) * oa.s[o2] + (i1 - oa.lb[o1]) * oa.s[o1] -
                 oa.lb[dir] * oa.s[dir];
   const int64_t od = oa.s[dir];
-  for (int n = sl.n0; n <= dim; n += sl.nst) dst[(int64_t)n * od] = trow[n];
+  if (add) {
+    for (int n = sl.n0; n <= dim; n += sl.nst) dst[(int64_t)n * od] += trow[n];
+  } else {
+    for (int n = sl.n0; n <= dim; n += sl.nst) dst[(int64_t)n * od] = trow[n];
+  }
 }
 
 // scan scratch of seg_solve_n: 2 * WPL doubles per solve, two solves per line group
 template <int S, int WPL>
 static cudaError_t launch_t(const DevOp& op, int dir, const double* f, const ArrDesc& fa, double* out,
-                            const ArrDesc& oa, int nfields, double scale, cudaStream_t st) {
+                            const ArrDesc& oa, int nfields, double scale, int add, cudaStream_t st) {
   const int o1 = (dir == 0) ? 1 : 0, o2 = (dir == 2) ? 1 : 2;
   // two lines per group of WPL warps, at most 512 threads and 16 lines, one named barrier per
   // group (WPL > 1: at most 15 groups)
@@ -179,19 +184,19 @@ static cudaError_t launch_t(const DevOp& op, int dir, const double* f, const Arr
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   dim3 grid((unsigned)((oa.n[o1] + TI - 1) / TI), (unsigned)oa.n[o2], (unsigned)nfields);
-  kern<<<grid, ngroups * WPL * 32, smem, st>>>(op.op, dir, f, fa, out, oa, TI, LP, scale);
+  kern<<<grid, ngroups * WPL * 32, smem, st>>>(op.op, dir, f, fa, out, oa, TI, LP, scale, add);
   return cudaGetLastError();
 }
 
 cudaError_t launch_line_api(const DevOp& op, int dir, const double* f, const ArrDesc& fa, double* out,
-                            const ArrDesc& oa, int nfields, double scale, cudaStream_t st) {
-  if (op.S == 3 && op.WPL == 1) return launch_t<3, 1>(op, dir, f, fa, out, oa, nfields, scale, st);
-  if (op.S == 5 && op.WPL == 1) return launch_t<5, 1>(op, dir, f, fa, out, oa, nfields, scale, st);
-  if (op.S == 5 && op.WPL == 2) return launch_t<5, 2>(op, dir, f, fa, out, oa, nfields, scale, st);
-  if (op.S == 5 && op.WPL == 4) return launch_t<5, 4>(op, dir, f, fa, out, oa, nfields, scale, st);
-  if (op.S == 9 && op.WPL == 1) return launch_t<9, 1>(op, dir, f, fa, out, oa, nfields, scale, st);
-  if (op.S == 9 && op.WPL == 2) return launch_t<9, 2>(op, dir, f, fa, out, oa, nfields, scale, st);
-  if (op.S == 9 && op.WPL == 4) return launch_t<9, 4>(op, dir, f, fa, out, oa, nfields, scale, st);
+                            const ArrDesc& oa, int nfields, double scale, cudaStream_t st, int add) {
+  if (op.S == 3 && op.WPL == 1) return launch_t<3, 1>(op, dir, f, fa, out, oa, nfields, scale, add, st);
+  if (op.S == 5 && op.WPL == 1) return launch_t<5, 1>(op, dir, f, fa, out, oa, nfields, scale, add, st);
+  if (op.S == 5 && op.WPL == 2) return launch_t<5, 2>(op, dir, f, fa, out, oa, nfields, scale, add, st);
+  if (op.S == 5 && op.WPL == 4) return launch_t<5, 4>(op, dir, f, fa, out, oa, nfields, scale, add, st);
+  if (op.S == 9 && op.WPL == 1) return launch_t<9, 1>(op, dir, f, fa, out, oa, nfields, scale, add, st);
+  if (op.S == 9 && op.WPL == 2) return launch_t<9, 2>(op, dir, f, fa, out, oa, nfields, scale, add, st);
+  if (op.S == 9 && op.WPL == 4) return launch_t<9, 4>(op, dir, f, fa, out, oa, nfields, scale, add, st);
   return cudaErrorInvalidValue;
 }
 

@@ -238,6 +238,46 @@ module astr_b200
       real(c_double), value :: mach, gamma, cfl
       real(c_double) :: dt
     end function
+    integer(c_int) function astr_full_create(ctx, p, fs) bind(C, name="astr_full_create")
+      import :: c_int, c_ptr, astr_params
+      type(c_ptr), value :: ctx
+      type(astr_params) :: p
+      type(c_ptr) :: fs
+    end function
+    integer(c_int) function astr_full_destroy(fs) bind(C, name="astr_full_destroy")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: fs
+    end function
+    integer(c_int) function astr_full_upload(fs, q, shape, lb, where) bind(C, name="astr_full_upload")
+      import :: c_int, c_ptr, c_int64_t
+      type(c_ptr), value :: fs, q
+      integer(c_int64_t) :: shape(3), lb(3)
+      integer(c_int), value :: where
+    end function
+    integer(c_int) function astr_full_download(fs, q, shape, lb, where) bind(C, name="astr_full_download")
+      import :: c_int, c_ptr, c_int64_t
+      type(c_ptr), value :: fs, q
+      integer(c_int64_t) :: shape(3), lb(3)
+      integer(c_int), value :: where
+    end function
+    integer(c_int) function astr_full_step(fs, dt, nsteps) bind(C, name="astr_full_step")
+      import :: c_int, c_ptr, c_double
+      type(c_ptr), value :: fs
+      real(c_double), value :: dt
+      integer(c_int), value :: nsteps
+    end function
+    integer(c_int) function astr_full_rhs(fs, qrhs, shape, lb, where) bind(C, name="astr_full_rhs")
+      import :: c_int, c_ptr, c_int64_t
+      type(c_ptr), value :: fs, qrhs
+      integer(c_int64_t) :: shape(3), lb(3)
+      integer(c_int), value :: where
+    end function
+    integer(c_int) function astr_full_history(fs, rows, maxrows, nrows) bind(C, name="astr_full_history")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: fs, rows
+      integer(c_int), value :: maxrows
+      integer(c_int) :: nrows
+    end function
   end interface
 
 contains

@@ -28,6 +28,8 @@
  *                                                                              tgvsolver.F90:893-942,
  *                                                                              src/statistic.F90:993-1040
  *   astr_rk3_step_host      one call of rk3 with the state in host memory: upload, nsteps, download
+ *   astr_full_*             time_integration_rk / rhscal of the full solver     src/mainloop.F90:298-476,
+ *                                                                              src/solver.F90:184-283
  */
 #ifndef ASTR_B200_H
 #define ASTR_B200_H
@@ -176,6 +178,29 @@ int astr_step_vjp(astr_adjoint* adj, double dt, const double* lam_in, double* la
 /* out = scale * L^T g along dir for a periodic scheme L (device arrays of dims, nodes 0..N along dir). */
 int astr_scheme_apply_transpose(astr_ctx* ctx, astr_scheme* s, int dir, const double* g, const int64_t dims[3],
                                 double* out, int nfields, double scale);
+
+/* ---- full-solver time integration ------------------------------------------------ */
+/* The full solver's rk3 stage (time_integration_rk, src/mainloop.F90:298-476) on a periodic box
+ * of one rank with a uniform grid, on the reference's array layout (nodes -5..N+5 on every axis,
+ * halos stored): filterq first (src/comsolver.F90:514-632), qswap (src/parallel.F90:4877-5060:
+ * periodic halo copy, average of nodes 0 and N, primitives recomputed on the boundary planes and
+ * halos only, so interior primitives stay those of the unfiltered state), rhscal in its metric
+ * form (src/solver.F90:184-283, 2174-2874; src/comsolver.F90:244-497), the update of q*jacob
+ * (src/mainloop.F90:426-446) and updatefvar (src/fludyna.F90:191-242). p->sutherland is 110.3 in
+ * the full solver (src/solver.F90:121-122). History rows as astr_history (stage 1 of each step). */
+typedef struct astr_full astr_full;
+int astr_full_create(astr_ctx* ctx, const astr_params* p, astr_full** out);
+int astr_full_destroy(astr_full* fs);
+/* Conserved variables on nodes 0..N of the caller's Fortran array q(lb.., 1:5); the primitives are
+ * computed from them (updatefvar). */
+int astr_full_upload(astr_full* fs, const double* q, const int64_t shape[3], const int64_t lbound[3], int where);
+int astr_full_download(astr_full* fs, double* q, const int64_t shape[3], const int64_t lbound[3], int where);
+/* nsteps calls of time_integration_rk (rk3) with time step dt. */
+int astr_full_step(astr_full* fs, double dt, int nsteps);
+/* One stage's filterq + qswap + rhscal of the current state into qrhs (nodes 0..N); the state keeps
+ * the filtered, averaged q, as the stage leaves it before its update. */
+int astr_full_rhs(astr_full* fs, double* qrhs, const int64_t shape[3], const int64_t lbound[3], int where);
+int astr_full_history(astr_full* fs, double* rows, int maxrows, int* nrows);
 
 /* ---- no-allocation variant -------------------------------------------------------- */
 /* dt such that cflcal's CFL equals `cfl` for the conserved variables q (a DEVICE array,

@@ -59,6 +59,8 @@ def lib():
             "orc_tgv_set_dt": (None, [vp, d]),
             "orc_tgv_cfl_dt": (d, [vp, d]),
             "orc_tgv_steps": (None, [vp, i]),
+            "orc_tgv_steps_full": (None, [vp, i]),
+            "orc_tgv_rhs_full": (None, [vp, dp]),
             "orc_tgv_history": (i, [vp, dp, i]),
             "orc_tgv_history_compensated": (i, [vp, dp, i]),
             "orc_tgv_rhs": (None, [vp, dp]),
@@ -196,6 +198,18 @@ class TGVOracle:
 
     def steps(self, n: int):
         lib().orc_tgv_steps(self._h, n)
+
+    def steps_full(self, n: int):
+        """n steps of the full solver's time_integration_rk (src/mainloop.F90:392-476) on this
+        periodic box: filterq before rhscal at every stage, qswap's averaging of nodes 0 and N,
+        interior primitives of the unfiltered state, the metric form of rhscal, q*jacob update."""
+        lib().orc_tgv_steps_full(self._h, n)
+
+    def rhs_full(self) -> np.ndarray:
+        """One full-solver stage's qrhs (after its filterq and qswap, which change the state's q)."""
+        out = np.zeros(self.shape + (5,), order="F")
+        lib().orc_tgv_rhs_full(self._h, _dp(out))
+        return out
 
     def history(self, compensated: bool = False) -> np.ndarray:
         """Rows of (nstep, time, tke, enstrophy, dissipation), one per step (stacal). The sums run

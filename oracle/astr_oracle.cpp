@@ -836,6 +836,173 @@ struct TGV {
         }
   }
 
+  // ---------------------------------------------------------------- full-solver mode
+  // The stage of the full solver's time_integration_rk (src/mainloop.F90:392-476) on a periodic
+  // box of one rank with a uniform Cartesian grid: filterq first (src/comsolver.F90:514-632), then
+  // qswap (src/parallel.F90:4877-5060: per direction the periodic halo copy of q, the average of
+  // nodes 0 and N, and q2fvar on the planes -hm..0 and N..N+hm only), rhscal (src/solver.F90:
+  // 184-283) in its metric form -- gradcal (src/comsolver.F90:244-497) multiplies by dxi,
+  // convrsdcal6 (src/solver.F90:2174-2342) and diffrsdcal6 (src/solver.F90:2355-2874) carry the
+  // Jacobian -- then the update of q*jacob (src/mainloop.F90:438-446) and updatefvar
+  // (src/fludyna.F90:191-242). The primitive variables of the interior nodes used by rhscal are
+  // those of the last updatefvar, i.e. of the unfiltered state: qswap recomputes them only on the
+  // boundary planes and halos. The metrics of a uniform grid are taken in closed form: dxi =
+  // diag(1/dx, 1/dy, 1/dz), jacob = dx*dy*dz (src/geom.F90:350-385 computes them numerically from
+  // the grid; for a uniform grid those equal these to rounding). The off-diagonal metric terms
+  // are zero and add exactly zero, so they are left out.
+  double jac() const { return dx * dy * dz; }
+
+  // qswap on one rank with every direction periodic (parallel.F90:4877-5060)
+  void fs_qswap() {
+    const int dims[3] = {im, jm, km};
+    for (int dir = 0; dir < 3; ++dir) {
+      bchomovec(q, 5, dir + 1);
+      const int dim = dims[dir];
+      const int o1 = (dir == 0) ? 1 : 0, o2 = (dir == 2) ? 1 : 2;
+#pragma omp parallel for collapse(2)
+      for (int b = 0; b <= dims[o2]; ++b)
+        for (int a = 0; a <= dims[o1]; ++a) {
+          int p0[3], pn[3];
+          p0[o1] = pn[o1] = a; p0[o2] = pn[o2] = b; p0[dir] = 0; pn[dir] = dim;
+          for (int m = 0; m < 5; ++m) {
+            q(p0[0], p0[1], p0[2], m) = 0.5 * (q(p0[0], p0[1], p0[2], m) + q(pn[0], pn[1], pn[2], m));
+            q(pn[0], pn[1], pn[2], m) = q(p0[0], p0[1], p0[2], m);
+          }
+          // q2fvar on the planes -hm..0 and dim..dim+hm of this line
+          for (int t = -HM; t <= dim + HM; ++t) {
+            if (t > 0 && t < dim) continue;
+            int p[3] = {p0[0], p0[1], p0[2]};
+            p[dir] = t;
+            double qq[5], u[3], r, pr, tt;
+            for (int m = 0; m < 5; ++m) qq[m] = q(p[0], p[1], p[2], m);
+            q2fvar(qq, r, u, pr, tt);
+            rho(p[0], p[1], p[2]) = r; prs(p[0], p[1], p[2]) = pr; tmp(p[0], p[1], p[2]) = tt;
+            for (int c = 0; c < 3; ++c) vel(p[0], p[1], p[2], c) = u[c];
+          }
+        }
+    }
+  }
+
+  // gradcal in the metric form: dvel(:,:,:,n,d) = df * dxi(d,d)
+  void fs_gradcal() {
+    for (int dir = 0; dir < 3; ++dir) {
+      const double dxi = 1.0 / dstep(dir);
+      line_loop(dir, 4,
+                [&](int n, int i, int j, int k) { return n < 3 ? vel(i, j, k, n) : tmp(i, j, k); },
+                [&](int n, int i, int j, int k, double v) {
+                  if (n < 3) dvel(i, j, k, n + 3 * dir) = v * dxi;
+                  else dtmp(i, j, k, dir) = v * dxi;
+                });
+    }
+  }
+
+  // convrsdcal6: fcs = jacob * (q uu + dxi p e_d), uu = dxi(d,d) u_d; qrhs += D(fcs)
+  void fs_convection() {
+    const double jb = jac();
+    for (int dir = 0; dir < 3; ++dir) {
+      const double dxi = 1.0 / dstep(dir);
+      line_loop(dir, 5,
+                [&](int n, int i, int j, int k) {
+                  const double uu = dxi * vel(i, j, k, dir);
+                  if (n == 0) return jb * q(i, j, k, 0) * uu;
+                  if (n == 4) return jb * (q(i, j, k, 4) + prs(i, j, k)) * uu;
+                  if (n == dir + 1) return jb * (q(i, j, k, n) * uu + dxi * prs(i, j, k));
+                  return jb * (q(i, j, k, n) * uu);
+                },
+                [&](int n, int i, int j, int k, double v) { qrhs(i, j, k, n) = qrhs(i, j, k, n) + v; });
+    }
+  }
+
+  // diffrsdcal6: sigma and qflux as in the miniapp, then ff = (sigma . dxi(d,:)) * jacob
+  void fs_diffusion() {
+#pragma omp parallel for collapse(2)
+    for (int k = 0; k <= km; ++k)
+      for (int j = 0; j <= jm; ++j)
+        for (int i = 0; i <= im; ++i) {
+          double s11 = dvel(i, j, k, 0);
+          double s12 = 0.5 * (dvel(i, j, k, 3) + dvel(i, j, k, 1));
+          double s13 = 0.5 * (dvel(i, j, k, 6) + dvel(i, j, k, 2));
+          double s22 = dvel(i, j, k, 4);
+          double s23 = 0.5 * (dvel(i, j, k, 7) + dvel(i, j, k, 5));
+          double s33 = dvel(i, j, k, 8);
+          double skk = num1d3 * (s11 + s22 + s33);
+          double miu = miucal(tmp(i, j, k)) / reynolds;
+          double miu2 = 2.0 * miu;
+          double hcc = (miu / prandtl) / const5;
+          sigma(i, j, k, 0) = miu2 * (s11 - skk);
+          sigma(i, j, k, 1) = miu2 * s12;
+          sigma(i, j, k, 2) = miu2 * s13;
+          sigma(i, j, k, 3) = miu2 * (s22 - skk);
+          sigma(i, j, k, 4) = miu2 * s23;
+          sigma(i, j, k, 5) = miu2 * (s33 - skk);
+          qflux(i, j, k, 0) = hcc * dtmp(i, j, k, 0) + sigma(i, j, k, 0) * vel(i, j, k, 0) +
+                              sigma(i, j, k, 1) * vel(i, j, k, 1) + sigma(i, j, k, 2) * vel(i, j, k, 2);
+          qflux(i, j, k, 1) = hcc * dtmp(i, j, k, 1) + sigma(i, j, k, 1) * vel(i, j, k, 0) +
+                              sigma(i, j, k, 3) * vel(i, j, k, 1) + sigma(i, j, k, 4) * vel(i, j, k, 2);
+          qflux(i, j, k, 2) = hcc * dtmp(i, j, k, 2) + sigma(i, j, k, 2) * vel(i, j, k, 0) +
+                              sigma(i, j, k, 4) * vel(i, j, k, 1) + sigma(i, j, k, 5) * vel(i, j, k, 2);
+        }
+    bchomovec(sigma, 6, 0);
+    bchomovec(qflux, 3, 0);
+    static const int sg[3][3] = {{0, 1, 2}, {1, 3, 4}, {2, 4, 5}};
+    const double jb = jac();
+    for (int dir = 0; dir < 3; ++dir) {
+      const double dxi = 1.0 / dstep(dir);
+      line_loop(dir, 4,
+                [&](int n, int i, int j, int k) {
+                  return (n < 3 ? sigma(i, j, k, sg[dir][n]) : qflux(i, j, k, dir)) * dxi * jb;
+                },
+                [&](int n, int i, int j, int k, double v) { qrhs(i, j, k, n + 1) = qrhs(i, j, k, n + 1) + v; });
+    }
+  }
+
+  void fs_rhscal() {
+    std::fill(qrhs.v.begin(), qrhs.v.end(), 0.0);
+    fs_gradcal();
+    fs_convection();
+    for (double& v : qrhs.v) v = -v;
+    fs_diffusion();
+  }
+
+  // One step of time_integration_rk (rk3), mainloop.F90:392-476; history row at stage 1 after
+  // gradcal, as in the miniapp.
+  void rk3_full() {
+    static const double rkcoe[3][3] = {{1.0, 0.0, 1.0}, {0.75, 0.25, 0.25}, {num1d3, num2d3, num2d3}};
+    const double jb = jac();
+    for (int rk = 0; rk < 3; ++rk) {
+      if (lfilter) filterq();
+      fs_qswap();
+      fs_rhscal();
+      if (rk == 0) {
+        stacal();
+#pragma omp parallel for collapse(2)
+        for (int k = 0; k <= km; ++k)
+          for (int j = 0; j <= jm; ++j)
+            for (int i = 0; i <= im; ++i)
+              for (int m = 0; m < 5; ++m) qsave(i, j, k, m) = q(i, j, k, m) * jb;
+      }
+      const double c1 = rkcoe[rk][0], c2 = rkcoe[rk][1], c3 = rkcoe[rk][2];
+#pragma omp parallel for collapse(2)
+      for (int k = 0; k <= km; ++k)
+        for (int j = 0; j <= jm; ++j)
+          for (int i = 0; i <= im; ++i)
+            for (int m = 0; m < 5; ++m) {
+              double v = c1 * qsave(i, j, k, m) + c2 * q(i, j, k, m) * jb + c3 * qrhs(i, j, k, m) * deltat;
+              q(i, j, k, m) = v / jb;
+            }
+      update_prims();
+    }
+    nstep += 1;
+    time = time + deltat;
+  }
+
+  // One rhscal of the full solver on the current state (filterq and qswap first, as a stage does)
+  void rhs_full() {
+    if (lfilter) filterq();
+    fs_qswap();
+    fs_rhscal();
+  }
+
   // rk3, tgvsolver.F90:994-1082, and the step counter of steploop (:944-960)
   void rk3() {
     static const double rkcoe[3][3] = {{1.0, 0.0, 1.0}, {0.75, 0.25, 0.25}, {num1d3, num2d3, num2d3}};
@@ -947,6 +1114,19 @@ void orc_tgv_get_q(void* h, double* q) { static_cast<TGV*>(h)->get_q(q); }
 void orc_tgv_set_dt(void* h, double dt) { static_cast<TGV*>(h)->deltat = dt; }
 double orc_tgv_cfl_dt(void* h, double cfl) { return static_cast<TGV*>(h)->cfl_dt(cfl); }
 void orc_tgv_steps(void* h, int n) { TGV* t = static_cast<TGV*>(h); for (int s = 0; s < n; ++s) t->rk3(); }
+// Full-solver mode (time_integration_rk of the full solver on a periodic box, see rk3_full).
+void orc_tgv_steps_full(void* h, int n) { TGV* t = static_cast<TGV*>(h); for (int s = 0; s < n; ++s) t->rk3_full(); }
+// One full-solver rhscal (after the stage's filterq and qswap) into qrhs on nodes 0..N; the state
+// keeps the filtered, averaged q.
+void orc_tgv_rhs_full(void* h, double* out) {
+  TGV* t = static_cast<TGV*>(h);
+  t->rhs_full();
+  const int64_t n0 = t->im + 1, n1 = t->jm + 1, n2 = t->km + 1, nn = n0 * n1 * n2;
+  for (int m = 0; m < 5; ++m)
+    for (int k = 0; k <= t->km; ++k)
+      for (int j = 0; j <= t->jm; ++j)
+        for (int i = 0; i <= t->im; ++i) out[m * nn + ((int64_t)k * n1 + j) * n0 + i] = t->qrhs(i, j, k, m);
+}
 int orc_tgv_history(void* h, double* out, int maxrows) {
   TGV* t = static_cast<TGV*>(h);
   int rows = (int)(t->hist.size() / 5);
