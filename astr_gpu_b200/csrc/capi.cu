@@ -356,6 +356,7 @@ int check_err(astr_state* st) {
   int h = 0;
   CK(cudaMemcpyAsync(&h, st->err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
+  if (h & 2) return fail(ctx, ASTR_ERR_CUDA, "a bulk copy into a tile did not complete within its wait limit");
   if (h) return fail(ctx, ASTR_ERR_STATE, "invalid state: non-finite or non-positive density (crashcheck)");
   return ASTR_OK;
 }

@@ -47,7 +47,8 @@ struct PassArgs {
   double c1, c2, c3, dt;    // SSP-RK3 stage coefficients (mainloop.F90:350-360)
   double* partials;         // pass C at the first stage: per-CTA (tke, enstrophy, dissipation)
   double* DC;               // pass C, optional: its 4 gradients along C are also stored here
-  int* err;                 // device error word: bit 0 = non-finite or non-positive density
+  int* err;                 // device error word: bit 0 = non-finite or non-positive density,
+                            // bit 1 = a bulk copy wait ran out of polls
 };
 
 cudaError_t launch_pass(int pass, const PassArgs& a, int S, int WPL, cudaStream_t st);

@@ -144,6 +144,74 @@ __device__ __forceinline__ void load_tile(const TileCtx<DIR, WPL, LW>& c, double
   for (; n <= dim + HT; n += nst) cp_async8(trow + n, src + (int64_t)(n - dim) * sd);
 }
 
+// ---- bulk copies completing on an mbarrier (the copy engine moves whole contiguous rows)
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, unsigned bytes) {
+  asm volatile("{\n .reg .b64 st;\n mbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n}\n" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+// Poll the barrier's phase `parity` at most `limit` times; false when it did not complete.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity, int limit) {
+  for (int it = 0; it < limit; ++it) {
+    unsigned done;
+    asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+                 : "=r"(done)
+                 : "r"(smem_u32(bar)), "r"(parity)
+                 : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+constexpr int kBarrierPolls = 1 << 22;   // bounded wait (far beyond any copy's duration)
+
+// Stage `nf` fields of the x lines of a tile with one bulk copy per line and field (nodes 0..dim
+// are contiguous: one row of the padded box, 16-byte aligned), completing on one mbarrier; then
+// the periodic halos -HT..-1 and dim+1..dim+HT are filled from the staged rows in shared memory.
+// Needs an even tile pitch (16-byte aligned tile rows). A wait that does not complete sets bit 1
+// of the error word; the kernel then runs to its end on whatever the tile holds.
+template <int WPL>
+__device__ __forceinline__ void stage_x_bulk(const TileCtx<0, WPL>& c, double* T, int tsz, const double* fld,
+                                             int64_t fs, int nf, const PassArgs& a, int bx, int by, uint64_t* bar) {
+  const int dim = c.dim;
+  const unsigned bytes = (unsigned)(((dim + 1) * 8 + 15) & ~15);   // within the padded row
+  if (threadIdx.x == 0) mbar_init(bar, 1);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int nvalid = 0;
+    for (int l = 0; l < c.TI; ++l) nvalid += ((int64_t)bx * c.TI + l < a.g.N[1] + 1) ? 1 : 0;
+    mbar_arrive_expect_tx(bar, bytes * (unsigned)(nf * nvalid));
+    for (int m = 0; m < nf; ++m)
+      for (int l = 0; l < nvalid; ++l) {
+        const int64_t row = ((int64_t)bx * c.TI + l) * a.g.st[1] + (int64_t)by * a.g.st[2];
+        bulk_g2s(T + m * tsz + l * c.LP + HT, fld + m * fs + row, bytes, bar);
+      }
+  }
+  if (!c.svalid) {
+    for (int m = 0; m < nf; ++m) c.for_nodes(-HT, dim + HT, [&](int o, int) { T[m * tsz + o] = 1.0; });
+  }
+  if (!mbar_wait(bar, 0, kBarrierPolls) && threadIdx.x == 0) atomicOr(a.err, 2);
+  if (c.svalid) {
+    for (int m = 0; m < nf; ++m) {
+      double* row = T + m * tsz + c.sl * c.LP + HT;
+      for (int k = 1 + c.sn0; k <= HT; k += c.nst) {
+        row[-k] = row[dim - k];
+        row[dim + k] = row[k];
+      }
+    }
+  }
+}
+
 // Write a lane's solution rows (nodes 0..dim) into a tile line, optionally with the periodic
 // halo images of those nodes.
 template <int S>
@@ -462,8 +530,13 @@ __device__ __forceinline__ void k_pass_c_body(const PassArgs& a, int bx, int by)
     const unsigned bytes = (unsigned)(((c.dim + 1) * 8 + 15) & ~15);   // within the padded row
     asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
   }
-  for (int m = 0; m < 5; ++m) load_tile(c, T + m * tsz, a.q + m * fs);
-  cp_async_wait_all();
+  __shared__ uint64_t bar;
+  if (DIR == 0 && (c.LP & 1) == 0) {
+    stage_x_bulk(c, T, tsz, a.q, fs, 5, a, bx, by, &bar);
+  } else {
+    for (int m = 0; m < 5; ++m) load_tile(c, T + m * tsz, a.q + m * fs);
+    cp_async_wait_all();
+  }
   __syncthreads();
   const int dim = c.dim;
   to_prims(c, T, tsz, a.th);
