@@ -7,6 +7,7 @@ compact filter alpha_f = 0.49 after every stage, dt fixed from CFL 0.5 at t = 0)
     python bench.py --workload ensemble [--gpus N] [--steps K]   # 48 uneven boxes, batched
     python bench.py --workload adjoint                          # 128^3 gradient, adjoint:forward
     python bench.py --workload gradient                         # 256^3 line operators, GB/s
+    python bench.py --workload full                             # full-solver time integration
 
 One JSON line on rank 0. `value` = grid-point RK3 updates/s over all ranks (each rank advances
 its own 512^3 box: replicas, weak scaling), device-timed with CUDA events on the library's stream,
@@ -706,6 +707,44 @@ def run_gradient(args, ws, rank, local):
         pg.destroy_process_group()
 
 
+FULL_METRIC = "full-solver grid-point RK3 updates/s FP64 (time_integration_rk, periodic TGV)"
+
+
+def run_full(args, ws, rank, local):
+    """The full solver's time integration (astr_full_*, on the reference's halo-extended arrays,
+    one kernel per operation of the reference) on the Taylor-Green box of --full-size: device time
+    of --steps steps after --warmup. Every rank runs its own replica (no collective)."""
+    import torch
+    import astr_gpu_b200 as ag
+    from astr_gpu_b200.fields import tgv_q
+
+    torch.cuda.set_device(local)
+    n = args.full_size
+    stream = torch.cuda.Stream(device=local)
+    ctx = ag.Context(local, stream=stream)
+    s = ag.FullSolver(ctx, n, params=ag.FlowParams(sutherland=110.3, beta_bound=0.98))
+    s.set_q(tgv_q(n, 0.1))
+    dt = 1e-3
+    s.step(dt, args.warmup)
+    ctx.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        s.step(dt, args.steps)
+        e1.record(stream)
+        e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    if rank == 0:
+        line = {"metric": FULL_METRIC, "value": ws * n ** 3 * args.steps / (ms * 1e-3), "unit": UNIT, "n_gpus": ws,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (Taylor-Green initial field)",
+                "config": {"workload": f"full-solver mode, TGV {n}^3 (filter first, qswap averaging, metric form), "
+                                       f"dt {dt}", "grid": n},
+                "gpu_launches": None, "clocks": clk.summary()}
+        print(json.dumps(line), flush=True)
+    s.close()
+
+
 def run_profile(args, local):
     """The workload for an ncu capture: `--steps` eager RK3 steps of a TGV box (no graph, no
     timing, no JSON line), with the pass launch shapes pinned by `--shapes`."""
@@ -737,7 +776,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", default="tgv", choices=["tgv", "ensemble", "adjoint", "gradient"])
+    ap.add_argument("--workload", default="tgv", choices=["tgv", "ensemble", "adjoint", "gradient", "full"])
+    ap.add_argument("--full-size", type=int, default=256)
     ap.add_argument("--grad-size", type=int, default=256)
     ap.add_argument("--adj-size", type=int, default=128)
     ap.add_argument("--adj-steps", type=int, default=200)
@@ -760,6 +800,8 @@ def main():
         run_adjoint(args, ws, rank, local)
     elif args.workload == "gradient":
         run_gradient(args, ws, rank, local)
+    elif args.workload == "full":
+        run_full(args, ws, rank, local)
     else:
         run_ours(args, ws, rank, local)
 
