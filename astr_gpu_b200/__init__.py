@@ -180,6 +180,13 @@ class FlowParams:
     beta_halo: float = 1.11
     beta_bound: float = 1.09
     filter_on: bool = True
+    ntype: tuple = (3, 3, 3)   # per direction: 3 periodic; 1, 2, 4 physical ends (FullSolver only)
+    twall: float = 1.0         # isothermal no-slip walls at the physical ends (bctype 41)
+
+    def c_params(self, im, jm, km):
+        return AstrParams(im, jm, km, self.mach, self.reynolds, self.prandtl, self.gamma, self.ref_tem,
+                          self.sutherland, self.alfa_filter, self.beta_halo, self.beta_bound, int(self.filter_on),
+                          (ctypes.c_int * 3)(*[int(t) for t in self.ntype]), float(self.twall))
 
 
 class TGVSolver:
@@ -192,8 +199,7 @@ class TGVSolver:
         self.im, self.jm, self.km = im, jm or im, km or im
         p = params or FlowParams()
         self.params = p
-        cp = AstrParams(self.im, self.jm, self.km, p.mach, p.reynolds, p.prandtl, p.gamma, p.ref_tem, p.sutherland,
-                        p.alfa_filter, p.beta_halo, p.beta_bound, int(p.filter_on))
+        cp = p.c_params(self.im, self.jm, self.km)
         h = ctypes.c_void_p()
         ctx.check(ctx.L.astr_state_create(ctx._h, ctypes.byref(cp), ctypes.byref(h)))
         self._h = h
@@ -308,8 +314,7 @@ class FullSolver:
         self.im, self.jm, self.km = im, jm or im, km or im
         p = params or FlowParams(sutherland=110.3)
         self.params = p
-        cp = AstrParams(self.im, self.jm, self.km, p.mach, p.reynolds, p.prandtl, p.gamma, p.ref_tem, p.sutherland,
-                        p.alfa_filter, p.beta_halo, p.beta_bound, int(p.filter_on))
+        cp = p.c_params(self.im, self.jm, self.km)
         h = ctypes.c_void_p()
         ctx.check(ctx.L.astr_full_create(ctx._h, ctypes.byref(cp), ctypes.byref(h)))
         self._h = h

@@ -625,6 +625,9 @@ int astr_state_create(astr_ctx* ctx, const astr_params* p, astr_state** out) {
   const int N[3] = {p->im, p->jm, p->km};
   for (int d = 0; d < 3; ++d)
     if (N[d] < 16) return fail(ctx, ASTR_ERR_ARG, "each dimension must be >= 16");
+  for (int d = 0; d < 3; ++d)
+    if (p->ntype[d] != 0 && p->ntype[d] != 3)
+      return fail(ctx, ASTR_ERR_UNSUPPORTED, "the miniapp step is periodic: non-periodic boxes run in the full-solver mode (astr_full_create)");
   astr_state* st = new astr_state();
   st->ctx = ctx;
   st->p = *p;

@@ -1,4 +1,5 @@
-// The full solver's time integration on a periodic box, on the reference's own array layout.
+// The full solver's time integration on a box of one rank, on the reference's own array layout:
+// periodic directions, or physical ends with the compact closures and isothermal no-slip walls.
 //
 // ASTR's production stage (time_integration_rk with rk3, src/mainloop.F90:392-476) differs from
 // the miniapp's (tgvsolver.F90:994-1082) in four ways that change results: the filter runs
@@ -38,6 +39,7 @@ constexpr int HMW = 5;   // halo width of the reference's arrays (commvar.F90:19
 
 struct FsGeo {
   int N[3];
+  int ntype[3];    // 3 periodic; 1, 2, 4 physical ends
   int64_t s[3];    // element strides of i, j, k (s[0] = 1)
   int64_t fs;      // elements per field
   double rd[3];    // dxi: 1/dx, 1/dy, 1/dz
@@ -50,6 +52,7 @@ struct FsGeo {
 
 struct FsThermo {
   double const2, const5, const6, reynolds, prandtl, tc, tc1;
+  double twall;    // isothermal no-slip walls at the physical ends
 };
 
 // Node (i, j, k) of the flat index p over the box [lo[a], hi[a]] on each axis.
@@ -138,6 +141,30 @@ __global__ void k_fs_qswap(double* q, double* rho, double* vel, double* prs, dou
       fs_q2fvar(th, q[o], q[g.fs + o], q[2 * g.fs + o], q[3 * g.fs + o], q[4 * g.fs + o], r, u, v, w, pr, tt);
       rho[o] = r; vel[o] = u; vel[g.fs + o] = v; vel[2 * g.fs + o] = w; prs[o] = pr; tmp[o] = tt;
     }
+  }
+}
+
+// boucon with isothermal no-slip walls (bctype 41, noslip, src/bc.F90:6281-6595) on the end
+// `side` (0: node 0, 1: node N) along dir: u = v = w = 0, T = twall, p = (4 p_1 - p_2)/3 from the
+// two nodes next to the wall, rho = p/T gamma M^2 (thermal), q by fvar2q.
+__global__ void k_fs_noslip(double* q, double* rho, double* vel, double* prs, double* tmp, int dir, int side, FsGeo g,
+                            FsThermo th) {
+  const int N = g.N[dir];
+  const Box3 b = box_line(g, dir, side ? N : 0, side ? N : 0);
+  const int64_t sd = g.s[dir] * (side ? -1 : 1);   // towards the interior
+  GRID_STRIDE(p, b.size()) {
+    int i, j, k;
+    b.node(p, i, j, k);
+    const int64_t o = g.at(i, j, k);
+    const double pe = (1.0 / 3.0) * (4.0 * prs[o + sd] - prs[o + 2 * sd]);
+    vel[o] = 0.0; vel[g.fs + o] = 0.0; vel[2 * g.fs + o] = 0.0;
+    prs[o] = pe;
+    tmp[o] = th.twall;
+    const double r = pe / th.twall * th.const2;
+    rho[o] = r;
+    q[o] = r;
+    q[g.fs + o] = r * 0.0; q[2 * g.fs + o] = r * 0.0; q[3 * g.fs + o] = r * 0.0;
+    q[4 * g.fs + o] = pe * th.const6 + r * 0.0;   // fvar2q with |u|^2 = 0
   }
 }
 
@@ -395,13 +422,23 @@ cudaError_t fs_stage_rhs(astr_full* fs, bool diag) {
   const int64_t nn = nodes(fs);
   if (fs->p.filter_on) {
     for (int d = 0; d < 3; ++d) {
-      if ((e = fs_halo(fs, fs->q, 5, d)) != cudaSuccess) return e;
+      if (g.ntype[d] == 3 && (e = fs_halo(fs, fs->q, 5, d)) != cudaSuccess) return e;
       if ((e = line_op(fs, fs->df[d], d, fs->q, fs->qt, 5, 1.0, 0)) != cudaSuccess) return e;
       std::swap(fs->q, fs->qt);
     }
   }
   if ((e = cudaMemsetAsync(fs->qrhs, 0, 5 * (size_t)g.fs * sizeof(double), st)) != cudaSuccess) return e;
+  // boucon: no-slip walls at the physical ends, in boucon's order (i-min, i-max, j-min, ...)
+  for (int d = 0; d < 3; ++d)
+    for (int side = 0; side < 2; ++side) {
+      const int t = g.ntype[d];
+      if (!(side == 0 ? (t == 1 || t == 4) : (t == 2 || t == 4))) continue;
+      const int64_t nw = nn / (g.N[d] + 1);
+      k_fs_noslip<<<blocks_for(nw), 256, 0, st>>>(fs->q, fs->rho, fs->vel, fs->prs, fs->tmp, d, side, g, fs->th);
+      if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
   for (int d = 0; d < 3; ++d) {
+    if (g.ntype[d] != 3) continue;   // one rank, non-periodic: nothing to exchange
     const int64_t nl = nn / (g.N[d] + 1);
     k_fs_qswap<<<blocks_for(nl), 256, 0, st>>>(fs->q, fs->rho, fs->vel, fs->prs, fs->tmp, d, g, fs->th);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
@@ -424,6 +461,7 @@ cudaError_t fs_stage_rhs(astr_full* fs, bool diag) {
   k_fs_stress<<<blocks_for(nn), 256, 0, st>>>(fs->sigma, fs->qflux, fs->dvel, fs->dtmp, fs->vel, fs->tmp, g, fs->th);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   for (int d = 0; d < 3; ++d) {
+    if (g.ntype[d] != 3) continue;
     if ((e = fs_halo(fs, fs->sigma, 6, d)) != cudaSuccess) return e;
     if ((e = fs_halo(fs, fs->qflux, 3, d)) != cudaSuccess) return e;
   }
@@ -498,7 +536,15 @@ int astr_full_create(astr_ctx* ctx, const astr_params* p, astr_full** out) {
   fs->p = *p;
   FsGeo& g = fs->g;
   const double pi = 4.0 * std::atan(1.0);
-  for (int d = 0; d < 3; ++d) g.N[d] = N[d];
+  for (int d = 0; d < 3; ++d) {
+    g.N[d] = N[d];
+    g.ntype[d] = p->ntype[d] == 0 ? 3 : p->ntype[d];
+    if (g.ntype[d] < 1 || g.ntype[d] > 4 || (g.ntype[d] != 3 && !(p->twall > 0.0))) {
+      delete fs;
+      astr_ctx_set_error(ctx, "ntype must be 0 or 3 (periodic), 1, 2 or 4, and a wall needs twall > 0");
+      return ASTR_ERR_ARG;
+    }
+  }
   g.s[0] = 1;
   g.s[1] = N[0] + 1 + 2 * HMW;
   g.s[2] = g.s[1] * (N[1] + 1 + 2 * HMW);
@@ -514,9 +560,10 @@ int astr_full_create(astr_ctx* ctx, const astr_params* p, astr_full** out) {
   fs->th.prandtl = p->prandtl;
   fs->th.tc = p->sutherland / p->ref_tem;
   fs->th.tc1 = 1.0 + fs->th.tc;
+  fs->th.twall = p->twall;
   for (int d = 0; d < 3; ++d) {
-    build_fd_op(fs->hd[d], "643c", 3, N[d]);
-    build_filter_op(fs->hf[d], 3, N[d], p->alfa_filter, p->beta_halo, p->beta_bound, false);
+    build_fd_op(fs->hd[d], "643c", g.ntype[d], N[d]);
+    build_filter_op(fs->hf[d], g.ntype[d], N[d], p->alfa_filter, p->beta_halo, p->beta_bound, false);
     const Layout L = pick_layout(fs->hf[d].nsys());
     if (L.S == 0) { delete fs; astr_ctx_set_error(ctx, "dimension too large (max 1145)"); return ASTR_ERR_UNSUPPORTED; }
     if (make_devop(fs->hd[d], pick_layout(fs->hd[d].nsys()), fs->dd[d]) != cudaSuccess ||

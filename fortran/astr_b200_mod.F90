@@ -15,6 +15,8 @@ module astr_b200
     real(c_double) :: mach, reynolds, prandtl, gamma, ref_tem, sutherland
     real(c_double) :: alfa_filter, beta_halo, beta_bound
     integer(c_int) :: filter_on
+    integer(c_int) :: ntype(3)
+    real(c_double) :: twall
   end type astr_params
 
   interface

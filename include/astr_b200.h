@@ -64,6 +64,9 @@ typedef struct {
   double beta_halo;        /* 1.11 */
   double beta_bound;       /* 1.09 (miniapp) or 0.98 (full solver) */
   int filter_on;           /* apply filterq after every RK stage */
+  int ntype[3];            /* per direction: 0 or 3 periodic; 1, 2, 4 physical ends (full-solver
+                              mode only: fd_scheme_initiate's ntype, compact boundary closures) */
+  double twall;            /* temperature of the isothermal no-slip walls at physical ends (bctype 41) */
 } astr_params;
 
 /* ---- context ------------------------------------------------------------------------ */
@@ -187,7 +190,11 @@ int astr_scheme_apply_transpose(astr_ctx* ctx, astr_scheme* s, int dir, const do
  * halos only, so interior primitives stay those of the unfiltered state), rhscal in its metric
  * form (src/solver.F90:184-283, 2174-2874; src/comsolver.F90:244-497), the update of q*jacob
  * (src/mainloop.F90:426-446) and updatefvar (src/fludyna.F90:191-242). p->sutherland is 110.3 in
- * the full solver (src/solver.F90:121-122). History rows as astr_history (stage 1 of each step). */
+ * the full solver (src/solver.F90:121-122). History rows as astr_history (stage 1 of each step).
+ * Directions with p->ntype 1, 2 or 4 take the compact boundary closures (derivative.F90:230-281,
+ * filter.F90:176-249, with p->beta_bound) and isothermal no-slip walls at their physical ends
+ * (boucon's noslip, src/bc.F90:6281-6595, applied after filterq at every stage). The miniapp step
+ * (astr_state_*) is periodic only and rejects other ntypes. */
 typedef struct astr_full astr_full;
 int astr_full_create(astr_ctx* ctx, const astr_params* p, astr_full** out);
 int astr_full_destroy(astr_full* fs);

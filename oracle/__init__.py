@@ -60,6 +60,7 @@ def lib():
             "orc_tgv_cfl_dt": (d, [vp, d]),
             "orc_tgv_steps": (None, [vp, i]),
             "orc_tgv_steps_full": (None, [vp, i]),
+            "orc_tgv_set_boundaries": (None, [vp, i, i, i, d]),
             "orc_tgv_rhs_full": (None, [vp, dp]),
             "orc_tgv_history": (i, [vp, dp, i]),
             "orc_tgv_history_compensated": (i, [vp, dp, i]),
@@ -155,6 +156,8 @@ class FlowParams:
     beta_halo: float = 1.11
     beta_bound: float = 1.09      # tgvsolver.F90:253
     filter_on: bool = True
+    ntype: tuple = (3, 3, 3)      # per direction: 3 periodic; 1, 2, 4 physical ends (full-solver mode)
+    twall: float = 1.0            # isothermal no-slip walls at the physical ends (bctype 41)
 
 
 class TGVOracle:
@@ -167,6 +170,8 @@ class TGVOracle:
         self._h = lib().orc_tgv_create(self.im, self.jm, self.km, p.mach, p.reynolds, p.prandtl, p.gamma,
                                        p.ref_tem, p.sutherland, p.alfa_filter, p.beta_halo, p.beta_bound,
                                        int(p.filter_on))
+        if tuple(p.ntype) != (3, 3, 3):
+            lib().orc_tgv_set_boundaries(self._h, *[int(t) for t in p.ntype], float(p.twall))
 
     def __del__(self):
         if getattr(self, "_h", None) and _lib is not None:

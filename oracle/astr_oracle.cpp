@@ -453,6 +453,12 @@ struct TGV {
   int nstep;
   bool lfilter;
   Scheme fds[3], flt[3];
+  // boundary type per direction (fd_scheme_initiate's ntype: 3 periodic, 1/2/4 physical ends) and
+  // the temperature of the isothermal no-slip walls at the physical ends (bctype 41)
+  int ntype[3] = {3, 3, 3};
+  double twall = 1.0;
+  double alfa_f = 0.49, beta_h = 1.11, beta_b = 0.98;
+  bool periodic(int d) const { return ntype[d] == 3; }
   Field3 q, rho, prs, tmp, vel, qrhs, dvel, dtmp, sigma, qflux, qsave;
   std::vector<double> hist;   // rows of (nstep, time, tke, enst, diss)
   std::vector<double> hist_c; // the same rows with compensated sums
@@ -464,7 +470,9 @@ struct TGV {
     mach = mach_; reynolds = re_; prandtl = pr_; gamma = gam_; ref_tem = ref_tem_; suth = suth_;
     lfilter = filter_on != 0;
     const int dims[3] = {im, jm, km};
+    alfa_f = alfa_filter; beta_h = beta_halo; beta_b = beta_bound;
     for (int d = 0; d < 3; ++d) {
+      ntype[d] = 3;
       fd_scheme_initiate(fds[d], "643c", 3, dims[d]);
       compact_filter_initiate(flt[d], 3, dims[d], alfa_filter, false);
       filter_coefficient_cal(flt[d], alfa_filter, beta_halo, beta_bound);
@@ -732,7 +740,7 @@ struct TGV {
   void filterq() {
     const int dims[3] = {im, jm, km};
     for (int dir = 0; dir < 3; ++dir) {
-      bchomovec(q, 5, dir + 1);
+      if (periodic(dir)) bchomovec(q, 5, dir + 1);
       const int dim = dims[dir];
       const int o1 = (dir == 0) ? 1 : 0, o2 = (dir == 2) ? 1 : 2;
 #pragma omp parallel
@@ -856,6 +864,7 @@ struct TGV {
   void fs_qswap() {
     const int dims[3] = {im, jm, km};
     for (int dir = 0; dir < 3; ++dir) {
+      if (!periodic(dir)) continue;   // one rank, non-periodic: nothing to exchange
       bchomovec(q, 5, dir + 1);
       const int dim = dims[dir];
       const int o1 = (dir == 0) ? 1 : 0, o2 = (dir == 2) ? 1 : 2;
@@ -942,8 +951,11 @@ struct TGV {
           qflux(i, j, k, 2) = hcc * dtmp(i, j, k, 2) + sigma(i, j, k, 2) * vel(i, j, k, 0) +
                               sigma(i, j, k, 4) * vel(i, j, k, 1) + sigma(i, j, k, 5) * vel(i, j, k, 2);
         }
-    bchomovec(sigma, 6, 0);
-    bchomovec(qflux, 3, 0);
+    for (int d = 0; d < 3; ++d)
+      if (periodic(d)) {
+        bchomovec(sigma, 6, d + 1);
+        bchomovec(qflux, 3, d + 1);
+      }
     static const int sg[3][3] = {{0, 1, 2}, {1, 3, 4}, {2, 4, 5}};
     const double jb = jac();
     for (int dir = 0; dir < 3; ++dir) {
@@ -964,6 +976,38 @@ struct TGV {
     fs_diffusion();
   }
 
+  // boucon with isothermal no-slip walls (bctype 41, noslip, src/bc.F90:6281-6595) at every
+  // physical end: u = v = w = 0, T = twall, the pressure extrapolated from the two nodes next to
+  // the wall, p_w = (4 p_1 - p_2)/3, rho = p/T gamma M^2 (thermal), q by fvar2q. The ends are
+  // visited in boucon's order (i-min, i-max, j-min, j-max, k-min, k-max).
+  void fs_boucon() {
+    const int dims[3] = {im, jm, km};
+    for (int dir = 0; dir < 3; ++dir) {
+      const bool lo = ntype[dir] == 1 || ntype[dir] == 4, hi = ntype[dir] == 2 || ntype[dir] == 4;
+      const int o1 = (dir == 0) ? 1 : 0, o2 = (dir == 2) ? 1 : 2;
+      for (int side = 0; side < 2; ++side) {
+        if (!(side == 0 ? lo : hi)) continue;
+        const int w = side == 0 ? 0 : dims[dir], s1 = side == 0 ? 1 : -1;
+        for (int b = 0; b <= dims[o2]; ++b)
+          for (int a = 0; a <= dims[o1]; ++a) {
+            int p[3], p1[3], p2[3];
+            p[o1] = p1[o1] = p2[o1] = a;
+            p[o2] = p1[o2] = p2[o2] = b;
+            p[dir] = w; p1[dir] = w + s1; p2[dir] = w + 2 * s1;
+            const double pe = num1d3 * (4.0 * prs(p1[0], p1[1], p1[2]) - prs(p2[0], p2[1], p2[2]));
+            for (int c = 0; c < 3; ++c) vel(p[0], p[1], p[2], c) = 0.0;
+            prs(p[0], p[1], p[2]) = pe;
+            tmp(p[0], p[1], p[2]) = twall;
+            rho(p[0], p[1], p[2]) = pe / twall * const2;
+            const double u[3] = {0.0, 0.0, 0.0};
+            double qq[5];
+            fvar2q(qq, rho(p[0], p[1], p[2]), u, pe);
+            for (int m = 0; m < 5; ++m) q(p[0], p[1], p[2], m) = qq[m];
+          }
+      }
+    }
+  }
+
   // One step of time_integration_rk (rk3), mainloop.F90:392-476; history row at stage 1 after
   // gradcal, as in the miniapp.
   void rk3_full() {
@@ -971,6 +1015,7 @@ struct TGV {
     const double jb = jac();
     for (int rk = 0; rk < 3; ++rk) {
       if (lfilter) filterq();
+      fs_boucon();
       fs_qswap();
       fs_rhscal();
       if (rk == 0) {
@@ -999,8 +1044,24 @@ struct TGV {
   // One rhscal of the full solver on the current state (filterq and qswap first, as a stage does)
   void rhs_full() {
     if (lfilter) filterq();
+    fs_boucon();
     fs_qswap();
     fs_rhscal();
+  }
+
+  // Boundary types per direction (ntype of fd_scheme_initiate / compact_filter_initiate) and
+  // the wall temperature of the physical ends.
+  void set_boundaries(const int* nt, double tw) {
+    const int dims[3] = {im, jm, km};
+    twall = tw;
+    for (int d = 0; d < 3; ++d) {
+      ntype[d] = nt[d];
+      fds[d] = Scheme();
+      flt[d] = Scheme();
+      fd_scheme_initiate(fds[d], "643c", nt[d], dims[d]);
+      compact_filter_initiate(flt[d], nt[d], dims[d], alfa_f, false);
+      filter_coefficient_cal(flt[d], alfa_f, beta_h, beta_b);
+    }
   }
 
   // rk3, tgvsolver.F90:994-1082, and the step counter of steploop (:944-960)
@@ -1114,7 +1175,11 @@ void orc_tgv_get_q(void* h, double* q) { static_cast<TGV*>(h)->get_q(q); }
 void orc_tgv_set_dt(void* h, double dt) { static_cast<TGV*>(h)->deltat = dt; }
 double orc_tgv_cfl_dt(void* h, double cfl) { return static_cast<TGV*>(h)->cfl_dt(cfl); }
 void orc_tgv_steps(void* h, int n) { TGV* t = static_cast<TGV*>(h); for (int s = 0; s < n; ++s) t->rk3(); }
-// Full-solver mode (time_integration_rk of the full solver on a periodic box, see rk3_full).
+void orc_tgv_set_boundaries(void* h, int n0, int n1, int n2, double twall) {
+  const int nt[3] = {n0, n1, n2};
+  static_cast<TGV*>(h)->set_boundaries(nt, twall);
+}
+// Full-solver mode (time_integration_rk of the full solver, see rk3_full).
 void orc_tgv_steps_full(void* h, int n) { TGV* t = static_cast<TGV*>(h); for (int s = 0; s < n; ++s) t->rk3_full(); }
 // One full-solver rhscal (after the stage's filterq and qswap) into qrhs on nodes 0..N; the state
 // keeps the filtered, averaged q.

@@ -135,3 +135,69 @@ def test_full_and_miniapp_modes_differ_as_expected(ctx):
     scale = [np.abs(b[..., 0]).max(), mom, mom, mom, np.abs(b[..., 4]).max()]
     d = max(np.abs(a[..., m] - b[..., m]).max() / scale[m] for m in range(5))
     assert 1e-12 < d < 1e-5
+
+
+def _channel_state(dims, mach, seed):
+    """A wall-bounded state: x and z periodic, walls at y = 0 and y = L with zero velocity."""
+    rng = np.random.default_rng(seed)
+    x = [2 * np.pi * np.arange(n + 1) / n for n in dims]
+    X, Y, Z = np.meshgrid(*x, indexing="ij")
+    rho = 1.0 + 0.02 * np.cos(X) * np.sin(Y / 2)
+    u = np.sin(Y / 2) ** 2 * (1.0 + 0.1 * np.cos(X) * np.sin(Z))
+    v = 0.05 * np.sin(Y) * np.sin(X) * (1.0 + 0.1 * rng.standard_normal())
+    w = 0.05 * np.sin(Y) * np.cos(Z)
+    p = 1.0 / (1.4 * mach ** 2) + 0.05 * np.cos(X)
+    q = np.zeros(tuple(n + 1 for n in dims) + (5,), order="F")
+    q[..., 0] = rho
+    q[..., 1] = rho * u
+    q[..., 2] = rho * v
+    q[..., 3] = rho * w
+    q[..., 4] = p / 0.4 + 0.5 * rho * (u * u + v * v + w * w)
+    return q
+
+
+@pytest.mark.parametrize("ntype", [(3, 4, 3), (4, 3, 3)])
+def test_full_walls_match_oracle(ctx, ntype):
+    """Non-periodic closures end to end with isothermal no-slip walls (bctype 41, boucon's noslip,
+    src/bc.F90:6281-6595) at the physical ends of one direction: the compact boundary closures of the
+    derivative and the filter (beta_bound 0.98, the filter's boundary reset), the wall state set
+    after the filter at every stage, no exchange along the walled direction. One stage's RHS and 10
+    steps against the oracle's full-solver mode with the same boundaries."""
+    import astr_gpu_b200 as ag
+    dims = (40, 48, 36) if ntype[1] == 4 else (48, 40, 36)
+    mach = 0.2
+    q = _channel_state(dims, mach, 5)
+    if ntype[0] == 4:   # walls at x = 0 and x = L: rotate the velocity pattern
+        q = np.asfortranarray(np.transpose(_channel_state((dims[1], dims[0], dims[2]), mach, 5), (1, 0, 2, 3))[..., [0, 2, 1, 3, 4]])
+    kw = dict(mach=mach, reynolds=500.0, sutherland=110.3, beta_bound=0.98, ntype=ntype, twall=1.0)
+    o = oracle.TGVOracle(*dims, params=oracle.FlowParams(**kw))
+    o.set_q(q)
+    ref = o.rhs_full()
+    s = ag.FullSolver(ctx, *dims, params=ag.FlowParams(**kw))
+    s.set_q(q)
+    got = s.rhs()
+    h = [2 * np.pi / n for n in dims]
+    jac, p0 = h[0] * h[1] * h[2], 1.0 / (1.4 * mach ** 2)
+    for m in range(5):
+        scale = max(np.abs(ref[..., m]).max(), jac * p0 / min(h))
+        assert np.abs(got[..., m] - ref[..., m]).max() <= 1e-12 * scale, m
+    o2 = oracle.TGVOracle(*dims, params=oracle.FlowParams(**kw))
+    o2.set_q(q)
+    o2.set_dt(1e-3)
+    o2.steps_full(10)
+    s2 = ag.FullSolver(ctx, *dims, params=ag.FlowParams(**kw))
+    s2.set_q(q)
+    s2.step(1e-3, 10)
+    qo, qg = o2.get_q(), s2.get_q()
+    mom = max(np.abs(qo[..., m]).max() for m in (1, 2, 3))
+    scale = [np.abs(qo[..., 0]).max(), mom, mom, mom, np.abs(qo[..., 4]).max()]
+    assert max(np.abs(qg[..., m] - qo[..., m]).max() / scale[m] for m in range(5)) <= 1e-10
+    s.close()
+    s2.close()
+
+
+def test_miniapp_step_rejects_walls(ctx):
+    import astr_gpu_b200 as ag
+    with pytest.raises(ag.AstrError) as e:
+        ag.TGVSolver(ctx, 32, params=ag.FlowParams(ntype=(3, 4, 3)))
+    assert e.value.code == -4

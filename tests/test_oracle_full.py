@@ -64,3 +64,24 @@ def test_full_and_miniapp_steps_agree_to_the_averaging_level():
         scale = [np.abs(qa[..., 0]).max(), mom, mom, mom, np.abs(qa[..., 4]).max()]
         d = max(np.abs(qa[..., m] - qb[..., m]).max() / scale[m] for m in range(5))
         assert 1e-12 < d < 1e-6, (filt, d)
+
+
+def test_walls_hold_the_wall_state_after_boucon():
+    """Isothermal no-slip walls at the two ends along y: after a stage's filter and boucon the
+    wall nodes carry zero momentum and the wall temperature's density p/T gamma M^2."""
+    dims = (16, 20, 12)
+    p = oracle.FlowParams(mach=0.2, reynolds=500.0, sutherland=110.3, beta_bound=0.98, ntype=(3, 4, 3), twall=1.3)
+    o = oracle.TGVOracle(*dims, params=p)
+    x = [2 * np.pi * np.arange(n + 1) / n for n in dims]
+    X, Y, Z = np.meshgrid(*x, indexing="ij")
+    q = np.zeros(tuple(n + 1 for n in dims) + (5,), order="F")
+    q[..., 0] = 1.0 + 0.02 * np.cos(X)
+    q[..., 1] = q[..., 0] * np.sin(Y / 2) ** 2
+    q[..., 4] = 1.0 / (1.4 * 0.04) / 0.4 + 0.5 * q[..., 1] ** 2 / q[..., 0]
+    o.set_q(q)
+    o.rhs_full()
+    qs = o.get_q()
+    for j in (0, -1):
+        assert np.all(qs[:, j, :, 1:4] == 0.0)
+        pr = qs[:, j, :, 4] * 0.4
+        np.testing.assert_allclose(qs[:, j, :, 0], pr / 1.3 * (1.4 * 0.04), rtol=1e-14)
