@@ -25,7 +25,8 @@ from . import _lib
 from ._lib import ASTR_DEVICE, ASTR_HOST, AstrParams
 
 __all__ = ["AstrError", "Context", "Scheme", "fd_scheme_initiate", "compact_filter_initiate", "central",
-           "compact_filter", "FlowParams", "TGVSolver", "FullSolver", "Ensemble"]
+           "compact_filter", "compact_flux_initiate", "flux_compact", "flux_difference", "FlowParams",
+           "TGVSolver", "FullSolver", "Ensemble"]
 
 
 class AstrError(RuntimeError):
@@ -77,10 +78,11 @@ class Context:
 
 
 class Scheme:
-    """A ``compact_scheme`` living on the device (derivative or filter)."""
+    """A ``compact_scheme`` living on the device (derivative, filter or interface flux)."""
 
-    def __init__(self, ctx: Context, h, dim: int, ntype: int, is_filter: bool):
+    def __init__(self, ctx: Context, h, dim: int, ntype: int, is_filter: bool, wind: str | None = None):
         self.ctx, self._h, self.dim, self.ntype, self.is_filter = ctx, h, dim, ntype, is_filter
+        self.wind = wind   # '+' or '-' for an interface-flux scheme, else None
 
     def ac(self):
         """(first_node, last_node, ac(3,n)) — the pre-factored Thomas table."""
@@ -116,17 +118,30 @@ def compact_filter_initiate(ctx: Context, ntype: int, dim: int, alfa: float = 0.
     return Scheme(ctx, h, dim, ntype, True)
 
 
+def compact_flux_initiate(ctx: Context, ntype: int, dim: int, wind: str = "+", bfac: float = 0.0,
+                          scheme: int = 543) -> Scheme:
+    """flux.F90:32 — the '543' compact interface-flux scheme, ``wind`` '+' (upwind-biased,
+    ``flux_uw_*``) or '-' (downwind-biased, ``flux_dw_*``), ``bfac`` the MP-LD b factor."""
+    if wind not in ("+", "-"):
+        raise ValueError("wind must be '+' or '-'")
+    h = ctypes.c_void_p()
+    ctx.check(ctx.L.astr_flux_create(ctx._h, scheme, ntype, dim, wind.encode(), float(bfac), ctypes.byref(h)))
+    return Scheme(ctx, h, dim, ntype, False, wind)
+
+
 def _is_torch(x):
     return type(x).__module__.startswith("torch")
 
 
-def _apply(ctx, scheme, f, direction, lbound, out_lbound, out_shape, scale, is_filter):
+def _apply(ctx, scheme, f, direction, lbound, out_lbound, out_shape, scale, kind):
     dim = scheme.dim
     nf = f.shape[3] if f.ndim == 4 else 1
     fshape = list(f.shape[:3])
     lb = list(lbound)
-    oshape = list(out_shape) if out_shape is not None else [fshape[d] if d != direction else dim + 1 for d in range(3)]
-    olb = list(out_lbound) if out_lbound is not None else [lb[d] if d != direction else 0 for d in range(3)]
+    # the interface flux spans interfaces -1..dim along the direction, everything else nodes 0..dim
+    n_dir, lb_dir = (dim + 2, -1) if kind == "flux" else (dim + 1, 0)
+    oshape = list(out_shape) if out_shape is not None else [fshape[d] if d != direction else n_dir for d in range(3)]
+    olb = list(out_lbound) if out_lbound is not None else [lb[d] if d != direction else lb_dir for d in range(3)]
     if _is_torch(f):
         import torch
         assert f.is_cuda and f.dtype == torch.float64
@@ -142,9 +157,14 @@ def _apply(ctx, scheme, f, direction, lbound, out_lbound, out_shape, scale, is_f
         out = np.zeros(tuple(oshape) + ((nf,) if f.ndim == 4 else ()), order="F")
         fptr, optr, where = fp.ctypes.data, out.ctypes.data, ASTR_HOST
     L = ctx.L
-    if is_filter:
-        ctx.check(L.astr_filter_lines(ctx._h, scheme._h, direction, ctypes.c_void_p(fptr), _i64(fshape), _i64(lb),
-                                      ctypes.c_void_p(optr), _i64(oshape), _i64(olb), nf, where))
+    args = (ctx._h, scheme._h, direction, ctypes.c_void_p(fptr), _i64(fshape), _i64(lb), ctypes.c_void_p(optr),
+            _i64(oshape), _i64(olb), nf)
+    if kind == "filter":
+        ctx.check(L.astr_filter_lines(*args, where))
+    elif kind == "flux":
+        ctx.check(L.astr_flux_lines(*args, where))
+    elif kind == "fluxdiff":
+        ctx.check(L.astr_flux_diff_lines(*args, float(scale), 0, where))
     else:
         ctx.check(L.astr_deriv_lines(ctx._h, scheme._h, direction, ctypes.c_void_p(fptr), _i64(fshape), _i64(lb),
                                      ctypes.c_void_p(optr), _i64(oshape), _i64(olb), nf, float(scale), where))
@@ -158,13 +178,27 @@ def central(ctx: Context, scheme: Scheme, f, direction: int, lbound=(0, 0, 0), s
     """``df = fds%central(asolver, f, dim)`` for every line of ``f`` along ``direction``.
     ``f(lbound...)`` must carry nodes -5..dim+5 along ``direction`` when the scheme reads halos.
     The result spans nodes 0..dim along ``direction`` (index-space derivative times ``scale``)."""
-    return _apply(ctx, scheme, f, direction, lbound, out_lbound, out_shape, scale, False)
+    return _apply(ctx, scheme, f, direction, lbound, out_lbound, out_shape, scale, "deriv")
 
 
 def compact_filter(ctx: Context, scheme: Scheme, f, direction: int, lbound=(0, 0, 0), out_lbound=None,
                    out_shape=None):
     """``ff = compact_filter(afilter, f, dim)`` for every line of ``f`` along ``direction``."""
-    return _apply(ctx, scheme, f, direction, lbound, out_lbound, out_shape, 1.0, True)
+    return _apply(ctx, scheme, f, direction, lbound, out_lbound, out_shape, 1.0, "filter")
+
+
+def flux_compact(ctx: Context, scheme: Scheme, f, direction: int, lbound=(0, 0, 0), out_lbound=None,
+                 out_shape=None):
+    """``fh = flux_compact(asolver, f, dim)`` (flux.F90:125) for every line of ``f`` along
+    ``direction``; the result spans interfaces -1..dim along ``direction`` (lower bound -1)."""
+    return _apply(ctx, scheme, f, direction, lbound, out_lbound, out_shape, 1.0, "flux")
+
+
+def flux_difference(ctx: Context, scheme: Scheme, f, direction: int, lbound=(0, 0, 0), scale: float = 1.0,
+                    out_lbound=None, out_shape=None):
+    """``scale * (fh(i) - fh(i-1))`` at nodes 0..dim of every line (the flux-form derivative of
+    convrsdcmp, solver.F90:1509-1513, and of the reference's flux test, test.F90:755-765)."""
+    return _apply(ctx, scheme, f, direction, lbound, out_lbound, out_shape, scale, "fluxdiff")
 
 
 @dataclass

@@ -43,6 +43,9 @@ SIGNATURES = {
     "astr_scheme_ac": (_i, [_vp, _dp, _ip, _ip]),
     "astr_deriv_lines": (_i, [_vp, _vp, _i, _vp, _i64p, _i64p, _vp, _i64p, _i64p, _i, _d, _i]),
     "astr_filter_lines": (_i, [_vp, _vp, _i, _vp, _i64p, _i64p, _vp, _i64p, _i64p, _i, _i]),
+    "astr_flux_create": (_i, [_vp, _i, _i, _i, ctypes.c_char, _d, _pvp]),
+    "astr_flux_lines": (_i, [_vp, _vp, _i, _vp, _i64p, _i64p, _vp, _i64p, _i64p, _i, _i]),
+    "astr_flux_diff_lines": (_i, [_vp, _vp, _i, _vp, _i64p, _i64p, _vp, _i64p, _i64p, _i, _d, _i, _i]),
     "astr_state_create": (_i, [_vp, ctypes.POINTER(AstrParams), _pvp]),
     "astr_state_destroy": (_i, [_vp]),
     "astr_state_init_tgv": (_i, [_vp]),

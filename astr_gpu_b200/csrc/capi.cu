@@ -158,13 +158,19 @@ ArrDesc fortran_desc(const int64_t* shape, const int64_t* lb) {
 }
 
 int line_call(astr_ctx* ctx, const astr_scheme* s, int dir, const double* f, const int64_t* fsh, const int64_t* flb,
-              double* out, const int64_t* osh, const int64_t* olb, int nfields, double scale, int where) {
+              double* out, const int64_t* osh, const int64_t* olb, int nfields, double scale, int where,
+              int flags = 0) {
   if (!ctx || !s || !f || !out || !fsh || !flb || !osh || !olb) return fail(ctx, ASTR_ERR_ARG, "null argument");
   if (dir < 0 || dir > 2 || nfields < 1) return fail(ctx, ASTR_ERR_ARG, "bad dir or nfields");
   const int dim = s->h.dim;
   for (int d = 0; d < 3; ++d)
     if (fsh[d] < 1 || osh[d] < 1) return fail(ctx, ASTR_ERR_ARG, "empty extent");
-  if (!covers(osh, olb, dir, 0, dim)) return fail(ctx, ASTR_ERR_ARG, "output must cover nodes 0..dim along dir");
+  const bool interfaces = s->h.kind == OP_FLUX && !(flags & LINE_DIFF);
+  if (interfaces) {
+    if (!covers(osh, olb, dir, -1, dim)) return fail(ctx, ASTR_ERR_ARG, "output must cover interfaces -1..dim along dir");
+  } else if (!covers(osh, olb, dir, 0, dim)) {
+    return fail(ctx, ASTR_ERR_ARG, "output must cover nodes 0..dim along dir");
+  }
   const int64_t lo = s->h.left_phys ? 0 : -5, hi = s->h.right_phys ? dim : dim + 5;
   if (s->h.kind != OP_EXPLICIT || s->h.ntype != 4)
     if (!covers(fsh, flb, dir, lo, hi)) return fail(ctx, ASTR_ERR_ARG, "input line must hold nodes -5..dim+5 (halo) along dir");
@@ -195,7 +201,7 @@ int line_call(astr_ctx* ctx, const astr_scheme* s, int dir, const double* f, con
     df_ = tf;
     dout = to;
   }
-  cudaError_t e = launch_line_api(s->d, dir, df_, fa, dout, oa, nfields, scale, ctx->stream);
+  cudaError_t e = launch_line_api(s->d, dir, df_, fa, dout, oa, nfields, scale, ctx->stream, flags);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "line kernel");
   if (where == ASTR_HOST) {
     CK(cudaMemcpyAsync(out, to, ob, cudaMemcpyDeviceToHost, ctx->stream));
@@ -582,6 +588,25 @@ int astr_filter_create(astr_ctx* ctx, int ntype, int dim, double alpha_f, double
   return ASTR_OK;
 }
 
+int astr_flux_create(astr_ctx* ctx, int scheme, int ntype, int dim, char wind, double bfac, astr_scheme** out) {
+  const DeviceGuard dg_(ctx ? ctx->device : -1);
+  if (!ctx || !out) return fail(ctx, ASTR_ERR_ARG, "null argument");
+  if (wind != '+' && wind != '-') return fail(ctx, ASTR_ERR_ARG, "wind must be '+' or '-'");
+  if (!std::isfinite(bfac)) return fail(ctx, ASTR_ERR_ARG, "bfac must be finite");
+  astr_scheme* s = new astr_scheme();
+  s->ctx = ctx;
+  if (!build_flux_op(s->h, scheme, ntype, dim, wind == '+' ? 1 : -1, bfac)) {
+    delete s;
+    return fail(ctx, ASTR_ERR_ARG, "flux scheme not defined (only 543) or bad ntype/dim");
+  }
+  Layout lay = pick_layout(s->h.nsys());
+  if (lay.S == 0) { delete s; return fail(ctx, ASTR_ERR_UNSUPPORTED, "line longer than 1152 rows"); }
+  cudaError_t e = make_devop(s->h, lay, s->d);
+  if (e != cudaSuccess) { free_devop(s->d); delete s; return cuda_fail(ctx, e, "scheme tables"); }
+  *out = s;
+  return ASTR_OK;
+}
+
 int astr_scheme_destroy(astr_scheme* s) {
   const DeviceGuard dg_(s && s->ctx ? s->ctx->device : -1);
   if (!s) return ASTR_ERR_ARG;
@@ -617,6 +642,24 @@ int astr_filter_lines(astr_ctx* ctx, const astr_scheme* s, int dir, const double
   const DeviceGuard dg_(ctx ? ctx->device : -1);
   if (s && s->h.kind != OP_FILTER) return fail(ctx, ASTR_ERR_ARG, "scheme is not a filter");
   return line_call(ctx, s, dir, f, f_shape, f_lbound, ff, ff_shape, ff_lbound, nfields, 1.0, where);
+}
+
+int astr_flux_lines(astr_ctx* ctx, const astr_scheme* s, int dir, const double* f, const int64_t f_shape[3],
+                    const int64_t f_lbound[3], double* fh, const int64_t fh_shape[3], const int64_t fh_lbound[3],
+                    int nfields, int where) {
+  const DeviceGuard dg_(ctx ? ctx->device : -1);
+  if (s && s->h.kind != OP_FLUX) return fail(ctx, ASTR_ERR_ARG, "scheme is not an interface flux");
+  return line_call(ctx, s, dir, f, f_shape, f_lbound, fh, fh_shape, fh_lbound, nfields, 1.0, where);
+}
+
+int astr_flux_diff_lines(astr_ctx* ctx, const astr_scheme* s, int dir, const double* f, const int64_t f_shape[3],
+                         const int64_t f_lbound[3], double* df, const int64_t df_shape[3], const int64_t df_lbound[3],
+                         int nfields, double scale, int accumulate, int where) {
+  const DeviceGuard dg_(ctx ? ctx->device : -1);
+  if (s && s->h.kind != OP_FLUX) return fail(ctx, ASTR_ERR_ARG, "scheme is not an interface flux");
+  if (accumulate && where == ASTR_HOST) return fail(ctx, ASTR_ERR_ARG, "accumulate needs device arrays");
+  return line_call(ctx, s, dir, f, f_shape, f_lbound, df, df_shape, df_lbound, nfields, scale, where,
+                   LINE_DIFF | (accumulate ? LINE_ADD : 0));
 }
 
 int astr_state_create(astr_ctx* ctx, const astr_params* p, astr_state** out) {

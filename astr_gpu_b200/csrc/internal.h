@@ -17,11 +17,14 @@ struct HostOp {
   bool left_phys = false, right_phys = false, no_note = false;
   std::vector<double> a, c, ac1, ac2, ac3;
   double c10[6] = {0}, ch[3][11] = {{0}}, cb[3][7] = {{0}}, c6[4] = {0}, c8[5] = {0};
+  int wind = 1;                 // interface flux: +1 upwind-biased, -1 downwind-biased
+  double bfac = 0.0, cfl[4] = {0};
   int nsys() const { return last_node - first_node + 1; }
 };
 
 bool build_fd_op(HostOp& op, const char* scheme, int ntype, int dim);
 void build_filter_op(HostOp& op, int ntype, int dim, double alfa, double beta_halo, double beta_bound, bool note);
+bool build_flux_op(HostOp& op, int scheme, int ntype, int dim, int wind, double bfac);
 // Lane tables for S rows per lane and nseg segments (see ops.cuh). Returns host vector.
 std::vector<double> lane_tables(const HostOp& op, int S, int nseg);
 
@@ -47,8 +50,10 @@ int tile_pitch(int dim, int TI, int S);
 
 // Line-level API launch: op along dir over every line of an arbitrary strided array.
 struct ArrDesc { int64_t s[3]; int64_t lb[3]; int64_t n[3]; int64_t fs; };
-// add != 0 accumulates into out (out += result) instead of storing.
+// flags: LINE_ADD accumulates into out (out += result) instead of storing; LINE_DIFF (interface
+// flux only) writes scale * (fh(n) - fh(n-1)) at nodes 0..dim instead of fh(-1..dim).
+enum { LINE_ADD = 1, LINE_DIFF = 2 };
 cudaError_t launch_line_api(const DevOp& op, int dir, const double* f, const ArrDesc& fa, double* out,
-                            const ArrDesc& oa, int nfields, double scale, cudaStream_t st, int add = 0);
+                            const ArrDesc& oa, int nfields, double scale, cudaStream_t st, int flags = 0);
 
 }  // namespace astr

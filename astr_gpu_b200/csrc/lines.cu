@@ -1,7 +1,10 @@
 // Line-level operators over arbitrary Fortran-ordered arrays: the drop-in for
 //   df = fds%central(asolver, f, dim)      src/derivative.F90:22-41, 171-198
 //   ff = compact_filter(afilter, f, dim)   src/filter.F90:112-144
-// applied to every line of a 3-D array along one direction.
+//   fh = flux_compact(asolver, f, dim)     src/flux.F90:125-150 (interfaces -1..dim)
+// applied to every line of a 3-D array along one direction; the interface flux can also leave
+// its differences fh(i) - fh(i-1) at the nodes (the flux-form derivative of convrsdcmp,
+// src/solver.F90:1509-1513, and of the reference's flux test, src/test.F90:755-765).
 //
 // One CTA takes TI lines of one field. The lines (nodes -HT..dim+HT, the halos read from the
 // caller's array, zeros outside it) are staged in shared memory with asynchronous copies, all in
@@ -53,7 +56,7 @@ __device__ __forceinline__ Slot slot_of(int dir, int TI) {
 template <int S, int WPL>
 __global__ void __launch_bounds__(512) k_line_api(LineOp op, int dir, const double* __restrict__ f, ArrDesc fa,
                                                   double* __restrict__ out, ArrDesc oa, int TI, int LP, double scale,
-                                                  int add) {
+                                                  int flags) {
   extern __shared__ double sm[];
   double* tile = sm;
   double* scan = sm + (size_t)TI * LP;                 // SCAN_LINE doubles per line group
@@ -137,41 +140,55 @@ __global__ void __launch_bounds__(512) k_line_api(LineOp op, int dir, const doub
       const double* line = tile + l * LP + HT;
       auto get = [line](int nn) { return line[nn]; };
       if (op.kind == OP_DERIV) rhs_deriv<S>(v[i], op, seg, get, sp + l * 2 * NSP);
+      else if (op.kind == OP_FLUX) rhs_flux<S>(v[i], op, seg, get, sp + l * 2 * NSP);
       else rhs_filter<S>(v[i], op, seg, get, sp + l * 2 * NSP);
     }
     seg_solve_n<S, WPL, 2>(v, op.tab, seg, lane, part, g, scan + g * SCAN_LINE);
   }
   __syncthreads();
+  // outputs: nodes 0..dim, or the interfaces -1..dim of the flux (kept unscaled for differences)
+  const bool diff = (op.kind == OP_FLUX) && (flags & LINE_DIFF);
+  const int out_lo = (op.kind == OP_FLUX) ? -1 : 0;
+  const double sc = diff ? 1.0 : scale;
 #pragma unroll
   for (int i = 0; i < 2; ++i) {
     double* line = tile + (g + i * ngroups) * LP + HT;
 #pragma unroll
     for (int t = 0; t < S; ++t) {
       const int n = seg * S + t - ext;
-      if (n < 0 || n > dim) continue;
+      if (n < out_lo || n > dim) continue;
       // physical-boundary reset ff(0)=f(0), ff(dim)=f(dim) of compact_filter (filter.F90:141-142)
       if (op.kind == OP_FILTER && ((n == 0 && op.left_phys) || (n == dim && op.right_phys))) continue;
-      line[n] = (op.kind == OP_FILTER) ? v[i][t] : scale * v[i][t];
+      line[n] = (op.kind == OP_FILTER) ? v[i][t] : sc * v[i][t];
     }
   }
   __syncthreads();
 
-  // ---- stores of nodes 0..dim from the tile
+  // ---- stores from the tile: nodes 0..dim (interfaces -1..dim for the flux)
   if (!valid) return;
   double* dst = out + (int64_t)blockIdx.z * oa.fs + (i2 - oa.lb[o2]) * oa.s[o2] + (i1 - oa.lb[o1]) * oa.s[o1] -
                 oa.lb[dir] * oa.s[dir];
   const int64_t od = oa.s[dir];
-  if (add) {
-    for (int n = sl.n0; n <= dim; n += sl.nst) dst[(int64_t)n * od] += trow[n];
+  const bool add = flags & LINE_ADD;
+  if (diff) {
+    for (int n = sl.n0; n <= dim; n += sl.nst) {
+      const double d = scale * (trow[n] - trow[n - 1]);
+      if (add) dst[(int64_t)n * od] += d;
+      else dst[(int64_t)n * od] = d;
+    }
   } else {
-    for (int n = sl.n0; n <= dim; n += sl.nst) dst[(int64_t)n * od] = trow[n];
+    if (add) {
+      for (int n = out_lo + sl.n0; n <= dim; n += sl.nst) dst[(int64_t)n * od] += trow[n];
+    } else {
+      for (int n = out_lo + sl.n0; n <= dim; n += sl.nst) dst[(int64_t)n * od] = trow[n];
+    }
   }
 }
 
 // scan scratch of seg_solve_n: 2 * WPL doubles per solve, two solves per line group
 template <int S, int WPL>
 static cudaError_t launch_t(const DevOp& op, int dir, const double* f, const ArrDesc& fa, double* out,
-                            const ArrDesc& oa, int nfields, double scale, int add, cudaStream_t st) {
+                            const ArrDesc& oa, int nfields, double scale, int flags, cudaStream_t st) {
   const int o1 = (dir == 0) ? 1 : 0, o2 = (dir == 2) ? 1 : 2;
   // two lines per group of WPL warps, at most 512 threads and 16 lines, one named barrier per
   // group (WPL > 1: at most 15 groups)
@@ -184,19 +201,19 @@ static cudaError_t launch_t(const DevOp& op, int dir, const double* f, const Arr
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   dim3 grid((unsigned)((oa.n[o1] + TI - 1) / TI), (unsigned)oa.n[o2], (unsigned)nfields);
-  kern<<<grid, ngroups * WPL * 32, smem, st>>>(op.op, dir, f, fa, out, oa, TI, LP, scale, add);
+  kern<<<grid, ngroups * WPL * 32, smem, st>>>(op.op, dir, f, fa, out, oa, TI, LP, scale, flags);
   return cudaGetLastError();
 }
 
 cudaError_t launch_line_api(const DevOp& op, int dir, const double* f, const ArrDesc& fa, double* out,
-                            const ArrDesc& oa, int nfields, double scale, cudaStream_t st, int add) {
-  if (op.S == 3 && op.WPL == 1) return launch_t<3, 1>(op, dir, f, fa, out, oa, nfields, scale, add, st);
-  if (op.S == 5 && op.WPL == 1) return launch_t<5, 1>(op, dir, f, fa, out, oa, nfields, scale, add, st);
-  if (op.S == 5 && op.WPL == 2) return launch_t<5, 2>(op, dir, f, fa, out, oa, nfields, scale, add, st);
-  if (op.S == 5 && op.WPL == 4) return launch_t<5, 4>(op, dir, f, fa, out, oa, nfields, scale, add, st);
-  if (op.S == 9 && op.WPL == 1) return launch_t<9, 1>(op, dir, f, fa, out, oa, nfields, scale, add, st);
-  if (op.S == 9 && op.WPL == 2) return launch_t<9, 2>(op, dir, f, fa, out, oa, nfields, scale, add, st);
-  if (op.S == 9 && op.WPL == 4) return launch_t<9, 4>(op, dir, f, fa, out, oa, nfields, scale, add, st);
+                            const ArrDesc& oa, int nfields, double scale, cudaStream_t st, int flags) {
+  if (op.S == 3 && op.WPL == 1) return launch_t<3, 1>(op, dir, f, fa, out, oa, nfields, scale, flags, st);
+  if (op.S == 5 && op.WPL == 1) return launch_t<5, 1>(op, dir, f, fa, out, oa, nfields, scale, flags, st);
+  if (op.S == 5 && op.WPL == 2) return launch_t<5, 2>(op, dir, f, fa, out, oa, nfields, scale, flags, st);
+  if (op.S == 5 && op.WPL == 4) return launch_t<5, 4>(op, dir, f, fa, out, oa, nfields, scale, flags, st);
+  if (op.S == 9 && op.WPL == 1) return launch_t<9, 1>(op, dir, f, fa, out, oa, nfields, scale, flags, st);
+  if (op.S == 9 && op.WPL == 2) return launch_t<9, 2>(op, dir, f, fa, out, oa, nfields, scale, flags, st);
+  if (op.S == 9 && op.WPL == 4) return launch_t<9, 4>(op, dir, f, fa, out, oa, nfields, scale, flags, st);
   return cudaErrorInvalidValue;
 }
 

@@ -27,7 +27,8 @@ constexpr int WIN_SLACK = 8;
 __host__ __device__ constexpr int win_slack(int S) { return S > 9 ? WIN_SLACK : 0; }
 constexpr unsigned FULL = 0xffffffffu;
 
-enum OpKind { OP_DERIV = 0, OP_FILTER = 1, OP_EXPLICIT = 2 };
+// OP_FLUX: the compact interface flux of flux.F90 (rows are interfaces, outputs fh(-1..dim))
+enum OpKind { OP_DERIV = 0, OP_FILTER = 1, OP_EXPLICIT = 2, OP_FLUX = 3 };
 
 // One line operator (a compact_scheme of the reference plus the lane tables of its solve).
 // Table layout (doubles), NS = 32*WPL segments of S rows, row t of segment seg:
@@ -51,6 +52,10 @@ struct LineOp {
   int S;
   int spec_lo, spec_hi;        // closure rows at the start / end of the system (RHS not interior)
   double c10[6], ch[3][11], cb[3][7], c6[4], c8[5];  // filter coefficients (filter.F90:299-432)
+  // interface flux: wind +1 ('+', upwind-biased) or -1 ('-'), and the interior RHS weights
+  // (1/18 - b/36, 19/18 - 9b/36, 5/9 + 9b/36, b/36) of compact_flux_rhs (flux.F90:241-253)
+  int wind;
+  double cfl[4];
 };
 
 constexpr int NSP = 5;   // closure rows kept per end: sp[0..4] start, sp[5..9] end
@@ -217,11 +222,36 @@ __device__ __forceinline__ void fill_window(double (&w)[W], int n0, int dim, Get
 template <class Get>
 __host__ __device__ __forceinline__ bool filter_special(const LineOp& op, int r, Get f, double& out);
 
-// RHS value of closure row r (derivative or filter), for the precomputed closure table.
+// Compact interface-flux closure rows, compact_flux_rhs (flux.F90:188-230): 3rd-order rows at
+// physical ends, the explicit 6th-order central interface value elsewhere. Row r is interface
+// j = r - ext_lo (between nodes j and j + 1).
+template <class Get>
+__host__ __device__ __forceinline__ bool flux_special(const LineOp& op, int r, Get f, double& out) {
+  const int j = r - op.ext_lo;
+  auto central = [&]() {
+    const double var1 = f(j) + f(j + 1), var2 = f(j - 1) + f(j + 2), var3 = f(j - 2) + f(j + 3);
+    return (37.0 / 60.0) * var1 - (2.0 / 15.0) * var2 + (1.0 / 60.0) * var3;
+  };
+  if (r == 0) {
+    out = op.left_phys ? 2.5 * f(j + 1) + 0.5 * f(j + 2) : central();
+    return true;
+  }
+  if (r == 1 && op.left_phys) { out = 0.75 * f(j) + 0.75 * f(j + 1); return true; }
+  if (r == op.nsys - 1) {
+    out = op.right_phys ? 2.5 * f(j) + 0.5 * f(j - 1) : central();
+    return true;
+  }
+  if (r == op.nsys - 2 && op.right_phys) { out = 0.75 * f(j + 1) + 0.75 * f(j); return true; }
+  return false;
+}
+
+// RHS value of closure row r (derivative, filter or interface flux), for the precomputed
+// closure table.
 template <class Get>
 __device__ __forceinline__ double special_value(const LineOp& op, int r, Get f) {
   double s = 0.0;
   if (op.kind == OP_FILTER) filter_special(op, r, f, s);
+  else if (op.kind == OP_FLUX) flux_special(op, r, f, s);
   else deriv_special(op, r, f, s);
   return s;
 }
@@ -251,6 +281,25 @@ __device__ __forceinline__ void rhs_deriv(double (&v)[S], const LineOp& op, int 
   double w[S + 4];
   fill_window<S + 4, S>(w, r0 - op.ext_lo - 2, op.dim, f);
   stencil_deriv<S>(v, w);
+  apply_specials<S>(v, op, r0, sp);
+}
+
+// Interior rows of the compact interface flux (flux.F90:241-253), in the reference's order of
+// the four products for each wind; window w[t] = f(n0 - 1 + t), n0 = interface of the first row.
+template <int S, class Get>
+__device__ __forceinline__ void rhs_flux(double (&v)[S], const LineOp& op, int seg, Get f, const double* sp) {
+  const int r0 = seg * S;
+  double w[S + 3];
+  fill_window<S + 3, S>(w, r0 - op.ext_lo - 1, op.dim, f);
+  if (op.wind > 0) {
+#pragma unroll
+    for (int t = 0; t < S; ++t)
+      v[t] = op.cfl[0] * w[t] + op.cfl[1] * w[t + 1] + op.cfl[2] * w[t + 2] + op.cfl[3] * w[t + 3];
+  } else {
+#pragma unroll
+    for (int t = 0; t < S; ++t)
+      v[t] = op.cfl[0] * w[t + 3] + op.cfl[1] * w[t + 2] + op.cfl[2] * w[t + 1] + op.cfl[3] * w[t];
+  }
   apply_specials<S>(v, op, r0, sp);
 }
 

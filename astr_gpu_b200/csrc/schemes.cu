@@ -3,6 +3,7 @@
 //   fd_scheme_initiate          src/derivative.F90:63-158
 //   compact_filter_initiate     src/filter.F90:31-100
 //   filter_coefficient_cal      src/filter.F90:299-432
+//   compact_flux_initiate       src/flux.F90:32-112
 //   tridiagonal_thomas_proprocess src/commfunc.F90:752-774
 #include <cmath>
 #include <cstring>
@@ -127,6 +128,45 @@ void build_filter_op(HostOp& op, int ntype, int dim, double alfa, double bh, dou
   std::memcpy(op.ch, h, sizeof(h));
 }
 
+// The '543' compact interface-flux scheme: interfaces i_0..i_m with i_0 = -1 at a physical left
+// end (ntype 1, 4) else -2, i_m = dim at a physical right end (ntype 2, 4) else dim + 1. Interior
+// LHS a, c biased by the wind and blended by bfac (the MP-LD b factor, bfacmpld of commvar);
+// explicit central rows (a = c = 0) at interfaces; at physical ends the 3rd-order rows with
+// a = c = 2 and a = c = 1/4 next to them.
+bool build_flux_op(HostOp& op, int scheme, int ntype, int dim, int wind, double bfac) {
+  if (ntype < 1 || ntype > 4 || dim < 8 || scheme != 543 || (wind != 1 && wind != -1)) return false;
+  op.kind = OP_FLUX;
+  op.ntype = ntype;
+  op.dim = dim;
+  op.left_phys = (ntype == 1 || ntype == 4);
+  op.right_phys = (ntype == 2 || ntype == 4);
+  op.first_node = op.left_phys ? -1 : -2;
+  op.last_node = op.right_phys ? dim : dim + 1;
+  op.wind = wind;
+  op.bfac = bfac;
+  const int n = op.nsys();
+  const double a = (wind == 1) ? 0.5 - (1.0 / 6.0) * bfac : (1.0 / 6.0) + (1.0 / 6.0) * bfac;
+  const double c = (wind == 1) ? (1.0 / 6.0) + (1.0 / 6.0) * bfac : 0.5 - (1.0 / 6.0) * bfac;
+  op.a.assign(n, a);
+  op.c.assign(n, c);
+  op.a[0] = op.c[0] = 0.0;
+  op.a[n - 1] = op.c[n - 1] = 0.0;
+  if (op.left_phys) {
+    op.a[0] = op.c[0] = 2.0;
+    op.a[1] = op.c[1] = 0.25;
+  }
+  if (op.right_phys) {
+    op.a[n - 1] = op.c[n - 1] = 2.0;
+    op.a[n - 2] = op.c[n - 2] = 0.25;
+  }
+  thomas_factor(op);
+  op.cfl[0] = 1.0 / 18.0 - (1.0 / 36.0) * bfac;
+  op.cfl[1] = 19.0 / 18.0 - (9.0 / 36.0) * bfac;
+  op.cfl[2] = 5.0 / 9.0 + (9.0 / 36.0) * bfac;
+  op.cfl[3] = (1.0 / 36.0) * bfac;
+  return true;
+}
+
 std::vector<double> lane_tables(const HostOp& op, int S, int nseg) {
   const int nsys = op.nsys();
   const int WPL = nseg / 32;
@@ -231,7 +271,7 @@ void fill_lineop(const HostOp& h, LineOp& o) {
   if (h.kind == OP_FILTER) {
     o.spec_lo = h.left_phys ? 5 : 3;
     o.spec_hi = h.right_phys ? 5 : 3;
-  } else {
+  } else {   // derivative and interface flux: two closure rows at a physical end, else one
     o.spec_lo = h.left_phys ? 2 : 1;
     o.spec_hi = h.right_phys ? 2 : 1;
   }
@@ -240,6 +280,8 @@ void fill_lineop(const HostOp& h, LineOp& o) {
   std::memcpy(o.cb, h.cb, sizeof(o.cb));
   std::memcpy(o.c6, h.c6, sizeof(o.c6));
   std::memcpy(o.c8, h.c8, sizeof(o.c8));
+  o.wind = h.wind;
+  std::memcpy(o.cfl, h.cfl, sizeof(o.cfl));
 }
 
 cudaError_t make_devop(const HostOp& h, Layout lay, DevOp& out) {

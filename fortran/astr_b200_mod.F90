@@ -63,6 +63,29 @@ module astr_b200
       integer(c_int), value :: dir, nfields, where
       integer(c_int64_t) :: fshape(3), flb(3), oshape(3), olb(3)
     end function
+    integer(c_int) function astr_flux_create(ctx, scheme, ntype, dim, wind, bfac, s) bind(C, name="astr_flux_create")
+      import :: c_int, c_ptr, c_char, c_double
+      type(c_ptr), value :: ctx
+      integer(c_int), value :: scheme, ntype, dim
+      character(kind=c_char), value :: wind
+      real(c_double), value :: bfac
+      type(c_ptr) :: s
+    end function
+    integer(c_int) function astr_flux_lines(ctx, s, dir, f, fshape, flb, fh, oshape, olb, nfields, where) &
+        bind(C, name="astr_flux_lines")
+      import :: c_int, c_ptr, c_int64_t
+      type(c_ptr), value :: ctx, s, f, fh
+      integer(c_int), value :: dir, nfields, where
+      integer(c_int64_t) :: fshape(3), flb(3), oshape(3), olb(3)
+    end function
+    integer(c_int) function astr_flux_diff_lines(ctx, s, dir, f, fshape, flb, df, oshape, olb, nfields, scale, &
+        accumulate, where) bind(C, name="astr_flux_diff_lines")
+      import :: c_int, c_ptr, c_double, c_int64_t
+      type(c_ptr), value :: ctx, s, f, df
+      integer(c_int), value :: dir, nfields, accumulate, where
+      integer(c_int64_t) :: fshape(3), flb(3), oshape(3), olb(3)
+      real(c_double), value :: scale
+    end function
     integer(c_int) function astr_state_create(ctx, p, st) bind(C, name="astr_state_create")
       import :: c_int, c_ptr, astr_params
       type(c_ptr), value :: ctx

@@ -17,6 +17,10 @@
  *                                                                              src/commfunc.F90:752
  *   astr_deriv_lines        df = fds%central(asolver,f,dim) over every line    src/derivative.F90:22-41,171
  *   astr_filter_lines       ff = compact_filter(afilter,f,dim[,note])          src/filter.F90:112
+ *   astr_flux_create        compact_flux_initiate(asolver,scheme,ntype,dim,wind) src/flux.F90:32-112
+ *   astr_flux_lines         fh = flux_compact(asolver,f,dim), fh(-1:dim)       src/flux.F90:125-150
+ *   astr_flux_diff_lines    qrhs += Fh(i) - Fh(i-1) of the compact flux         src/solver.F90:1509-1513,
+ *                                                                              src/test.F90:755-765
  *   astr_state_*            the module arrays q/rho/vel/prs/tmp of commarray  miniapps/tgv_solver_3d/
  *                                                                              tgvsolver.F90:1-40
  *   astr_state_init_tgv     flowfield_init                                    tgvsolver.F90:172-234
@@ -103,6 +107,25 @@ int astr_deriv_lines(astr_ctx* ctx, const astr_scheme* s, int dir, const double*
 int astr_filter_lines(astr_ctx* ctx, const astr_scheme* s, int dir, const double* f,
                       const int64_t f_shape[3], const int64_t f_lbound[3], double* ff,
                       const int64_t ff_shape[3], const int64_t ff_lbound[3], int nfields, int where);
+
+/* ---- compact interface flux (upwind-biased compact scheme) ------------------------- */
+/* The '543' scheme of compact_flux_initiate: scheme must be 543; wind '+' (upwind-biased, the
+ * reference's flux_uw_*) or '-' (downwind-biased, flux_dw_*); bfac is the MP-LD b factor
+ * (bfacmpld of the reference's input). ntype 1..4 as for the derivative. */
+int astr_flux_create(astr_ctx* ctx, int scheme, int ntype, int dim, char wind, double bfac,
+                     astr_scheme** out);
+/* Interface values fh(-1..dim) of every line along dir (interface i lies between nodes i and
+ * i+1): f as for astr_deriv_lines (nodes -5..dim+5 where the scheme reads them), fh's range
+ * along dir must cover -1..dim. */
+int astr_flux_lines(astr_ctx* ctx, const astr_scheme* s, int dir, const double* f,
+                    const int64_t f_shape[3], const int64_t f_lbound[3], double* fh,
+                    const int64_t fh_shape[3], const int64_t fh_lbound[3], int nfields, int where);
+/* The flux-form derivative: df(n) = scale * (fh(n) - fh(n-1)) at nodes 0..dim, fh as above
+ * (never stored); accumulate != 0 adds it to df (device arrays only). */
+int astr_flux_diff_lines(astr_ctx* ctx, const astr_scheme* s, int dir, const double* f,
+                         const int64_t f_shape[3], const int64_t f_lbound[3], double* df,
+                         const int64_t df_shape[3], const int64_t df_lbound[3], int nfields,
+                         double scale, int accumulate, int where);
 
 /* ---- solver state and the RK3 step ------------------------------------------------ */
 int astr_state_create(astr_ctx* ctx, const astr_params* p, astr_state** out);

@@ -51,6 +51,9 @@ def lib():
             "orc_filter_line": (None, [vp, dp, dp]),
             "orc_deriv3d": (None, [vp, i, dp, i64p, i64p, i, dp]),
             "orc_filter3d": (None, [vp, i, dp, i64p, i64p, i, dp]),
+            "orc_flux_create": (vp, [i, i, i, i, d]),
+            "orc_flux_line": (None, [vp, dp, dp]),
+            "orc_flux3d": (None, [vp, i, dp, i64p, i64p, i, dp]),
             "orc_tgv_create": (vp, [i, i, i, d, d, d, d, d, d, d, d, d, i]),
             "orc_tgv_free": (None, [vp]),
             "orc_tgv_init_tgv": (None, [vp]),
@@ -142,6 +145,48 @@ def compact_filter_initiate(ntype: int, dim: int, alfa: float = 0.49, beta_halo:
     """filter.F90:31-100 with the coefficients of filter_coefficient_cal (filter.F90:299-432)."""
     h = lib().orc_filter_create(ntype, dim, alfa, beta_halo, beta_bound, int(boundary_no_filter))
     return Scheme(h, dim, ntype, True)
+
+
+class FluxScheme(Scheme):
+    """A compact interface-flux scheme (``compact_flux_initiate``, flux.F90:32-112): the
+    tridiagonal '543' scheme with wind-biased interior coefficients blended by ``bfac``; its
+    outputs are the interface values fh(-1..dim) of ``flux_compact`` (flux.F90:125-150)."""
+
+    def __init__(self, handle, dim, ntype, wind, bfac):
+        super().__init__(handle, dim, ntype, False)
+        self.wind = wind
+        self.bfac = bfac
+
+    def line(self, f: np.ndarray) -> np.ndarray:
+        """f holds f(-5..dim+5); returns the dim+2 interface values fh(-1..dim)."""
+        f = np.ascontiguousarray(f, dtype=np.float64)
+        assert f.shape == (self.dim + 1 + 2 * HM,)
+        out = np.zeros(self.dim + 2)
+        lib().orc_flux_line(self._h, _dp(f), _dp(out))
+        return out
+
+    def apply3d(self, f: np.ndarray, direction: int, lbound=(0, 0, 0)) -> np.ndarray:
+        """Every line of a Fortran-ordered f(l0:, l1:, l2:[, nfields]) along ``direction``; the output
+        spans -1..dim along that direction (dim+2 planes), the input's extents elsewhere."""
+        f = np.asfortranarray(f, dtype=np.float64)
+        nf = f.shape[3] if f.ndim == 4 else 1
+        shape = np.array(f.shape[:3], dtype=np.int64)
+        lb = np.array(lbound, dtype=np.int64)
+        oshape = list(f.shape)
+        oshape[direction] = self.dim + 2
+        out = np.zeros(oshape, order="F")
+        lib().orc_flux3d(self._h, direction, _dp(f), shape.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)),
+                         lb.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), nf, _dp(out))
+        return out
+
+
+def compact_flux_initiate(ntype: int, dim: int, wind: str = "+", bfac: float = 0.0, scheme: int = 543) -> FluxScheme:
+    """flux.F90:32-112; ``wind`` is '+' (upwind-biased) or '-' (downwind-biased)."""
+    w = {"+": 1, "-": -1}[wind]
+    h = lib().orc_flux_create(scheme, ntype, dim, w, bfac)
+    if not h:
+        raise ValueError(f"flux scheme not defined: {scheme}, ntype {ntype}")
+    return FluxScheme(h, dim, ntype, w, bfac)
 
 
 @dataclass

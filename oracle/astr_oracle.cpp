@@ -40,6 +40,13 @@ constexpr double num7d9 = 7.0 / 9.0;
 constexpr double num1d36 = 1.0 / 36.0;
 constexpr double num1d60 = 1.0 / 60.0;
 constexpr double num1d12 = 1.0 / 12.0;
+constexpr double num1d6 = 1.0 / 6.0;
+constexpr double num1d18 = 1.0 / 18.0;
+constexpr double num19d18 = 19.0 / 18.0;
+constexpr double num5d9 = 5.0 / 9.0;
+constexpr double num9d36 = 9.0 / 36.0;
+constexpr double num2d15 = 2.0 / 15.0;
+constexpr double num37d60 = 37.0 / 60.0;
 
 // ---------------------------------------------------------------- compact_scheme (commtype.F90:13-23)
 struct Scheme {
@@ -52,6 +59,10 @@ struct Scheme {
   // filter coefficients carried by the scheme (filter.F90:17-20 keeps them module-global)
   double coef6i[4], coef8i[5], coef10i[6], coefb[5][9], coefh[5][11];
   int n() const { return last_node - first_node + 1; }
+  // compact interface flux (flux.F90): wind '+' (upwind-biased) or '-', and the MP-LD b factor
+  bool is_flux = false;
+  int wind = 1;
+  double bfac = 0.0;
 };
 
 // tridiagonal_thomas_proprocess, commfunc.F90:752-774
@@ -193,6 +204,87 @@ void df_line(const Scheme& s, const double* f, double* df, double* scratch) {
   compact_fd_rhs(s, f, d);
   thomas_solve(s, d, xx);
   for (int i = 0; i <= s.dimension; ++i) df[i] = xx[i - s.first_node];
+}
+
+// ---------------------------------------------------------------- compact interface flux
+// compact_flux_initiate, flux.F90:32-112: the '543' compact interface scheme, rows i_0..i_m with
+// i_0 = -1 (ntype 1, 4) or -2 (2, 3) and i_m = dim+1 (1, 3) or dim (2, 4); interior a, c biased
+// by the wind and blended by bfac; explicit central rows at interfaces, 3rd-order rows at
+// physical ends.
+bool compact_flux_initiate(Scheme& s, int scheme, int ntype, int dim, int wind, double bfac) {
+  int i0, imx;
+  switch (ntype) {
+    case 1: i0 = -1; imx = dim + 1; break;
+    case 2: i0 = -2; imx = dim;     break;
+    case 3: i0 = -2; imx = dim + 1; break;
+    case 4: i0 = -1; imx = dim;     break;
+    default: return false;
+  }
+  s.first_node = i0; s.last_node = imx; s.dimension = dim; s.nbctype = ntype;
+  s.is_flux = true; s.wind = wind; s.bfac = bfac;
+  const int n = s.n();
+  s.a.assign(n, 0.0); s.c.assign(n, 0.0);
+  if (scheme / 100 != 5 || (wind != 1 && wind != -1)) return false;
+  for (int i = 0; i < n; ++i) {
+    if (wind == 1) { s.a[i] = 0.5 - num1d6 * bfac; s.c[i] = num1d6 + num1d6 * bfac; }
+    else { s.a[i] = num1d6 + num1d6 * bfac; s.c[i] = 0.5 - num1d6 * bfac; }
+  }
+  s.a[0] = 0.0; s.c[0] = 0.0;
+  s.a[n - 1] = 0.0; s.c[n - 1] = 0.0;
+  if (scheme != 543) return false;
+  if (ntype == 1 || ntype == 4) { s.a[0] = 2.0; s.c[0] = 2.0; s.a[1] = 0.25; s.c[1] = 0.25; }
+  if (ntype == 2 || ntype == 4) { s.a[n - 1] = 2.0; s.c[n - 1] = 2.0; s.a[n - 2] = 0.25; s.c[n - 2] = 0.25; }
+  thomas_proprocess(s);
+  return true;
+}
+
+// compact_flux_rhs, flux.F90:163-256 (f points at node 0 of f(-hm..dim+hm))
+void compact_flux_rhs(const Scheme& s, const double* f, double* d) {
+  const int i0 = s.first_node, imx = s.last_node, ntype = s.nbctype;
+  const double b = s.bfac;
+  auto D = [&](int j) -> double& { return d[j - i0]; };
+  int is = i0 + 1, ie = imx - 1;
+  if (ntype == 1 || ntype == 4) {
+    int j = i0;
+    D(j) = 2.5 * f[j + 1] + 0.5 * f[j + 2];
+    j = i0 + 1;
+    D(j) = 0.75 * f[j] + 0.75 * f[j + 1];
+    is = i0 + 2;
+  } else {
+    const int j = i0;
+    const double var1 = f[j] + f[j + 1], var2 = f[j - 1] + f[j + 2], var3 = f[j - 2] + f[j + 3];
+    D(j) = num37d60 * var1 - num2d15 * var2 + num1d60 * var3;
+  }
+  if (ntype == 2 || ntype == 4) {
+    int j = imx - 1;
+    D(j) = 0.75 * f[j + 1] + 0.75 * f[j];
+    j = imx;
+    D(j) = 2.5 * f[j] + 0.5 * f[j - 1];
+    ie = imx - 2;
+  } else {
+    const int j = imx;
+    const double var1 = f[j] + f[j + 1], var2 = f[j - 1] + f[j + 2], var3 = f[j - 2] + f[j + 3];
+    D(j) = num37d60 * var1 - num2d15 * var2 + num1d60 * var3;
+  }
+  if (s.wind == 1) {
+    for (int j = is; j <= ie; ++j)
+      D(j) = (num1d18 - num1d36 * b) * f[j - 1] + (num19d18 - num9d36 * b) * f[j] + (num5d9 + num9d36 * b) * f[j + 1] +
+             num1d36 * b * f[j + 2];
+  } else {
+    for (int j = is; j <= ie; ++j)
+      D(j) = (num1d18 - num1d36 * b) * f[j + 2] + (num19d18 - num9d36 * b) * f[j + 1] + (num5d9 + num9d36 * b) * f[j] +
+             num1d36 * b * f[j - 1];
+  }
+}
+
+// flux_compact, flux.F90:125-150: interface values fh(-1:dim) -> fh[0..dim+1]. scratch >= 2*(dim+4)
+void flux_line(const Scheme& s, const double* f, double* fh, double* scratch) {
+  const int n = s.n();
+  double* d = scratch;
+  double* xx = scratch + n;
+  compact_flux_rhs(s, f, d);
+  thomas_solve(s, d, xx);
+  for (int i = -1; i <= s.dimension; ++i) fh[i + 1] = xx[i - s.first_node];
 }
 
 // filter_coefficient_cal, filter.F90:299-432
@@ -1155,6 +1247,51 @@ void orc_deriv3d(void* h, int dir, const double* f, const int64_t* shape, const 
   Scheme* s = static_cast<Scheme*>(h);
   Box b{{shape[0], shape[1], shape[2]}, {lbound[0], lbound[1], lbound[2]}};
   apply_lines(*s, dir, f, b, nfields, out, [](const Scheme& sc, const double* fi, double* o, double* scr) { df_line(sc, fi, o, scr); });
+}
+void* orc_flux_create(int scheme, int ntype, int dim, int wind, double bfac) {
+  Scheme* s = new Scheme();
+  if (!compact_flux_initiate(*s, scheme, ntype, dim, wind, bfac)) { delete s; return nullptr; }
+  return s;
+}
+// One line: f holds f(-5..dim+5), out holds the dim+2 interface values fh(-1..dim).
+void orc_flux_line(void* h, const double* f, double* out) {
+  Scheme* s = static_cast<Scheme*>(h);
+  std::vector<double> scr(2 * (s->dimension + 8));
+  flux_line(*s, f + HM, out, scr.data());
+}
+// Every line of a Fortran-ordered multi-field array; output extent along dir is -1..dim.
+void orc_flux3d(void* h, int dir, const double* f, const int64_t* shape, const int64_t* lbound, int nfields, double* out) {
+  Scheme* s = static_cast<Scheme*>(h);
+  Box bf{{shape[0], shape[1], shape[2]}, {lbound[0], lbound[1], lbound[2]}};
+  Box bo = bf;
+  bo.n[dir] = s->dimension + 2;
+  bo.l[dir] = -1;
+  const int o1 = (dir == 0) ? 1 : 0, o2 = (dir == 2) ? 1 : 2;
+  const int dim = s->dimension;
+#pragma omp parallel
+  {
+    std::vector<double> lin(dim + 1 + 2 * HM, 0.0), lout(dim + 2), scr(2 * (dim + 8));
+#pragma omp for collapse(2) schedule(static)
+    for (int64_t b = 0; b < bf.n[o2]; ++b)
+      for (int64_t a = 0; a < bf.n[o1]; ++a) {
+        int64_t ijk[3];
+        ijk[o1] = bf.l[o1] + a;
+        ijk[o2] = bf.l[o2] + b;
+        for (int m = 0; m < nfields; ++m) {
+          for (int t = -HM; t <= dim + HM; ++t) {
+            int64_t p[3] = {ijk[0], ijk[1], ijk[2]};
+            p[dir] = t;
+            lin[t + HM] = (t >= bf.l[dir] && t < bf.l[dir] + bf.n[dir]) ? f[m * bf.size() + bf.idx(p[0], p[1], p[2])] : 0.0;
+          }
+          flux_line(*s, lin.data() + HM, lout.data(), scr.data());
+          for (int t = -1; t <= dim; ++t) {
+            int64_t p[3] = {ijk[0], ijk[1], ijk[2]};
+            p[dir] = t;
+            out[m * bo.size() + bo.idx(p[0], p[1], p[2])] = lout[t + 1];
+          }
+        }
+      }
+  }
 }
 void orc_filter3d(void* h, int dir, const double* f, const int64_t* shape, const int64_t* lbound, int nfields, double* out) {
   Scheme* s = static_cast<Scheme*>(h);

@@ -1,0 +1,118 @@
+"""The oracle's compact interface flux (compact_flux_initiate / flux_compact, flux.F90:32-256)
+against an independent numpy restatement that assembles the same tridiagonal system densely
+(row i: a_i x_{i-1} + x_i + c_i x_{i+1} = d_i, the convention of tridiagonal_thomas_proprocess,
+commfunc.F90:752-813) and solves it with LAPACK; plus the scheme's own accuracy properties.
+
+The reference carries no golden vectors for this path; its flux test (test.F90:675-870) prints
+an L2 error only, so the pin here is the second restatement and the order of accuracy."""
+import numpy as np
+import pytest
+
+import oracle
+
+HM = 5
+
+
+def _dense_flux(f, ntype, dim, wind, b):
+    """fh(-1..dim) of one line, f = f(-5..dim+5)."""
+    F = lambda j: f[j + HM]
+    i0 = -1 if ntype in (1, 4) else -2
+    im = dim if ntype in (2, 4) else dim + 1
+    n = im - i0 + 1
+    if wind == "+":
+        a = np.full(n, 0.5 - b / 6.0)
+        c = np.full(n, 1.0 / 6.0 + b / 6.0)
+    else:
+        a = np.full(n, 1.0 / 6.0 + b / 6.0)
+        c = np.full(n, 0.5 - b / 6.0)
+    a[0] = c[0] = a[-1] = c[-1] = 0.0
+    if ntype in (1, 4):
+        a[0] = c[0] = 2.0
+        a[1] = c[1] = 0.25
+    if ntype in (2, 4):
+        a[-1] = c[-1] = 2.0
+        a[-2] = c[-2] = 0.25
+    d = np.zeros(n)
+
+    def central(j):
+        return 37 / 60 * (F(j) + F(j + 1)) - 2 / 15 * (F(j - 1) + F(j + 2)) + 1 / 60 * (F(j - 2) + F(j + 3))
+
+    for r in range(n):
+        j = i0 + r
+        if wind == "+":
+            d[r] = (1 / 18 - b / 36) * F(j - 1) + (19 / 18 - 9 * b / 36) * F(j) + (5 / 9 + 9 * b / 36) * F(j + 1) \
+                + b / 36 * F(j + 2)
+        else:
+            d[r] = (1 / 18 - b / 36) * F(j + 2) + (19 / 18 - 9 * b / 36) * F(j + 1) + (5 / 9 + 9 * b / 36) * F(j) \
+                + b / 36 * F(j - 1)
+    if ntype in (1, 4):
+        d[0] = 2.5 * F(i0 + 1) + 0.5 * F(i0 + 2)
+        d[1] = 0.75 * F(i0 + 1) + 0.75 * F(i0 + 2)
+    else:
+        d[0] = central(i0)
+    if ntype in (2, 4):
+        d[-2] = 0.75 * F(im) + 0.75 * F(im - 1)
+        d[-1] = 2.5 * F(im) + 0.5 * F(im - 1)
+    else:
+        d[-1] = central(im)
+    A = np.eye(n)
+    for r in range(n):
+        if r > 0:
+            A[r, r - 1] = a[r]
+        if r < n - 1:
+            A[r, r + 1] = c[r]
+    x = np.linalg.solve(A, d)
+    return x[-1 - i0: -1 - i0 + dim + 2]
+
+
+@pytest.mark.parametrize("ntype", [1, 2, 3, 4])
+@pytest.mark.parametrize("wind", ["+", "-"])
+@pytest.mark.parametrize("bfac", [0.0, 1.0, 0.37])
+def test_oracle_flux_matches_dense_restatement(ntype, wind, bfac):
+    dim = 40
+    rng = np.random.default_rng(100 * ntype + int(10 * bfac) + (wind == "-"))
+    f = rng.standard_normal(dim + 1 + 2 * HM)
+    s = oracle.compact_flux_initiate(ntype, dim, wind, bfac)
+    got = s.line(f)
+    ref = _dense_flux(f, ntype, dim, wind, bfac)
+    assert got.shape == (dim + 2,)
+    assert np.abs(got - ref).max() <= 1e-13 * np.abs(ref).max()
+
+
+def test_oracle_flux_rejects_other_schemes():
+    with pytest.raises(ValueError):
+        oracle.compact_flux_initiate(3, 32, "+", 0.0, scheme=553)
+
+
+@pytest.mark.parametrize("wind", ["+", "-"])
+def test_oracle_flux_periodic_is_exact_on_cubic_cell_averages(wind):
+    """Interface values reconstructed from cell averages: a periodic line of cubic cell averages
+    gives the cubic's interface values to rounding (the interior scheme is 5th order)."""
+    dim = 48
+    s = oracle.compact_flux_initiate(3, dim, wind, 1.0)
+    t = np.arange(-HM, dim + HM + 1, dtype=float)
+    c = (1.0, 0.3, 0.01, 5e-4)
+    f = c[0] + c[1] * t + c[2] * (t * t + 1 / 12) + c[3] * (t ** 3 + t / 4)
+    xi = np.arange(-1, dim + 1) + 0.5
+    ex = c[0] + c[1] * xi + c[2] * xi ** 2 + c[3] * xi ** 3
+    assert np.abs(s.line(f) - ex).max() <= 1e-12
+
+
+@pytest.mark.parametrize("bfac,order", [(0.0, 5), (1.0, 6)])
+def test_oracle_flux_difference_converges(bfac, order):
+    """The conservative finite-difference derivative (fh(i) - fh(i-1))/dx of sin on a periodic
+    line (point values in, as in the reference's flux test) converges in the middle of the line
+    at 5th order for b = 0 (the upwind compact scheme) and 6th order for b = 1 (the MP-LD blend),
+    for both winds."""
+    errs = []
+    for n in (64, 128):
+        dx = 2 * np.pi / n
+        x = dx * np.arange(-HM, n + HM + 1)
+        f = np.sin(x)
+        e = 0.0
+        for wind in "+-":
+            fh = oracle.compact_flux_initiate(3, n, wind, bfac).line(f)
+            d = (fh[1:] - fh[:-1]) / dx
+            e = max(e, np.abs(d - np.cos(x[HM:HM + n + 1]))[n // 4: 3 * n // 4].max())
+        errs.append(e)
+    assert errs[0] / errs[1] > 2 ** (order - 0.2)
