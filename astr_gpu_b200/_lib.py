@@ -28,7 +28,8 @@ _d = ctypes.c_double
 class AstrParams(ctypes.Structure):
     _fields_ = [("im", _i), ("jm", _i), ("km", _i), ("mach", _d), ("reynolds", _d), ("prandtl", _d),
                 ("gamma", _d), ("ref_tem", _d), ("sutherland", _d), ("alfa_filter", _d), ("beta_halo", _d),
-                ("beta_bound", _d), ("filter_on", _i), ("ntype", _i * 3), ("twall", _d)]
+                ("beta_bound", _d), ("filter_on", _i), ("ntype", _i * 3), ("twall", _d),
+                ("conschm", _i), ("bfacmpld", _d)]
 
 
 SIGNATURES = {

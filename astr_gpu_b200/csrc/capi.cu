@@ -671,6 +671,8 @@ int astr_state_create(astr_ctx* ctx, const astr_params* p, astr_state** out) {
   for (int d = 0; d < 3; ++d)
     if (p->ntype[d] != 0 && p->ntype[d] != 3)
       return fail(ctx, ASTR_ERR_UNSUPPORTED, "the miniapp step is periodic: non-periodic boxes run in the full-solver mode (astr_full_create)");
+  if (p->conschm != 0 && p->conschm != 643)
+    return fail(ctx, ASTR_ERR_UNSUPPORTED, "the miniapp step is central (643): the upwind compact flux runs in the full-solver mode (astr_full_create)");
   astr_state* st = new astr_state();
   st->ctx = ctx;
   st->p = *p;

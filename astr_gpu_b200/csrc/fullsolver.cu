@@ -17,6 +17,13 @@
 // sequence of small pointwise kernels and line-operator launches (lines.cu) over those arrays,
 // one operation of the reference at a time. The metrics of the uniform grid are taken in closed
 // form: dxi = diag(1/dx, 1/dy, 1/dz), jacob = dx*dy*dz; the off-diagonal terms add zeros.
+//
+// Convection is the central compact scheme (convrsdcal6) or, with conschm 543, the upwind
+// compact interface flux of convrsdcmp (src/solver.F90:1272-1938) without the characteristic
+// decomposition: Steger-Warming splitting (src/riemann.F90:23-161) on the line's range, the
+// compact flux of each split part (flux_uw/flux_dw, src/flux.F90:125-150), the MP limiter at
+// every interface (shock = .true. with no Ducros sensor, crinod .false.), and the flux
+// difference added to qrhs.
 #include <cmath>
 #include <new>
 #include <string>
@@ -53,6 +60,7 @@ struct FsGeo {
 struct FsThermo {
   double const2, const5, const6, reynolds, prandtl, tc, tc1;
   double twall;    // isothermal no-slip walls at the physical ends
+  double mach, gamma;
 };
 
 // Node (i, j, k) of the flat index p over the box [lo[a], hi[a]] on each axis.
@@ -114,33 +122,49 @@ __global__ void k_fs_halo(double* F, int nf, int dir, FsGeo g) {
   }
 }
 
-// qswap along dir (one thread per line): the halo copy of q, the average of nodes 0 and N, and
-// q2fvar on the nodes -hm..0 and N..N+hm of the line (parallel.F90:4877-5060).
-__global__ void k_fs_qswap(double* q, double* rho, double* vel, double* prs, double* tmp, int dir, FsGeo g,
-                           FsThermo th) {
+// qswap along dir (parallel.F90:4877-5060), first part: per line and field, the halo copy of q
+// (thread kk = 1..hm: q(-kk) = q(N-kk), q(N+kk) = q(kk)) and the average of nodes 0 and N (thread
+// kk = 0). The copies read nodes 1..hm and N-hm..N-1 only, which no thread writes.
+__global__ void k_fs_qswap(double* q, int dir, FsGeo g) {
   const Box3 b = box_line(g, dir, 0, 0);
   const int N = g.N[dir];
   const int64_t sd = g.s[dir];
-  GRID_STRIDE(p, b.size()) {
+  const int64_t per_line = 5 * (HMW + 1);
+  GRID_STRIDE(p, b.size() * per_line) {
+    const int64_t line = p / per_line;
+    const int r = (int)(p - line * per_line);
+    const int m = r / (HMW + 1), kk = r - m * (HMW + 1);
     int i, j, k;
-    b.node(p, i, j, k);
-    const int64_t o0 = g.at(i, j, k);   // node 0 of the line (index along dir is 0)
-    for (int m = 0; m < 5; ++m) {
-      double* f = q + m * g.fs + o0;
-      for (int kk = 1; kk <= HMW; ++kk) {
-        f[-kk * sd] = f[(int64_t)(N - kk) * sd];
-        f[(int64_t)(N + kk) * sd] = f[(int64_t)kk * sd];
-      }
-      f[0] = 0.5 * (f[0] + f[(int64_t)N * sd]);
-      f[(int64_t)N * sd] = f[0];
+    b.node(line, i, j, k);
+    double* f = q + m * g.fs + g.at(i, j, k);   // node 0 of the line
+    if (kk == 0) {
+      const double avg = 0.5 * (f[0] + f[(int64_t)N * sd]);
+      f[0] = avg;
+      f[(int64_t)N * sd] = avg;
+    } else {
+      f[-kk * sd] = f[(int64_t)(N - kk) * sd];
+      f[(int64_t)(N + kk) * sd] = f[(int64_t)kk * sd];
     }
-    for (int t = -HMW; t <= N + HMW; ++t) {
-      if (t > 0 && t < N) { t = N - 1; continue; }
-      const int64_t o = o0 + (int64_t)t * sd;
-      double r, u, v, w, pr, tt;
-      fs_q2fvar(th, q[o], q[g.fs + o], q[2 * g.fs + o], q[3 * g.fs + o], q[4 * g.fs + o], r, u, v, w, pr, tt);
-      rho[o] = r; vel[o] = u; vel[g.fs + o] = v; vel[2 * g.fs + o] = w; prs[o] = pr; tmp[o] = tt;
-    }
+  }
+}
+
+// qswap, second part: q2fvar on the nodes -hm..0 and N..N+hm of every line along dir.
+__global__ void k_fs_qswap_prims(const double* q, double* rho, double* vel, double* prs, double* tmp, int dir,
+                                 FsGeo g, FsThermo th) {
+  const Box3 b = box_line(g, dir, 0, 0);
+  const int N = g.N[dir];
+  const int64_t sd = g.s[dir];
+  const int per_line = 2 * (HMW + 1);
+  GRID_STRIDE(p, b.size() * per_line) {
+    const int64_t line = p / per_line;
+    const int r = (int)(p - line * per_line);
+    const int t = r <= HMW ? r - HMW : N + (r - HMW - 1);   // -hm..0, then N..N+hm
+    int i, j, k;
+    b.node(line, i, j, k);
+    const int64_t o = g.at(i, j, k) + (int64_t)t * sd;
+    double rr, u, v, w, pr, tt;
+    fs_q2fvar(th, q[o], q[g.fs + o], q[2 * g.fs + o], q[3 * g.fs + o], q[4 * g.fs + o], rr, u, v, w, pr, tt);
+    rho[o] = rr; vel[o] = u; vel[g.fs + o] = v; vel[2 * g.fs + o] = w; prs[o] = pr; tmp[o] = tt;
   }
 }
 
@@ -186,6 +210,154 @@ __global__ void k_fs_conv_flux(double* F, const double* q, const double* vel, co
       F[m * g.fs + o] = (m - 1 == dir) ? jb * (qm * uu + dxi * pr) : jb * (qm * uu);
     }
     F[4 * g.fs + o] = jb * (q[4 * g.fs + o] + pr) * uu;
+  }
+}
+
+// flux_steger_warming of one node (riemann.F90:23-161, non-reacting) for the metric row
+// dxi e_dir: uu = dxi u_dir, the sound speed sqrt(T)/M (sos, fludyna.F90:832-859), eigenvalues
+// (uu, uu, uu, uu + c dxi, uu - c dxi) split with the entropy fix eps = 0.04. The operations
+// follow the reference's order with the zero metric components left out (they add zeros).
+__device__ __forceinline__ void fs_sw_split(const FsThermo& th, int dir, double dxi, double jb, double r, const double* u,
+                                            double p, double t, const double* qq, double* fp, double* fm) {
+  const double eps = 0.04;
+  const double uu = dxi * u[dir];
+  const double var0 = 1.0 / sqrt(dxi * dxi);
+  const double gpd = dxi * var0;                 // the dir component; the others are zero
+  const double gm2 = 0.5 / th.gamma;
+  const double css = sqrt(t) / th.mach;
+  const double csa = css / var0;
+  const double lmach = uu / csa;
+  const double lmda[5] = {uu, uu, uu, uu + csa, uu - csa};
+  double lp[5], lm[5];
+#pragma unroll
+  for (int k = 0; k < 5; ++k) {
+    lp[k] = 0.5 * (lmda[k] + sqrt(lmda[k] * lmda[k] + eps * eps));
+    lm[k] = lmda[k] - lp[k];
+  }
+  if (lmach >= 1.0 || lmach <= -1.0) {
+    double* f = lmach >= 1.0 ? fp : fm;
+    double* z = lmach >= 1.0 ? fm : fp;
+    f[0] = jb * qq[0] * uu;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) f[1 + c] = (c == dir) ? jb * (qq[1 + c] * uu + dxi * p) : jb * (qq[1 + c] * uu);
+    f[4] = jb * (qq[4] + p) * uu;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) z[k] = 0.0;
+    return;
+  }
+  const double fhi = 0.5 * (th.gamma - 1.0) * (u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
+  const double jro = jb * r;
+#pragma unroll
+  for (int side = 0; side < 2; ++side) {
+    const double* l = side == 0 ? lp : lm;
+    double* f = side == 0 ? fp : fm;
+    const double var1 = l[0];
+    const double var2 = l[3] - l[4];
+    const double var3 = 2.0 * l[0] - l[3] - l[4];
+    const double var4 = var1 - var3 * gm2;
+    f[0] = jro * var4;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) f[1 + c] = (c == dir) ? jro * (var4 * u[c] + var2 * css * gpd * gm2) : jro * (var4 * u[c]);
+    f[4] = jb * (var1 * qq[4] + r * (var2 * uu * var0 * css * gm2 - var3 * (fhi + css * css) * gm2 / (th.gamma - 1.0)));
+  }
+}
+
+// The split fluxes along dir on the nodes iss..iee of every line (solver.F90:1333-1345); the
+// rest of the line stays zero (never read).
+__global__ void k_fs_sw_split(double* fsp, double* fsm, const double* q, const double* rho, const double* vel,
+                              const double* prs, const double* tmp, int dir, int iss, int iee, FsGeo g, FsThermo th) {
+  const Box3 b = box_line(g, dir, iss, iee);
+  const double dxi = g.rd[dir], jb = g.jac;
+  const int64_t fs = g.fs;
+  GRID_STRIDE(p, b.size()) {
+    int i, j, k;
+    b.node(p, i, j, k);
+    const int64_t o = g.at(i, j, k);
+    const double u[3] = {vel[o], vel[fs + o], vel[2 * fs + o]};
+    const double qq[5] = {q[o], q[fs + o], q[2 * fs + o], q[3 * fs + o], q[4 * fs + o]};
+    double fp[5], fm[5];
+    fs_sw_split(th, dir, dxi, jb, rho[o], u, prs[o], tmp[o], qq, fp, fm);
+#pragma unroll
+    for (int m = 0; m < 5; ++m) {
+      fsp[m * fs + o] = fp[m];
+      fsm[m * fs + o] = fm[m];
+    }
+  }
+}
+
+__device__ __forceinline__ double fs_minmod2(double a, double b) {   // commfunc.F90:699-714
+  if (a > 0.0 && b > 0.0) return fmin(fabs(a), fabs(b));
+  if (a < 0.0 && b < 0.0) return -1.0 * fmin(fabs(a), fabs(b));
+  return 0.0;
+}
+__device__ __forceinline__ double fs_minmod4(double a, double b, double c, double d) {   // commfunc.F90:722-738
+  if (a > 0.0 && b > 0.0 && c > 0.0 && d > 0.0) return fmin(fmin(fmin(fabs(a), fabs(b)), fabs(c)), fabs(d));
+  if (a < 0.0 && b < 0.0 && c < 0.0 && d < 0.0) return -1.0 * fmin(fmin(fmin(fabs(a), fabs(b)), fabs(c)), fabs(d));
+  return 0.0;
+}
+// MP5 with the compact value as the linear value and discont = .true. (flux.F90:434-496)
+__device__ __forceinline__ double fs_mp5(const double* u, double ul) {
+  double var1 = u[3] - u[2];
+  double var2 = 4.0 * (u[2] - u[1]);
+  const double ump = u[2] + fs_minmod2(var1, var2);
+  var1 = (ul - u[2]) * (ul - ump);
+  if (!(var1 >= 1.0e-10)) return ul;
+  const double dm1 = u[0] - 2.0 * u[1] + u[2];
+  const double d0 = u[1] - 2.0 * u[2] + u[3];
+  const double d1 = u[2] - 2.0 * u[3] + u[4];
+  const double dhm1 = fs_minmod4(4.0 * dm1 - d0, 4.0 * d0 - dm1, dm1, d0);
+  const double dh0 = fs_minmod4(4.0 * d0 - d1, 4.0 * d1 - d0, d0, d1);
+  const double uul = u[2] + 4.0 * (u[2] - u[1]);
+  const double uav = 0.5 * (u[2] + u[3]);
+  const double umd = uav - 0.5 * dh0;
+  const double ulc = u[2] + 0.5 * (u[2] - u[1]) + 1.333333333333333 * dhm1;
+  const double umin = fmax(fmin(fmin(u[2], u[3]), umd), fmin(fmin(u[2], uul), ulc));
+  const double umax = fmin(fmax(fmax(u[2], u[3]), umd), fmax(fmax(u[2], uul), ulc));
+  return ul + fs_minmod2(umin - ul, umax - ul);
+}
+// mplimiter (flux.F90:363-379): the compact value at the two interfaces next to a block's
+// physical end for ntype 1 or 2 only, MP5 elsewhere.
+__device__ __forceinline__ double fs_mplimiter(const double* f, double fl, int inode, int dim, int nt) {
+  if ((nt == 1 && (inode == 0 || inode == 1)) || (nt == 2 && (inode == dim - 1 || inode == dim - 2))) return fl;
+  return fs_mp5(f, fl);
+}
+
+// Interface flux Fh(i) = mplimiter(+) + mplimiter(-) of field m at interface i of the line whose
+// node 0 is at o0 (solver.F90:1423-1478 with no characteristic decomposition): the stencils of
+// iwind6 (solver.F90:1237-1258), clamped to iss..iee.
+__device__ __forceinline__ double fs_interface(const double* fsp, const double* fsm, const double* fhp,
+                                               const double* fhm, int64_t o0, int64_t sd, int i, int dim, int nt,
+                                               int iss, int iee) {
+  double up[5], um[5];
+#pragma unroll
+  for (int n = 1; n <= 5; ++n) {
+    const int jp = min(max(i + n - 3, iss), iee);
+    const int jm = min(max(i + 4 - n, iss), iee);
+    up[n - 1] = fsp[o0 + (int64_t)jp * sd];
+    um[n - 1] = fsm[o0 + (int64_t)jm * sd];
+  }
+  const double v1 = fs_mplimiter(up, fhp[o0 + (int64_t)i * sd], i, dim, nt);
+  const double v2 = fs_mplimiter(um, fhm[o0 + (int64_t)i * sd], i, dim, nt);
+  return v1 + v2;
+}
+
+// qrhs(i) = qrhs(i) + Fh(i) - Fh(i-1) at nodes 0..N of every line (solver.F90:1509-1513)
+__global__ void k_fs_mp_update(double* qrhs, const double* fsp, const double* fsm, const double* fhp,
+                               const double* fhm, int dir, int nt, int iss, int iee, FsGeo g) {
+  const Box3 b = box_line(g, -1, 0, 0);
+  const int64_t sd = g.s[dir];
+  const int dim = g.N[dir];
+  GRID_STRIDE(p, b.size() * 5) {
+    const int m = (int)(p / b.size());
+    int i, j, k;
+    b.node(p - (int64_t)m * b.size(), i, j, k);
+    const int idx[3] = {i, j, k};
+    const int t = idx[dir];
+    const int64_t o = m * g.fs + g.at(i, j, k);
+    const int64_t o0 = o - (int64_t)t * sd;   // node 0 of the line, field m
+    const double fh1 = fs_interface(fsp, fsm, fhp, fhm, o0, sd, t, dim, nt, iss, iee);
+    const double fh0 = fs_interface(fsp, fsm, fhp, fhm, o0, sd, t - 1, dim, nt, iss, iee);
+    qrhs[o] = qrhs[o] + fh1 - fh0;
   }
 }
 
@@ -350,13 +522,14 @@ struct astr_full {
   double *q = nullptr, *qt = nullptr, *rho = nullptr, *vel = nullptr, *prs = nullptr, *tmp = nullptr;
   double *qsave = nullptr, *qrhs = nullptr, *dvel = nullptr, *dtmp = nullptr, *sigma = nullptr, *qflux = nullptr;
   double* work = nullptr;   // flux lines of one direction (5 fields)
+  double* up = nullptr;     // upwind convection: split fluxes f+ f- and their compact fluxes (20 fields)
   double* partials = nullptr;
   int nparts = 0;
   double* hist = nullptr;
   int* counter = nullptr;
   int hist_cap = 1 << 16;
-  HostOp hd[3], hf[3];
-  DevOp dd[3], df[3];
+  HostOp hd[3], hf[3], hfu[3], hfd[3];
+  DevOp dd[3], df[3], dfu[3], dfd[3];
   int nstep = 0;
   double time = 0.0;
   std::vector<double> row_key;
@@ -406,6 +579,40 @@ cudaError_t line_op(astr_full* fs, const DevOp& op, int dir, double* in, double*
   return launch_line_api(op, dir, fp, fa, op_, oa, nf, scale, astr_ctx_stream(fs->ctx), add);
 }
 
+// fh (interfaces -1..N along dir, nodes 0..N elsewhere) = the compact flux of in along dir
+cudaError_t flux_op(astr_full* fs, const DevOp& op, int dir, double* in, double* out, int nf) {
+  ArrDesc fa, oa;
+  double* fp = view(fs, in, dir, fa);
+  double* op_ = view(fs, out, -1, oa);
+  oa.lb[dir] = -1;
+  oa.n[dir] = fs->g.N[dir] + 2;
+  op_ -= fs->g.s[dir];   // the descriptor is relative to node -1 along dir
+  return launch_line_api(op, dir, fp, fa, op_, oa, nf, 1.0, astr_ctx_stream(fs->ctx), 0);
+}
+
+// convrsdcmp without the characteristic decomposition, every direction (see the file header)
+cudaError_t fs_convection_upwind(astr_full* fs) {
+  cudaStream_t st = astr_ctx_stream(fs->ctx);
+  const FsGeo& g = fs->g;
+  const int64_t nn = (int64_t)(g.N[0] + 1) * (g.N[1] + 1) * (g.N[2] + 1);
+  double *fsp = fs->up, *fsm = fs->up + 5 * g.fs, *fhp = fs->up + 10 * g.fs, *fhm = fs->up + 15 * g.fs;
+  cudaError_t e;
+  for (int d = 0; d < 3; ++d) {
+    const int nt = g.ntype[d];
+    const int iss = (nt == 1 || nt == 4) ? 0 : -HMW;
+    const int iee = (nt == 2 || nt == 4) ? g.N[d] : g.N[d] + HMW;
+    const int64_t nl = nn / (g.N[d] + 1) * (iee - iss + 1);
+    k_fs_sw_split<<<blocks_for(nl), 256, 0, st>>>(fsp, fsm, fs->q, fs->rho, fs->vel, fs->prs, fs->tmp, d, iss, iee, g,
+                                                  fs->th);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if ((e = flux_op(fs, fs->dfu[d], d, fsp, fhp, 5)) != cudaSuccess) return e;
+    if ((e = flux_op(fs, fs->dfd[d], d, fsm, fhm, 5)) != cudaSuccess) return e;
+    k_fs_mp_update<<<blocks_for(5 * nn), 256, 0, st>>>(fs->qrhs, fsp, fsm, fhp, fhm, d, nt, iss, iee, g);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
 cudaError_t fs_halo(astr_full* fs, double* F, int nf, int dir) {
   const int64_t n = (int64_t)nf * HMW * (fs->g.N[0] + 1) * (fs->g.N[1] + 1) * (fs->g.N[2] + 1) / (fs->g.N[dir] + 1);
   k_fs_halo<<<blocks_for(n), 256, 0, astr_ctx_stream(fs->ctx)>>>(F, nf, dir, fs->g);
@@ -440,7 +647,10 @@ cudaError_t fs_stage_rhs(astr_full* fs, bool diag) {
   for (int d = 0; d < 3; ++d) {
     if (g.ntype[d] != 3) continue;   // one rank, non-periodic: nothing to exchange
     const int64_t nl = nn / (g.N[d] + 1);
-    k_fs_qswap<<<blocks_for(nl), 256, 0, st>>>(fs->q, fs->rho, fs->vel, fs->prs, fs->tmp, d, g, fs->th);
+    k_fs_qswap<<<blocks_for(nl * 5 * (HMW + 1)), 256, 0, st>>>(fs->q, d, g);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    k_fs_qswap_prims<<<blocks_for(nl * 2 * (HMW + 1)), 256, 0, st>>>(fs->q, fs->rho, fs->vel, fs->prs, fs->tmp, d, g,
+                                                                     fs->th);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
   }
   // gradcal
@@ -448,12 +658,16 @@ cudaError_t fs_stage_rhs(astr_full* fs, bool diag) {
     if ((e = line_op(fs, fs->dd[d], d, fs->vel, fs->dvel + 3 * d * g.fs, 3, g.rd[d], 0)) != cudaSuccess) return e;
     if ((e = line_op(fs, fs->dd[d], d, fs->tmp, fs->dtmp + d * g.fs, 1, g.rd[d], 0)) != cudaSuccess) return e;
   }
-  // convrsdcal6
-  for (int d = 0; d < 3; ++d) {
-    const int64_t nl = nn / (g.N[d] + 1) * (g.N[d] + 1 + 2 * HMW);
-    k_fs_conv_flux<<<blocks_for(nl), 256, 0, st>>>(fs->work, fs->q, fs->vel, fs->prs, d, g);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    if ((e = line_op(fs, fs->dd[d], d, fs->work, fs->qrhs, 5, 1.0, 1)) != cudaSuccess) return e;
+  if (fs->up) {
+    if ((e = fs_convection_upwind(fs)) != cudaSuccess) return e;
+  } else {
+    // convrsdcal6
+    for (int d = 0; d < 3; ++d) {
+      const int64_t nl = nn / (g.N[d] + 1) * (g.N[d] + 1 + 2 * HMW);
+      k_fs_conv_flux<<<blocks_for(nl), 256, 0, st>>>(fs->work, fs->q, fs->vel, fs->prs, d, g);
+      if ((e = cudaGetLastError()) != cudaSuccess) return e;
+      if ((e = line_op(fs, fs->dd[d], d, fs->work, fs->qrhs, 5, 1.0, 1)) != cudaSuccess) return e;
+    }
   }
   k_fs_negate<<<blocks_for(5 * nn), 256, 0, st>>>(fs->qrhs, g);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
@@ -561,6 +775,14 @@ int astr_full_create(astr_ctx* ctx, const astr_params* p, astr_full** out) {
   fs->th.tc = p->sutherland / p->ref_tem;
   fs->th.tc1 = 1.0 + fs->th.tc;
   fs->th.twall = p->twall;
+  fs->th.mach = p->mach;
+  fs->th.gamma = p->gamma;
+  const bool upwind = p->conschm == 543;
+  if (p->conschm != 0 && p->conschm != 643 && !upwind) {
+    delete fs;
+    astr_ctx_set_error(ctx, "conschm must be 0 or 643 (central compact) or 543 (upwind compact flux)");
+    return ASTR_ERR_ARG;
+  }
   for (int d = 0; d < 3; ++d) {
     build_fd_op(fs->hd[d], "643c", g.ntype[d], N[d]);
     build_filter_op(fs->hf[d], g.ntype[d], N[d], p->alfa_filter, p->beta_halo, p->beta_bound, false);
@@ -572,9 +794,20 @@ int astr_full_create(astr_ctx* ctx, const astr_params* p, astr_full** out) {
       astr_ctx_set_error(ctx, "scheme tables");
       return ASTR_ERR_CUDA;
     }
+    if (upwind) {
+      build_flux_op(fs->hfu[d], 543, g.ntype[d], N[d], 1, p->bfacmpld);
+      build_flux_op(fs->hfd[d], 543, g.ntype[d], N[d], -1, p->bfacmpld);
+      const Layout Lf = pick_layout(fs->hfu[d].nsys());
+      if (make_devop(fs->hfu[d], Lf, fs->dfu[d]) != cudaSuccess || make_devop(fs->hfd[d], Lf, fs->dfd[d]) != cudaSuccess) {
+        astr_full_destroy(fs);
+        astr_ctx_set_error(ctx, "scheme tables");
+        return ASTR_ERR_CUDA;
+      }
+    }
   }
   // q(5) qt(5) rho vel(3) prs tmp qsave(5) qrhs(5) dvel(9) dtmp(3) sigma(6) qflux(3) work(5)
-  const size_t nf = 52;
+  // [+ f+ f- fh+ fh- (20) for the upwind convection]
+  const size_t nf = upwind ? 72 : 52;
   if (cudaMalloc(&fs->buf, nf * (size_t)g.fs * sizeof(double)) != cudaSuccess) {
     astr_full_destroy(fs);
     astr_ctx_set_error(ctx, "full-solver state allocation");
@@ -587,6 +820,7 @@ int astr_full_create(astr_ctx* ctx, const astr_params* p, astr_full** out) {
   fs->q = take(5); fs->qt = take(5); fs->rho = take(1); fs->vel = take(3); fs->prs = take(1); fs->tmp = take(1);
   fs->qsave = take(5); fs->qrhs = take(5); fs->dvel = take(9); fs->dtmp = take(3); fs->sigma = take(6);
   fs->qflux = take(3); fs->work = take(5);
+  if (upwind) fs->up = take(20);
   fs->nparts = 148 * 4;
   if (cudaMalloc(&fs->partials, (size_t)fs->nparts * 3 * sizeof(double)) != cudaSuccess ||
       cudaMalloc(&fs->hist, (size_t)fs->hist_cap * 3 * sizeof(double)) != cudaSuccess ||
@@ -605,7 +839,9 @@ int astr_full_destroy(astr_full* fs) {
   if (!fs) return ASTR_ERR_ARG;
   const OnDev on(astr_ctx_device(fs->ctx));
   cudaStreamSynchronize(astr_ctx_stream(fs->ctx));
-  for (int d = 0; d < 3; ++d) { free_devop(fs->dd[d]); free_devop(fs->df[d]); }
+  for (int d = 0; d < 3; ++d) {
+    free_devop(fs->dd[d]); free_devop(fs->df[d]); free_devop(fs->dfu[d]); free_devop(fs->dfd[d]);
+  }
   if (fs->buf) cudaFree(fs->buf);
   if (fs->partials) cudaFree(fs->partials);
   if (fs->hist) cudaFree(fs->hist);

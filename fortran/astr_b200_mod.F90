@@ -17,6 +17,8 @@ module astr_b200
     integer(c_int) :: filter_on
     integer(c_int) :: ntype(3)
     real(c_double) :: twall
+    integer(c_int) :: conschm
+    real(c_double) :: bfacmpld
   end type astr_params
 
   interface

@@ -71,6 +71,11 @@ typedef struct {
   int ntype[3];            /* per direction: 0 or 3 periodic; 1, 2, 4 physical ends (full-solver
                               mode only: fd_scheme_initiate's ntype, compact boundary closures) */
   double twall;            /* temperature of the isothermal no-slip walls at physical ends (bctype 41) */
+  int conschm;             /* convection scheme of the full-solver mode: 0 or 643 the central compact
+                              scheme (convrsdcal6); 543 the upwind compact interface flux with
+                              Steger-Warming splitting and the MP limiter (convrsdcmp, no
+                              characteristic decomposition). The miniapp step is central only. */
+  double bfacmpld;         /* b factor of the upwind compact flux (bfacmpld of the input) */
 } astr_params;
 
 /* ---- context ------------------------------------------------------------------------ */

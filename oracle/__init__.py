@@ -64,6 +64,7 @@ def lib():
             "orc_tgv_steps": (None, [vp, i]),
             "orc_tgv_steps_full": (None, [vp, i]),
             "orc_tgv_set_boundaries": (None, [vp, i, i, i, d]),
+            "orc_tgv_set_convection": (i, [vp, i, d]),
             "orc_tgv_rhs_full": (None, [vp, dp]),
             "orc_tgv_history": (i, [vp, dp, i]),
             "orc_tgv_history_compensated": (i, [vp, dp, i]),
@@ -203,6 +204,8 @@ class FlowParams:
     filter_on: bool = True
     ntype: tuple = (3, 3, 3)      # per direction: 3 periodic; 1, 2, 4 physical ends (full-solver mode)
     twall: float = 1.0            # isothermal no-slip walls at the physical ends (bctype 41)
+    conschm: int = 643            # full-solver convection: 643 central compact, 543 upwind compact flux
+    bfacmpld: float = 0.0         # b factor of the upwind compact flux (bfacmpld of the input)
 
 
 class TGVOracle:
@@ -217,6 +220,9 @@ class TGVOracle:
                                        int(p.filter_on))
         if tuple(p.ntype) != (3, 3, 3):
             lib().orc_tgv_set_boundaries(self._h, *[int(t) for t in p.ntype], float(p.twall))
+        if p.conschm != 643:
+            if lib().orc_tgv_set_convection(self._h, int(p.conschm), float(p.bfacmpld)) != 0:
+                raise ValueError(f"convection scheme not defined: {p.conschm}")
 
     def __del__(self):
         if getattr(self, "_h", None) and _lib is not None:

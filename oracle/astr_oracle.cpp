@@ -551,6 +551,11 @@ struct TGV {
   double twall = 1.0;
   double alfa_f = 0.49, beta_h = 1.11, beta_b = 0.98;
   bool periodic(int d) const { return ntype[d] == 3; }
+  // convection scheme of the full-solver mode: 643 central compact (convrsdcal6) or 543 the
+  // upwind compact flux (convrsdcmp without characteristic decomposition), with its b factor
+  int conschm = 643;
+  double bfacmpld = 0.0;
+  Scheme fuw[3], fdw[3];
   Field3 q, rho, prs, tmp, vel, qrhs, dvel, dtmp, sigma, qflux, qsave;
   std::vector<double> hist;   // rows of (nstep, time, tke, enst, diss)
   std::vector<double> hist_c; // the same rows with compensated sums
@@ -1060,10 +1065,171 @@ struct TGV {
     }
   }
 
+  // ---- upwind compact convection: convrsdcmp (src/solver.F90:1272-1938) with lchardecomp off.
+  // Without the characteristic decomposition no Ducros sensor runs, so lshock stays unallocated
+  // (shock = .true. at every interface, solver.F90:1440-1455); crinod is .false. everywhere
+  // (mainloop.F90:80), so every interface goes through the MP limiter.
+
+  // flux_steger_warming of one node (riemann.F90:23-161, the non-reacting branch) with the metric
+  // row m = dxi(dir, :) and sos = sqrt(T)/M (fludyna.F90:832-859, nondimensional).
+  void sw_split(double r, const double* u, double p, double t, const double* qq, const double* m, double jb,
+                double* fp, double* fm) const {
+    const double eps = 0.04;
+    const double uu = m[0] * u[0] + m[1] * u[1] + m[2] * u[2];
+    const double var0 = 1.0 / std::sqrt(m[0] * m[0] + m[1] * m[1] + m[2] * m[2]);
+    const double gpd[3] = {m[0] * var0, m[1] * var0, m[2] * var0};
+    const double gm2 = 0.5 / gamma;
+    const double css = std::sqrt(t) / mach;
+    const double csa = css / var0;
+    const double lmach = uu / csa;
+    const double lmda[5] = {uu, uu, uu, uu + csa, uu - csa};
+    double lp[5], lm[5];
+    for (int k = 0; k < 5; ++k) {
+      lp[k] = 0.5 * (lmda[k] + std::sqrt(lmda[k] * lmda[k] + eps * eps));
+      lm[k] = lmda[k] - lp[k];
+    }
+    if (lmach >= 1.0 || lmach <= -1.0) {
+      double* f = lmach >= 1.0 ? fp : fm;
+      double* z = lmach >= 1.0 ? fm : fp;
+      f[0] = jb * qq[0] * uu;
+      f[1] = jb * (qq[1] * uu + m[0] * p);
+      f[2] = jb * (qq[2] * uu + m[1] * p);
+      f[3] = jb * (qq[3] * uu + m[2] * p);
+      f[4] = jb * (qq[4] + p) * uu;
+      for (int k = 0; k < 5; ++k) z[k] = 0.0;
+      return;
+    }
+    const double fhi = 0.5 * (gamma - 1.0) * (u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
+    const double jro = jb * r;
+    for (int side = 0; side < 2; ++side) {
+      const double* l = side == 0 ? lp : lm;
+      double* f = side == 0 ? fp : fm;
+      const double var1 = l[0];
+      const double var2 = l[3] - l[4];
+      const double var3 = 2.0 * l[0] - l[3] - l[4];
+      const double var4 = var1 - var3 * gm2;
+      f[0] = jro * var4;
+      f[1] = jro * (var4 * u[0] + var2 * css * gpd[0] * gm2);
+      f[2] = jro * (var4 * u[1] + var2 * css * gpd[1] * gm2);
+      f[3] = jro * (var4 * u[2] + var2 * css * gpd[2] * gm2);
+      f[4] = jb * (var1 * qq[4] + r * (var2 * uu * var0 * css * gm2 - var3 * (fhi + css * css) * gm2 / (gamma - 1.0)));
+    }
+  }
+
+  static double minmod2(double a, double b) {   // commfunc.F90:699-714
+    if (a > 0.0 && b > 0.0) return std::min(std::fabs(a), std::fabs(b));
+    if (a < 0.0 && b < 0.0) return -1.0 * std::min(std::fabs(a), std::fabs(b));
+    return 0.0;
+  }
+  static double minmod4(double a, double b, double c, double d) {   // commfunc.F90:722-738
+    if (a > 0.0 && b > 0.0 && c > 0.0 && d > 0.0)
+      return std::min(std::min(std::min(std::fabs(a), std::fabs(b)), std::fabs(c)), std::fabs(d));
+    if (a < 0.0 && b < 0.0 && c < 0.0 && d < 0.0)
+      return -1.0 * std::min(std::min(std::min(std::fabs(a), std::fabs(b)), std::fabs(c)), std::fabs(d));
+    return 0.0;
+  }
+  // MP5 with the compact value as the linear value and discont = .true. (flux.F90:434-496)
+  static double mp5(const double* u, double ul) {
+    double var1 = u[3] - u[2];
+    double var2 = 4.0 * (u[2] - u[1]);
+    const double ump = u[2] + minmod2(var1, var2);
+    var1 = (ul - u[2]) * (ul - ump);
+    if (!(var1 >= 1.0e-10)) return ul;
+    const double dm1 = u[0] - 2.0 * u[1] + u[2];
+    const double d0 = u[1] - 2.0 * u[2] + u[3];
+    const double d1 = u[2] - 2.0 * u[3] + u[4];
+    const double dhm1 = minmod4(4.0 * dm1 - d0, 4.0 * d0 - dm1, dm1, d0);
+    const double dh0 = minmod4(4.0 * d0 - d1, 4.0 * d1 - d0, d0, d1);
+    const double uul = u[2] + 4.0 * (u[2] - u[1]);
+    const double uav = 0.5 * (u[2] + u[3]);
+    const double umd = uav - 0.5 * dh0;
+    const double ulc = u[2] + 0.5 * (u[2] - u[1]) + 1.333333333333333 * dhm1;
+    const double umin = std::max(std::min(std::min(u[2], u[3]), umd), std::min(std::min(u[2], uul), ulc));
+    const double umax = std::min(std::max(std::max(u[2], u[3]), umd), std::max(std::max(u[2], uul), ulc));
+    return ul + minmod2(umin - ul, umax - ul);
+  }
+  // mplimiter, flux.F90:363-379: the compact value itself at the two interfaces next to a block's
+  // physical end (ntype 1 or 2 only), MP5 elsewhere
+  static double mplimiter(const double* f, double fl, int inode, int dim, int nt) {
+    if ((nt == 1 && inode == 0) || (nt == 2 && inode == dim - 1) || (nt == 1 && inode == 1) ||
+        (nt == 2 && inode == dim - 2))
+      return fl;
+    return mp5(f, fl);
+  }
+
+  void build_flux_schemes() {
+    const int dims[3] = {im, jm, km};
+    for (int d = 0; d < 3; ++d) {
+      fuw[d] = Scheme();
+      fdw[d] = Scheme();
+      if (conschm != 543) continue;
+      compact_flux_initiate(fuw[d], 543, ntype[d], dims[d], 1, bfacmpld);
+      compact_flux_initiate(fdw[d], 543, ntype[d], dims[d], -1, bfacmpld);
+    }
+  }
+
+  void fs_convection_upwind() {
+    const int dims[3] = {im, jm, km};
+    const double jb = jac();
+    for (int dir = 0; dir < 3; ++dir) {
+      const int dim = dims[dir], nt = ntype[dir];
+      const int iss = (nt == 1 || nt == 4) ? 0 : -HM;
+      const int iee = (nt == 2 || nt == 4) ? dim : dim + HM;
+      double mrow[3] = {0.0, 0.0, 0.0};
+      mrow[dir] = 1.0 / dstep(dir);
+      const int o1 = (dir == 0) ? 1 : 0, o2 = (dir == 2) ? 1 : 2;
+      const int L = dim + 1 + 2 * HM;
+#pragma omp parallel
+      {
+        std::vector<double> fsp(5 * L), fsm(5 * L), fhp(5 * (dim + 2)), fhm(5 * (dim + 2)), fh(5 * (dim + 2)),
+            scr(2 * (dim + 8));
+#pragma omp for collapse(2) schedule(static)
+        for (int b = 0; b <= dims[o2]; ++b)
+          for (int a = 0; a <= dims[o1]; ++a) {
+            int p[3];
+            p[o1] = a; p[o2] = b;
+            std::fill(fsp.begin(), fsp.end(), 0.0);
+            std::fill(fsm.begin(), fsm.end(), 0.0);
+            for (int t = iss; t <= iee; ++t) {
+              p[dir] = t;
+              const double u[3] = {vel(p[0], p[1], p[2], 0), vel(p[0], p[1], p[2], 1), vel(p[0], p[1], p[2], 2)};
+              double qq[5], fp[5], fm[5];
+              for (int m = 0; m < 5; ++m) qq[m] = q(p[0], p[1], p[2], m);
+              sw_split(rho(p[0], p[1], p[2]), u, prs(p[0], p[1], p[2]), tmp(p[0], p[1], p[2]), qq, mrow, jb, fp, fm);
+              for (int m = 0; m < 5; ++m) { fsp[m * L + t + HM] = fp[m]; fsm[m * L + t + HM] = fm[m]; }
+            }
+            for (int m = 0; m < 5; ++m) {
+              flux_line(fuw[dir], fsp.data() + m * L + HM, fhp.data() + m * (dim + 2), scr.data());
+              flux_line(fdw[dir], fsm.data() + m * L + HM, fhm.data() + m * (dim + 2), scr.data());
+            }
+            for (int i = -1; i <= dim; ++i)
+              for (int m = 0; m < 5; ++m) {
+                double up[5], um[5];
+                for (int n = 1; n <= 5; ++n) {   // iwind6 (solver.F90:1237-1258)
+                  const int jp = std::min(std::max(i + n - 3, iss), iee);
+                  const int jm_ = std::min(std::max(i + 4 - n, iss), iee);
+                  up[n - 1] = fsp[m * L + jp + HM];
+                  um[n - 1] = fsm[m * L + jm_ + HM];
+                }
+                const double v1 = mplimiter(up, fhp[m * (dim + 2) + i + 1], i, dim, nt);
+                const double v2 = mplimiter(um, fhm[m * (dim + 2) + i + 1], i, dim, nt);
+                fh[m * (dim + 2) + i + 1] = v1 + v2;
+              }
+            for (int i = 0; i <= dim; ++i) {
+              p[dir] = i;
+              for (int m = 0; m < 5; ++m)
+                qrhs(p[0], p[1], p[2], m) = qrhs(p[0], p[1], p[2], m) + fh[m * (dim + 2) + i + 1] - fh[m * (dim + 2) + i];
+            }
+          }
+      }
+    }
+  }
+
   void fs_rhscal() {
     std::fill(qrhs.v.begin(), qrhs.v.end(), 0.0);
     fs_gradcal();
-    fs_convection();
+    if (conschm == 543) fs_convection_upwind();
+    else fs_convection();
     for (double& v : qrhs.v) v = -v;
     fs_diffusion();
   }
@@ -1154,6 +1320,16 @@ struct TGV {
       compact_filter_initiate(flt[d], nt[d], dims[d], alfa_f, false);
       filter_coefficient_cal(flt[d], alfa_f, beta_h, beta_b);
     }
+    build_flux_schemes();
+  }
+
+  // Convection scheme of the full-solver mode: 643 (central) or 543 (upwind compact flux).
+  bool set_convection(int scheme, double bfac) {
+    if (scheme != 643 && scheme != 543) return false;
+    conschm = scheme;
+    bfacmpld = bfac;
+    build_flux_schemes();
+    return true;
   }
 
   // rk3, tgvsolver.F90:994-1082, and the step counter of steploop (:944-960)
@@ -1315,6 +1491,9 @@ void orc_tgv_steps(void* h, int n) { TGV* t = static_cast<TGV*>(h); for (int s =
 void orc_tgv_set_boundaries(void* h, int n0, int n1, int n2, double twall) {
   const int nt[3] = {n0, n1, n2};
   static_cast<TGV*>(h)->set_boundaries(nt, twall);
+}
+int orc_tgv_set_convection(void* h, int scheme, double bfac) {
+  return static_cast<TGV*>(h)->set_convection(scheme, bfac) ? 0 : -1;
 }
 // Full-solver mode (time_integration_rk of the full solver, see rk3_full).
 void orc_tgv_steps_full(void* h, int n) { TGV* t = static_cast<TGV*>(h); for (int s = 0; s < n; ++s) t->rk3_full(); }
