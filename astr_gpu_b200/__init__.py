@@ -218,12 +218,14 @@ class FlowParams:
     twall: float = 1.0         # isothermal no-slip walls at the physical ends (bctype 41)
     conschm: int = 643         # convection: 643 central compact, 543 upwind compact flux (FullSolver only)
     bfacmpld: float = 0.0      # b factor of the upwind compact flux
+    lchardecomp: bool = False  # upwind flux in characteristic variables with the Ducros sensor
+    shkcrt: float = 0.01       # the Ducros sensor's threshold
 
     def c_params(self, im, jm, km):
         return AstrParams(im, jm, km, self.mach, self.reynolds, self.prandtl, self.gamma, self.ref_tem,
                           self.sutherland, self.alfa_filter, self.beta_halo, self.beta_bound, int(self.filter_on),
                           (ctypes.c_int * 3)(*[int(t) for t in self.ntype]), float(self.twall), int(self.conschm),
-                          float(self.bfacmpld))
+                          float(self.bfacmpld), int(self.lchardecomp), float(self.shkcrt))
 
 
 class TGVSolver:

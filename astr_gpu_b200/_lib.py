@@ -29,7 +29,7 @@ class AstrParams(ctypes.Structure):
     _fields_ = [("im", _i), ("jm", _i), ("km", _i), ("mach", _d), ("reynolds", _d), ("prandtl", _d),
                 ("gamma", _d), ("ref_tem", _d), ("sutherland", _d), ("alfa_filter", _d), ("beta_halo", _d),
                 ("beta_bound", _d), ("filter_on", _i), ("ntype", _i * 3), ("twall", _d),
-                ("conschm", _i), ("bfacmpld", _d)]
+                ("conschm", _i), ("bfacmpld", _d), ("lchardecomp", _i), ("shkcrt", _d)]
 
 
 SIGNATURES = {

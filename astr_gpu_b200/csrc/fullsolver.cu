@@ -295,13 +295,14 @@ __device__ __forceinline__ double fs_minmod4(double a, double b, double c, doubl
   if (a < 0.0 && b < 0.0 && c < 0.0 && d < 0.0) return -1.0 * fmin(fmin(fmin(fabs(a), fabs(b)), fabs(c)), fabs(d));
   return 0.0;
 }
-// MP5 with the compact value as the linear value and discont = .true. (flux.F90:434-496)
-__device__ __forceinline__ double fs_mp5(const double* u, double ul) {
+// MP5 with the compact value as the linear value (flux.F90:434-496); no limiting unless
+// discont (the shock flag) is set
+__device__ __forceinline__ double fs_mp5(const double* u, double ul, bool discont) {
   double var1 = u[3] - u[2];
   double var2 = 4.0 * (u[2] - u[1]);
   const double ump = u[2] + fs_minmod2(var1, var2);
   var1 = (ul - u[2]) * (ul - ump);
-  if (!(var1 >= 1.0e-10)) return ul;
+  if (!(discont && var1 >= 1.0e-10)) return ul;
   const double dm1 = u[0] - 2.0 * u[1] + u[2];
   const double d0 = u[1] - 2.0 * u[2] + u[3];
   const double d1 = u[2] - 2.0 * u[3] + u[4];
@@ -317,9 +318,9 @@ __device__ __forceinline__ double fs_mp5(const double* u, double ul) {
 }
 // mplimiter (flux.F90:363-379): the compact value at the two interfaces next to a block's
 // physical end for ntype 1 or 2 only, MP5 elsewhere.
-__device__ __forceinline__ double fs_mplimiter(const double* f, double fl, int inode, int dim, int nt) {
+__device__ __forceinline__ double fs_mplimiter(const double* f, double fl, bool shock, int inode, int dim, int nt) {
   if ((nt == 1 && (inode == 0 || inode == 1)) || (nt == 2 && (inode == dim - 1 || inode == dim - 2))) return fl;
-  return fs_mp5(f, fl);
+  return fs_mp5(f, fl, shock);
 }
 
 // Interface flux Fh(i) = mplimiter(+) + mplimiter(-) of field m at interface i of the line whose
@@ -336,9 +337,190 @@ __device__ __forceinline__ double fs_interface(const double* fsp, const double* 
     up[n - 1] = fsp[o0 + (int64_t)jp * sd];
     um[n - 1] = fsm[o0 + (int64_t)jm * sd];
   }
-  const double v1 = fs_mplimiter(up, fhp[o0 + (int64_t)i * sd], i, dim, nt);
-  const double v2 = fs_mplimiter(um, fhm[o0 + (int64_t)i * sd], i, dim, nt);
+  const double v1 = fs_mplimiter(up, fhp[o0 + (int64_t)i * sd], true, i, dim, nt);
+  const double v2 = fs_mplimiter(um, fhm[o0 + (int64_t)i * sd], true, i, dim, nt);
   return v1 + v2;
+}
+
+// chardecomp (solver.F90:1959-2163, non-reacting) of the interface between nodes a and b along
+// the metric row m: the Roe-averaged right (R) and left (L) eigenvectors, R[row][col].
+__device__ __forceinline__ void fs_chardecomp(const FsThermo& th, double rl, double pl, double el, const double* vl,
+                                              double rr, double pr, double er, const double* vr, const double* m,
+                                              double (&R)[5][5], double (&L)[5][5]) {
+  const double gamma = th.gamma;
+  const double wroe = sqrt(rl) / (sqrt(rl) + sqrt(rr));
+  const double wroe1 = 1.0 - wroe;
+  const double u1 = wroe * vl[0] + wroe1 * vr[0];
+  const double u2 = wroe * vl[1] + wroe1 * vr[1];
+  const double u3 = wroe * vl[2] + wroe1 * vr[2];
+  const double kroe = 0.5 * (u1 * u1 + u2 * u2 + u3 * u3);
+  const double hl = (el + pl) / rl;
+  const double hr = (er + pr) / rr;
+  const double hroe = wroe * hl + wroe1 * hr;
+  const double css = sqrt((gamma - 1.0) * (hroe - kroe));
+  const double rcs = 1.0 / css;
+  const double var1 = 0.5 * (m[0] + m[0]), var2 = 0.5 * (m[1] + m[1]), var3 = 0.5 * (m[2] + m[2]);
+  const double var4 = 1.0 / sqrt(var1 * var1 + var2 * var2 + var3 * var3);
+  const double g1 = var1 * var4, g2 = var2 * var4, g3 = var3 * var4;
+  const double ugp = u1 * g1 + u2 * g2 + u3 * g3;
+  const double b1 = (gamma - 1.0) / (css * css);
+  const double b2 = 1.0 + 2.0 * b1 * kroe - b1 * hroe;
+  L[0][0] = 0.5 * (b2 + ugp * rcs);
+  L[0][1] = -0.5 * (b1 * u1 + g1 * rcs);
+  L[0][2] = -0.5 * (b1 * u2 + g2 * rcs);
+  L[0][3] = -0.5 * (b1 * u3 + g3 * rcs);
+  L[0][4] = 0.5 * b1;
+  R[0][0] = 1.0; R[1][0] = u1 - css * g1; R[2][0] = u2 - css * g2; R[3][0] = u3 - css * g3; R[4][0] = hroe - ugp * css;
+  L[1][0] = 1.0 - b2; L[1][1] = b1 * u1; L[1][2] = b1 * u2; L[1][3] = b1 * u3; L[1][4] = -b1;
+  R[0][1] = 1.0; R[1][1] = u1; R[2][1] = u2; R[3][1] = u3; R[4][1] = hroe - 1.0 / b1;
+  if (fabs(var1) > 1.0e-12) {
+    const double rgp = 1.0 / g1;
+    L[2][0] = (ugp * g2 - u2) * rgp; L[2][1] = -g2; L[2][2] = (1.0 - g2 * g2) * rgp; L[2][3] = -g2 * g3 * rgp; L[2][4] = 0.0;
+    L[3][0] = (ugp * g3 - u3) * rgp; L[3][1] = -g3; L[3][2] = -g2 * g3 * rgp; L[3][3] = (1.0 - g3 * g3) * rgp; L[3][4] = 0.0;
+    R[0][2] = 0.0; R[1][2] = -g2; R[2][2] = g1; R[3][2] = 0.0; R[4][2] = u2 * g1 - u1 * g2;
+    R[0][3] = 0.0; R[1][3] = -g3; R[2][3] = 0.0; R[3][3] = g1; R[4][3] = u3 * g1 - u1 * g3;
+  } else if (fabs(var2) > 1.0e-12) {
+    const double rgp = 1.0 / g2;
+    L[2][0] = (ugp * g1 - u1) * rgp; L[2][1] = (1.0 - g1 * g1) * rgp; L[2][2] = -g1; L[2][3] = -g1 * g3 * rgp; L[2][4] = 0.0;
+    L[3][0] = (ugp * g3 - u3) * rgp; L[3][1] = -g1 * g3 * rgp; L[3][2] = -g3; L[3][3] = (1.0 - g3 * g3) * rgp; L[3][4] = 0.0;
+    R[0][2] = 0.0; R[1][2] = g2; R[2][2] = -g1; R[3][2] = 0.0; R[4][2] = u1 * g2 - u2 * g1;
+    R[0][3] = 0.0; R[1][3] = 0.0; R[2][3] = -g3; R[3][3] = g2; R[4][3] = u3 * g2 - u2 * g3;
+  } else {
+    const double rgp = 1.0 / g3;
+    L[2][0] = (ugp * g1 - u1) * rgp; L[2][1] = (1.0 - g1 * g1) * rgp; L[2][2] = -g1 * g2 * rgp; L[2][3] = -g1; L[2][4] = 0.0;
+    L[3][0] = (ugp * g2 - u2) * rgp; L[3][1] = -g1 * g2 * rgp; L[3][2] = (1.0 - g2 * g2) * rgp; L[3][3] = -g2; L[3][4] = 0.0;
+    R[0][2] = 0.0; R[1][2] = g3; R[2][2] = 0.0; R[3][2] = -g1; R[4][2] = u1 * g3 - u3 * g1;
+    R[0][3] = 0.0; R[1][3] = 0.0; R[2][3] = g3; R[3][3] = -g2; R[4][3] = u2 * g3 - u3 * g2;
+  }
+  L[4][0] = 0.5 * (b2 - ugp * rcs);
+  L[4][1] = -0.5 * (b1 * u1 - g1 * rcs);
+  L[4][2] = -0.5 * (b1 * u2 - g2 * rcs);
+  L[4][3] = -0.5 * (b1 * u3 - g3 * rcs);
+  L[4][4] = 0.5 * b1;
+  R[0][4] = 1.0; R[1][4] = u1 + css * g1; R[2][4] = u2 + css * g2; R[3][4] = u3 + css * g3; R[4][4] = hroe + ugp * css;
+}
+
+// ducrossensor, first part (commcal.F90:224-269): ssf on nodes 0..N from the velocity gradients
+// (dvel field n + 3d = du_n/dx_d) and the normalised second differences of p; neighbours clamped
+// at physical ends for ntype 1 (low) and 2 (high) only, as the reference does.
+__global__ void k_fs_ssf(double* ssf, const double* dvel, const double* prs, FsGeo g) {
+  const Box3 b = box_line(g, -1, 0, 0);
+  const int64_t fs = g.fs;
+  GRID_STRIDE(p, b.size()) {
+    int i, j, k;
+    b.node(p, i, j, k);
+    const int64_t o = g.at(i, j, k);
+    const double div = dvel[o] + dvel[4 * fs + o] + dvel[8 * fs + o];
+    const double div2 = div * div;
+    const double vx = dvel[5 * fs + o] - dvel[7 * fs + o];
+    const double vy = dvel[6 * fs + o] - dvel[2 * fs + o];
+    const double vz = dvel[1 * fs + o] - dvel[3 * fs + o];
+    const double vort = vx * vx + vy * vy + vz * vz;
+    const int idx[3] = {i, j, k};
+    double dmax = 0.0;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      int lo = -1, hi = 1;
+      if (g.ntype[d] == 1 && idx[d] - 1 < 0) lo = 0;
+      if (g.ntype[d] == 2 && idx[d] + 1 > g.N[d]) hi = 0;
+      const double p0 = prs[o], pp = prs[o + hi * g.s[d]], pm = prs[o + lo * g.s[d]];
+      const double dd = fabs(pp - 2.0 * p0 + pm) / (pp + 2.0 * p0 + pm);
+      dmax = d == 0 ? dd : fmax(dmax, dd);
+    }
+    ssf[o] = div2 / (div2 + vort + 1.0e-30) * dmax;
+  }
+}
+
+// ducrossensor, second part (commcal.F90:273-318): lshock (1 or 0) on nodes 0..N, the largest ssf
+// over the 10-node stencils i-4..i+5 along each axis above shkcrt.
+__global__ void k_fs_lshock(double* lsh, const double* ssf, double shkcrt, FsGeo g) {
+  const Box3 b = box_line(g, -1, 0, 0);
+  GRID_STRIDE(p, b.size()) {
+    int i, j, k;
+    b.node(p, i, j, k);
+    const int64_t o = g.at(i, j, k);
+    const int idx[3] = {i, j, k};
+    double mx = 0.0;
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+      for (int off = -HMW + 1; off <= HMW; ++off) {
+        int t = idx[d] + off;
+        if (g.ntype[d] == 1 && t < 0) t = 0;
+        if (g.ntype[d] == 2 && t > g.N[d]) t = g.N[d];
+        mx = fmax(mx, ssf[o + (int64_t)(t - idx[d]) * g.s[d]]);
+      }
+    lsh[o] = mx > shkcrt ? 1.0 : 0.0;
+  }
+}
+
+// Interface fluxes of convrsdcmp with the characteristic decomposition (solver.F90:1359-1495):
+// one thread per interface i = -1..N of a line, all five components: the split fluxes of the
+// iwind6 stencils and the compact fluxes projected on the left eigenvectors, the MP limiter in
+// characteristic variables with the interface's shock flag, back by the right eigenvectors.
+// Fh(i) is stored at node i of the layout (work fields).
+__global__ void k_fs_char_flux(double* Fh, const double* fsp, const double* fsm, const double* fhp, const double* fhm,
+                               const double* q, const double* rho, const double* vel, const double* prs,
+                               const double* lsh, int dir, int nt, int iss, int iee, FsGeo g, FsThermo th) {
+  const int N = g.N[dir];
+  const Box3 b = box_line(g, dir, -1, N);
+  const int64_t sd = g.s[dir], fs = g.fs;
+  double mrow[3] = {0.0, 0.0, 0.0};
+  mrow[dir] = g.rd[dir];
+  GRID_STRIDE(p, b.size()) {
+    int i, j, k;
+    b.node(p, i, j, k);
+    const int idx[3] = {i, j, k};
+    const int t = idx[dir];
+    const int64_t oa = g.at(i, j, k), ob = oa + sd;
+    const int64_t o0 = oa - (int64_t)t * sd;
+    bool shock;
+    if (t < 0) shock = lsh[ob] != 0.0;
+    else if (t + 1 > N) shock = lsh[oa] != 0.0;
+    else shock = lsh[oa] != 0.0 || lsh[ob] != 0.0;
+    const double vl[3] = {vel[oa], vel[fs + oa], vel[2 * fs + oa]};
+    const double vr[3] = {vel[ob], vel[fs + ob], vel[2 * fs + ob]};
+    double R[5][5], L[5][5];
+    fs_chardecomp(th, rho[oa], prs[oa], q[4 * fs + oa], vl, rho[ob], prs[ob], q[4 * fs + ob], vr, mrow, R, L);
+    int64_t jp[5], jn[5];
+#pragma unroll
+    for (int n = 1; n <= 5; ++n) {
+      jp[n - 1] = o0 + (int64_t)min(max(t + n - 3, iss), iee) * sd;
+      jn[n - 1] = o0 + (int64_t)min(max(t + 4 - n, iss), iee) * sd;
+    }
+    double fhc[5];
+#pragma unroll
+    for (int m = 0; m < 5; ++m) {
+      double up[5], um[5];
+#pragma unroll
+      for (int n = 0; n < 5; ++n) {
+        up[n] = L[m][0] * fsp[jp[n]] + L[m][1] * fsp[fs + jp[n]] + L[m][2] * fsp[2 * fs + jp[n]] +
+                L[m][3] * fsp[3 * fs + jp[n]] + L[m][4] * fsp[4 * fs + jp[n]];
+        um[n] = L[m][0] * fsm[jn[n]] + L[m][1] * fsm[fs + jn[n]] + L[m][2] * fsm[2 * fs + jn[n]] +
+                L[m][3] * fsm[3 * fs + jn[n]] + L[m][4] * fsm[4 * fs + jn[n]];
+      }
+      const double hp = L[m][0] * fhp[oa] + L[m][1] * fhp[fs + oa] + L[m][2] * fhp[2 * fs + oa] +
+                        L[m][3] * fhp[3 * fs + oa] + L[m][4] * fhp[4 * fs + oa];
+      const double hm = L[m][0] * fhm[oa] + L[m][1] * fhm[fs + oa] + L[m][2] * fhm[2 * fs + oa] +
+                        L[m][3] * fhm[3 * fs + oa] + L[m][4] * fhm[4 * fs + oa];
+      fhc[m] = fs_mplimiter(up, hp, shock, t, N, nt) + fs_mplimiter(um, hm, shock, t, N, nt);
+    }
+#pragma unroll
+    for (int m = 0; m < 5; ++m)
+      Fh[m * fs + oa] = R[m][0] * fhc[0] + R[m][1] * fhc[1] + R[m][2] * fhc[2] + R[m][3] * fhc[3] + R[m][4] * fhc[4];
+  }
+}
+
+// qrhs(i) = qrhs(i) + Fh(i) - Fh(i-1) at nodes 0..N, Fh stored per interface (solver.F90:1509-1513)
+__global__ void k_fs_flux_diff(double* qrhs, const double* Fh, int dir, FsGeo g) {
+  const Box3 b = box_line(g, -1, 0, 0);
+  const int64_t sd = g.s[dir];
+  GRID_STRIDE(p, b.size() * 5) {
+    const int m = (int)(p / b.size());
+    int i, j, k;
+    b.node(p - (int64_t)m * b.size(), i, j, k);
+    const int64_t o = m * g.fs + g.at(i, j, k);
+    qrhs[o] = qrhs[o] + Fh[o] - Fh[o - sd];
+  }
 }
 
 // qrhs(i) = qrhs(i) + Fh(i) - Fh(i-1) at nodes 0..N of every line (solver.F90:1509-1513)
@@ -522,7 +704,7 @@ struct astr_full {
   double *q = nullptr, *qt = nullptr, *rho = nullptr, *vel = nullptr, *prs = nullptr, *tmp = nullptr;
   double *qsave = nullptr, *qrhs = nullptr, *dvel = nullptr, *dtmp = nullptr, *sigma = nullptr, *qflux = nullptr;
   double* work = nullptr;   // flux lines of one direction (5 fields)
-  double* up = nullptr;     // upwind convection: split fluxes f+ f- and their compact fluxes (20 fields)
+  double* up = nullptr;     // upwind convection: split fluxes f+ f-, their compact fluxes, ssf, lshock (22)
   double* partials = nullptr;
   int nparts = 0;
   double* hist = nullptr;
@@ -590,13 +772,25 @@ cudaError_t flux_op(astr_full* fs, const DevOp& op, int dir, double* in, double*
   return launch_line_api(op, dir, fp, fa, op_, oa, nf, 1.0, astr_ctx_stream(fs->ctx), 0);
 }
 
-// convrsdcmp without the characteristic decomposition, every direction (see the file header)
+cudaError_t fs_halo(astr_full* fs, double* F, int nf, int dir);
+
+// convrsdcmp, every direction (see the file header); with the characteristic decomposition the
+// Ducros sensor runs first (ducrossensor, called by rhscal before convrsdcmp, solver.F90:228-231)
 cudaError_t fs_convection_upwind(astr_full* fs) {
   cudaStream_t st = astr_ctx_stream(fs->ctx);
   const FsGeo& g = fs->g;
   const int64_t nn = (int64_t)(g.N[0] + 1) * (g.N[1] + 1) * (g.N[2] + 1);
   double *fsp = fs->up, *fsm = fs->up + 5 * g.fs, *fhp = fs->up + 10 * g.fs, *fhm = fs->up + 15 * g.fs;
+  double *ssf = fs->up + 20 * g.fs, *lsh = fs->up + 21 * g.fs;
   cudaError_t e;
+  if (fs->p.lchardecomp) {
+    k_fs_ssf<<<blocks_for(nn), 256, 0, st>>>(ssf, fs->dvel, fs->prs, g);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    for (int d = 0; d < 3; ++d)
+      if (g.ntype[d] == 3 && (e = fs_halo(fs, ssf, 1, d)) != cudaSuccess) return e;
+    k_fs_lshock<<<blocks_for(nn), 256, 0, st>>>(lsh, ssf, fs->p.shkcrt, g);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  }
   for (int d = 0; d < 3; ++d) {
     const int nt = g.ntype[d];
     const int iss = (nt == 1 || nt == 4) ? 0 : -HMW;
@@ -607,7 +801,15 @@ cudaError_t fs_convection_upwind(astr_full* fs) {
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     if ((e = flux_op(fs, fs->dfu[d], d, fsp, fhp, 5)) != cudaSuccess) return e;
     if ((e = flux_op(fs, fs->dfd[d], d, fsm, fhm, 5)) != cudaSuccess) return e;
-    k_fs_mp_update<<<blocks_for(5 * nn), 256, 0, st>>>(fs->qrhs, fsp, fsm, fhp, fhm, d, nt, iss, iee, g);
+    if (fs->p.lchardecomp) {
+      const int64_t ni = nn / (g.N[d] + 1) * (g.N[d] + 2);
+      k_fs_char_flux<<<blocks_for(ni), 256, 0, st>>>(fs->work, fsp, fsm, fhp, fhm, fs->q, fs->rho, fs->vel, fs->prs,
+                                                     lsh, d, nt, iss, iee, g, fs->th);
+      if ((e = cudaGetLastError()) != cudaSuccess) return e;
+      k_fs_flux_diff<<<blocks_for(5 * nn), 256, 0, st>>>(fs->qrhs, fs->work, d, g);
+    } else {
+      k_fs_mp_update<<<blocks_for(5 * nn), 256, 0, st>>>(fs->qrhs, fsp, fsm, fhp, fhm, d, nt, iss, iee, g);
+    }
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
   }
   return cudaSuccess;
@@ -783,6 +985,13 @@ int astr_full_create(astr_ctx* ctx, const astr_params* p, astr_full** out) {
     astr_ctx_set_error(ctx, "conschm must be 0 or 643 (central compact) or 543 (upwind compact flux)");
     return ASTR_ERR_ARG;
   }
+  if (p->lchardecomp && !upwind) fs->p.lchardecomp = 0;   // the decomposition belongs to convrsdcmp
+  if (fs->p.lchardecomp && (g.ntype[0] != 3 || g.ntype[1] != 3 || g.ntype[2] != 3)) {
+    delete fs;
+    astr_ctx_set_error(ctx, "the characteristic decomposition reads the primitives of the halo node beyond each end: "
+                            "periodic directions only on one rank");
+    return ASTR_ERR_UNSUPPORTED;
+  }
   for (int d = 0; d < 3; ++d) {
     build_fd_op(fs->hd[d], "643c", g.ntype[d], N[d]);
     build_filter_op(fs->hf[d], g.ntype[d], N[d], p->alfa_filter, p->beta_halo, p->beta_bound, false);
@@ -806,8 +1015,8 @@ int astr_full_create(astr_ctx* ctx, const astr_params* p, astr_full** out) {
     }
   }
   // q(5) qt(5) rho vel(3) prs tmp qsave(5) qrhs(5) dvel(9) dtmp(3) sigma(6) qflux(3) work(5)
-  // [+ f+ f- fh+ fh- (20) for the upwind convection]
-  const size_t nf = upwind ? 72 : 52;
+  // [+ f+ f- fh+ fh- (20), ssf and lshock (2) for the upwind convection]
+  const size_t nf = upwind ? 74 : 52;
   if (cudaMalloc(&fs->buf, nf * (size_t)g.fs * sizeof(double)) != cudaSuccess) {
     astr_full_destroy(fs);
     astr_ctx_set_error(ctx, "full-solver state allocation");
@@ -820,7 +1029,7 @@ int astr_full_create(astr_ctx* ctx, const astr_params* p, astr_full** out) {
   fs->q = take(5); fs->qt = take(5); fs->rho = take(1); fs->vel = take(3); fs->prs = take(1); fs->tmp = take(1);
   fs->qsave = take(5); fs->qrhs = take(5); fs->dvel = take(9); fs->dtmp = take(3); fs->sigma = take(6);
   fs->qflux = take(3); fs->work = take(5);
-  if (upwind) fs->up = take(20);
+  if (upwind) fs->up = take(22);
   fs->nparts = 148 * 4;
   if (cudaMalloc(&fs->partials, (size_t)fs->nparts * 3 * sizeof(double)) != cudaSuccess ||
       cudaMalloc(&fs->hist, (size_t)fs->hist_cap * 3 * sizeof(double)) != cudaSuccess ||

@@ -19,6 +19,8 @@ module astr_b200
     real(c_double) :: twall
     integer(c_int) :: conschm
     real(c_double) :: bfacmpld
+    integer(c_int) :: lchardecomp
+    real(c_double) :: shkcrt
   end type astr_params
 
   interface

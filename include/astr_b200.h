@@ -76,6 +76,10 @@ typedef struct {
                               Steger-Warming splitting and the MP limiter (convrsdcmp, no
                               characteristic decomposition). The miniapp step is central only. */
   double bfacmpld;         /* b factor of the upwind compact flux (bfacmpld of the input) */
+  int lchardecomp;         /* conschm 543: limit in characteristic variables (chardecomp, Roe
+                              averages) with the Ducros shock sensor (ducrossensor); periodic
+                              directions only */
+  double shkcrt;           /* the Ducros sensor's threshold (shkcrt of the input) */
 } astr_params;
 
 /* ---- context ------------------------------------------------------------------------ */

@@ -64,7 +64,9 @@ def lib():
             "orc_tgv_steps": (None, [vp, i]),
             "orc_tgv_steps_full": (None, [vp, i]),
             "orc_tgv_set_boundaries": (None, [vp, i, i, i, d]),
-            "orc_tgv_set_convection": (i, [vp, i, d]),
+            "orc_tgv_set_convection": (i, [vp, i, d, i, d]),
+            "orc_tgv_shock_flags": (i, [vp, ctypes.c_void_p]),
+            "orc_chardecomp": (None, [d, d, d, d, dp, d, d, d, dp, dp, dp, dp]),
             "orc_tgv_rhs_full": (None, [vp, dp]),
             "orc_tgv_history": (i, [vp, dp, i]),
             "orc_tgv_history_compensated": (i, [vp, dp, i]),
@@ -190,6 +192,16 @@ def compact_flux_initiate(ntype: int, dim: int, wind: str = "+", bfac: float = 0
     return FluxScheme(h, dim, ntype, w, bfac)
 
 
+def chardecomp(gamma, left, right, ddi):
+    """chardecomp (solver.F90:1959-2163): left/right = (rho, p, rhoE, (u, v, w)); returns (R, L)."""
+    R, L = np.zeros(25), np.zeros(25)
+    arr = lambda v: np.ascontiguousarray(v, dtype=np.float64)
+    vl, vr, dd = arr(left[3]), arr(right[3]), arr(ddi)
+    lib().orc_chardecomp(gamma, left[0], left[1], left[2], _dp(vl), right[0], right[1], right[2], _dp(vr), _dp(dd),
+                         _dp(R), _dp(L))
+    return R.reshape(5, 5), L.reshape(5, 5)
+
+
 @dataclass
 class FlowParams:
     mach: float = 0.1
@@ -206,6 +218,8 @@ class FlowParams:
     twall: float = 1.0            # isothermal no-slip walls at the physical ends (bctype 41)
     conschm: int = 643            # full-solver convection: 643 central compact, 543 upwind compact flux
     bfacmpld: float = 0.0         # b factor of the upwind compact flux (bfacmpld of the input)
+    lchardecomp: bool = False     # upwind flux in characteristic variables, with the Ducros sensor
+    shkcrt: float = 0.01          # the Ducros sensor's threshold
 
 
 class TGVOracle:
@@ -221,7 +235,8 @@ class TGVOracle:
         if tuple(p.ntype) != (3, 3, 3):
             lib().orc_tgv_set_boundaries(self._h, *[int(t) for t in p.ntype], float(p.twall))
         if p.conschm != 643:
-            if lib().orc_tgv_set_convection(self._h, int(p.conschm), float(p.bfacmpld)) != 0:
+            if lib().orc_tgv_set_convection(self._h, int(p.conschm), float(p.bfacmpld), int(p.lchardecomp),
+                                            float(p.shkcrt)) != 0:
                 raise ValueError(f"convection scheme not defined: {p.conschm}")
 
     def __del__(self):
@@ -267,6 +282,12 @@ class TGVOracle:
         lib().orc_tgv_rhs_full(self._h, _dp(out))
         return out
 
+    def shock_flags(self) -> np.ndarray:
+        """The Ducros sensor's shock flags of the last full-solver rhscal (characteristic mode)."""
+        out = np.zeros(self.shape, dtype=np.uint8, order="F")
+        if lib().orc_tgv_shock_flags(self._h, out.ctypes.data) != 0:
+            raise ValueError("no shock flags: the characteristic decomposition is off")
+        return out.astype(bool)
     def history(self, compensated: bool = False) -> np.ndarray:
         """Rows of (nstep, time, tke, enstrophy, dissipation), one per step (stacal). The sums run
         over the nodes in the reference's sequential order; with ``compensated`` the same per-node

@@ -555,6 +555,11 @@ struct TGV {
   // upwind compact flux (convrsdcmp without characteristic decomposition), with its b factor
   int conschm = 643;
   double bfacmpld = 0.0;
+  // characteristic decomposition of convrsdcmp (lchardecomp) with the Ducros sensor's threshold
+  bool lchardecomp = false;
+  double shkcrt = 0.0;
+  Field3 ssf;                  // Ducros sensor (allocated with the decomposition)
+  std::vector<char> lshock;    // shock flag on nodes 0..N
   Scheme fuw[3], fdw[3];
   Field3 q, rho, prs, tmp, vel, qrhs, dvel, dtmp, sigma, qflux, qsave;
   std::vector<double> hist;   // rows of (nstep, time, tke, enst, diss)
@@ -1128,13 +1133,14 @@ struct TGV {
       return -1.0 * std::min(std::min(std::min(std::fabs(a), std::fabs(b)), std::fabs(c)), std::fabs(d));
     return 0.0;
   }
-  // MP5 with the compact value as the linear value and discont = .true. (flux.F90:434-496)
-  static double mp5(const double* u, double ul) {
+  // MP5 with the compact value as the linear value (flux.F90:434-496); no limiting unless
+  // discont (the shock flag) is set
+  static double mp5(const double* u, double ul, bool discont) {
     double var1 = u[3] - u[2];
     double var2 = 4.0 * (u[2] - u[1]);
     const double ump = u[2] + minmod2(var1, var2);
     var1 = (ul - u[2]) * (ul - ump);
-    if (!(var1 >= 1.0e-10)) return ul;
+    if (!(discont && var1 >= 1.0e-10)) return ul;
     const double dm1 = u[0] - 2.0 * u[1] + u[2];
     const double d0 = u[1] - 2.0 * u[2] + u[3];
     const double d1 = u[2] - 2.0 * u[3] + u[4];
@@ -1150,12 +1156,155 @@ struct TGV {
   }
   // mplimiter, flux.F90:363-379: the compact value itself at the two interfaces next to a block's
   // physical end (ntype 1 or 2 only), MP5 elsewhere
-  static double mplimiter(const double* f, double fl, int inode, int dim, int nt) {
+  static double mplimiter(const double* f, double fl, bool shock, int inode, int dim, int nt) {
     if ((nt == 1 && inode == 0) || (nt == 2 && inode == dim - 1) || (nt == 1 && inode == 1) ||
         (nt == 2 && inode == dim - 2))
       return fl;
-    return mp5(f, fl);
+    return mp5(f, fl, shock);
   }
+
+  // chardecomp (solver.F90:1959-2163, non-reacting): Roe-averaged right and left eigenvectors of
+  // the interface between two nodes for the metric direction ddi (the same at both nodes here).
+  void chardecomp(double tl, double rl, double pl, double el, const double* vl, double tr, double rr, double pr,
+                  double er, const double* vr, const double* ddi, double (&REV)[5][5], double (&LEV)[5][5]) const {
+    (void)tl; (void)tr;
+    const double rero = 1.0e-12;
+    const double wroe = std::sqrt(rl) / (std::sqrt(rl) + std::sqrt(rr));
+    const double wroe1 = 1.0 - wroe;
+    const double u1 = wroe * vl[0] + wroe1 * vr[0];
+    const double u2 = wroe * vl[1] + wroe1 * vr[1];
+    const double u3 = wroe * vl[2] + wroe1 * vr[2];
+    const double kroe = 0.5 * (u1 * u1 + u2 * u2 + u3 * u3);
+    const double hl = (el + pl) / rl;
+    const double hr = (er + pr) / rr;
+    const double hroe = wroe * hl + wroe1 * hr;
+    const double css = std::sqrt((gamma - 1.0) * (hroe - kroe));
+    const double rcs = 1.0 / css;
+    const double var1 = 0.5 * (ddi[0] + ddi[0]);
+    const double var2 = 0.5 * (ddi[1] + ddi[1]);
+    const double var3 = 0.5 * (ddi[2] + ddi[2]);
+    const double var4 = 1.0 / std::sqrt(var1 * var1 + var2 * var2 + var3 * var3);
+    const double g1 = var1 * var4, g2 = var2 * var4, g3 = var3 * var4;
+    const double ugp = u1 * g1 + u2 * g2 + u3 * g3;
+    const double b1 = (gamma - 1.0) / (css * css);
+    const double b2 = 1.0 + 2.0 * b1 * kroe - b1 * hroe;
+    LEV[0][0] = 0.5 * (b2 + ugp * rcs);
+    LEV[0][1] = -0.5 * (b1 * u1 + g1 * rcs);
+    LEV[0][2] = -0.5 * (b1 * u2 + g2 * rcs);
+    LEV[0][3] = -0.5 * (b1 * u3 + g3 * rcs);
+    LEV[0][4] = 0.5 * b1;
+    REV[0][0] = 1.0;
+    REV[1][0] = u1 - css * g1;
+    REV[2][0] = u2 - css * g2;
+    REV[3][0] = u3 - css * g3;
+    REV[4][0] = hroe - ugp * css;
+    LEV[1][0] = 1.0 - b2;
+    LEV[1][1] = b1 * u1;
+    LEV[1][2] = b1 * u2;
+    LEV[1][3] = b1 * u3;
+    LEV[1][4] = -b1;
+    REV[0][1] = 1.0;
+    REV[1][1] = u1;
+    REV[2][1] = u2;
+    REV[3][1] = u3;
+    REV[4][1] = hroe - 1.0 / b1;
+    if (std::fabs(var1) > rero) {
+      const double rgp = 1.0 / g1;
+      LEV[2][0] = (ugp * g2 - u2) * rgp; LEV[2][1] = -g2; LEV[2][2] = (1.0 - g2 * g2) * rgp;
+      LEV[2][3] = -g2 * g3 * rgp; LEV[2][4] = 0.0;
+      LEV[3][0] = (ugp * g3 - u3) * rgp; LEV[3][1] = -g3; LEV[3][2] = -g2 * g3 * rgp;
+      LEV[3][3] = (1.0 - g3 * g3) * rgp; LEV[3][4] = 0.0;
+      REV[0][2] = 0.0; REV[1][2] = -g2; REV[2][2] = g1; REV[3][2] = 0.0; REV[4][2] = u2 * g1 - u1 * g2;
+      REV[0][3] = 0.0; REV[1][3] = -g3; REV[2][3] = 0.0; REV[3][3] = g1; REV[4][3] = u3 * g1 - u1 * g3;
+    } else if (std::fabs(var2) > rero) {
+      const double rgp = 1.0 / g2;
+      LEV[2][0] = (ugp * g1 - u1) * rgp; LEV[2][1] = (1.0 - g1 * g1) * rgp; LEV[2][2] = -g1;
+      LEV[2][3] = -g1 * g3 * rgp; LEV[2][4] = 0.0;
+      LEV[3][0] = (ugp * g3 - u3) * rgp; LEV[3][1] = -g1 * g3 * rgp; LEV[3][2] = -g3;
+      LEV[3][3] = (1.0 - g3 * g3) * rgp; LEV[3][4] = 0.0;
+      REV[0][2] = 0.0; REV[1][2] = g2; REV[2][2] = -g1; REV[3][2] = 0.0; REV[4][2] = u1 * g2 - u2 * g1;
+      REV[0][3] = 0.0; REV[1][3] = 0.0; REV[2][3] = -g3; REV[3][3] = g2; REV[4][3] = u3 * g2 - u2 * g3;
+    } else {
+      const double rgp = 1.0 / g3;
+      LEV[2][0] = (ugp * g1 - u1) * rgp; LEV[2][1] = (1.0 - g1 * g1) * rgp; LEV[2][2] = -g1 * g2 * rgp;
+      LEV[2][3] = -g1; LEV[2][4] = 0.0;
+      LEV[3][0] = (ugp * g2 - u2) * rgp; LEV[3][1] = -g1 * g2 * rgp; LEV[3][2] = (1.0 - g2 * g2) * rgp;
+      LEV[3][3] = -g2; LEV[3][4] = 0.0;
+      REV[0][2] = 0.0; REV[1][2] = g3; REV[2][2] = 0.0; REV[3][2] = -g1; REV[4][2] = u1 * g3 - u3 * g1;
+      REV[0][3] = 0.0; REV[1][3] = 0.0; REV[2][3] = g3; REV[3][3] = -g2; REV[4][3] = u2 * g3 - u3 * g2;
+    }
+    LEV[4][0] = 0.5 * (b2 - ugp * rcs);
+    LEV[4][1] = -0.5 * (b1 * u1 - g1 * rcs);
+    LEV[4][2] = -0.5 * (b1 * u2 - g2 * rcs);
+    LEV[4][3] = -0.5 * (b1 * u3 - g3 * rcs);
+    LEV[4][4] = 0.5 * b1;
+    REV[0][4] = 1.0;
+    REV[1][4] = u1 + css * g1;
+    REV[2][4] = u2 + css * g2;
+    REV[3][4] = u3 + css * g3;
+    REV[4][4] = hroe + ugp * css;
+  }
+
+  // ducrossensor (commcal.F90:196-353): ssf = div^2/(div^2 + |omega|^2 + 1e-30) times the largest
+  // normalised second difference of p, the periodic halo swap of ssf, then lshock = the maximum
+  // of ssf over the 10-node stencils i-4..i+5 along each axis exceeds shkcrt. Neighbours are
+  // clamped at physical ends only for ntype 1 (low) and 2 (high), as the reference does.
+  void ducros_sensor() {
+    const int dims[3] = {im, jm, km};
+#pragma omp parallel for collapse(2)
+    for (int k = 0; k <= km; ++k)
+      for (int j = 0; j <= jm; ++j)
+        for (int i = 0; i <= im; ++i) {
+          const double div = dvel(i, j, k, 0) + dvel(i, j, k, 4) + dvel(i, j, k, 8);
+          const double div2 = div * div;
+          // dvel(i,j,k,n,d) is field n + 3 d here
+          const double vx = dvel(i, j, k, 2 + 3) - dvel(i, j, k, 1 + 6);
+          const double vy = dvel(i, j, k, 0 + 6) - dvel(i, j, k, 2 + 0);
+          const double vz = dvel(i, j, k, 1 + 0) - dvel(i, j, k, 0 + 3);
+          const double vort = vx * vx + vy * vy + vz * vz;
+          int ip = i + 1, imn = i - 1, jp = j + 1, jmn = j - 1, kp = k + 1, kmn = k - 1;
+          if (ntype[0] == 1 && imn < 0) imn = 0;
+          if (ntype[1] == 1 && jmn < 0) jmn = 0;
+          if (ntype[2] == 1 && kmn < 0) kmn = 0;
+          if (ntype[0] == 2 && ip > im) ip = im;
+          if (ntype[1] == 2 && jp > jm) jp = jm;
+          if (ntype[2] == 2 && kp > km) kp = km;
+          const double p0 = prs(i, j, k);
+          const double di = std::fabs(prs(ip, j, k) - 2.0 * p0 + prs(imn, j, k)) / (prs(ip, j, k) + 2.0 * p0 + prs(imn, j, k));
+          const double dj = std::fabs(prs(i, jp, k) - 2.0 * p0 + prs(i, jmn, k)) / (prs(i, jp, k) + 2.0 * p0 + prs(i, jmn, k));
+          const double dk = std::fabs(prs(i, j, kp) - 2.0 * p0 + prs(i, j, kmn)) / (prs(i, j, kp) + 2.0 * p0 + prs(i, j, kmn));
+          ssf(i, j, k) = div2 / (div2 + vort + 1.0e-30) * std::max(std::max(di, dj), dk);
+        }
+    for (int d = 0; d < 3; ++d)
+      if (periodic(d)) bchomovec(ssf, 1, d + 1);
+#pragma omp parallel for collapse(2)
+    for (int k = 0; k <= km; ++k)
+      for (int j = 0; j <= jm; ++j)
+        for (int i = 0; i <= im; ++i) {
+          double mx = 0.0;
+          for (int o = -HM + 1; o <= HM; ++o) {
+            int ii = i + o;
+            if (ntype[0] == 1 && ii < 0) ii = 0;
+            if (ntype[0] == 2 && ii > im) ii = im;
+            mx = std::max(mx, ssf(ii, j, k));
+          }
+          for (int o = -HM + 1; o <= HM; ++o) {
+            int jj = j + o;
+            if (ntype[1] == 1 && jj < 0) jj = 0;
+            if (ntype[1] == 2 && jj > jm) jj = jm;
+            mx = std::max(mx, ssf(i, jj, k));
+          }
+          for (int o = -HM + 1; o <= HM; ++o) {
+            int kk = k + o;
+            if (ntype[2] == 1 && kk < 0) kk = 0;
+            if (ntype[2] == 2 && kk > km) kk = km;
+            mx = std::max(mx, ssf(i, j, kk));
+          }
+          lshock[((size_t)k * (jm + 1) + j) * (im + 1) + i] = mx > shkcrt;
+        }
+    (void)dims;
+  }
+  bool shock_at(int i, int j, int k) const { return lshock[((size_t)k * (jm + 1) + j) * (im + 1) + i] != 0; }
 
   void build_flux_schemes() {
     const int dims[3] = {im, jm, km};
@@ -1202,19 +1351,70 @@ struct TGV {
               flux_line(fuw[dir], fsp.data() + m * L + HM, fhp.data() + m * (dim + 2), scr.data());
               flux_line(fdw[dir], fsm.data() + m * L + HM, fhm.data() + m * (dim + 2), scr.data());
             }
-            for (int i = -1; i <= dim; ++i)
+            for (int i = -1; i <= dim; ++i) {
+              int jp[5], jn[5];
+              for (int n = 1; n <= 5; ++n) {   // iwind6 (solver.F90:1237-1258)
+                jp[n - 1] = std::min(std::max(i + n - 3, iss), iee);
+                jn[n - 1] = std::min(std::max(i + 4 - n, iss), iee);
+              }
+              // the shock flag of the interface (solver.F90:1440-1455): both nodes' flags, or the
+              // one node inside 0..dim
+              bool lsh = true;
+              if (lchardecomp) {
+                int pa[3] = {p[0], p[1], p[2]}, pb[3] = {p[0], p[1], p[2]};
+                pa[dir] = i; pb[dir] = i + 1;
+                if (i < 0) lsh = shock_at(pb[0], pb[1], pb[2]);
+                else if (i + 1 > dim) lsh = shock_at(pa[0], pa[1], pa[2]);
+                else lsh = shock_at(pa[0], pa[1], pa[2]) || shock_at(pb[0], pb[1], pb[2]);
+              }
+              if (lchardecomp) {
+                int pa[3] = {p[0], p[1], p[2]}, pb[3] = {p[0], p[1], p[2]};
+                pa[dir] = i; pb[dir] = i + 1;
+                const double vl[3] = {vel(pa[0], pa[1], pa[2], 0), vel(pa[0], pa[1], pa[2], 1), vel(pa[0], pa[1], pa[2], 2)};
+                const double vr[3] = {vel(pb[0], pb[1], pb[2], 0), vel(pb[0], pb[1], pb[2], 1), vel(pb[0], pb[1], pb[2], 2)};
+                double REV[5][5], LEV[5][5];
+                chardecomp(tmp(pa[0], pa[1], pa[2]), rho(pa[0], pa[1], pa[2]), prs(pa[0], pa[1], pa[2]),
+                           q(pa[0], pa[1], pa[2], 4), vl, tmp(pb[0], pb[1], pb[2]), rho(pb[0], pb[1], pb[2]),
+                           prs(pb[0], pb[1], pb[2]), q(pb[0], pb[1], pb[2], 4), vr, mrow, REV, LEV);
+                double fhc[5];
+                for (int m = 0; m < 5; ++m) {
+                  double up[5], um[5];
+                  for (int n = 0; n < 5; ++n) {
+                    double sp = 0.0, sm = 0.0;
+                    sp = LEV[m][0] * fsp[0 * L + jp[n] + HM] + LEV[m][1] * fsp[1 * L + jp[n] + HM] +
+                         LEV[m][2] * fsp[2 * L + jp[n] + HM] + LEV[m][3] * fsp[3 * L + jp[n] + HM] +
+                         LEV[m][4] * fsp[4 * L + jp[n] + HM];
+                    sm = LEV[m][0] * fsm[0 * L + jn[n] + HM] + LEV[m][1] * fsm[1 * L + jn[n] + HM] +
+                         LEV[m][2] * fsm[2 * L + jn[n] + HM] + LEV[m][3] * fsm[3 * L + jn[n] + HM] +
+                         LEV[m][4] * fsm[4 * L + jn[n] + HM];
+                    up[n] = sp;
+                    um[n] = sm;
+                  }
+                  const int c = i + 1;
+                  const double hp = LEV[m][0] * fhp[0 * (dim + 2) + c] + LEV[m][1] * fhp[1 * (dim + 2) + c] +
+                                    LEV[m][2] * fhp[2 * (dim + 2) + c] + LEV[m][3] * fhp[3 * (dim + 2) + c] +
+                                    LEV[m][4] * fhp[4 * (dim + 2) + c];
+                  const double hm = LEV[m][0] * fhm[0 * (dim + 2) + c] + LEV[m][1] * fhm[1 * (dim + 2) + c] +
+                                    LEV[m][2] * fhm[2 * (dim + 2) + c] + LEV[m][3] * fhm[3 * (dim + 2) + c] +
+                                    LEV[m][4] * fhm[4 * (dim + 2) + c];
+                  fhc[m] = mplimiter(up, hp, lsh, i, dim, nt) + mplimiter(um, hm, lsh, i, dim, nt);
+                }
+                for (int m = 0; m < 5; ++m)
+                  fh[m * (dim + 2) + i + 1] = REV[m][0] * fhc[0] + REV[m][1] * fhc[1] + REV[m][2] * fhc[2] +
+                                              REV[m][3] * fhc[3] + REV[m][4] * fhc[4];
+                continue;
+              }
               for (int m = 0; m < 5; ++m) {
                 double up[5], um[5];
-                for (int n = 1; n <= 5; ++n) {   // iwind6 (solver.F90:1237-1258)
-                  const int jp = std::min(std::max(i + n - 3, iss), iee);
-                  const int jm_ = std::min(std::max(i + 4 - n, iss), iee);
-                  up[n - 1] = fsp[m * L + jp + HM];
-                  um[n - 1] = fsm[m * L + jm_ + HM];
+                for (int n = 0; n < 5; ++n) {
+                  up[n] = fsp[m * L + jp[n] + HM];
+                  um[n] = fsm[m * L + jn[n] + HM];
                 }
-                const double v1 = mplimiter(up, fhp[m * (dim + 2) + i + 1], i, dim, nt);
-                const double v2 = mplimiter(um, fhm[m * (dim + 2) + i + 1], i, dim, nt);
+                const double v1 = mplimiter(up, fhp[m * (dim + 2) + i + 1], lsh, i, dim, nt);
+                const double v2 = mplimiter(um, fhm[m * (dim + 2) + i + 1], lsh, i, dim, nt);
                 fh[m * (dim + 2) + i + 1] = v1 + v2;
               }
+            }
             for (int i = 0; i <= dim; ++i) {
               p[dir] = i;
               for (int m = 0; m < 5; ++m)
@@ -1228,8 +1428,12 @@ struct TGV {
   void fs_rhscal() {
     std::fill(qrhs.v.begin(), qrhs.v.end(), 0.0);
     fs_gradcal();
-    if (conschm == 543) fs_convection_upwind();
-    else fs_convection();
+    if (conschm == 543) {
+      if (lchardecomp) ducros_sensor();
+      fs_convection_upwind();
+    } else {
+      fs_convection();
+    }
     for (double& v : qrhs.v) v = -v;
     fs_diffusion();
   }
@@ -1324,10 +1528,16 @@ struct TGV {
   }
 
   // Convection scheme of the full-solver mode: 643 (central) or 543 (upwind compact flux).
-  bool set_convection(int scheme, double bfac) {
+  bool set_convection(int scheme, double bfac, int chardecomp_on, double shock_threshold) {
     if (scheme != 643 && scheme != 543) return false;
     conschm = scheme;
     bfacmpld = bfac;
+    lchardecomp = scheme == 543 && chardecomp_on != 0;
+    shkcrt = shock_threshold;
+    if (lchardecomp) {
+      ssf.init(im, jm, km, HM, 1);
+      lshock.assign((size_t)(im + 1) * (jm + 1) * (km + 1), 0);
+    }
     build_flux_schemes();
     return true;
   }
@@ -1492,8 +1702,25 @@ void orc_tgv_set_boundaries(void* h, int n0, int n1, int n2, double twall) {
   const int nt[3] = {n0, n1, n2};
   static_cast<TGV*>(h)->set_boundaries(nt, twall);
 }
-int orc_tgv_set_convection(void* h, int scheme, double bfac) {
-  return static_cast<TGV*>(h)->set_convection(scheme, bfac) ? 0 : -1;
+int orc_tgv_set_convection(void* h, int scheme, double bfac, int lchardecomp, double shkcrt) {
+  return static_cast<TGV*>(h)->set_convection(scheme, bfac, lchardecomp, shkcrt) ? 0 : -1;
+}
+// chardecomp of one interface (row-major R[5][5], L[5][5]) for a gas with ratio of specific heats gamma.
+void orc_chardecomp(double gamma, double rl, double pl, double el, const double* vl, double rr, double pr, double er,
+                    const double* vr, const double* ddi, double* R, double* L) {
+  TGV t;
+  t.gamma = gamma;
+  double RR[5][5], LL[5][5];
+  t.chardecomp(1.0, rl, pl, el, vl, 1.0, rr, pr, er, vr, ddi, RR, LL);
+  for (int a = 0; a < 5; ++a)
+    for (int b = 0; b < 5; ++b) { R[5 * a + b] = RR[a][b]; L[5 * a + b] = LL[a][b]; }
+}
+// The shock flags of the last rhscal with the characteristic decomposition (nodes 0..N, x fastest).
+int orc_tgv_shock_flags(void* h, unsigned char* out) {
+  TGV* t = static_cast<TGV*>(h);
+  if (!t->lchardecomp) return -1;
+  for (size_t n = 0; n < t->lshock.size(); ++n) out[n] = (unsigned char)t->lshock[n];
+  return 0;
 }
 // Full-solver mode (time_integration_rk of the full solver, see rk3_full).
 void orc_tgv_steps_full(void* h, int n) { TGV* t = static_cast<TGV*>(h); for (int s = 0; s < n; ++s) t->rk3_full(); }

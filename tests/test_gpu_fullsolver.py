@@ -251,6 +251,59 @@ def test_full_upwind_steps_match_oracle(ctx, ntype):
     s.close()
 
 
+@pytest.mark.parametrize("shkcrt", [1e-5, 0.01])
+def test_full_upwind_characteristic_rhs_matches_oracle(ctx, shkcrt):
+    """lchardecomp: the Ducros sensor (ducrossensor, commcal.F90:196-353) flags the nodes, and
+    convrsdcmp limits in characteristic variables (chardecomp's Roe-averaged eigenvectors,
+    solver.F90:1959-2163) with each interface's flag. shkcrt 1e-5 flags about 60 % of the nodes
+    of this state, 0.01 none (the limiter then never acts)."""
+    import astr_gpu_b200 as ag
+    dims = (40, 48, 36)
+    mach = 0.2
+    q = _state(dims, 19, mach)
+    kw = dict(mach=mach, reynolds=800.0, sutherland=110.3, beta_bound=0.98, conschm=543, bfacmpld=0.3,
+              lchardecomp=True, shkcrt=shkcrt)
+    o = oracle.TGVOracle(*dims, params=oracle.FlowParams(**kw))
+    o.set_q(q)
+    ref = o.rhs_full()
+    flags = o.shock_flags()
+    assert (0.3 < flags.mean() < 0.9) if shkcrt < 1e-3 else not flags.any()
+    s = ag.FullSolver(ctx, *dims, params=ag.FlowParams(**kw))
+    s.set_q(q)
+    got = s.rhs()
+    h = [2 * np.pi / n for n in dims]
+    jac, p0 = h[0] * h[1] * h[2], 1.0 / (1.4 * mach ** 2)
+    for m in range(5):
+        scale = max(np.abs(ref[..., m]).max(), jac * p0 / min(h))
+        assert np.abs(got[..., m] - ref[..., m]).max() <= 1e-12 * scale, m
+    s.close()
+
+
+def test_full_upwind_characteristic_steps_match_oracle(ctx):
+    import astr_gpu_b200 as ag
+    dims = (40, 48, 36)
+    mach = 0.2
+    q = _state(dims, 23, mach)
+    kw = dict(mach=mach, reynolds=800.0, sutherland=110.3, beta_bound=0.98, conschm=543, bfacmpld=0.1,
+              lchardecomp=True, shkcrt=1e-5)
+    o = oracle.TGVOracle(*dims, params=oracle.FlowParams(**kw))
+    o.set_q(q)
+    o.set_dt(1e-3)
+    o.steps_full(10)
+    s = ag.FullSolver(ctx, *dims, params=ag.FlowParams(**kw))
+    s.set_q(q)
+    s.step(1e-3, 10)
+    assert _rel_fields(s.get_q(), o.get_q()) <= 1e-10
+    s.close()
+
+
+def test_characteristic_mode_rejects_walls(ctx):
+    import astr_gpu_b200 as ag
+    with pytest.raises(ag.AstrError) as e:
+        ag.FullSolver(ctx, 32, params=ag.FlowParams(conschm=543, lchardecomp=True, ntype=(3, 4, 3)))
+    assert e.value.code == -4
+
+
 def test_upwind_and_central_differ_as_expected(ctx):
     """The two convection schemes are different discretisations: on a smooth Taylor-Green box the
     upwind flux with b = 1 (a symmetric 6th-order interface scheme) keeps the momentum RHS within

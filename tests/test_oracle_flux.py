@@ -116,3 +116,40 @@ def test_oracle_flux_difference_converges(bfac, order):
             e = max(e, np.abs(d - np.cos(x[HM:HM + n + 1]))[n // 4: 3 * n // 4].max())
         errs.append(e)
     assert errs[0] / errs[1] > 2 ** (order - 0.2)
+
+
+@pytest.mark.parametrize("direction", [0, 1, 2])
+def test_oracle_chardecomp_eigenvectors(direction):
+    """chardecomp's Roe-averaged eigenvectors (solver.F90:1959-2163): L is the inverse of R, and
+    L A R is diagonal with the eigenvalues (ugp - c, ugp, ugp, ugp, ugp + c) of the Roe-averaged
+    flux Jacobian A along the metric direction, for each branch of the metric test."""
+    g = 1.4
+    rng = np.random.default_rng(direction)
+    def state():
+        rho = 1.0 + 0.2 * rng.random()
+        u = rng.standard_normal(3) * 0.3
+        p = 1.0 / (g * 0.2 ** 2) * (1.0 + 0.1 * rng.random())
+        return rho, p, p / (g - 1) + 0.5 * rho * (u @ u), u
+    left, right = state(), state()
+    ddi = np.zeros(3)
+    ddi[direction] = 7.5
+    R, L = oracle.chardecomp(g, left, right, ddi)
+    assert np.abs(L @ R - np.eye(5)).max() < 1e-12
+    # the Roe-averaged Jacobian of the flux along n = ddi/|ddi|, in conserved variables
+    wl = np.sqrt(left[0]) / (np.sqrt(left[0]) + np.sqrt(right[0]))
+    u = wl * left[3] + (1 - wl) * right[3]
+    H = wl * (left[2] + left[1]) / left[0] + (1 - wl) * (right[2] + right[1]) / right[0]
+    n = ddi / np.linalg.norm(ddi)
+    un, k = u @ n, 0.5 * (u @ u)
+    c = np.sqrt((g - 1) * (H - k))
+    A = np.zeros((5, 5))
+    A[0, 1:4] = n
+    A[1:4, 0] = (g - 1) * k * n - u * un
+    A[1:4, 1:4] = np.outer(u, n) - (g - 1) * np.outer(n, u) + un * np.eye(3)
+    A[1:4, 4] = (g - 1) * n
+    A[4, 0] = ((g - 1) * k - H) * un
+    A[4, 1:4] = H * n - (g - 1) * u * un
+    A[4, 4] = g * un
+    D = L @ A @ R
+    lam = np.array([un - c, un, un, un, un + c])
+    assert np.abs(D - np.diag(lam)).max() < 1e-10 * np.abs(lam).max()
