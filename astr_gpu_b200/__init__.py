@@ -65,6 +65,11 @@ class Context:
     def synchronize(self):
         self.check(self.L.astr_synchronize(self._h))
 
+    def alive(self) -> bool:
+        """False once the context is destroyed: the objects made on it then drop their handles
+        without calling into the library (their device memory goes with the process)."""
+        return bool(getattr(self, "_h", None))
+
     def close(self):
         if getattr(self, "_h", None):
             self.L.astr_destroy(self._h)
@@ -95,7 +100,7 @@ class Scheme:
 
     def __del__(self):
         try:
-            if getattr(self, "_h", None):
+            if getattr(self, "_h", None) and self.ctx.alive():
                 self.ctx.L.astr_scheme_destroy(self._h)
                 self._h = None
         except Exception:
@@ -248,7 +253,7 @@ class TGVSolver:
         return (self.im + 1, self.jm + 1, self.km + 1)
 
     def close(self):
-        if getattr(self, "_h", None):
+        if getattr(self, "_h", None) and self.ctx.alive():
             self.ctx.L.astr_state_destroy(self._h)
             self._h = None
 
@@ -363,7 +368,7 @@ class FullSolver:
         return (self.im + 1, self.jm + 1, self.km + 1)
 
     def close(self):
-        if getattr(self, "_h", None):
+        if getattr(self, "_h", None) and self.ctx.alive():
             self.ctx.L.astr_full_destroy(self._h)
             self._h = None
 
@@ -421,7 +426,7 @@ class Ensemble:
         self.ctx.check(self.ctx.L.astr_ensemble_step(self._h, d.ctypes.data_as(_lib._dp), nsteps))
 
     def close(self):
-        if getattr(self, "_h", None):
+        if getattr(self, "_h", None) and self.ctx.alive():
             self.ctx.L.astr_ensemble_destroy(self._h)
             self._h = None
 

@@ -81,7 +81,8 @@ class Adjoint:
         return out
 
     def close(self):
-        if getattr(self, "_h", None):
+        # the adjoint reads its state's context on destruction: skip it once either is gone
+        if getattr(self, "_h", None) and self.ctx.alive() and getattr(self.solver, "_h", None):
             self.ctx.L.astr_adjoint_destroy(self._h)
             self._h = None
 

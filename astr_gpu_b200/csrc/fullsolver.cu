@@ -523,12 +523,14 @@ __global__ void k_fs_flux_diff(double* qrhs, const double* Fh, int dir, FsGeo g)
   }
 }
 
-// qrhs(i) = qrhs(i) + Fh(i) - Fh(i-1) at nodes 0..N of every line (solver.F90:1509-1513)
-__global__ void k_fs_mp_update(double* qrhs, const double* fsp, const double* fsm, const double* fhp,
-                               const double* fhm, int dir, int nt, int iss, int iee, FsGeo g) {
-  const Box3 b = box_line(g, -1, 0, 0);
+// Interface fluxes without the characteristic decomposition (solver.F90:1423-1478): one thread
+// per interface i = -1..N of a line and field, Fh(i) = mplimiter(+) + mplimiter(-) with shock =
+// .true., stored at node i of the layout (work fields).
+__global__ void k_fs_mp_flux(double* Fh, const double* fsp, const double* fsm, const double* fhp, const double* fhm,
+                             int dir, int nt, int iss, int iee, FsGeo g) {
+  const int N = g.N[dir];
+  const Box3 b = box_line(g, dir, -1, N);
   const int64_t sd = g.s[dir];
-  const int dim = g.N[dir];
   GRID_STRIDE(p, b.size() * 5) {
     const int m = (int)(p / b.size());
     int i, j, k;
@@ -536,10 +538,7 @@ __global__ void k_fs_mp_update(double* qrhs, const double* fsp, const double* fs
     const int idx[3] = {i, j, k};
     const int t = idx[dir];
     const int64_t o = m * g.fs + g.at(i, j, k);
-    const int64_t o0 = o - (int64_t)t * sd;   // node 0 of the line, field m
-    const double fh1 = fs_interface(fsp, fsm, fhp, fhm, o0, sd, t, dim, nt, iss, iee);
-    const double fh0 = fs_interface(fsp, fsm, fhp, fhm, o0, sd, t - 1, dim, nt, iss, iee);
-    qrhs[o] = qrhs[o] + fh1 - fh0;
+    Fh[o] = fs_interface(fsp, fsm, fhp, fhm, o - (int64_t)t * sd, sd, t, N, nt, iss, iee);
   }
 }
 
@@ -808,7 +807,10 @@ cudaError_t fs_convection_upwind(astr_full* fs) {
       if ((e = cudaGetLastError()) != cudaSuccess) return e;
       k_fs_flux_diff<<<blocks_for(5 * nn), 256, 0, st>>>(fs->qrhs, fs->work, d, g);
     } else {
-      k_fs_mp_update<<<blocks_for(5 * nn), 256, 0, st>>>(fs->qrhs, fsp, fsm, fhp, fhm, d, nt, iss, iee, g);
+      const int64_t ni = nn / (g.N[d] + 1) * (g.N[d] + 2);
+      k_fs_mp_flux<<<blocks_for(5 * ni), 256, 0, st>>>(fs->work, fsp, fsm, fhp, fhm, d, nt, iss, iee, g);
+      if ((e = cudaGetLastError()) != cudaSuccess) return e;
+      k_fs_flux_diff<<<blocks_for(5 * nn), 256, 0, st>>>(fs->qrhs, fs->work, d, g);
     }
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
   }

