@@ -723,7 +723,8 @@ def run_full(args, ws, rank, local):
     stream = torch.cuda.Stream(device=local)
     ctx = ag.Context(local, stream=stream)
     s = ag.FullSolver(ctx, n, params=ag.FlowParams(sutherland=110.3, beta_bound=0.98, conschm=args.conschm,
-                                                   bfacmpld=args.bfac))
+                                                   bfacmpld=args.bfac, lchardecomp=args.chardecomp,
+                                                   shkcrt=args.shkcrt))
     s.set_q(tgv_q(n, 0.1))
     dt = 1e-3
     s.step(dt, args.warmup)
@@ -741,7 +742,9 @@ def run_full(args, ws, rank, local):
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (Taylor-Green initial field)",
                 "config": {"workload": f"full-solver mode, TGV {n}^3 (filter first, qswap averaging, metric form), "
                                        f"dt {dt}, " + ("central compact convection (643)" if args.conschm != 543 else
-                                                       f"upwind compact flux convection (543, b {args.bfac})"),
+                                                       f"upwind compact flux convection (543, b {args.bfac}"
+                                                       + (f", characteristic, shkcrt {args.shkcrt})" if args.chardecomp
+                                                          else ")")),
                            "grid": n},
                 "gpu_launches": None, "clocks": clk.summary()}
         print(json.dumps(line), flush=True)
@@ -783,6 +786,8 @@ def main():
     ap.add_argument("--full-size", type=int, default=256)
     ap.add_argument("--conschm", type=int, default=643, choices=[643, 543], help="convection of --workload full")
     ap.add_argument("--bfac", type=float, default=0.3, help="b factor of the upwind compact flux (--conschm 543)")
+    ap.add_argument("--chardecomp", action="store_true", help="--conschm 543 in characteristic variables")
+    ap.add_argument("--shkcrt", type=float, default=0.01, help="Ducros sensor threshold (--chardecomp)")
     ap.add_argument("--grad-size", type=int, default=256)
     ap.add_argument("--adj-size", type=int, default=128)
     ap.add_argument("--adj-steps", type=int, default=200)
