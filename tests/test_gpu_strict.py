@@ -57,3 +57,57 @@ def test_strict_build_rhs_matches_oracle():
         ctx.close()
     print(f"rhs vs oracle, scaled: strict {errs[True]:.3e}, default {errs[False]:.3e}")
     assert errs[True] <= STRICT_TOL, errs
+
+
+@pytest.mark.parametrize("wind", ["+", "-"])
+def test_strict_build_flux_lines_match_oracle(wind):
+    """The interface flux (flux_compact, flux.F90:125-150) from the strict build: the right-hand
+    sides in the reference's order without contraction, so only the solve's rounding remains."""
+    import astr_gpu_b200 as ag
+    dim = 256
+    rng = np.random.default_rng(11)
+    f = np.asfortranarray(rng.standard_normal((dim + 11, 6, 5)))
+    ref = oracle.compact_flux_initiate(3, dim, wind, 0.3).apply3d(f, 0, lbound=(-5, 0, 0))
+    ctx = ag.Context(0, strict=True)
+    got = ag.flux_compact(ctx, ag.compact_flux_initiate(ctx, 3, dim, wind, 0.3), f, 0, lbound=(-5, 0, 0))
+    err = float(np.abs(got - ref).max() / np.abs(ref).max())
+    print(f"flux lines '{wind}', strict build: {err:.3e}")
+    assert err <= STRICT_TOL
+    ctx.close()
+
+
+def test_strict_build_upwind_rhs_matches_oracle():
+    """One full-solver stage with the upwind compact flux in characteristic variables from the
+    strict build (Steger-Warming split, Roe eigenvectors and MP limiter without contraction),
+    scaled as the upwind test of the default build (1e-14 times 1/M of each field's scale)."""
+    import astr_gpu_b200 as ag
+    dims = (40, 48, 36)
+    mach = 0.2
+    rng = np.random.default_rng(29)
+    x = [2 * np.pi * np.arange(n + 1) / n for n in dims]
+    X, Y, Z = np.meshgrid(*x, indexing="ij")
+    rho = 1.0 + 0.05 * np.sin(X + Y) * np.cos(Z)
+    u = np.sin(X) * np.cos(Y) * np.cos(Z)
+    v = -np.cos(X) * np.sin(Y) * np.cos(Z) + 0.1 * rng.standard_normal() * np.sin(X)
+    w = 0.2 * np.sin(Y + Z)
+    p = 1.0 / (1.4 * mach ** 2) + 0.1 * np.cos(2 * X)
+    q = np.zeros(tuple(n + 1 for n in dims) + (5,), order="F")
+    q[..., 0], q[..., 1], q[..., 2], q[..., 3] = rho, rho * u, rho * v, rho * w
+    q[..., 4] = p / 0.4 + 0.5 * rho * (u * u + v * v + w * w)
+    kw = dict(mach=mach, reynolds=800.0, sutherland=110.3, beta_bound=0.98, conschm=543, bfacmpld=0.3,
+              lchardecomp=True, shkcrt=1e-5)
+    o = oracle.TGVOracle(*dims, params=oracle.FlowParams(**kw))
+    o.set_q(q)
+    ref = o.rhs_full()
+    ctx = ag.Context(0, strict=True)
+    s = ag.FullSolver(ctx, *dims, params=ag.FlowParams(**kw))
+    s.set_q(q)
+    got = s.rhs()
+    s.close()
+    ctx.close()
+    h = [2 * np.pi / n for n in dims]
+    jac, p0 = h[0] * h[1] * h[2], 1.0 / (1.4 * mach ** 2)
+    err = max(float(np.abs(got[..., m] - ref[..., m]).max()) / max(np.abs(ref[..., m]).max(), jac * p0 / min(h))
+              for m in range(5))
+    print(f"upwind characteristic rhs, strict build, scaled: {err:.3e}")
+    assert err <= STRICT_TOL / mach
