@@ -6,7 +6,12 @@ metric form, the update of q*jacob, Sutherland 110.3.
 Tolerances: one stage's RHS within 1e-12 of max(|R_m|_inf, jacob p0/dx) per field (the rounding
 floor of differentiating the O(p0) pressure, p0 = 1/(gamma M^2)); the state after one stage's
 filter and averaging within 1e-13 of each field's largest value; conserved variables after the
-steps within 1e-10 of each field's largest value; diagnostics rows within 1e-12 relative."""
+steps within 1e-10 of each field's largest value; diagnostics rows within 1e-12 relative.
+
+The upwind convection (conschm 543, convrsdcmp, src/solver.F90:1272-1938: Steger-Warming split,
+compact interface flux, MP limiter, optionally in characteristic variables with the Ducros
+sensor) is checked the same way; its RHS tolerance carries a factor 1/M for the split fluxes'
+acoustic parts (see test_full_upwind_rhs_matches_oracle)."""
 import numpy as np
 import pytest
 
