@@ -67,6 +67,8 @@ def lib():
             "orc_tgv_set_convection": (i, [vp, i, d, i, d]),
             "orc_tgv_shock_flags": (i, [vp, ctypes.c_void_p]),
             "orc_chardecomp": (None, [d, d, d, d, dp, d, d, d, dp, dp, dp, dp]),
+            "orc_sw_split": (None, [d, d, d, dp, d, d, dp, dp, d, dp, dp]),
+            "orc_mp5": (d, [dp, d, i]),
             "orc_tgv_rhs_full": (None, [vp, dp]),
             "orc_tgv_history": (i, [vp, dp, i]),
             "orc_tgv_history_compensated": (i, [vp, dp, i]),
@@ -200,6 +202,24 @@ def chardecomp(gamma, left, right, ddi):
     lib().orc_chardecomp(gamma, left[0], left[1], left[2], _dp(vl), right[0], right[1], right[2], _dp(vr), _dp(dd),
                          _dp(R), _dp(L))
     return R.reshape(5, 5), L.reshape(5, 5)
+
+
+def sw_split(gamma, mach, rho, u, p, metric, jacob=1.0):
+    """flux_steger_warming (riemann.F90:23-161) of one node: returns (f+, f-)."""
+    arr = lambda v: np.ascontiguousarray(v, dtype=np.float64)
+    u = arr(u)
+    t = p / rho * gamma * mach ** 2
+    qq = arr([rho, rho * u[0], rho * u[1], rho * u[2], p / (gamma - 1) + 0.5 * rho * (u @ u)])
+    fp, fm = np.zeros(5), np.zeros(5)
+    m = arr(metric)
+    lib().orc_sw_split(gamma, mach, rho, _dp(u), p, t, _dp(qq), _dp(m), jacob, _dp(fp), _dp(fm))
+    return fp, fm
+
+
+def mp5(u, ul, discont=True):
+    """MP5 (flux.F90:434-496) of the stencil u[0..4] with the linear value ul."""
+    u = np.ascontiguousarray(u, dtype=np.float64)
+    return lib().orc_mp5(_dp(u), float(ul), int(discont))
 
 
 @dataclass

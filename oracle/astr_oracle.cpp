@@ -1705,6 +1705,16 @@ void orc_tgv_set_boundaries(void* h, int n0, int n1, int n2, double twall) {
 int orc_tgv_set_convection(void* h, int scheme, double bfac, int lchardecomp, double shkcrt) {
   return static_cast<TGV*>(h)->set_convection(scheme, bfac, lchardecomp, shkcrt) ? 0 : -1;
 }
+// flux_steger_warming of one node for a gas (gamma, mach): fp[5], fm[5].
+void orc_sw_split(double gamma, double mach, double r, const double* u, double p, double t, const double* qq,
+                  const double* metric, double jb, double* fp, double* fm) {
+  TGV tg;
+  tg.gamma = gamma;
+  tg.mach = mach;
+  tg.sw_split(r, u, p, t, qq, metric, jb, fp, fm);
+}
+// MP5 of one stencil u[5] with the linear value ul (flux.F90:434-496).
+double orc_mp5(const double* u, double ul, int discont) { return TGV::mp5(u, ul, discont != 0); }
 // chardecomp of one interface (row-major R[5][5], L[5][5]) for a gas with ratio of specific heats gamma.
 void orc_chardecomp(double gamma, double rl, double pl, double el, const double* vl, double rr, double pr, double er,
                     const double* vr, const double* ddi, double* R, double* L) {

@@ -153,3 +153,51 @@ def test_oracle_chardecomp_eigenvectors(direction):
     D = L @ A @ R
     lam = np.array([un - c, un, un, un, un + c])
     assert np.abs(D - np.diag(lam)).max() < 1e-10 * np.abs(lam).max()
+
+
+@pytest.mark.parametrize("direction", [0, 1, 2])
+def test_oracle_steger_warming_split_sums_to_the_flux(direction):
+    """flux_steger_warming (riemann.F90:23-161): f+ + f- is the Euler flux jacob*(q uu + dxi p e,
+    (E + p) uu) at subsonic and supersonic nodes, the supersonic branches put all of it on one
+    side, and f+ (f-) carries only non-negative (non-positive) eigenvalue weights: the mass
+    flux f+_1 >= 0 >= f-_1."""
+    g, mach, jb = 1.4, 0.3, 0.7
+    rng = np.random.default_rng(7 + direction)
+    metric = np.zeros(3)
+    metric[direction] = 4.0
+    for speed in (0.2, 0.9, 2.5, -2.5):   # |u| / c: subsonic, near sonic, supersonic both ways
+        rho = 1.0 + 0.3 * rng.random()
+        p = 1.0 / (g * mach ** 2) * (1.0 + 0.2 * rng.random())
+        c = np.sqrt(g * p / rho)
+        u = 0.1 * c * rng.standard_normal(3)
+        u[direction] = speed * c
+        fp, fm = oracle.sw_split(g, mach, rho, u, p, metric, jb)
+        uu = metric[direction] * u[direction]
+        E = p / (g - 1) + 0.5 * rho * (u @ u)
+        F = jb * np.array([rho * uu, rho * u[0] * uu, rho * u[1] * uu, rho * u[2] * uu, (E + p) * uu])
+        F[1 + direction] += jb * metric[direction] * p
+        assert np.abs(fp + fm - F).max() <= 1e-13 * np.abs(F).max() + 1e-13 * np.abs(fp).max()
+        if speed >= 1:
+            assert np.all(fm == 0.0)
+        elif speed <= -1:
+            assert np.all(fp == 0.0)
+        assert fp[0] >= 0.0 >= fm[0]
+
+
+def test_oracle_mp5_limiter_properties():
+    """MP5 (flux.F90:434-496) with a linear value ul: without the shock flag it returns ul; on
+    smooth monotone data ul inside the monotonicity bounds passes unchanged; an overshooting ul
+    next to a jump is pulled back to the bound u_MP = u3 + minmod(u4 - u3, 4 (u3 - u2))."""
+    u = np.array([1.0, 1.0, 1.0, 0.0, 0.0])
+    assert oracle.mp5(u, 1.7, discont=False) == 1.7
+    # smooth monotone stencil, ul from the 5th-order upwind formula: unchanged
+    x = np.arange(5) * 0.1
+    us = np.sin(x)
+    ul = (2 * us[0] - 13 * us[1] + 47 * us[2] + 27 * us[3] - 3 * us[4]) / 60
+    assert oracle.mp5(us, ul) == ul
+    # a step: an overshoot beyond u3 is clipped into [min, max] of the local data
+    ustep = np.array([0.0, 0.0, 0.0, 1.0, 1.0])
+    lim = oracle.mp5(ustep, 1.3)
+    assert 0.0 <= lim <= 1.0
+    lim = oracle.mp5(ustep, -0.2)
+    assert 0.0 <= lim <= 1.0
