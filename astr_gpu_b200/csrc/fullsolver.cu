@@ -55,7 +55,15 @@ struct FsGeo {
   __host__ __device__ int64_t at(int i, int j, int k) const {
     return (int64_t)(i + HMW) + (int64_t)(j + HMW) * s[1] + (int64_t)(k + HMW) * s[2];
   }
+  // Per-direction members by a runtime direction, as selects (an indexed read of a kernel
+  // parameter's array would move the whole parameter into local memory).
+  __host__ __device__ int n_(int d) const { return d == 0 ? N[0] : (d == 1 ? N[1] : N[2]); }
+  __host__ __device__ int64_t s_(int d) const { return d == 0 ? s[0] : (d == 1 ? s[1] : s[2]); }
+  __host__ __device__ double rd_(int d) const { return d == 0 ? rd[0] : (d == 1 ? rd[1] : rd[2]); }
 };
+
+// Coordinate d of node (i, j, k), as a select.
+__host__ __device__ __forceinline__ int coord(int d, int i, int j, int k) { return d == 0 ? i : (d == 1 ? j : k); }
 
 struct FsThermo {
   double const2, const5, const6, reynolds, prandtl, tc, tc1;
@@ -75,11 +83,14 @@ struct Box3 {
   }
 };
 
-// The box of nodes 0..N on every axis except `dir`, where it spans [a, b].
+// The box of nodes 0..N on every axis except `dir`, where it spans [a, b] (dir < 0: none).
 __host__ __device__ Box3 box_line(const FsGeo& g, int dir, int a, int b) {
   Box3 x;
-  for (int d = 0; d < 3; ++d) { x.lo[d] = 0; x.n[d] = g.N[d] + 1; }
-  if (dir >= 0) { x.lo[dir] = a; x.n[dir] = b - a + 1; }
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    x.lo[d] = (d == dir) ? a : 0;
+    x.n[d] = (d == dir) ? b - a + 1 : g.N[d] + 1;
+  }
   return x;
 }
 
@@ -100,25 +111,18 @@ __device__ __forceinline__ void fs_q2fvar(const FsThermo& th, double q0, double 
 // Periodic halo copy along dir of nf fields (dataswap / bchomovec): F(-k) = F(N-k), F(N+k) = F(k),
 // k = 1..hm, on the lines whose other indices lie in 0..N.
 __global__ void k_fs_halo(double* F, int nf, int dir, FsGeo g) {
-  const Box3 b = [&] {
-    Box3 x;
-    for (int d = 0; d < 3; ++d) { x.lo[d] = 0; x.n[d] = g.N[d] + 1; }
-    x.lo[dir] = 1; x.n[dir] = HMW;
-    return x;
-  }();
+  const Box3 b = box_line(g, dir, 1, HMW);
   const int64_t total = b.size() * nf;
-  const int N = g.N[dir];
+  const int N = g.n_(dir);
+  const int64_t sd = g.s_(dir);
   GRID_STRIDE(p, total) {
     const int m = (int)(p / b.size());
     int i, j, k;
     b.node(p - (int64_t)m * b.size(), i, j, k);
-    int lo[3] = {i, j, k}, hi[3] = {i, j, k}, slo[3] = {i, j, k}, shi[3] = {i, j, k};
-    const int kk = lo[dir];   // 1..hm
-    lo[dir] = -kk; slo[dir] = N - kk;
-    hi[dir] = N + kk; shi[dir] = kk;
-    double* f = F + m * g.fs;
-    f[g.at(lo[0], lo[1], lo[2])] = f[g.at(slo[0], slo[1], slo[2])];
-    f[g.at(hi[0], hi[1], hi[2])] = f[g.at(shi[0], shi[1], shi[2])];
+    const int kk = coord(dir, i, j, k);   // 1..hm
+    double* f = F + m * g.fs + g.at(i, j, k) - (int64_t)kk * sd;   // node 0 of the line
+    f[-(int64_t)kk * sd] = f[(int64_t)(N - kk) * sd];
+    f[(int64_t)(N + kk) * sd] = f[(int64_t)kk * sd];
   }
 }
 
@@ -127,8 +131,8 @@ __global__ void k_fs_halo(double* F, int nf, int dir, FsGeo g) {
 // kk = 0). The copies read nodes 1..hm and N-hm..N-1 only, which no thread writes.
 __global__ void k_fs_qswap(double* q, int dir, FsGeo g) {
   const Box3 b = box_line(g, dir, 0, 0);
-  const int N = g.N[dir];
-  const int64_t sd = g.s[dir];
+  const int N = g.n_(dir);
+  const int64_t sd = g.s_(dir);
   const int64_t per_line = 5 * (HMW + 1);
   GRID_STRIDE(p, b.size() * per_line) {
     const int64_t line = p / per_line;
@@ -152,8 +156,8 @@ __global__ void k_fs_qswap(double* q, int dir, FsGeo g) {
 __global__ void k_fs_qswap_prims(const double* q, double* rho, double* vel, double* prs, double* tmp, int dir,
                                  FsGeo g, FsThermo th) {
   const Box3 b = box_line(g, dir, 0, 0);
-  const int N = g.N[dir];
-  const int64_t sd = g.s[dir];
+  const int N = g.n_(dir);
+  const int64_t sd = g.s_(dir);
   const int per_line = 2 * (HMW + 1);
   GRID_STRIDE(p, b.size() * per_line) {
     const int64_t line = p / per_line;
@@ -173,9 +177,9 @@ __global__ void k_fs_qswap_prims(const double* q, double* rho, double* vel, doub
 // two nodes next to the wall, rho = p/T gamma M^2 (thermal), q by fvar2q.
 __global__ void k_fs_noslip(double* q, double* rho, double* vel, double* prs, double* tmp, int dir, int side, FsGeo g,
                             FsThermo th) {
-  const int N = g.N[dir];
+  const int N = g.n_(dir);
   const Box3 b = box_line(g, dir, side ? N : 0, side ? N : 0);
-  const int64_t sd = g.s[dir] * (side ? -1 : 1);   // towards the interior
+  const int64_t sd = g.s_(dir) * (side ? -1 : 1);   // towards the interior
   GRID_STRIDE(p, b.size()) {
     int i, j, k;
     b.node(p, i, j, k);
@@ -195,8 +199,8 @@ __global__ void k_fs_noslip(double* q, double* rho, double* vel, double* prs, do
 // convrsdcal6's fluxes along dir at nodes -hm..N+hm (solver.F90:2201-2207): uu = dxi u_dir,
 // fcs1 = jacob q1 uu, fcs(1+m) = jacob (q(1+m) uu + dxi p delta(m,dir)), fcs5 = jacob (q5 + p) uu.
 __global__ void k_fs_conv_flux(double* F, const double* q, const double* vel, const double* prs, int dir, FsGeo g) {
-  const Box3 b = box_line(g, dir, -HMW, g.N[dir] + HMW);
-  const double dxi = g.rd[dir], jb = g.jac;
+  const Box3 b = box_line(g, dir, -HMW, g.n_(dir) + HMW);
+  const double dxi = g.rd_(dir), jb = g.jac;
   GRID_STRIDE(p, b.size()) {
     int i, j, k;
     b.node(p, i, j, k);
@@ -213,53 +217,64 @@ __global__ void k_fs_conv_flux(double* F, const double* q, const double* vel, co
   }
 }
 
+// The full flux jacob (q uu + dxi p e_dir, (E + p) uu) of a supersonic node (one side of the split).
+__device__ __forceinline__ void fs_sw_full(double (&f)[5], int dir, double dxi, double jb, double uu, double p,
+                                           const double (&qq)[5]) {
+  f[0] = jb * qq[0] * uu;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) f[1 + c] = (c == dir) ? jb * (qq[1 + c] * uu + dxi * p) : jb * (qq[1 + c] * uu);
+  f[4] = jb * (qq[4] + p) * uu;
+}
+// One side of the subsonic split from its eigenvalue weights l1 (= l2 = l3), l4, l5.
+__device__ __forceinline__ void fs_sw_side(double (&f)[5], const FsThermo& th, int dir, double jb, double jro, double r,
+                                           double l1, double l4, double l5, const double (&u)[3], double uu,
+                                           double var0, double css, double gpd, double gm2, double fhi, double q4) {
+  const double var1 = l1;
+  const double var2 = l4 - l5;
+  const double var3 = 2.0 * l1 - l4 - l5;
+  const double var4 = var1 - var3 * gm2;
+  f[0] = jro * var4;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) f[1 + c] = (c == dir) ? jro * (var4 * u[c] + var2 * css * gpd * gm2) : jro * (var4 * u[c]);
+  f[4] = jb * (var1 * q4 + r * (var2 * uu * var0 * css * gm2 - var3 * (fhi + css * css) * gm2 / (th.gamma - 1.0)));
+}
+
 // flux_steger_warming of one node (riemann.F90:23-161, non-reacting) for the metric row
 // dxi e_dir: uu = dxi u_dir, the sound speed sqrt(T)/M (sos, fludyna.F90:832-859), eigenvalues
 // (uu, uu, uu, uu + c dxi, uu - c dxi) split with the entropy fix eps = 0.04. The operations
 // follow the reference's order with the zero metric components left out (they add zeros).
-__device__ __forceinline__ void fs_sw_split(const FsThermo& th, int dir, double dxi, double jb, double r, const double* u,
-                                            double p, double t, const double* qq, double* fp, double* fm) {
+__device__ __forceinline__ void fs_sw_split(const FsThermo& th, int dir, double dxi, double jb, double r,
+                                            const double (&u)[3], double p, double t, const double (&qq)[5],
+                                            double (&fp)[5], double (&fm)[5]) {
   const double eps = 0.04;
-  const double uu = dxi * u[dir];
+  const double ud = dir == 0 ? u[0] : (dir == 1 ? u[1] : u[2]);
+  const double uu = dxi * ud;
   const double var0 = 1.0 / sqrt(dxi * dxi);
   const double gpd = dxi * var0;                 // the dir component; the others are zero
   const double gm2 = 0.5 / th.gamma;
   const double css = sqrt(t) / th.mach;
   const double csa = css / var0;
   const double lmach = uu / csa;
-  const double lmda[5] = {uu, uu, uu, uu + csa, uu - csa};
-  double lp[5], lm[5];
+  if (lmach >= 1.0) {
+    fs_sw_full(fp, dir, dxi, jb, uu, p, qq);
 #pragma unroll
-  for (int k = 0; k < 5; ++k) {
-    lp[k] = 0.5 * (lmda[k] + sqrt(lmda[k] * lmda[k] + eps * eps));
-    lm[k] = lmda[k] - lp[k];
-  }
-  if (lmach >= 1.0 || lmach <= -1.0) {
-    double* f = lmach >= 1.0 ? fp : fm;
-    double* z = lmach >= 1.0 ? fm : fp;
-    f[0] = jb * qq[0] * uu;
-#pragma unroll
-    for (int c = 0; c < 3; ++c) f[1 + c] = (c == dir) ? jb * (qq[1 + c] * uu + dxi * p) : jb * (qq[1 + c] * uu);
-    f[4] = jb * (qq[4] + p) * uu;
-#pragma unroll
-    for (int k = 0; k < 5; ++k) z[k] = 0.0;
+    for (int k = 0; k < 5; ++k) fm[k] = 0.0;
     return;
   }
+  if (lmach <= -1.0) {
+    fs_sw_full(fm, dir, dxi, jb, uu, p, qq);
+#pragma unroll
+    for (int k = 0; k < 5; ++k) fp[k] = 0.0;
+    return;
+  }
+  const double l4 = uu + csa, l5 = uu - csa;
+  const double p1 = 0.5 * (uu + sqrt(uu * uu + eps * eps));
+  const double p4 = 0.5 * (l4 + sqrt(l4 * l4 + eps * eps));
+  const double p5 = 0.5 * (l5 + sqrt(l5 * l5 + eps * eps));
   const double fhi = 0.5 * (th.gamma - 1.0) * (u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
   const double jro = jb * r;
-#pragma unroll
-  for (int side = 0; side < 2; ++side) {
-    const double* l = side == 0 ? lp : lm;
-    double* f = side == 0 ? fp : fm;
-    const double var1 = l[0];
-    const double var2 = l[3] - l[4];
-    const double var3 = 2.0 * l[0] - l[3] - l[4];
-    const double var4 = var1 - var3 * gm2;
-    f[0] = jro * var4;
-#pragma unroll
-    for (int c = 0; c < 3; ++c) f[1 + c] = (c == dir) ? jro * (var4 * u[c] + var2 * css * gpd * gm2) : jro * (var4 * u[c]);
-    f[4] = jb * (var1 * qq[4] + r * (var2 * uu * var0 * css * gm2 - var3 * (fhi + css * css) * gm2 / (th.gamma - 1.0)));
-  }
+  fs_sw_side(fp, th, dir, jb, jro, r, p1, p4, p5, u, uu, var0, css, gpd, gm2, fhi, qq[4]);
+  fs_sw_side(fm, th, dir, jb, jro, r, uu - p1, l4 - p4, l5 - p5, u, uu, var0, css, gpd, gm2, fhi, qq[4]);
 }
 
 // The split fluxes along dir on the nodes iss..iee of every line (solver.F90:1333-1345); the
@@ -267,7 +282,7 @@ __device__ __forceinline__ void fs_sw_split(const FsThermo& th, int dir, double 
 __global__ void k_fs_sw_split(double* fsp, double* fsm, const double* q, const double* rho, const double* vel,
                               const double* prs, const double* tmp, int dir, int iss, int iee, FsGeo g, FsThermo th) {
   const Box3 b = box_line(g, dir, iss, iee);
-  const double dxi = g.rd[dir], jb = g.jac;
+  const double dxi = g.rd_(dir), jb = g.jac;
   const int64_t fs = g.fs;
   GRID_STRIDE(p, b.size()) {
     int i, j, k;
@@ -461,16 +476,14 @@ __global__ void k_fs_lshock(double* lsh, const double* ssf, double shkcrt, FsGeo
 __global__ void k_fs_char_flux(double* Fh, const double* fsp, const double* fsm, const double* fhp, const double* fhm,
                                const double* q, const double* rho, const double* vel, const double* prs,
                                const double* lsh, int dir, int nt, int iss, int iee, FsGeo g, FsThermo th) {
-  const int N = g.N[dir];
+  const int N = g.n_(dir);
   const Box3 b = box_line(g, dir, -1, N);
-  const int64_t sd = g.s[dir], fs = g.fs;
-  double mrow[3] = {0.0, 0.0, 0.0};
-  mrow[dir] = g.rd[dir];
+  const int64_t sd = g.s_(dir), fs = g.fs;
+  const double mrow[3] = {dir == 0 ? g.rd[0] : 0.0, dir == 1 ? g.rd[1] : 0.0, dir == 2 ? g.rd[2] : 0.0};
   GRID_STRIDE(p, b.size()) {
     int i, j, k;
     b.node(p, i, j, k);
-    const int idx[3] = {i, j, k};
-    const int t = idx[dir];
+    const int t = dir == 0 ? i : (dir == 1 ? j : k);
     const int64_t oa = g.at(i, j, k), ob = oa + sd;
     const int64_t o0 = oa - (int64_t)t * sd;
     bool shock;
@@ -513,7 +526,7 @@ __global__ void k_fs_char_flux(double* Fh, const double* fsp, const double* fsm,
 // qrhs(i) = qrhs(i) + Fh(i) - Fh(i-1) at nodes 0..N, Fh stored per interface (solver.F90:1509-1513)
 __global__ void k_fs_flux_diff(double* qrhs, const double* Fh, int dir, FsGeo g) {
   const Box3 b = box_line(g, -1, 0, 0);
-  const int64_t sd = g.s[dir];
+  const int64_t sd = g.s_(dir);
   GRID_STRIDE(p, b.size() * 5) {
     const int m = (int)(p / b.size());
     int i, j, k;
@@ -528,15 +541,14 @@ __global__ void k_fs_flux_diff(double* qrhs, const double* Fh, int dir, FsGeo g)
 // .true., stored at node i of the layout (work fields).
 __global__ void k_fs_mp_flux(double* Fh, const double* fsp, const double* fsm, const double* fhp, const double* fhm,
                              int dir, int nt, int iss, int iee, FsGeo g) {
-  const int N = g.N[dir];
+  const int N = g.n_(dir);
   const Box3 b = box_line(g, dir, -1, N);
-  const int64_t sd = g.s[dir];
+  const int64_t sd = g.s_(dir);
   GRID_STRIDE(p, b.size() * 5) {
     const int m = (int)(p / b.size());
     int i, j, k;
     b.node(p - (int64_t)m * b.size(), i, j, k);
-    const int idx[3] = {i, j, k};
-    const int t = idx[dir];
+    const int t = dir == 0 ? i : (dir == 1 ? j : k);
     const int64_t o = m * g.fs + g.at(i, j, k);
     Fh[o] = fs_interface(fsp, fsm, fhp, fhm, o - (int64_t)t * sd, sd, t, N, nt, iss, iee);
   }
@@ -578,15 +590,19 @@ __global__ void k_fs_stress(double* sigma, double* qflux, const double* dvel, co
 // diffrsdcal6's fluxes along dir at nodes -hm..N+hm (solver.F90:2622-2640):
 // ff = (sigma(row dir) . dxi) * jacob for the momenta, (qflux . dxi) * jacob for the energy.
 __global__ void k_fs_visc_flux(double* F, const double* sigma, const double* qflux, int dir, FsGeo g) {
-  const Box3 b = box_line(g, dir, -HMW, g.N[dir] + HMW);
-  const double dxi = g.rd[dir], jb = g.jac;
-  const int sgi[3][3] = {{0, 1, 2}, {1, 3, 4}, {2, 4, 5}};
+  const Box3 b = box_line(g, dir, -HMW, g.n_(dir) + HMW);
+  const double dxi = g.rd_(dir), jb = g.jac;
   GRID_STRIDE(p, b.size()) {
     int i, j, k;
     b.node(p, i, j, k);
     const int64_t o = g.at(i, j, k);
 #pragma unroll
-    for (int n = 0; n < 3; ++n) F[n * g.fs + o] = sigma[sgi[dir][n] * g.fs + o] * dxi * jb;
+    for (int n = 0; n < 3; ++n) {
+      // sigma(dir, n) in the symmetric storage 11 12 13 22 23 33
+      const int lo = min(dir, n), hi = max(dir, n);
+      const int sg = lo == 0 ? hi : (lo == 1 ? 2 + hi : 5);
+      F[n * g.fs + o] = sigma[sg * g.fs + o] * dxi * jb;
+    }
     F[3 * g.fs + o] = qflux[dir * g.fs + o] * dxi * jb;
   }
 }
@@ -766,8 +782,8 @@ cudaError_t flux_op(astr_full* fs, const DevOp& op, int dir, double* in, double*
   double* fp = view(fs, in, dir, fa);
   double* op_ = view(fs, out, -1, oa);
   oa.lb[dir] = -1;
-  oa.n[dir] = fs->g.N[dir] + 2;
-  op_ -= fs->g.s[dir];   // the descriptor is relative to node -1 along dir
+  oa.n[dir] = fs->g.n_(dir) + 2;
+  op_ -= fs->g.s_(dir);   // the descriptor is relative to node -1 along dir
   return launch_line_api(op, dir, fp, fa, op_, oa, nf, 1.0, astr_ctx_stream(fs->ctx), 0);
 }
 
@@ -818,7 +834,7 @@ cudaError_t fs_convection_upwind(astr_full* fs) {
 }
 
 cudaError_t fs_halo(astr_full* fs, double* F, int nf, int dir) {
-  const int64_t n = (int64_t)nf * HMW * (fs->g.N[0] + 1) * (fs->g.N[1] + 1) * (fs->g.N[2] + 1) / (fs->g.N[dir] + 1);
+  const int64_t n = (int64_t)nf * HMW * (fs->g.N[0] + 1) * (fs->g.N[1] + 1) * (fs->g.N[2] + 1) / (fs->g.n_(dir) + 1);
   k_fs_halo<<<blocks_for(n), 256, 0, astr_ctx_stream(fs->ctx)>>>(F, nf, dir, fs->g);
   return cudaGetLastError();
 }

@@ -112,7 +112,7 @@ __global__ void __launch_bounds__(512) k_line_api(LineOp op, int dir, const doub
       if (lo ? (j >= op.spec_lo) : (j - NSP >= op.spec_hi)) continue;
       const int r = lo ? j : op.nsys - op.spec_hi + (j - NSP);
       const double* li = tile + ll * LP + HT;
-      sp[it] = special_value(op, r, [li](int nn) { return li[nn]; });
+      sp[it] = special_value<true>(op, r, [li](int nn) { return li[nn]; });
     }
     __syncthreads();
   }
