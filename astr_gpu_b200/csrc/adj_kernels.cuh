@@ -109,7 +109,7 @@ __global__ void __launch_bounds__(512) k_adj_grad(PassArgs a) {
   __syncthreads();
   to_prims(c, T, tsz, a.th);
   __syncthreads();
-  compute_specials(a.opd, c.TI, spb, 4, [&](int l, int k, int n) { return gprim_rt<DIR>(k, T + l * c.LP + HT, tsz, n, a.th); });
+  compute_specials<OP_DERIV>(a.opd, c.TI, spb, 4, [&](int l, int k, int n) { return gprim_rt<DIR>(k, T + l * c.LP + HT, tsz, n, a.th); });
   __syncthreads();
   const LaneIds z = lane_ids<WPL>();
   double* scl = scan + z.l * SCAN_PER_LINE * WPL;

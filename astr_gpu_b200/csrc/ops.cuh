@@ -248,10 +248,14 @@ __host__ __device__ __forceinline__ bool flux_special(const LineOp& op, int r, G
 // RHS value of closure row r (derivative or filter; with FLUX also the interface flux, which only
 // the line operators take, so that the fused passes compile without its branch), for the
 // precomputed closure table.
-template <bool FLUX = false, class Get>
+// KIND >= 0 fixes the operator kind at compile time (a pass that only differentiates then
+// carries no filter closure code).
+template <bool FLUX = false, int KIND = -1, class Get>
 __device__ __forceinline__ double special_value(const LineOp& op, int r, Get f) {
   double s = 0.0;
-  if (op.kind == OP_FILTER) filter_special(op, r, f, s);
+  if (KIND == OP_DERIV) deriv_special(op, r, f, s);
+  else if (KIND == OP_FILTER) filter_special(op, r, f, s);
+  else if (op.kind == OP_FILTER) filter_special(op, r, f, s);
   else if (FLUX && op.kind == OP_FLUX) flux_special(op, r, f, s);
   else deriv_special(op, r, f, s);
   return s;

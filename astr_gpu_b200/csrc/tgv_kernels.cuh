@@ -333,7 +333,7 @@ __device__ __forceinline__ LaneIds lane_ids() {
 // Closure-row RHS values of `ns` pending solves on every line of the tile, computed up front by
 // a few threads so that no warp diverges on closure rows during its solve:
 // sp[(l*ns + k)*2*NSP + j] for line l, solve k. getk(l, k, n) = input of solve k at node n.
-template <class GetK>
+template <int KIND = -1, class GetK>
 __device__ __forceinline__ void compute_specials(const LineOp& op, int TI, double* sp, int ns, GetK getk) {
   const int per = 2 * NSP;
   for (int it = threadIdx.x; it < TI * ns * per; it += blockDim.x) {
@@ -342,7 +342,7 @@ __device__ __forceinline__ void compute_specials(const LineOp& op, int TI, doubl
     const bool lo = j < NSP;
     if (lo ? (j >= op.spec_lo) : (j - NSP >= op.spec_hi)) continue;
     const int r = lo ? j : op.nsys - op.spec_hi + (j - NSP);
-    sp[(l * ns + k) * per + j] = special_value(op, r, [&](int n) { return getk(l, k, n); });
+    sp[(l * ns + k) * per + j] = special_value<false, KIND>(op, r, [&](int n) { return getk(l, k, n); });
   }
 }
 
@@ -411,9 +411,10 @@ __device__ __forceinline__ void solve_lines(double* line, int stride, int count,
 
 // Closure tables of `count` tile lines spaced by `stride` (line l of solve k at
 // base + k*stride + l*LP + HT).
+template <int KIND>
 __device__ __forceinline__ void tile_specials(const LineOp& op, int TI, int LP, const double* base, int stride, int count,
                                               double* sp) {
-  compute_specials(op, TI, sp, count, [&](int l, int k, int n) { return base[k * stride + l * LP + HT + n]; });
+  compute_specials<KIND>(op, TI, sp, count, [&](int l, int k, int n) { return base[k * stride + l * LP + HT + n]; });
 }
 
 // Euler flux along DIR at one node from the primitives (convection, tgvsolver.F90:559-564, with
@@ -491,7 +492,7 @@ __device__ __forceinline__ void k_pass_ab_body(const PassArgs& a, int bx, int by
   const int dim = c.dim;
 
   if (IS_A && a.do_filter) {
-    tile_specials(a.opf, c.TI, c.LP, T, tsz, 5, spb);
+    tile_specials<OP_FILTER>(a.opf, c.TI, c.LP, T, tsz, 5, spb);
     __syncthreads();
     solve_lines<S, WPL>(T + z.l * c.LP + HT, tsz, 5, a.opf, z, scl, 1.0, true, spb + z.l * 5 * 2 * NSP);
     __syncthreads();
@@ -500,7 +501,7 @@ __device__ __forceinline__ void k_pass_ab_body(const PassArgs& a, int bx, int by
   }
   to_prims<DIR, WPL, true>(c, T, tsz, a.th);
   __syncthreads();
-  tile_specials(a.opd, c.TI, c.LP, T + tsz, tsz, 4, spb);
+  tile_specials<OP_DERIV>(a.opd, c.TI, c.LP, T + tsz, tsz, 4, spb);
   __syncthreads();
   solve_lines<S, WPL>(T + tsz + z.l * c.LP + HT, tsz, 4, a.opd, z, scl, a.g.rd[DIR], false, spb + z.l * 4 * 2 * NSP);
   __syncthreads();
@@ -549,7 +550,7 @@ __device__ __forceinline__ void k_pass_c_body(const PassArgs& a, int bx, int by)
     G[3 * tsz + o] = T[4 * tsz + o] / T[o] * a.th.const2;
   });
   __syncthreads();
-  tile_specials(a.opd, c.TI, c.LP, G, tsz, 4, spb);
+  tile_specials<OP_DERIV>(a.opd, c.TI, c.LP, G, tsz, 4, spb);
   __syncthreads();
   const LaneIds z = lane_ids<WPL>();
   double* scl = scan + z.l * SCAN_PER_LINE * WPL;
@@ -678,7 +679,7 @@ __device__ __forceinline__ void k_pass_c_body(const PassArgs& a, int bx, int by)
     pp[0] = s0; pp[1] = s1; pp[2] = s2;
   }
   // R = D_C(VF_C - F_C): one solve per component (convection + diffusion, tgvsolver.F90:539-787)
-  tile_specials(a.opd, c.TI, c.LP, G, tsz, 5, spv);
+  tile_specials<OP_DERIV>(a.opd, c.TI, c.LP, G, tsz, 5, spv);
   __syncthreads();
   solve_lines<S, WPL>(G + z.l * c.LP + HT, tsz, 5, a.opd, z, scl, rd, false, spv + z.l * 5 * 2 * NSP);
   __syncthreads();
@@ -761,7 +762,7 @@ __device__ __forceinline__ void k_pass_vas_body(const PassArgs& a, int bx, int b
   const LaneIds z = lane_ids<WPL>();
   double* scl = scan + z.l * SCAN_PER_LINE * WPL;
   stream_fields(c, sm, tsz, 5, nbuf, fps, [&](int m) { return a.VF + m * fs; }, [&](int m0, int cnt, double* T) {
-    tile_specials(a.opd, c.TI, c.LP, T, tsz, cnt, spb);
+    tile_specials<OP_DERIV>(a.opd, c.TI, c.LP, T, tsz, cnt, spb);
     __syncthreads();
     solve_tile<S, WPL>(T, tsz, cnt, c.TI, c.LP, a.LPW, a.opd, z, scl, a.g.rd[DIR], spb);
     __syncthreads();
@@ -782,7 +783,7 @@ __device__ __forceinline__ void k_pass_vbs_body(const PassArgs& a, int bx, int b
   double* scl = scan + z.l * SCAN_PER_LINE * WPL;
   const int dim = c.dim;
   stream_fields(c, sm, tsz, 5, nbuf, fps, [&](int m) { return a.VF + (5 + m) * fs; }, [&](int m0, int cnt, double* T) {
-    tile_specials(a.opd, c.TI, c.LP, T, tsz, cnt, spb);
+    tile_specials<OP_DERIV>(a.opd, c.TI, c.LP, T, tsz, cnt, spb);
     __syncthreads();
     solve_tile<S, WPL>(T, tsz, cnt, c.TI, c.LP, a.LPW, a.opd, z, scl, a.g.rd[DIR], spb);
     __syncthreads();
@@ -818,7 +819,7 @@ __device__ __forceinline__ void k_pass_vbs_body(const PassArgs& a, int bx, int b
     }
     __syncthreads();
     if (a.do_filter) {
-      tile_specials(a.opf, c.TI, c.LP, T, tsz, cnt, spb);
+      tile_specials<OP_FILTER>(a.opf, c.TI, c.LP, T, tsz, cnt, spb);
       __syncthreads();
       solve_tile<S, WPL>(T, tsz, cnt, c.TI, c.LP, a.LPW, a.opf, z, scl, 1.0, spb);
       __syncthreads();
@@ -839,7 +840,7 @@ __device__ __forceinline__ void k_pass_fs_body(const PassArgs& a, int bx, int by
   const LaneIds z = lane_ids<WPL>();
   double* scl = scan + z.l * SCAN_PER_LINE * WPL;
   stream_fields(c, sm, tsz, 5, nbuf, fps, [&](int m) { return a.q + m * fs; }, [&](int m0, int cnt, double* T) {
-    tile_specials(a.opf, c.TI, c.LP, T, tsz, cnt, spb);
+    tile_specials<OP_FILTER>(a.opf, c.TI, c.LP, T, tsz, cnt, spb);
     __syncthreads();
     solve_tile<S, WPL>(T, tsz, cnt, c.TI, c.LP, a.LPW, a.opf, z, scl, 1.0, spb);
     __syncthreads();
@@ -861,7 +862,7 @@ __device__ __forceinline__ void k_pass_va_body(const PassArgs& a, int bx, int by
   for (int m = 0; m < 5; ++m) load_tile(c, T + m * tsz, a.VF + m * fs);
   cp_async_wait_all();
   __syncthreads();
-  tile_specials(a.opd, c.TI, c.LP, T, tsz, 5, spb);
+  tile_specials<OP_DERIV>(a.opd, c.TI, c.LP, T, tsz, 5, spb);
   __syncthreads();
   const LaneIds z = lane_ids<WPL>();
   double* scl = scan + z.l * SCAN_PER_LINE * WPL;
@@ -885,7 +886,7 @@ __device__ __forceinline__ void k_pass_vb_body(const PassArgs& a, int bx, int by
   for (int m = 0; m < 5; ++m) load_tile(c, T + m * tsz, a.VF + (5 + m) * fs);
   cp_async_wait_all();
   __syncthreads();
-  tile_specials(a.opd, c.TI, c.LP, T, tsz, 5, spb);
+  tile_specials<OP_DERIV>(a.opd, c.TI, c.LP, T, tsz, 5, spb);
   __syncthreads();
   const LaneIds z = lane_ids<WPL>();
   double* scl = scan + z.l * SCAN_PER_LINE * WPL;
@@ -923,7 +924,7 @@ __device__ __forceinline__ void k_pass_vb_body(const PassArgs& a, int bx, int by
   }
   __syncthreads();
   if (a.do_filter) {
-    tile_specials(a.opf, c.TI, c.LP, T, tsz, 5, spb);
+    tile_specials<OP_FILTER>(a.opf, c.TI, c.LP, T, tsz, 5, spb);
     __syncthreads();
     solve_lines<S, WPL>(T + z.l * c.LP + HT, tsz, 5, a.opf, z, scl, 1.0, false, spb + z.l * 5 * 2 * NSP);
     __syncthreads();
@@ -944,7 +945,7 @@ __device__ __forceinline__ void k_pass_f_body(const PassArgs& a, int bx, int by)
   for (int m = 0; m < 5; ++m) load_tile(c, T + m * tsz, a.q + m * fs);
   cp_async_wait_all();
   __syncthreads();
-  tile_specials(a.opf, c.TI, c.LP, T, tsz, 5, spb);
+  tile_specials<OP_FILTER>(a.opf, c.TI, c.LP, T, tsz, 5, spb);
   __syncthreads();
   const LaneIds z = lane_ids<WPL>();
   double* scl = scan + z.l * SCAN_PER_LINE * WPL;
