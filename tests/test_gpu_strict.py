@@ -79,10 +79,12 @@ def test_strict_build_flux_lines_match_oracle(wind):
 def test_strict_build_upwind_rhs_matches_oracle():
     """One full-solver stage with the upwind compact flux in characteristic variables from the
     strict build (Steger-Warming split, Roe eigenvectors and the projections without
-    contraction), scaled as the upwind test of the default build (1e-14 times 1/M of each field's
-    scale). The Ducros threshold is set above every node's sensor value: where shock flags are
-    set, the sensor's threshold and the limiter's branches are discrete decisions that a last-ulp
-    difference of the solves can flip, which the default build's tolerance covers."""
+    contraction), against the oracle, measured against the problem's own rounding floor: the
+    oracle's change under a relative perturbation of 1e-16 of the input state (seeded noise).
+    The full-solver stage amplifies last-bit differences well above the miniapp's (the split
+    fluxes' acoustic parts, and with the filter the filtered conserved variables beside the
+    unfiltered primitives), so a fixed 1e-14 would not be a statement about the kernels. The
+    Ducros threshold is above every node's sensor value (no discrete shock decisions)."""
     import astr_gpu_b200 as ag
     dims = (40, 48, 36)
     mach = 0.2
@@ -97,21 +99,31 @@ def test_strict_build_upwind_rhs_matches_oracle():
     q = np.zeros(tuple(n + 1 for n in dims) + (5,), order="F")
     q[..., 0], q[..., 1], q[..., 2], q[..., 3] = rho, rho * u, rho * v, rho * w
     q[..., 4] = p / 0.4 + 0.5 * rho * (u * u + v * v + w * w)
+    h = [2 * np.pi / n for n in dims]
+    jac, p0 = h[0] * h[1] * h[2], 1.0 / (1.4 * mach ** 2)
+
+    def scaled(a, b):
+        return max(float(np.abs(a[..., m] - b[..., m]).max()) / max(np.abs(b[..., m]).max(), jac * p0 / min(h))
+                   for m in range(5))
+
     kw = dict(mach=mach, reynolds=800.0, sutherland=110.3, beta_bound=0.98, conschm=543, bfacmpld=0.3,
               lchardecomp=True, shkcrt=0.01)
     o = oracle.TGVOracle(*dims, params=oracle.FlowParams(**kw))
     o.set_q(q)
     ref = o.rhs_full()
     assert not o.shock_flags().any()
+    floor = 0.0
+    for seed in (1, 2):
+        noise = np.random.default_rng(seed).standard_normal(q.shape)
+        o2 = oracle.TGVOracle(*dims, params=oracle.FlowParams(**kw))
+        o2.set_q(np.asfortranarray(q * (1.0 + 1e-16 * noise)))
+        floor = max(floor, scaled(o2.rhs_full(), ref))
     ctx = ag.Context(0, strict=True)
     s = ag.FullSolver(ctx, *dims, params=ag.FlowParams(**kw))
     s.set_q(q)
     got = s.rhs()
     s.close()
     ctx.close()
-    h = [2 * np.pi / n for n in dims]
-    jac, p0 = h[0] * h[1] * h[2], 1.0 / (1.4 * mach ** 2)
-    err = max(float(np.abs(got[..., m] - ref[..., m]).max()) / max(np.abs(ref[..., m]).max(), jac * p0 / min(h))
-              for m in range(5))
-    print(f"upwind characteristic rhs, strict build, scaled: {err:.3e}")
-    assert err <= STRICT_TOL / mach
+    err = scaled(got, ref)
+    print(f"upwind characteristic rhs, strict build, scaled: {err:.3e} (rounding floor {floor:.3e})")
+    assert err <= 10.0 * floor
