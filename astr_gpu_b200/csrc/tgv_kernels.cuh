@@ -369,14 +369,15 @@ __device__ __forceinline__ void dsolve_n(double (&v)[NV][S], int K0, const PassA
 
 // Solves of NV staged tile lines (derivative or filter) in place, together; `stride` separates
 // the lines of consecutive solves.
-template <int S, int WPL, int NV>
+// KIND: OP_DERIV or OP_FILTER, the operator's kind known at compile time.
+template <int S, int WPL, int NV, int KIND>
 __device__ __forceinline__ void solve_lines_n(double* line, int stride, const LineOp& op, const LaneIds& z, double* scl,
                                               double scale, bool images, const double* sp) {
   double v[NV][S];
 #pragma unroll
   for (int i = 0; i < NV; ++i) {
     const double* li = line + i * stride;
-    if (op.kind == OP_FILTER) rhs_filter<S>(v[i], op, z.seg, [li](int n) { return li[n]; }, sp + i * 2 * NSP);
+    if (KIND == OP_FILTER) rhs_filter<S>(v[i], op, z.seg, [li](int n) { return li[n]; }, sp + i * 2 * NSP);
     else rhs_deriv<S>(v[i], op, z.seg, [li](int n) { return li[n]; }, sp + i * 2 * NSP);
   }
   seg_solve_n<S, WPL, NV>(v, op.tab, z.seg, z.lane, z.part, z.l, scl);
@@ -395,18 +396,18 @@ __device__ __forceinline__ void solve_lines_n(double* line, int stride, const Li
 // -7 %), one at a time for 17 rows per lane, where a pair's registers exceed the 128 cap, and
 // for 3, the small boxes' layout.
 // sp: this line's closure tables of the `count` solves (see compute_specials).
-template <int S, int WPL>
+template <int S, int WPL, int KIND>
 __device__ __forceinline__ void solve_lines(double* line, int stride, int count, const LineOp& op, const LaneIds& z,
                                             double* scl, double scale, bool images, const double* sp) {
   int i = 0;
   if (S == 5)
     for (; i + 3 < count; i += 4)
-      solve_lines_n<S, WPL, 4>(line + i * stride, stride, op, z, scl, scale, images, sp + i * 2 * NSP);
+      solve_lines_n<S, WPL, 4, KIND>(line + i * stride, stride, op, z, scl, scale, images, sp + i * 2 * NSP);
   if (S == 5 || S == 9)
     for (; i + 1 < count; i += 2)
-      solve_lines_n<S, WPL, 2>(line + i * stride, stride, op, z, scl, scale, images, sp + i * 2 * NSP);
+      solve_lines_n<S, WPL, 2, KIND>(line + i * stride, stride, op, z, scl, scale, images, sp + i * 2 * NSP);
   for (; i < count; ++i)
-    solve_lines_n<S, WPL, 1>(line + i * stride, stride, op, z, scl, scale, images, sp + i * 2 * NSP);
+    solve_lines_n<S, WPL, 1, KIND>(line + i * stride, stride, op, z, scl, scale, images, sp + i * 2 * NSP);
 }
 
 // Closure tables of `count` tile lines spaced by `stride` (line l of solve k at
@@ -494,7 +495,7 @@ __device__ __forceinline__ void k_pass_ab_body(const PassArgs& a, int bx, int by
   if (IS_A && a.do_filter) {
     tile_specials<OP_FILTER>(a.opf, c.TI, c.LP, T, tsz, 5, spb);
     __syncthreads();
-    solve_lines<S, WPL>(T + z.l * c.LP + HT, tsz, 5, a.opf, z, scl, 1.0, true, spb + z.l * 5 * 2 * NSP);
+    solve_lines<S, WPL, OP_FILTER>(T + z.l * c.LP + HT, tsz, 5, a.opf, z, scl, 1.0, true, spb + z.l * 5 * 2 * NSP);
     __syncthreads();
     store_tiles<DIR, WPL, false>(c, T, tsz, a.q, fs, 5);
     __syncthreads();   // every filtered value is stored before the tiles turn into primitives
@@ -503,7 +504,7 @@ __device__ __forceinline__ void k_pass_ab_body(const PassArgs& a, int bx, int by
   __syncthreads();
   tile_specials<OP_DERIV>(a.opd, c.TI, c.LP, T + tsz, tsz, 4, spb);
   __syncthreads();
-  solve_lines<S, WPL>(T + tsz + z.l * c.LP + HT, tsz, 4, a.opd, z, scl, a.g.rd[DIR], false, spb + z.l * 4 * 2 * NSP);
+  solve_lines<S, WPL, OP_DERIV>(T + tsz + z.l * c.LP + HT, tsz, 4, a.opd, z, scl, a.g.rd[DIR], false, spb + z.l * 4 * 2 * NSP);
   __syncthreads();
   store_tiles<DIR, WPL, false>(c, T + tsz, tsz, a.D, fs, 4);
 }
@@ -555,7 +556,7 @@ __device__ __forceinline__ void k_pass_c_body(const PassArgs& a, int bx, int by)
   const LaneIds z = lane_ids<WPL>();
   double* scl = scan + z.l * SCAN_PER_LINE * WPL;
   const double rd = a.g.rd[DIR];
-  solve_lines<S, WPL>(G + z.l * c.LP + HT, tsz, 4, a.opd, z, scl, rd, false, spb + z.l * 4 * 2 * NSP);
+  solve_lines<S, WPL, OP_DERIV>(G + z.l * c.LP + HT, tsz, 4, a.opd, z, scl, rd, false, spb + z.l * 4 * 2 * NSP);
   __syncthreads();
   if (a.DC) {   // kept for the discrete adjoint
     store_tiles<DIR, WPL, false>(c, G, tsz, a.DC, fs, 4);
@@ -681,7 +682,7 @@ __device__ __forceinline__ void k_pass_c_body(const PassArgs& a, int bx, int by)
   // R = D_C(VF_C - F_C): one solve per component (convection + diffusion, tgvsolver.F90:539-787)
   tile_specials<OP_DERIV>(a.opd, c.TI, c.LP, G, tsz, 5, spv);
   __syncthreads();
-  solve_lines<S, WPL>(G + z.l * c.LP + HT, tsz, 5, a.opd, z, scl, rd, false, spv + z.l * 5 * 2 * NSP);
+  solve_lines<S, WPL, OP_DERIV>(G + z.l * c.LP + HT, tsz, 5, a.opd, z, scl, rd, false, spv + z.l * 5 * 2 * NSP);
   __syncthreads();
   store_tiles<DIR, WPL, false>(c, G, tsz, a.R + fs, fs, 4);
   store_tiles<DIR, WPL, false>(c, G + 4 * tsz, tsz, a.R, fs, 1);
@@ -733,14 +734,14 @@ __device__ __forceinline__ void stream_fields(const TileCtx<DIR, WPL, LW>& c, do
 // `count` solves (tiles spaced by tsz) on every line of a tile: the CTA's warps form TI / LPW
 // line groups of WPL warps, and group g solves lines g, g + TI/LPW, ... (LPW lines per group;
 // LPW = 1 on x lines). spb: closure tables laid out by tile_specials with `count` solves.
-template <int S, int WPL>
+template <int S, int WPL, int KIND>
 __device__ __forceinline__ void solve_tile(double* tile, int tsz, int count, int TI, int LP, int LPW, const LineOp& op,
                                            const LaneIds& z, double* scl, double scale, const double* spb) {
   const int ng = TI / LPW;
 #pragma unroll 1
   for (int k = 0; k < LPW; ++k) {
     const int l = z.l + k * ng;
-    solve_lines<S, WPL>(tile + l * LP + HT, tsz, count, op, z, scl, scale, false, spb + l * count * 2 * NSP);
+    solve_lines<S, WPL, KIND>(tile + l * LP + HT, tsz, count, op, z, scl, scale, false, spb + l * count * 2 * NSP);
   }
 }
 
@@ -764,7 +765,7 @@ __device__ __forceinline__ void k_pass_vas_body(const PassArgs& a, int bx, int b
   stream_fields(c, sm, tsz, 5, nbuf, fps, [&](int m) { return a.VF + m * fs; }, [&](int m0, int cnt, double* T) {
     tile_specials<OP_DERIV>(a.opd, c.TI, c.LP, T, tsz, cnt, spb);
     __syncthreads();
-    solve_tile<S, WPL>(T, tsz, cnt, c.TI, c.LP, a.LPW, a.opd, z, scl, a.g.rd[DIR], spb);
+    solve_tile<S, WPL, OP_DERIV>(T, tsz, cnt, c.TI, c.LP, a.LPW, a.opd, z, scl, a.g.rd[DIR], spb);
     __syncthreads();
     store_tiles<DIR, WPL, true>(c, T, tsz, a.R + m0 * fs, fs, cnt);
   });
@@ -785,7 +786,7 @@ __device__ __forceinline__ void k_pass_vbs_body(const PassArgs& a, int bx, int b
   stream_fields(c, sm, tsz, 5, nbuf, fps, [&](int m) { return a.VF + (5 + m) * fs; }, [&](int m0, int cnt, double* T) {
     tile_specials<OP_DERIV>(a.opd, c.TI, c.LP, T, tsz, cnt, spb);
     __syncthreads();
-    solve_tile<S, WPL>(T, tsz, cnt, c.TI, c.LP, a.LPW, a.opd, z, scl, a.g.rd[DIR], spb);
+    solve_tile<S, WPL, OP_DERIV>(T, tsz, cnt, c.TI, c.LP, a.LPW, a.opd, z, scl, a.g.rd[DIR], spb);
     __syncthreads();
     if (a.mode == 0) {
       store_tiles<DIR, WPL, true>(c, T, tsz, a.R + m0 * fs, fs, cnt);
@@ -821,7 +822,7 @@ __device__ __forceinline__ void k_pass_vbs_body(const PassArgs& a, int bx, int b
     if (a.do_filter) {
       tile_specials<OP_FILTER>(a.opf, c.TI, c.LP, T, tsz, cnt, spb);
       __syncthreads();
-      solve_tile<S, WPL>(T, tsz, cnt, c.TI, c.LP, a.LPW, a.opf, z, scl, 1.0, spb);
+      solve_tile<S, WPL, OP_FILTER>(T, tsz, cnt, c.TI, c.LP, a.LPW, a.opf, z, scl, 1.0, spb);
       __syncthreads();
     }
     store_tiles<DIR, WPL, false>(c, T, tsz, a.qout + m0 * fs, fs, cnt);
@@ -842,7 +843,7 @@ __device__ __forceinline__ void k_pass_fs_body(const PassArgs& a, int bx, int by
   stream_fields(c, sm, tsz, 5, nbuf, fps, [&](int m) { return a.q + m * fs; }, [&](int m0, int cnt, double* T) {
     tile_specials<OP_FILTER>(a.opf, c.TI, c.LP, T, tsz, cnt, spb);
     __syncthreads();
-    solve_tile<S, WPL>(T, tsz, cnt, c.TI, c.LP, a.LPW, a.opf, z, scl, 1.0, spb);
+    solve_tile<S, WPL, OP_FILTER>(T, tsz, cnt, c.TI, c.LP, a.LPW, a.opf, z, scl, 1.0, spb);
     __syncthreads();
     store_tiles<DIR, WPL, false>(c, T, tsz, a.q + m0 * fs, fs, cnt);
   });
@@ -866,7 +867,7 @@ __device__ __forceinline__ void k_pass_va_body(const PassArgs& a, int bx, int by
   __syncthreads();
   const LaneIds z = lane_ids<WPL>();
   double* scl = scan + z.l * SCAN_PER_LINE * WPL;
-  solve_lines<S, WPL>(T + z.l * c.LP + HT, tsz, 5, a.opd, z, scl, a.g.rd[DIR], false, spb + z.l * 5 * 2 * NSP);
+  solve_lines<S, WPL, OP_DERIV>(T + z.l * c.LP + HT, tsz, 5, a.opd, z, scl, a.g.rd[DIR], false, spb + z.l * 5 * 2 * NSP);
   __syncthreads();
   store_tiles<DIR, WPL, true>(c, T, tsz, a.R, fs, 5);
 }
@@ -890,7 +891,7 @@ __device__ __forceinline__ void k_pass_vb_body(const PassArgs& a, int bx, int by
   __syncthreads();
   const LaneIds z = lane_ids<WPL>();
   double* scl = scan + z.l * SCAN_PER_LINE * WPL;
-  solve_lines<S, WPL>(T + z.l * c.LP + HT, tsz, 5, a.opd, z, scl, a.g.rd[DIR], false, spb + z.l * 5 * 2 * NSP);
+  solve_lines<S, WPL, OP_DERIV>(T + z.l * c.LP + HT, tsz, 5, a.opd, z, scl, a.g.rd[DIR], false, spb + z.l * 5 * 2 * NSP);
   __syncthreads();
   if (a.mode == 0) {
     store_tiles<DIR, WPL, true>(c, T, tsz, a.R, fs, 5);
@@ -926,7 +927,7 @@ __device__ __forceinline__ void k_pass_vb_body(const PassArgs& a, int bx, int by
   if (a.do_filter) {
     tile_specials<OP_FILTER>(a.opf, c.TI, c.LP, T, tsz, 5, spb);
     __syncthreads();
-    solve_lines<S, WPL>(T + z.l * c.LP + HT, tsz, 5, a.opf, z, scl, 1.0, false, spb + z.l * 5 * 2 * NSP);
+    solve_lines<S, WPL, OP_FILTER>(T + z.l * c.LP + HT, tsz, 5, a.opf, z, scl, 1.0, false, spb + z.l * 5 * 2 * NSP);
     __syncthreads();
   }
   store_tiles<DIR, WPL, false>(c, T, tsz, a.qout, fs, 5);
@@ -949,7 +950,7 @@ __device__ __forceinline__ void k_pass_f_body(const PassArgs& a, int bx, int by)
   __syncthreads();
   const LaneIds z = lane_ids<WPL>();
   double* scl = scan + z.l * SCAN_PER_LINE * WPL;
-  solve_lines<S, WPL>(T + z.l * c.LP + HT, tsz, 5, a.opf, z, scl, 1.0, false, spb + z.l * 5 * 2 * NSP);
+  solve_lines<S, WPL, OP_FILTER>(T + z.l * c.LP + HT, tsz, 5, a.opf, z, scl, 1.0, false, spb + z.l * 5 * 2 * NSP);
   __syncthreads();
   store_tiles<DIR, WPL, false>(c, T, tsz, a.q, fs, 5);
 }
