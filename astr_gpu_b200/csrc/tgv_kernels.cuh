@@ -369,7 +369,8 @@ __device__ __forceinline__ void dsolve_n(double (&v)[NV][S], int K0, const PassA
 
 // Solves of NV staged tile lines (derivative or filter) in place, together; `stride` separates
 // the lines of consecutive solves.
-// KIND: OP_DERIV or OP_FILTER, the operator's kind known at compile time.
+// KIND: OP_DERIV or OP_FILTER, the operator's kind known at compile time, or -1: read from op
+// (one instantiation serving both kinds, which some passes allocate registers better with).
 template <int S, int WPL, int NV, int KIND>
 __device__ __forceinline__ void solve_lines_n(double* line, int stride, const LineOp& op, const LaneIds& z, double* scl,
                                               double scale, bool images, const double* sp) {
@@ -377,7 +378,8 @@ __device__ __forceinline__ void solve_lines_n(double* line, int stride, const Li
 #pragma unroll
   for (int i = 0; i < NV; ++i) {
     const double* li = line + i * stride;
-    if (KIND == OP_FILTER) rhs_filter<S>(v[i], op, z.seg, [li](int n) { return li[n]; }, sp + i * 2 * NSP);
+    if (KIND == OP_FILTER || (KIND < 0 && op.kind == OP_FILTER))
+      rhs_filter<S>(v[i], op, z.seg, [li](int n) { return li[n]; }, sp + i * 2 * NSP);
     else rhs_deriv<S>(v[i], op, z.seg, [li](int n) { return li[n]; }, sp + i * 2 * NSP);
   }
   seg_solve_n<S, WPL, NV>(v, op.tab, z.seg, z.lane, z.part, z.l, scl);
@@ -786,7 +788,7 @@ __device__ __forceinline__ void k_pass_vbs_body(const PassArgs& a, int bx, int b
   stream_fields(c, sm, tsz, 5, nbuf, fps, [&](int m) { return a.VF + (5 + m) * fs; }, [&](int m0, int cnt, double* T) {
     tile_specials<OP_DERIV>(a.opd, c.TI, c.LP, T, tsz, cnt, spb);
     __syncthreads();
-    solve_tile<S, WPL, OP_DERIV>(T, tsz, cnt, c.TI, c.LP, a.LPW, a.opd, z, scl, a.g.rd[DIR], spb);
+    solve_tile<S, WPL, -1>(T, tsz, cnt, c.TI, c.LP, a.LPW, a.opd, z, scl, a.g.rd[DIR], spb);
     __syncthreads();
     if (a.mode == 0) {
       store_tiles<DIR, WPL, true>(c, T, tsz, a.R + m0 * fs, fs, cnt);
@@ -822,7 +824,7 @@ __device__ __forceinline__ void k_pass_vbs_body(const PassArgs& a, int bx, int b
     if (a.do_filter) {
       tile_specials<OP_FILTER>(a.opf, c.TI, c.LP, T, tsz, cnt, spb);
       __syncthreads();
-      solve_tile<S, WPL, OP_FILTER>(T, tsz, cnt, c.TI, c.LP, a.LPW, a.opf, z, scl, 1.0, spb);
+      solve_tile<S, WPL, -1>(T, tsz, cnt, c.TI, c.LP, a.LPW, a.opf, z, scl, 1.0, spb);
       __syncthreads();
     }
     store_tiles<DIR, WPL, false>(c, T, tsz, a.qout + m0 * fs, fs, cnt);
