@@ -515,7 +515,9 @@ __device__ __forceinline__ void k_pass_ab_body(const PassArgs& a, int bx, int by
 // Gradients along C, viscous stress and heat flux at every node (diffusion,
 // tgvsolver.F90:635-694) with the A and B gradients, the viscous fluxes of A and B stored for
 // passes A' and B', diagnostics, then R = D_C(VF_C - F_C) (the first contribution to R).
-template <int S, int WPL, int DIR>
+// DIAG: the stage-1 form with the diagnostics partial sums (a.partials); stages 2 and 3 run a
+// kernel without them (fewer live registers in the flux loop).
+template <int S, int WPL, int DIR, bool DIAG>
 __device__ __forceinline__ void k_pass_c_body(const PassArgs& a, int bx, int by) {
   extern __shared__ double sm[];
   const TileCtx<DIR, WPL> c(a, bx, by);
@@ -569,7 +571,7 @@ __device__ __forceinline__ void k_pass_c_body(const PassArgs& a, int bx, int by)
   constexpr int dA = DIR_A, dB = DIR_B, dC = DIR_C;
   static_assert(DIR == DIR_C, "pass C runs along DIR_C");
   double ke = 0.0, en = 0.0, di = 0.0;
-  const bool diag = a.partials != nullptr;
+  const bool diag = DIAG && a.partials != nullptr;
   int bad = 0;
   if (c.svalid) {
     const double* DA = a.DA + c.sbase;
@@ -1003,7 +1005,7 @@ __device__ __forceinline__ const PassArgs& batch_decode(const BatchArgs& b, Pass
 
 #define ASTR_COMMA ,
 ASTR_PASS_KERNELS(k_pass_ab, int S ASTR_COMMA int WPL ASTR_COMMA int DIR ASTR_COMMA bool IS_A, S ASTR_COMMA WPL ASTR_COMMA DIR ASTR_COMMA IS_A)
-ASTR_PASS_KERNELS(k_pass_c, int S ASTR_COMMA int WPL ASTR_COMMA int DIR, S ASTR_COMMA WPL ASTR_COMMA DIR)
+ASTR_PASS_KERNELS(k_pass_c, int S ASTR_COMMA int WPL ASTR_COMMA int DIR ASTR_COMMA bool DIAG, S ASTR_COMMA WPL ASTR_COMMA DIR ASTR_COMMA DIAG)
 ASTR_PASS_KERNELS(k_pass_va, int S ASTR_COMMA int WPL ASTR_COMMA int DIR, S ASTR_COMMA WPL ASTR_COMMA DIR)
 ASTR_PASS_KERNELS(k_pass_vb, int S ASTR_COMMA int WPL ASTR_COMMA int DIR, S ASTR_COMMA WPL ASTR_COMMA DIR)
 ASTR_PASS_KERNELS(k_pass_f, int S ASTR_COMMA int WPL ASTR_COMMA int DIR, S ASTR_COMMA WPL ASTR_COMMA DIR)
@@ -1045,7 +1047,9 @@ cudaError_t launch_pass_t(int pass, const PassArgs& a, cudaStream_t st) {
   switch (pass) {
     case PASS_A: return launch_k(k_pass_ab<S, WPL, DIR_A, true>, grid, threads, smem, st, a);
     case PASS_B: return launch_k(k_pass_ab<S, WPL, DIR_B, false>, grid, threads, smem, st, a);
-    case PASS_C: return launch_k(k_pass_c<S, WPL, DIR_C>, grid, threads, smem, st, a);
+    case PASS_C:
+      return a.partials ? launch_k(k_pass_c<S, WPL, DIR_C, true>, grid, threads, smem, st, a)
+                        : launch_k(k_pass_c<S, WPL, DIR_C, false>, grid, threads, smem, st, a);
     case PASS_VA:
       if (a.FPS == 1) return launch_k(k_pass_vas<S, WPL, DIR_A>, grid, threads, smem, st, a);
       return launch_k(k_pass_va<S, WPL, DIR_A>, grid, threads, smem, st, a);
@@ -1087,7 +1091,7 @@ cudaError_t launch_pass_batch_t(int pass, int dir, const PassArgs* dargs, const 
   switch (pass) {
     case PASS_A: return launch_kb(k_pass_ab_batch<S, WPL, DIR_A, true>, nctas, threads, smem, st, b);
     case PASS_B: return launch_kb(k_pass_ab_batch<S, WPL, DIR_B, false>, nctas, threads, smem, st, b);
-    case PASS_C: return launch_kb(k_pass_c_batch<S, WPL, DIR_C>, nctas, threads, smem, st, b);
+    case PASS_C: return launch_kb(k_pass_c_batch<S, WPL, DIR_C, true>, nctas, threads, smem, st, b);
     case PASS_VA: return launch_kb(k_pass_va_batch<S, WPL, DIR_A>, nctas, threads, smem, st, b);
     case PASS_VB: return launch_kb(k_pass_vb_batch<S, WPL, DIR_B>, nctas, threads, smem, st, b);
     case PASS_F:
