@@ -1003,6 +1003,16 @@ int astr_full_create(astr_ctx* ctx, const astr_params* p, astr_full** out) {
     astr_ctx_set_error(ctx, "conschm must be 0 or 643 (central compact) or 543 (upwind compact flux)");
     return ASTR_ERR_ARG;
   }
+  if (upwind && !(std::isfinite(p->bfacmpld) && (!p->lchardecomp || std::isfinite(p->shkcrt)))) {
+    delete fs;
+    astr_ctx_set_error(ctx, "bfacmpld (and shkcrt with the characteristic decomposition) must be finite");
+    return ASTR_ERR_ARG;
+  }
+  if (!(p->mach > 0.0 && p->gamma > 1.0 && p->reynolds > 0.0 && p->prandtl > 0.0)) {
+    delete fs;
+    astr_ctx_set_error(ctx, "mach, reynolds and prandtl must be positive and gamma above 1");
+    return ASTR_ERR_ARG;
+  }
   if (p->lchardecomp && !upwind) fs->p.lchardecomp = 0;   // the decomposition belongs to convrsdcmp
   if (fs->p.lchardecomp && (g.ntype[0] != 3 || g.ntype[1] != 3 || g.ntype[2] != 3)) {
     delete fs;

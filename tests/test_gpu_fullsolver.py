@@ -306,6 +306,15 @@ def test_full_upwind_characteristic_steps_match_oracle(ctx):
     s.close()
 
 
+def test_full_solver_rejects_bad_parameters(ctx):
+    import astr_gpu_b200 as ag
+    for kw in (dict(conschm=543, bfacmpld=float("nan")), dict(conschm=543, lchardecomp=True, shkcrt=float("inf")),
+               dict(mach=0.0), dict(gamma=1.0), dict(conschm=642)):
+        with pytest.raises(ag.AstrError) as e:
+            ag.FullSolver(ctx, 32, params=ag.FlowParams(**kw))
+        assert e.value.code == -1, kw
+
+
 def test_characteristic_mode_rejects_walls(ctx):
     import astr_gpu_b200 as ag
     with pytest.raises(ag.AstrError) as e:
