@@ -523,7 +523,9 @@ __global__ void k_fs_char_flux(double* Fh, const double* fsp, const double* fsm,
   }
 }
 
-// qrhs(i) = qrhs(i) + Fh(i) - Fh(i-1) at nodes 0..N, Fh stored per interface (solver.F90:1509-1513)
+// qrhs(i) = qrhs(i) + Fh(i) - Fh(i-1) at nodes 0..N, Fh stored per interface (solver.F90:1509-1513),
+// kept negated: rhscal negates qrhs after the convection (qrhs = -qrhs, solver.F90:243), and with
+// q holding -qrhs, (q - Fh(i)) + Fh(i-1) is -((qrhs + Fh(i)) - Fh(i-1)) exactly.
 __global__ void k_fs_flux_diff(double* qrhs, const double* Fh, int dir, FsGeo g) {
   const Box3 b = box_line(g, -1, 0, 0);
   const int64_t sd = g.s_(dir);
@@ -532,7 +534,7 @@ __global__ void k_fs_flux_diff(double* qrhs, const double* Fh, int dir, FsGeo g)
     int i, j, k;
     b.node(p - (int64_t)m * b.size(), i, j, k);
     const int64_t o = m * g.fs + g.at(i, j, k);
-    qrhs[o] = qrhs[o] + Fh[o] - Fh[o - sd];
+    qrhs[o] = (qrhs[o] - Fh[o]) + Fh[o - sd];
   }
 }
 
@@ -604,17 +606,6 @@ __global__ void k_fs_visc_flux(double* F, const double* sigma, const double* qfl
       F[n * g.fs + o] = sigma[sg * g.fs + o] * dxi * jb;
     }
     F[3 * g.fs + o] = qflux[dir * g.fs + o] * dxi * jb;
-  }
-}
-
-__global__ void k_fs_negate(double* f, FsGeo g) {
-  const Box3 b = box_line(g, -1, 0, 0);
-  GRID_STRIDE(p, b.size() * 5) {
-    const int m = (int)(p / b.size());
-    int i, j, k;
-    b.node(p - (int64_t)m * b.size(), i, j, k);
-    const int64_t o = m * g.fs + g.at(i, j, k);
-    f[o] = -f[o];
   }
 }
 
@@ -881,16 +872,15 @@ cudaError_t fs_stage_rhs(astr_full* fs, bool diag) {
   if (fs->up) {
     if ((e = fs_convection_upwind(fs)) != cudaSuccess) return e;
   } else {
-    // convrsdcal6
+    // convrsdcal6, accumulated negated (scale -1: qrhs holds -qrhs, which is what rhscal's
+    // qrhs = -qrhs leaves; negation is exact, so the sums are the reference's bit for bit)
     for (int d = 0; d < 3; ++d) {
       const int64_t nl = nn / (g.N[d] + 1) * (g.N[d] + 1 + 2 * HMW);
       k_fs_conv_flux<<<blocks_for(nl), 256, 0, st>>>(fs->work, fs->q, fs->vel, fs->prs, d, g);
       if ((e = cudaGetLastError()) != cudaSuccess) return e;
-      if ((e = line_op(fs, fs->dd[d], d, fs->work, fs->qrhs, 5, 1.0, 1)) != cudaSuccess) return e;
+      if ((e = line_op(fs, fs->dd[d], d, fs->work, fs->qrhs, 5, -1.0, 1)) != cudaSuccess) return e;
     }
   }
-  k_fs_negate<<<blocks_for(5 * nn), 256, 0, st>>>(fs->qrhs, g);
-  if ((e = cudaGetLastError()) != cudaSuccess) return e;
   // diffrsdcal6
   k_fs_stress<<<blocks_for(nn), 256, 0, st>>>(fs->sigma, fs->qflux, fs->dvel, fs->dtmp, fs->vel, fs->tmp, g, fs->th);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
