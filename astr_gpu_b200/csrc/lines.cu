@@ -53,10 +53,11 @@ __device__ __forceinline__ Slot slot_of(int dir, int TI) {
 
 }  // namespace
 
-// One-warp-per-line layouts launch 256-thread CTAs: bounding them for three CTAs per SM keeps 24
-// warps resident instead of the 16 that their register use would otherwise allow.
+// One-warp-per-line layouts launch 256-thread CTAs: bounding them for three CTAs per SM (four for
+// up to 5 rows per lane, which then still need no spills) keeps 24 or 32 warps resident instead
+// of the 16 that their register use would otherwise allow.
 template <int S, int WPL>
-__global__ void __launch_bounds__(WPL == 1 ? 256 : 512, WPL == 1 ? 3 : 1) k_line_api(LineOp op, int dir, const double* __restrict__ f, ArrDesc fa,
+__global__ void __launch_bounds__(WPL == 1 ? 256 : 512, WPL == 1 ? (S <= 5 ? 4 : 3) : 1) k_line_api(LineOp op, int dir, const double* __restrict__ f, ArrDesc fa,
                                                   double* __restrict__ out, ArrDesc oa, int TI, int LP, double scale,
                                                   int flags) {
   extern __shared__ double sm[];
