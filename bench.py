@@ -722,9 +722,10 @@ def run_full(args, ws, rank, local):
     n = args.full_size
     stream = torch.cuda.Stream(device=local)
     ctx = ag.Context(local, stream=stream)
+    ntype = tuple(int(t) for t in args.full_ntype.split(","))
     s = ag.FullSolver(ctx, n, params=ag.FlowParams(sutherland=110.3, beta_bound=0.98, conschm=args.conschm,
                                                    bfacmpld=args.bfac, lchardecomp=args.chardecomp,
-                                                   shkcrt=args.shkcrt))
+                                                   shkcrt=args.shkcrt, ntype=ntype, twall=1.0))
     s.set_q(tgv_q(n, 0.1))
     dt = 1e-3
     s.step(dt, args.warmup)
@@ -744,7 +745,8 @@ def run_full(args, ws, rank, local):
                                        f"dt {dt}, " + ("central compact convection (643)" if args.conschm != 543 else
                                                        f"upwind compact flux convection (543, b {args.bfac}"
                                                        + (f", characteristic, shkcrt {args.shkcrt})" if args.chardecomp
-                                                          else ")")),
+                                                          else ")"))
+                                       + ("" if ntype == (3, 3, 3) else f", ntype {ntype} with isothermal no-slip walls"),
                            "grid": n},
                 "gpu_launches": None, "clocks": clk.summary()}
         print(json.dumps(line), flush=True)
@@ -787,6 +789,8 @@ def main():
     ap.add_argument("--conschm", type=int, default=643, choices=[643, 543], help="convection of --workload full")
     ap.add_argument("--bfac", type=float, default=0.3, help="b factor of the upwind compact flux (--conschm 543)")
     ap.add_argument("--chardecomp", action="store_true", help="--conschm 543 in characteristic variables")
+    ap.add_argument("--full-ntype", default="3,3,3",
+                    help="boundary type per direction of --workload full (3 periodic, 4 no-slip walls at both ends)")
     ap.add_argument("--shkcrt", type=float, default=0.01, help="Ducros sensor threshold (--chardecomp)")
     ap.add_argument("--grad-size", type=int, default=256)
     ap.add_argument("--adj-size", type=int, default=128)
