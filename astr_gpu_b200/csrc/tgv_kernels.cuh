@@ -990,13 +990,17 @@ __device__ __forceinline__ const PassArgs& batch_decode(const BatchArgs& b, Pass
   return sa;
 }
 
-#define ASTR_PASS_KERNELS(NAME, TPARAMS, TARGS)                                      \
-  template <TPARAMS>                                                                   \
-  __global__ void __launch_bounds__(512) NAME(PassArgs a) {                            \
-    NAME##_body<TARGS>(a, blockIdx.x, blockIdx.y);                                     \
-  }                                                                                    \
-  template <TPARAMS>                                                                   \
-  __global__ void __launch_bounds__(512) NAME##_batch(BatchArgs b) {                   \
+// The small-box layout (3 rows per lane, one warp per line) is bounded for two 512-thread CTAs per
+// SM where that costs no more than a few spilled words (every pass but C): the boxes that use it
+// have small grids, and the SMs they fill need the second CTA to hide latency.
+#define ASTR_MINB(S, WPL, SMALL) (((SMALL) && (S) == 3 && (WPL) == 1) ? 2 : 1)
+#define ASTR_PASS_KERNELS(NAME, SMALL, TPARAMS, TARGS)                                          \
+  template <TPARAMS>                                                                              \
+  __global__ void __launch_bounds__(512, ASTR_MINB(S, WPL, SMALL)) NAME(PassArgs a) {             \
+    NAME##_body<TARGS>(a, blockIdx.x, blockIdx.y);                                                \
+  }                                                                                               \
+  template <TPARAMS>                                                                              \
+  __global__ void __launch_bounds__(512, ASTR_MINB(S, WPL, SMALL)) NAME##_batch(BatchArgs b) {    \
     __shared__ PassArgs sa;                                                            \
     int bx, by;                                                                        \
     const PassArgs& a = batch_decode(b, sa, bx, by);                                   \
@@ -1004,18 +1008,18 @@ __device__ __forceinline__ const PassArgs& batch_decode(const BatchArgs& b, Pass
   }
 
 #define ASTR_COMMA ,
-ASTR_PASS_KERNELS(k_pass_ab, int S ASTR_COMMA int WPL ASTR_COMMA int DIR ASTR_COMMA bool IS_A, S ASTR_COMMA WPL ASTR_COMMA DIR ASTR_COMMA IS_A)
-ASTR_PASS_KERNELS(k_pass_c, int S ASTR_COMMA int WPL ASTR_COMMA int DIR ASTR_COMMA bool DIAG, S ASTR_COMMA WPL ASTR_COMMA DIR ASTR_COMMA DIAG)
-ASTR_PASS_KERNELS(k_pass_va, int S ASTR_COMMA int WPL ASTR_COMMA int DIR, S ASTR_COMMA WPL ASTR_COMMA DIR)
-ASTR_PASS_KERNELS(k_pass_vb, int S ASTR_COMMA int WPL ASTR_COMMA int DIR, S ASTR_COMMA WPL ASTR_COMMA DIR)
-ASTR_PASS_KERNELS(k_pass_f, int S ASTR_COMMA int WPL ASTR_COMMA int DIR, S ASTR_COMMA WPL ASTR_COMMA DIR)
+ASTR_PASS_KERNELS(k_pass_ab, true, int S ASTR_COMMA int WPL ASTR_COMMA int DIR ASTR_COMMA bool IS_A, S ASTR_COMMA WPL ASTR_COMMA DIR ASTR_COMMA IS_A)
+ASTR_PASS_KERNELS(k_pass_c, false, int S ASTR_COMMA int WPL ASTR_COMMA int DIR ASTR_COMMA bool DIAG, S ASTR_COMMA WPL ASTR_COMMA DIR ASTR_COMMA DIAG)
+ASTR_PASS_KERNELS(k_pass_va, true, int S ASTR_COMMA int WPL ASTR_COMMA int DIR, S ASTR_COMMA WPL ASTR_COMMA DIR)
+ASTR_PASS_KERNELS(k_pass_vb, true, int S ASTR_COMMA int WPL ASTR_COMMA int DIR, S ASTR_COMMA WPL ASTR_COMMA DIR)
+ASTR_PASS_KERNELS(k_pass_f, true, int S ASTR_COMMA int WPL ASTR_COMMA int DIR, S ASTR_COMMA WPL ASTR_COMMA DIR)
 #undef ASTR_PASS_KERNELS
 #undef ASTR_COMMA
 
 // streamed forms: single-box launches only (the batched ensemble passes take all fields at once)
 #define ASTR_STREAM_KERNEL(NAME)                                         \
   template <int S, int WPL, int DIR>                                     \
-  __global__ void __launch_bounds__(512) NAME(PassArgs a) {              \
+  __global__ void __launch_bounds__(512, ASTR_MINB(S, WPL, true)) NAME(PassArgs a) { \
     NAME##_body<S, WPL, DIR>(a, blockIdx.x, blockIdx.y);                 \
   }
 ASTR_STREAM_KERNEL(k_pass_vas)
