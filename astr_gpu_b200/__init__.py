@@ -10,6 +10,10 @@ Host-side mirror of the reference's interface (Perrbit/astr_gpu), over the C ABI
   ``stacal`` (miniapps/tgv_solver_3d/tgvsolver.F90)
 * ``FullSolver`` — the full solver's ``time_integration_rk`` / ``rhscal`` on a periodic box
   (src/mainloop.F90:298-476, src/solver.F90:184-283)
+* ``h5io_init`` / ``H5File`` — the HDF5 file interface of the reference's checkpoints
+  (src/hdf5io.F90: h5io_init, h5write, h5read, h5io_end), without the HDF5 library; the solvers'
+  ``write_flowfield`` / ``read_flowfield`` are writeflfed's flow field and readcheckpoint + updateq
+  (src/readwrite.F90:1378-1528, 1720-1979)
 
 Arrays are Fortran-ordered numpy arrays (host) or CUDA torch tensors laid out the same way
 (device). All compute runs in the CUDA library; there is no CPU path.
@@ -26,7 +30,7 @@ from ._lib import ASTR_DEVICE, ASTR_HOST, AstrParams
 
 __all__ = ["AstrError", "Context", "Scheme", "fd_scheme_initiate", "compact_filter_initiate", "central",
            "compact_filter", "compact_flux_initiate", "flux_compact", "flux_difference", "FlowParams",
-           "TGVSolver", "FullSolver", "Ensemble"]
+           "TGVSolver", "FullSolver", "Ensemble", "H5File", "h5io_init"]
 
 
 class AstrError(RuntimeError):
@@ -233,6 +237,99 @@ class FlowParams:
                           float(self.bfacmpld), int(self.lchardecomp), float(self.shkcrt))
 
 
+class H5File:
+    """One HDF5 file opened by ``h5io_init`` (src/hdf5io.F90:86-135): mode "read", "write"
+    (create or truncate) or "rdwr" (add datasets to an existing file, as h5srite does). Arrays are
+    Fortran-ordered: a dataset's HDF5 dataspace is the reversed shape, as the reference's Fortran
+    HDF5 calls store it. Host memory only; needs no GPU."""
+
+    def __init__(self, filename: str, mode: str = "read"):
+        self.L = _lib.load()
+        h = ctypes.c_void_p()
+        rc = self.L.astr_h5io_init(str(filename).encode(), mode.encode(), ctypes.byref(h))
+        if rc != 0:
+            raise AstrError(rc, self.L.astr_h5_last_error(None).decode())
+        self._h = h
+        self.filename, self.mode = str(filename), mode
+
+    def _check(self, rc):
+        if rc != 0:
+            raise AstrError(rc, self.L.astr_h5_last_error(self._h).decode())
+
+    def names(self) -> list[str]:
+        n = ctypes.c_int()
+        self._check(self.L.astr_h5_count(self._h, ctypes.byref(n)))
+        out = []
+        for i in range(n.value):
+            buf = ctypes.create_string_buffer(4096)
+            self._check(self.L.astr_h5_name(self._h, i, buf, len(buf)))
+            out.append(buf.value.decode())
+        return out
+
+    def info(self, varname: str):
+        """(Fortran shape, type class 0 integer / 1 float / -1 other, element size)."""
+        rank, cls, size = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        dims = (ctypes.c_int64 * 32)()
+        self._check(self.L.astr_h5_dataset_info(self._h, varname.encode(), ctypes.byref(rank), dims,
+                                                ctypes.byref(cls), ctypes.byref(size)))
+        return tuple(dims[i] for i in range(rank.value)), cls.value, size.value
+
+    def write(self, varname: str, var):
+        """h5write: a real(8) or integer(4) dataset from a numpy array (float64 or int32)."""
+        a = np.asfortranarray(var)
+        dims = (ctypes.c_int64 * max(a.ndim, 1))(*(a.shape or (1,)))
+        if a.dtype == np.int32:
+            fn = self.L.astr_h5write_i4
+        else:
+            a = np.asfortranarray(a, dtype=np.float64)
+            fn = self.L.astr_h5write_r8
+        self._check(fn(self._h, varname.encode(), max(a.ndim, 1), dims, ctypes.c_void_p(a.ctypes.data)))
+
+    def read(self, varname: str, shape=None, offset=None, mode: str = "h", dtype=np.float64) -> np.ndarray:
+        """h5read: the block of Fortran `shape` at `offset` of the dataset (mode 'h'; default the
+        whole dataset), or prod(shape) elements from element offset[0] of a 1-D dataset (mode 's',
+        the stream layout); float64, or int32 for integer datasets."""
+        if shape is None:
+            shape = self.info(varname)[0]
+        shape = tuple(int(x) for x in shape)
+        out = np.zeros(shape, dtype=np.int32 if np.dtype(dtype) == np.int32 else np.float64, order="F")
+        dims = (ctypes.c_int64 * len(shape))(*shape)
+        off = None if offset is None else (ctypes.c_int64 * len(offset))(*[int(x) for x in offset])
+        fn = self.L.astr_h5read_i4 if out.dtype == np.int32 else self.L.astr_h5read_r8
+        self._check(fn(self._h, varname.encode(), len(shape), dims, off, mode.encode(), ctypes.c_void_p(out.ctypes.data)))
+        return out
+
+    def close(self):
+        """h5io_end (src/hdf5io.F90:149-163)."""
+        if getattr(self, "_h", None):
+            h, self._h = self._h, None
+            rc = self.L.astr_h5io_end(h)
+            if rc != 0:
+                raise AstrError(rc, self.L.astr_h5_last_error(None).decode())
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def h5io_init(filename: str, mode: str = "read") -> H5File:
+    return H5File(filename, mode)
+
+
+def _read_flowfield(ctx, fn, h, filename, mode):
+    ns, t = ctypes.c_int(), ctypes.c_double()
+    ctx.check(fn(h, str(filename).encode(), mode.encode(), ctypes.byref(ns), ctypes.byref(t)))
+    return ns.value, t.value
+
+
 class TGVSolver:
     """The miniapp ``boxsolver`` on the GPU: a periodic im x jm x km box advanced by SSP-RK3 with
     the compact scheme and the compact filter (tgvsolver.F90:994-1082)."""
@@ -297,6 +394,14 @@ class TGVSolver:
 
     def rk3(self, dt: float, nsteps: int = 1):
         self.ctx.check(self.ctx.L.astr_rk3_step(self._h, dt, nsteps))
+
+    def write_flowfield(self, filename: str):
+        """writeflfed's flow field: ro, u1, u2, u3, p, t (q2fvar of the state), nstep, time."""
+        self.ctx.check(self.ctx.L.astr_state_write_flowfield(self._h, str(filename).encode()))
+
+    def read_flowfield(self, filename: str, mode: str = "h"):
+        """readcheckpoint's flow field + updateq; returns (nstep, time), which the state takes."""
+        return _read_flowfield(self.ctx, self.ctx.L.astr_state_read_flowfield, self._h, filename, mode)
 
     def rk3_host(self, q: np.ndarray, dt: float, nsteps: int = 1) -> np.ndarray:
         """One call with the state in host memory (uploaded, advanced, downloaded in place)."""
@@ -391,6 +496,15 @@ class FullSolver:
 
     def step(self, dt: float, nsteps: int = 1):
         self.ctx.check(self.ctx.L.astr_full_step(self._h, dt, nsteps))
+
+    def write_flowfield(self, filename: str):
+        """writeflfed's flow field: the primitive arrays ro, u1, u2, u3, p, t, nstep, time."""
+        self.ctx.check(self.ctx.L.astr_full_write_flowfield(self._h, str(filename).encode()))
+
+    def read_flowfield(self, filename: str, mode: str = "h"):
+        """readcheckpoint + updateq: q from the file's (ro, u, t), interior primitives as read;
+        returns (nstep, time), which the solver takes."""
+        return _read_flowfield(self.ctx, self.ctx.L.astr_full_read_flowfield, self._h, filename, mode)
 
     def rhs(self) -> np.ndarray:
         """One stage's filterq + qswap + rhscal (the state keeps the filtered, averaged q)."""

@@ -81,6 +81,20 @@ SIGNATURES = {
     "astr_full_step": (_i, [_vp, _d, _i]),
     "astr_full_rhs": (_i, [_vp, _vp, _i64p, _i64p, _i]),
     "astr_full_history": (_i, [_vp, _dp, _i, _ip]),
+    "astr_h5io_init": (_i, [ctypes.c_char_p, ctypes.c_char_p, _pvp]),
+    "astr_h5io_end": (_i, [_vp]),
+    "astr_h5_last_error": (ctypes.c_char_p, [_vp]),
+    "astr_h5write_r8": (_i, [_vp, ctypes.c_char_p, _i, _i64p, _vp]),
+    "astr_h5write_i4": (_i, [_vp, ctypes.c_char_p, _i, _i64p, _vp]),
+    "astr_h5read_r8": (_i, [_vp, ctypes.c_char_p, _i, _i64p, _i64p, ctypes.c_char, _vp]),
+    "astr_h5read_i4": (_i, [_vp, ctypes.c_char_p, _i, _i64p, _i64p, ctypes.c_char, _vp]),
+    "astr_h5_dataset_info": (_i, [_vp, ctypes.c_char_p, _ip, _i64p, _ip, _ip]),
+    "astr_h5_count": (_i, [_vp, _ip]),
+    "astr_h5_name": (_i, [_vp, _i, ctypes.c_char_p, _i]),
+    "astr_state_write_flowfield": (_i, [_vp, ctypes.c_char_p]),
+    "astr_state_read_flowfield": (_i, [_vp, ctypes.c_char_p, ctypes.c_char, _ip, _dp]),
+    "astr_full_write_flowfield": (_i, [_vp, ctypes.c_char_p]),
+    "astr_full_read_flowfield": (_i, [_vp, ctypes.c_char_p, ctypes.c_char, _ip, _dp]),
 }
 
 _libs = {}

@@ -18,7 +18,7 @@ LIB = os.path.join(HERE, "libastr_b200.so")
 LIB_STRICT = os.path.join(HERE, "libastr_b200_strict.so")
 SOURCES = ["capi.cu", "tgv.cu", "lines.cu", "schemes.cu", "tgv_l3_1.cu", "tgv_l5_1.cu", "tgv_l9_1.cu", "tgv_l9_2.cu",
            "tgv_l9_4.cu", "tgv_l5_2.cu", "tgv_l5_4.cu", "tgv_l17_1.cu", "noalloc.cu", "fullsolver.cu", "adjoint.cu", "adj_l3_1.cu", "adj_l5_1.cu",
-           "adj_l9_1.cu", "adj_l9_2.cu", "adj_l9_4.cu", "adj_l5_2.cu", "adj_l5_4.cu"]
+           "adj_l9_1.cu", "adj_l9_2.cu", "adj_l9_4.cu", "adj_l5_2.cu", "adj_l5_4.cu", "checkpoint.cu", "h5file.cpp"]
 HEADERS = ["ops.cuh", "internal.h", "tgv.cuh", "tgv_kernels.cuh", "adjoint.cuh", "adj_kernels.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
@@ -56,7 +56,7 @@ def build(force: bool = False, verbose: bool = False, extra: list[str] | None = 
         flags.extend(extra)
     procs, objs = [], []
     for src in SOURCES:
-        obj = os.path.join(objdir, src.replace(".cu", ".o"))
+        obj = os.path.join(objdir, os.path.splitext(src)[0] + ".o")
         objs.append(obj)
         procs.append(subprocess.Popen([nvcc(), *flags, "-c", os.path.join(CSRC, src), "-o", obj],
                                       stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True))

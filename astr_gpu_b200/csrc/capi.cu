@@ -118,6 +118,9 @@ struct DeviceGuard {
   DeviceGuard& operator=(const DeviceGuard&) = delete;
 };
 
+// History rows written so far (the step counter may start elsewhere after a restart).
+int hist_rows(const astr_state* st) { return (int)(st->row_key.size() / 2); }
+
 #define CK(call)                                          \
   do {                                                    \
     cudaError_t e_ = (call);                              \
@@ -806,6 +809,54 @@ int astr_state_download(astr_state* st, double* q, const int64_t shape[3], const
   return ASTR_OK;
 }
 
+int astr_state_write_flowfield(astr_state* st, const char* filename) {
+  const DeviceGuard dg_(st ? st->ctx->device : -1);
+  if (!st || !filename) return ASTR_ERR_ARG;
+  astr_ctx* ctx = st->ctx;
+  const int64_t shape[3] = {st->p.im + 1, st->p.jm + 1, st->p.km + 1}, lb[3] = {0, 0, 0};
+  const int64_t n = shape[0] * shape[1] * shape[2];
+  double* buf = nullptr;   // q (5 fields), then the file's 6 primitive fields
+  if (cudaMalloc(&buf, 11 * (size_t)n * sizeof(double)) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(ctx, ASTR_ERR_NOMEM, "flow-field buffers");
+  }
+  int rc = astr_state_download(st, buf, shape, lb, ASTR_DEVICE);
+  if (rc == ASTR_OK) {
+    cudaError_t e = flowfield_prims_from_q(ctx->stream, buf, buf + 5 * n, n, st->p.mach, st->p.gamma);
+    rc = e != cudaSuccess ? cuda_fail(ctx, e, "q2fvar") : flowfield_write(ctx->stream, buf + 5 * n, shape, st->nstep,
+                                                                          st->time, filename, ctx->err);
+  }
+  cudaFree(buf);
+  return rc;
+}
+
+int astr_state_read_flowfield(astr_state* st, const char* filename, char mode, int* nstep, double* time) {
+  const DeviceGuard dg_(st ? st->ctx->device : -1);
+  if (!st || !filename) return ASTR_ERR_ARG;
+  astr_ctx* ctx = st->ctx;
+  const int64_t shape[3] = {st->p.im + 1, st->p.jm + 1, st->p.km + 1}, lb[3] = {0, 0, 0};
+  const int64_t n = shape[0] * shape[1] * shape[2];
+  double* buf = nullptr;
+  if (cudaMalloc(&buf, 11 * (size_t)n * sizeof(double)) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(ctx, ASTR_ERR_NOMEM, "flow-field buffers");
+  }
+  int ns = 0;
+  double t = 0.0;
+  int rc = flowfield_read(ctx->stream, buf + 5 * n, shape, filename, mode, &ns, &t, ctx->err);
+  if (rc == ASTR_OK) {
+    cudaError_t e = flowfield_q_from_prims(ctx->stream, buf + 5 * n, buf, n, st->p.mach, st->p.gamma);
+    rc = e != cudaSuccess ? cuda_fail(ctx, e, "fvar2q") : astr_state_upload(st, buf, shape, lb, ASTR_DEVICE);
+  }
+  cudaFree(buf);
+  if (rc != ASTR_OK) return rc;
+  st->nstep = ns;
+  st->time = t;
+  if (nstep) *nstep = ns;
+  if (time) *time = t;
+  return ASTR_OK;
+}
+
 int astr_cfl_dt(astr_state* st, double cfl, double* dt) {
   const DeviceGuard dg_(st ? st->ctx->device : -1);
   if (!st || !dt) return ASTR_ERR_ARG;
@@ -905,7 +956,7 @@ int astr_rk3_step(astr_state* st, double dt, int nsteps) {
   const DeviceGuard dg_(st ? st->ctx->device : -1);
   if (!st || nsteps < 0 || !(dt > 0.0)) return ASTR_ERR_ARG;
   astr_ctx* ctx = st->ctx;
-  if (st->nstep + nsteps > st->hist_cap) return fail(ctx, ASTR_ERR_UNSUPPORTED, "history buffer full (65536 steps)");
+  if (hist_rows(st) + nsteps > st->hist_cap) return fail(ctx, ASTR_ERR_UNSUPPORTED, "history buffer full (65536 steps)");
   if (st->autotune && !st->tuned && nsteps > 0) {
     drop_graphs(st);
     CK(autotune(st));
@@ -951,8 +1002,8 @@ int astr_rk3_step_host(astr_state* st, double* q, const int64_t shape[3], const 
   CK(finalize_filter(st));
   rc = copy_fields(st, st->Q0, q, shape, lbound, 0, ASTR_HOST);
   if (rc) return rc;
-  if (diag_out && st->nstep > 0) {
-    CK(cudaMemcpyAsync(diag_out, st->hist + 3 * (size_t)(st->nstep - 1), 3 * sizeof(double), cudaMemcpyDeviceToHost,
+  if (diag_out && hist_rows(st) > 0) {
+    CK(cudaMemcpyAsync(diag_out, st->hist + 3 * (size_t)(hist_rows(st) - 1), 3 * sizeof(double), cudaMemcpyDeviceToHost,
                        ctx->stream));
   }
   CK(cudaStreamSynchronize(ctx->stream));
@@ -963,7 +1014,7 @@ int astr_pass_timings(astr_state* st, double dt, int nsteps, double ms[8]) {
   const DeviceGuard dg_(st ? st->ctx->device : -1);
   if (!st || !ms || nsteps < 1) return ASTR_ERR_ARG;
   astr_ctx* ctx = st->ctx;
-  if (st->nstep + nsteps > st->hist_cap) return fail(ctx, ASTR_ERR_UNSUPPORTED, "history buffer full");
+  if (hist_rows(st) + nsteps > st->hist_cap) return fail(ctx, ASTR_ERR_UNSUPPORTED, "history buffer full");
   PassTimer timer;
   g_timer = &timer;
   cudaError_t e = cudaSuccess;
@@ -994,7 +1045,7 @@ int astr_history(astr_state* st, double* rows, int maxrows, int* nrows) {
   const DeviceGuard dg_(st ? st->ctx->device : -1);
   if (!st || !nrows) return ASTR_ERR_ARG;
   astr_ctx* ctx = st->ctx;
-  const int n = st->nstep;
+  const int n = hist_rows(st);
   *nrows = n;
   if (!rows || maxrows <= 0 || n == 0) return ASTR_OK;
   const int k = n < maxrows ? n : maxrows;
@@ -1293,7 +1344,7 @@ int astr_ensemble_step(astr_ensemble* e, const double* dt, int nsteps) {
   const int nbox = (int)e->boxes.size();
   for (int b = 0; b < nbox; ++b) {
     if (!(dt[b] > 0.0)) return fail(ctx, ASTR_ERR_ARG, "dt must be positive");
-    if (e->boxes[b]->nstep + nsteps > e->boxes[b]->hist_cap) return fail(ctx, ASTR_ERR_UNSUPPORTED, "history buffer full");
+    if (hist_rows(e->boxes[b]) + nsteps > e->boxes[b]->hist_cap) return fail(ctx, ASTR_ERR_UNSUPPORTED, "history buffer full");
   }
   bool changed = e->dt.size() != (size_t)nbox;
   for (int b = 0; b < nbox && !changed; ++b) changed = e->dt[b] != dt[b];

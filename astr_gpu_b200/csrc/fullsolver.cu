@@ -678,11 +678,12 @@ __global__ void k_fs_diag(double* partials, const double* rho, const double* vel
     for (int c = 0; c < 3; ++c) partials[3 * blockIdx.x + c] = s[c][0];
 }
 
-// Copy between the caller's Fortran array (nodes 0..N inside it) and nodes 0..N of the layout.
+// Copy between the caller's Fortran array (nodes 0..N inside it) and nodes 0..N of the layout,
+// nf fields.
 __global__ void k_fs_pack(double* state, double* user, FsGeo g, int64_t u0, int64_t u1, int64_t u2, int64_t ufs,
-                          int64_t uoff, int to_state) {
+                          int64_t uoff, int to_state, int nf) {
   const Box3 b = box_line(g, -1, 0, 0);
-  GRID_STRIDE(p, b.size() * 5) {
+  GRID_STRIDE(p, b.size() * nf) {
     const int m = (int)(p / b.size());
     int i, j, k;
     b.node(p - (int64_t)m * b.size(), i, j, k);
@@ -934,7 +935,7 @@ int fs_copy(astr_full* fs, double* user, const int64_t* shape, const int64_t* lb
     dev = fs->qt;
     if (to_state) FCK(cudaMemcpyAsync(dev, user, 5 * ufs * sizeof(double), cudaMemcpyHostToDevice, st));
   }
-  k_fs_pack<<<blocks_for(5 * nodes(fs)), 256, 0, st>>>(fs->q, dev, fs->g, 1, u1, u2, ufs, uoff, to_state);
+  k_fs_pack<<<blocks_for(5 * nodes(fs)), 256, 0, st>>>(fs->q, dev, fs->g, 1, u1, u2, ufs, uoff, to_state, 5);
   FCK(cudaGetLastError());
   if (where == ASTR_HOST && !to_state) FCK(cudaMemcpyAsync(user, dev, 5 * ufs * sizeof(double), cudaMemcpyDeviceToHost, st));
   FCK(cudaStreamSynchronize(st));
@@ -1089,6 +1090,72 @@ int astr_full_upload(astr_full* fs, const double* q, const int64_t shape[3], con
   return ASTR_OK;
 }
 
+// The file's fields are the primitive arrays rho, vel(1:3), prs, tmp, which the layout holds as six
+// consecutive fields from fs->rho in the file's order (ro, u1, u2, u3, p, t).
+int astr_full_write_flowfield(astr_full* fs, const char* filename) {
+  if (!fs || !filename) return ASTR_ERR_ARG;
+  const OnDev on(astr_ctx_device(fs->ctx));
+  cudaStream_t st = astr_ctx_stream(fs->ctx);
+  const int64_t shape[3] = {fs->p.im + 1, fs->p.jm + 1, fs->p.km + 1};
+  const int64_t n = shape[0] * shape[1] * shape[2];
+  double* buf = nullptr;
+  if (cudaMalloc(&buf, 6 * (size_t)n * sizeof(double)) != cudaSuccess) {
+    cudaGetLastError();
+    return ffail(fs, ASTR_ERR_NOMEM, "flow-field buffers");
+  }
+  k_fs_pack<<<blocks_for(6 * n), 256, 0, st>>>(fs->rho, buf, fs->g, 1, shape[0], shape[0] * shape[1], n, 0, 0, 6);
+  cudaError_t e = cudaGetLastError();
+  std::string err;
+  int rc = e != cudaSuccess ? ASTR_ERR_CUDA : flowfield_write(st, buf, shape, fs->nstep, fs->time, filename, err);
+  if (e != cudaSuccess) err = std::string("k_fs_pack: ") + cudaGetErrorString(e);
+  cudaFree(buf);
+  return rc == ASTR_OK ? rc : ffail(fs, rc, err);
+}
+
+// readcheckpoint + updateq: q = fvar2q(ro, u, t) on nodes 0..N, the primitives of the layout
+// recomputed from q (upload), then the interior primitives replaced by the file's, which the
+// reference's first stage after a restart uses as read.
+int astr_full_read_flowfield(astr_full* fs, const char* filename, char mode, int* nstep, double* time) {
+  if (!fs || !filename) return ASTR_ERR_ARG;
+  const OnDev on(astr_ctx_device(fs->ctx));
+  cudaStream_t st = astr_ctx_stream(fs->ctx);
+  const int64_t shape[3] = {fs->p.im + 1, fs->p.jm + 1, fs->p.km + 1}, lb[3] = {0, 0, 0};
+  const int64_t n = shape[0] * shape[1] * shape[2];
+  double* buf = nullptr;
+  if (cudaMalloc(&buf, 11 * (size_t)n * sizeof(double)) != cudaSuccess) {
+    cudaGetLastError();
+    return ffail(fs, ASTR_ERR_NOMEM, "flow-field buffers");
+  }
+  std::string err;
+  int ns = 0;
+  double t = 0.0;
+  int rc = flowfield_read(st, buf + 5 * n, shape, filename, mode, &ns, &t, err);
+  cudaError_t e = cudaSuccess;
+  if (rc == ASTR_OK && (e = flowfield_q_from_prims(st, buf + 5 * n, buf, n, fs->p.mach, fs->p.gamma)) != cudaSuccess) {
+    rc = ASTR_ERR_CUDA;
+    err = std::string("fvar2q: ") + cudaGetErrorString(e);
+  }
+  if (rc == ASTR_OK) {
+    rc = astr_full_upload(fs, buf, shape, lb, ASTR_DEVICE);   // sets the context's message on failure
+    if (rc == ASTR_OK) {
+      k_fs_pack<<<blocks_for(6 * n), 256, 0, st>>>(fs->rho, buf + 5 * n, fs->g, 1, shape[0], shape[0] * shape[1], n, 0, 1,
+                                                   6);
+      if ((e = cudaGetLastError()) == cudaSuccess) e = cudaStreamSynchronize(st);
+      if (e != cudaSuccess) {
+        rc = ASTR_ERR_CUDA;
+        err = std::string("k_fs_pack: ") + cudaGetErrorString(e);
+      }
+    }
+  }
+  cudaFree(buf);
+  if (rc != ASTR_OK) return err.empty() ? rc : ffail(fs, rc, err);
+  fs->nstep = ns;
+  fs->time = t;
+  if (nstep) *nstep = ns;
+  if (time) *time = t;
+  return ASTR_OK;
+}
+
 int astr_full_download(astr_full* fs, double* q, const int64_t shape[3], const int64_t lbound[3], int where) {
   if (!fs || !q || !shape || !lbound) return ASTR_ERR_ARG;
   const OnDev on(astr_ctx_device(fs->ctx));
@@ -1109,7 +1176,7 @@ int astr_full_rhs(astr_full* fs, double* qrhs, const int64_t shape[3], const int
 int astr_full_step(astr_full* fs, double dt, int nsteps) {
   if (!fs || !(dt > 0.0) || nsteps < 0) return ASTR_ERR_ARG;
   const OnDev on(astr_ctx_device(fs->ctx));
-  if (fs->nstep + nsteps > fs->hist_cap) return ffail(fs, ASTR_ERR_UNSUPPORTED, "history buffer full (65536 steps)");
+  if ((int)(fs->row_key.size() / 2) + nsteps > fs->hist_cap) return ffail(fs, ASTR_ERR_UNSUPPORTED, "history buffer full (65536 steps)");
   for (int s = 0; s < nsteps; ++s) {
     fs->row_key.push_back((double)fs->nstep);
     fs->row_key.push_back(fs->time);
@@ -1124,7 +1191,7 @@ int astr_full_step(astr_full* fs, double dt, int nsteps) {
 int astr_full_history(astr_full* fs, double* rows, int maxrows, int* nrows) {
   if (!fs || !nrows) return ASTR_ERR_ARG;
   const OnDev on(astr_ctx_device(fs->ctx));
-  const int n = fs->nstep;
+  const int n = (int)(fs->row_key.size() / 2);   // rows written (nstep may start elsewhere after a restart)
   *nrows = n;
   if (!rows || maxrows <= 0 || n == 0) return ASTR_OK;
   const int k = n < maxrows ? n : maxrows;

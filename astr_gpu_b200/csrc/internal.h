@@ -56,4 +56,15 @@ enum { LINE_ADD = 1, LINE_DIFF = 2 };
 cudaError_t launch_line_api(const DevOp& op, int dir, const double* f, const ArrDesc& fa, double* out,
                             const ArrDesc& oa, int nfields, double scale, cudaStream_t st, int flags = 0);
 
+// Flow-field checkpoints (checkpoint.cu): q(n, 5) <-> the file's ro, u1, u2, u3, p, t (6 fields of
+// n nodes each, contiguous), and the transfers between such a device array and the file.
+cudaError_t flowfield_prims_from_q(cudaStream_t st, const double* dq, double* dprims, int64_t n, double mach,
+                                   double gamma);
+cudaError_t flowfield_q_from_prims(cudaStream_t st, const double* dprims, double* dq, int64_t n, double mach,
+                                   double gamma);
+int flowfield_write(cudaStream_t st, const double* dprims, const int64_t shape[3], int nstep, double time,
+                    const char* filename, std::string& err);
+int flowfield_read(cudaStream_t st, double* dprims, const int64_t shape[3], const char* filename, char mode,
+                   int* nstep, double* time, std::string& err);
+
 }  // namespace astr

@@ -8,6 +8,7 @@ compact filter alpha_f = 0.49 after every stage, dt fixed from CFL 0.5 at t = 0)
     python bench.py --workload adjoint                          # 128^3 gradient, adjoint:forward
     python bench.py --workload gradient                         # 256^3 line operators, GB/s
     python bench.py --workload full                             # full-solver time integration
+    python bench.py --workload checkpoint                       # HDF5 flow-field write + restart read
 
 One JSON line on rank 0. `value` = grid-point RK3 updates/s over all ranks (each rank advances
 its own 512^3 box: replicas, weak scaling), device-timed with CUDA events on the library's stream,
@@ -753,6 +754,80 @@ def run_full(args, ws, rank, local):
     s.close()
 
 
+def run_checkpoint(args, ws, rank, local):
+    """The checkpoint path of the reference's restart (writeflfed's flow field, readcheckpoint +
+    updateq): a TGV state of --ckpt-size written to an HDF5 file on the host's disk and read back
+    into a second state, through astr_state_write_flowfield / astr_state_read_flowfield (q2fvar and
+    fvar2q on the GPU, pinned double-buffered transfers, the library's HDF5 writer and reader).
+    One step = one write and one read of the same file; wall time (the host's file I/O is the
+    work), the file in the page cache as right after a checkpoint. CPU baseline: the oracle's
+    numpy conversions with its Python HDF5 writer and reader, one write and one read."""
+    import tempfile
+
+    import numpy as np
+    import torch
+    import astr_gpu_b200 as ag
+
+    torch.cuda.set_device(local)
+    n = args.ckpt_size
+    ctx = ag.Context(local)
+    a, b = ag.TGVSolver(ctx, n), ag.TGVSolver(ctx, n)
+    a.init_tgv()
+    tmp = tempfile.mkdtemp(prefix="astr_ckpt_")
+    fn = os.path.join(tmp, f"flowfield_r{rank}.h5")
+    for _ in range(max(args.warmup, 1)):
+        a.write_flowfield(fn)
+        b.read_flowfield(fn)
+    tw = tr = 0.0
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            a.write_flowfield(fn)
+            t1 = time.perf_counter()
+            b.read_flowfield(fn)
+            t2 = time.perf_counter()
+            tw += t1 - t0
+            tr += t2 - t1
+    fbytes = os.path.getsize(fn)
+    ok = bool(np.array_equal(b.get_q()[..., 0], a.get_q()[..., 0]))
+    os.remove(fn)
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        import oracle
+        from oracle import h5format
+        q = a.get_q()
+        t0 = time.perf_counter()
+        f = oracle.q2fvar(q, 0.1, 1.4)
+        h5format.write(fn, [(nm, np.ascontiguousarray(f[..., m].T)) for m, nm in enumerate(("ro", "u1", "u2", "u3",
+                                                                                          "p", "t"))]
+                       + [("nstep", np.array([0], np.int32)), ("time", np.array([0.0]))])
+        info = h5format.read(fn)
+        g = np.stack([info.entries[nm].data.T for nm in ("ro", "u1", "u2", "u3", "p", "t")], axis=-1)
+        oracle.fvar2q_temperature(g, 0.1, 1.4)
+        tc = time.perf_counter() - t0
+        os.remove(fn)
+        cpu = {"value": 2 * fbytes / tc / 1e9, "unit": "GB/s", "cores": 1, "kind": "port",
+               "sample": f"one write + one read of the {n}^3 flow field by the oracle (numpy, Python HDF5)"}
+    os.rmdir(tmp)
+    if rank == 0:
+        total = tw + tr
+        line = {"metric": "flow-field checkpoint write + restart read, file GB/s", "value": ws * 2 * fbytes
+                * args.steps / total / 1e9, "unit": "GB/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic (Taylor-Green initial field)",
+                "config": {"workload": f"HDF5 flow field of a TGV {n}^3 state (ro, u1, u2, u3, p, t, nstep, time; "
+                                       f"{fbytes / 1e9:.3f} GB): astr_state_write_flowfield then "
+                                       "astr_state_read_flowfield, wall time, host page cache", "grid": n},
+                "write_gbs": fbytes * args.steps / tw / 1e9, "read_gbs": fbytes * args.steps / tr / 1e9,
+                "round_trip_density_equal": ok, "cpu_baseline": cpu,
+                # per step: the state's pack kernel and q2fvar (write), fvar2q and the pack kernel (read)
+                "gpu_launches": 4 * args.steps,
+                "clocks": clk.summary()}
+        print(json.dumps(line), flush=True)
+    a.close()
+    b.close()
+
+
 def run_profile(args, local):
     """The workload for an ncu capture: `--steps` eager RK3 steps of a TGV box (no graph, no
     timing, no JSON line), with the pass launch shapes pinned by `--shapes`."""
@@ -784,7 +859,9 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", default="tgv", choices=["tgv", "ensemble", "adjoint", "gradient", "full"])
+    ap.add_argument("--workload", default="tgv", choices=["tgv", "ensemble", "adjoint", "gradient", "full",
+                                                          "checkpoint"])
+    ap.add_argument("--ckpt-size", type=int, default=256, help="grid of --workload checkpoint")
     ap.add_argument("--full-size", type=int, default=256)
     ap.add_argument("--conschm", type=int, default=643, choices=[643, 543], help="convection of --workload full")
     ap.add_argument("--bfac", type=float, default=0.3, help="b factor of the upwind compact flux (--conschm 543)")
@@ -816,6 +893,8 @@ def main():
         run_gradient(args, ws, rank, local)
     elif args.workload == "full":
         run_full(args, ws, rank, local)
+    elif args.workload == "checkpoint":
+        run_checkpoint(args, ws, rank, local)
     else:
         run_ours(args, ws, rank, local)
 

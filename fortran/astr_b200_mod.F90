@@ -307,6 +307,100 @@ module astr_b200
       integer(c_int), value :: maxrows
       integer(c_int) :: nrows
     end function
+
+    ! ---- checkpoint files: h5io_init / h5write / h5read / h5io_end (src/hdf5io.F90) without the
+    ! HDF5 library; strings are NUL-terminated (trim(name)//c_null_char)
+    integer(c_int) function astr_h5io_init(filename, mode, h) bind(C, name="astr_h5io_init")
+      import :: c_int, c_ptr, c_char
+      character(kind=c_char) :: filename(*), mode(*)
+      type(c_ptr) :: h
+    end function
+    integer(c_int) function astr_h5io_end(h) bind(C, name="astr_h5io_end")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: h
+    end function
+    type(c_ptr) function astr_h5_last_error(h) bind(C, name="astr_h5_last_error")
+      import :: c_ptr
+      type(c_ptr), value :: h
+    end function
+    integer(c_int) function astr_h5write_r8(h, varname, rank, dims, var) bind(C, name="astr_h5write_r8")
+      import :: c_int, c_ptr, c_char, c_int64_t
+      type(c_ptr), value :: h, var
+      character(kind=c_char) :: varname(*)
+      integer(c_int), value :: rank
+      integer(c_int64_t) :: dims(*)
+    end function
+    integer(c_int) function astr_h5write_i4(h, varname, rank, dims, var) bind(C, name="astr_h5write_i4")
+      import :: c_int, c_ptr, c_char, c_int64_t
+      type(c_ptr), value :: h, var
+      character(kind=c_char) :: varname(*)
+      integer(c_int), value :: rank
+      integer(c_int64_t) :: dims(*)
+    end function
+    integer(c_int) function astr_h5read_r8(h, varname, rank, dims, offset, mode, var) bind(C, name="astr_h5read_r8")
+      import :: c_int, c_ptr, c_char, c_int64_t
+      type(c_ptr), value :: h, offset, var
+      character(kind=c_char) :: varname(*)
+      integer(c_int), value :: rank
+      integer(c_int64_t) :: dims(*)
+      character(kind=c_char), value :: mode
+    end function
+    integer(c_int) function astr_h5read_i4(h, varname, rank, dims, offset, mode, var) bind(C, name="astr_h5read_i4")
+      import :: c_int, c_ptr, c_char, c_int64_t
+      type(c_ptr), value :: h, offset, var
+      character(kind=c_char) :: varname(*)
+      integer(c_int), value :: rank
+      integer(c_int64_t) :: dims(*)
+      character(kind=c_char), value :: mode
+    end function
+    integer(c_int) function astr_h5_dataset_info(h, varname, rank, dims, type_class, type_size) &
+        bind(C, name="astr_h5_dataset_info")
+      import :: c_int, c_ptr, c_char, c_int64_t
+      type(c_ptr), value :: h
+      character(kind=c_char) :: varname(*)
+      integer(c_int) :: rank, type_class, type_size
+      integer(c_int64_t) :: dims(*)
+    end function
+    integer(c_int) function astr_h5_count(h, n) bind(C, name="astr_h5_count")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: h
+      integer(c_int) :: n
+    end function
+    integer(c_int) function astr_h5_name(h, i, name, len) bind(C, name="astr_h5_name")
+      import :: c_int, c_ptr, c_char
+      type(c_ptr), value :: h
+      integer(c_int), value :: i, len
+      character(kind=c_char) :: name(*)
+    end function
+    ! writeflfed's flow field / readcheckpoint + updateq (src/readwrite.F90:1378-1528, 1720-1979)
+    integer(c_int) function astr_state_write_flowfield(st, filename) bind(C, name="astr_state_write_flowfield")
+      import :: c_int, c_ptr, c_char
+      type(c_ptr), value :: st
+      character(kind=c_char) :: filename(*)
+    end function
+    integer(c_int) function astr_full_write_flowfield(fs, filename) bind(C, name="astr_full_write_flowfield")
+      import :: c_int, c_ptr, c_char
+      type(c_ptr), value :: fs
+      character(kind=c_char) :: filename(*)
+    end function
+    integer(c_int) function astr_state_read_flowfield(st, filename, mode, nstep, time) &
+        bind(C, name="astr_state_read_flowfield")
+      import :: c_int, c_ptr, c_char, c_double
+      type(c_ptr), value :: st
+      character(kind=c_char) :: filename(*)
+      character(kind=c_char), value :: mode
+      integer(c_int) :: nstep
+      real(c_double) :: time
+    end function
+    integer(c_int) function astr_full_read_flowfield(fs, filename, mode, nstep, time) &
+        bind(C, name="astr_full_read_flowfield")
+      import :: c_int, c_ptr, c_char, c_double
+      type(c_ptr), value :: fs
+      character(kind=c_char) :: filename(*)
+      character(kind=c_char), value :: mode
+      integer(c_int) :: nstep
+      real(c_double) :: time
+    end function
   end interface
 
 contains

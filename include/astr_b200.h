@@ -34,6 +34,13 @@
  *   astr_rk3_step_host      one call of rk3 with the state in host memory: upload, nsteps, download
  *   astr_full_*             time_integration_rk / rhscal of the full solver     src/mainloop.F90:298-476,
  *                                                                              src/solver.F90:184-283
+ *   astr_h5io_init/_end     h5io_init(filename,mode) / h5io_end                src/hdf5io.F90:86-163
+ *   astr_h5write_r8/_i4     h5write (h5wa3d_r8_struct, h5w_int4, h5srite)      src/hdf5io.F90:684-808,
+ *                                                                              :1015-1100
+ *   astr_h5read_r8/_i4      h5read (h5ra3d_r8_struct/_stream, h5r_int4)        src/hdf5io.F90:175-452
+ *   astr_*_write_flowfield  writeflfed's flow field (write_io_tree + h5srite)  src/readwrite.F90:1720-1980
+ *   astr_*_read_flowfield   readcheckpoint's flow field + updateq              src/readwrite.F90:1378-1528,
+ *                                                                              src/fludyna.F90:254-300
  */
 #ifndef ASTR_B200_H
 #define ASTR_B200_H
@@ -240,6 +247,56 @@ int astr_full_step(astr_full* fs, double dt, int nsteps);
  * the filtered, averaged q, as the stage leaves it before its update. */
 int astr_full_rhs(astr_full* fs, double* qrhs, const int64_t shape[3], const int64_t lbound[3], int where);
 int astr_full_history(astr_full* fs, double* rows, int maxrows, int* nrows);
+
+/* ---- checkpoint files: the reference's HDF5 flow field ---------------------------------- */
+/* HDF5 files read and written by the library itself (the HDF5 library is not needed): the
+ * reference's flow-field checkpoints and what the HDF5 library writes for its h5write calls
+ * (superblock version 0, the root group as a symbol table, contiguous little-endian datasets).
+ * Reading also takes superblocks version 1-3, version-2 object headers, compact link groups,
+ * compact storage, float32 / integer / big-endian elements and a user block; chunked or
+ * compressed datasets return ASTR_ERR_UNSUPPORTED. Host memory only; no context, no GPU.
+ * Errors: ASTR_ERR_ARG (bad argument, missing dataset, shape mismatch), ASTR_ERR_STATE (I/O error,
+ * malformed file), ASTR_ERR_UNSUPPORTED (a format feature outside the above). */
+typedef struct astr_h5 astr_h5;
+/* mode "write" creates or truncates the file; "read" opens it; "rdwr" opens an existing
+ * version-0 file to add datasets (what h5srite does to the flow-field file). */
+int astr_h5io_init(const char* filename, const char* mode, astr_h5** out);
+/* Writes the group structures and the superblock (write, rdwr) and closes the file. */
+int astr_h5io_end(astr_h5* h);
+/* The message of the last failed call on h (h == NULL: of the last failed astr_h5io_init or
+ * astr_h5io_end of this thread). */
+const char* astr_h5_last_error(const astr_h5* h);
+/* A dataset holding the Fortran array var of shape dims[0..rank-1] (first index fastest; the
+ * HDF5 dataspace is the reversed shape, as the Fortran HDF5 interface stores it). */
+int astr_h5write_r8(astr_h5* h, const char* varname, int rank, const int64_t dims[], const double* var);
+int astr_h5write_i4(astr_h5* h, const char* varname, int rank, const int64_t dims[], const int32_t* var);
+/* The block of Fortran shape dims at Fortran offsets offset[] (NULL: all zero) of a dataset of
+ * rank `rank` (mode 'h', h5ra3d_r8_struct's hyperslab), or dims' element count from element
+ * offset[0] of a one-dimensional dataset (mode 's', h5ra3d_r8_stream). Elements are converted to
+ * the output type; astr_h5read_i4 takes integer datasets only. */
+int astr_h5read_r8(astr_h5* h, const char* varname, int rank, const int64_t dims[], const int64_t offset[],
+                   char mode, double* var);
+int astr_h5read_i4(astr_h5* h, const char* varname, int rank, const int64_t dims[], const int64_t offset[],
+                   char mode, int32_t* var);
+/* Rank, Fortran-order shape (up to 32 entries), type class (0 integer, 1 float, -1 other) and
+ * element size of a dataset. */
+int astr_h5_dataset_info(astr_h5* h, const char* varname, int* rank, int64_t dims[], int* type_class,
+                         int* type_size);
+/* Members of the root group: their number and the i-th name (NUL-terminated, len bytes at most). */
+int astr_h5_count(astr_h5* h, int* n);
+int astr_h5_name(astr_h5* h, int i, char* name, int len);
+
+/* The flow-field file of writeflfed: datasets ro, u1, u2, u3, p, t of Fortran shape (im+1, jm+1,
+ * km+1) from the state's q by q2fvar (src/fludyna.F90:545-634, on the GPU), then nstep (integer)
+ * and time (real(8)), one element each, the state's step counter and time. */
+int astr_state_write_flowfield(astr_state* st, const char* filename);
+int astr_full_write_flowfield(astr_full* fs, const char* filename);
+/* readcheckpoint's flow-field read and updateq: ro, u1, u2, u3, p, t (mode 'h': 3-D datasets of
+ * Fortran shape (im+1, jm+1, km+1); 's': 1-D datasets of as many elements) and nstep, time; q =
+ * fvar2q(ro, u, t) (src/fludyna.F90:449-533, the temperature branch, on the GPU); the state's step
+ * counter and time are set from the file and returned in *nstep, *time when not NULL. */
+int astr_state_read_flowfield(astr_state* st, const char* filename, char mode, int* nstep, double* time);
+int astr_full_read_flowfield(astr_full* fs, const char* filename, char mode, int* nstep, double* time);
 
 /* ---- no-allocation variant -------------------------------------------------------- */
 /* dt such that cflcal's CFL equals `cfl` for the conserved variables q (a DEVICE array,

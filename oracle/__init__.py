@@ -59,6 +59,8 @@ def lib():
             "orc_tgv_init_tgv": (None, [vp]),
             "orc_tgv_set_q": (None, [vp, dp]),
             "orc_tgv_get_q": (None, [vp, dp]),
+            "orc_tgv_set_flowfield": (None, [vp, dp]),
+            "orc_tgv_get_flowfield": (None, [vp, dp]),
             "orc_tgv_set_dt": (None, [vp, d]),
             "orc_tgv_cfl_dt": (d, [vp, d]),
             "orc_tgv_steps": (None, [vp, i]),
@@ -242,6 +244,29 @@ class FlowParams:
     shkcrt: float = 0.01          # the Ducros sensor's threshold
 
 
+def thermo_constants(mach: float, gamma: float):
+    """const1, const2, const6 of a nondimensional run (tgvsolver.F90:189-195)."""
+    return 1.0 / (gamma * (gamma - 1.0) * (mach * mach)), gamma * (mach * mach), 1.0 / (gamma - 1.0)
+
+
+def q2fvar(q: np.ndarray, mach: float, gamma: float) -> np.ndarray:
+    """q2fvar_3da (src/fludyna.F90:545-634) with thermal_3d (:136-153): (ro, u1, u2, u3, p, t)
+    from q(..., 0:5), every operation in the reference's order (numpy rounds each one)."""
+    _c1, c2, c6 = thermo_constants(mach, gamma)
+    r = q[..., 0]
+    u, v, w = q[..., 1] / r, q[..., 2] / r, q[..., 3] / r
+    p = (q[..., 4] - 0.5 * r * (u * u + v * v + w * w)) / c6
+    return np.stack([r, u, v, w, p, p / r * c2], axis=-1)
+
+
+def fvar2q_temperature(f: np.ndarray, mach: float, gamma: float) -> np.ndarray:
+    """fvar2q_3da's temperature branch (src/fludyna.F90:449-533), which updateq takes after
+    readcheckpoint (src/fludyna.F90:254-300): q from (ro, u1, u2, u3, p, t) = f(..., 0:6)."""
+    c1, _c2, _c6 = thermo_constants(mach, gamma)
+    r, u, v, w, t = f[..., 0], f[..., 1], f[..., 2], f[..., 3], f[..., 5]
+    return np.stack([r, r * u, r * v, r * w, r * (t * c1 + 0.5 * (u * u + v * v + w * w))], axis=-1)
+
+
 class TGVOracle:
     """The miniapp ``boxsolver`` (tgvsolver.F90:1086-1116) on an im x jm x km periodic box."""
 
@@ -283,6 +308,19 @@ class TGVOracle:
 
     def set_dt(self, dt: float):
         lib().orc_tgv_set_dt(self._h, dt)
+
+    def set_flowfield(self, prims: np.ndarray):
+        """readcheckpoint + updateq: the primitive arrays take the file's (ro, u1, u2, u3, p, t),
+        prims[..., 0:6] on nodes 0..N, and q = fvar2q(ro, u, t) (src/fludyna.F90:449-533)."""
+        f = np.asfortranarray(prims, dtype=np.float64)
+        assert f.shape == self.shape + (6,)
+        lib().orc_tgv_set_flowfield(self._h, _dp(f))
+
+    def get_flowfield(self) -> np.ndarray:
+        """The primitive arrays (ro, u1, u2, u3, p, t) on nodes 0..N, as writeflfed writes them."""
+        out = np.zeros(self.shape + (6,), order="F")
+        lib().orc_tgv_get_flowfield(self._h, _dp(out))
+        return out
 
     def cfl_dt(self, cfl: float) -> float:
         return lib().orc_tgv_cfl_dt(self._h, cfl)

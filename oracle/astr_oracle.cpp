@@ -933,6 +933,40 @@ struct TGV {
     diffusion();
   }
 
+  // readcheckpoint + updateq (src/readwrite.F90:1378-1528, src/fludyna.F90:254-300): the
+  // primitive arrays take the file's ro, u1, u2, u3, p, t on nodes 0..N (6 Fortran fields) and q
+  // is fvar2q's temperature branch (src/fludyna.F90:449-533):
+  // q5 = rho (t const1 + 0.5 (u1^2 + u2^2 + u3^2)).
+  void set_flowfield(const double* f) {
+    const int64_t n0 = im + 1, n1 = jm + 1, n2 = km + 1, nn = n0 * n1 * n2;
+    for (int k = 0; k <= km; ++k)
+      for (int j = 0; j <= jm; ++j)
+        for (int i = 0; i <= im; ++i) {
+          const int64_t o = ((int64_t)k * n1 + j) * n0 + i;
+          const double r = f[o], u[3] = {f[nn + o], f[2 * nn + o], f[3 * nn + o]};
+          rho(i, j, k) = r;
+          for (int c = 0; c < 3; ++c) vel(i, j, k, c) = u[c];
+          prs(i, j, k) = f[4 * nn + o];
+          tmp(i, j, k) = f[5 * nn + o];
+          q(i, j, k, 0) = r;
+          for (int c = 0; c < 3; ++c) q(i, j, k, 1 + c) = r * u[c];
+          q(i, j, k, 4) = r * (tmp(i, j, k) * const1 + 0.5 * (u[0] * u[0] + u[1] * u[1] + u[2] * u[2]));
+        }
+  }
+  // The primitive arrays on nodes 0..N as writeflfed writes them (ro, u1, u2, u3, p, t).
+  void get_flowfield(double* f) {
+    const int64_t n0 = im + 1, n1 = jm + 1, n2 = km + 1, nn = n0 * n1 * n2;
+    for (int k = 0; k <= km; ++k)
+      for (int j = 0; j <= jm; ++j)
+        for (int i = 0; i <= im; ++i) {
+          const int64_t o = ((int64_t)k * n1 + j) * n0 + i;
+          f[o] = rho(i, j, k);
+          for (int c = 0; c < 3; ++c) f[(1 + c) * nn + o] = vel(i, j, k, c);
+          f[4 * nn + o] = prs(i, j, k);
+          f[5 * nn + o] = tmp(i, j, k);
+        }
+  }
+
   void update_prims() {
 #pragma omp parallel for collapse(2)
     for (int k = 0; k <= km; ++k)
@@ -1695,6 +1729,8 @@ void orc_tgv_free(void* h) { delete static_cast<TGV*>(h); }
 void orc_tgv_init_tgv(void* h) { static_cast<TGV*>(h)->init_tgv(); }
 void orc_tgv_set_q(void* h, const double* q) { static_cast<TGV*>(h)->set_q(q); }
 void orc_tgv_get_q(void* h, double* q) { static_cast<TGV*>(h)->get_q(q); }
+void orc_tgv_set_flowfield(void* h, const double* f) { static_cast<TGV*>(h)->set_flowfield(f); }
+void orc_tgv_get_flowfield(void* h, double* f) { static_cast<TGV*>(h)->get_flowfield(f); }
 void orc_tgv_set_dt(void* h, double dt) { static_cast<TGV*>(h)->deltat = dt; }
 double orc_tgv_cfl_dt(void* h, double cfl) { return static_cast<TGV*>(h)->cfl_dt(cfl); }
 void orc_tgv_steps(void* h, int n) { TGV* t = static_cast<TGV*>(h); for (int s = 0; s < n; ++s) t->rk3(); }
