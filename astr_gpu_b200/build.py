@@ -19,7 +19,7 @@ LIB_STRICT = os.path.join(HERE, "libastr_b200_strict.so")
 SOURCES = ["capi.cu", "tgv.cu", "lines.cu", "schemes.cu", "tgv_l3_1.cu", "tgv_l5_1.cu", "tgv_l9_1.cu", "tgv_l9_2.cu",
            "tgv_l9_4.cu", "tgv_l5_2.cu", "tgv_l5_4.cu", "tgv_l17_1.cu", "noalloc.cu", "fullsolver.cu", "adjoint.cu", "adj_l3_1.cu", "adj_l5_1.cu",
            "adj_l9_1.cu", "adj_l9_2.cu", "adj_l9_4.cu", "adj_l5_2.cu", "adj_l5_4.cu", "checkpoint.cu", "h5file.cpp"]
-HEADERS = ["ops.cuh", "internal.h", "tgv.cuh", "tgv_kernels.cuh", "adjoint.cuh", "adj_kernels.cuh"]
+HEADERS = ["ops.cuh", "internal.h", "tgv.cuh", "tgv_kernels.cuh", "adjoint.cuh", "adj_kernels.cuh", "h5file.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -1,6 +1,7 @@
 // Flow-field checkpoints of the solver states (the flow-field part of writeflfed and of
 // readcheckpoint + updateq): conversions between the conserved variables and the file's primitive
-// fields on the GPU, and the transfers between HBM and the file (h5file.cpp).
+// fields on the GPU, and chunked transfers between HBM and the file through pinned slots and host
+// I/O threads (the file format itself is h5file.cpp).
 //
 // File: datasets ro, u1, u2, u3, p, t of Fortran shape (im+1, jm+1, km+1) (write_io_tree,
 // src/readwrite.F90:1920-1979), nstep (integer) and time (real(8)) of one element each (h5srite,
@@ -14,11 +15,21 @@
 // const1 = 1/(gamma (gamma-1) M^2), const2 = gamma M^2, const6 = 1/(gamma-1) (nondimensional run).
 
 #include <cuda_runtime.h>
+#include <unistd.h>
 
+#include <algorithm>
+#include <cerrno>
+#include <condition_variable>
 #include <cstdint>
+#include <cstring>
+#include <deque>
+#include <mutex>
 #include <string>
+#include <thread>
+#include <vector>
 
 #include "../../include/astr_b200.h"
+#include "h5file.h"
 #include "internal.h"
 
 namespace astr {
@@ -60,27 +71,6 @@ unsigned grid_for(int64_t n) {
 
 const char* const NAMES[6] = {"ro", "u1", "u2", "u3", "p", "t"};
 
-// Two pinned host buffers of one field each: field f moves through buf[f % 2] while the other
-// buffer's file I/O or copy proceeds.
-struct Pinned {
-  double* buf[2] = {nullptr, nullptr};
-  cudaEvent_t done[2] = {nullptr, nullptr};
-  ~Pinned() {
-    for (int b = 0; b < 2; ++b) {
-      if (done[b]) cudaEventDestroy(done[b]);
-      if (buf[b]) cudaFreeHost(buf[b]);
-    }
-  }
-  cudaError_t init(size_t bytes) {
-    cudaError_t e;
-    for (int b = 0; b < 2; ++b) {
-      if ((e = cudaMallocHost(&buf[b], bytes)) != cudaSuccess) return e;
-      if ((e = cudaEventCreateWithFlags(&done[b], cudaEventDisableTiming)) != cudaSuccess) return e;
-    }
-    return cudaSuccess;
-  }
-};
-
 int cuda_err(std::string& err, cudaError_t e, const char* what) {
   err = std::string(what) + ": " + cudaGetErrorString(e);
   return ASTR_ERR_CUDA;
@@ -88,6 +78,149 @@ int cuda_err(std::string& err, cudaError_t e, const char* what) {
 int h5_err(std::string& err, astr_h5* h, int rc) {
   err = astr_h5_last_error(h);
   return rc;
+}
+
+// One contiguous run of doubles between device memory and a file.
+struct Piece {
+  int fd;
+  uint64_t off;          // absolute file offset
+  const double* dsrc;    // device source (to the file)
+  double* ddst;          // device destination (from the file)
+  size_t bytes;
+};
+
+// Pinned staging slots, allocated on first use and kept for the process (portable, so any
+// device's transfers may use them); one transfer at a time holds them.
+struct SlotPool {
+  std::mutex m;
+  std::vector<char*> buf;
+};
+SlotPool& slot_pool() {
+  static SlotPool p;
+  return p;
+}
+constexpr size_t SLOT_BYTES = size_t(8) << 20;
+
+bool file_io(int fd, char* p, size_t n, uint64_t off, bool write) {
+  while (n) {
+    ssize_t r = write ? ::pwrite(fd, p, n, off_t(off)) : ::pread(fd, p, n, off_t(off));
+    if (r < 0 && errno == EINTR) continue;
+    if (r <= 0) return false;
+    p += r; n -= size_t(r); off += uint64_t(r);
+  }
+  return true;
+}
+
+// Moves every piece between HBM and its file range in chunks of SLOT_BYTES: to the file, the
+// calling thread queues device-to-host copies into free slots on the stream and host threads write
+// each slot once its copy has completed; from the file, host threads read into free slots and
+// queue the host-to-device copy of each. The copy engine, the file I/O of several chunks and the
+// page cache work concurrently.
+int transfer(const std::vector<Piece>& pieces, bool to_file, cudaStream_t st, std::string& err) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  SlotPool& P = slot_pool();
+  std::lock_guard<std::mutex> hold(P.m);
+  const int nthreads = (int)std::max(1u, std::min(8u, std::thread::hardware_concurrency()));
+  const int nslots = 2 * nthreads;
+  while ((int)P.buf.size() < nslots) {
+    void* b = nullptr;
+    cudaError_t e = cudaHostAlloc(&b, SLOT_BYTES, cudaHostAllocPortable);
+    if (e != cudaSuccess) return cuda_err(err, e, "pinned staging slots");
+    P.buf.push_back(static_cast<char*>(b));
+  }
+  std::vector<cudaEvent_t> ev(nslots, nullptr);
+  for (cudaEvent_t& e : ev)
+    if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) {
+      for (cudaEvent_t& x : ev)
+        if (x) cudaEventDestroy(x);
+      return cuda_err(err, cudaGetLastError(), "transfer events");
+    }
+  struct Job { int slot; const Piece* pc; size_t at, bytes; };
+  std::mutex qm;
+  std::condition_variable qcv, freecv;
+  std::deque<Job> queue;
+  std::vector<int> free_slots;
+  for (int k = 0; k < nslots; ++k) free_slots.push_back(k);
+  bool closing = false;
+  int code = ASTR_OK;
+  std::string msg;
+  auto failure = [&](int c, const std::string& m) {
+    std::lock_guard<std::mutex> lk(qm);
+    if (code == ASTR_OK) { code = c; msg = m; }
+  };
+  auto worker = [&]() {
+    cudaSetDevice(dev);
+    for (;;) {
+      Job j;
+      {
+        std::unique_lock<std::mutex> lk(qm);
+        qcv.wait(lk, [&] { return closing || !queue.empty(); });
+        if (queue.empty()) return;
+        j = queue.front();
+        queue.pop_front();
+      }
+      char* hb = P.buf[j.slot];
+      if (to_file) {
+        cudaError_t e = cudaEventSynchronize(ev[j.slot]);
+        if (e != cudaSuccess) failure(ASTR_ERR_CUDA, std::string("flow-field download: ") + cudaGetErrorString(e));
+        else if (!file_io(j.pc->fd, hb, j.bytes, j.pc->off + j.at, true))
+          failure(ASTR_ERR_STATE, std::string("file write failed: ") + std::strerror(errno));
+      } else if (!file_io(j.pc->fd, hb, j.bytes, j.pc->off + j.at, false)) {
+        failure(ASTR_ERR_STATE, "file read failed (truncated file?)");
+      } else {
+        cudaError_t e = cudaMemcpyAsync(reinterpret_cast<char*>(j.pc->ddst) + j.at, hb, j.bytes,
+                                        cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess) e = cudaEventRecord(ev[j.slot], st);
+        if (e == cudaSuccess) e = cudaEventSynchronize(ev[j.slot]);
+        if (e != cudaSuccess) failure(ASTR_ERR_CUDA, std::string("flow-field upload: ") + cudaGetErrorString(e));
+      }
+      {
+        std::lock_guard<std::mutex> lk(qm);
+        free_slots.push_back(j.slot);
+      }
+      freecv.notify_one();
+    }
+  };
+  std::vector<std::thread> threads;
+  for (int t = 0; t < nthreads; ++t) threads.emplace_back(worker);
+  bool stop = false;
+  for (const Piece& pc : pieces) {
+    for (size_t at = 0; at < pc.bytes && !stop; at += SLOT_BYTES) {
+      const size_t bytes = std::min(SLOT_BYTES, pc.bytes - at);
+      int slot;
+      {
+        std::unique_lock<std::mutex> lk(qm);
+        freecv.wait(lk, [&] { return !free_slots.empty(); });
+        slot = free_slots.back();
+        free_slots.pop_back();
+        stop = code != ASTR_OK;
+      }
+      if (!stop && to_file) {
+        cudaError_t e = cudaMemcpyAsync(P.buf[slot], reinterpret_cast<const char*>(pc.dsrc) + at, bytes,
+                                        cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaEventRecord(ev[slot], st);
+        if (e != cudaSuccess) {
+          failure(ASTR_ERR_CUDA, std::string("flow-field download: ") + cudaGetErrorString(e));
+          stop = true;
+        }
+      }
+      std::lock_guard<std::mutex> lk(qm);
+      if (stop) free_slots.push_back(slot);
+      else queue.push_back({slot, &pc, at, bytes});
+      qcv.notify_one();
+    }
+  }
+  {
+    std::lock_guard<std::mutex> lk(qm);
+    closing = true;
+  }
+  qcv.notify_all();
+  for (std::thread& t : threads) t.join();
+  cudaStreamSynchronize(st);
+  for (cudaEvent_t& e : ev) cudaEventDestroy(e);
+  if (code != ASTR_OK) err = msg;
+  return code;
 }
 
 }  // namespace
@@ -117,30 +250,16 @@ cudaError_t flowfield_q_from_prims(cudaStream_t st, const double* dprims, double
 int flowfield_write(cudaStream_t st, const double* dprims, const int64_t shape[3], int nstep, double time,
                     const char* filename, std::string& err) {
   const int64_t n = shape[0] * shape[1] * shape[2];
-  Pinned pin;
-  cudaError_t e;
-  if ((e = pin.init((size_t)n * sizeof(double))) != cudaSuccess) return cuda_err(err, e, "pinned host buffers");
   astr_h5* h = nullptr;
   int rc = astr_h5io_init(filename, "write", &h);
   if (rc != ASTR_OK) return h5_err(err, nullptr, rc);
-  // field f: copied into buf[f % 2] while field f - 1 is written from the other buffer
-  if ((e = cudaMemcpyAsync(pin.buf[0], dprims, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
-      (e = cudaEventRecord(pin.done[0], st)) != cudaSuccess) {
-    astr_h5io_end(h);
-    return cuda_err(err, e, "flow-field download");
-  }
+  std::vector<Piece> pieces;
   for (int f = 0; f < 6 && rc == ASTR_OK; ++f) {
-    if ((e = cudaEventSynchronize(pin.done[f % 2])) != cudaSuccess) { rc = cuda_err(err, e, "flow-field download"); break; }
-    if (f + 1 < 6 &&
-        ((e = cudaMemcpyAsync(pin.buf[(f + 1) % 2], dprims + (size_t)(f + 1) * n, (size_t)n * sizeof(double),
-                              cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
-         (e = cudaEventRecord(pin.done[(f + 1) % 2], st)) != cudaSuccess)) {
-      rc = cuda_err(err, e, "flow-field download");
-      break;
-    }
-    if ((rc = astr_h5write_r8(h, NAMES[f], 3, shape, pin.buf[f % 2])) != ASTR_OK) h5_err(err, h, rc);
+    Piece pc{-1, 0, dprims + (size_t)f * n, nullptr, (size_t)n * sizeof(double)};
+    if ((rc = h5_reserve_r8(h, NAMES[f], 3, shape, &pc.fd, &pc.off)) != ASTR_OK) h5_err(err, h, rc);
+    else pieces.push_back(pc);
   }
-  cudaStreamSynchronize(st);
+  if (rc == ASTR_OK) rc = transfer(pieces, true, st, err);
   const int64_t one = 1;
   const int32_t ns = nstep;
   if (rc == ASTR_OK && (rc = astr_h5write_i4(h, "nstep", 1, &one, &ns)) != ASTR_OK) h5_err(err, h, rc);
@@ -163,33 +282,37 @@ int flowfield_read(cudaStream_t st, double* dprims, const int64_t shape[3], cons
   const int64_t one = 1;
   int32_t ns = 0;
   double t = 0.0;
+  const int rank = mode == 'h' ? 3 : 1;
+  const int64_t* dims = mode == 'h' ? shape : &n;
+  std::vector<Piece> pieces;
+  std::vector<int> elementwise;
   if ((rc = astr_h5read_i4(h, "nstep", 1, &one, nullptr, 'h', &ns)) != ASTR_OK ||
       (rc = astr_h5read_r8(h, "time", 1, &one, nullptr, 'h', &t)) != ASTR_OK) {
     h5_err(err, h, rc);
-    astr_h5io_end(h);
-    return rc;
-  }
-  Pinned pin;
-  cudaError_t e;
-  if ((e = pin.init((size_t)n * sizeof(double))) != cudaSuccess) {
-    astr_h5io_end(h);
-    return cuda_err(err, e, "pinned host buffers");
-  }
-  // field f is read into buf[f % 2] once the upload of field f - 2 from it has finished
-  const int64_t flat = n;
-  for (int f = 0; f < 6; ++f) {
-    if (f >= 2 && (e = cudaEventSynchronize(pin.done[f % 2])) != cudaSuccess) { rc = cuda_err(err, e, "flow-field upload"); break; }
-    rc = mode == 'h' ? astr_h5read_r8(h, NAMES[f], 3, shape, nullptr, 'h', pin.buf[f % 2])
-                     : astr_h5read_r8(h, NAMES[f], 1, &flat, nullptr, 's', pin.buf[f % 2]);
-    if (rc != ASTR_OK) { h5_err(err, h, rc); break; }
-    if ((e = cudaMemcpyAsync(dprims + (size_t)f * n, pin.buf[f % 2], (size_t)n * sizeof(double), cudaMemcpyHostToDevice,
-                             st)) != cudaSuccess ||
-        (e = cudaEventRecord(pin.done[f % 2], st)) != cudaSuccess) {
-      rc = cuda_err(err, e, "flow-field upload");
-      break;
+  } else {
+    for (int f = 0; f < 6; ++f) {
+      // every field must be there with the state's shape before anything reaches the device
+      int64_t fdims[32];
+      int r = 0, cls = 0, size = 0;
+      if ((rc = astr_h5_dataset_info(h, NAMES[f], &r, fdims, &cls, &size)) != ASTR_OK) { h5_err(err, h, rc); break; }
+      Piece pc{-1, 0, nullptr, dprims + (size_t)f * n, (size_t)n * sizeof(double)};
+      if (h5_locate_r8(h, NAMES[f], rank, dims, mode, &pc.fd, &pc.off) == ASTR_OK) pieces.push_back(pc);
+      else elementwise.push_back(f);
     }
   }
-  if ((e = cudaStreamSynchronize(st)) != cudaSuccess && rc == ASTR_OK) rc = cuda_err(err, e, "flow-field upload");
+  // datasets stored otherwise (other element type or byte order, compact storage): read through
+  // the converting reader first, which also rejects a wrong shape before any transfer
+  std::vector<double> tmp;
+  for (size_t k = 0; k < elementwise.size() && rc == ASTR_OK; ++k) {
+    const int f = elementwise[k];
+    tmp.resize((size_t)n);
+    if ((rc = astr_h5read_r8(h, NAMES[f], rank, dims, nullptr, mode, tmp.data())) != ASTR_OK) { h5_err(err, h, rc); break; }
+    cudaError_t e = cudaMemcpyAsync(dprims + (size_t)f * n, tmp.data(), (size_t)n * sizeof(double),
+                                    cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) rc = cuda_err(err, e, "flow-field upload");
+  }
+  if (rc == ASTR_OK) rc = transfer(pieces, false, st, err);
   astr_h5io_end(h);
   if (rc == ASTR_OK) {
     *nstep = ns;

@@ -40,6 +40,7 @@
 #include <vector>
 
 #include "../../include/astr_b200.h"
+#include "h5file.h"
 
 namespace {
 
@@ -520,7 +521,10 @@ uint64_t append(astr_h5* h, const void* p, uint64_t n) {
   return a;
 }
 
-void write_dataset(astr_h5* h, const char* name, int rank, const int64_t* fd, const void* data, int cls, int esize) {
+// Writes a dataset's object header and its data; with reserve_only, the data's storage is only
+// reserved (the caller writes it). Returns the absolute file offset of the data.
+uint64_t write_dataset(astr_h5* h, const char* name, int rank, const int64_t* fd, const void* data, int cls,
+                       int esize, bool reserve_only = false) {
   if (h->mode == 0) bad(h->path + " is open for reading");
   if (!name || !*name || std::strchr(name, '/') || !std::strcmp(name, ".")) bad("invalid dataset name");
   if (h->index.count(name)) bad(std::string("dataset '") + name + "' already exists");
@@ -530,7 +534,7 @@ void write_dataset(astr_h5* h, const char* name, int rank, const int64_t* fd, co
     if (fd[d] < 0) bad("negative dims");
     n *= uint64_t(fd[d]);
   }
-  if (n && !data) bad("null data");
+  if (n && !data && !reserve_only) bad("null data");
   if (h->members.size() >= size_t(2 * LEAF_K * 2 * NODE_K)) bad("too many datasets in one file", ASTR_ERR_UNSUPPORTED);
   const uint64_t nbytes = n * uint64_t(esize);
   std::vector<uint8_t> msgs, dt, sp, lay;
@@ -561,8 +565,10 @@ void write_dataset(astr_h5* h, const char* name, int rank, const int64_t* fd, co
   std::vector<uint8_t> oh = object_header_v1(msgs, 4);
   if (oh.size() != oh_len) bad("internal: object header size", ASTR_ERR_STATE);
   append(h, oh.data(), oh.size());
-  if (nbytes) {
-    if (h->eoa != oh_at + oh_len) bad("internal: data address", ASTR_ERR_STATE);
+  if (nbytes && h->eoa != oh_at + oh_len) bad("internal: data address", ASTR_ERR_STATE);
+  if (nbytes && reserve_only) {
+    h->eoa += nbytes;
+  } else if (nbytes) {
     const uint8_t* p = static_cast<const uint8_t*>(data);
     for (uint64_t done = 0; done < nbytes;) {
       uint64_t k = std::min<uint64_t>(nbytes - done, uint64_t(1) << 30);
@@ -585,6 +591,7 @@ void write_dataset(astr_h5* h, const char* name, int rank, const int64_t* fd, co
   h->index[mb.name] = h->members.size();
   h->members.push_back(std::move(mb));
   h->modified = true;
+  return h->base + oh_at + oh_len;
 }
 
 // The root group as a symbol table (local heap, symbol table nodes, one B-tree node), written
@@ -812,3 +819,38 @@ int astr_h5_name(astr_h5* h, int i, char* name, int len) {
 }
 
 }  // extern "C"
+
+namespace astr {
+
+int h5_reserve_r8(astr_h5* h, const char* varname, int rank, const int64_t dims[], int* fd, uint64_t* offset) {
+  if (!h || !fd || !offset) return ASTR_ERR_ARG;
+  return run(h, [&] {
+    *offset = write_dataset(h, varname, rank, dims, nullptr, 1, 8, true);
+    *fd = h->fd;
+  });
+}
+
+int h5_locate_r8(astr_h5* h, const char* varname, int rank, const int64_t dims[], char mode, int* fd,
+                 uint64_t* offset) {
+  if (!h || !fd || !offset || !dims || rank < 1) return ASTR_ERR_ARG;
+  const auto it = h->index.find(varname ? varname : "");
+  if (it == h->index.end()) return ASTR_ERR_UNSUPPORTED;
+  const Member& m = h->members[it->second];
+  if (!m.dataset || m.cls != 1 || m.esize != 8 || m.be || m.filtered || m.layout != 1 || m.addr == UNDEF)
+    return ASTR_ERR_UNSUPPORTED;
+  uint64_t n = 1;
+  for (int d = 0; d < rank; ++d) n *= uint64_t(dims[d]);
+  bool match;
+  if (mode == 's') {
+    match = m.dims.size() == 1 && m.dims[0] == n;
+  } else {
+    match = int(m.dims.size()) == rank;
+    for (int d = 0; match && d < rank; ++d) match = m.dims[size_t(rank - 1 - d)] == uint64_t(dims[d]);
+  }
+  if (!match || m.nbytes < 8 * n) return ASTR_ERR_UNSUPPORTED;
+  *fd = h->fd;
+  *offset = h->base + m.addr;
+  return ASTR_OK;
+}
+
+}  // namespace astr

@@ -791,6 +791,18 @@ def run_checkpoint(args, ws, rank, local):
     fbytes = os.path.getsize(fn)
     ok = bool(np.array_equal(b.get_q()[..., 0], a.get_q()[..., 0]))
     os.remove(fn)
+    # the host's own file speed for the same bytes: one thread, pwrite / pread of a host buffer
+    raw = np.ones(fbytes // 8)
+    fd = os.open(fn, os.O_RDWR | os.O_CREAT | os.O_TRUNC, 0o644)
+    t0 = time.perf_counter()
+    os.pwrite(fd, memoryview(raw).cast("B"), 0)
+    t1 = time.perf_counter()
+    os.preadv(fd, [memoryview(raw).cast("B")], 0)
+    t2 = time.perf_counter()
+    os.close(fd)
+    os.remove(fn)
+    io_ref = {"write_gbs": raw.nbytes / (t1 - t0) / 1e9, "read_gbs": raw.nbytes / (t2 - t1) / 1e9,
+              "what": "one host thread, pwrite then pread of the same number of bytes (page cache)"}
     cpu = None
     if rank == 0 and not args.no_cpu:
         import oracle
@@ -819,7 +831,7 @@ def run_checkpoint(args, ws, rank, local):
                                        f"{fbytes / 1e9:.3f} GB): astr_state_write_flowfield then "
                                        "astr_state_read_flowfield, wall time, host page cache", "grid": n},
                 "write_gbs": fbytes * args.steps / tw / 1e9, "read_gbs": fbytes * args.steps / tr / 1e9,
-                "round_trip_density_equal": ok, "cpu_baseline": cpu,
+                "round_trip_density_equal": ok, "host_file_io_one_thread": io_ref, "cpu_baseline": cpu,
                 # per step: the state's pack kernel and q2fvar (write), fvar2q and the pack kernel (read)
                 "gpu_launches": 4 * args.steps,
                 "clocks": clk.summary()}
