@@ -815,18 +815,16 @@ int astr_state_write_flowfield(astr_state* st, const char* filename) {
   astr_ctx* ctx = st->ctx;
   const int64_t shape[3] = {st->p.im + 1, st->p.jm + 1, st->p.km + 1}, lb[3] = {0, 0, 0};
   const int64_t n = shape[0] * shape[1] * shape[2];
-  double* buf = nullptr;   // q (5 fields), then the file's 6 primitive fields
-  if (cudaMalloc(&buf, 11 * (size_t)n * sizeof(double)) != cudaSuccess) {
-    cudaGetLastError();
-    return fail(ctx, ASTR_ERR_NOMEM, "flow-field buffers");
-  }
-  int rc = astr_state_download(st, buf, shape, lb, ASTR_DEVICE);
+  // q (5 x n) in R and the file's 6 primitive fields (6 x n) from DA on: stage buffers, free
+  // between steps (R..VF hold 23 padded fields)
+  double* dq = st->R;
+  double* dprims = st->DA;
+  int rc = astr_state_download(st, dq, shape, lb, ASTR_DEVICE);
   if (rc == ASTR_OK) {
-    cudaError_t e = flowfield_prims_from_q(ctx->stream, buf, buf + 5 * n, n, st->p.mach, st->p.gamma);
-    rc = e != cudaSuccess ? cuda_fail(ctx, e, "q2fvar") : flowfield_write(ctx->stream, buf + 5 * n, shape, st->nstep,
+    cudaError_t e = flowfield_prims_from_q(ctx->stream, dq, dprims, n, st->p.mach, st->p.gamma);
+    rc = e != cudaSuccess ? cuda_fail(ctx, e, "q2fvar") : flowfield_write(ctx->stream, dprims, shape, st->nstep,
                                                                           st->time, filename, ctx->err);
   }
-  cudaFree(buf);
   return rc;
 }
 
@@ -836,19 +834,15 @@ int astr_state_read_flowfield(astr_state* st, const char* filename, char mode, i
   astr_ctx* ctx = st->ctx;
   const int64_t shape[3] = {st->p.im + 1, st->p.jm + 1, st->p.km + 1}, lb[3] = {0, 0, 0};
   const int64_t n = shape[0] * shape[1] * shape[2];
-  double* buf = nullptr;
-  if (cudaMalloc(&buf, 11 * (size_t)n * sizeof(double)) != cudaSuccess) {
-    cudaGetLastError();
-    return fail(ctx, ASTR_ERR_NOMEM, "flow-field buffers");
-  }
+  double* dq = st->R;          // as in astr_state_write_flowfield
+  double* dprims = st->DA;
   int ns = 0;
   double t = 0.0;
-  int rc = flowfield_read(ctx->stream, buf + 5 * n, shape, filename, mode, &ns, &t, ctx->err);
+  int rc = flowfield_read(ctx->stream, dprims, shape, filename, mode, &ns, &t, ctx->err);
   if (rc == ASTR_OK) {
-    cudaError_t e = flowfield_q_from_prims(ctx->stream, buf + 5 * n, buf, n, st->p.mach, st->p.gamma);
-    rc = e != cudaSuccess ? cuda_fail(ctx, e, "fvar2q") : astr_state_upload(st, buf, shape, lb, ASTR_DEVICE);
+    cudaError_t e = flowfield_q_from_prims(ctx->stream, dprims, dq, n, st->p.mach, st->p.gamma);
+    rc = e != cudaSuccess ? cuda_fail(ctx, e, "fvar2q") : astr_state_upload(st, dq, shape, lb, ASTR_DEVICE);
   }
-  cudaFree(buf);
   if (rc != ASTR_OK) return rc;
   st->nstep = ns;
   st->time = t;

@@ -1098,17 +1098,12 @@ int astr_full_write_flowfield(astr_full* fs, const char* filename) {
   cudaStream_t st = astr_ctx_stream(fs->ctx);
   const int64_t shape[3] = {fs->p.im + 1, fs->p.jm + 1, fs->p.km + 1};
   const int64_t n = shape[0] * shape[1] * shape[2];
-  double* buf = nullptr;
-  if (cudaMalloc(&buf, 6 * (size_t)n * sizeof(double)) != cudaSuccess) {
-    cudaGetLastError();
-    return ffail(fs, ASTR_ERR_NOMEM, "flow-field buffers");
-  }
-  k_fs_pack<<<blocks_for(6 * n), 256, 0, st>>>(fs->rho, buf, fs->g, 1, shape[0], shape[0] * shape[1], n, 0, 0, 6);
+  double* dprims = fs->dvel;   // 9 layout fields, free between steps
+  k_fs_pack<<<blocks_for(6 * n), 256, 0, st>>>(fs->rho, dprims, fs->g, 1, shape[0], shape[0] * shape[1], n, 0, 0, 6);
   cudaError_t e = cudaGetLastError();
   std::string err;
-  int rc = e != cudaSuccess ? ASTR_ERR_CUDA : flowfield_write(st, buf, shape, fs->nstep, fs->time, filename, err);
+  int rc = e != cudaSuccess ? ASTR_ERR_CUDA : flowfield_write(st, dprims, shape, fs->nstep, fs->time, filename, err);
   if (e != cudaSuccess) err = std::string("k_fs_pack: ") + cudaGetErrorString(e);
-  cudaFree(buf);
   return rc == ASTR_OK ? rc : ffail(fs, rc, err);
 }
 
@@ -1121,25 +1116,22 @@ int astr_full_read_flowfield(astr_full* fs, const char* filename, char mode, int
   cudaStream_t st = astr_ctx_stream(fs->ctx);
   const int64_t shape[3] = {fs->p.im + 1, fs->p.jm + 1, fs->p.km + 1}, lb[3] = {0, 0, 0};
   const int64_t n = shape[0] * shape[1] * shape[2];
-  double* buf = nullptr;
-  if (cudaMalloc(&buf, 11 * (size_t)n * sizeof(double)) != cudaSuccess) {
-    cudaGetLastError();
-    return ffail(fs, ASTR_ERR_NOMEM, "flow-field buffers");
-  }
+  // q (5 x n) in qsave and the file's primitives (6 x n) in dvel: stage buffers, free between steps
+  double* dq = fs->qsave;
+  double* dprims = fs->dvel;
   std::string err;
   int ns = 0;
   double t = 0.0;
-  int rc = flowfield_read(st, buf + 5 * n, shape, filename, mode, &ns, &t, err);
+  int rc = flowfield_read(st, dprims, shape, filename, mode, &ns, &t, err);
   cudaError_t e = cudaSuccess;
-  if (rc == ASTR_OK && (e = flowfield_q_from_prims(st, buf + 5 * n, buf, n, fs->p.mach, fs->p.gamma)) != cudaSuccess) {
+  if (rc == ASTR_OK && (e = flowfield_q_from_prims(st, dprims, dq, n, fs->p.mach, fs->p.gamma)) != cudaSuccess) {
     rc = ASTR_ERR_CUDA;
     err = std::string("fvar2q: ") + cudaGetErrorString(e);
   }
   if (rc == ASTR_OK) {
-    rc = astr_full_upload(fs, buf, shape, lb, ASTR_DEVICE);   // sets the context's message on failure
+    rc = astr_full_upload(fs, dq, shape, lb, ASTR_DEVICE);   // sets the context's message on failure
     if (rc == ASTR_OK) {
-      k_fs_pack<<<blocks_for(6 * n), 256, 0, st>>>(fs->rho, buf + 5 * n, fs->g, 1, shape[0], shape[0] * shape[1], n, 0, 1,
-                                                   6);
+      k_fs_pack<<<blocks_for(6 * n), 256, 0, st>>>(fs->rho, dprims, fs->g, 1, shape[0], shape[0] * shape[1], n, 0, 1, 6);
       if ((e = cudaGetLastError()) == cudaSuccess) e = cudaStreamSynchronize(st);
       if (e != cudaSuccess) {
         rc = ASTR_ERR_CUDA;
@@ -1147,7 +1139,6 @@ int astr_full_read_flowfield(astr_full* fs, const char* filename, char mode, int
       }
     }
   }
-  cudaFree(buf);
   if (rc != ASTR_OK) return err.empty() ? rc : ffail(fs, rc, err);
   fs->nstep = ns;
   fs->time = t;

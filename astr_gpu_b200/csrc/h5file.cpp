@@ -83,6 +83,7 @@ struct Member {
 
 struct Msg {
   int type = 0;
+  int flags = 0;                  // bit 1: the data is a reference to a shared message
   uint64_t at = 0;                // absolute file offset of the message data
   std::vector<uint8_t> d;
 };
@@ -202,8 +203,8 @@ std::vector<Msg> object_header(const astr_h5* h, uint64_t rel) {
     while (pos + uint64_t(hs) <= size) {
       Msg m;
       uint64_t ms;
-      if (ver == 1) { m.type = int(le(&body[pos], 2)); ms = le(&body[pos + 2], 2); }
-      else { m.type = body[pos]; ms = le(&body[pos + 1], 2); }
+      if (ver == 1) { m.type = int(le(&body[pos], 2)); ms = le(&body[pos + 2], 2); m.flags = body[pos + 4]; }
+      else { m.type = body[pos]; ms = le(&body[pos + 1], 2); m.flags = body[pos + 3]; }
       if (pos + hs + ms > size) bad("object header message runs past its block", ASTR_ERR_STATE);
       m.d.assign(body.begin() + long(pos + hs), body.begin() + long(pos + hs + ms));
       m.at = h->base + start + pos + uint64_t(hs);
@@ -370,13 +371,16 @@ void read_structure(astr_h5* h) {
     mb.name = l.first;
     mb.oh = l.second;
     bool space = false, type = false, lay = false;
+    bool shared = false;
     for (const Msg& m : object_header(h, mb.oh)) {
-      if (m.type == 0x01) { parse_dataspace(mb, m.d); space = true; }
+      if ((m.type == 0x01 || m.type == 0x03) && (m.flags & 0x02)) { shared = true; space |= m.type == 0x01; type |= m.type == 0x03; }
+      else if (m.type == 0x01) { parse_dataspace(mb, m.d); space = true; }
       else if (m.type == 0x03) { parse_datatype(mb, m.d); type = true; }
       else if (m.type == 0x08) { parse_layout(mb, m.d); lay = true; }
       else if (m.type == 0x0B) mb.filtered = true;
     }
     mb.dataset = space && type && lay;
+    if (shared) mb.cls = -1;      // a committed (shared) datatype or dataspace: not read here
     h->index[mb.name] = h->members.size();
     h->members.push_back(std::move(mb));
   }
@@ -447,7 +451,9 @@ void read_run(const astr_h5* h, const Member& m, uint64_t first, uint64_t n, T* 
 template <class T>
 void read_block(const astr_h5* h, const char* name, int rank, const int64_t* fd, const int64_t* off, char mode, T* out) {
   const Member& m = find(h, name);
-  if (m.cls < 0) bad(std::string("dataset '") + name + "' is not of an IEEE float or integer type", ASTR_ERR_UNSUPPORTED);
+  if (m.cls < 0)
+    bad(std::string("dataset '") + name + "' is not of an IEEE float or integer type (or its type is a shared message)",
+        ASTR_ERR_UNSUPPORTED);
   if (m.filtered || m.layout == 2) bad(std::string("dataset '") + name + "' is chunked or filtered", ASTR_ERR_UNSUPPORTED);
   if (rank < 1 || rank > MAX_RANK || !fd) bad("bad rank or dims");
   uint64_t n = 1;

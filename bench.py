@@ -775,19 +775,36 @@ def run_checkpoint(args, ws, rank, local):
     a.init_tgv()
     tmp = tempfile.mkdtemp(prefix="astr_ckpt_")
     fn = os.path.join(tmp, f"flowfield_r{rank}.h5")
+    bak = os.path.join(tmp, "bakup")
+    os.mkdir(bak)
+
+    def bakupfile():
+        # writeflfed moves the previous file aside first (bakupfile, src/readwrite.F90:1696-1708),
+        # so every checkpoint is a new file; the moved copies are deleted outside the timed region
+        if os.path.exists(fn):
+            os.rename(fn, os.path.join(bak, os.path.basename(fn)))
+
+    def drop_backups():
+        for f in os.listdir(bak):
+            os.remove(os.path.join(bak, f))
+
     for _ in range(max(args.warmup, 1)):
+        bakupfile()
         a.write_flowfield(fn)
         b.read_flowfield(fn)
+        drop_backups()
     tw = tr = 0.0
     with ClockSampler(local) as clk:
         for _ in range(args.steps):
             t0 = time.perf_counter()
+            bakupfile()
             a.write_flowfield(fn)
             t1 = time.perf_counter()
             b.read_flowfield(fn)
             t2 = time.perf_counter()
             tw += t1 - t0
             tr += t2 - t1
+            drop_backups()
     fbytes = os.path.getsize(fn)
     ok = bool(np.array_equal(b.get_q()[..., 0], a.get_q()[..., 0]))
     os.remove(fn)
@@ -820,6 +837,7 @@ def run_checkpoint(args, ws, rank, local):
         os.remove(fn)
         cpu = {"value": 2 * fbytes / tc / 1e9, "unit": "GB/s", "cores": 1, "kind": "port",
                "sample": f"one write + one read of the {n}^3 flow field by the oracle (numpy, Python HDF5)"}
+    os.rmdir(bak)
     os.rmdir(tmp)
     if rank == 0:
         total = tw + tr
@@ -828,8 +846,9 @@ def run_checkpoint(args, ws, rank, local):
                 "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f64", "data": "synthetic (Taylor-Green initial field)",
                 "config": {"workload": f"HDF5 flow field of a TGV {n}^3 state (ro, u1, u2, u3, p, t, nstep, time; "
-                                       f"{fbytes / 1e9:.3f} GB): astr_state_write_flowfield then "
-                                       "astr_state_read_flowfield, wall time, host page cache", "grid": n},
+                                       f"{fbytes / 1e9:.3f} GB): the previous file moved aside (bakupfile), "
+                                       "astr_state_write_flowfield, then astr_state_read_flowfield; wall time, "
+                                       "host page cache", "grid": n},
                 "write_gbs": fbytes * args.steps / tw / 1e9, "read_gbs": fbytes * args.steps / tr / 1e9,
                 "round_trip_density_equal": ok, "host_file_io_one_thread": io_ref, "cpu_baseline": cpu,
                 # per step: the state's pack kernel and q2fvar (write), fvar2q and the pack kernel (read)

@@ -372,15 +372,16 @@ def _object_header_v1(msgs) -> bytes:
 
 
 def write(path, datasets, *, user_block=0, layout_version=3, snod_capacity=8, byte_order="<", compact=(),
-          chunked=(), filtered=()):
+          chunked=(), filtered=(), shared_type=()):
     """A version-0 file whose root group holds `datasets`: a sequence of (name, numpy array); the
     array's shape is the dataspace (C order). user_block: bytes before the superblock (a power of
     two >= 512, or 0); layout_version: 2 (dims with the element size, as older libraries wrote)
     or 3; snod_capacity: entries per symbol table node (2 x the leaf K written to the superblock,
     so 8 is the library's default); byte_order: '<' or '>' for the stored numbers. Datasets named
     in `compact` keep their data inside the layout message (version 3); those in `chunked` get a
-    chunked layout message and those in `filtered` a deflate filter pipeline message (header
-    only, for readers that must refuse them)."""
+    chunked layout message, those in `filtered` a deflate filter pipeline message (header only)
+    and those in `shared_type` a datatype message flagged as shared, for readers that must
+    refuse them."""
     leaf_k = snod_capacity // 2
     ik = 16
     names = [n for n, _ in datasets]
@@ -400,7 +401,7 @@ def write(path, datasets, *, user_block=0, layout_version=3, snod_capacity=8, by
         align()
         oh_at = addr()
         fixed = [_message_v1(0x05, 1, bytes([1, 2, 2, 1, 0, 0, 0, 0])),
-                 _message_v1(0x03, 1, _dtype_message(a.dtype)),
+                 _message_v1(0x03, 3 if name in shared_type else 1, _dtype_message(a.dtype)),
                  _message_v1(0x01, 0, space)]
         if name in filtered:
             fixed.append(_message_v1(0x0B, 0, struct.pack("<BB6xHHHHI", 1, 1, 1, 0, 0, 1, 6)))

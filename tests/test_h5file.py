@@ -200,9 +200,12 @@ def test_many_datasets_and_long_names(tmp_path):
 
 def test_refusals(tmp_path):
     fn = tmp_path / "r.h5"
-    h5format.write(fn, [("c", np.ones((4, 4))), ("z", np.ones(3)), ("ok", np.ones(2))], chunked=("c",),
-                   filtered=("z",))
+    h5format.write(fn, [("c", np.ones((4, 4))), ("z", np.ones(3)), ("ok", np.ones(2)), ("s", np.ones(2))],
+                   chunked=("c",), filtered=("z",), shared_type=("s",))
     with ag.h5io_init(fn) as f:
+        with pytest.raises(ag.AstrError) as e:
+            f.read("s")                             # a committed (shared) datatype
+        assert e.value.code == ASTR_ERR_UNSUPPORTED
         with pytest.raises(ag.AstrError) as e:
             f.read("c")
         assert e.value.code == ASTR_ERR_UNSUPPORTED
