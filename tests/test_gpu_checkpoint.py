@@ -100,6 +100,23 @@ def test_state_reads_an_oracle_written_flowfield(ctx, tmp_path, stream):
     s.close()
 
 
+def test_state_reads_fields_stored_otherwise(ctx, tmp_path):
+    """Fields the chunked transfers cannot take directly (big-endian float32 in a file with a user
+    block and version-2 layout messages) go through the converting reader: q is the oracle's
+    fvar2q of the widened values."""
+    import astr_gpu_b200 as ag
+    dims = (24, 20, 16)
+    prims = _prims(tuple(n + 1 for n in dims), 0.1, 4).astype(np.float32)
+    items = [(n, np.ascontiguousarray(prims[..., m].T)) for m, n in enumerate(NAMES)]
+    items += [("nstep", np.array([3], dtype=np.int64)), ("time", np.array([0.125], dtype=np.float32))]
+    fn = tmp_path / "f32.h5"
+    h5format.write(fn, items, user_block=512, layout_version=2, byte_order=">")
+    s = ag.TGVSolver(ctx, *dims)
+    assert s.read_flowfield(fn) == (3, 0.125)
+    assert np.array_equal(s.get_q(), oracle.fvar2q_temperature(prims.astype(np.float64), 0.1, 1.4))
+    s.close()
+
+
 def test_state_restart_continues_the_run(ctx, tmp_path):
     """Four steps, checkpoint, four more steps; a second state restarted from the checkpoint takes
     the same four steps. Both agree with the oracle restarted from the same file."""
@@ -161,6 +178,23 @@ def test_full_solver_checkpoint_and_restart(ctx, tmp_path, ntype):
     assert s2.history()[:, 0].tolist() == [3.0, 4.0, 5.0]
     s.close()
     s2.close()
+
+
+def test_full_solver_reads_a_stream_file(ctx, tmp_path):
+    """readcheckpoint's mode 's' (h5ra3d_r8_stream): 1-D datasets of the block's nodes."""
+    import astr_gpu_b200 as ag
+    dims, mach = (20, 24, 16), 0.2
+    prims = _prims(tuple(n + 1 for n in dims), mach, 6)
+    fn = tmp_path / "stream.h5"
+    _write_oracle_file(fn, prims, 40, 2.0, stream=True)
+    s = ag.FullSolver(ctx, *dims, params=ag.FlowParams(mach=mach, sutherland=110.3))
+    assert s.read_flowfield(fn, "s") == (40, 2.0)
+    assert np.array_equal(s.get_q(), oracle.fvar2q_temperature(prims, mach, 1.4))
+    s.write_flowfield(tmp_path / "back.h5")
+    back, nstep, time = _file_prims(tmp_path / "back.h5")
+    assert (nstep, time) == (40, 2.0)
+    assert np.array_equal(back, prims)       # the primitives as read, written back unchanged
+    s.close()
 
 
 def test_flowfield_refusals_leave_the_state_unchanged(ctx, tmp_path):
