@@ -20,8 +20,8 @@ attribute. No other HDF5 file exists in this image.
 
 The writer here makes version-0 files like the library's default output, with switchable choices
 (user block, layout message version, byte order, SNOD capacity, 1-D "stream" datasets) that the
-library's writer does not make, so that the reader under test meets more than its own writer's
-output.
+library's writer does not make, and version-2 files (`write_v2`: checksummed superblock and object
+headers, compact links), so that the reader under test meets more than its own writer's output.
 """
 from __future__ import annotations
 
@@ -69,6 +69,47 @@ def _u(b, off, n):
     return int.from_bytes(b[off:off + n], "little")
 
 
+_M32 = 0xFFFFFFFF
+
+
+def _rot(x, k):
+    return ((x << k) | (x >> (32 - k))) & _M32
+
+
+def lookup3(data: bytes, initval: int = 0) -> int:
+    """Bob Jenkins' lookup3 hash (hashlittle, public domain, 2006), the checksum of the HDF5
+    format's version-2 structures: 12-byte blocks mixed into three 32-bit words, the last block
+    zero-padded and finalised (an empty input returns the initial value)."""
+    n = len(data)
+    a = b = c = (0xDEADBEEF + n + initval) & _M32
+    i = 0
+    while n - i > 12:
+        a = (a + _u(data, i, 4)) & _M32
+        b = (b + _u(data, i + 4, 4)) & _M32
+        c = (c + _u(data, i + 8, 4)) & _M32
+        a = (a - c) & _M32; a ^= _rot(c, 4); c = (c + b) & _M32
+        b = (b - a) & _M32; b ^= _rot(a, 6); a = (a + c) & _M32
+        c = (c - b) & _M32; c ^= _rot(b, 8); b = (b + a) & _M32
+        a = (a - c) & _M32; a ^= _rot(c, 16); c = (c + b) & _M32
+        b = (b - a) & _M32; b ^= _rot(a, 19); a = (a + c) & _M32
+        c = (c - b) & _M32; c ^= _rot(b, 4); b = (b + a) & _M32
+        i += 12
+    if i == n:
+        return c
+    t = bytes(data[i:]) + bytes(12 - (n - i))
+    a = (a + _u(t, 0, 4)) & _M32
+    b = (b + _u(t, 4, 4)) & _M32
+    c = (c + _u(t, 8, 4)) & _M32
+    c ^= b; c = (c - _rot(b, 14)) & _M32
+    a ^= c; a = (a - _rot(c, 11)) & _M32
+    b ^= a; b = (b - _rot(a, 25)) & _M32
+    c ^= b; c = (c - _rot(b, 16)) & _M32
+    a ^= c; a = (a - _rot(c, 4)) & _M32
+    b ^= a; b = (b - _rot(a, 14)) & _M32
+    c ^= b; c = (c - _rot(b, 24)) & _M32
+    return c
+
+
 class _Reader:
     def __init__(self, raw: bytes):
         self.raw = raw
@@ -102,6 +143,8 @@ class _Reader:
             if b[9] != 8 or b[10] != 8:
                 raise H5FormatError("only 8-byte offsets and lengths")
             base, _ext, eof, root = (_u(b, 12 + 8 * i, 8) for i in range(4))
+            if lookup3(b[:44]) != _u(b, 44, 4):
+                raise H5FormatError("superblock checksum")
         else:
             raise H5FormatError(f"superblock version {ver}")
         self.base = base
@@ -118,6 +161,9 @@ class _Reader:
             pos = 6 + (16 if flags & 0x20 else 0) + (4 if flags & 0x10 else 0)
             w = 1 << (flags & 3)
             size0 = _u(self.at(addr + pos, w), 0, w)
+            whole = self.at(addr, pos + w + size0 + 4)
+            if lookup3(whole[:-4]) != _u(whole, len(whole) - 4, 4):
+                raise H5FormatError("object header checksum")
             chunks = [(addr + pos + w, size0)]
             ohv = 2
         else:
@@ -369,6 +415,43 @@ def _message_v1(t, flags, body):
 def _object_header_v1(msgs) -> bytes:
     body = b"".join(msgs)
     return struct.pack("<BBHII4x", 1, 0, len(msgs), 1, len(body)) + body
+
+
+def _ohdr(msgs) -> bytes:
+    """A version-2 object header holding `msgs` (type, flags, body) in one chunk, checksummed."""
+    body = b"".join(struct.pack("<BHB", t, len(d), f) + d for t, f, d in msgs)
+    w, fl = (1, 0) if len(body) < 256 else (2, 1) if len(body) < 65536 else (4, 2)
+    blob = b"OHDR" + bytes([2, fl]) + len(body).to_bytes(w, "little") + body
+    return blob + struct.pack("<I", lookup3(blob))
+
+
+def write_v2(path, datasets):
+    """A file in the format's newer layout (what the HDF5 library writes with its latest format
+    bounds): superblock version 2, version-2 object headers, the root group as compact link
+    messages (with link info and group info messages), dataspace version 2, fill value version 3,
+    contiguous layout version 3; every superblock and object header checksummed with lookup3."""
+    out = bytearray(48)
+    links = []
+    for name, arr in datasets:
+        a = np.ascontiguousarray(arr)
+        dims = a.shape
+        space = struct.pack("<BBBB", 2, len(dims), 0, 1) + b"".join(struct.pack("<Q", d) for d in dims)
+        fixed = [(0x01, 0, space), (0x03, 1, _dtype_message(a.dtype)), (0x05, 1, bytes([3, 0x0A]))]
+        oh_at = len(out)
+        oh_len = len(_ohdr(fixed + [(0x08, 0, bytes(18))]))
+        data_at = oh_at + oh_len if a.nbytes else UNDEF
+        out.extend(_ohdr(fixed + [(0x08, 0, struct.pack("<BBQQ", 3, 1, data_at, a.nbytes))]))
+        out.extend(a.tobytes())
+        nm = name.encode()
+        if len(nm) > 255:
+            raise H5FormatError("names up to 255 bytes")
+        links.append((0x06, 0, bytes([1, 0, len(nm)]) + nm + struct.pack("<Q", oh_at)))
+    root_at = len(out)
+    out.extend(_ohdr([(0x02, 0, bytes([0, 0]) + struct.pack("<QQ", UNDEF, UNDEF)), (0x0A, 0, bytes([0, 0]))] + links))
+    sb = SIGNATURE + bytes([2, 8, 8, 0]) + struct.pack("<QQQQ", 0, UNDEF, len(out), root_at)
+    out[0:48] = sb + struct.pack("<I", lookup3(sb))
+    with open(path, "wb") as fh:
+        fh.write(out)
 
 
 def write(path, datasets, *, user_block=0, layout_version=3, snod_capacity=8, byte_order="<", compact=(),

@@ -117,6 +117,19 @@ def test_state_reads_fields_stored_otherwise(ctx, tmp_path):
     s.close()
 
 
+def test_state_reads_a_version2_file(ctx, tmp_path):
+    """A flow field in the format's version-2 layout (checksummed headers, compact links)."""
+    import astr_gpu_b200 as ag
+    dims = (24, 20, 16)
+    prims = _prims(tuple(n + 1 for n in dims), 0.1, 8)
+    items = [(n, np.ascontiguousarray(prims[..., m].T)) for m, n in enumerate(NAMES)]
+    h5format.write_v2(tmp_path / "v2.h5", items + [("nstep", np.array([11], np.int32)), ("time", np.array([0.5]))])
+    s = ag.TGVSolver(ctx, *dims)
+    assert s.read_flowfield(tmp_path / "v2.h5") == (11, 0.5)
+    assert np.array_equal(s.get_q(), oracle.fvar2q_temperature(prims, 0.1, 1.4))
+    s.close()
+
+
 def test_state_restart_continues_the_run(ctx, tmp_path):
     """Four steps, checkpoint, four more steps; a second state restarted from the checkpoint takes
     the same four steps. Both agree with the oracle restarted from the same file."""

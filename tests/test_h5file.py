@@ -8,7 +8,8 @@ writer emits the same message encodings (fill value, datatype, dataspace) as tha
 
 Then: files of the library's writer read by the oracle (bit-exact), files of the oracle's writer
 in variants the library's writer does not make (user block, layout version 2, big-endian, float32
-and integer elements, compact storage, several symbol table nodes) read by the library, the
+and integer elements, compact storage, several symbol table nodes, the version-2 superblock and
+object headers with compact links) read by the library, the
 read-write mode that h5srite uses (src/hdf5io.F90:1015-1100), hyperslab and stream reads
 (h5ra3d_r8_struct / h5ra3d_r8_stream, src/hdf5io.F90:204-348), and the refusals."""
 import os
@@ -125,6 +126,37 @@ def test_library_reads_oracle_written_files(tmp_path, user_block, layout_version
         with pytest.raises(ag.AstrError) as e:
             f.read("i64", dtype=np.int32)            # values beyond int32
         assert e.value.code == ASTR_ERR_ARG
+
+
+def test_lookup3_known_answers():
+    """The checksum of the format's version-2 structures: lookup3's published test values."""
+    assert h5format.lookup3(b"") == 0xDEADBEEF
+    assert h5format.lookup3(b"", 0xDEADBEEF) == 0xBD5B7DDE
+    assert h5format.lookup3(b"Four score and seven years ago") == 0x17770551
+    assert h5format.lookup3(b"Four score and seven years ago", 1) == 0xCD628161
+
+
+def test_library_reads_version2_files(tmp_path):
+    """Superblock version 2, version-2 object headers and a compact-link root group (the HDF5
+    library's output with its latest format bounds); the library reads them but does not add to
+    them (read-write needs a version-0 file)."""
+    rng = np.random.default_rng(5)
+    items = [("ro", rng.standard_normal((4, 5, 6))), ("nstep", np.array([7], dtype=np.int32)),
+             ("f32be", rng.standard_normal(9).astype(">f4")), ("empty", np.zeros((0, 2))),
+             ("a" * 200, np.array([1.5]))]
+    fn = tmp_path / "v2.h5"
+    h5format.write_v2(fn, items)
+    info = h5format.read(fn)        # checks the checksums
+    assert info.superblock_version == 2 and info.group_kind == "links"
+    with ag.h5io_init(fn) as f:
+        assert f.names() == [n for n, _ in items]
+        for n, a in items:
+            assert f.info(n)[0] == a.shape[::-1]
+            assert np.array_equal(f.read(n), a.T.astype(np.float64)), n
+        assert f.read("nstep", dtype=np.int32).tolist() == [7]
+    with pytest.raises(ag.AstrError) as e:
+        ag.h5io_init(fn, "rdwr")
+    assert e.value.code == ASTR_ERR_UNSUPPORTED
 
 
 def test_hyperslab_and_stream_reads(tmp_path):
