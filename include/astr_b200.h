@@ -288,7 +288,11 @@ int astr_h5_name(astr_h5* h, int i, char* name, int len);
 
 /* The flow-field file of writeflfed: datasets ro, u1, u2, u3, p, t of Fortran shape (im+1, jm+1,
  * km+1) from the state's q by q2fvar (src/fludyna.F90:545-634, on the GPU), then nstep (integer)
- * and time (real(8)), one element each, the state's step counter and time. */
+ * and time (real(8)), one element each, the state's step counter and time. The conversions use
+ * the state's stage buffers (no device allocation); the transfers go through 128 MB of pinned
+ * host memory that the first checkpoint call of the process allocates and keeps, and up to 8
+ * host threads for the duration of the call. A file of that name is replaced (the reference
+ * moves the previous one aside first, bakupfile). */
 int astr_state_write_flowfield(astr_state* st, const char* filename);
 int astr_full_write_flowfield(astr_full* fs, const char* filename);
 /* readcheckpoint's flow-field read and updateq: ro, u1, u2, u3, p, t (mode 'h': 3-D datasets of
