@@ -247,7 +247,7 @@ def run_ours(args, ws, rank, local):
     # the metric's second part (adjoint:forward step time, config 4) and the batched ensemble
     # against its boxes one at a time (config 3), on one GPU, after the timed region
     shapes = {k: list(v) for k, v in s.launch_shapes().items()}
-    adjoint = ensemble = None
+    adjoint = ensemble = checkpoint = None
     if ws == 1 and not args.no_extras:
         s.close()
         tl, acfg = measure_adjoint(ctx, stream, local, args.adj_size, args.adj_steps, 20, 3)
@@ -266,6 +266,15 @@ def run_ours(args, ws, rank, local):
         ens.close()
         for b in boxes:
             b.close()
+        # the restart path: the HDF5 flow field of a 256^3 state written and read back
+        import tempfile
+        tmp = tempfile.mkdtemp(prefix="astr_ckpt_")
+        tw, tr, fbytes, ok = measure_checkpoint(ctx, 256, 2, 1, tmp, rank)
+        os.rmdir(tmp)
+        checkpoint = {"metric": "flow-field checkpoint write + restart read, file GB/s", "grid": 256,
+                      "file_gb": fbytes / 1e9, "write_gbs": 2 * fbytes / tw / 1e9, "read_gbs": 2 * fbytes / tr / 1e9,
+                      "round_trip_gbs": 4 * fbytes / (tw + tr) / 1e9, "steps": 2, "density_equal": ok,
+                      "how": "wall time; previous file moved aside first (bakupfile); host page cache"}
 
     if rank == 0:
         line = {
@@ -278,7 +287,7 @@ def run_ours(args, ws, rank, local):
                        "launch_shapes": shapes},
             "roofline": roof, "step_roofline": step_roof, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": (3 * (7 if split_fa else 6) + 1) * args.steps, "clocks": clk.summary(),
-            "adjoint": adjoint, "ensemble": ensemble,
+            "adjoint": adjoint, "ensemble": ensemble, "checkpoint": checkpoint,
         }
         print(json.dumps(line), flush=True)
     s.close()
@@ -754,11 +763,59 @@ def run_full(args, ws, rank, local):
     s.close()
 
 
+def measure_checkpoint(ctx, n, steps, warmup, tmp, rank):
+    """Write + restart-read wall times of the flow field of a TGV n^3 state in the directory tmp:
+    (total write s, total read s, file bytes, density equal after the round trip). Each step moves
+    the previous file aside first, as writeflfed does (bakupfile, src/readwrite.F90:1696-1708), so
+    every checkpoint is a new file; the moved copies are deleted outside the timed region."""
+    import numpy as np
+    import astr_gpu_b200 as ag
+
+    a, b = ag.TGVSolver(ctx, n), ag.TGVSolver(ctx, n)
+    a.init_tgv()
+    fn = os.path.join(tmp, f"flowfield_r{rank}.h5")
+    bak = os.path.join(tmp, "bakup")
+    os.makedirs(bak, exist_ok=True)
+
+    def bakupfile():
+        if os.path.exists(fn):
+            os.rename(fn, os.path.join(bak, os.path.basename(fn)))
+
+    def drop_backups():
+        for f in os.listdir(bak):
+            os.remove(os.path.join(bak, f))
+
+    for _ in range(max(warmup, 1)):
+        bakupfile()
+        a.write_flowfield(fn)
+        b.read_flowfield(fn)
+        drop_backups()
+    tw = tr = 0.0
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        bakupfile()
+        a.write_flowfield(fn)
+        t1 = time.perf_counter()
+        b.read_flowfield(fn)
+        t2 = time.perf_counter()
+        tw += t1 - t0
+        tr += t2 - t1
+        drop_backups()
+    fbytes = os.path.getsize(fn)
+    ok = bool(np.array_equal(b.get_q()[..., 0], a.get_q()[..., 0]))
+    os.remove(fn)
+    os.rmdir(bak)
+    a.close()
+    b.close()
+    return tw, tr, fbytes, ok
+
+
 def run_checkpoint(args, ws, rank, local):
     """The checkpoint path of the reference's restart (writeflfed's flow field, readcheckpoint +
     updateq): a TGV state of --ckpt-size written to an HDF5 file on the host's disk and read back
     into a second state, through astr_state_write_flowfield / astr_state_read_flowfield (q2fvar and
-    fvar2q on the GPU, pinned double-buffered transfers, the library's HDF5 writer and reader).
+    fvar2q on the GPU, chunked transfers through pinned slots and host I/O threads, the library's
+    HDF5 writer and reader).
     One step = one write and one read of the same file; wall time (the host's file I/O is the
     work), the file in the page cache as right after a checkpoint. CPU baseline: the oracle's
     numpy conversions with its Python HDF5 writer and reader, one write and one read."""
@@ -771,43 +828,10 @@ def run_checkpoint(args, ws, rank, local):
     torch.cuda.set_device(local)
     n = args.ckpt_size
     ctx = ag.Context(local)
-    a, b = ag.TGVSolver(ctx, n), ag.TGVSolver(ctx, n)
-    a.init_tgv()
     tmp = tempfile.mkdtemp(prefix="astr_ckpt_")
     fn = os.path.join(tmp, f"flowfield_r{rank}.h5")
-    bak = os.path.join(tmp, "bakup")
-    os.mkdir(bak)
-
-    def bakupfile():
-        # writeflfed moves the previous file aside first (bakupfile, src/readwrite.F90:1696-1708),
-        # so every checkpoint is a new file; the moved copies are deleted outside the timed region
-        if os.path.exists(fn):
-            os.rename(fn, os.path.join(bak, os.path.basename(fn)))
-
-    def drop_backups():
-        for f in os.listdir(bak):
-            os.remove(os.path.join(bak, f))
-
-    for _ in range(max(args.warmup, 1)):
-        bakupfile()
-        a.write_flowfield(fn)
-        b.read_flowfield(fn)
-        drop_backups()
-    tw = tr = 0.0
     with ClockSampler(local) as clk:
-        for _ in range(args.steps):
-            t0 = time.perf_counter()
-            bakupfile()
-            a.write_flowfield(fn)
-            t1 = time.perf_counter()
-            b.read_flowfield(fn)
-            t2 = time.perf_counter()
-            tw += t1 - t0
-            tr += t2 - t1
-            drop_backups()
-    fbytes = os.path.getsize(fn)
-    ok = bool(np.array_equal(b.get_q()[..., 0], a.get_q()[..., 0]))
-    os.remove(fn)
+        tw, tr, fbytes, ok = measure_checkpoint(ctx, n, args.steps, args.warmup, tmp, rank)
     # the host's own file speed for the same bytes, without the library: a new file written by one
     # thread in 32 MB pwrite calls, then read back by 8 threads in 32 MB pread calls (page cache)
     import threading
@@ -840,7 +864,8 @@ def run_checkpoint(args, ws, rank, local):
     if rank == 0 and not args.no_cpu:
         import oracle
         from oracle import h5format
-        q = a.get_q()
+        from astr_gpu_b200.fields import tgv_q
+        q = tgv_q(n, 0.1)
         t0 = time.perf_counter()
         f = oracle.q2fvar(q, 0.1, 1.4)
         h5format.write(fn, [(nm, np.ascontiguousarray(f[..., m].T)) for m, nm in enumerate(("ro", "u1", "u2", "u3",
@@ -853,7 +878,6 @@ def run_checkpoint(args, ws, rank, local):
         os.remove(fn)
         cpu = {"value": 2 * fbytes / tc / 1e9, "unit": "GB/s", "cores": 1, "kind": "port",
                "sample": f"one write + one read of the {n}^3 flow field by the oracle (numpy, Python HDF5)"}
-    os.rmdir(bak)
     os.rmdir(tmp)
     if rank == 0:
         total = tw + tr
@@ -871,8 +895,6 @@ def run_checkpoint(args, ws, rank, local):
                 "gpu_launches": 4 * args.steps,
                 "clocks": clk.summary()}
         print(json.dumps(line), flush=True)
-    a.close()
-    b.close()
 
 
 def run_profile(args, local):
@@ -920,7 +942,8 @@ def main():
     ap.add_argument("--adj-size", type=int, default=128)
     ap.add_argument("--adj-steps", type=int, default=200)
     ap.add_argument("--no-single", action="store_true")
-    ap.add_argument("--no-extras", action="store_true", help="skip the adjoint and ensemble keys of the default line")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the adjoint, ensemble and checkpoint keys of the default line")
     ap.add_argument("--ens-steps", type=int, default=10)
     ap.add_argument("--profile", action="store_true", help="eager steps only, for ncu captures")
     ap.add_argument("--shapes", default="", help='pinned launch shapes, e.g. {"A": [9, 2, 8], ...}')
