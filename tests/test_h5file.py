@@ -78,6 +78,29 @@ def test_writer_emits_the_library_encodings(tmp_path):
     assert ours[0x08][0] == 3          # layout version 3, contiguous
 
 
+@needs_lib_file
+def test_rdwr_adds_to_the_library_written_file(tmp_path):
+    """h5srite's read-write step on a file the HDF5 library wrote (user block, its own heap with a
+    free block, its symbol table node): the existing dataset and its attribute stay readable and
+    the new dataset is found by both readers."""
+    import shutil
+    fn = tmp_path / "copy.mat"
+    shutil.copyfile(LIB_FILE, fn)
+    with ag.h5io_init(fn, "rdwr") as f:
+        f.write("nstep", np.array([12], dtype=np.int32))
+        f.write("time", np.array([0.25]))
+    info = h5format.read(fn)
+    assert sorted(info.entries) == ["nstep", "testdouble", "time"]
+    ref = h5format.read(LIB_FILE).entries["testdouble"]
+    assert np.array_equal(info.entries["testdouble"].data, ref.data)
+    assert info.entries["testdouble"].attrs["MATLAB_class"].tobytes() == b"double"
+    assert info.eof == os.path.getsize(fn)
+    with ag.h5io_init(fn) as f:
+        assert f.names() == ["nstep", "testdouble", "time"]
+        assert f.read("nstep", dtype=np.int32).tolist() == [12] and f.read("time").tolist() == [0.25]
+        assert np.array_equal(f.read("testdouble"), ref.data.T)
+
+
 def test_flowfield_file_written_by_the_library_matches_the_oracle(tmp_path):
     fn = tmp_path / "flowfield.h5"
     arrays = _flowfield_arrays((9, 7, 5), 1)
