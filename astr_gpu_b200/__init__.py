@@ -292,12 +292,14 @@ class H5File:
         if shape is None:
             shape = self.info(varname)[0]
         shape = tuple(int(x) for x in shape)
-        out = np.zeros(shape, dtype=np.int32 if np.dtype(dtype) == np.int32 else np.float64, order="F")
+        scalar = len(shape) == 0           # a scalar dataspace: read as one element
+        out = np.zeros(shape or (1,), dtype=np.int32 if np.dtype(dtype) == np.int32 else np.float64, order="F")
+        shape = shape or (1,)
         dims = (ctypes.c_int64 * len(shape))(*shape)
         off = None if offset is None else (ctypes.c_int64 * len(offset))(*[int(x) for x in offset])
         fn = self.L.astr_h5read_i4 if out.dtype == np.int32 else self.L.astr_h5read_r8
         self._check(fn(self._h, varname.encode(), len(shape), dims, off, mode.encode(), ctypes.c_void_p(out.ctypes.data)))
-        return out
+        return out.reshape(()) if scalar else out
 
     def close(self):
         """h5io_end (src/hdf5io.F90:149-163)."""

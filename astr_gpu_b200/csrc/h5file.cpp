@@ -97,6 +97,7 @@ struct astr_h5 {
   uint64_t base = 0;              // absolute offset of the superblock (addresses are relative to it)
   int sbver = 0;
   uint64_t eoa = 0;               // next free relative address (write / read-write)
+  uint64_t fsize = 0;             // file size when opened (bounds every metadata read)
   uint64_t root = UNDEF;
   uint64_t stab_at = UNDEF;       // absolute offset of the root symbol table message's data
   std::vector<Member> members;
@@ -127,8 +128,12 @@ void pwrite_all(const astr_h5* h, uint64_t abs, const void* buf, size_t n) {
     p += r; n -= size_t(r); abs += uint64_t(r);
   }
 }
+// Metadata (superblock, object headers, heaps, nodes) at relative address rel: it must lie inside
+// the file as opened, so a corrupt size or address fails here without a large allocation.
 std::vector<uint8_t> at(const astr_h5* h, uint64_t rel, size_t n) {
-  if (rel == UNDEF || n > (size_t(1) << 32)) bad("undefined or oversized address in " + h->path, ASTR_ERR_STATE);
+  if (rel == UNDEF || rel > h->fsize || n > h->fsize || h->base + rel + n > h->fsize)
+    bad("metadata outside the file " + h->path + " (truncated or corrupt file)", ASTR_ERR_STATE);
+  if (n > (size_t(256) << 20)) bad("metadata block larger than 256 MB in " + h->path + " (corrupt file)", ASTR_ERR_STATE);
   std::vector<uint8_t> b(n);
   if (n) pread_all(h, h->base + rel, b.data(), n);
   return b;
@@ -139,6 +144,7 @@ void superblock(astr_h5* h) {
   struct stat st{};
   if (fstat(h->fd, &st) != 0) bad("cannot stat " + h->path, ASTR_ERR_STATE);
   uint64_t size = uint64_t(st.st_size), off = 0;
+  h->fsize = size;
   uint8_t b[128] = {0};
   for (;;) {
     if (off + 8 > size) bad(h->path + " is not an HDF5 file (no signature)", ASTR_ERR_STATE);
@@ -221,9 +227,12 @@ std::vector<Msg> object_header(const astr_h5* h, uint64_t rel) {
   return out;
 }
 
+// visits counts the nodes read so far: a corrupt tree whose children point back at its own nodes
+// stops after 65536 visits instead of walking an exponential number of paths.
 void btree_members(const astr_h5* h, uint64_t node, const std::vector<uint8_t>& heap,
-                   std::vector<std::pair<std::string, uint64_t>>& out, int depth) {
+                   std::vector<std::pair<std::string, uint64_t>>& out, int depth, int& visits) {
   if (depth > 16) bad("group B-tree too deep", ASTR_ERR_STATE);
+  if (++visits > 65536 || out.size() > (size_t(1) << 20)) bad("group B-tree too large (corrupt file)", ASTR_ERR_STATE);
   std::vector<uint8_t> p = at(h, node, 24);
   if (std::memcmp(p.data(), "TREE", 4) || p[4] != 0) bad("group B-tree node", ASTR_ERR_STATE);
   int level = p[5];
@@ -231,7 +240,7 @@ void btree_members(const astr_h5* h, uint64_t node, const std::vector<uint8_t>& 
   std::vector<uint8_t> kc = at(h, node + 24, size_t(16 * n + 8));
   for (uint64_t i = 0; i < n; ++i) {
     uint64_t child = le(&kc[8 + 16 * i], 8);
-    if (level > 0) { btree_members(h, child, heap, out, depth + 1); continue; }
+    if (level > 0) { btree_members(h, child, heap, out, depth + 1, visits); continue; }
     std::vector<uint8_t> s = at(h, child, 8);
     if (std::memcmp(s.data(), "SNOD", 4)) bad("symbol table node", ASTR_ERR_STATE);
     uint64_t ns = le(&s[6], 2);
@@ -342,7 +351,7 @@ void link_members(const std::vector<Msg>& msgs, std::vector<std::pair<std::strin
     uint64_t ln = le(&d[pos], w);
     pos += size_t(w);
     if (d.size() < pos + ln + (ltype == 0 ? 8 : 0)) bad("link message", ASTR_ERR_STATE);
-    std::string name(reinterpret_cast<const char*>(&d[pos]), size_t(ln));
+    std::string name(reinterpret_cast<const char*>(d.data() + pos), size_t(ln));
     pos += ln;
     if (ltype == 0) out.emplace_back(name, le(&d[pos], 8));
   }
@@ -362,7 +371,8 @@ void read_structure(astr_h5* h) {
     std::vector<uint8_t> hp = at(h, heap_at, 32);
     if (std::memcmp(hp.data(), "HEAP", 4)) bad("local heap", ASTR_ERR_STATE);
     std::vector<uint8_t> heap = at(h, le(&hp[24], 8), size_t(le(&hp[8], 8)));
-    btree_members(h, le(m.d.data(), 8), heap, links, 0);
+    int visits = 0;
+    btree_members(h, le(m.d.data(), 8), heap, links, 0, visits);
     break;
   }
   if (!stab) link_members(rm, links);
@@ -395,9 +405,13 @@ const Member& find(const astr_h5* h, const char* name) {
   return m;
 }
 
+// Elements of a dataspace, saturating (a corrupt dataspace must not wrap around).
 uint64_t count(const std::vector<uint64_t>& dims) {
   uint64_t n = 1;
-  for (uint64_t d : dims) n *= d;
+  for (uint64_t d : dims) {
+    if (d && n > UINT64_MAX / d) return UINT64_MAX;
+    n *= d;
+  }
   return n;
 }
 
@@ -461,8 +475,13 @@ void read_block(const astr_h5* h, const char* name, int rank, const int64_t* fd,
     if (fd[d] < 0 || (off && off[d] < 0)) bad("negative dims or offset");
     n *= uint64_t(fd[d]);
   }
-  if (m.layout == 1 && m.addr != UNDEF && m.nbytes < count(m.dims) * uint64_t(m.esize))
+  if (m.layout == 1 && m.addr != UNDEF && m.nbytes / uint64_t(m.esize) < count(m.dims))
     bad(std::string("dataset '") + name + "' storage shorter than its dataspace", ASTR_ERR_STATE);
+  if (m.dims.empty()) {           // a scalar dataspace: one element
+    if (n != 1 || (off && off[0] != 0)) bad(std::string("dataset '") + name + "' is a scalar");
+    read_run(h, m, 0, 1, out);
+    return;
+  }
   if (mode == 's') {
     if (m.dims.size() != 1) bad(std::string("dataset '") + name + "' is not one-dimensional (stream mode)");
     uint64_t o = off ? uint64_t(off[0]) : 0;

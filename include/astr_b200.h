@@ -272,8 +272,9 @@ int astr_h5write_r8(astr_h5* h, const char* varname, int rank, const int64_t dim
 int astr_h5write_i4(astr_h5* h, const char* varname, int rank, const int64_t dims[], const int32_t* var);
 /* The block of Fortran shape dims at Fortran offsets offset[] (NULL: all zero) of a dataset of
  * rank `rank` (mode 'h', h5ra3d_r8_struct's hyperslab), or dims' element count from element
- * offset[0] of a one-dimensional dataset (mode 's', h5ra3d_r8_stream). Elements are converted to
- * the output type; astr_h5read_i4 takes integer datasets only. */
+ * offset[0] of a one-dimensional dataset (mode 's', h5ra3d_r8_stream); a scalar dataset reads as
+ * rank 1, dims {1}. Elements are converted to the output type; astr_h5read_i4 takes integer
+ * datasets only. */
 int astr_h5read_r8(astr_h5* h, const char* varname, int rank, const int64_t dims[], const int64_t offset[],
                    char mode, double* var);
 int astr_h5read_i4(astr_h5* h, const char* varname, int rank, const int64_t dims[], const int64_t offset[],

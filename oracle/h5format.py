@@ -433,7 +433,7 @@ def write_v2(path, datasets):
     out = bytearray(48)
     links = []
     for name, arr in datasets:
-        a = np.ascontiguousarray(arr)
+        a = np.asarray(arr, order="C")
         dims = a.shape
         space = struct.pack("<BBBB", 2, len(dims), 0, 1) + b"".join(struct.pack("<Q", d) for d in dims)
         fixed = [(0x01, 0, space), (0x03, 1, _dtype_message(a.dtype)), (0x05, 1, bytes([3, 0x0A]))]
@@ -477,7 +477,7 @@ def write(path, datasets, *, user_block=0, layout_version=3, snod_capacity=8, by
         out.extend(bytes(-len(out) % 8))
     ohs = {}
     for name, arr in datasets:
-        a = np.ascontiguousarray(arr).astype(np.dtype(arr.dtype).newbyteorder(byte_order), copy=False)
+        a = np.asarray(arr, order="C").astype(np.dtype(arr.dtype).newbyteorder(byte_order), copy=False)
         dims = a.shape
         space = struct.pack("<BBBB4x", 1, len(dims), 0, 0) + b"".join(struct.pack("<Q", d) for d in dims)
         nbytes = a.nbytes

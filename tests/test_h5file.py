@@ -131,6 +131,7 @@ def test_library_reads_oracle_written_files(tmp_path, user_block, layout_version
               ("i64", rng.integers(-2**40, 2**40, 7).astype(np.int64)),
               ("u16", rng.integers(0, 2**16, 4).astype(np.uint16)),
               ("small", np.array([2.5, -1.0])),
+              ("scalar", np.array(3.25)),
               ("empty", np.zeros((0, 3)))]
     fn = tmp_path / "o.h5"
     h5format.write(fn, items, user_block=user_block, layout_version=layout_version, snod_capacity=snod,
