@@ -388,12 +388,25 @@ int copy_fields(astr_state* st, double* dev, double* user, const int64_t* shape,
                      shape[2] == N[2] + 1;
   if (exact && dev != st->Q1) {
     const size_t bytes = 5 * ufs * sizeof(double);
+    // large pageable arrays move through pinned staging slots with several host threads
+    // (several times the rate of the driver's own staging of pageable memory)
+    const bool staged = bytes >= STAGED_MIN_BYTES && host_pageable(user);
     if (to_state) {
-      CK(cudaMemcpyAsync(st->Q1, user, bytes, cudaMemcpyHostToDevice, ctx->stream));
+      if (staged) {
+        const int rc = staged_copy(st->Q1, user, bytes, true, ctx->stream, ctx->err);
+        if (rc != ASTR_OK) return rc;
+      } else {
+        CK(cudaMemcpyAsync(st->Q1, user, bytes, cudaMemcpyHostToDevice, ctx->stream));
+      }
       CK(launch_pack(st->g, dev, st->Q1, shape, lb, 5, 1, ctx->stream));
     } else {
       CK(launch_pack(st->g, dev, st->Q1, shape, lb, 5, 0, ctx->stream));
-      CK(cudaMemcpyAsync(user, st->Q1, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+      if (staged) {
+        const int rc = staged_copy(user, st->Q1, bytes, false, ctx->stream, ctx->err);
+        if (rc != ASTR_OK) return rc;
+      } else {
+        CK(cudaMemcpyAsync(user, st->Q1, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+      }
     }
     return ASTR_OK;
   }

@@ -101,6 +101,19 @@ SlotPool& slot_pool() {
 }
 constexpr size_t SLOT_BYTES = size_t(8) << 20;
 
+int io_threads() { return (int)std::max(1u, std::min(8u, std::thread::hardware_concurrency())); }
+
+// Grows the pool to nslots slots (the caller holds P.m).
+int ensure_slots(SlotPool& P, int nslots, std::string& err) {
+  while ((int)P.buf.size() < nslots) {
+    void* b = nullptr;
+    cudaError_t e = cudaHostAlloc(&b, SLOT_BYTES, cudaHostAllocPortable);
+    if (e != cudaSuccess) return cuda_err(err, e, "pinned staging slots");
+    P.buf.push_back(static_cast<char*>(b));
+  }
+  return ASTR_OK;
+}
+
 bool file_io(int fd, char* p, size_t n, uint64_t off, bool write) {
   while (n) {
     ssize_t r = write ? ::pwrite(fd, p, n, off_t(off)) : ::pread(fd, p, n, off_t(off));
@@ -121,14 +134,9 @@ int transfer(const std::vector<Piece>& pieces, bool to_file, cudaStream_t st, st
   cudaGetDevice(&dev);
   SlotPool& P = slot_pool();
   std::lock_guard<std::mutex> hold(P.m);
-  const int nthreads = (int)std::max(1u, std::min(8u, std::thread::hardware_concurrency()));
+  const int nthreads = io_threads();
   const int nslots = 2 * nthreads;
-  while ((int)P.buf.size() < nslots) {
-    void* b = nullptr;
-    cudaError_t e = cudaHostAlloc(&b, SLOT_BYTES, cudaHostAllocPortable);
-    if (e != cudaSuccess) return cuda_err(err, e, "pinned staging slots");
-    P.buf.push_back(static_cast<char*>(b));
-  }
+  if (ensure_slots(P, nslots, err) != ASTR_OK) return ASTR_ERR_CUDA;
   std::vector<cudaEvent_t> ev(nslots, nullptr);
   for (cudaEvent_t& e : ev)
     if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) {
@@ -319,6 +327,81 @@ int flowfield_read(cudaStream_t st, double* dprims, const int64_t shape[3], cons
     *time = t;
   }
   return rc;
+}
+
+bool host_pageable(const void* p) {
+  cudaPointerAttributes a{};
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeUnregistered;
+}
+
+// Pageable host memory <-> device through the pinned slots: host thread t takes chunks t, t + T,
+// ... and alternates between its two slots. To the device it copies a chunk into a slot and queues
+// that slot's host-to-device copy, waiting for the slot's previous copy first; from the device it
+// queues the device-to-host copy of a chunk into a slot, waits for it and copies the slot out. The
+// threads' host copies overlap each other and the copy engine's transfers.
+int staged_copy(void* dst, const void* src, size_t bytes, bool to_device, cudaStream_t st, std::string& err) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  SlotPool& P = slot_pool();
+  std::lock_guard<std::mutex> hold(P.m);
+  const int nthreads = io_threads();
+  if (ensure_slots(P, 2 * nthreads, err) != ASTR_OK) return ASTR_ERR_CUDA;
+  const size_t nchunks = (bytes + SLOT_BYTES - 1) / SLOT_BYTES;
+  std::mutex em;
+  int code = ASTR_OK;
+  auto failure = [&](cudaError_t e, const char* what) {
+    std::lock_guard<std::mutex> lk(em);
+    if (code == ASTR_OK) code = cuda_err(err, e, what);
+  };
+  auto failed = [&]() {
+    std::lock_guard<std::mutex> lk(em);
+    return code != ASTR_OK;
+  };
+  auto worker = [&](int t) {
+    cudaSetDevice(dev);
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    bool busy[2] = {false, false};
+    for (int k = 0; k < 2; ++k)
+      if (cudaEventCreateWithFlags(&ev[k], cudaEventDisableTiming) != cudaSuccess) {
+        failure(cudaGetLastError(), "staging events");
+        return;
+      }
+    int k = 0;
+    for (size_t c = (size_t)t; c < nchunks && !failed(); c += (size_t)nthreads, k ^= 1) {
+      char* slot = P.buf[2 * t + k];
+      const size_t at = c * SLOT_BYTES, n = std::min(SLOT_BYTES, bytes - at);
+      cudaError_t e = cudaSuccess;
+      if (busy[k] && (e = cudaEventSynchronize(ev[k])) != cudaSuccess) { failure(e, "staged copy"); break; }
+      busy[k] = false;
+      if (to_device) {
+        std::memcpy(slot, static_cast<const char*>(src) + at, n);
+        e = cudaMemcpyAsync(static_cast<char*>(dst) + at, slot, n, cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess) e = cudaEventRecord(ev[k], st);
+        busy[k] = e == cudaSuccess;
+      } else {
+        e = cudaMemcpyAsync(slot, static_cast<const char*>(src) + at, n, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaEventRecord(ev[k], st);
+        if (e == cudaSuccess) e = cudaEventSynchronize(ev[k]);
+        if (e == cudaSuccess) std::memcpy(static_cast<char*>(dst) + at, slot, n);
+      }
+      if (e != cudaSuccess) { failure(e, "staged copy"); break; }
+    }
+    for (int j = 0; j < 2; ++j) {
+      if (busy[j]) {
+        cudaError_t e = cudaEventSynchronize(ev[j]);
+        if (e != cudaSuccess) failure(e, "staged copy");
+      }
+      if (ev[j]) cudaEventDestroy(ev[j]);
+    }
+  };
+  std::vector<std::thread> threads;
+  for (int t = 0; t < nthreads; ++t) threads.emplace_back(worker, t);
+  for (std::thread& th : threads) th.join();
+  return code;
 }
 
 }  // namespace astr

@@ -933,11 +933,29 @@ int fs_copy(astr_full* fs, double* user, const int64_t* shape, const int64_t* lb
     // through the filter's second buffer (free between calls)
     if ((size_t)(5 * ufs) > 5 * (size_t)fs->g.fs) return ffail(fs, ASTR_ERR_ARG, "host array larger than the staging buffer");
     dev = fs->qt;
-    if (to_state) FCK(cudaMemcpyAsync(dev, user, 5 * ufs * sizeof(double), cudaMemcpyHostToDevice, st));
+  }
+  // large pageable arrays move through pinned staging slots with several host threads
+  const size_t bytes = 5 * (size_t)ufs * sizeof(double);
+  const bool staged = where == ASTR_HOST && bytes >= STAGED_MIN_BYTES && host_pageable(user);
+  std::string err;
+  if (where == ASTR_HOST && to_state) {
+    if (staged) {
+      const int rc = staged_copy(dev, user, bytes, true, st, err);
+      if (rc != ASTR_OK) return ffail(fs, rc, err);
+    } else {
+      FCK(cudaMemcpyAsync(dev, user, bytes, cudaMemcpyHostToDevice, st));
+    }
   }
   k_fs_pack<<<blocks_for(5 * nodes(fs)), 256, 0, st>>>(fs->q, dev, fs->g, 1, u1, u2, ufs, uoff, to_state, 5);
   FCK(cudaGetLastError());
-  if (where == ASTR_HOST && !to_state) FCK(cudaMemcpyAsync(user, dev, 5 * ufs * sizeof(double), cudaMemcpyDeviceToHost, st));
+  if (where == ASTR_HOST && !to_state) {
+    if (staged) {
+      const int rc = staged_copy(user, dev, bytes, false, st, err);
+      if (rc != ASTR_OK) return ffail(fs, rc, err);
+    } else {
+      FCK(cudaMemcpyAsync(user, dev, bytes, cudaMemcpyDeviceToHost, st));
+    }
+  }
   FCK(cudaStreamSynchronize(st));
   return ASTR_OK;
 }

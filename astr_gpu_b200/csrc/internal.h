@@ -67,4 +67,13 @@ int flowfield_write(cudaStream_t st, const double* dprims, const int64_t shape[3
 int flowfield_read(cudaStream_t st, double* dprims, const int64_t shape[3], const char* filename, char mode,
                    int* nstep, double* time, std::string& err);
 
+// Host <-> device copies of pageable host memory (checkpoint.cu): host_pageable tells whether a
+// host pointer is ordinary (unregistered) memory; staged_copy moves `bytes` between such memory and
+// the device through the pinned staging slots with several host threads (to_device: dst is the
+// device pointer), on stream st, and returns once the copy has completed. Copies from pinned memory
+// need neither: the copy engine reads it directly.
+bool host_pageable(const void* p);
+int staged_copy(void* dst, const void* src, size_t bytes, bool to_device, cudaStream_t st, std::string& err);
+constexpr size_t STAGED_MIN_BYTES = size_t(32) << 20;   // smaller copies go through cudaMemcpyAsync
+
 }  // namespace astr

@@ -235,6 +235,22 @@ def run_ours(args, ws, rank, local):
         e2e = {"value": ws * n ** 3 * ne / te, "unit": UNIT, "h2d_bytes_per_step": qb,
                "d2h_bytes_per_step": qb + 24, "steps": ne, "call": "astr_rk3_step_host"}
         del qh
+        # the same call on an ordinary (pageable) host array, as a Python caller or a Fortran caller
+        # that does not pin its arrays passes it: the copies go through the library's pinned staging
+        qp = np.array(q, order="F", copy=True)
+        s.rk3_host(qp, dt, 1)
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(ne):
+            s.rk3_host(qp, dt, 1)
+        tp = time.perf_counter() - t0
+        tt = torch.tensor([tp], dtype=torch.float64, device=f"cuda:{local}")
+        if pg:
+            pg.all_reduce(tt, op=pg.ReduceOp.MAX)
+        tp = float(tt.item())
+        e2e["pageable"] = {"value": ws * n ** 3 * ne / tp, "unit": UNIT, "ms_per_step": 1e3 * tp / ne,
+                           "memory": "pageable numpy array (not pinned)"}
+        del qp
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:

@@ -1,0 +1,82 @@
+"""Host arrays in ordinary (pageable) memory: above 32 MB the state's upload and download move them
+through pinned staging slots with several host threads instead of the driver's own staging. The
+results must be bit for bit those of the same calls on pinned memory, for the miniapp state
+(astr_state_upload / _download / astr_rk3_step_host) and the full solver (astr_full_upload /
+_download), in both directions, at sizes that exercise whole and partial staging chunks."""
+import ctypes
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    import astr_gpu_b200 as ag
+    return ag.Context(0)
+
+
+def _pinned_like(a):
+    import torch
+    t = torch.empty(a.size, dtype=torch.float64, pin_memory=True)
+    t.numpy()[:] = a.ravel(order="F")
+    return t
+
+
+def _i64(v):
+    return (ctypes.c_int64 * 3)(*v)
+
+
+@pytest.mark.parametrize("n", [128, 161])
+def test_state_copies_and_host_step_agree_with_pinned(ctx, n):
+    import astr_gpu_b200 as ag
+    from astr_gpu_b200 import _lib
+    s = ag.TGVSolver(ctx, n)
+    s.autotune(False)
+    s.init_tgv()
+    q0 = s.get_q()                         # a pageable download (> 32 MB for both sizes)
+    assert q0.nbytes >= 32 << 20
+    pinned = _pinned_like(q0)
+    got = np.asfortranarray(pinned.numpy().reshape(q0.shape, order="F"))
+    assert np.array_equal(got, q0)         # pinned and pageable downloads agree
+    # an upload of a perturbed field from pageable memory equals the one from pinned memory
+    rng = np.random.default_rng(n)
+    q1 = np.asfortranarray(q0 * (1.0 + 1e-3 * rng.standard_normal(q0.shape)))
+    s.set_q(q1)
+    assert np.array_equal(s.get_q(), q1)
+    p1 = _pinned_like(q1)
+    shape, lb = _i64(q1.shape[:3]), _i64((0, 0, 0))
+    ctx.check(ctx.L.astr_state_upload(s._h, ctypes.c_void_p(p1.data_ptr()), shape, lb, _lib.ASTR_HOST))
+    assert np.array_equal(s.get_q(), q1)
+    # two host steps from each kind of memory
+    dt = s.cfl_dt(0.5)
+    qa = q1.copy(order="F")
+    for _ in range(2):
+        ctx.check(ctx.L.astr_rk3_step_host(s._h, ctypes.c_void_p(qa.ctypes.data), shape, lb, dt, 1, None))
+    for _ in range(2):
+        ctx.check(ctx.L.astr_rk3_step_host(s._h, ctypes.c_void_p(p1.data_ptr()), shape, lb, dt, 1, None))
+    qb = np.asfortranarray(p1.numpy().reshape(q1.shape, order="F"))
+    assert np.array_equal(qa, qb)
+    s.close()
+
+
+def test_full_solver_copies_agree_with_pinned(ctx):
+    import astr_gpu_b200 as ag
+    from astr_gpu_b200 import _lib
+    from astr_gpu_b200.fields import tgv_q
+    n = 136
+    s = ag.FullSolver(ctx, n)
+    q = tgv_q(n, 0.1)
+    assert q.nbytes >= 32 << 20
+    s.set_q(q)                             # pageable
+    a = s.get_q()                          # pageable
+    assert np.array_equal(a, q)
+    p = _pinned_like(q)
+    shape, lb = _i64(q.shape[:3]), _i64((0, 0, 0))
+    ctx.check(ctx.L.astr_full_upload(s._h, ctypes.c_void_p(p.data_ptr()), shape, lb, _lib.ASTR_HOST))
+    s.step(1e-3, 1)
+    b = s.get_q()
+    ctx.check(ctx.L.astr_full_download(s._h, ctypes.c_void_p(p.data_ptr()), shape, lb, _lib.ASTR_HOST))
+    assert np.array_equal(b, np.asfortranarray(p.numpy().reshape(q.shape, order="F")))
+    s.close()
