@@ -234,10 +234,10 @@ def run_ours(args, ws, rank, local):
         qb = 5 * (n + 1) ** 3 * 8
         e2e = {"value": ws * n ** 3 * ne / te, "unit": UNIT, "h2d_bytes_per_step": qb,
                "d2h_bytes_per_step": qb + 24, "steps": ne, "call": "astr_rk3_step_host"}
-        del qh
         # the same call on an ordinary (pageable) host array, as a Python caller or a Fortran caller
         # that does not pin its arrays passes it: the copies go through the library's pinned staging
         qp = np.array(q, order="F", copy=True)
+        del q, qh                                     # release the pinned buffer first
         s.rk3_host(qp, dt, 1)
         barrier()
         t0 = time.perf_counter()
