@@ -410,6 +410,25 @@ int copy_fields(astr_state* st, double* dev, double* user, const int64_t* shape,
     }
     return ASTR_OK;
   }
+  // Other bounds (halos in the caller's array): a large pageable array moves whole through the
+  // pinned staging slots into the stage buffers DA.. (18 fields, free between steps; never the
+  // source or target, which is Q0, R or an adjoint buffer) and is repacked on the device; on the way
+  // back only its node rows are written, so its halo entries stay as they were.
+  const size_t ubytes = 5 * ufs * sizeof(double);
+  if (ubytes >= STAGED_MIN_BYTES && 5 * ufs <= 18 * (size_t)st->g.fs && host_pageable(user)) {
+    double* stage = st->DA;
+    if (to_state) {
+      const int rc = staged_copy(stage, user, ubytes, true, ctx->stream, ctx->err);
+      if (rc != ASTR_OK) return rc;
+      CK(launch_pack(st->g, dev, stage, shape, lb, 5, 1, ctx->stream));
+    } else {
+      CK(launch_pack(st->g, dev, stage, shape, lb, 5, 0, ctx->stream));
+      const RowMask m{shape[0], shape[1], shape[2], -lb[0], N[0] - lb[0], -lb[1], N[1] - lb[1], -lb[2], N[2] - lb[2]};
+      const int rc = staged_copy(user, stage, ubytes, false, ctx->stream, ctx->err, &m);
+      if (rc != ASTR_OK) return rc;
+    }
+    return ASTR_OK;
+  }
   for (int m = 0; m < 5; ++m) {
     cudaMemcpy3DParms prm{};
     cudaPitchedPtr hp = make_cudaPitchedPtr(user + m * ufs, (size_t)shape[0] * 8, (size_t)shape[0], (size_t)shape[1]);

@@ -343,7 +343,19 @@ bool host_pageable(const void* p) {
 // that slot's host-to-device copy, waiting for the slot's previous copy first; from the device it
 // queues the device-to-host copy of a chunk into a slot, waits for it and copies the slot out. The
 // threads' host copies overlap each other and the copy engine's transfers.
-int staged_copy(void* dst, const void* src, size_t bytes, bool to_device, cudaStream_t st, std::string& err) {
+// Copies the node-row segments of elements [e0, e0 + n) from the slot to the caller's array.
+void masked_out(char* dst, const char* slot, uint64_t e0, uint64_t n, const RowMask& m) {
+  const uint64_t s0 = (uint64_t)m.s0, e1 = e0 + n;
+  for (uint64_t r = e0 / s0; r * s0 < e1; ++r) {
+    const int64_t j = (int64_t)(r % (uint64_t)m.s1), k = (int64_t)((r / (uint64_t)m.s1) % (uint64_t)m.s2);
+    if (j < m.y_lo || j > m.y_hi || k < m.z_lo || k > m.z_hi) continue;
+    const uint64_t a = std::max(e0, r * s0 + (uint64_t)m.x_lo), b = std::min(e1, r * s0 + (uint64_t)m.x_hi + 1);
+    if (a < b) std::memcpy(dst + 8 * a, slot + 8 * (a - e0), 8 * (b - a));
+  }
+}
+
+int staged_copy(void* dst, const void* src, size_t bytes, bool to_device, cudaStream_t st, std::string& err,
+                const RowMask* mask) {
   int dev = 0;
   cudaGetDevice(&dev);
   SlotPool& P = slot_pool();
@@ -386,7 +398,10 @@ int staged_copy(void* dst, const void* src, size_t bytes, bool to_device, cudaSt
         e = cudaMemcpyAsync(slot, static_cast<const char*>(src) + at, n, cudaMemcpyDeviceToHost, st);
         if (e == cudaSuccess) e = cudaEventRecord(ev[k], st);
         if (e == cudaSuccess) e = cudaEventSynchronize(ev[k]);
-        if (e == cudaSuccess) std::memcpy(static_cast<char*>(dst) + at, slot, n);
+        if (e == cudaSuccess) {
+          if (mask) masked_out(static_cast<char*>(dst), slot, at / 8, n / 8, *mask);
+          else std::memcpy(static_cast<char*>(dst) + at, slot, n);
+        }
       }
       if (e != cudaSuccess) { failure(e, "staged copy"); break; }
     }

@@ -73,7 +73,15 @@ int flowfield_read(cudaStream_t st, double* dprims, const int64_t shape[3], cons
 // device pointer), on stream st, and returns once the copy has completed. Copies from pinned memory
 // need neither: the copy engine reads it directly.
 bool host_pageable(const void* p);
-int staged_copy(void* dst, const void* src, size_t bytes, bool to_device, cudaStream_t st, std::string& err);
+// A device-to-host staged copy may be limited to the node rows of a Fortran array: element
+// ((m*s2 + k)*s1 + j)*s0 + i is copied only when x_lo <= i <= x_hi, y_lo <= j <= y_hi and
+// z_lo <= k <= z_hi, so the caller's halo entries stay as they were.
+struct RowMask {
+  int64_t s0, s1, s2;
+  int64_t x_lo, x_hi, y_lo, y_hi, z_lo, z_hi;
+};
+int staged_copy(void* dst, const void* src, size_t bytes, bool to_device, cudaStream_t st, std::string& err,
+                const RowMask* mask = nullptr);
 constexpr size_t STAGED_MIN_BYTES = size_t(32) << 20;   // smaller copies go through cudaMemcpyAsync
 
 }  // namespace astr

@@ -151,8 +151,9 @@ int astr_state_init_tgv(astr_state* st);
  * array is ignored on upload and left untouched on download). A host array of exactly those nodes
  * moves as one contiguous copy; when it is ordinary (pageable) memory of 32 MB or more, the copy
  * goes through the library's pinned staging memory (128 MB, kept once allocated, shared with the
- * checkpoint calls) with up to 8 host threads. The same holds for astr_rk3_step_host and the
- * full solver's upload and download. */
+ * checkpoint calls) with up to 8 host threads, and a pageable array with halos moves whole (only
+ * its node rows are written back). The same holds for astr_rk3_step_host and, for arrays of
+ * exactly the nodes, the full solver's upload and download. */
 int astr_state_upload(astr_state* st, const double* q, const int64_t shape[3], const int64_t lbound[3], int where);
 int astr_state_download(astr_state* st, double* q, const int64_t shape[3], const int64_t lbound[3], int where);
 /* dt such that cflcal's CFL equals `cfl` on the current state. */

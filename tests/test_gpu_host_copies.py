@@ -2,7 +2,8 @@
 through pinned staging slots with several host threads instead of the driver's own staging. The
 results must be bit for bit those of the same calls on pinned memory, for the miniapp state
 (astr_state_upload / _download / astr_rk3_step_host) and the full solver (astr_full_upload /
-_download), in both directions, at sizes that exercise whole and partial staging chunks."""
+_download), in both directions, at sizes that exercise whole and partial staging chunks; arrays
+with halos go whole to the device and come back node rows only."""
 import ctypes
 
 import numpy as np
@@ -79,4 +80,43 @@ def test_full_solver_copies_agree_with_pinned(ctx):
     b = s.get_q()
     ctx.check(ctx.L.astr_full_download(s._h, ctypes.c_void_p(p.data_ptr()), shape, lb, _lib.ASTR_HOST))
     assert np.array_equal(b, np.asfortranarray(p.numpy().reshape(q.shape, order="F")))
+    s.close()
+
+
+def test_state_halo_arrays_agree_with_pinned_and_keep_their_halos(ctx):
+    """Arrays with halos (the reference's q(-hm:im+hm, ...)): from pageable memory they go whole to
+    the device and come back node rows only; the results equal the pinned path's (pitched copies)
+    and the caller's halo entries are left as they were."""
+    import astr_gpu_b200 as ag
+    from astr_gpu_b200 import _lib
+    n, hm = 128, 5
+    s = ag.TGVSolver(ctx, n)
+    s.autotune(False)
+    s.init_tgv()
+    q0 = s.get_q()
+    full = (n + 1 + 2 * hm,) * 3 + (5,)
+    assert np.prod(full) * 8 >= 32 << 20
+    shape, lb = _i64(full[:3]), _i64((-hm, -hm, -hm))
+    inner = (slice(hm, hm + n + 1),) * 3
+    # pageable halo array: interior = q0, halos = a sentinel that must survive the download
+    qa = np.full(full, 7.0, order="F")
+    qa[inner] = q0
+    ctx.check(ctx.L.astr_state_upload(s._h, ctypes.c_void_p(qa.ctypes.data), shape, lb, _lib.ASTR_HOST))
+    assert np.array_equal(s.get_q(), q0)
+    dt = s.cfl_dt(0.5)
+    ctx.check(ctx.L.astr_rk3_step_host(s._h, ctypes.c_void_p(qa.ctypes.data), shape, lb, dt, 1, None))
+    halo = np.ones(full[:3], dtype=bool)
+    halo[inner] = False
+    assert np.all(qa[halo] == 7.0)
+    # the same step from a pinned halo array (pitched copies)
+    s.set_q(q0)
+    qp = _pinned_like(np.full(full, 7.0, order="F"))
+    qpv = qp.numpy().reshape(full, order="F")
+    qpv[inner] = q0
+    ctx.check(ctx.L.astr_rk3_step_host(s._h, ctypes.c_void_p(qp.data_ptr()), shape, lb, dt, 1, None))
+    assert np.array_equal(qa, qpv)
+    # a download into a pageable halo array leaves its halos alone
+    qd = np.full(full, -3.0, order="F")
+    ctx.check(ctx.L.astr_state_download(s._h, ctypes.c_void_p(qd.ctypes.data), shape, lb, _lib.ASTR_HOST))
+    assert np.array_equal(qd[inner], qpv[inner]) and np.all(qd[halo] == -3.0)
     s.close()
