@@ -949,11 +949,26 @@ int fs_copy(astr_full* fs, double* user, const int64_t* shape, const int64_t* lb
   k_fs_pack<<<blocks_for(5 * nodes(fs)), 256, 0, st>>>(fs->q, dev, fs->g, 1, u1, u2, ufs, uoff, to_state, 5);
   FCK(cudaGetLastError());
   if (where == ASTR_HOST && !to_state) {
+    // the staging buffer holds the caller's layout with only nodes 0..N written: an array with
+    // halos gets its node rows back and keeps its own halo entries
+    const bool exact = lb[0] == 0 && lb[1] == 0 && lb[2] == 0 && shape[0] == N[0] + 1 && shape[1] == N[1] + 1 &&
+                       shape[2] == N[2] + 1;
     if (staged) {
-      const int rc = staged_copy(user, dev, bytes, false, st, err);
+      const RowMask m{shape[0], shape[1], shape[2], -lb[0], N[0] - lb[0], -lb[1], N[1] - lb[1], -lb[2], N[2] - lb[2]};
+      const int rc = staged_copy(user, dev, bytes, false, st, err, exact ? nullptr : &m);
       if (rc != ASTR_OK) return ffail(fs, rc, err);
-    } else {
+    } else if (exact) {
       FCK(cudaMemcpyAsync(user, dev, bytes, cudaMemcpyDeviceToHost, st));
+    } else {
+      for (int m = 0; m < 5; ++m) {
+        cudaMemcpy3DParms prm{};
+        prm.srcPtr = make_cudaPitchedPtr(dev + m * ufs, (size_t)shape[0] * 8, (size_t)shape[0], (size_t)shape[1]);
+        prm.dstPtr = make_cudaPitchedPtr(user + m * ufs, (size_t)shape[0] * 8, (size_t)shape[0], (size_t)shape[1]);
+        prm.srcPos = prm.dstPos = make_cudaPos((size_t)(-lb[0]) * 8, (size_t)(-lb[1]), (size_t)(-lb[2]));
+        prm.extent = make_cudaExtent((size_t)(N[0] + 1) * 8, (size_t)N[1] + 1, (size_t)N[2] + 1);
+        prm.kind = cudaMemcpyDeviceToHost;
+        FCK(cudaMemcpy3DAsync(&prm, st));
+      }
     }
   }
   FCK(cudaStreamSynchronize(st));

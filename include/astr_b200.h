@@ -152,8 +152,8 @@ int astr_state_init_tgv(astr_state* st);
  * moves as one contiguous copy; when it is ordinary (pageable) memory of 32 MB or more, the copy
  * goes through the library's pinned staging memory (128 MB, kept once allocated, shared with the
  * checkpoint calls) with up to 8 host threads, and a pageable array with halos moves whole (only
- * its node rows are written back). The same holds for astr_rk3_step_host and, for arrays of
- * exactly the nodes, the full solver's upload and download. */
+ * its node rows are written back). The same holds for astr_rk3_step_host and the full solver's
+ * upload and download. */
 int astr_state_upload(astr_state* st, const double* q, const int64_t shape[3], const int64_t lbound[3], int where);
 int astr_state_download(astr_state* st, double* q, const int64_t shape[3], const int64_t lbound[3], int where);
 /* dt such that cflcal's CFL equals `cfl` on the current state. */
@@ -243,7 +243,8 @@ typedef struct astr_full astr_full;
 int astr_full_create(astr_ctx* ctx, const astr_params* p, astr_full** out);
 int astr_full_destroy(astr_full* fs);
 /* Conserved variables on nodes 0..N of the caller's Fortran array q(lb.., 1:5); the primitives are
- * computed from them (updatefvar). */
+ * computed from them (updatefvar). Halo entries of the caller's array are ignored on upload and
+ * left untouched on download. */
 int astr_full_upload(astr_full* fs, const double* q, const int64_t shape[3], const int64_t lbound[3], int where);
 int astr_full_download(astr_full* fs, double* q, const int64_t shape[3], const int64_t lbound[3], int where);
 /* nsteps calls of time_integration_rk (rk3) with time step dt. */

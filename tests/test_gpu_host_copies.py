@@ -120,3 +120,34 @@ def test_state_halo_arrays_agree_with_pinned_and_keep_their_halos(ctx):
     ctx.check(ctx.L.astr_state_download(s._h, ctypes.c_void_p(qd.ctypes.data), shape, lb, _lib.ASTR_HOST))
     assert np.array_equal(qd[inner], qpv[inner]) and np.all(qd[halo] == -3.0)
     s.close()
+
+
+@pytest.mark.parametrize("n", [40, 128])
+def test_full_solver_halo_downloads_keep_the_halos(ctx, n):
+    """The full solver's download into an array with halos (the reference's own q layout) writes
+    nodes 0..N only, from pageable (small and staged) and pinned memory alike."""
+    import astr_gpu_b200 as ag
+    from astr_gpu_b200 import _lib
+    from astr_gpu_b200.fields import tgv_q
+    hm = 5
+    s = ag.FullSolver(ctx, n)
+    q = tgv_q(n, 0.1)
+    full = (n + 1 + 2 * hm,) * 3 + (5,)
+    inner = (slice(hm, hm + n + 1),) * 3
+    shape, lb = _i64(full[:3]), _i64((-hm, -hm, -hm))
+    halo = np.ones(full[:3], dtype=bool)
+    halo[inner] = False
+    qa = np.full(full, 9.0, order="F")
+    qa[inner] = q
+    ctx.check(ctx.L.astr_full_upload(s._h, ctypes.c_void_p(qa.ctypes.data), shape, lb, _lib.ASTR_HOST))
+    assert np.array_equal(s.get_q(), q)
+    s.step(1e-3, 1)
+    ref = s.get_q()
+    qd = np.full(full, -2.0, order="F")
+    ctx.check(ctx.L.astr_full_download(s._h, ctypes.c_void_p(qd.ctypes.data), shape, lb, _lib.ASTR_HOST))
+    assert np.array_equal(qd[inner], ref) and np.all(qd[halo] == -2.0)
+    qp = _pinned_like(np.full(full, -4.0, order="F"))
+    ctx.check(ctx.L.astr_full_download(s._h, ctypes.c_void_p(qp.data_ptr()), shape, lb, _lib.ASTR_HOST))
+    qpv = qp.numpy().reshape(full, order="F")
+    assert np.array_equal(qpv[inner], ref) and np.all(qpv[halo] == -4.0)
+    s.close()
