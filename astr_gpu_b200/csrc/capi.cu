@@ -201,6 +201,11 @@ int line_call(astr_ctx* ctx, const astr_scheme* s, int dir, const double* f, con
     tf = ctx->stage;
     to = ctx->stage + fpad / sizeof(double);
     CK(cudaMemcpyAsync(tf, f, fb, cudaMemcpyHostToDevice, ctx->stream));
+    // an output whose range along dir reaches past the entries the kernel writes (nodes 0..dim,
+    // interfaces -1..dim) starts from the caller's values, so those entries come back unchanged
+    const int64_t wlo = interfaces ? -1 : 0;
+    if (olb[dir] < wlo || olb[dir] + osh[dir] - 1 > dim)
+      CK(cudaMemcpyAsync(to, out, ob, cudaMemcpyHostToDevice, ctx->stream));
     df_ = tf;
     dout = to;
   }

@@ -112,3 +112,30 @@ def test_device_tensors_and_mixed_bc_gradient(ctx):
         sl = [slice(HM, HM + n + 1), slice(0, n + 1), slice(HM, HM + n + 1)]
         sl[d] = slice(None)
         assert _rel(got.cpu().numpy(), ref[tuple(sl)]) <= TOL
+
+
+@pytest.mark.parametrize("direction", [0, 2])
+def test_host_output_entries_outside_the_written_range_stay(ctx, direction):
+    """A host output array whose range along the line reaches past nodes 0..dim (here the same
+    halo'd layout as the input) gets nodes 0..dim from the call and keeps its other entries."""
+    import ctypes
+    import astr_gpu_b200 as ag
+    from astr_gpu_b200 import _lib
+    dim = 64
+    shape = [7, 6, 5]
+    shape[direction] = dim + 1 + 2 * HM
+    lb = [0, 0, 0]
+    lb[direction] = -HM
+    f = _field(shape + [2], 77 + direction)
+    ref = oracle.fd_scheme_initiate("643c", 3, dim).apply3d(f, direction, lbound=lb)
+    out = np.full(f.shape, 5.5, order="F")
+    s = ag.fd_scheme_initiate(ctx, "643c", 3, dim)
+    i64 = lambda v: (ctypes.c_int64 * 3)(*v)
+    ctx.check(ctx.L.astr_deriv_lines(ctx._h, s._h, direction, ctypes.c_void_p(f.ctypes.data), i64(shape), i64(lb),
+                                     ctypes.c_void_p(out.ctypes.data), i64(shape), i64(lb), 2, 1.0, _lib.ASTR_HOST))
+    inner = [slice(None)] * 4
+    inner[direction] = slice(HM, HM + dim + 1)
+    assert _rel(out[tuple(inner)], ref) <= TOL
+    keep = np.ones(f.shape, dtype=bool)
+    keep[tuple(inner)] = False
+    assert np.all(out[keep] == 5.5)
