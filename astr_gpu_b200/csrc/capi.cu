@@ -160,6 +160,13 @@ ArrDesc fortran_desc(const int64_t* shape, const int64_t* lb) {
   return a;
 }
 
+// A host array to device memory: large pageable arrays through the pinned staging slots.
+int host_to_device(astr_ctx* ctx, double* dst, const double* src, size_t bytes) {
+  if (bytes >= STAGED_MIN_BYTES && host_pageable(src)) return staged_copy(dst, src, bytes, true, ctx->stream, ctx->err);
+  CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, ctx->stream));
+  return ASTR_OK;
+}
+
 int line_call(astr_ctx* ctx, const astr_scheme* s, int dir, const double* f, const int64_t* fsh, const int64_t* flb,
               double* out, const int64_t* osh, const int64_t* olb, int nfields, double scale, int where,
               int flags = 0) {
@@ -200,19 +207,27 @@ int line_call(astr_ctx* ctx, const astr_scheme* s, int dir, const double* f, con
     }
     tf = ctx->stage;
     to = ctx->stage + fpad / sizeof(double);
-    CK(cudaMemcpyAsync(tf, f, fb, cudaMemcpyHostToDevice, ctx->stream));
+    int rc = host_to_device(ctx, tf, f, fb);
+    if (rc != ASTR_OK) return rc;
     // an output whose range along dir reaches past the entries the kernel writes (nodes 0..dim,
     // interfaces -1..dim) starts from the caller's values, so those entries come back unchanged
     const int64_t wlo = interfaces ? -1 : 0;
-    if (olb[dir] < wlo || olb[dir] + osh[dir] - 1 > dim)
-      CK(cudaMemcpyAsync(to, out, ob, cudaMemcpyHostToDevice, ctx->stream));
+    if (olb[dir] < wlo || olb[dir] + osh[dir] - 1 > dim) {
+      rc = host_to_device(ctx, to, out, ob);
+      if (rc != ASTR_OK) return rc;
+    }
     df_ = tf;
     dout = to;
   }
   cudaError_t e = launch_line_api(s->d, dir, df_, fa, dout, oa, nfields, scale, ctx->stream, flags);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "line kernel");
   if (where == ASTR_HOST) {
-    CK(cudaMemcpyAsync(out, to, ob, cudaMemcpyDeviceToHost, ctx->stream));
+    if (ob >= STAGED_MIN_BYTES && host_pageable(out)) {
+      const int rc = staged_copy(out, to, ob, false, ctx->stream, ctx->err);
+      if (rc != ASTR_OK) return rc;
+    } else {
+      CK(cudaMemcpyAsync(out, to, ob, cudaMemcpyDeviceToHost, ctx->stream));
+    }
     CK(cudaStreamSynchronize(ctx->stream));
   }
   return ASTR_OK;

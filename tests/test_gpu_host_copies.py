@@ -151,3 +151,31 @@ def test_full_solver_halo_downloads_keep_the_halos(ctx, n):
     qpv = qp.numpy().reshape(full, order="F")
     assert np.array_equal(qpv[inner], ref) and np.all(qpv[halo] == -4.0)
     s.close()
+
+
+def test_line_calls_on_large_pageable_arrays_agree_with_pinned(ctx):
+    """astr_deriv_lines / astr_filter_lines on a host field of more than 32 MB: the staged copies
+    of a pageable array give the pinned array's result bit for bit."""
+    import torch
+    import astr_gpu_b200 as ag
+    from astr_gpu_b200 import _lib
+    dim, hm = 256, 5
+    shape = (dim + 1, dim + 1 + 2 * hm, 70)
+    lb = (0, -hm, 0)
+    f = np.asfortranarray(np.random.default_rng(3).standard_normal(shape))
+    assert f.nbytes >= 32 << 20
+    i64 = lambda v: (ctypes.c_int64 * 3)(*v)
+    oshape = (dim + 1, dim + 1, 70)
+    for make, call in ((lambda: ag.fd_scheme_initiate(ctx, "643c", 4, dim), ctx.L.astr_deriv_lines),
+                       (lambda: ag.compact_filter_initiate(ctx, 4, dim), ctx.L.astr_filter_lines)):
+        sch = make()
+        a = np.zeros(oshape, order="F")
+        args = (ctx._h, sch._h, 1, ctypes.c_void_p(f.ctypes.data), i64(shape), i64(lb), ctypes.c_void_p(a.ctypes.data),
+                i64(oshape), i64((0, 0, 0)), 1)
+        ctx.check(call(*args, 1.0, _lib.ASTR_HOST) if call is ctx.L.astr_deriv_lines else call(*args, _lib.ASTR_HOST))
+        fp = torch.from_numpy(f.ravel(order="F")).pin_memory()
+        bp = torch.zeros(int(np.prod(oshape)), dtype=torch.float64).pin_memory()
+        args = (ctx._h, sch._h, 1, ctypes.c_void_p(fp.data_ptr()), i64(shape), i64(lb), ctypes.c_void_p(bp.data_ptr()),
+                i64(oshape), i64((0, 0, 0)), 1)
+        ctx.check(call(*args, 1.0, _lib.ASTR_HOST) if call is ctx.L.astr_deriv_lines else call(*args, _lib.ASTR_HOST))
+        assert np.array_equal(a, bp.numpy().reshape(oshape, order="F"))
